@@ -1,0 +1,349 @@
+"""Benchmark: site*energy RGF updates/s of the NEGF induced-charge pass.
+
+Workload (one step = one full induced-charge pass over resident inputs):
+  (17,0) CNT, 1000 unit cells -> N = 4000 sites, M = 8 lowest distinct modes,
+  E = 4096 energies = 1024 equilibrium-contour points (Gauss-Legendre 256 + 256
+  line, 512 arc) + 3072 real-axis points uniform on [-1.5, 1.5] eV with
+  eta = 1e-4 eV; contacts mu = (0, -0.5) eV at 300 K; site potential = seeded
+  sum of 5 Gaussian bumps (amplitude U(-0.4, 0.4) V, width U(2, 10) nm) plus a
+  0-0.5 V linear ramp.  Updates per pass = N * M * E = 131,072,000.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp64|mixed]
+
+Multi-GPU (torchrun, one rank per GPU): every rank integrates its own tube
+(independent objects, weak scaling, no collective in the data path); the step
+time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_UNITCELLS = 1000
+N_MODES = 8
+EQ_PTS = (256, 256, 512)
+RT_PTS = 3072
+ETA = 1e-4
+MU = (0.0, -0.5)
+TEMP = (300.0, 300.0)
+SEED = 20261203 + 2
+FLOP_CONTOUR = 53  # per contour update: forward 15 + backward 15 + G_nn 15 + accumulate 8
+FLOP_REALAXIS = 76  # + two running products 12, two |G|^2 Gamma f terms 8, accumulate 3
+WORKLOAD = (f"mode-space RGF induced-charge pass: (17,0) CNT N={4 * N_UNITCELLS} sites, M={N_MODES} modes, "
+            f"E={sum(EQ_PTS) + RT_PTS} energies ({sum(EQ_PTS)} contour GL + {RT_PTS} real-axis uniform on "
+            f"[-1.5,1.5] eV, eta={ETA} eV), mu=(0,-0.5) eV, 300 K")
+
+
+def tube_kwargs(precision="fp64"):
+    return dict(type_id=(17, 0), num_unitcells=N_UNITCELLS, num_modes=N_MODES, contact_mu=MU, contact_T=TEMP,
+                eq_integration_pts=EQ_PTS, E_zPlus_imag=ETA, realaxis_window=(-1.5, 1.5, RT_PTS, 0),
+                precision=precision)
+
+
+def site_potential(y_nm, seed):
+    """Seeded sum of 5 Gaussian bumps + linear ramp 0-0.5 V (as U in eV = -phi)."""
+    rng = np.random.default_rng(seed)
+    L = y_nm[-1] - y_nm[0]
+    U = np.zeros_like(y_nm)
+    for _ in range(5):
+        A = rng.uniform(-0.4, 0.4)
+        w = rng.uniform(2.0, 10.0)
+        c = rng.uniform(0.0, L)
+        U += A * np.exp(-((y_nm - y_nm[0] - c) ** 2) / (2 * w * w))
+    return U + 0.5 * (y_nm - y_nm[0]) / L
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_fp64_peak(torch):
+    """FP64 throughput of a cuBLAS DGEMM (8192^3, best of 5) on this GPU [TFLOP/s]."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.mm(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.mm(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def load_profile_traffic(name):
+    p = os.path.join(ROOT, "profiles", name)
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+def run_reference_arm(args, rank, world):
+    """Reference arm: the reference path's CPU implementation (oracle port,
+    faithful walk) on the host cores, each step a bounded strided sample."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build()
+    kw = tube_kwargs()
+    kw.pop("precision")
+    t = O.OracleTube(**kw)
+    y = ring_positions_nm(N_UNITCELLS)
+    U = site_potential(y, SEED)
+    t.set_potential(U, (U[0], U[-1]))
+    threads = len(os.sched_getaffinity(0))
+    stride = 512
+    for i in range(args.warmup):
+        t.sample(stride, i % stride, faithful=True, nthreads=threads)
+    tot_upd, tot_t = 0, 0.0
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        _, n = t.sample(stride, (args.warmup + i) % stride, faithful=True, nthreads=threads)
+        tot_t += time.perf_counter() - t0
+        tot_upd += n
+    v = tot_upd / tot_t
+    sample = (f"every {stride}th of the 4096 energy points per step (8 points incl. contour and real-axis, all 8 "
+              f"modes, N=4000), faithful O(N)-per-site contact walk as in NEGF_Common.cpp:3418-3426")
+    line = {"impl": "reference", "metric": "site*energy RGF updates/s", "value": v, "unit": "updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp64", "implementation": "oracle port of the reference "
+                       "CPU path (reference not buildable here: AMReX and MPI absent)"},
+            "cpu_baseline": {"value": v, "unit": "updates/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ring_positions_nm(unitcells, acc=1.42e-10):
+    """Axial ring positions [nm] of a zigzag tube (CNT.cpp:93-132)."""
+    y0 = -(unitcells / 2.0) * 3.0 * acc - acc / 2.0
+    ring = np.array([acc, 1.5 * acc, 2.5 * acc, 3.0 * acc])
+    r = np.arange(4 * unitcells)
+    return (ring[r % 4] + 3 * acc * (r // 4) + y0) / 1e-9
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from electrostatic_b200 import build
+    build.build()
+    from electrostatic_b200.negf import CNT, compute_charge, last_stats, set_timing
+
+    tube = CNT(**tube_kwargs(args.precision))
+    y = tube.site_positions()
+    U = site_potential(y, SEED + rank)
+    Uc = (U[0], U[-1])
+    tube.set_potential(U, Uc)
+    N = tube.num_field_sites
+    Q = torch.zeros(N, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        compute_charge([tube], out=Q, stream=stream)
+    torch.cuda.synchronize()
+
+    # ---- timed: K passes over resident inputs, L2 flushed between passes
+    set_timing(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    rgf_ms, red_ms = [], []
+    barrier()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            compute_charge([tube], out=Q, stream=stream)
+            ev[i][1].record(stream)
+            st = last_stats()  # waits for this pass's kernel events
+            rgf_ms.append(st["rgf_kernel_ms"])
+            red_ms.append(st["reduce_kernel_ms"])
+        barrier()
+    set_timing(False)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_local = float(np.sum(step_ms))
+    t_all = torch.tensor([t_local], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
+    t_max = float(t_all.item())
+    updates = st["updates"]
+    value = updates * world * args.steps / (t_max * 1e-3)
+
+    # ---- end to end through the C-ABI with host buffers (H2D of U, D2H of Q)
+    U_pinned = torch.from_numpy(U).pin_memory()
+    Uh = U_pinned.numpy()
+    e2e_ev = []
+    barrier()
+    for i in range(args.steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        s.record(stream)
+        tube.set_potential(Uh, Uc)
+        Qh = compute_charge([tube], stream=stream)
+        e.record(stream)
+        e2e_ev.append((s, e))
+    barrier()
+    e2e_local = float(np.sum([s.elapsed_time(e) for s, e in e2e_ev]))
+    e2e_all = torch.tensor([e2e_local], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(e2e_all, op=dist.ReduceOp.MAX)
+    e2e_value = updates * world * args.steps / (float(e2e_all.item()) * 1e-3)
+    assert np.all(np.isfinite(Qh))
+
+    # ---- roofline of the dominant kernel (the RGF sweep kernel)
+    flops = st["contour_updates"] * FLOP_CONTOUR + st["realaxis_updates"] * FLOP_REALAXIS
+    k_ms = float(np.mean(rgf_ms))
+    achieved_tf = flops / (k_ms * 1e-3) / 1e12
+    peak_tf = measured_fp64_peak(torch) if rank == 0 else None
+    prof = load_profile_traffic("rgf_kernel_config2_ncu.json") or {}
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    scratch_gbs = st["checkpoint_bytes"] / (k_ms * 1e-3) / 1e9
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            from oracle import oracle as O
+            O.build()
+            kw = tube_kwargs()
+            kw.pop("precision")
+            ot = O.OracleTube(**kw)
+            ot.set_potential(U, Uc)
+            threads = len(os.sched_getaffinity(0))
+            t0 = time.perf_counter()
+            _, n = ot.sample(512, 0, faithful=True, nthreads=threads)
+            dt = time.perf_counter() - t0
+            cpu = {"value": n / dt, "unit": "updates/s", "cores": threads, "kind": "port",
+                   "sample": "8 of the 4096 energy points (every 512th: 2 contour + 6 real-axis), all 8 modes, "
+                             "N=4000, faithful O(N)-per-site contact walk (NEGF_Common.cpp:3418-3426), "
+                             f"{threads} threads over energies; {dt:.2f} s"}
+        roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                "frac": achieved_tf / peak_tf if peak_tf else None,
+                "traffic": prof.get("dram_bytes_per_launch"),
+                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)",
+                "flops_per_launch": flops, "kernel_ms": k_ms,
+                "flop_convention": "complex add 2, mul 6, real*complex 2, div 11, |z|^2 3; "
+                                   f"{FLOP_CONTOUR}/contour update, {FLOP_REALAXIS}/real-axis update",
+                "hbm": {"scratch_bytes_per_launch": st["checkpoint_bytes"], "achieved_gbs": scratch_gbs,
+                        "peak_gbs": hbm_peak, "frac": scratch_gbs / hbm_peak}}
+        line = {"metric": "site*energy RGF updates/s", "value": value, "unit": "updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+                "data": "synthetic (seeded potential; no dataset)",
+                "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
+                           "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
+                           "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
+                "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
+                        "d2h_bytes_per_step": 8 * N,
+                        "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},
+                "gpu_launches": 2 * args.steps, "clocks": clk.summary(),
+                "kernel_ms_per_pass": {"rgf": k_ms, "reduce": float(np.mean(red_ms))}}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+"""ctypes binding of libnegf_b200.so (declarations of include/negf_b200.h).
+
+Loading fails loudly when the library has not been built: the package has no
+CPU fallback for any compute call.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libnegf_b200.so")
+
+NEGF_OK = 0
+NEGF_PREC_FP64 = 0
+NEGF_PREC_MIXED = 1
+NEGF_NORM_ABSOLUTE = 0
+NEGF_NORM_RELATIVE = 1
+NEGF_MAX_NONEQ_PATHS = 8
+
+# Every symbol include/negf_b200.h declares (checked by the CPU test suite).
+EXPORTED = [
+    "negf_tube_desc_init", "negf_tube_create", "negf_tube_destroy", "negf_tube_num_sites", "negf_tube_modes",
+    "negf_tube_site_positions", "negf_tube_set_potential", "negf_tube_set_potential_device",
+    "negf_tube_potential_device_ptr", "negf_tube_set_contact_mu", "negf_tube_energy_points",
+    "negf_desc_energy_points", "negf_tube_noneq",
+    "negf_tube_total_integration_pts", "negf_tube_set_energy_shard", "negf_shard_range", "negf_compute_charge",
+    "negf_last_stats", "negf_set_timing", "negf_broyden_create", "negf_broyden_destroy", "negf_broyden_set_input",
+    "negf_broyden_step", "negf_broyden_reset", "negf_broyden_step_number", "negf_broyden_input_device_ptr",
+    "negf_affine_potential", "negf_write_step", "negf_last_error",
+]
+
+
+class TubeDesc(C.Structure):
+    _fields_ = [
+        ("type_id", C.c_int * 2),
+        ("num_unitcells", C.c_int),
+        ("num_modes", C.c_int),
+        ("acc", C.c_double),
+        ("gamma", C.c_double),
+        ("contact_T", C.c_double * 2),
+        ("contact_mu", C.c_double * 2),
+        ("eq_integration_pts", C.c_int * 3),
+        ("num_noneq_paths", C.c_int),
+        ("noneq_integration_pts", C.c_int * NEGF_MAX_NONEQ_PATHS),
+        ("noneq_percent_intercuts", C.c_double * NEGF_MAX_NONEQ_PATHS),
+        ("E_valence_min", C.c_double),
+        ("E_pole_max", C.c_double),
+        ("E_zPlus_imag", C.c_double),
+        ("Fermi_tail_factors", C.c_double * 2),
+        ("use_decimation", C.c_int),
+        ("decimation_max_iter", C.c_int),
+        ("decimation_layers", C.c_int),
+        ("realaxis_min", C.c_double),
+        ("realaxis_max", C.c_double),
+        ("realaxis_pts", C.c_int),
+        ("realaxis_kind", C.c_int),
+        ("precision", C.c_int),
+        ("mixed_fp64_band", C.c_double),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("rgf_kernel_ms", C.c_double),
+        ("reduce_kernel_ms", C.c_double),
+        ("updates", C.c_longlong),
+        ("updates_fp32", C.c_longlong),
+        ("contour_updates", C.c_longlong),
+        ("realaxis_updates", C.c_longlong),
+        ("chains", C.c_int),
+        ("warps", C.c_int),
+        ("kernel_launches", C.c_int),
+        ("checkpoint_bytes", C.c_longlong),
+    ]
+
+
+class NEGFError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load():
+    """Load libnegf_b200.so (build it first with electrostatic_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise NEGFError(f"{LIB_PATH} is missing: build it with `python -m electrostatic_b200.build` "
+                        "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+    sig = {
+        "negf_tube_desc_init": [C.POINTER(TubeDesc)],
+        "negf_tube_create": [C.POINTER(TubeDesc), C.POINTER(vp)],
+        "negf_tube_destroy": [vp],
+        "negf_tube_num_sites": [vp, ip],
+        "negf_tube_modes": [vp, ip, ip, ip, dp],
+        "negf_tube_site_positions": [vp, dp],
+        "negf_tube_set_potential": [vp, dp, C.c_int, dp],
+        "negf_tube_set_potential_device": [vp, vp, C.c_int, dp, vp],
+        "negf_tube_potential_device_ptr": [vp, C.POINTER(vp)],
+        "negf_tube_set_contact_mu": [vp, dp],
+        "negf_tube_energy_points": [vp, C.c_int, dp, ip],
+        "negf_desc_energy_points": [C.POINTER(TubeDesc), C.c_int, dp, ip],
+        "negf_tube_noneq": [vp, ip],
+        "negf_tube_total_integration_pts": [vp, ip],
+        "negf_tube_set_energy_shard": [vp, C.c_int, C.c_int],
+        "negf_shard_range": [C.c_int, C.c_int, C.c_int, ip, ip],
+        "negf_compute_charge": [C.POINTER(vp), C.c_int, vp, C.c_int, vp],
+        "negf_last_stats": [C.POINTER(Stats)],
+        "negf_set_timing": [C.c_int],
+        "negf_broyden_create": [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(vp)],
+        "negf_broyden_destroy": [vp],
+        "negf_broyden_set_input": [vp, vp, C.c_int, vp],
+        "negf_broyden_step": [vp, vp, vp, vp, dp, ip, vp],
+        "negf_broyden_reset": [vp, C.c_int, C.c_double, vp],
+        "negf_broyden_step_number": [vp, ip],
+        "negf_broyden_input_device_ptr": [vp, C.POINTER(vp)],
+        "negf_affine_potential": [vp, vp, vp, vp, C.c_int, vp],
+        "negf_write_step": [vp, C.c_char_p, dp, dp],
+        "negf_last_error": [],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.negf_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != NEGF_OK:
+        msg = load().negf_last_error().decode(errors="replace")
+        raise NEGFError(f"{what} failed ({rc}): {msg}")

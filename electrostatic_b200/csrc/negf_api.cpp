@@ -1,0 +1,1020 @@
+// Host layer of the B200 NEGF engine: the C-ABI declared in include/negf_b200.h.
+//
+// Mirrors the charge-path interface of c_NEGF_Common<T> / c_CNT
+// (Source/Solver/Transport/NEGF/NEGF_Common.H:518-606, CNT.H:13-103) and the
+// Broyden interface of c_TransportSolver (Transport.H:203-208).  Physics set-up
+// (modes, Hamiltonian constants, energy limits, integration paths, Fermi
+// factors) runs here in FP64; every per-site, per-energy operation runs in the
+// CUDA kernels of negf_rgf.cu / negf_broyden.cu.  There is no CPU compute path.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/negf_b200.h"
+#include "negf_internal.h"
+
+using cplx = std::complex<double>;
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kKbEvPerK = 8.617333262e-5;  // Utils/SelectWarpXUtils/WarpXConst.H:61-62
+constexpr double kSpinDegen = 2.0;            // NEGF_Common.H:351
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define NEGF_CUDA(call)                                                                             \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(NEGF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+    } while (0)
+
+// ------------------------------------------------------------------ quadrature
+// Gauss-Legendre nodes/weights on [-1, 1] by Newton iteration on P_n from the
+// Chebyshev-like initial guess cos(pi (i - 1/4) / (n + 1/2)), stopping when the
+// Newton step is below 3e-11 -- the published "gauleg" scheme that
+// Utils/CodeUtils/CodeUtil.cpp:640-690 uses, so the energy grids coincide.
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    for (int i = 1; i <= (n + 1) / 2; ++i) {
+        double z = std::cos(kPi * (i - 0.25) / (n + 0.5)), step, dp;
+        do {
+            double p = 1.0, pm1 = 0.0;
+            for (int j = 1; j <= n; ++j) {
+                const double pm2 = pm1;
+                pm1 = p;
+                p = ((2.0 * j - 1.0) * z * pm1 - (j - 1.0) * pm2) / j;
+            }
+            dp = n * (z * p - pm1) / (z * z - 1.0);
+            step = p / dp;
+            z -= step;
+        } while (std::fabs(step) > 3.0e-11);
+        x[i - 1] = -z;
+        x[n - i] = z;
+        w[i - 1] = w[n - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+struct Pt {
+    cplx E, w, J;
+};
+
+// IntegrationPath.cpp:41-147: line (id 0) or circular arc through both end
+// points with centre on Im = Im(max) (id 1), Gauss-Legendre in the parameter.
+void gl_path(cplx a, cplx b, int n, int id, std::vector<Pt>& out) {
+    if (n <= 0) return;
+    std::vector<double> x, w;
+    gauss_legendre(n, x, w);
+    if (id == 0) {
+        const cplx half = (b - a) * 0.5, mid = (b + a) * 0.5;
+        for (int i = 0; i < n; ++i) out.push_back({half * x[i] + mid, w[i], half});
+        return;
+    }
+    const double cr = (b.real() * b.real() - a.real() * a.real() - a.imag() * a.imag()) / (2 * (b.real() - a.real()));
+    const double R = cr - b.real();
+    double t1 = std::asin(std::fabs(a.imag()) / R);
+    if (cr > a.real()) t1 = kPi - t1;
+    const double t2 = kPi;
+    for (int i = 0; i < n; ++i) {
+        const double th = (t2 - t1) * 0.5 * x[i] + (t2 + t1) * 0.5;
+        const cplx E(cr + R * std::cos(th), b.imag() + R * std::sin(th));
+        const cplx J = (t2 - t1) * 0.5 * R * std::exp(cplx(0.0, th)) * cplx(0.0, 1.0);
+        out.push_back({E, w[i], J});
+    }
+}
+
+// IntegrationPath.cpp:149-168: uniform points, weight dE, factor 1.
+void regular_path(cplx a, cplx b, int n, std::vector<Pt>& out) {
+    if (n <= 0) return;
+    if (n == 1) {
+        out.push_back({a, b - a, 1.0});
+        return;
+    }
+    const cplx dE = (b - a) / double(n - 1);
+    for (int i = 0; i < n; ++i) out.push_back({a + double(i) * dE, dE, 1.0});
+}
+
+// NEGF_Common.cpp:1790-1795
+cplx fermi(cplx EmMu, double kT) { return 1.0 / (std::exp(EmMu / kT) + 1.0); }
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t reserve(size_t b) {
+        if (b <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    template <typename T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+struct ChainTable {
+    std::vector<negf::ChainRec> chains;
+    std::vector<negf::WarpRec> warps;
+    std::vector<negf::ReduceTube> rts;
+    long long partial_doubles = 0, scratch_doubles = 0;
+    long long updates = 0, updates_fp32 = 0, contour_updates = 0, realaxis_updates = 0;
+    int max_N = 0;
+};
+
+}  // namespace
+
+struct negf_tube {
+    negf_tube_desc d;
+    int device = 0;
+    // material (CNT.cpp:23-41, 155-292)
+    double R = 0.0;
+    int rings_per_uc = 4, atoms_per_ring = 17, N = 0;
+    std::vector<int> modeJ, degen;
+    std::vector<double> beta, gaps, y_nm;
+    // potential
+    double Uc[2] = {0.0, 0.0};
+    double* d_U = nullptr;
+    double* d_zero = nullptr;
+    double* d_rho0 = nullptr;
+    // contacts / limits (NEGF_Common.cpp:1687-1787)
+    double mu[2] = {0.0, 0.0}, kT[2] = {0.0, 0.0};
+    double kT_min = 0, kT_max = 0, mu_min = 0, mu_max = 0;
+    bool noneq = false, limits_dirty = true;
+    cplx E_left, E_right, E_rightmost, E_zeta, E_eta;
+    std::vector<Pt> eq_pts, noneq_pts, rho0_pts;
+    std::vector<cplx> poles;
+    int version = 0;
+    int shard_rank = 0, shard_world = 1;
+    ~negf_tube() {
+        if (d_U) cudaFree(d_U);
+        if (d_zero) cudaFree(d_zero);
+        if (d_rho0) cudaFree(d_rho0);
+    }
+};
+
+struct negf_broyden {
+    negf::BroydenDev dev{};
+    int step = 1;
+    int device = 0;
+    ~negf_broyden() {
+        double* bufs[] = {dev.n_in, dev.n_prev, dev.F, dev.dF, dev.norm, dev.V, dev.W, dev.c, dev.sum, dev.scal, dev.part};
+        for (double* p : bufs)
+            if (p) cudaFree(p);
+    }
+};
+
+namespace {
+
+std::mutex g_mu;
+struct Workspace {
+    DevBuf tubes, chains, warps, rts, partial, scratch;
+    // cached chain table
+    std::vector<const negf_tube*> key_tubes;
+    std::vector<int> key_versions;
+    std::vector<int> key_shard;
+    ChainTable table;
+    bool table_valid = false;
+    // stats / timing
+    bool timing = false;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    negf_stats stats{};
+    bool stats_pending = false;
+    int warps_per_block = 4;
+};
+Workspace& ws() {
+    static Workspace w;
+    return w;
+}
+
+int require_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(NEGF_ERR_CUDA, std::string("no CUDA device available: ") +
+                                       (e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e)));
+    return NEGF_OK;
+}
+
+// ------------------------------------------------------------------ material
+double bandgap_of_mode(const negf_tube& t, int p) {  // CNT.cpp:155-176
+    const int m = t.d.type_id[0], n = t.d.type_id[1];
+    const double f = t.d.acc * t.d.gamma / t.R;
+    const double c[6] = {std::fabs(3.0 * p - (2 * m + n)),  std::fabs(3.0 * p - (m + 2 * n)),
+                         std::fabs(3.0 * p - (m - n)),       std::fabs(-3.0 * p + (2 * m + n)),
+                         std::fabs(-3.0 * p + (m + 2 * n)),  std::fabs(3.0 * p - (m - n))};
+    double best = f * c[0];
+    for (int i = 1; i < 6; ++i) best = std::min(best, f * c[i]);
+    return best;
+}
+
+// Sort of mode gaps.  The reference sorts with a last-element-pivot quicksort
+// (CNT.cpp:178-225) whose tie order decides which J represents a degenerate
+// pair; the same partition scheme is used so the representative J matches.
+void sort_modes(std::vector<double>& v, std::vector<int>& id, int lo, int hi) {
+    while (lo < hi) {
+        const double pivot = v[hi];
+        int j = lo;
+        for (int i = lo; i <= hi; ++i)
+            if (!(v[i] > pivot)) {
+                std::swap(v[i], v[j]);
+                std::swap(id[i], id[j]);
+                ++j;
+            }
+        const int pos = j - 1;
+        sort_modes(v, id, lo, pos - 1);
+        lo = pos + 1;
+    }
+}
+
+int setup_material(negf_tube& t) {
+    const int m = t.d.type_id[0], n = t.d.type_id[1];
+    if (m <= 0 || n < 0) return fail(NEGF_ERR_ARG, "type_id must be (m>0, n>=0)");
+    if (t.d.num_unitcells <= 0) return fail(NEGF_ERR_ARG, "num_unitcells must be > 0");
+    t.R = t.d.acc * std::sqrt(3.0 * (double(m) * m + double(n) * n + double(m) * n)) / (2.0 * kPi);
+    if (n == 0) {
+        t.rings_per_uc = 4;
+        t.atoms_per_ring = m;
+    } else {
+        t.rings_per_uc = 2;
+        t.atoms_per_ring = m - 1;
+    }
+    t.N = t.d.num_unitcells * t.rings_per_uc;
+    std::vector<double> eg(t.atoms_per_ring);
+    std::vector<int> idx(t.atoms_per_ring);
+    for (int p = 1; p <= t.atoms_per_ring; ++p) {
+        eg[p - 1] = bandgap_of_mode(t, p);
+        idx[p - 1] = p;
+    }
+    sort_modes(eg, idx, 0, t.atoms_per_ring - 1);
+    std::vector<int> J{idx[0]}, dg{1};
+    std::vector<double> gp{eg[0]};
+    for (int p = 1; p < t.atoms_per_ring; ++p) {  // distinct gaps, CNT.cpp:256-270
+        if (eg[p] - gp.back() > 1e-6) {
+            J.push_back(idx[p]);
+            gp.push_back(eg[p]);
+            dg.push_back(1);
+        } else {
+            dg.back() += 1;
+        }
+    }
+    const int M = t.d.num_modes;
+    if (M <= 0 || M > (int)J.size() || M > negf::kMaxModes)
+        return fail(NEGF_ERR_ARG, "num_modes must be in [1, " + std::to_string(std::min<int>(J.size(), negf::kMaxModes)) +
+                                      "] for this chirality");
+    for (int j = 0; j < M; ++j) {
+        t.modeJ.push_back(J[j]);
+        t.degen.push_back(dg[j]);
+        t.gaps.push_back(gp[j]);
+        t.beta.push_back(2.0 * t.d.gamma * std::cos(kPi * J[j] / m));  // CNT.cpp:288-292
+    }
+    // axial ring positions, CNT.cpp:93-132 (atom 0 of each ring), in nm
+    const double acc = t.d.acc;
+    const double y0 = -(t.d.num_unitcells / 2.0) * 3.0 * acc - acc / 2.0;
+    const double ring_y[4] = {acc, 1.5 * acc, 2.5 * acc, 3.0 * acc};
+    t.y_nm.resize(t.N);
+    for (int r = 0; r < t.N; ++r) {
+        const int uc = r / t.rings_per_uc;
+        const int k = r % t.rings_per_uc;
+        const double y = (k < 4 ? ring_y[k] : 0.0) + 3 * acc * uc + y0;
+        t.y_nm[r] = y / 1.e-9;
+    }
+    return NEGF_OK;
+}
+
+// ------------------------------------------------------------------ limits and paths
+// Define_EnergyLimits, NEGF_Common.cpp:1687-1787.
+void energy_limits(const negf_tube_desc& d, const double mu_in[2], double& kT_min, double& kT_max, double& mu_min,
+                   double& mu_max, double kT[2], bool& noneq, cplx& E_left, cplx& E_right, cplx& E_rightmost,
+                   cplx& E_zeta, cplx& E_eta, std::vector<cplx>& poles, bool window) {
+    for (int c = 0; c < 2; ++c) kT[c] = kKbEvPerK * d.contact_T[c];
+    mu_min = std::min(mu_in[0], mu_in[1]);
+    mu_max = std::max(mu_in[0], mu_in[1]);
+    kT_min = std::min(kT[0], kT[1]);
+    kT_max = std::max(kT[0], kT[1]);
+    noneq = std::fabs(mu_min - mu_max) > 1e-8 || std::fabs(kT_min - kT_max) > 0.01 || window;
+    const cplx zp(0.0, d.E_zPlus_imag);
+    E_left = d.E_valence_min + zp;
+    E_rightmost = mu_max + d.Fermi_tail_factors[1] * kT_max + zp;
+    const int num_poles = int((d.E_pole_max - kPi * kT_max) / (2.0 * kPi * kT_max) + 1);
+    poles.clear();
+    if (noneq) {
+        E_right = mu_min - d.Fermi_tail_factors[0] * kT_max + zp;
+        if (window) {
+            E_right = cplx(d.realaxis_min, d.E_zPlus_imag);
+            E_rightmost = cplx(d.realaxis_max, d.E_zPlus_imag);
+        }
+        E_zeta = cplx(E_right.real(), 2 * num_poles * kPi * kT_max);
+        E_eta = cplx(E_right.real() - 14 * kT_max, E_zeta.imag());
+    } else {
+        E_right = E_rightmost;
+        for (int p = 0; p < num_poles; ++p) poles.push_back(cplx(mu_min, kPi * kT_max * (2 * p + 1)));
+        E_zeta = cplx(E_right.real(), 2 * num_poles * kPi * kT_max);
+        const double tf = std::max(d.Fermi_tail_factors[0], d.Fermi_tail_factors[1]);
+        E_eta = cplx(mu_min - tf * kT_max, E_zeta.imag());
+    }
+}
+
+void update_paths(negf_tube& t) {
+    if (!t.limits_dirty) return;
+    const bool window = t.d.realaxis_pts > 0;
+    energy_limits(t.d, t.mu, t.kT_min, t.kT_max, t.mu_min, t.mu_max, t.kT, t.noneq, t.E_left, t.E_right,
+                  t.E_rightmost, t.E_zeta, t.E_eta, t.poles, window);
+    // Update_IntegrationPaths, NEGF_Common.cpp:2188-2250
+    t.eq_pts.clear();
+    gl_path(t.E_right, t.E_zeta, t.d.eq_integration_pts[0], 0, t.eq_pts);
+    gl_path(t.E_zeta, t.E_eta, t.d.eq_integration_pts[1], 0, t.eq_pts);
+    gl_path(t.E_eta, t.E_left, t.d.eq_integration_pts[2], 1, t.eq_pts);
+    t.noneq_pts.clear();
+    if (t.noneq) {
+        if (window) {
+            if (t.d.realaxis_kind == 0)
+                regular_path(t.E_right, t.E_rightmost, t.d.realaxis_pts, t.noneq_pts);
+            else
+                gl_path(t.E_right, t.E_rightmost, t.d.realaxis_pts, 0, t.noneq_pts);
+        } else {  // Generate_NonEq_Paths, NEGF_Common.cpp:2018-2059
+            const int np = std::max(1, t.d.num_noneq_paths);
+            std::vector<cplx> mn(np), mx(np);
+            mn[0] = t.E_right;
+            mx[np - 1] = t.E_rightmost;
+            const cplx len = t.E_rightmost - t.E_right;
+            for (int p = 0; p < np - 1; ++p) {
+                const double cut = t.d.noneq_percent_intercuts[0] < 0 ? (p + 1) * (100. / np)
+                                                                       : t.d.noneq_percent_intercuts[p];
+                mx[p] = t.E_right + (cut / 100.0) * len;
+            }
+            for (int p = 1; p < np; ++p) mn[p] = mx[p - 1];
+            for (int p = 0; p < np; ++p) gl_path(mn[p], mx[p], t.d.noneq_integration_pts[p], 0, t.noneq_pts);
+        }
+    }
+    t.limits_dirty = false;
+    t.version++;
+}
+
+// Rho0 paths: Define_IntegrationPaths (NEGF_Common.cpp:1798-1806) with the
+// limits of initialisation time (mu = 0, no window).
+void rho0_paths(negf_tube& t) {
+    const double mu0[2] = {0.0, 0.0};
+    double kT[2], kTmin, kTmax, mumin, mumax;
+    bool noneq;
+    cplx L, Rr, Rm, Z, H;
+    std::vector<cplx> poles;
+    energy_limits(t.d, mu0, kTmin, kTmax, mumin, mumax, kT, noneq, L, Rr, Rm, Z, H, poles, false);
+    t.rho0_pts.clear();
+    const cplx zp(0.0, t.d.E_zPlus_imag);
+    gl_path(zp, Z, 30, 0, t.rho0_pts);
+    gl_path(Z, H, 30, 0, t.rho0_pts);
+    gl_path(H, L, 30, 1, t.rho0_pts);
+}
+
+// ------------------------------------------------------------------ chain tables
+struct TubePass {
+    const negf_tube* t;
+    int tube_index;    // index in the launch's TubeDev array
+    long long q_off;   // offset of the tube's sites in Q
+    bool rho0_pass;    // Rho0 (zero potential) instead of the charge pass
+};
+
+void push_group(ChainTable& ct, std::vector<negf::ChainRec>& lanes, const negf_tube& t, int tube_index, int kind,
+                int fp32) {
+    if (lanes.empty()) return;
+    const negf::ChainRec pad_proto = lanes.front();
+    while (lanes.size() % negf::kWarp) {
+        negf::ChainRec p = pad_proto;
+        p.mode = -1;
+        p.cr = p.ci = p.b0 = p.b1 = 0.0;
+        lanes.push_back(p);
+    }
+    const int nw = int(lanes.size() / negf::kWarp);
+    for (int w = 0; w < nw; ++w) {
+        negf::WarpRec wr{};
+        wr.tube = tube_index;
+        wr.kind = kind;
+        wr.fp32 = fp32;
+        ct.warps.push_back(wr);
+        for (int l = 0; l < negf::kWarp; ++l) {
+            const negf::ChainRec& c = lanes[(size_t)w * negf::kWarp + l];
+            ct.chains.push_back(c);
+            if (c.mode >= 0) {
+                ct.updates += t.N;
+                if (fp32) ct.updates_fp32 += t.N;
+                if (kind == negf::kRealAxis)
+                    ct.realaxis_updates += t.N;
+                else
+                    ct.contour_updates += t.N;
+            }
+        }
+    }
+    lanes.clear();
+}
+
+// Chains of one tube.  Contour chains: Im(c G) with c = (-2/pi) w J f_eq
+// (RhoEq, NEGF_Common.cpp:3738-3754), (-2/pi) w J (Rho0, :4071-4084) or
+// -4 i kT (poles, :3934-3948).  Real-axis chains: b_k = Re((-1/pi) w J f_k)
+// (RhoNonEq, :3372-3466).  The degeneracy and Gamma_k are applied in the kernel.
+void build_tube_chains(ChainTable& ct, const TubePass& tp) {
+    const negf_tube& t = *tp.t;
+    const int M = t.d.num_modes;
+    struct Item {
+        cplx E;
+        cplx c;
+        double b0, b1;
+        int kind;
+    };
+    std::vector<Item> items;
+    if (tp.rho0_pass) {
+        for (const Pt& p : t.rho0_pts) items.push_back({p.E, (-kSpinDegen / kPi) * p.w * p.J, 0, 0, negf::kContour});
+    } else {
+        for (const Pt& p : t.eq_pts) {
+            const cplx f = fermi(p.E - t.mu_min, t.kT_min);
+            items.push_back({p.E, (-kSpinDegen / kPi) * p.w * p.J * f, 0, 0, negf::kContour});
+        }
+        for (const cplx& E : t.poles) items.push_back({E, cplx(0.0, -2 * t.kT_min * kSpinDegen), 0, 0, negf::kContour});
+        for (const Pt& p : t.noneq_pts) {
+            const cplx base = (-kSpinDegen / (2 * kPi)) * p.w * p.J;
+            const double b0 = (base * fermi(p.E - t.mu[0], t.kT[0])).real();
+            const double b1 = (base * fermi(p.E - t.mu[1], t.kT[1])).real();
+            items.push_back({p.E, 0.0, b0, b1, negf::kRealAxis});
+        }
+        int lo = 0, hi = (int)items.size();
+        negf_shard_range((int)items.size(), t.shard_rank, t.shard_world, &lo, &hi);
+        items = std::vector<Item>(items.begin() + lo, items.begin() + hi);
+    }
+    const bool mixed = t.d.precision == NEGF_PREC_MIXED && !tp.rho0_pass;
+    const double band = t.d.mixed_fp64_band;
+    std::vector<negf::ChainRec> lanes;
+    // groups: (kind, precision); the FP64 group first
+    for (int kind = 0; kind < 2; ++kind)
+        for (int fp32 = 0; fp32 < 2; ++fp32) {
+            if (fp32 && !mixed) continue;
+            for (int m = 0; m < M; ++m)
+                for (const Item& it : items) {
+                    if (it.kind != kind) continue;
+                    const int want32 = mixed && std::fabs(it.E.imag()) >= band ? 1 : 0;
+                    if (want32 != fp32) continue;
+                    negf::ChainRec c{};
+                    c.Er = it.E.real();
+                    c.Ei = it.E.imag();
+                    c.cr = it.c.real();
+                    c.ci = it.c.imag();
+                    c.b0 = it.b0;
+                    c.b1 = it.b1;
+                    c.mode = m;
+                    lanes.push_back(c);
+                }
+            push_group(ct, lanes, t, tp.tube_index, kind, fp32);
+        }
+}
+
+void build_table(ChainTable& ct, const std::vector<TubePass>& passes) {
+    ct = ChainTable();
+    // launch order: longest tubes first
+    std::vector<int> order(passes.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return passes[a].t->N > passes[b].t->N; });
+    std::vector<negf::ReduceTube> rts(passes.size());
+    long long row = 0, ck = 0;
+    for (int oi : order) {
+        const TubePass& tp = passes[oi];
+        const size_t w0 = ct.warps.size();
+        build_tube_chains(ct, tp);
+        const int N = tp.t->N;
+        negf::ReduceTube rt{};
+        rt.row_base = row;
+        rt.q_off = tp.q_off;
+        rt.N = N;
+        rt.num_rows = int(ct.warps.size() - w0);
+        rt.rho0 = (!tp.rho0_pass && tp.t->shard_rank == 0) ? tp.t->d_rho0 : nullptr;
+        for (size_t w = w0; w < ct.warps.size(); ++w) {
+            ct.warps[w].row_off = row;
+            row += N;
+            ct.warps[w].ck_off = ck;
+            ck += negf::rgf_scratch_doubles(N, ct.warps[w].kind, ct.warps[w].fp32);
+        }
+        rts[oi] = rt;
+        ct.max_N = std::max(ct.max_N, N);
+    }
+    ct.rts = rts;
+    ct.partial_doubles = row;
+    ct.scratch_doubles = ck;
+}
+
+int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<negf::TubeDev>& tdev, bool rebuild,
+                      double* d_Q, cudaStream_t stream) {
+    Workspace& W = ws();
+    ChainTable& ct = W.table;
+    if (rebuild) {
+        build_table(ct, passes);
+        NEGF_CUDA(W.chains.reserve(std::max<size_t>(1, ct.chains.size()) * sizeof(negf::ChainRec)));
+        NEGF_CUDA(W.warps.reserve(std::max<size_t>(1, ct.warps.size()) * sizeof(negf::WarpRec)));
+        NEGF_CUDA(W.rts.reserve(std::max<size_t>(1, ct.rts.size()) * sizeof(negf::ReduceTube)));
+        NEGF_CUDA(W.partial.reserve(std::max<long long>(1, ct.partial_doubles) * sizeof(double)));
+        NEGF_CUDA(W.scratch.reserve(std::max<long long>(1, ct.scratch_doubles) * sizeof(double)));
+        if (!ct.chains.empty())
+            NEGF_CUDA(cudaMemcpyAsync(W.chains.p, ct.chains.data(), ct.chains.size() * sizeof(negf::ChainRec),
+                                      cudaMemcpyHostToDevice, stream));
+        if (!ct.warps.empty())
+            NEGF_CUDA(cudaMemcpyAsync(W.warps.p, ct.warps.data(), ct.warps.size() * sizeof(negf::WarpRec),
+                                      cudaMemcpyHostToDevice, stream));
+    }
+    // the reduce table carries device pointers that can change (rho0 of a rebuilt tube)
+    for (size_t i = 0; i < passes.size(); ++i)
+        ct.rts[i].rho0 = (!passes[i].rho0_pass && passes[i].t->shard_rank == 0) ? passes[i].t->d_rho0 : nullptr;
+    NEGF_CUDA(cudaMemcpyAsync(W.rts.p, ct.rts.data(), ct.rts.size() * sizeof(negf::ReduceTube), cudaMemcpyHostToDevice,
+                              stream));
+    NEGF_CUDA(W.tubes.reserve(tdev.size() * sizeof(negf::TubeDev)));
+    NEGF_CUDA(cudaMemcpyAsync(W.tubes.p, tdev.data(), tdev.size() * sizeof(negf::TubeDev), cudaMemcpyHostToDevice,
+                              stream));
+    const int nw = (int)ct.warps.size();
+    if (W.timing) {
+        for (auto& e : W.ev)
+            if (!e) NEGF_CUDA(cudaEventCreate(&e));
+        NEGF_CUDA(cudaEventRecord(W.ev[0], stream));
+    }
+    NEGF_CUDA(negf::launch_rgf(W.tubes.as<negf::TubeDev>(), W.chains.as<negf::ChainRec>(), W.warps.as<negf::WarpRec>(),
+                               nw, W.partial.as<double>(), W.scratch.p, W.warps_per_block, stream));
+    if (W.timing) NEGF_CUDA(cudaEventRecord(W.ev[1], stream));
+    NEGF_CUDA(negf::launch_reduce(W.rts.as<negf::ReduceTube>(), (int)ct.rts.size(), ct.max_N, W.partial.as<double>(),
+                                  d_Q, stream));
+    if (W.timing) NEGF_CUDA(cudaEventRecord(W.ev[2], stream));
+    negf_stats& st = W.stats;
+    st = negf_stats{};
+    st.updates = ct.updates;
+    st.updates_fp32 = ct.updates_fp32;
+    st.contour_updates = ct.contour_updates;
+    st.realaxis_updates = ct.realaxis_updates;
+    st.chains = (int)ct.chains.size();
+    st.warps = nw;
+    st.kernel_launches = (nw > 0 ? 1 : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
+    st.checkpoint_bytes = 2 * ct.scratch_doubles * 8;
+    W.stats_pending = W.timing;
+    return NEGF_OK;
+}
+
+negf::TubeDev make_tubedev(const negf_tube& t, bool rho0_pass) {
+    negf::TubeDev d{};
+    d.U = rho0_pass ? t.d_zero : t.d_U;
+    d.N = t.N;
+    d.num_modes = t.d.num_modes;
+    d.gamma = t.d.gamma;
+    d.Uc0 = rho0_pass ? 0.0 : t.Uc[0];
+    d.Uc1 = rho0_pass ? 0.0 : t.Uc[1];
+    d.use_decimation = t.d.use_decimation;
+    d.dec_iters = t.d.decimation_max_iter + 2;
+    d.dec_layers = t.d.decimation_layers;
+    for (int m = 0; m < t.d.num_modes; ++m) {
+        d.beta[m] = t.beta[m];
+        d.degen[m] = t.degen[m];
+    }
+    return d;
+}
+
+int compute_rho0(negf_tube* t) {
+    Workspace& W = ws();
+    rho0_paths(*t);
+    std::vector<TubePass> passes{{t, 0, 0, true}};
+    std::vector<negf::TubeDev> tdev{make_tubedev(*t, true)};
+    W.table_valid = false;
+    int rc = upload_and_launch(passes, tdev, true, t->d_rho0, 0);
+    W.table_valid = false;
+    if (rc != NEGF_OK) return rc;
+    NEGF_CUDA(cudaStreamSynchronize(0));
+    return NEGF_OK;
+}
+
+void write_table(FILE* f, const std::vector<double>& pos, const double* v, int n) {
+    // Write_Table1D, NEGF_Common.cpp:4221-4254: setprecision(15), setw(35)
+    for (int i = 0; i < n; ++i) std::fprintf(f, "%35.15g%35.15g\n", pos[i], v[i]);
+}
+
+}  // namespace
+
+// ====================================================================== C-ABI
+extern "C" {
+
+const char* negf_last_error(void) { return g_err.c_str(); }
+
+int negf_tube_desc_init(negf_tube_desc* d) {
+    if (!d) return fail(NEGF_ERR_ARG, "null descriptor");
+    std::memset(d, 0, sizeof(*d));
+    d->type_id[0] = 17;
+    d->type_id[1] = 0;
+    d->num_unitcells = 100;
+    d->num_modes = 1;
+    d->acc = 1.42e-10;
+    d->gamma = 2.5;
+    d->contact_T[0] = d->contact_T[1] = 298.0;
+    d->eq_integration_pts[0] = d->eq_integration_pts[1] = d->eq_integration_pts[2] = 30;
+    d->num_noneq_paths = 1;
+    d->noneq_integration_pts[0] = 100;
+    d->noneq_percent_intercuts[0] = -1.0;
+    d->E_valence_min = -14.0;
+    d->E_pole_max = 10.0;
+    d->E_zPlus_imag = 1e-8;
+    d->Fermi_tail_factors[0] = d->Fermi_tail_factors[1] = 14.0;
+    d->use_decimation = 0;
+    d->decimation_max_iter = 30;
+    d->decimation_layers = 10;
+    d->precision = NEGF_PREC_FP64;
+    d->mixed_fp64_band = 1e-3;
+    return NEGF_OK;
+}
+
+int negf_tube_create(const negf_tube_desc* d, negf_tube** out) {
+    if (!d || !out) return fail(NEGF_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (d->num_noneq_paths < 1 || d->num_noneq_paths > NEGF_MAX_NONEQ_PATHS)
+        return fail(NEGF_ERR_ARG, "num_noneq_paths out of range");
+    for (int i = 0; i < 3; ++i)
+        if (d->eq_integration_pts[i] < 0) return fail(NEGF_ERR_ARG, "eq_integration_pts must be >= 0");
+    if (d->use_decimation && (d->decimation_layers < 2 || d->decimation_layers > 64))
+        return fail(NEGF_ERR_ARG, "decimation_layers must be in [2, 64]");
+    if (d->precision != NEGF_PREC_FP64 && d->precision != NEGF_PREC_MIXED)
+        return fail(NEGF_ERR_ARG, "unknown precision mode");
+    if (!(d->gamma > 0) || !(d->acc > 0)) return fail(NEGF_ERR_ARG, "gamma and acc must be > 0");
+    if (!(d->contact_T[0] > 0) || !(d->contact_T[1] > 0)) return fail(NEGF_ERR_ARG, "contact_T must be > 0");
+    if (d->realaxis_pts < 0 || (d->realaxis_pts > 0 && !(d->realaxis_max > d->realaxis_min)))
+        return fail(NEGF_ERR_ARG, "real-axis window needs realaxis_max > realaxis_min");
+    int rc = require_device();
+    if (rc) return rc;
+    std::unique_ptr<negf_tube> t(new negf_tube());
+    t->d = *d;
+    rc = setup_material(*t);
+    if (rc) return rc;
+    cudaGetDevice(&t->device);
+    t->mu[0] = d->contact_mu[0];
+    t->mu[1] = d->contact_mu[1];
+    NEGF_CUDA(cudaMalloc(&t->d_U, sizeof(double) * t->N));
+    NEGF_CUDA(cudaMalloc(&t->d_zero, sizeof(double) * t->N));
+    NEGF_CUDA(cudaMalloc(&t->d_rho0, sizeof(double) * t->N));
+    NEGF_CUDA(cudaMemset(t->d_U, 0, sizeof(double) * t->N));
+    NEGF_CUDA(cudaMemset(t->d_zero, 0, sizeof(double) * t->N));
+    NEGF_CUDA(cudaMemset(t->d_rho0, 0, sizeof(double) * t->N));
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        rc = compute_rho0(t.get());
+    }
+    if (rc) return rc;
+    update_paths(*t);
+    *out = t.release();
+    return NEGF_OK;
+}
+
+int negf_tube_destroy(negf_tube* t) {
+    if (t) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        ws().table_valid = false;
+        delete t;
+    }
+    return NEGF_OK;
+}
+
+int negf_tube_num_sites(const negf_tube* t, int* n) {
+    if (!t || !n) return fail(NEGF_ERR_ARG, "null argument");
+    *n = t->N;
+    return NEGF_OK;
+}
+
+int negf_tube_modes(const negf_tube* t, int* num_modes, int* J, int* degeneracy, double* beta) {
+    if (!t) return fail(NEGF_ERR_ARG, "null tube");
+    const int M = t->d.num_modes;
+    if (num_modes) *num_modes = M;
+    for (int m = 0; m < M; ++m) {
+        if (J) J[m] = t->modeJ[m];
+        if (degeneracy) degeneracy[m] = t->degen[m];
+        if (beta) beta[m] = t->beta[m];
+    }
+    return NEGF_OK;
+}
+
+int negf_tube_site_positions(const negf_tube* t, double* y) {
+    if (!t || !y) return fail(NEGF_ERR_ARG, "null argument");
+    std::copy(t->y_nm.begin(), t->y_nm.end(), y);
+    return NEGF_OK;
+}
+
+int negf_tube_set_potential(negf_tube* t, const double* U, int n, const double Uc[2]) {
+    if (!t || !U || !Uc) return fail(NEGF_ERR_ARG, "null argument");
+    if (n != t->N) return fail(NEGF_ERR_ARG, "potential has " + std::to_string(n) + " sites, tube has " + std::to_string(t->N));
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(U[i])) return fail(NEGF_ERR_NUMERIC, "non-finite potential at site " + std::to_string(i));
+    if (!std::isfinite(Uc[0]) || !std::isfinite(Uc[1])) return fail(NEGF_ERR_NUMERIC, "non-finite contact potential");
+    NEGF_CUDA(cudaMemcpy(t->d_U, U, sizeof(double) * n, cudaMemcpyHostToDevice));
+    t->Uc[0] = Uc[0];
+    t->Uc[1] = Uc[1];
+    return NEGF_OK;
+}
+
+int negf_tube_set_potential_device(negf_tube* t, const double* dU, int n, const double Uc[2], void* stream) {
+    if (!t || !dU || !Uc) return fail(NEGF_ERR_ARG, "null argument");
+    if (n != t->N) return fail(NEGF_ERR_ARG, "potential size mismatch");
+    if (!std::isfinite(Uc[0]) || !std::isfinite(Uc[1])) return fail(NEGF_ERR_NUMERIC, "non-finite contact potential");
+    if (dU != t->d_U)
+        NEGF_CUDA(cudaMemcpyAsync(t->d_U, dU, sizeof(double) * n, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    t->Uc[0] = Uc[0];
+    t->Uc[1] = Uc[1];
+    return NEGF_OK;
+}
+
+int negf_tube_potential_device_ptr(negf_tube* t, double** dU) {
+    if (!t || !dU) return fail(NEGF_ERR_ARG, "null argument");
+    *dU = t->d_U;
+    return NEGF_OK;
+}
+
+int negf_tube_set_contact_mu(negf_tube* t, const double mu[2]) {
+    if (!t || !mu) return fail(NEGF_ERR_ARG, "null argument");
+    if (!std::isfinite(mu[0]) || !std::isfinite(mu[1])) return fail(NEGF_ERR_NUMERIC, "non-finite contact mu");
+    t->mu[0] = mu[0];
+    t->mu[1] = mu[1];
+    t->limits_dirty = true;
+    return NEGF_OK;
+}
+
+int negf_tube_energy_points(negf_tube* t, int kind, double* buf, int* count) {
+    if (!t || !count) return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    if (kind == 0) rho0_paths(*t);
+    if (kind == 2) {
+        *count = (int)t->poles.size();
+        if (buf)
+            for (size_t i = 0; i < t->poles.size(); ++i) {
+                double* b = buf + 6 * i;
+                b[0] = t->poles[i].real();
+                b[1] = t->poles[i].imag();
+                b[2] = b[3] = b[4] = b[5] = 0.0;
+            }
+        return NEGF_OK;
+    }
+    const std::vector<Pt>* v = kind == 0 ? &t->rho0_pts : kind == 1 ? &t->eq_pts : kind == 3 ? &t->noneq_pts : nullptr;
+    if (!v) return fail(NEGF_ERR_ARG, "kind must be 0..3");
+    *count = (int)v->size();
+    if (buf)
+        for (size_t i = 0; i < v->size(); ++i) {
+            double* b = buf + 6 * i;
+            b[0] = (*v)[i].E.real();
+            b[1] = (*v)[i].E.imag();
+            b[2] = (*v)[i].w.real();
+            b[3] = (*v)[i].w.imag();
+            b[4] = (*v)[i].J.real();
+            b[5] = (*v)[i].J.imag();
+        }
+    return NEGF_OK;
+}
+
+int negf_desc_energy_points(const negf_tube_desc* d, int kind, double* buf, int* count) {
+    if (!d || !count) return fail(NEGF_ERR_ARG, "null argument");
+    negf_tube t;  // host-only: no device buffers are allocated
+    t.d = *d;
+    t.mu[0] = d->contact_mu[0];
+    t.mu[1] = d->contact_mu[1];
+    return negf_tube_energy_points(&t, kind, buf, count);
+}
+
+int negf_tube_noneq(negf_tube* t, int* noneq) {
+    if (!t || !noneq) return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    *noneq = t->noneq ? 1 : 0;
+    return NEGF_OK;
+}
+
+int negf_tube_total_integration_pts(negf_tube* t, int* pts) {
+    if (!t || !pts) return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    *pts = t->noneq ? (int)t->noneq_pts.size() : (int)t->eq_pts.size();
+    return NEGF_OK;
+}
+
+int negf_shard_range(int num_points, int rank, int world, int* lo, int* hi) {
+    if (!lo || !hi || world < 1 || rank < 0 || rank >= world || num_points < 0)
+        return fail(NEGF_ERR_ARG, "bad shard arguments");
+    *lo = (int)((long long)num_points * rank / world);
+    *hi = (int)((long long)num_points * (rank + 1) / world);
+    return NEGF_OK;
+}
+
+int negf_tube_set_energy_shard(negf_tube* t, int rank, int world) {
+    if (!t || world < 1 || rank < 0 || rank >= world) return fail(NEGF_ERR_ARG, "bad shard arguments");
+    t->shard_rank = rank;
+    t->shard_world = world;
+    t->version++;
+    return NEGF_OK;
+}
+
+int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q_on_device, void* stream) {
+    if (!tubes || num_tubes <= 0 || !Q) return fail(NEGF_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> lk(g_mu);
+    Workspace& W = ws();
+    std::vector<TubePass> passes;
+    std::vector<negf::TubeDev> tdev;
+    long long off = 0;
+    bool same = W.table_valid && W.key_tubes.size() == (size_t)num_tubes;
+    for (int i = 0; i < num_tubes; ++i) {
+        negf_tube* t = tubes[i];
+        if (!t) return fail(NEGF_ERR_ARG, "null tube in batch");
+        update_paths(*t);
+        passes.push_back({t, i, off, false});
+        tdev.push_back(make_tubedev(*t, false));
+        off += t->N;
+        if (same && (W.key_tubes[i] != t || W.key_versions[i] != t->version)) same = false;
+    }
+    double* dQ = Q;
+    DevBuf tmpQ;
+    if (!q_on_device) {
+        NEGF_CUDA(tmpQ.reserve(sizeof(double) * off));
+        dQ = tmpQ.as<double>();
+    }
+    int rc = upload_and_launch(passes, tdev, !same, dQ, s);
+    if (rc) {
+        W.table_valid = false;
+        return rc;
+    }
+    W.key_tubes.assign(tubes, tubes + num_tubes);
+    W.key_versions.clear();
+    for (int i = 0; i < num_tubes; ++i) W.key_versions.push_back(tubes[i]->version);
+    W.table_valid = true;
+    if (!q_on_device) {
+        NEGF_CUDA(cudaMemcpyAsync(Q, dQ, sizeof(double) * off, cudaMemcpyDeviceToHost, s));
+        NEGF_CUDA(cudaStreamSynchronize(s));
+    }
+    return NEGF_OK;
+}
+
+int negf_set_timing(int enable) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ws().timing = enable != 0;
+    return NEGF_OK;
+}
+
+int negf_last_stats(negf_stats* s) {
+    if (!s) return fail(NEGF_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_mu);
+    Workspace& W = ws();
+    if (W.stats_pending) {
+        NEGF_CUDA(cudaEventSynchronize(W.ev[2]));
+        float a = 0, b = 0;
+        NEGF_CUDA(cudaEventElapsedTime(&a, W.ev[0], W.ev[1]));
+        NEGF_CUDA(cudaEventElapsedTime(&b, W.ev[1], W.ev[2]));
+        W.stats.rgf_kernel_ms = a;
+        W.stats.reduce_kernel_ms = b;
+        W.stats_pending = false;
+    }
+    *s = W.stats;
+    return NEGF_OK;
+}
+
+// ------------------------------------------------------------------ Broyden
+int negf_broyden_create(int S, int max_step, double fraction, int norm_type, negf_broyden** out) {
+    if (!out || S <= 0 || max_step < 2) return fail(NEGF_ERR_ARG, "bad Broyden arguments");
+    if (norm_type != NEGF_NORM_ABSOLUTE && norm_type != NEGF_NORM_RELATIVE) return fail(NEGF_ERR_ARG, "bad norm type");
+    int rc = require_device();
+    if (rc) return rc;
+    std::unique_ptr<negf_broyden> b(new negf_broyden());
+    cudaGetDevice(&b->device);
+    negf::BroydenDev& d = b->dev;
+    d.S = S;
+    d.max_step = max_step;
+    d.norm_type = norm_type;
+    d.fraction = fraction;
+    d.scalar = 1.0;
+    d.nblocks = std::min(1024, (S + 255) / 256);
+    double** vec[] = {&d.n_in, &d.n_prev, &d.F, &d.dF, &d.norm, &d.sum};
+    for (double** p : vec) {
+        NEGF_CUDA(cudaMalloc(p, sizeof(double) * S));
+        NEGF_CUDA(cudaMemset(*p, 0, sizeof(double) * S));
+    }
+    NEGF_CUDA(cudaMalloc(&d.V, sizeof(double) * (size_t)S * max_step));
+    NEGF_CUDA(cudaMalloc(&d.W, sizeof(double) * (size_t)S * max_step));
+    NEGF_CUDA(cudaMemset(d.V, 0, sizeof(double) * (size_t)S * max_step));
+    NEGF_CUDA(cudaMemset(d.W, 0, sizeof(double) * (size_t)S * max_step));
+    NEGF_CUDA(cudaMalloc(&d.c, sizeof(double) * max_step));
+    NEGF_CUDA(cudaMemset(d.c, 0, sizeof(double) * max_step));
+    NEGF_CUDA(cudaMalloc(&d.scal, sizeof(double) * 4));
+    NEGF_CUDA(cudaMemset(d.scal, 0, sizeof(double) * 4));
+    NEGF_CUDA(cudaMalloc(&d.part, sizeof(double) * 3 * d.nblocks));
+    *out = b.release();
+    return NEGF_OK;
+}
+
+int negf_broyden_destroy(negf_broyden* b) {
+    delete b;
+    return NEGF_OK;
+}
+
+int negf_broyden_set_input(negf_broyden* b, const double* n_in, int on_device, void* stream) {
+    if (!b || !n_in) return fail(NEGF_ERR_ARG, "null argument");
+    NEGF_CUDA(cudaMemcpyAsync(b->dev.n_in, n_in, sizeof(double) * b->dev.S,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    if (!on_device) NEGF_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return NEGF_OK;
+}
+
+int negf_broyden_step(negf_broyden* b, const double* d_n_out, double* d_n_in_out, double* d_norm, double* max_norm,
+                      int* status, void* stream) {
+    if (!b || !d_n_out) return fail(NEGF_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (status) *status = 0;
+    if (b->step > b->dev.max_step) {  // Transport.cpp:389-393
+        if (status) *status = 1;
+        return fail(NEGF_ERR_STATE, "Broyden_Step has exceeded the Broyden_Threshold_MaxStep");
+    }
+    NEGF_CUDA(negf::broyden_norm(b->dev, d_n_out, s));
+    NEGF_CUDA(negf::broyden_update(b->dev, b->step - 1, s));
+    b->step += 1;
+    if (d_n_in_out)
+        NEGF_CUDA(cudaMemcpyAsync(d_n_in_out, b->dev.n_in, sizeof(double) * b->dev.S, cudaMemcpyDeviceToDevice, s));
+    if (d_norm)
+        NEGF_CUDA(cudaMemcpyAsync(d_norm, b->dev.norm, sizeof(double) * b->dev.S, cudaMemcpyDeviceToDevice, s));
+    if (max_norm) {
+        NEGF_CUDA(cudaMemcpyAsync(max_norm, b->dev.scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        NEGF_CUDA(cudaStreamSynchronize(s));
+        if (!std::isfinite(*max_norm)) return fail(NEGF_ERR_NUMERIC, "non-finite Broyden norm");
+    }
+    return NEGF_OK;
+}
+
+int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void* stream) {
+    if (!b) return fail(NEGF_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    negf::BroydenDev& d = b->dev;
+    if (!keep_charge) NEGF_CUDA(negf::broyden_set(d.n_in, init_value, d.S, s));
+    double* vec[] = {d.n_prev, d.F, d.dF, d.norm, d.sum};
+    for (double* p : vec) NEGF_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * d.S, s));
+    NEGF_CUDA(cudaMemsetAsync(d.V, 0, sizeof(double) * (size_t)d.S * d.max_step, s));
+    NEGF_CUDA(cudaMemsetAsync(d.W, 0, sizeof(double) * (size_t)d.S * d.max_step, s));
+    NEGF_CUDA(cudaMemsetAsync(d.c, 0, sizeof(double) * d.max_step, s));
+    b->step = 1;
+    return NEGF_OK;
+}
+
+int negf_broyden_step_number(const negf_broyden* b, int* step) {
+    if (!b || !step) return fail(NEGF_ERR_ARG, "null argument");
+    *step = b->step;
+    return NEGF_OK;
+}
+
+int negf_broyden_input_device_ptr(negf_broyden* b, double** p) {
+    if (!b || !p) return fail(NEGF_ERR_ARG, "null argument");
+    *p = b->dev.n_in;
+    return NEGF_OK;
+}
+
+int negf_affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, void* stream) {
+    if (!K || !U0 || !Q || !U || n <= 0) return fail(NEGF_ERR_ARG, "bad affine-potential arguments");
+    NEGF_CUDA(negf::affine_potential(K, U0, Q, U, n, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+
+// ------------------------------------------------------------------ output
+int negf_write_step(negf_tube* t, const char* prefix, const double* Q, const double* norm) {
+    if (!t || !prefix || !Q) return fail(NEGF_ERR_ARG, "null argument");
+    const std::string p(prefix);
+    std::vector<double> U(t->N);
+    NEGF_CUDA(cudaMemcpy(U.data(), t->d_U, sizeof(double) * t->N, cudaMemcpyDeviceToHost));
+    {
+        FILE* f = std::fopen((p + "_U.dat").c_str(), "w");  // Write_PotentialAtSites, NEGF_Common.cpp:3043-3078
+        if (!f) return fail(NEGF_ERR_IO, "cannot open " + p + "_U.dat");
+        for (int l = 0; l < t->N; ++l) std::fprintf(f, "%d%35.6g%35.6g\n", l, t->y_nm[l], U[l]);
+        std::fclose(f);
+    }
+    {
+        FILE* f = std::fopen((p + "_Qout.dat").c_str(), "w");  // Write_InducedCharge, :3094-3102
+        if (!f) return fail(NEGF_ERR_IO, "cannot open " + p + "_Qout.dat");
+        std::fprintf(f, "'axial location / (nm)', 'Induced charge per site / (e)'\n");
+        write_table(f, t->y_nm, Q, t->N);
+        std::fclose(f);
+    }
+    if (norm) {
+        FILE* f = std::fopen((p + "_norm.dat").c_str(), "w");  // Write_ChargeNorm, :3104-3112
+        if (!f) return fail(NEGF_ERR_IO, "cannot open " + p + "_norm.dat");
+        std::fprintf(f, "'axial location / (nm)', 'norm\n");
+        write_table(f, t->y_nm, norm, t->N);
+        std::fclose(f);
+    }
+    return NEGF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,199 @@
+// Broyden modified-second mixing on the device, with deterministic
+// reductions (fixed-shape block trees, fixed-order partial sums).
+//
+// Reference: Source/Solver/Transport/Broyden_Second_Parallel.cpp:213-486
+// (GPU branch; its CPU twin :9-211 defines the same arithmetic) and
+// Broyden_Parallel_General.cpp:68-355.  The reference accumulates
+// V^T x with one atomic per element (:355-365, :412-422) and finishes the
+// norms with atomics (:268-272); here each dot product is one block-level
+// tree reduction, so repeated runs are bitwise identical.
+//
+// Storage: V^T and W as [max_step][S] row-major (row `it` = iteration it),
+// so every dot product and row update is a coalesced sweep over sites.
+
+#include "negf_internal.h"
+
+namespace negf {
+namespace {
+
+constexpr int kThreads = 256;
+
+// Block reduction of (max, sum, sum) in a fixed order.
+__device__ __forceinline__ void block_reduce3(double& a, double& b, double& c) {
+    __shared__ double sh[3][kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0) {
+        sh[0][wid] = a;
+        sh[1][wid] = b;
+        sh[2][wid] = c;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        a = lane < nw ? sh[0][lane] : 0.0;
+        b = lane < nw ? sh[1][lane] : 0.0;
+        c = lane < nw ? sh[2][lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+            c += __shfl_xor_sync(0xffffffffu, c, o);
+        }
+    }
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[kThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    v = 0.0;
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        v = lane < nw ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+// Broyden_Second_Parallel.cpp:243-315: F, |F| (or relative), dF, and the
+// three scalars (max norm, sum of squares, dF^T dF) as block partials.
+__global__ void norm_kernel(BroydenDev b, const double* __restrict__ n_out) {
+    double mx = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
+        const double nin = b.n_in[s], nout = n_out[s];
+        const double Fc = nin - nout;
+        double nr, sq;
+        if (b.norm_type == 0) {
+            nr = fabs(Fc);
+            sq = Fc * Fc;
+        } else {
+            nr = fabs(Fc / (nin + nout));
+            sq = nr * nr;
+        }
+        b.norm[s] = nr;
+        const double d = Fc - b.F[s];
+        b.dF[s] = d;
+        b.F[s] = Fc;
+        b.sum[s] = 0.0;
+        mx = fmax(mx, nr);
+        s1 += sq;
+        s2 += d * d;
+    }
+    block_reduce3(mx, s1, s2);
+    if (threadIdx.x == 0) {
+        b.part[3 * blockIdx.x + 0] = mx;
+        b.part[3 * blockIdx.x + 1] = s1;
+        b.part[3 * blockIdx.x + 2] = s2;
+    }
+}
+
+__global__ void norm_finalize(BroydenDev b) {
+    if (threadIdx.x != 0) return;
+    double mx = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int i = 0; i < b.nblocks; ++i) {
+        mx = fmax(mx, b.part[3 * i]);
+        s1 += b.part[3 * i + 1];
+        s2 += b.part[3 * i + 2];
+    }
+    b.scal[0] = mx;
+    b.scal[1] = sqrt(s1);
+    b.scal[2] = s2;
+}
+
+// c[it] = sum_s V[it][s] x[s] for it = 1..rows (one block per row).
+__global__ void dots_kernel(BroydenDev b, const double* __restrict__ x, int rows) {
+    const int it = blockIdx.x + 1;
+    if (it > rows) return;
+    const double* v = b.V + (size_t)it * b.S;
+    double acc = 0.0;
+    for (int s = threadIdx.x; s < b.S; s += blockDim.x) acc += v[s] * x[s];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) b.c[it] = acc;
+}
+
+// Broyden_Second_Parallel.cpp:381-403: sum = W c (it < m), new V and W rows at m.
+__global__ void newrow_kernel(BroydenDev b, int m) {
+    const double denom = b.scal[2];
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int it = 1; it <= m - 1; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
+        const double dF = b.dF[s];
+        const double dn = b.n_in[s] - b.n_prev[s];
+        b.V[(size_t)m * b.S + s] = dF / denom;
+        b.W[(size_t)m * b.S + s] = -b.fraction * dF + dn - acc;
+    }
+}
+
+// Broyden_Second_Parallel.cpp:455-481: sum = W c (it <= m), then the new input.
+__global__ void final_kernel(BroydenDev b, int m) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int it = 1; it <= m; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
+        b.sum[s] = acc;
+        const double prev = b.n_in[s];
+        b.n_prev[s] = prev;
+        b.n_in[s] = prev - b.scalar * b.fraction * b.F[s] - b.scalar * acc;
+    }
+}
+
+__global__ void set_kernel(double* p, double v, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+// U[i] = U0[i] + sum_j K[i][j] Q[j]: one warp per row, fixed-order lane tree.
+__global__ void affine_kernel(const double* __restrict__ K, const double* __restrict__ U0,
+                              const double* __restrict__ Q, double* __restrict__ U, int n) {
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= n) return;
+    const double* k = K + (size_t)row * n;
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc += k[j] * Q[j];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) U[row] = U0[row] + acc;
+}
+
+}  // namespace
+
+cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s) {
+    norm_kernel<<<b.nblocks, kThreads, 0, s>>>(b, n_out);
+    norm_finalize<<<1, 32, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s) {
+    if (m > 0) {
+        if (m - 1 >= 1) dots_kernel<<<m - 1, kThreads, 0, s>>>(b, b.dF, m - 1);
+        newrow_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m);
+        dots_kernel<<<m, kThreads, 0, s>>>(b, b.F, m);
+    }
+    final_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m);
+    return cudaGetLastError();
+}
+
+cudaError_t broyden_set(double* p, double v, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int blocks = (n + kThreads - 1) / kThreads;
+    set_kernel<<<blocks < 1024 ? blocks : 1024, kThreads, 0, s>>>(p, v, n);
+    return cudaGetLastError();
+}
+
+cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int warps_per_block = 8;
+    affine_kernel<<<(n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, s>>>(K, U0, Q, U, n);
+    return cudaGetLastError();
+}
+
+}  // namespace negf

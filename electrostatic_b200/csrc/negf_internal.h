@@ -1,0 +1,92 @@
+// Internal declarations shared by the host layer (negf_api.cpp) and the
+// CUDA translation units (negf_rgf.cu, negf_broyden.cu).  Not part of the
+// public C-ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace negf {
+
+constexpr int kMaxModes = 32;   // distinct modes per tube kept on the device
+constexpr int kSeg = 16;        // sites per checkpoint segment of the RGF sweeps
+constexpr int kWarp = 32;
+
+// Per-tube record read by the RGF kernel (one per tube of a launch).
+struct __align__(16) TubeDev {
+    const double* U;   // site potential [N] (device)
+    int N;             // sites
+    int num_modes;
+    double gamma;      // hopping [eV]
+    double Uc0, Uc1;   // contact potentials [eV]
+    int use_decimation, dec_iters, dec_layers, pad0;
+    double beta[kMaxModes];
+    double degen[kMaxModes];
+};
+
+// One (tube, mode, energy) chain = one lane of a warp.  Kind and precision
+// are uniform over the 32 lanes of a warp (the host pads each group).
+//   contour/pole lane:  contribution Im(c * G_nn) * degen
+//   real-axis lane:     |G_nn|^2 (lambda_n Gamma_0 b0 + rho_n Gamma_1 b1) * degen
+struct __align__(16) ChainRec {
+    double Er, Ei;  // energy
+    double cr, ci;  // complex coefficient of G_nn
+    double b0, b1;  // real-axis coefficients Re(c f_k w J)
+    int mode;       // mode index (-1 for padding lanes)
+    int pad;
+};
+
+enum WarpKind : int { kContour = 0, kRealAxis = 1 };
+
+struct __align__(16) WarpRec {
+    long long row_off;   // offset of this warp's per-site partial row (doubles)
+    long long ck_off;    // offset of this warp's checkpoint scratch (elements of its precision)
+    int tube;            // index into TubeDev[]
+    int kind;            // WarpKind
+    int fp32;            // 1: recursion in complex FP32
+    int pad;
+};
+
+// Per-tube description of the reduction of warp rows into site charge.
+struct __align__(16) ReduceTube {
+    long long row_base;  // first partial row of the tube
+    long long q_off;     // offset of the tube's sites in Q
+    const double* rho0;  // per-site sum over modes of Im Rho0 (device) or null
+    int N;
+    int num_rows;        // warps of the tube
+};
+
+// RGF launch: one warp per WarpRec, lane = chain.
+cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
+                       double* d_partial, void* d_scratch, int warps_per_block, cudaStream_t stream);
+// Per-site reduction (Kahan) of warp rows, minus Rho0 when rho0 != null.
+cudaError_t launch_reduce(const ReduceTube* d_rt, int num_tubes, int max_N, const double* d_partial, double* d_Q,
+                          cudaStream_t stream);
+// Scratch elements (doubles, rounded up) needed per warp for a tube of N sites.
+long long rgf_scratch_doubles(int N, int kind, int fp32);
+int rgf_kernel_regs();  // registers per thread of the RGF kernel (0 if unknown)
+
+// Broyden kernels (negf_broyden.cu).
+struct BroydenDev {
+    int S, max_step, norm_type;
+    double fraction, scalar;
+    double* n_in;
+    double* n_prev;
+    double* F;
+    double* dF;
+    double* norm;
+    double* V;        // [max_step][S] (row it = V^T column it)
+    double* W;        // [max_step][S]
+    double* c;        // [max_step]
+    double* sum;      // [S]
+    double* scal;     // [4]: max norm, sum of squares, denominator, spare
+    double* part;     // [3 * nblocks] block partials
+    int nblocks;
+};
+cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s);
+cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s);
+cudaError_t broyden_set(double* p, double v, int n, cudaStream_t s);
+cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s);
+
+}  // namespace negf

@@ -1,0 +1,296 @@
+"""Host-side mirror of the reference's NEGF charge interface.
+
+``CNT`` follows ``c_CNT`` / ``c_NEGF_Common<T>`` (Source/Solver/Transport/NEGF/
+CNT.H:13-103, NEGF_Common.H:518-606): construction = Initialize_NEGF_Params +
+Initialize_NEGF (Hamiltonian, contacts, energy limits, paths, Rho0);
+``Solve_NEGF`` = set potential, update paths when the contact electrochemical
+potentials changed, Compute_InducedCharge.  ``Broyden`` follows the
+c_TransportSolver Broyden API (Transport.H:203-208).  Every compute call goes
+through the C-ABI of libnegf_b200.so; there is no Python or CPU compute path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+_dp = C.POINTER(C.c_double)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _ptr(x):
+    """Device pointer of a torch tensor (or an int address)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return C.c_void_p(x)
+    return C.c_void_p(x.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+class CNT:
+    """Mode-space zigzag carbon nanotube (c_CNT) on the GPU.
+
+    Keyword names follow the reference input keys: type_id, num_unitcells,
+    num_modes (BLOCK_SIZE), acc, gamma, contact_T, contact_mu,
+    eq_integration_pts, num_noneq_paths, noneq_integration_pts,
+    noneq_percent_intercuts, E_valence_min, E_pole_max, E_zPlus_imag,
+    Fermi_tail_factors, use_decimation, decimation_max_iter,
+    decimation_layers; plus realaxis_window=(min, max, pts, kind),
+    precision ("fp64" | "mixed") and mixed_fp64_band.
+    """
+
+    def __init__(self, type_id=(17, 0), num_unitcells=100, num_modes=1, acc=1.42e-10, gamma=2.5,
+                 contact_T=(298.0, 298.0), contact_mu=(0.0, 0.0), eq_integration_pts=(30, 30, 30),
+                 noneq_integration_pts=(100,), noneq_percent_intercuts=None, E_valence_min=-14.0,
+                 E_pole_max=10.0, E_zPlus_imag=1e-8, Fermi_tail_factors=(14.0, 14.0), use_decimation=0,
+                 decimation_max_iter=30, decimation_layers=10, realaxis_window=None, precision="fp64",
+                 mixed_fp64_band=1e-3):
+        L = _lib.load()
+        d = _lib.TubeDesc()
+        check(L.negf_tube_desc_init(C.byref(d)), "negf_tube_desc_init")
+        d.type_id[0], d.type_id[1] = int(type_id[0]), int(type_id[1])
+        d.num_unitcells = int(num_unitcells)
+        d.num_modes = int(num_modes)
+        d.acc = float(acc)
+        d.gamma = float(gamma)
+        d.contact_T[0], d.contact_T[1] = map(float, contact_T)
+        d.contact_mu[0], d.contact_mu[1] = map(float, contact_mu)
+        for i in range(3):
+            d.eq_integration_pts[i] = int(eq_integration_pts[i])
+        ne = list(noneq_integration_pts)
+        d.num_noneq_paths = len(ne)
+        for i, v in enumerate(ne):
+            d.noneq_integration_pts[i] = int(v)
+        if noneq_percent_intercuts is None:
+            d.noneq_percent_intercuts[0] = -1.0
+        else:
+            for i, v in enumerate(noneq_percent_intercuts):
+                d.noneq_percent_intercuts[i] = float(v)
+        d.E_valence_min = float(E_valence_min)
+        d.E_pole_max = float(E_pole_max)
+        d.E_zPlus_imag = float(E_zPlus_imag)
+        d.Fermi_tail_factors[0], d.Fermi_tail_factors[1] = map(float, Fermi_tail_factors)
+        d.use_decimation = int(use_decimation)
+        d.decimation_max_iter = int(decimation_max_iter)
+        d.decimation_layers = int(decimation_layers)
+        if realaxis_window is not None:
+            lo, hi, pts, kind = realaxis_window
+            d.realaxis_min, d.realaxis_max, d.realaxis_pts, d.realaxis_kind = float(lo), float(hi), int(pts), int(kind)
+        d.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
+        d.mixed_fp64_band = float(mixed_fp64_band)
+        self.desc = d
+        h = C.c_void_p()
+        check(L.negf_tube_create(C.byref(d), C.byref(h)), "negf_tube_create")
+        self._h = h
+        n = C.c_int()
+        check(L.negf_tube_num_sites(h, C.byref(n)), "negf_tube_num_sites")
+        self.num_field_sites = n.value
+        self.U_contact = (0.0, 0.0)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().negf_tube_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # --- geometry / modes
+    def modes(self):
+        L = _lib.load()
+        M = int(self.desc.num_modes)
+        J = (C.c_int * M)()
+        dg = (C.c_int * M)()
+        b = (C.c_double * M)()
+        m = C.c_int()
+        check(L.negf_tube_modes(self._h, C.byref(m), J, dg, b), "negf_tube_modes")
+        return np.array(J[:]), np.array(dg[:]), np.array(b[:])
+
+    def site_positions(self) -> np.ndarray:
+        y = np.zeros(self.num_field_sites)
+        check(_lib.load().negf_tube_site_positions(self._h, _dptr(y)), "negf_tube_site_positions")
+        return y
+
+    # --- potential and contacts
+    def set_potential(self, U, U_contact=None):
+        """h_U_loc_data and U_contact (default: the end-site potentials, Nanostructure.cpp:500-504)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U_contact is None:
+            U_contact = (U[0], U[-1])
+        uc = (C.c_double * 2)(*map(float, U_contact))
+        check(_lib.load().negf_tube_set_potential(self._h, _dptr(U), len(U), uc), "negf_tube_set_potential")
+        self.U_contact = tuple(U_contact)
+
+    def set_potential_device(self, U_dev, U_contact, stream=None):
+        uc = (C.c_double * 2)(*map(float, U_contact))
+        check(_lib.load().negf_tube_set_potential_device(self._h, _ptr(U_dev), self.num_field_sites, uc,
+                                                         _stream(stream)), "negf_tube_set_potential_device")
+        self.U_contact = tuple(U_contact)
+
+    def potential_device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(_lib.load().negf_tube_potential_device_ptr(self._h, C.byref(p)), "negf_tube_potential_device_ptr")
+        return p.value
+
+    def set_Contact_Electrochemical_Potential(self, mu):
+        arr = (C.c_double * 2)(*map(float, mu))
+        check(_lib.load().negf_tube_set_contact_mu(self._h, arr), "negf_tube_set_contact_mu")
+
+    set_contact_mu = set_Contact_Electrochemical_Potential
+
+    def set_energy_shard(self, rank: int, world: int):
+        check(_lib.load().negf_tube_set_energy_shard(self._h, int(rank), int(world)), "negf_tube_set_energy_shard")
+
+    # --- paths
+    def energy_points(self, kind: int):
+        """kind 0 Rho0, 1 RhoEq contour, 2 poles, 3 NonEq -> (E, w, J) complex arrays."""
+        L = _lib.load()
+        n = C.c_int()
+        check(L.negf_tube_energy_points(self._h, int(kind), None, C.byref(n)), "negf_tube_energy_points")
+        buf = np.zeros(6 * max(n.value, 1))
+        check(L.negf_tube_energy_points(self._h, int(kind), _dptr(buf), C.byref(n)), "negf_tube_energy_points")
+        b = buf[: 6 * n.value].reshape(-1, 6)
+        return b[:, 0] + 1j * b[:, 1], b[:, 2] + 1j * b[:, 3], b[:, 4] + 1j * b[:, 5]
+
+    def noneq(self) -> bool:
+        v = C.c_int()
+        check(_lib.load().negf_tube_noneq(self._h, C.byref(v)), "negf_tube_noneq")
+        return bool(v.value)
+
+    def get_Total_Integration_Pts(self) -> int:
+        v = C.c_int()
+        check(_lib.load().negf_tube_total_integration_pts(self._h, C.byref(v)), "negf_tube_total_integration_pts")
+        return v.value
+
+    # --- charge
+    def Solve_NEGF(self, U=None, U_contact=None, out=None, stream=None):
+        """Solve_NEGF (NEGF_Common.cpp:1309-1340).  Returns the induced charge
+        per site (numpy) or writes it into the device tensor `out`."""
+        if U is not None:
+            self.set_potential(U, U_contact)
+        return compute_charge([self], out=out, stream=stream)
+
+    def Compute_InducedCharge(self, out=None, stream=None):
+        return compute_charge([self], out=out, stream=stream)
+
+    def Write_Data(self, prefix: str, Q, norm=None):
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        nrm = None if norm is None else _dptr(np.ascontiguousarray(norm, dtype=np.float64))
+        check(_lib.load().negf_write_step(self._h, prefix.encode(), _dptr(Q), nrm), "negf_write_step")
+
+
+def compute_charge(tubes: Sequence[CNT], out=None, stream=None):
+    """Induced charge of a batch of tubes in one launch (Q of tube t at offset
+    sum of the previous tubes' sites).  `out`: device tensor (float64) or None
+    for a host numpy result."""
+    L = _lib.load()
+    arr = (C.c_void_p * len(tubes))(*[t.handle for t in tubes])
+    total = sum(t.num_field_sites for t in tubes)
+    if out is None:
+        Q = np.zeros(total)
+        check(L.negf_compute_charge(arr, len(tubes), Q.ctypes.data_as(C.c_void_p), 0, _stream(stream)),
+              "negf_compute_charge")
+        return Q
+    check(L.negf_compute_charge(arr, len(tubes), _ptr(out), 1, _stream(stream)), "negf_compute_charge")
+    return out
+
+
+def last_stats() -> dict:
+    s = _lib.Stats()
+    check(_lib.load().negf_last_stats(C.byref(s)), "negf_last_stats")
+    return {k: getattr(s, k) for k, _ in _lib.Stats._fields_}
+
+
+def set_timing(enable: bool):
+    check(_lib.load().negf_set_timing(int(bool(enable))), "negf_set_timing")
+
+
+def shard_range(num_points: int, rank: int, world: int):
+    lo, hi = C.c_int(), C.c_int()
+    check(_lib.load().negf_shard_range(int(num_points), int(rank), int(world), C.byref(lo), C.byref(hi)),
+          "negf_shard_range")
+    return lo.value, hi.value
+
+
+class Broyden:
+    """Broyden modified-second mixing on the device (Set_Broyden_Parallel /
+    Execute_Broyden_Modified_Second_Algorithm_Parallel / Reset_Broyden_Parallel)."""
+
+    def __init__(self, n_in, max_step=200, fraction=0.1, norm_type="absolute", stream=None):
+        L = _lib.load()
+        self.S = int(n_in.shape[0])
+        nt = _lib.NEGF_NORM_ABSOLUTE if norm_type.lower().startswith("abs") else _lib.NEGF_NORM_RELATIVE
+        h = C.c_void_p()
+        check(L.negf_broyden_create(self.S, int(max_step), float(fraction), nt, C.byref(h)), "negf_broyden_create")
+        self._h = h
+        if isinstance(n_in, np.ndarray):
+            a = np.ascontiguousarray(n_in, dtype=np.float64)
+            check(L.negf_broyden_set_input(h, a.ctypes.data_as(C.c_void_p), 0, _stream(stream)), "set_input")
+        else:
+            check(L.negf_broyden_set_input(h, _ptr(n_in), 1, _stream(stream)), "set_input")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().negf_broyden_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n_out_dev, n_in_out=None, norm_out=None, stream=None) -> float:
+        """One mixing step; returns Broyden_Norm (max residual of this input)."""
+        mx = C.c_double()
+        st = C.c_int()
+        check(_lib.load().negf_broyden_step(self._h, _ptr(n_out_dev), _ptr(n_in_out), _ptr(norm_out),
+                                            C.byref(mx), C.byref(st), _stream(stream)), "negf_broyden_step")
+        return mx.value
+
+    Execute_Broyden_Modified_Second_Algorithm_Parallel = step
+
+    def reset(self, keep_charge=False, init_value=0.0, stream=None):
+        check(_lib.load().negf_broyden_reset(self._h, int(bool(keep_charge)), float(init_value), _stream(stream)),
+              "negf_broyden_reset")
+
+    Reset_Broyden_Parallel = reset
+
+    @property
+    def step_number(self) -> int:
+        v = C.c_int()
+        check(_lib.load().negf_broyden_step_number(self._h, C.byref(v)), "negf_broyden_step_number")
+        return v.value
+
+    def input_device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(_lib.load().negf_broyden_input_device_ptr(self._h, C.byref(p)), "negf_broyden_input_device_ptr")
+        return p.value
+
+
+def affine_potential(K_dev, U0_dev, Q_dev, U_dev, stream=None):
+    n = int(U0_dev.shape[0])
+    check(_lib.load().negf_affine_potential(_ptr(K_dev), _ptr(U0_dev), _ptr(Q_dev), _ptr(U_dev), n, _stream(stream)),
+          "negf_affine_potential")

@@ -1,0 +1,202 @@
+/*
+ * negf_b200.h — C-ABI of the B200-native NEGF induced-charge engine.
+ *
+ * Drop-in boundary for ELEQTRONeX's NEGF/transport interface
+ * (Source/Solver/Transport/NEGF/NEGF_Common.H:518-606,
+ *  Source/Solver/Transport/Nanostructure.H:15-45,
+ *  Source/Solver/Transport/Transport.H:203-208).
+ *
+ * Conventions
+ *   - every function returns an int status: NEGF_OK (0) or a negative code;
+ *     negf_last_error() gives the message of the last failure on the calling
+ *     thread.  Nothing aborts the process.
+ *   - buffers are caller-owned; pointers are plain host or device pointers
+ *     as documented per argument; sizes are element counts.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *   - one handle is not thread-safe; distinct handles are independent.
+ *   - reductions are deterministic: the same inputs give bitwise-identical
+ *     charge on the same GPU and launch configuration.
+ *   - the library has no CPU fallback: every compute call needs a CUDA
+ *     device and fails with NEGF_ERR_CUDA when none is present.
+ */
+#ifndef NEGF_B200_H_
+#define NEGF_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NEGF_OK 0
+#define NEGF_ERR_ARG (-1)
+#define NEGF_ERR_CUDA (-2)
+#define NEGF_ERR_STATE (-3)
+#define NEGF_ERR_NUMERIC (-4)
+#define NEGF_ERR_IO (-5)
+
+#define NEGF_PREC_FP64 0  /* complex FP64 recursion throughout */
+#define NEGF_PREC_MIXED 1 /* complex FP32 recursion, FP64 lead GF / near-axis points / reduction */
+
+#define NEGF_NORM_ABSOLUTE 0 /* Broyden_norm_type = absolute */
+#define NEGF_NORM_RELATIVE 1 /* Broyden_norm_type = relative */
+
+#define NEGF_MAX_NONEQ_PATHS 8
+
+typedef struct negf_tube negf_tube;
+typedef struct negf_broyden negf_broyden;
+
+/* Nanotube + NEGF parameters.  Field names follow the reference input keys
+ * (NEGF_Common.cpp:288-643, CNT.cpp:13-21).  negf_tube_desc_init() fills the
+ * reference defaults. */
+typedef struct negf_tube_desc {
+    int type_id[2];                /* (m, n) chirality; CNT.cpp:11 default (17, 0) */
+    int num_unitcells;             /* NS.num_unitcells */
+    int num_modes;                 /* BLOCK_SIZE: lowest distinct modes kept (Code_Definitions.H:9) */
+    double acc;                    /* C-C distance [m] (CNT.H:16, 1.42e-10) */
+    double gamma;                  /* hopping [eV] (CNT.H:17, 2.5) */
+    double contact_T[2];           /* contact_T [K] (NEGF_Common.H:442) */
+    double contact_mu[2];          /* contact_mu [eV] (NEGF_Common.cpp:395-407) */
+    int eq_integration_pts[3];     /* NEGF_Common.cpp:445-449 */
+    int num_noneq_paths;           /* NEGF_Common.cpp:473-497 */
+    int noneq_integration_pts[NEGF_MAX_NONEQ_PATHS];
+    double noneq_percent_intercuts[NEGF_MAX_NONEQ_PATHS]; /* <0 in [0] = uniform default */
+    double E_valence_min;          /* NEGF_Common.H:387 (-14) */
+    double E_pole_max;             /* NEGF_Common.H:388 (10) */
+    double E_zPlus_imag;           /* NEGF_Common.H:386 (1e-8) */
+    double Fermi_tail_factors[2];  /* NEGF_Common.H:395-396 (14, 14) */
+    int use_decimation;            /* NEGF_Common.H:469 (CNT default 0: analytic lead GF) */
+    int decimation_max_iter;       /* NEGF_Common.H:474 (30) */
+    int decimation_layers;         /* NEGF_Common.H:476 (10) */
+    /* Optional explicit real-axis window: when realaxis_pts > 0 the equilibrium
+     * contour ends at realaxis_min + i*E_zPlus_imag and the non-equilibrium
+     * integral runs over [realaxis_min, realaxis_max] with realaxis_pts points
+     * (kind 0: uniform grid of IntegrationPath.cpp:149-168, kind 1: Gauss-Legendre). */
+    double realaxis_min, realaxis_max;
+    int realaxis_pts, realaxis_kind;
+    int precision;                 /* NEGF_PREC_FP64 or NEGF_PREC_MIXED */
+    double mixed_fp64_band;        /* mixed mode: points with Im E below this [eV] stay FP64 (1e-3) */
+} negf_tube_desc;
+
+/* Fill `d` with the reference defaults. */
+int negf_tube_desc_init(negf_tube_desc* d);
+
+/* c_NEGF_Common::Initialize_NEGF_Params + Initialize_NEGF
+ * (NEGF_Common.cpp:1256-1306): material parameters, sorted modes and
+ * degeneracies (CNT.cpp:155-286), Hamiltonian (CNT.cpp:301-336), contact
+ * info (CNT.cpp:338-352), energy limits and paths (NEGF_Common.cpp:1687-1816)
+ * and Rho0 (NEGF_Common.cpp:3957-4092), on the current CUDA device. */
+int negf_tube_create(const negf_tube_desc* d, negf_tube** out);
+int negf_tube_destroy(negf_tube* t);
+
+/* c_NEGF_Common::get_num_field_sites (NEGF_Common.H:555). */
+int negf_tube_num_sites(const negf_tube* t, int* n_sites);
+/* Modes kept: J index, degeneracy and beta_J = 2 gamma cos(pi J / m)
+ * (CNT.cpp:227-292).  Arrays of length num_modes (may be NULL). */
+int negf_tube_modes(const negf_tube* t, int* num_modes, int* J, int* degeneracy, double* beta);
+/* Axial site positions [nm] (h_PTD_glo_vec, NEGF_Common.cpp:1074-1100, CNT.cpp:93-132). */
+int negf_tube_site_positions(const negf_tube* t, double* y_nm);
+
+/* Site potential U_n [eV] and the two contact potentials
+ * (h_U_loc_data / U_contact; Nanostructure.cpp:494-504,
+ * Add_PotentialToHamiltonian NEGF_Common.cpp:1656-1666).  Host pointer. */
+int negf_tube_set_potential(negf_tube* t, const double* U, int n_sites, const double U_contact[2]);
+/* Same with a device pointer; the copy is ordered on `stream`. */
+int negf_tube_set_potential_device(negf_tube* t, const double* d_U, int n_sites, const double U_contact[2],
+                                   void* stream);
+/* Device pointer of the tube's potential buffer (writers must order their
+ * writes before the next negf_compute_charge on the same stream). */
+int negf_tube_potential_device_ptr(negf_tube* t, double** d_U);
+
+/* set_Contact_Electrochemical_Potential (NEGF_Common.cpp:359-372): marks the
+ * energy limits and paths for rebuilding at the next charge computation
+ * (Solve_NEGF, NEGF_Common.cpp:1328-1337). */
+int negf_tube_set_contact_mu(negf_tube* t, const double mu[2]);
+
+/* Energy-point tables of the current paths (Define_EnergyLimits +
+ * Update_IntegrationPaths).  kind: 0 Rho0, 1 RhoEq contour, 2 poles, 3 NonEq.
+ * When buf != NULL writes (E.re, E.im, w.re, w.im, J.re, J.im) per point.
+ * *count receives the number of points. */
+int negf_tube_energy_points(negf_tube* t, int kind, double* buf, int* count);
+/* Same tables computed from a descriptor alone (contact_mu of the
+ * descriptor), without a device: host-side path logic only. */
+int negf_desc_energy_points(const negf_tube_desc* d, int kind, double* buf, int* count);
+/* Whether the non-equilibrium window is active (flag_noneq_exists). */
+int negf_tube_noneq(negf_tube* t, int* noneq);
+/* get_Total_Integration_Pts (NEGF_Common.cpp:1826-1841). */
+int negf_tube_total_integration_pts(negf_tube* t, int* pts);
+
+/* Restrict the energy points this process integrates to shard `rank` of
+ * `world` (contiguous ranges of every tube's point list, Rho0 subtracted on
+ * rank 0 only).  The partial charges of all ranks sum to the full charge. */
+int negf_tube_set_energy_shard(negf_tube* t, int rank, int world);
+/* The [lo, hi) range of point indices (RhoEq+poles first, then NonEq) that
+ * shard `rank` of `world` integrates for a tube with `num_points` points. */
+int negf_shard_range(int num_points, int rank, int world, int* lo, int* hi);
+
+/* Solve_NEGF + Compute_InducedCharge (NEGF_Common.cpp:1309-1340, 2850-2900)
+ * for a batch of tubes in one launch:
+ *   Q[offset_t + n] = sum_modes [Im RhoEq_n + Re RhoNonEq_n - Im Rho0_n]
+ * where offset_t is the running sum of the previous tubes' site counts
+ * (num_field_sites_loc_NS_offset).  Q is a device pointer when
+ * q_on_device != 0, else a host pointer (the call then synchronises `stream`). */
+int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q_on_device, void* stream);
+
+/* Per-call timing and work counters of the last negf_compute_charge
+ * (kernel milliseconds measured with CUDA events on `stream`). */
+typedef struct negf_stats {
+    double rgf_kernel_ms;      /* main RGF kernel */
+    double reduce_kernel_ms;   /* per-site reduction kernel */
+    long long updates;         /* sum over chains of N (site*energy*mode updates) */
+    long long updates_fp32;    /* of which computed in FP32 (mixed mode) */
+    long long contour_updates; /* updates on contour/pole points */
+    long long realaxis_updates;/* updates on real-axis points */
+    int chains;                /* (tube, mode, energy) chains incl. padding */
+    int warps;                 /* warps launched */
+    int kernel_launches;       /* kernels launched by the call */
+    long long checkpoint_bytes;/* scratch bytes written+read by the kernel */
+} negf_stats;
+int negf_last_stats(negf_stats* s);
+/* Enable CUDA-event timing of negf_compute_charge (off by default). */
+int negf_set_timing(int enable);
+
+/* Broyden modified-second mixing (Transport.H:203-208):
+ * Set_Broyden_Parallel (Broyden_Parallel_General.cpp:68-248),
+ * Execute_Broyden_Modified_Second_Algorithm_Parallel
+ * (Broyden_Second_Parallel.cpp:213-486), Reset_Broyden_Parallel
+ * (Broyden_Parallel_General.cpp:250-355).  All vectors live on the device. */
+int negf_broyden_create(int num_sites, int max_step, double fraction, int norm_type, negf_broyden** out);
+int negf_broyden_destroy(negf_broyden* b);
+/* Initial input charge n_in (device or host pointer). */
+int negf_broyden_set_input(negf_broyden* b, const double* n_in, int on_device, void* stream);
+/* One mixing step with n_out (device pointer): updates the internal n_in and
+ * copies it to d_n_in_out (device, may be NULL); *max_norm receives
+ * Broyden_Norm (max over sites of the abs/rel residual of this step's input)
+ * and d_norm (device, may be NULL) the per-site norm.  *status is 0, or 1 when
+ * the step count would exceed max_step (the reference aborts there). */
+int negf_broyden_step(negf_broyden* b, const double* d_n_out, double* d_n_in_out, double* d_norm,
+                      double* max_norm, int* status, void* stream);
+/* Reset for the next bias step; keep_charge mirrors
+ * reset_with_previous_charge_distribution, otherwise n_in = init_value. */
+int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void* stream);
+/* Broyden_Step (1-based). */
+int negf_broyden_step_number(const negf_broyden* b, int* step);
+/* Device pointer of the current input charge n_in. */
+int negf_broyden_input_device_ptr(negf_broyden* b, double** d_n_in);
+
+/* Affine electrostatics stand-in used by the SCF harness:
+ * d_U[i] = d_U0[i] + sum_j K[i*n + j] * d_Q[j]   (all device pointers). */
+int negf_affine_potential(const double* d_K, const double* d_U0, const double* d_Q, double* d_U, int n,
+                          void* stream);
+
+/* Write_Data (NEGF_Common.cpp:1407-1418, 3043-3112, 4221-4254):
+ * <prefix>_Qout.dat, <prefix>_norm.dat (axial position [nm], value; one
+ * header line; precision 15) and <prefix>_U.dat (index, position, U).
+ * Q and norm are host pointers of num_sites values (norm may be NULL). */
+int negf_write_step(negf_tube* t, const char* prefix, const double* Q, const double* norm);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* negf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NEGF_B200_H_ */

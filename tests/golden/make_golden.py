@@ -1,0 +1,41 @@
+"""Extract the reference's own known-answer files for the NEGF recursion.
+
+The reference ships three standalone RGF programs whose outputs are committed
+in its tree.  This script copies the numeric tables (data only, no source)
+into ``tests/golden/`` so that the tests can run where the reference tree is
+absent.  It reads the reference checkout given by ``--ref`` (default: the
+read-only mount used when this repository was built).
+
+  decimation_technique/Exec/output/{Sigma,DOS,Transmission}
+      N=4, 10 energies on [-6, 0] + 1e-8 i, beta = 2*2.5*cos(6 pi/17),
+      surface GF root (F - S)/D  (scripts/negf_cpp/decimation_technique/Source/main.cpp)
+  negf_python/PointContact/cpp_results/1gpu/{Sigma,DOS,Transmission}
+      N=4, 1000 energies on [-1, 1] + 1e-8 i, root (F + S)/D
+      (scripts/negf_cpp/spectral_function_1D_pll/Source/main.cpp)
+"""
+import argparse
+import os
+import shutil
+
+SETS = {
+    "decimation": "scripts/negf_cpp/decimation_technique/Exec/output",
+    "pointcontact_1gpu": "scripts/negf_python/PointContact/cpp_results/1gpu",
+}
+FILES = ["Sigma", "DOS", "Transmission"]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    here = os.path.dirname(os.path.abspath(__file__))
+    for tag, rel in SETS.items():
+        for f in FILES:
+            src = os.path.join(args.ref, rel, f)
+            dst = os.path.join(here, f"{tag}_{f}.txt")
+            shutil.copyfile(src, dst)
+            print(f"{src} -> {dst}")
+
+
+if __name__ == "__main__":
+    main()

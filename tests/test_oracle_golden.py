@@ -1,0 +1,156 @@
+"""The oracle against the reference's own known-answer files.
+
+tests/golden/*.txt are the committed outputs of the reference's standalone RGF
+programs (tests/golden/make_golden.py lists their origin).  The files print 6
+significant digits, so the bound is 1e-5 relative.
+"""
+import numpy as np
+import pytest
+
+BETA = 2 * 2.5 * np.cos(np.pi * 6 / 17)  # get_beta(2.5, 17, 6), decimation_technique/Source/main.cpp:976-979
+GOLDEN = {
+    # tag: (surface-GF root, E range)
+    "decimation": (1, (-6.0, 0.0)),
+    "pointcontact_1gpu": (2, (-1.0, 1.0)),
+}
+
+
+def _load(tag, name):
+    import os
+    p = os.path.join(os.path.dirname(__file__), "golden", f"{tag}_{name}.txt")
+    return np.loadtxt(p, skiprows=1)
+
+
+@pytest.mark.parametrize("tag", sorted(GOLDEN))
+def test_fixture_sigma_dos_transmission(oracle, tag):
+    root, (lo, hi) = GOLDEN[tag]
+    S, D, T = _load(tag, "Sigma"), _load(tag, "DOS"), _load(tag, "Transmission")
+    n = len(S)
+    E = lo + np.arange(n) * ((hi - lo) / (n - 1))
+    assert np.allclose(E, S[:, 0], rtol=0, atol=5e-6)
+    sig, dos, tr = oracle.fixture_sigma_dos_T(4, BETA, 2.5, E, 1e-8, root)
+    # Sigma of both contacts (real, imag); 6 printed digits
+    for col, gold in ((0, S[:, 1]), (1, S[:, 2]), (2, S[:, 3]), (3, S[:, 4])):
+        np.testing.assert_allclose(sig[:, col], gold, rtol=1e-5, atol=1e-12)
+    np.testing.assert_allclose(dos[:, 0], D[:, 1], rtol=1e-5, atol=1e-30)
+    np.testing.assert_allclose(tr[:, 0], T[:, 1], rtol=1e-5, atol=1e-30)
+
+
+def test_gauss_legendre_exactness(oracle):
+    # CodeUtil.cpp:640-690 stops Newton at a 3e-11 step and evaluates the
+    # weight derivative at the previous iterate: moments are exact to ~1e-10.
+    for n in (1, 2, 3, 7, 30, 64):
+        x, w = oracle.gauss_legendre(n)
+        assert np.all(np.diff(x) > 0)
+        for k in range(2 * n):
+            exact = 0.0 if k % 2 else 2.0 / (k + 1)
+            assert abs(np.sum(w * x ** k) - exact) < 1e-9
+
+
+def test_modes_17_0(oracle):
+    t = oracle.OracleTube(type_id=(17, 0), num_unitcells=10, num_modes=3)
+    J, deg, beta, gap = t.modes()
+    assert t.N == 40
+    assert abs(t.radius - 0.6655e-9) < 1e-12
+    assert list(deg) == [2, 2, 2]
+    assert np.all(np.diff(gap) > 0)
+    np.testing.assert_allclose(np.abs(beta), 2 * 2.5 * np.abs(np.cos(np.pi * J / 17)))
+
+
+def _dense_G(E, U, beta, gamma, sig0, sig1):
+    """Dense (E - H - Sigma)^-1 of the mode-space chain, numpy inverse."""
+    N = len(U)
+    A = np.zeros((N, N), complex)
+    for n in range(N):
+        A[n, n] = E - U[n]
+    A[0, 0] -= sig0
+    A[N - 1, N - 1] -= sig1
+    for n in range(N - 1):
+        h = -beta if n % 2 == 0 else -gamma
+        A[n, n + 1] = A[n + 1, n] = h
+    return np.linalg.inv(A)
+
+
+def test_fixture_against_dense_inverse(oracle):
+    """DOS/T of the fixture kernel equal trace/|G_0,N-1|^2 of the dense inverse."""
+    N, gamma = 6, 2.5
+    E = np.array([-2.0, -0.3, 0.4, 1.7])
+    sig, dos, tr = oracle.fixture_sigma_dos_T(N, BETA, gamma, E, 1e-3, 2)
+    for i, e in enumerate(E):
+        s0 = complex(sig[i, 0], sig[i, 1])
+        G = _dense_G(e + 1e-3j, np.zeros(N), BETA, gamma, s0, s0)
+        g0 = -2 * s0.imag
+        A = G[:, [0]] * g0 @ G[:, [0]].conj().T + G[:, [N - 1]] * g0 @ G[:, [N - 1]].conj().T
+        np.testing.assert_allclose(dos[i, 0], np.trace(A).real / (2 * np.pi), rtol=1e-10)
+        np.testing.assert_allclose(tr[i, 0], g0 * g0 * abs(G[0, N - 1]) ** 2, rtol=1e-10)
+
+
+def _small_tube(oracle, **kw):
+    base = dict(type_id=(17, 0), num_unitcells=6, num_modes=2, eq_integration_pts=(20, 20, 24),
+                noneq_integration_pts=(40,), E_zPlus_imag=1e-3)
+    base.update(kw)
+    return oracle.OracleTube(**base)
+
+
+def test_faithful_walk_equals_running_products(oracle):
+    """The reference's O(N)-per-site contact walk equals the O(N) running products."""
+    t = _small_tube(oracle, contact_mu=(0.0, -0.3))
+    rng = np.random.default_rng(1)
+    t.set_potential(rng.uniform(-0.2, 0.2, t.N), (0.05, -0.25))
+    a = t.charge(faithful=True)
+    b = t.charge(faithful=False)
+    np.testing.assert_allclose(a, b, rtol=1e-11, atol=1e-14 * np.abs(a).max())
+
+
+def test_flat_band_zero_charge(oracle):
+    """U = 0, mu = 0 equilibrium: RhoEq equals Rho0 up to the pole/contour split."""
+    t = _small_tube(oracle, eq_integration_pts=(60, 60, 60), E_zPlus_imag=1e-8)
+    t.set_potential(np.zeros(t.N), (0.0, 0.0))
+    Q, eq, ne, r0 = t.charge(components=True)
+    assert np.max(np.abs(Q)) < 2e-3 * np.max(np.abs(r0))
+
+
+def test_charge_components_against_dense_inverse(oracle):
+    """RhoEq of a few contour points, recomputed from the dense inverse."""
+    t = _small_tube(oracle, num_unitcells=3, eq_integration_pts=(4, 4, 6))
+    N = t.N
+    rng = np.random.default_rng(7)
+    U = rng.uniform(-0.3, 0.3, N)
+    Uc = (0.1, -0.1)
+    t.set_potential(U, Uc)
+    E, w, J = t.paths(1)
+    J_, deg, beta, _ = t.modes()
+    kT = 8.617333262e-5 * 298.0
+    # RhoEq = sum (-2/pi) w J f(E - mu_min) G_nn deg  + poles(-4i kT G_nn deg)
+    acc = np.zeros(N)
+    for m in range(t.M):
+        for e, ww, jj in zip(E, w, J):
+            s0, s1 = t.sigma(m, e, Uc[0]), t.sigma(m, e, Uc[1])
+            G = _dense_G(e, U, beta[m], 2.5, s0, s1)
+            f = 1.0 / (np.exp(e / kT) + 1.0)
+            acc += ((-2 / np.pi) * ww * jj * f * np.diag(G) * deg[m]).imag
+        Ep, _, _ = t.paths(2)
+        for e in Ep:
+            s0, s1 = t.sigma(m, e, Uc[0]), t.sigma(m, e, Uc[1])
+            G = _dense_G(e, U, beta[m], 2.5, s0, s1)
+            acc += (-4j * kT * np.diag(G) * deg[m]).imag
+    Q, eq, ne, r0 = t.charge(components=True)
+    np.testing.assert_allclose(eq, acc, rtol=1e-9, atol=1e-12)
+
+
+def test_broyden_oracle_linear_problem(oracle):
+    """Broyden modified-second converges on a contractive linear map n_out = A n + b."""
+    rng = np.random.default_rng(3)
+    S = 30
+    A = rng.normal(0, 0.5 / np.sqrt(S), (S, S))
+    b = rng.normal(0, 1, S)
+    n = np.zeros(S)
+    br = oracle.OracleBroyden(n, max_step=100, fraction=0.1, norm_type="absolute")
+    nrm = 1.0
+    it = 0
+    while nrm > 1e-10 and it < 90:
+        nrm, n, _ = br.step(A @ n + b)
+        it += 1
+    fixed = np.linalg.solve(np.eye(S) - A, b)
+    assert it < 2 * S + 5  # Broyden terminates in <= 2S steps on linear maps (exact arithmetic)
+    np.testing.assert_allclose(n, fixed, atol=1e-8)
