@@ -90,6 +90,14 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.rows.append([x.strip() for x in line.split(",")])
 
+    def wait_first(self, timeout=5.0):
+        t0 = time.time()
+        while self.proc and not self.rows and time.time() - t0 < timeout:
+            time.sleep(0.02)
+
+    def mark(self):
+        return len(self.rows)
+
     def __exit__(self, *a):
         if self.proc:
             self.proc.terminate()
@@ -98,10 +106,10 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def summary(self, lo=0, hi=None):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+        for r in self.rows[lo:hi]:
             try:
                 sm.append(float(r[1]))
                 mx = float(r[2])
@@ -191,12 +199,19 @@ def ring_positions_nm(unitcells, acc=1.42e-10):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true",
+                    help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis)")
     args = ap.parse_args()
+    if args.small:
+        global EQ_PTS, RT_PTS, WORKLOAD
+        EQ_PTS, RT_PTS = (64, 64, 128), 768
+        WORKLOAD = WORKLOAD.replace("E=4096", "E=1024").replace("1024 contour", "256 contour").replace(
+            "3072 real-axis", "768 real-axis")
     args.warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -236,26 +251,32 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    clk = ClockSampler(local).__enter__()
     # ---- warm-up
     for _ in range(args.warmup):
         compute_charge([tube], out=Q, stream=stream)
     torch.cuda.synchronize()
+    clk.wait_first()
 
     # ---- timed: K passes over resident inputs, L2 flushed between passes
     set_timing(True)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    rgf_ms, red_ms = [], []
+    rgf_ms, red_ms, p1_ms, p2_ms = [], [], [], []
     barrier()
-    with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            flush.zero_()
-            ev[i][0].record(stream)
-            compute_charge([tube], out=Q, stream=stream)
-            ev[i][1].record(stream)
-            st = last_stats()  # waits for this pass's kernel events
-            rgf_ms.append(st["rgf_kernel_ms"])
-            red_ms.append(st["reduce_kernel_ms"])
-        barrier()
+    clk_lo = clk.mark()
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        compute_charge([tube], out=Q, stream=stream)
+        ev[i][1].record(stream)
+        st = last_stats()  # waits for this pass's kernel events
+        rgf_ms.append(st["rgf_kernel_ms"])
+        red_ms.append(st["reduce_kernel_ms"])
+        p1_ms.append(st["pass1_kernel_ms"])
+        p2_ms.append(st["pass2_kernel_ms"])
+    barrier()
+    clk_hi = clk.mark() + 1
+    clk.__exit__()
     set_timing(False)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     t_local = float(np.sum(step_ms))
@@ -337,8 +358,9 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
                         "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},
-                "gpu_launches": 2 * args.steps, "clocks": clk.summary(),
-                "kernel_ms_per_pass": {"rgf": k_ms, "reduce": float(np.mean(red_ms))}}
+                "gpu_launches": 2 * args.steps, "clocks": clk.summary(clk_lo, clk_hi),
+                "kernel_ms_per_pass": {"rgf": k_ms, "rgf_pass1": float(np.mean(p1_ms)),
+                                       "rgf_pass2": float(np.mean(p2_ms)), "reduce": float(np.mean(red_ms))}}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -27,7 +27,7 @@ EXPORTED = [
     "negf_tube_total_integration_pts", "negf_tube_set_energy_shard", "negf_shard_range", "negf_compute_charge",
     "negf_last_stats", "negf_set_timing", "negf_broyden_create", "negf_broyden_destroy", "negf_broyden_set_input",
     "negf_broyden_step", "negf_broyden_reset", "negf_broyden_step_number", "negf_broyden_input_device_ptr",
-    "negf_affine_potential", "negf_write_step", "negf_last_error",
+    "negf_affine_potential", "negf_write_step", "negf_last_error", "negf_device_selftest",
 ]
 
 
@@ -63,6 +63,8 @@ class TubeDesc(C.Structure):
 class Stats(C.Structure):
     _fields_ = [
         ("rgf_kernel_ms", C.c_double),
+        ("pass1_kernel_ms", C.c_double),
+        ("pass2_kernel_ms", C.c_double),
         ("reduce_kernel_ms", C.c_double),
         ("updates", C.c_longlong),
         ("updates_fp32", C.c_longlong),
@@ -70,6 +72,7 @@ class Stats(C.Structure):
         ("realaxis_updates", C.c_longlong),
         ("chains", C.c_int),
         ("warps", C.c_int),
+        ("units", C.c_int),
         ("kernel_launches", C.c_int),
         ("checkpoint_bytes", C.c_longlong),
     ]
@@ -122,6 +125,7 @@ def load():
         "negf_affine_potential": [vp, vp, vp, vp, C.c_int, vp],
         "negf_write_step": [vp, C.c_char_p, dp, dp],
         "negf_last_error": [],
+        "negf_device_selftest": [C.c_int, C.c_int, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -139,6 +139,7 @@ struct ChainTable {
     std::vector<negf::ChainRec> chains;
     std::vector<negf::WarpRec> warps;
     std::vector<negf::ReduceTube> rts;
+    std::vector<negf::SegUnit> units;
     long long partial_doubles = 0, scratch_doubles = 0;
     long long updates = 0, updates_fp32 = 0, contour_updates = 0, realaxis_updates = 0;
     int max_N = 0;
@@ -190,7 +191,7 @@ namespace {
 
 std::mutex g_mu;
 struct Workspace {
-    DevBuf tubes, chains, warps, rts, partial, scratch;
+    DevBuf tubes, chains, warps, rts, units, partial, scratch, qbuf;
     // cached chain table
     std::vector<const negf_tube*> key_tubes;
     std::vector<int> key_versions;
@@ -199,7 +200,7 @@ struct Workspace {
     bool table_valid = false;
     // stats / timing
     bool timing = false;
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     negf_stats stats{};
     bool stats_pending = false;
     int warps_per_block = 4;
@@ -507,11 +508,14 @@ void build_table(ChainTable& ct, const std::vector<TubePass>& passes) {
         rt.N = N;
         rt.num_rows = int(ct.warps.size() - w0);
         rt.rho0 = (!tp.rho0_pass && tp.t->shard_rank == 0) ? tp.t->d_rho0 : nullptr;
+        const int nseg = (N + negf::kSeg - 1) / negf::kSeg;
         for (size_t w = w0; w < ct.warps.size(); ++w) {
             ct.warps[w].row_off = row;
             row += N;
             ct.warps[w].ck_off = ck;
             ck += negf::rgf_scratch_doubles(N, ct.warps[w].kind, ct.warps[w].fp32);
+            for (int s0 = 0; s0 < nseg; s0 += negf::kSegsPerUnit)
+                ct.units.push_back({(int)w, s0, std::min(nseg, s0 + negf::kSegsPerUnit), 0});
         }
         rts[oi] = rt;
         ct.max_N = std::max(ct.max_N, N);
@@ -530,6 +534,7 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
         NEGF_CUDA(W.chains.reserve(std::max<size_t>(1, ct.chains.size()) * sizeof(negf::ChainRec)));
         NEGF_CUDA(W.warps.reserve(std::max<size_t>(1, ct.warps.size()) * sizeof(negf::WarpRec)));
         NEGF_CUDA(W.rts.reserve(std::max<size_t>(1, ct.rts.size()) * sizeof(negf::ReduceTube)));
+        NEGF_CUDA(W.units.reserve(std::max<size_t>(1, ct.units.size()) * sizeof(negf::SegUnit)));
         NEGF_CUDA(W.partial.reserve(std::max<long long>(1, ct.partial_doubles) * sizeof(double)));
         NEGF_CUDA(W.scratch.reserve(std::max<long long>(1, ct.scratch_doubles) * sizeof(double)));
         if (!ct.chains.empty())
@@ -537,6 +542,9 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
                                       cudaMemcpyHostToDevice, stream));
         if (!ct.warps.empty())
             NEGF_CUDA(cudaMemcpyAsync(W.warps.p, ct.warps.data(), ct.warps.size() * sizeof(negf::WarpRec),
+                                      cudaMemcpyHostToDevice, stream));
+        if (!ct.units.empty())
+            NEGF_CUDA(cudaMemcpyAsync(W.units.p, ct.units.data(), ct.units.size() * sizeof(negf::SegUnit),
                                       cudaMemcpyHostToDevice, stream));
     }
     // the reduce table carries device pointers that can change (rho0 of a rebuilt tube)
@@ -554,7 +562,8 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
         NEGF_CUDA(cudaEventRecord(W.ev[0], stream));
     }
     NEGF_CUDA(negf::launch_rgf(W.tubes.as<negf::TubeDev>(), W.chains.as<negf::ChainRec>(), W.warps.as<negf::WarpRec>(),
-                               nw, W.partial.as<double>(), W.scratch.p, W.warps_per_block, stream));
+                               nw, W.units.as<negf::SegUnit>(), (int)ct.units.size(), W.partial.as<double>(),
+                               W.scratch.p, W.warps_per_block, stream, W.timing ? W.ev[3] : nullptr));
     if (W.timing) NEGF_CUDA(cudaEventRecord(W.ev[1], stream));
     NEGF_CUDA(negf::launch_reduce(W.rts.as<negf::ReduceTube>(), (int)ct.rts.size(), ct.max_N, W.partial.as<double>(),
                                   d_Q, stream));
@@ -567,7 +576,8 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
     st.realaxis_updates = ct.realaxis_updates;
     st.chains = (int)ct.chains.size();
     st.warps = nw;
-    st.kernel_launches = (nw > 0 ? 1 : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
+    st.kernel_launches = (nw > 0 ? 2 : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
+    st.units = (int)ct.units.size();
     st.checkpoint_bytes = 2 * ct.scratch_doubles * 8;
     W.stats_pending = W.timing;
     return NEGF_OK;
@@ -842,10 +852,9 @@ int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q
         if (same && (W.key_tubes[i] != t || W.key_versions[i] != t->version)) same = false;
     }
     double* dQ = Q;
-    DevBuf tmpQ;
     if (!q_on_device) {
-        NEGF_CUDA(tmpQ.reserve(sizeof(double) * off));
-        dQ = tmpQ.as<double>();
+        NEGF_CUDA(W.qbuf.reserve(sizeof(double) * off));
+        dQ = W.qbuf.as<double>();
     }
     int rc = upload_and_launch(passes, tdev, !same, dQ, s);
     if (rc) {
@@ -875,10 +884,13 @@ int negf_last_stats(negf_stats* s) {
     Workspace& W = ws();
     if (W.stats_pending) {
         NEGF_CUDA(cudaEventSynchronize(W.ev[2]));
-        float a = 0, b = 0;
+        float a = 0, b = 0, p1 = 0;
         NEGF_CUDA(cudaEventElapsedTime(&a, W.ev[0], W.ev[1]));
         NEGF_CUDA(cudaEventElapsedTime(&b, W.ev[1], W.ev[2]));
+        NEGF_CUDA(cudaEventElapsedTime(&p1, W.ev[0], W.ev[3]));
         W.stats.rgf_kernel_ms = a;
+        W.stats.pass1_kernel_ms = p1;
+        W.stats.pass2_kernel_ms = a - p1;
         W.stats.reduce_kernel_ms = b;
         W.stats_pending = false;
     }
@@ -979,6 +991,19 @@ int negf_broyden_step_number(const negf_broyden* b, int* step) {
 int negf_broyden_input_device_ptr(negf_broyden* b, double** p) {
     if (!b || !p) return fail(NEGF_ERR_ARG, "null argument");
     *p = b->dev.n_in;
+    return NEGF_OK;
+}
+
+int negf_device_selftest(int which, int n, const double* in, double* out) {
+    if (!in || !out || n <= 0 || which < 0 || which > 1) return fail(NEGF_ERR_ARG, "bad self-test arguments");
+    int rc = require_device();
+    if (rc) return rc;
+    DevBuf a, b;
+    NEGF_CUDA(a.reserve(sizeof(double) * n));
+    NEGF_CUDA(b.reserve(sizeof(double) * n));
+    NEGF_CUDA(cudaMemcpy(a.p, in, sizeof(double) * n, cudaMemcpyHostToDevice));
+    NEGF_CUDA(negf::selftest(which, n, a.as<double>(), b.as<double>(), 0));
+    NEGF_CUDA(cudaMemcpy(out, b.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return NEGF_OK;
 }
 

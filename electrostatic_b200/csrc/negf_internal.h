@@ -10,7 +10,7 @@
 namespace negf {
 
 constexpr int kMaxModes = 32;   // distinct modes per tube kept on the device
-constexpr int kSeg = 16;        // sites per checkpoint segment of the RGF sweeps
+constexpr int kSeg = 8;         // sites per checkpoint segment of the RGF sweeps
 constexpr int kWarp = 32;
 
 // Per-tube record read by the RGF kernel (one per tube of a launch).
@@ -57,13 +57,29 @@ struct __align__(16) ReduceTube {
     int num_rows;        // warps of the tube
 };
 
-// RGF launch: one warp per WarpRec, lane = chain.
+// Pass-2 work unit: segments [seg0, seg1) of the chains of one warp.
+struct __align__(16) SegUnit {
+    int warp;
+    int seg0, seg1;
+    int pad;
+};
+constexpr int kSegsPerUnit = 32;  // segments per pass-2 unit (256 sites)
+
+// RGF launch: pass 1 (one warp per WarpRec, lane = chain: concurrent forward
+// and backward sweeps storing boundary checkpoints) then pass 2 (one warp per
+// SegUnit: independent segments, per-site contributions into partial rows).
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
-                       double* d_partial, void* d_scratch, int warps_per_block, cudaStream_t stream);
+                       const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
+                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event);
+// Device self-test of numeric primitives: which = 0 FP64 reciprocal,
+// 1 FP32 reciprocal (input/output as doubles), n values, device pointers.
+cudaError_t selftest(int which, int n, const double* d_in, double* d_out, cudaStream_t stream);
 // Per-site reduction (Kahan) of warp rows, minus Rho0 when rho0 != null.
 cudaError_t launch_reduce(const ReduceTube* d_rt, int num_tubes, int max_N, const double* d_partial, double* d_Q,
                           cudaStream_t stream);
 // Scratch elements (doubles, rounded up) needed per warp for a tube of N sites.
+// Scratch of one warp: per-lane lead self-energies (4 x 32 doubles) then the
+// segment checkpoints (Y, lambda at segment starts; X, rho at segment ends).
 long long rgf_scratch_doubles(int N, int kind, int fp32);
 int rgf_kernel_regs();  // registers per thread of the RGF kernel (0 if unknown)
 

@@ -23,13 +23,18 @@
 // reference's per-site walk G_00 prod_{m<n}(-Xtil_m), so the O(N) walk per
 // site (O(N^2) per energy) becomes two running products.
 //
-// The forward sweep stores (Y, lambda) every kSeg sites; the backward sweep
-// recomputes each segment into registers and walks it in reverse, so the
-// per-site state never goes to HBM (kSeg x fewer scratch bytes).  Each
+// Pass 1 (one warp per 32 chains) runs the forward and the backward
+// recursions together -- they are independent, so each lane carries two
+// dependency chains -- and stores (Y, lambda) at every kSeg-site segment
+// start and (X, rho) at every segment end.  With both boundary states known,
+// the segments are independent: pass 2 launches one warp per (32 chains,
+// group of kSegsPerUnit segments), recomputes Y forward inside a segment,
+// walks X backward through it and forms the site contributions, so the
+// per-site state never goes to HBM and the GPU is filled with
+// throughput-bound warps instead of N-long latency-bound chains.  Each
 // segment's per-lane contributions are summed over the 32 lanes with a
-// butterfly reduce-scatter (one shuffle per site) and written as one
-// coalesced row segment; a second kernel sums the rows per site in a fixed
-// order (deterministic).
+// butterfly reduce-scatter and written as one coalesced row segment; a third
+// kernel sums the rows per site in a fixed order (deterministic).
 
 #include "negf_internal.h"
 
@@ -38,8 +43,22 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
-__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+// Reciprocal: hardware approximation y0 = rcp.approx.ftz(x) with relative
+// error e = 1 - x y0 (|e| <= 2^-20 or better), corrected by the truncated
+// series 1/x = y0 / (1 - e) = y0 (1 + e + e^2 + ...): keeping e^2 leaves a
+// relative error of order e^3 (< 2^-60) in FP64; FP32 keeps e (order e^2).
+// Inputs here are squared moduli in [1e-30, 1e30]; x = 0 or inf is not handled.
+__device__ __forceinline__ double rcp(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
+}
+__device__ __forceinline__ float rcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return fmaf(y, fmaf(-x, y, 1.0f), y);
+}
 
 struct cd {
     double x, y;
@@ -50,7 +69,7 @@ __device__ __forceinline__ cd cmul(cd a, cd b) { return {a.x * b.x - a.y * b.y, 
 __device__ __forceinline__ cd cscale(double s, cd a) { return {s * a.x, s * a.y}; }
 __device__ __forceinline__ cd cconj(cd a) { return {a.x, -a.y}; }
 __device__ __forceinline__ cd cinv(cd a) {
-    const double r = rcp(a.x * a.x + a.y * a.y);
+    const double r = 1.0 / (a.x * a.x + a.y * a.y);
     return {a.x * r, -a.y * r};
 }
 // Principal square root: with m = |z|, t = sqrt((m + |Re z|)/2),
@@ -130,11 +149,10 @@ __device__ cd sigma_contact(cd E, double Uc, double beta, const TubeDev& T) {
 }
 
 // Butterfly reduce-scatter of K per-lane values over the 32 lanes: returns
-// the sum over lanes of element j = lane >> (5 - log2 K).  K - 1 + log2(32/K)
-// shuffles in total, fixed order (deterministic).
+// the sum over lanes of element j = lane >> (5 - log2 K).  Fixed order.
 template <int K>
 __device__ __forceinline__ double warp_reduce_scatter(double (&a)[K], int lane) {
-    static_assert(K == 8 || K == 16 || K == 32, "K");
+    static_assert(K == 8 || K == 16, "K");
 #pragma unroll
     for (int half = K / 2, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
         const bool up = (lane & bit) != 0;
@@ -145,210 +163,451 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&a)[K], int lane) 
             a[i] = keep + __shfl_xor_sync(kFull, send, bit);
         }
     }
-    constexpr int rest = (K == 8) ? 2 : (K == 16 ? 1 : 0);
-#pragma unroll
-    for (int r = 0, bit = (K == 8 ? 2 : 1); r < rest; ++r, bit >>= 1) a[0] += __shfl_xor_sync(kFull, a[0], bit);
+    if (K == 8) {
+        a[0] += __shfl_xor_sync(kFull, a[0], 2);
+        a[0] += __shfl_xor_sync(kFull, a[0], 1);
+    } else {
+        a[0] += __shfl_xor_sync(kFull, a[0], 1);
+    }
     return a[0];
 }
 
-// One warp of chains.  R: recursion precision.  RA: real-axis (non-equilibrium) chains.
+template <typename R>
+struct Chain {
+    int N;
+    R Er, Ei, s0r, s0i, s1r, s1i, hb2, hg2;
+    double cr, ci, k0, k1;
+    bool valid;
+};
+
+// alpha_n = E - U_n - delta_{n,0} Sigma_0 - delta_{n,N-1} Sigma_1
+template <typename R>
+__device__ __forceinline__ void alpha(const Chain<R>& c, int n, R u, R& ar, R& ai) {
+    ar = c.Er - u;
+    ai = c.Ei;
+    if (n == 0) {
+        ar -= c.s0r;
+        ai -= c.s0i;
+    }
+    if (n == c.N - 1) {
+        ar -= c.s1r;
+        ai -= c.s1i;
+    }
+}
+
+// Forward step at site n (< N-1): Y_{n+1} = h_n^2 / (alpha_n - Y_n), lambda_{n+1}.
 template <typename R, bool RA>
-__device__ __forceinline__ void rgf_warp(const TubeDev* __restrict__ tubes, const ChainRec& c, const WarpRec& wr,
-                                         double* __restrict__ prow, R* __restrict__ ck, int lane) {
+__device__ __forceinline__ void fwd_step(const Chain<R>& c, int n, R u, R yr, R yi, R l, R& oyr, R& oyi, R& ol) {
+    R ar, ai;
+    alpha(c, n, u, ar, ai);
+    const R dr = ar - yr, di = ai - yi;
+    const R h2 = (n & 1) ? c.hg2 : c.hb2;
+    const R inv = rcp(dr * dr + di * di);
+    const R hi = h2 * inv;
+    oyr = hi * dr;
+    oyi = -hi * di;
+    if (RA) ol = l * hi;
+}
+
+// Backward step at site n (> 0): X_{n-1} = h_{n-1}^2 / (alpha_n - X_n), rho_{n-1}.
+template <typename R, bool RA>
+__device__ __forceinline__ void bwd_step(const Chain<R>& c, int n, R u, R& xr, R& xi, R& rho) {
+    R ar, ai;
+    alpha(c, n, u, ar, ai);
+    const R er = ar - xr, ei = ai - xi;
+    const R h2 = ((n - 1) & 1) ? c.hg2 : c.hb2;
+    const R hi = h2 * rcp(er * er + ei * ei);
+    xr = hi * er;
+    xi = -hi * ei;
+    if (RA) rho = rho * hi;
+}
+
+// Contribution of site n: Im(c G_nn) [+ |G_nn|^2 (lambda k0 + rho k1)].
+template <typename R, bool RA>
+__device__ __forceinline__ double site_value(const Chain<R>& c, int n, R u, R yr, R yi, R l, R xr, R xi, R rho) {
+    R ar, ai;
+    alpha(c, n, u, ar, ai);
+    const R gr = ar - xr - yr, gi = ai - xi - yi;
+    const R ginv = rcp(gr * gr + gi * gi);  // |G_nn|^2
+    double v = c.cr * (double)(-gi * ginv) + c.ci * (double)(gr * ginv);
+    if (RA) v += (double)ginv * ((double)l * c.k0 + (double)rho * c.k1);
+    return c.valid ? v : 0.0;
+}
+
+template <typename R, bool RA>
+__device__ __forceinline__ Chain<R> make_chain(const TubeDev& T, const ChainRec& cr, double s0r, double s0i,
+                                               double s1r, double s1i) {
+    const bool valid = cr.mode >= 0;
+    const int mode = valid ? cr.mode : 0;
+    const double beta = T.beta[mode];
+    const double deg = valid ? T.degen[mode] : 0.0;
+    Chain<R> c;
+    c.N = T.N;
+    c.Er = (R)cr.Er;
+    c.Ei = (R)cr.Ei;
+    c.s0r = (R)s0r;
+    c.s0i = (R)s0i;
+    c.s1r = (R)s1r;
+    c.s1i = (R)s1i;
+    c.hb2 = (R)(beta * beta);
+    c.hg2 = (R)(T.gamma * T.gamma);
+    c.cr = cr.cr * deg;
+    c.ci = cr.ci * deg;
+    // Gamma_k = i (Sigma_k - Sigma_k^dagger) = -2 Im Sigma_k
+    c.k0 = RA ? (-2.0 * s0i) * cr.b0 * deg : 0.0;
+    c.k1 = RA ? (-2.0 * s1i) * cr.b1 * deg : 0.0;
+    c.valid = valid;
+    return c;
+}
+
+// Checkpoint record of segment s (per lane): Y_start (2), lambda_start,
+// X_end (2), rho_end for real-axis warps; Y_start, X_end for contour warps.
+template <bool RA>
+struct CkLayout {
+    static constexpr int NC = RA ? 6 : 4;
+    static constexpr int Y = 0, L = 2, X = RA ? 3 : 2, RHO = 5;
+};
+
+// Projective form of the two recursions used by pass 1.  With
+// Y_n = P_n / Q_n the forward map Y_{n+1} = h_n^2 / (alpha_n - Y_n) is the
+// linear update (P, Q) <- (h_n^2 Q, alpha_n Q - P), and
+// lambda_n = lambda_{n0} prod_{m=n0}^{n-1} h_m^2 / |Q_n|^2 when Q_{n0} = 1
+// (the moduli |alpha_m - Y_m| = |Q_{m+1} / Q_m| telescope).  Likewise
+// X_n = R_n / S_n with (R, S) <- (h_{n-1}^2 S, alpha_n S - R) going down.
+// Im(alpha_n - Y_n) >= Im E > 0, so Q never vanishes; renormalising to
+// Q = 1 once per segment keeps |P|, |Q| < (max |alpha|)^kSeg.
+template <typename R>
+struct Proj {
+    R pr, pi, qr, qi;  // P, Q
+    R lam;             // lambda (or rho) at the last renormalisation
+    R H;               // product of h^2 since the last renormalisation
+};
+
+// Linear step with hopping square h2 at a site of potential u; `edge`
+// adds the contact self-energy sr + i si to alpha.
+template <typename R>
+__device__ __forceinline__ void proj_step(const Chain<R>& c, Proj<R>& p, R u, R h2) {
+    const R ar = c.Er - u;
+    const R npr = h2 * p.qr, npi = h2 * p.qi;
+    const R nqr = fma(ar, p.qr, fma(-c.Ei, p.qi, -p.pr));
+    const R nqi = fma(ar, p.qi, fma(c.Ei, p.qr, -p.pi));
+    p.pr = npr;
+    p.pi = npi;
+    p.qr = nqr;
+    p.qi = nqi;
+    p.H *= h2;
+}
+template <typename R>
+__device__ __forceinline__ void proj_step_edge(const Chain<R>& c, Proj<R>& p, R u, R h2, R sr, R si) {
+    const R ar = c.Er - u - sr, ai = c.Ei - si;
+    const R npr = h2 * p.qr, npi = h2 * p.qi;
+    const R nqr = ar * p.qr - ai * p.qi - p.pr;
+    const R nqi = ar * p.qi + ai * p.qr - p.pi;
+    p.pr = npr;
+    p.pi = npi;
+    p.qr = nqr;
+    p.qi = nqi;
+    p.H *= h2;
+}
+// Y = P / Q, lambda *= H / |Q|^2, then (P, Q) = (Y, 1), H = 1.
+template <typename R, bool RA>
+__device__ __forceinline__ void proj_normalise(Proj<R>& p, R& yr, R& yi) {
+    const R rq = rcp(p.qr * p.qr + p.qi * p.qi);
+    yr = (p.pr * p.qr + p.pi * p.qi) * rq;
+    yi = (p.pi * p.qr - p.pr * p.qi) * rq;
+    if (RA) p.lam = p.lam * (p.H * rq);
+    p.pr = yr;
+    p.pi = yi;
+    p.qr = 1;
+    p.qi = 0;
+    p.H = 1;
+}
+
+// Pass 1: forward (Y, lambda) and backward (X, rho) sweeps run together
+// (they are independent), in projective form, storing the state at every
+// segment start (forward) and segment end (backward).  Block b advances the
+// forward sweep through segment b and the backward sweep through segment
+// nseg-1-b; interior blocks (full segments, no contact site) take a
+// branch-free path with the hopping parity fixed by the unrolled index.
+template <typename R, bool RA>
+__device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, const ChainRec& cr, const WarpRec& wr,
+                                           double* __restrict__ wscratch, int lane) {
     constexpr int K = kSeg;
-    constexpr int NC = RA ? 3 : 2;  // checkpoint components: Y.re, Y.im (, lambda)
+    static_assert(K % 2 == 0, "segment length must be even");
+    using CL = CkLayout<RA>;
     const TubeDev& T = tubes[wr.tube];
     const int N = T.N;
     const double* __restrict__ U = T.U;
-    const bool valid = c.mode >= 0;
-    const int mode = valid ? c.mode : 0;
-    const double beta = T.beta[mode];
-    const double deg = valid ? T.degen[mode] : 0.0;
-
-    // Lead self-energies in FP64 (both precisions).
-    const cd E = {c.Er, c.Ei};
+    const bool valid = cr.mode >= 0;
+    const double beta = T.beta[valid ? cr.mode : 0];
+    const cd E = {cr.Er, cr.Ei};
     const cd S0 = sigma_contact(E, T.Uc0, beta, T);
     const cd S1 = sigma_contact(E, T.Uc1, beta, T);
-
-    const R Er = (R)c.Er, Ei = (R)c.Ei;
-    const R s0r = (R)S0.x, s0i = (R)S0.y, s1r = (R)S1.x, s1i = (R)S1.y;
-    const R hb2 = (R)(beta * beta), hg2 = (R)(T.gamma * T.gamma);
-    const double cr = c.cr * deg, ci = c.ci * deg;
-    // Gamma_k = i (Sigma_k - Sigma_k^dagger) = -2 Im Sigma_k
-    const double k0 = RA ? (-2.0 * S0.y) * c.b0 * deg : 0.0;
-    const double k1 = RA ? (-2.0 * S1.y) * c.b1 * deg : 0.0;
+    wscratch[0 * kWarp + lane] = S0.x;
+    wscratch[1 * kWarp + lane] = S0.y;
+    wscratch[2 * kWarp + lane] = S1.x;
+    wscratch[3 * kWarp + lane] = S1.y;
+    R* __restrict__ ck = reinterpret_cast<R*>(wscratch + 4 * kWarp) + lane;
+    const Chain<R> c = make_chain<R, RA>(T, cr, S0.x, S0.y, S1.x, S1.y);
     const int nseg = (N + K - 1) / K;
 
-    // ---- pass 1: forward sweep with checkpoints at segment starts
-    {
-        R yr = 0, yi = 0, lam = 1;
-        for (int s = 0; s < nseg; ++s) {
-            R* cks = ck + (size_t)s * NC * kWarp + lane;
-            cks[0] = yr;
-            cks[kWarp] = yi;
-            if (RA) cks[2 * kWarp] = lam;
-            const int n0 = s * K;
-            R u[K];
+    Proj<R> f{0, 0, 1, 0, 1, 1};  // Y_0 = 0, lambda_0 = 1
+    Proj<R> b{0, 0, 1, 0, 1, 1};  // X_{N-1} = 0, rho_{N-1} = 1
+    for (int blk = 0; blk < nseg; ++blk) {
+        const int fs = blk, bs = nseg - 1 - blk;
+        const int f0 = fs * K;                       // forward segment start
+        const int be = min(bs * K + K, N) - 1;       // backward segment end
+        R yr, yi, xr, xi;
+        proj_normalise<R, RA>(f, yr, yi);
+        proj_normalise<R, RA>(b, xr, xi);
+        {
+            R* p = ck + (size_t)fs * CL::NC * kWarp;
+            p[CL::Y * kWarp] = yr;
+            p[(CL::Y + 1) * kWarp] = yi;
+            if (RA) p[CL::L * kWarp] = f.lam;
+            R* q = ck + (size_t)bs * CL::NC * kWarp;
+            q[CL::X * kWarp] = xr;
+            q[(CL::X + 1) * kWarp] = xi;
+            if (RA) q[CL::RHO * kWarp] = b.lam;
+        }
+        R uf[K], ub[K];
 #pragma unroll
-            for (int j = 0; j < K; ++j) u[j] = (n0 + j < N) ? (R)__ldg(U + n0 + j) : (R)0;
+        for (int j = 0; j < K; ++j) {
+            uf[j] = (f0 + j < N) ? (R)__ldg(U + f0 + j) : (R)0;
+            ub[j] = (be - j >= 0) ? (R)__ldg(U + be - j) : (R)0;
+        }
+        const bool interior = (f0 > 0) && (f0 + K < N) && (be < N - 1) && (be - K + 1 > 0) && (be == bs * K + K - 1);
+        if (interior) {
+            // forward sites f0 + j (parity of j since f0 is even); backward sites
+            // be - j use h_{be-j-1}, parity of j since be - 1 is even.
 #pragma unroll
             for (int j = 0; j < K; ++j) {
-                const int n = n0 + j;
-                if (n >= N - 1) break;
-                R ar = Er - u[j], ai = Ei;
-                if (n == 0) {
-                    ar -= s0r;
-                    ai -= s0i;
+                const R h2 = (j & 1) ? c.hg2 : c.hb2;
+                proj_step(c, f, uf[j], h2);
+                proj_step(c, b, ub[j], h2);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                const int n = f0 + j;
+                if (n < N - 1) {
+                    const R h2 = (n & 1) ? c.hg2 : c.hb2;
+                    if (n == 0)
+                        proj_step_edge(c, f, uf[j], h2, c.s0r, c.s0i);
+                    else
+                        proj_step(c, f, uf[j], h2);
                 }
-                const R dr = ar - yr, di = ai - yi;
-                const R inv = rcp(dr * dr + di * di);
-                const R h2 = (n & 1) ? hg2 : hb2;
-                yr = h2 * dr * inv;
-                yi = -h2 * di * inv;
-                if (RA) lam = lam * (h2 * inv);
+                const int m = be - j;  // backward step at site m gives X_{m-1}
+                if (m >= bs * K && m >= 1) {
+                    const R h2 = ((m - 1) & 1) ? c.hg2 : c.hb2;
+                    if (m == N - 1)
+                        proj_step_edge(c, b, ub[j], h2, c.s1r, c.s1i);
+                    else
+                        proj_step(c, b, ub[j], h2);
+                }
             }
         }
     }
+}
 
-    // ---- pass 2: backward sweep, segment by segment
-    R xr = 0, xi = 0, rho = 1;
-    for (int s = nseg - 1; s >= 0; --s) {
+// Pass 2: segments [seg0, seg1) of one warp's chains.  Per segment: forward
+// recompute of Y (and lambda) from the start checkpoint, then the backward
+// walk of X (and rho) from the end checkpoint with the site contributions,
+// a 32-lane reduce-scatter and one coalesced row write.
+template <typename R, bool RA>
+__device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, const ChainRec& cr, const WarpRec& wr,
+                                           const SegUnit& su, const double* __restrict__ wscratch,
+                                           double* __restrict__ prow, int lane) {
+    constexpr int K = kSeg;
+    using CL = CkLayout<RA>;
+    const TubeDev& T = tubes[wr.tube];
+    const int N = T.N;
+    const double* __restrict__ U = T.U;
+    const double s0r = wscratch[0 * kWarp + lane], s0i = wscratch[1 * kWarp + lane];
+    const double s1r = wscratch[2 * kWarp + lane], s1i = wscratch[3 * kWarp + lane];
+    const R* __restrict__ ck = reinterpret_cast<const R*>(wscratch + 4 * kWarp) + lane;
+    const Chain<R> c = make_chain<R, RA>(T, cr, s0r, s0i, s1r, s1i);
+
+    for (int s = su.seg0; s < su.seg1; ++s) {
         const int n0 = s * K;
-        const R* cks = ck + (size_t)s * NC * kWarp + lane;
-        R u[K], Yr[K], Yi[K], L[K];
+        const R* p = ck + (size_t)s * CL::NC * kWarp;
+        R yr[K], yi[K], l[K], u[K];
+        yr[0] = p[CL::Y * kWarp];
+        yi[0] = p[(CL::Y + 1) * kWarp];
+        l[0] = RA ? p[CL::L * kWarp] : (R)1;
+        R xr = p[CL::X * kWarp], xi = p[(CL::X + 1) * kWarp];
+        R rho = RA ? p[CL::RHO * kWarp] : (R)1;
 #pragma unroll
-        for (int j = 0; j < K; ++j) u[j] = (n0 + j < N) ? (R)__ldg(U + n0 + j) : (R)0;
-        Yr[0] = cks[0];
-        Yi[0] = cks[kWarp];
-        L[0] = RA ? cks[2 * kWarp] : (R)1;
+        for (int k = 0; k < K; ++k) u[k] = (n0 + k < N) ? (R)__ldg(U + n0 + k) : (R)0;
 #pragma unroll
-        for (int j = 0; j < K - 1; ++j) {
-            const int n = n0 + j;
-            if (n >= N - 1) break;
-            R ar = Er - u[j], ai = Ei;
-            if (n == 0) {
-                ar -= s0r;
-                ai -= s0i;
-            }
-            const R dr = ar - Yr[j], di = ai - Yi[j];
-            const R inv = rcp(dr * dr + di * di);
-            const R h2 = (n & 1) ? hg2 : hb2;
-            Yr[j + 1] = h2 * dr * inv;
-            Yi[j + 1] = -h2 * di * inv;
-            if (RA) L[j + 1] = L[j] * (h2 * inv);
-        }
+        for (int k = 0; k < K - 1; ++k)
+            if (n0 + k < N - 1) fwd_step<R, RA>(c, n0 + k, u[k], yr[k], yi[k], l[k], yr[k + 1], yi[k + 1], l[k + 1]);
         double acc[K];
 #pragma unroll
-        for (int j = K - 1; j >= 0; --j) {
-            const int n = n0 + j;
-            acc[j] = 0.0;
+        for (int k = K - 1; k >= 0; --k) {
+            const int n = n0 + k;
+            acc[k] = 0.0;
             if (n < N) {
-                R ar = Er - u[j], ai = Ei;
-                if (n == 0) {
-                    ar -= s0r;
-                    ai -= s0i;
-                }
-                if (n == N - 1) {
-                    ar -= s1r;
-                    ai -= s1i;
-                }
-                const R er = ar - xr, ei = ai - xi;  // alpha_n - X_n
-                const R gr = er - Yr[j], gi = ei - Yi[j];
-                const R ginv = rcp(gr * gr + gi * gi);  // = |G_nn|^2
-                const double Gr = (double)(gr * ginv), Gi = (double)(-gi * ginv);
-                double v = cr * Gi + ci * Gr;  // Im(c G)
-                if (RA) v += (double)ginv * ((double)L[j] * k0 + (double)rho * k1);
-                acc[j] = valid ? v : 0.0;
-                if (n > 0) {
-                    const R einv = rcp(er * er + ei * ei);
-                    const R h2 = ((n - 1) & 1) ? hg2 : hb2;
-                    xr = h2 * er * einv;
-                    xi = -h2 * ei * einv;
-                    if (RA) rho = rho * (h2 * einv);
-                }
+                acc[k] = site_value<R, RA>(c, n, u[k], yr[k], yi[k], l[k], xr, xi, rho);
+                if (k > 0) bwd_step<R, RA>(c, n, u[k], xr, xi, rho);
             }
         }
         const double tot = warp_reduce_scatter<K>(acc, lane);
-        constexpr int shift = (K == 16) ? 1 : (K == 8 ? 2 : 0);
+        constexpr int shift = (K == 16) ? 1 : 2;
         const int j = lane >> shift;
         if ((lane & ((1 << shift) - 1)) == 0 && n0 + j < N) prow[n0 + j] = tot;
     }
 }
 
-__global__ void __launch_bounds__(128) rgf_kernel(const TubeDev* __restrict__ tubes,
-                                                  const ChainRec* __restrict__ chains,
-                                                  const WarpRec* __restrict__ warps, int num_warps,
-                                                  double* __restrict__ partial, double* __restrict__ scratch) {
+__global__ void __launch_bounds__(128) rgf_pass1_kernel(const TubeDev* __restrict__ tubes,
+                                                        const ChainRec* __restrict__ chains,
+                                                        const WarpRec* __restrict__ warps, int num_warps,
+                                                        double* __restrict__ scratch) {
     const int lane = threadIdx.x & 31;
     const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (w >= num_warps) return;
     const WarpRec wr = warps[w];
     const ChainRec c = chains[(size_t)w * kWarp + lane];
-    double* prow = partial + wr.row_off;
+    double* ws = scratch + wr.ck_off;
     if (wr.fp32) {
-        float* ck = reinterpret_cast<float*>(scratch + wr.ck_off);
         if (wr.kind == kRealAxis)
-            rgf_warp<float, true>(tubes, c, wr, prow, ck, lane);
+            pass1_warp<float, true>(tubes, c, wr, ws, lane);
         else
-            rgf_warp<float, false>(tubes, c, wr, prow, ck, lane);
+            pass1_warp<float, false>(tubes, c, wr, ws, lane);
     } else {
-        double* ck = scratch + wr.ck_off;
         if (wr.kind == kRealAxis)
-            rgf_warp<double, true>(tubes, c, wr, prow, ck, lane);
+            pass1_warp<double, true>(tubes, c, wr, ws, lane);
         else
-            rgf_warp<double, false>(tubes, c, wr, prow, ck, lane);
+            pass1_warp<double, false>(tubes, c, wr, ws, lane);
     }
 }
 
-// Q[q_off + n] = sum_w partial[row_base + w N + n] (Kahan, fixed order) - rho0[n]
-__global__ void reduce_kernel(const ReduceTube* __restrict__ rts, const double* __restrict__ partial,
-                              double* __restrict__ Q) {
-    const ReduceTube r = rts[blockIdx.y];
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= r.N) return;
-    const double* p = partial + r.row_base + n;
-    double s = 0.0, comp = 0.0;
-    for (int w = 0; w < r.num_rows; ++w) {
-        const double y = p[(size_t)w * r.N] - comp;
-        const double t = s + y;
-        comp = (t - s) - y;
-        s = t;
+__global__ void __launch_bounds__(128) rgf_pass2_kernel(const TubeDev* __restrict__ tubes,
+                                                        const ChainRec* __restrict__ chains,
+                                                        const WarpRec* __restrict__ warps,
+                                                        const SegUnit* __restrict__ units, int num_units,
+                                                        double* __restrict__ partial,
+                                                        const double* __restrict__ scratch) {
+    const int lane = threadIdx.x & 31;
+    const int ui = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (ui >= num_units) return;
+    const SegUnit su = units[ui];
+    const WarpRec wr = warps[su.warp];
+    const ChainRec c = chains[(size_t)su.warp * kWarp + lane];
+    const double* ws = scratch + wr.ck_off;
+    double* prow = partial + wr.row_off;
+    if (wr.fp32) {
+        if (wr.kind == kRealAxis)
+            pass2_unit<float, true>(tubes, c, wr, su, ws, prow, lane);
+        else
+            pass2_unit<float, false>(tubes, c, wr, su, ws, prow, lane);
+    } else {
+        if (wr.kind == kRealAxis)
+            pass2_unit<double, true>(tubes, c, wr, su, ws, prow, lane);
+        else
+            pass2_unit<double, false>(tubes, c, wr, su, ws, prow, lane);
     }
-    if (r.rho0) s -= r.rho0[n];
-    Q[r.q_off + n] = s;
+}
+
+__global__ void selftest_kernel(int which, int n, const double* __restrict__ in, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = which == 0 ? rcp(in[i]) : (double)rcp((float)in[i]);
+}
+
+// Q[q_off + n] = sum_w partial[row_base + w N + n] - rho0[n].
+// Block = 32 sites x kRowGroups row groups; each thread sums rows
+// g, g + kRowGroups, ... with Kahan compensation, then the row groups are
+// combined in a fixed order (deterministic).
+constexpr int kRowGroups = 8;
+__global__ void __launch_bounds__(32 * kRowGroups) reduce_kernel(const ReduceTube* __restrict__ rts,
+                                                                 const double* __restrict__ partial,
+                                                                 double* __restrict__ Q) {
+    __shared__ double sh_s[kRowGroups][32], sh_c[kRowGroups][32];
+    const ReduceTube r = rts[blockIdx.y];
+    const int n = blockIdx.x * 32 + threadIdx.x;
+    const int g = threadIdx.y;
+    double s = 0.0, comp = 0.0;
+    if (n < r.N) {
+        const double* p = partial + r.row_base + n;
+        int w = g;
+        for (; w + 3 * kRowGroups < r.num_rows; w += 4 * kRowGroups) {
+            double v[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[k] = p[(size_t)(w + k * kRowGroups) * r.N];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double y = v[k] - comp;
+                const double t = s + y;
+                comp = (t - s) - y;
+                s = t;
+            }
+        }
+        for (; w < r.num_rows; w += kRowGroups) {
+            const double y = p[(size_t)w * r.N] - comp;
+            const double t = s + y;
+            comp = (t - s) - y;
+            s = t;
+        }
+    }
+    sh_s[g][threadIdx.x] = s;
+    sh_c[g][threadIdx.x] = comp;
+    __syncthreads();
+    if (g == 0 && n < r.N) {
+        double tot = 0.0, cc = 0.0;
+        for (int k = 0; k < kRowGroups; ++k) {
+            const double y = (sh_s[k][threadIdx.x] - sh_c[k][threadIdx.x]) - cc;
+            const double t = tot + y;
+            cc = (t - tot) - y;
+            tot = t;
+        }
+        if (r.rho0) tot -= r.rho0[n];
+        Q[r.q_off + n] = tot;
+    }
 }
 
 }  // namespace
 
 long long rgf_scratch_doubles(int N, int kind, int fp32) {
     const long long nseg = (N + kSeg - 1) / kSeg;
-    const long long nc = (kind == kRealAxis) ? 3 : 2;
+    const long long nc = (kind == kRealAxis) ? 6 : 4;
     const long long bytes = nseg * nc * kWarp * (fp32 ? 4 : 8);
-    return (bytes + 15) / 16 * 2;  // 16-byte granules
+    return 4 * kWarp + (bytes + 15) / 16 * 2;  // self-energies, then 16-byte granules
 }
 
 int rgf_kernel_regs() {
     cudaFuncAttributes a;
-    if (cudaFuncGetAttributes(&a, rgf_kernel) != cudaSuccess) return 0;
+    if (cudaFuncGetAttributes(&a, rgf_pass2_kernel) != cudaSuccess) return 0;
     return a.numRegs;
 }
 
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
-                       double* d_partial, void* d_scratch, int warps_per_block, cudaStream_t stream) {
+                       const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
+                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event) {
     if (num_warps <= 0) return cudaSuccess;
     if (warps_per_block < 1 || warps_per_block > 4) warps_per_block = 4;
     const int threads = warps_per_block * kWarp;
-    const int blocks = (num_warps + warps_per_block - 1) / warps_per_block;
-    rgf_kernel<<<blocks, threads, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps, d_partial,
-                                               static_cast<double*>(d_scratch));
+    rgf_pass1_kernel<<<(num_warps + warps_per_block - 1) / warps_per_block, threads, 0, stream>>>(
+        d_tubes, d_chains, d_warps, num_warps, static_cast<double*>(d_scratch));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (mid_event) cudaEventRecord(mid_event, stream);
+    rgf_pass2_kernel<<<(num_units + 3) / 4, 128, 0, stream>>>(d_tubes, d_chains, d_warps, d_units, num_units,
+                                                               d_partial, static_cast<const double*>(d_scratch));
+    return cudaGetLastError();
+}
+
+cudaError_t selftest(int which, int n, const double* d_in, double* d_out, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    selftest_kernel<<<(n + 255) / 256, 256, 0, stream>>>(which, n, d_in, d_out);
     return cudaGetLastError();
 }
 
 cudaError_t launch_reduce(const ReduceTube* d_rt, int num_tubes, int max_N, const double* d_partial, double* d_Q,
                           cudaStream_t stream) {
     if (num_tubes <= 0 || max_N <= 0) return cudaSuccess;
-    dim3 grid((max_N + 127) / 128, num_tubes);
-    reduce_kernel<<<grid, 128, 0, stream>>>(d_rt, d_partial, d_Q);
+    dim3 grid((max_N + 31) / 32, num_tubes);
+    dim3 block(32, kRowGroups);
+    reduce_kernel<<<grid, block, 0, stream>>>(d_rt, d_partial, d_Q);
     return cudaGetLastError();
 }
 

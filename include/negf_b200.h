@@ -143,14 +143,17 @@ int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q
 /* Per-call timing and work counters of the last negf_compute_charge
  * (kernel milliseconds measured with CUDA events on `stream`). */
 typedef struct negf_stats {
-    double rgf_kernel_ms;      /* main RGF kernel */
+    double rgf_kernel_ms;      /* both RGF passes */
+    double pass1_kernel_ms;    /* pass 1: concurrent forward/backward sweeps */
+    double pass2_kernel_ms;    /* pass 2: segment-parallel recompute + site contributions */
     double reduce_kernel_ms;   /* per-site reduction kernel */
     long long updates;         /* sum over chains of N (site*energy*mode updates) */
     long long updates_fp32;    /* of which computed in FP32 (mixed mode) */
     long long contour_updates; /* updates on contour/pole points */
     long long realaxis_updates;/* updates on real-axis points */
     int chains;                /* (tube, mode, energy) chains incl. padding */
-    int warps;                 /* warps launched */
+    int warps;                 /* pass-1 warps launched */
+    int units;                 /* pass-2 warps (segment groups) launched */
     int kernel_launches;       /* kernels launched by the call */
     long long checkpoint_bytes;/* scratch bytes written+read by the kernel */
 } negf_stats;
@@ -181,6 +184,11 @@ int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void
 int negf_broyden_step_number(const negf_broyden* b, int* step);
 /* Device pointer of the current input charge n_in. */
 int negf_broyden_input_device_ptr(negf_broyden* b, double** d_n_in);
+
+/* Device self-test of the kernels' numeric primitives (no counterpart in the
+ * reference): which = 0 FP64 reciprocal, 1 FP32 reciprocal; n host values in,
+ * n host values out. */
+int negf_device_selftest(int which, int n, const double* in, double* out);
 
 /* Affine electrostatics stand-in used by the SCF harness:
  * d_U[i] = d_U0[i] + sum_j K[i*n + j] * d_Q[j]   (all device pointers). */

@@ -130,9 +130,9 @@ def test_energy_shards_sum_to_full(oracle):
         parts.append(g.Compute_InducedCharge())
     g.set_energy_shard(0, 1)
     assert _rel(sum(parts), full) <= 1e-12
-    # more shards than points: empty shards contribute nothing
+    # more shards than points: shard 1 of 2P+1 holds no point and (rank != 0) no Rho0
     pts = g.get_Total_Integration_Pts() + len(g.energy_points(1)[0])
-    g.set_energy_shard(pts + 5, pts + 10)
+    g.set_energy_shard(1, 2 * pts + 1)
     assert np.all(g.Compute_InducedCharge() == 0.0)
     g.set_energy_shard(0, 1)
 
@@ -219,3 +219,19 @@ def test_broyden_matches_oracle(oracle):
         assert gb.step_number == 1
         ptr_vals = torch.empty(S, dtype=torch.float64, device="cuda")
         ptr_vals.copy_(n_g)
+
+
+def test_device_reciprocal_accuracy(negf_lib):
+    """The kernels' reciprocal (hardware seed + series correction) against 1/x."""
+    import ctypes as C
+    rng = np.random.default_rng(0)
+    x = np.exp(rng.uniform(np.log(1e-30), np.log(1e30), 200000))
+    out = np.zeros_like(x)
+    dp = C.POINTER(C.c_double)
+    assert negf_lib.negf_device_selftest(0, len(x), x.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
+    rel = np.abs(out * x - 1.0)
+    assert rel.max() <= 4 * np.finfo(np.float64).eps, rel.max()
+    assert negf_lib.negf_device_selftest(1, len(x), x.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
+    xf = x.astype(np.float32).astype(np.float64)
+    rel32 = np.abs(out * xf - 1.0)
+    assert rel32.max() <= 4 * np.finfo(np.float32).eps, rel32.max()
