@@ -283,8 +283,20 @@ struct Proj {
     R H;               // product of h^2 since the last renormalisation
 };
 
-// Linear step with hopping square h2 at a site of potential u; `edge`
-// adds the contact self-energy sr + i si to alpha.
+// Linear step with hopping square h2 at a site of potential u (interior
+// site: the caller accounts for the product of h^2); proj_step_edge adds
+// the contact self-energy sr + i si to alpha and tracks the product.
+template <typename R>
+__device__ __forceinline__ void proj_step_int(const Chain<R>& c, Proj<R>& p, R u, R h2) {
+    const R ar = c.Er - u;
+    const R npr = h2 * p.qr, npi = h2 * p.qi;
+    const R nqr = fma(ar, p.qr, fma(-c.Ei, p.qi, -p.pr));
+    const R nqi = fma(ar, p.qi, fma(c.Ei, p.qr, -p.pi));
+    p.pr = npr;
+    p.pi = npi;
+    p.qr = nqr;
+    p.qi = nqi;
+}
 template <typename R>
 __device__ __forceinline__ void proj_step(const Chain<R>& c, Proj<R>& p, R u, R h2) {
     const R ar = c.Er - u;
@@ -353,6 +365,18 @@ __device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, co
 
     Proj<R> f{0, 0, 1, 0, 1, 1};  // Y_0 = 0, lambda_0 = 1
     Proj<R> b{0, 0, 1, 0, 1, 1};  // X_{N-1} = 0, rho_{N-1} = 1
+    R hfull = 1;                  // prod of h^2 over a full segment: (beta^2 gamma^2)^(K/2)
+#pragma unroll
+    for (int j = 0; j < K / 2; ++j) hfull *= c.hb2 * c.hg2;
+    R uf[K], ub[K];
+    {
+        const int be = min((nseg - 1) * K + K, N) - 1;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            uf[j] = (j < N) ? (R)__ldg(U + j) : (R)0;
+            ub[j] = (be - j >= 0) ? (R)__ldg(U + be - j) : (R)0;
+        }
+    }
     for (int blk = 0; blk < nseg; ++blk) {
         const int fs = blk, bs = nseg - 1 - blk;
         const int f0 = fs * K;                       // forward segment start
@@ -370,11 +394,15 @@ __device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, co
             q[(CL::X + 1) * kWarp] = xi;
             if (RA) q[CL::RHO * kWarp] = b.lam;
         }
-        R uf[K], ub[K];
+        // prefetch the next block's potentials
+        R nf[K], nb[K];
+        {
+            const int f1 = f0 + K, be1 = bs * K - 1;
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-            uf[j] = (f0 + j < N) ? (R)__ldg(U + f0 + j) : (R)0;
-            ub[j] = (be - j >= 0) ? (R)__ldg(U + be - j) : (R)0;
+            for (int j = 0; j < K; ++j) {
+                nf[j] = (f1 + j < N) ? (R)__ldg(U + f1 + j) : (R)0;
+                nb[j] = (be1 - j >= 0) ? (R)__ldg(U + be1 - j) : (R)0;
+            }
         }
         const bool interior = (f0 > 0) && (f0 + K < N) && (be < N - 1) && (be - K + 1 > 0) && (be == bs * K + K - 1);
         if (interior) {
@@ -383,9 +411,11 @@ __device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, co
 #pragma unroll
             for (int j = 0; j < K; ++j) {
                 const R h2 = (j & 1) ? c.hg2 : c.hb2;
-                proj_step(c, f, uf[j], h2);
-                proj_step(c, b, ub[j], h2);
+                proj_step_int(c, f, uf[j], h2);
+                proj_step_int(c, b, ub[j], h2);
             }
+            f.H = hfull;
+            b.H = hfull;
         } else {
 #pragma unroll
             for (int j = 0; j < K; ++j) {
@@ -406,6 +436,111 @@ __device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, co
                         proj_step(c, b, ub[j], h2);
                 }
             }
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            uf[j] = nf[j];
+            ub[j] = nb[j];
+        }
+    }
+}
+
+// Pass 2 segment in projective form (FP64).  From (P, Q) = (Y_{n0}, 1) the
+// forward recurrence gives P_n, Q_n and Q_{n+1} = alpha_n Q_n - P_n; from
+// (R, S) = (X_e, 1) the backward one gives R_n, S_n.  Then
+//   D_n = alpha_n Q_n S_n - R_n Q_n - P_n S_n = S_n Q_{n+1} - R_n Q_n,
+//   G_nn = Q_n S_n / D_n,
+//   |G_nn|^2 lambda_n = lambda_{n0} prod_{n0<=m<n} h_m^2 |S_n|^2 / |D_n|^2,
+//   |G_nn|^2 rho_n    = rho_e prod_{n<=m<e} h_m^2 |Q_n|^2 / |D_n|^2,
+// one reciprocal per site and only short linear dependency chains.
+struct CkVals {  // one lane's checkpoint of a segment
+    double yr, yi, lam, xr, xi, rho;
+};
+template <bool RA>
+__device__ __forceinline__ CkVals load_ck(const double* __restrict__ p) {
+    using CL = CkLayout<RA>;
+    CkVals v;
+    v.yr = p[CL::Y * kWarp];
+    v.yi = p[(CL::Y + 1) * kWarp];
+    v.lam = RA ? p[CL::L * kWarp] : 1.0;
+    v.xr = p[CL::X * kWarp];
+    v.xi = p[(CL::X + 1) * kWarp];
+    v.rho = RA ? p[CL::RHO * kWarp] : 1.0;
+    return v;
+}
+
+template <bool RA, bool EDGE>
+__device__ __forceinline__ void segment_proj(const Chain<double>& c, int n0, const CkVals& ckv,
+                                             const double (&u)[kSeg], double (&acc)[kSeg]) {
+    constexpr int K = kSeg;
+    const int N = c.N;
+    double pr[K], pi[K], qr[K + 1], qi[K + 1], lm[K];
+    pr[0] = ckv.yr;
+    pi[0] = ckv.yi;
+    qr[0] = 1.0;
+    qi[0] = 0.0;
+    lm[0] = ckv.lam;
+    double Rr = ckv.xr, Ri = ckv.xi, Sr = 1.0, Si = 0.0;
+    double rh = ckv.rho;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int n = n0 + j;
+        double ar = c.Er - u[j], ai = c.Ei;
+        if (EDGE) {
+            if (n >= N) break;
+            if (n == 0) {
+                ar -= c.s0r;
+                ai -= c.s0i;
+            }
+            if (n == N - 1) {
+                ar -= c.s1r;
+                ai -= c.s1i;
+            }
+        }
+        qr[j + 1] = fma(ar, qr[j], fma(-ai, qi[j], -pr[j]));
+        qi[j + 1] = fma(ar, qi[j], fma(ai, qr[j], -pi[j]));
+        if (j + 1 < K) {
+            const double h2 = EDGE ? ((n & 1) ? c.hg2 : c.hb2) : ((j & 1) ? c.hg2 : c.hb2);
+            pr[j + 1] = h2 * qr[j];
+            pi[j + 1] = h2 * qi[j];
+            if (RA) lm[j + 1] = lm[j] * h2;
+        }
+    }
+#pragma unroll
+    for (int j = K - 1; j >= 0; --j) {
+        const int n = n0 + j;
+        acc[j] = 0.0;
+        if (EDGE && n >= N) continue;
+        // D = S Q_{n+1} - R Q_n
+        const double dr = fma(Sr, qr[j + 1], fma(-Si, qi[j + 1], fma(-Rr, qr[j], Ri * qi[j])));
+        const double di = fma(Sr, qi[j + 1], fma(Si, qr[j + 1], fma(-Rr, qi[j], -Ri * qr[j])));
+        const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);  // T = Q S
+        const double inv = rcp(fma(dr, dr, di * di));
+        // Im(c T conj(D)) / |D|^2
+        const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
+        double v = fma(c.cr, ui, c.ci * ur) * inv;
+        if (RA) {
+            const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
+            v = fma(inv, fma(lm[j] * s2, c.k0, rh * q2 * c.k1), v);
+        }
+        acc[j] = c.valid ? v : 0.0;
+        if (j > 0) {  // (R, S) at site n - 1
+            double ar = c.Er - u[j], ai = c.Ei;
+            if (EDGE) {
+                if (n == N - 1) {
+                    ar -= c.s1r;
+                    ai -= c.s1i;
+                }
+            }
+            const double h2 = EDGE ? (((n - 1) & 1) ? c.hg2 : c.hb2) : (((j - 1) & 1) ? c.hg2 : c.hb2);
+            const double nrr = h2 * Sr, nri = h2 * Si;
+            const double nsr = fma(ar, Sr, fma(-ai, Si, -Rr));
+            const double nsi = fma(ar, Si, fma(ai, Sr, -Ri));
+            Rr = nrr;
+            Ri = nri;
+            Sr = nsr;
+            Si = nsi;
+            if (RA) rh *= h2;
         }
     }
 }
@@ -428,6 +563,37 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
     const R* __restrict__ ck = reinterpret_cast<const R*>(wscratch + 4 * kWarp) + lane;
     const Chain<R> c = make_chain<R, RA>(T, cr, s0r, s0i, s1r, s1i);
 
+    if constexpr (sizeof(R) == 8) {
+        // the next segment's checkpoint is loaded while this one is computed
+        CkVals cur = load_ck<RA>(ck + (size_t)su.seg0 * CL::NC * kWarp);
+        for (int s = su.seg0; s < su.seg1; ++s) {
+            const int n0 = s * K;
+            CkVals nxt = cur;
+            if (s + 1 < su.seg1) nxt = load_ck<RA>(ck + (size_t)(s + 1) * CL::NC * kWarp);
+            double u[K], acc[K];
+            const bool interior = n0 > 0 && n0 + K < N;
+            if (interior) {
+                const double2* u2 = reinterpret_cast<const double2*>(U + n0);  // n0 even, U 16-byte aligned
+#pragma unroll
+                for (int k = 0; k < K / 2; ++k) {
+                    const double2 v = __ldg(u2 + k);
+                    u[2 * k] = v.x;
+                    u[2 * k + 1] = v.y;
+                }
+                segment_proj<RA, false>(c, n0, cur, u, acc);
+            } else {
+#pragma unroll
+                for (int k = 0; k < K; ++k) u[k] = (n0 + k < N) ? __ldg(U + n0 + k) : 0.0;
+                segment_proj<RA, true>(c, n0, cur, u, acc);
+            }
+            cur = nxt;
+            const double tot = warp_reduce_scatter<K>(acc, lane);
+            constexpr int shift = (K == 16) ? 1 : 2;
+            const int j = lane >> shift;
+            if ((lane & ((1 << shift) - 1)) == 0 && n0 + j < N) prow[n0 + j] = tot;
+        }
+        return;
+    }
     for (int s = su.seg0; s < su.seg1; ++s) {
         const int n0 = s * K;
         const R* p = ck + (size_t)s * CL::NC * kWarp;
@@ -586,8 +752,10 @@ cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const W
     if (num_warps <= 0) return cudaSuccess;
     if (warps_per_block < 1 || warps_per_block > 4) warps_per_block = 4;
     const int threads = warps_per_block * kWarp;
-    rgf_pass1_kernel<<<(num_warps + warps_per_block - 1) / warps_per_block, threads, 0, stream>>>(
-        d_tubes, d_chains, d_warps, num_warps, static_cast<double*>(d_scratch));
+    (void)threads;
+    // pass 1 is latency-bound: one warp per block spreads the chains evenly over the SMs
+    rgf_pass1_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
+                                                        static_cast<double*>(d_scratch));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (mid_event) cudaEventRecord(mid_event, stream);
