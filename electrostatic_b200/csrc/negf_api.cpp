@@ -157,8 +157,10 @@ struct negf_tube {
     std::vector<double> beta, gaps, y_nm;
     // potential
     double Uc[2] = {0.0, 0.0};
-    double* d_U = nullptr;
-    double* d_zero = nullptr;
+    double* d_U = nullptr;     // interior of d_U_pad: N sites
+    double* d_zero = nullptr;  // interior of d_zero_pad
+    double* d_U_pad = nullptr;  // kPadLo zeros, N sites, kPadHi zeros
+    double* d_zero_pad = nullptr;
     double* d_rho0 = nullptr;
     // contacts / limits (NEGF_Common.cpp:1687-1787)
     double mu[2] = {0.0, 0.0}, kT[2] = {0.0, 0.0};
@@ -170,8 +172,8 @@ struct negf_tube {
     int version = 0;
     int shard_rank = 0, shard_world = 1;
     ~negf_tube() {
-        if (d_U) cudaFree(d_U);
-        if (d_zero) cudaFree(d_zero);
+        if (d_U_pad) cudaFree(d_U_pad);
+        if (d_zero_pad) cudaFree(d_zero_pad);
         if (d_rho0) cudaFree(d_rho0);
     }
 };
@@ -676,11 +678,16 @@ int negf_tube_create(const negf_tube_desc* d, negf_tube** out) {
     cudaGetDevice(&t->device);
     t->mu[0] = d->contact_mu[0];
     t->mu[1] = d->contact_mu[1];
-    NEGF_CUDA(cudaMalloc(&t->d_U, sizeof(double) * t->N));
-    NEGF_CUDA(cudaMalloc(&t->d_zero, sizeof(double) * t->N));
+    // zero padding on both sides lets the kernels load whole segments of U
+    // without bounds checks
+    const size_t padded = sizeof(double) * (negf::kPadLo + t->N + negf::kPadHi);
+    NEGF_CUDA(cudaMalloc(&t->d_U_pad, padded));
+    NEGF_CUDA(cudaMalloc(&t->d_zero_pad, padded));
+    NEGF_CUDA(cudaMemset(t->d_U_pad, 0, padded));
+    NEGF_CUDA(cudaMemset(t->d_zero_pad, 0, padded));
+    t->d_U = t->d_U_pad + negf::kPadLo;
+    t->d_zero = t->d_zero_pad + negf::kPadLo;
     NEGF_CUDA(cudaMalloc(&t->d_rho0, sizeof(double) * t->N));
-    NEGF_CUDA(cudaMemset(t->d_U, 0, sizeof(double) * t->N));
-    NEGF_CUDA(cudaMemset(t->d_zero, 0, sizeof(double) * t->N));
     NEGF_CUDA(cudaMemset(t->d_rho0, 0, sizeof(double) * t->N));
     {
         std::lock_guard<std::mutex> lk(g_mu);

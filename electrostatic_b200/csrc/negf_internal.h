@@ -12,10 +12,12 @@ namespace negf {
 constexpr int kMaxModes = 32;   // distinct modes per tube kept on the device
 constexpr int kSeg = 8;         // sites per checkpoint segment of the RGF sweeps
 constexpr int kWarp = 32;
+constexpr int kPadLo = kSeg;      // zero doubles before a tube's potential buffer
+constexpr int kPadHi = 2 * kSeg;  // zero doubles after it
 
 // Per-tube record read by the RGF kernel (one per tube of a launch).
 struct __align__(16) TubeDev {
-    const double* U;   // site potential [N] (device)
+    const double* U;   // site potential [N] (device), kPadLo / kPadHi zeros around it
     int N;             // sites
     int num_modes;
     double gamma;      // hopping [eV]

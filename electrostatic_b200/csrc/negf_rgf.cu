@@ -335,6 +335,82 @@ __device__ __forceinline__ void proj_normalise(Proj<R>& p, R& yr, R& yi) {
     p.H = 1;
 }
 
+// One block of pass 1: renormalise both sweeps and store their checkpoints,
+// prefetch the potentials of the next block into (nf, nb), then advance the
+// forward sweep through segment blk and the backward sweep through segment
+// nseg-1-blk.
+template <typename R, bool RA>
+__device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<R>& b, int blk, int nseg,
+                                            const double* __restrict__ U, R* __restrict__ ck, const R (&uf)[kSeg],
+                                            const R (&ub)[kSeg], R (&nf)[kSeg], R (&nb)[kSeg], R hfull) {
+    constexpr int K = kSeg;
+    using CL = CkLayout<RA>;
+    const int N = c.N;
+    const int fs = blk, bs = nseg - 1 - blk;
+    const int f0 = fs * K;                  // forward segment start
+    const int be = min(bs * K + K, N) - 1;  // backward segment end
+    R yr, yi, xr, xi;
+    proj_normalise<R, RA>(f, yr, yi);
+    proj_normalise<R, RA>(b, xr, xi);
+    {
+        R* p = ck + (size_t)fs * CL::NC * kWarp;
+        p[CL::Y * kWarp] = yr;
+        p[(CL::Y + 1) * kWarp] = yi;
+        if (RA) p[CL::L * kWarp] = f.lam;
+        R* q = ck + (size_t)bs * CL::NC * kWarp;
+        q[CL::X * kWarp] = xr;
+        q[(CL::X + 1) * kWarp] = xi;
+        if (RA) q[CL::RHO * kWarp] = b.lam;
+    }
+    if (blk + 1 < nseg) {
+        // next forward segment fs+1 and next backward segment bs-1 (full, bs >= 1):
+        // 16-byte aligned, inside the padded buffer
+        const double2* pf = reinterpret_cast<const double2*>(U + f0 + K);
+        const double2* pb = reinterpret_cast<const double2*>(U + (bs - 1) * K);
+#pragma unroll
+        for (int k = 0; k < K / 2; ++k) {
+            const double2 vf = __ldg(pf + k), vb = __ldg(pb + k);
+            nf[2 * k] = (R)vf.x;
+            nf[2 * k + 1] = (R)vf.y;
+            nb[K - 1 - 2 * k] = (R)vb.x;
+            nb[K - 2 - 2 * k] = (R)vb.y;
+        }
+    }
+    const bool interior = (f0 > 0) && (f0 + K < N) && (be < N - 1) && (bs > 0) && (be == bs * K + K - 1);
+    if (interior) {
+        // forward sites f0 + j (parity of j since f0 is even); backward sites
+        // be - j use h_{be-j-1}, parity of j since be - 1 is even.
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const R h2 = (j & 1) ? c.hg2 : c.hb2;
+            proj_step_int(c, f, uf[j], h2);
+            proj_step_int(c, b, ub[j], h2);
+        }
+        f.H = hfull;
+        b.H = hfull;
+    } else {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int n = f0 + j;
+            if (n < N - 1) {
+                const R h2 = (n & 1) ? c.hg2 : c.hb2;
+                if (n == 0)
+                    proj_step_edge(c, f, uf[j], h2, c.s0r, c.s0i);
+                else
+                    proj_step(c, f, uf[j], h2);
+            }
+            const int m = be - j;  // backward step at site m gives X_{m-1}
+            if (m >= bs * K && m >= 1) {
+                const R h2 = ((m - 1) & 1) ? c.hg2 : c.hb2;
+                if (m == N - 1)
+                    proj_step_edge(c, b, ub[j], h2, c.s1r, c.s1i);
+                else
+                    proj_step(c, b, ub[j], h2);
+            }
+        }
+    }
+}
+
 // Pass 1: forward (Y, lambda) and backward (X, rho) sweeps run together
 // (they are independent), in projective form, storing the state at every
 // segment start (forward) and segment end (backward).  Block b advances the
@@ -368,80 +444,21 @@ __device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, co
     R hfull = 1;                  // prod of h^2 over a full segment: (beta^2 gamma^2)^(K/2)
 #pragma unroll
     for (int j = 0; j < K / 2; ++j) hfull *= c.hb2 * c.hg2;
-    R uf[K], ub[K];
+    // potentials of the first block: forward segment 0, backward segment nseg-1
+    // (the buffer has kPadLo zeros before site 0 and kPadHi after site N-1)
+    R ua_f[K], ua_b[K], ub_f[K], ub_b[K];
     {
-        const int be = min((nseg - 1) * K + K, N) - 1;
+        const int be = N - 1;
 #pragma unroll
         for (int j = 0; j < K; ++j) {
-            uf[j] = (j < N) ? (R)__ldg(U + j) : (R)0;
-            ub[j] = (be - j >= 0) ? (R)__ldg(U + be - j) : (R)0;
+            ua_f[j] = (R)__ldg(U + j);
+            ua_b[j] = (R)__ldg(U + be - j);
         }
     }
-    for (int blk = 0; blk < nseg; ++blk) {
-        const int fs = blk, bs = nseg - 1 - blk;
-        const int f0 = fs * K;                       // forward segment start
-        const int be = min(bs * K + K, N) - 1;       // backward segment end
-        R yr, yi, xr, xi;
-        proj_normalise<R, RA>(f, yr, yi);
-        proj_normalise<R, RA>(b, xr, xi);
-        {
-            R* p = ck + (size_t)fs * CL::NC * kWarp;
-            p[CL::Y * kWarp] = yr;
-            p[(CL::Y + 1) * kWarp] = yi;
-            if (RA) p[CL::L * kWarp] = f.lam;
-            R* q = ck + (size_t)bs * CL::NC * kWarp;
-            q[CL::X * kWarp] = xr;
-            q[(CL::X + 1) * kWarp] = xi;
-            if (RA) q[CL::RHO * kWarp] = b.lam;
-        }
-        // prefetch the next block's potentials
-        R nf[K], nb[K];
-        {
-            const int f1 = f0 + K, be1 = bs * K - 1;
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                nf[j] = (f1 + j < N) ? (R)__ldg(U + f1 + j) : (R)0;
-                nb[j] = (be1 - j >= 0) ? (R)__ldg(U + be1 - j) : (R)0;
-            }
-        }
-        const bool interior = (f0 > 0) && (f0 + K < N) && (be < N - 1) && (be - K + 1 > 0) && (be == bs * K + K - 1);
-        if (interior) {
-            // forward sites f0 + j (parity of j since f0 is even); backward sites
-            // be - j use h_{be-j-1}, parity of j since be - 1 is even.
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                const R h2 = (j & 1) ? c.hg2 : c.hb2;
-                proj_step_int(c, f, uf[j], h2);
-                proj_step_int(c, b, ub[j], h2);
-            }
-            f.H = hfull;
-            b.H = hfull;
-        } else {
-#pragma unroll
-            for (int j = 0; j < K; ++j) {
-                const int n = f0 + j;
-                if (n < N - 1) {
-                    const R h2 = (n & 1) ? c.hg2 : c.hb2;
-                    if (n == 0)
-                        proj_step_edge(c, f, uf[j], h2, c.s0r, c.s0i);
-                    else
-                        proj_step(c, f, uf[j], h2);
-                }
-                const int m = be - j;  // backward step at site m gives X_{m-1}
-                if (m >= bs * K && m >= 1) {
-                    const R h2 = ((m - 1) & 1) ? c.hg2 : c.hb2;
-                    if (m == N - 1)
-                        proj_step_edge(c, b, ub[j], h2, c.s1r, c.s1i);
-                    else
-                        proj_step(c, b, ub[j], h2);
-                }
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            uf[j] = nf[j];
-            ub[j] = nb[j];
-        }
+    for (int blk = 0; blk < nseg; blk += 2) {
+        pass1_block<R, RA>(c, f, b, blk, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+        if (blk + 1 >= nseg) break;
+        pass1_block<R, RA>(c, f, b, blk + 1, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
     }
 }
 
@@ -514,14 +531,15 @@ __device__ __forceinline__ void segment_proj(const Chain<double>& c, int n0, con
         // D = S Q_{n+1} - R Q_n
         const double dr = fma(Sr, qr[j + 1], fma(-Si, qi[j + 1], fma(-Rr, qr[j], Ri * qi[j])));
         const double di = fma(Sr, qi[j + 1], fma(Si, qr[j + 1], fma(-Rr, qi[j], -Ri * qr[j])));
-        const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);  // T = Q S
         const double inv = rcp(fma(dr, dr, di * di));
-        // Im(c T conj(D)) / |D|^2
-        const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
-        double v = fma(c.cr, ui, c.ci * ur) * inv;
-        if (RA) {
+        double v;
+        if (RA) {  // real-axis chains carry no contour coefficient (c = 0)
             const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
-            v = fma(inv, fma(lm[j] * s2, c.k0, rh * q2 * c.k1), v);
+            v = inv * fma(lm[j] * s2, c.k0, rh * q2 * c.k1);
+        } else {  // Im(c T conj(D)) / |D|^2 with T = Q S
+            const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
+            const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
+            v = fma(c.cr, ui, c.ci * ur) * inv;
         }
         acc[j] = c.valid ? v : 0.0;
         if (j > 0) {  // (R, S) at site n - 1
