@@ -400,83 +400,85 @@ struct TubePass {
     bool rho0_pass;    // Rho0 (zero potential) instead of the charge pass
 };
 
-void push_group(ChainTable& ct, std::vector<negf::ChainRec>& lanes, const negf_tube& t, int tube_index, int kind,
-                int fp32) {
-    if (lanes.empty()) return;
-    const negf::ChainRec pad_proto = lanes.front();
-    while (lanes.size() % negf::kWarp) {
-        negf::ChainRec p = pad_proto;
-        p.mode = -1;
-        p.cr = p.ci = p.b0 = p.b1 = 0.0;
-        lanes.push_back(p);
-    }
-    const int nw = int(lanes.size() / negf::kWarp);
-    for (int w = 0; w < nw; ++w) {
-        negf::WarpRec wr{};
-        wr.tube = tube_index;
-        wr.kind = kind;
-        wr.fp32 = fp32;
-        ct.warps.push_back(wr);
-        for (int l = 0; l < negf::kWarp; ++l) {
-            const negf::ChainRec& c = lanes[(size_t)w * negf::kWarp + l];
-            ct.chains.push_back(c);
-            if (c.mode >= 0) {
-                ct.updates += t.N;
-                if (fp32) ct.updates_fp32 += t.N;
-                if (kind == negf::kRealAxis)
-                    ct.realaxis_updates += t.N;
-                else
-                    ct.contour_updates += t.N;
-            }
+// Append-only output used by the chain-table builder: a growing std::vector
+// (negf_compute_charge) or a fixed caller-provided array (the
+// allocation-free entry point; overflow is reported, never allocated).
+template <class T>
+struct Out {
+    std::vector<T>* vec = nullptr;
+    T* arr = nullptr;
+    size_t cap = 0, n = 0;
+    bool overflow = false;
+    void push(const T& v) {
+        if (vec) {
+            vec->push_back(v);
+            ++n;
+        } else if (n < cap) {
+            arr[n++] = v;
+        } else {
+            overflow = true;
         }
     }
-    lanes.clear();
+    T& at(size_t i) { return vec ? (*vec)[i] : arr[i]; }
+    size_t size() const { return n; }
+};
+
+struct TableCounts {
+    long long updates = 0, updates_fp32 = 0, contour_updates = 0, realaxis_updates = 0;
+    long long partial_doubles = 0, scratch_doubles = 0;
+    int max_N = 0;
+};
+
+// Energy point idx of a pass.  Contour chains: Im(c G) with
+// c = (-2/pi) w J f_eq (RhoEq, NEGF_Common.cpp:3738-3754), (-2/pi) w J
+// (Rho0, :4071-4084) or -4 i kT (poles, :3934-3948).  Real-axis chains:
+// b_k = Re((-1/pi) w J f_k) (RhoNonEq, :3372-3466).  The degeneracy and
+// Gamma_k are applied in the kernel.
+struct Item {
+    cplx E, c;
+    double b0, b1;
+    int kind;
+};
+int pass_items(const negf_tube& t, bool rho0_pass) {
+    return rho0_pass ? (int)t.rho0_pts.size() : (int)(t.eq_pts.size() + t.poles.size() + t.noneq_pts.size());
+}
+Item pass_item(const negf_tube& t, bool rho0_pass, int idx) {
+    if (rho0_pass) {
+        const Pt& p = t.rho0_pts[idx];
+        return {p.E, (-kSpinDegen / kPi) * p.w * p.J, 0, 0, negf::kContour};
+    }
+    const int ne = (int)t.eq_pts.size(), np = (int)t.poles.size();
+    if (idx < ne) {
+        const Pt& p = t.eq_pts[idx];
+        return {p.E, (-kSpinDegen / kPi) * p.w * p.J * fermi(p.E - t.mu_min, t.kT_min), 0, 0, negf::kContour};
+    }
+    if (idx < ne + np) return {t.poles[idx - ne], cplx(0.0, -2 * t.kT_min * kSpinDegen), 0, 0, negf::kContour};
+    const Pt& p = t.noneq_pts[idx - ne - np];
+    const cplx base = (-kSpinDegen / (2 * kPi)) * p.w * p.J;
+    return {p.E, 0.0, (base * fermi(p.E - t.mu[0], t.kT[0])).real(), (base * fermi(p.E - t.mu[1], t.kT[1])).real(),
+            negf::kRealAxis};
 }
 
-// Chains of one tube.  Contour chains: Im(c G) with c = (-2/pi) w J f_eq
-// (RhoEq, NEGF_Common.cpp:3738-3754), (-2/pi) w J (Rho0, :4071-4084) or
-// -4 i kT (poles, :3934-3948).  Real-axis chains: b_k = Re((-1/pi) w J f_k)
-// (RhoNonEq, :3372-3466).  The degeneracy and Gamma_k are applied in the kernel.
-void build_tube_chains(ChainTable& ct, const TubePass& tp) {
+// Chains of one tube, grouped by (kind, precision) with each group padded
+// to whole warps (padding lanes: mode -1, zero coefficients).
+void build_tube_chains(Out<negf::ChainRec>& chains, Out<negf::WarpRec>& warps, TableCounts& cnt, const TubePass& tp) {
     const negf_tube& t = *tp.t;
     const int M = t.d.num_modes;
-    struct Item {
-        cplx E;
-        cplx c;
-        double b0, b1;
-        int kind;
-    };
-    std::vector<Item> items;
-    if (tp.rho0_pass) {
-        for (const Pt& p : t.rho0_pts) items.push_back({p.E, (-kSpinDegen / kPi) * p.w * p.J, 0, 0, negf::kContour});
-    } else {
-        for (const Pt& p : t.eq_pts) {
-            const cplx f = fermi(p.E - t.mu_min, t.kT_min);
-            items.push_back({p.E, (-kSpinDegen / kPi) * p.w * p.J * f, 0, 0, negf::kContour});
-        }
-        for (const cplx& E : t.poles) items.push_back({E, cplx(0.0, -2 * t.kT_min * kSpinDegen), 0, 0, negf::kContour});
-        for (const Pt& p : t.noneq_pts) {
-            const cplx base = (-kSpinDegen / (2 * kPi)) * p.w * p.J;
-            const double b0 = (base * fermi(p.E - t.mu[0], t.kT[0])).real();
-            const double b1 = (base * fermi(p.E - t.mu[1], t.kT[1])).real();
-            items.push_back({p.E, 0.0, b0, b1, negf::kRealAxis});
-        }
-        int lo = 0, hi = (int)items.size();
-        negf_shard_range((int)items.size(), t.shard_rank, t.shard_world, &lo, &hi);
-        items = std::vector<Item>(items.begin() + lo, items.begin() + hi);
-    }
+    const int total = pass_items(t, tp.rho0_pass);
+    int lo = 0, hi = total;
+    if (!tp.rho0_pass) negf_shard_range(total, t.shard_rank, t.shard_world, &lo, &hi);
     const bool mixed = t.d.precision == NEGF_PREC_MIXED && !tp.rho0_pass;
     const double band = t.d.mixed_fp64_band;
-    std::vector<negf::ChainRec> lanes;
-    // groups: (kind, precision); the FP64 group first
     for (int kind = 0; kind < 2; ++kind)
         for (int fp32 = 0; fp32 < 2; ++fp32) {
             if (fp32 && !mixed) continue;
-            for (int m = 0; m < M; ++m)
-                for (const Item& it : items) {
-                    if (it.kind != kind) continue;
-                    const int want32 = mixed && std::fabs(it.E.imag()) >= band ? 1 : 0;
-                    if (want32 != fp32) continue;
+            const size_t first = chains.size();
+            for (int idx = lo; idx < hi; ++idx) {
+                const Item it = pass_item(t, tp.rho0_pass, idx);
+                if (it.kind != kind) continue;
+                const int want32 = mixed && std::fabs(it.E.imag()) >= band ? 1 : 0;
+                if (want32 != fp32) continue;
+                for (int m = 0; m < M; ++m) {
                     negf::ChainRec c{};
                     c.Er = it.E.real();
                     c.Ei = it.E.imag();
@@ -485,46 +487,98 @@ void build_tube_chains(ChainTable& ct, const TubePass& tp) {
                     c.b0 = it.b0;
                     c.b1 = it.b1;
                     c.mode = m;
-                    lanes.push_back(c);
+                    chains.push(c);
+                    cnt.updates += t.N;
+                    if (fp32) cnt.updates_fp32 += t.N;
+                    if (kind == negf::kRealAxis)
+                        cnt.realaxis_updates += t.N;
+                    else
+                        cnt.contour_updates += t.N;
                 }
-            push_group(ct, lanes, t, tp.tube_index, kind, fp32);
+            }
+            const size_t n = chains.size() - first;
+            if (n == 0 || chains.overflow) continue;
+            const negf::ChainRec proto = chains.at(first);
+            for (size_t k = n; k % negf::kWarp; ++k) {
+                negf::ChainRec p = proto;
+                p.mode = -1;
+                p.cr = p.ci = p.b0 = p.b1 = 0.0;
+                chains.push(p);
+            }
+            for (size_t w = 0; w < (n + negf::kWarp - 1) / negf::kWarp; ++w) {
+                negf::WarpRec wr{};
+                wr.tube = tp.tube_index;
+                wr.kind = kind;
+                wr.fp32 = fp32;
+                warps.push(wr);
+            }
         }
 }
 
-void build_table(ChainTable& ct, const std::vector<TubePass>& passes) {
-    ct = ChainTable();
-    // launch order: longest tubes first
-    std::vector<int> order(passes.size());
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return passes[a].t->N > passes[b].t->N; });
-    std::vector<negf::ReduceTube> rts(passes.size());
+// Launch tables of a set of tube passes.  Launch order: longest tubes first
+// (order[] is caller scratch of passes.size() ints); rts[i] describes pass i.
+void build_table_generic(const TubePass* passes, int num_passes, int* order, Out<negf::ChainRec>& chains,
+                         Out<negf::WarpRec>& warps, Out<negf::SegUnit>& units, negf::ReduceTube* rts,
+                         TableCounts& cnt) {
+    cnt = TableCounts();
+    for (int i = 0; i < num_passes; ++i) order[i] = i;
+    for (int i = 1; i < num_passes; ++i) {  // stable insertion sort by descending N
+        const int v = order[i];
+        int j = i - 1;
+        while (j >= 0 && passes[order[j]].t->N < passes[v].t->N) {
+            order[j + 1] = order[j];
+            --j;
+        }
+        order[j + 1] = v;
+    }
     long long row = 0, ck = 0;
-    for (int oi : order) {
+    for (int k = 0; k < num_passes; ++k) {
+        const int oi = order[k];
         const TubePass& tp = passes[oi];
-        const size_t w0 = ct.warps.size();
-        build_tube_chains(ct, tp);
+        const size_t w0 = warps.size();
+        build_tube_chains(chains, warps, cnt, tp);
         const int N = tp.t->N;
         negf::ReduceTube rt{};
         rt.row_base = row;
         rt.q_off = tp.q_off;
         rt.N = N;
-        rt.num_rows = int(ct.warps.size() - w0);
+        rt.num_rows = int(warps.size() - w0);
         rt.rho0 = (!tp.rho0_pass && tp.t->shard_rank == 0) ? tp.t->d_rho0 : nullptr;
         const int nseg = (N + negf::kSeg - 1) / negf::kSeg;
-        for (size_t w = w0; w < ct.warps.size(); ++w) {
-            ct.warps[w].row_off = row;
+        for (size_t w = w0; w < warps.size() && !warps.overflow; ++w) {
+            warps.at(w).row_off = row;
             row += N;
-            ct.warps[w].ck_off = ck;
-            ck += negf::rgf_scratch_doubles(N, ct.warps[w].kind, ct.warps[w].fp32);
+            warps.at(w).ck_off = ck;
+            ck += negf::rgf_scratch_doubles(N, warps.at(w).kind, warps.at(w).fp32);
             for (int s0 = 0; s0 < nseg; s0 += negf::kSegsPerUnit)
-                ct.units.push_back({(int)w, s0, std::min(nseg, s0 + negf::kSegsPerUnit), 0});
+                units.push({(int)w, s0, std::min(nseg, s0 + negf::kSegsPerUnit), 0});
         }
         rts[oi] = rt;
-        ct.max_N = std::max(ct.max_N, N);
+        cnt.max_N = std::max(cnt.max_N, N);
     }
-    ct.rts = rts;
-    ct.partial_doubles = row;
-    ct.scratch_doubles = ck;
+    cnt.partial_doubles = row;
+    cnt.scratch_doubles = ck;
+}
+
+void build_table(ChainTable& ct, const std::vector<TubePass>& passes) {
+    ct = ChainTable();
+    Out<negf::ChainRec> oc;
+    oc.vec = &ct.chains;
+    Out<negf::WarpRec> ow;
+    ow.vec = &ct.warps;
+    Out<negf::SegUnit> ou;
+    ou.vec = &ct.units;
+    ct.rts.resize(passes.size());
+    std::vector<int> order(passes.size());
+    TableCounts cnt;
+    build_table_generic(passes.data(), (int)passes.size(), order.data(), oc, ow, ou, ct.rts.data(), cnt);
+    ct.updates = cnt.updates;
+    ct.updates_fp32 = cnt.updates_fp32;
+    ct.contour_updates = cnt.contour_updates;
+    ct.realaxis_updates = cnt.realaxis_updates;
+    ct.partial_doubles = cnt.partial_doubles;
+    ct.scratch_doubles = cnt.scratch_doubles;
+    ct.max_N = cnt.max_N;
 }
 
 int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<negf::TubeDev>& tdev, bool rebuild,
@@ -767,6 +821,7 @@ int negf_tube_set_contact_mu(negf_tube* t, const double mu[2]) {
     t->mu[0] = mu[0];
     t->mu[1] = mu[1];
     t->limits_dirty = true;
+    update_paths(*t);  // host tables rebuilt here, not inside the charge calls
     return NEGF_OK;
 }
 
