@@ -28,6 +28,7 @@ EXPORTED = [
     "negf_last_stats", "negf_set_timing", "negf_broyden_create", "negf_broyden_destroy", "negf_broyden_set_input",
     "negf_broyden_step", "negf_broyden_reset", "negf_broyden_step_number", "negf_broyden_input_device_ptr",
     "negf_affine_potential", "negf_write_step", "negf_last_error", "negf_device_selftest",
+    "negf_compute_charge_noalloc",
 ]
 
 
@@ -113,6 +114,7 @@ def load():
         "negf_tube_set_energy_shard": [vp, C.c_int, C.c_int],
         "negf_shard_range": [C.c_int, C.c_int, C.c_int, ip, ip],
         "negf_compute_charge": [C.POINTER(vp), C.c_int, vp, C.c_int, vp],
+        "negf_compute_charge_noalloc": [C.POINTER(vp), C.c_int, vp, vp],
         "negf_last_stats": [C.POINTER(Stats)],
         "negf_set_timing": [C.c_int],
         "negf_broyden_create": [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(vp)],

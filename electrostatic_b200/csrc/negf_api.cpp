@@ -677,6 +677,59 @@ void write_table(FILE* f, const std::vector<double>& pos, const double* v, int n
 
 }  // namespace
 
+// ====================================================================== allocation-free planning
+namespace negf {
+
+int report(int code, const char* msg) { return fail(code, msg); }
+
+// Plans one charge launch into caller-provided fixed arrays (no allocation).
+// Requires every tube's energy paths to be current (they are rebuilt by
+// negf_tube_create / negf_tube_set_contact_mu).
+int plan_charge_fixed(negf_tube* const* tubes, int num_tubes, FixedPlan& fp) {
+    constexpr int kMaxPlanTubes = 64;
+    if (!tubes || num_tubes <= 0) return fail(NEGF_ERR_ARG, "null or empty tube batch");
+    if (num_tubes > kMaxPlanTubes || num_tubes > fp.tube_cap)
+        return fail(NEGF_ERR_ARG, "too many tubes for the allocation-free entry point (max " +
+                                      std::to_string(std::min(kMaxPlanTubes, fp.tube_cap)) + ")");
+    static TubePass passes[kMaxPlanTubes];  // calls of the allocation-free entry point never overlap (documented)
+    static int order[kMaxPlanTubes];
+    long long off = 0;
+    for (int i = 0; i < num_tubes; ++i) {
+        const negf_tube* t = tubes[i];
+        if (!t) return fail(NEGF_ERR_ARG, "null tube in batch");
+        if (t->limits_dirty) return fail(NEGF_ERR_STATE, "tube energy paths are not current");
+        passes[i] = {t, i, off, false};
+        fp.tubes[i] = make_tubedev(*t, false);
+        off += t->N;
+    }
+    Out<ChainRec> oc;
+    oc.arr = fp.chains;
+    oc.cap = fp.chain_cap;
+    Out<WarpRec> ow;
+    ow.arr = fp.warps;
+    ow.cap = fp.warp_cap;
+    Out<SegUnit> ou;
+    ou.arr = fp.units;
+    ou.cap = fp.unit_cap;
+    TableCounts cnt;
+    build_table_generic(passes, num_tubes, order, oc, ow, ou, fp.rts, cnt);
+    if (oc.overflow || ow.overflow || ou.overflow)
+        return fail(NEGF_ERR_ARG, "problem exceeds the launch-table capacity of the allocation-free entry point (" +
+                                      std::to_string(fp.chain_cap) + " chains, " + std::to_string(fp.warp_cap) +
+                                      " warps)");
+    fp.num_tubes = num_tubes;
+    fp.num_chains = oc.size();
+    fp.num_warps = ow.size();
+    fp.num_units = ou.size();
+    fp.partial_doubles = cnt.partial_doubles;
+    fp.scratch_doubles = cnt.scratch_doubles;
+    fp.max_N = cnt.max_N;
+    fp.total_sites = off;
+    return NEGF_OK;
+}
+
+}  // namespace negf
+
 // ====================================================================== C-ABI
 extern "C" {
 

@@ -85,6 +85,27 @@ cudaError_t launch_reduce(const ReduceTube* d_rt, int num_tubes, int max_N, cons
 long long rgf_scratch_doubles(int N, int kind, int fp32);
 int rgf_kernel_regs();  // registers per thread of the RGF kernel (0 if unknown)
 
+// Launch tables written into caller-provided fixed arrays (used by the
+// allocation-free entry point in negf_noalloc.cu).
+struct FixedPlan {
+    TubeDev* tubes;
+    ReduceTube* rts;
+    ChainRec* chains;
+    WarpRec* warps;
+    SegUnit* units;
+    int tube_cap;
+    size_t chain_cap, warp_cap, unit_cap;
+    // outputs
+    int num_tubes, max_N;
+    size_t num_chains, num_warps, num_units;
+    long long partial_doubles, scratch_doubles, total_sites;
+};
+}  // namespace negf
+struct negf_tube;
+namespace negf {
+int plan_charge_fixed(negf_tube* const* tubes, int num_tubes, FixedPlan& fp);
+int report(int code, const char* msg);  // sets negf_last_error, returns code
+
 // Broyden kernels (negf_broyden.cu).
 struct BroydenDev {
     int S, max_step, norm_type;

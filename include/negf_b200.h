@@ -140,6 +140,20 @@ int negf_shard_range(int num_points, int rank, int world, int* lo, int* hi);
  * q_on_device != 0, else a host pointer (the call then synchronises `stream`). */
 int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q_on_device, void* stream);
 
+/* Allocation-free variant of negf_compute_charge -- no counterpart in the
+ * reference.  For callers that cannot allocate device memory when they need
+ * the charge (work recorded while a stream is captured, applications whose
+ * device memory comes from their own pool, plugins that must not grow the
+ * host program's footprint).  It runs the same kernels, but keeps the launch
+ * tables, partial rows and checkpoints in one static device array of 32 MiB
+ * that every GPU loading this library holds until exit; it calls no
+ * cudaMalloc/cudaFree.  d_Q is a device pointer.  Problems that need more
+ * than 32 MiB of scratch are rejected with NEGF_ERR_ARG.  The first call on
+ * a device looks up the array's address (set-up), so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int negf_compute_charge_noalloc(negf_tube* const* tubes, int num_tubes, double* d_Q, void* stream);
+
 /* Per-call timing and work counters of the last negf_compute_charge
  * (kernel milliseconds measured with CUDA events on `stream`). */
 typedef struct negf_stats {
