@@ -188,6 +188,34 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+SCF_KW = dict(type_id=(17, 0), num_unitcells=100, num_modes=2, contact_mu=(-1.0, -1.0), contact_T=(300.0, 300.0),
+              eq_integration_pts=(32, 32, 32), E_valence_min=-10.0, E_pole_max=3.0)
+SCF_VG = [0.0, 0.1, 0.2, 0.3]
+SCF_WORKLOAD = ("config-1 self-consistent sweep: (17,0) CNT N=400, M=2, mu=(-1,-1) eV, 300 K, contour 32+32+32 "
+                "GL + Matsubara poles (E_pole_max 3 eV), gate-all-around stand-in (gate radius R+1.5 nm, eps 3.9), "
+                "Vg 0..0.3 V step 0.1, Broyden alpha=0.1 to 1e-6 absolute max-norm")
+
+
+def scf_measure(threads):
+    """Config-1 SCF sweep: device loop (FP64) vs the same loop on the CPU oracle."""
+    from electrostatic_b200.electrostatics import GateAllAround
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.scf import run_scf, run_scf_oracle
+    from oracle import oracle as O
+    tube = CNT(**SCF_KW)
+    y = tube.site_positions()
+    ot = O.OracleTube(**SCF_KW)
+    ga = GateAllAround(y, ot.radius, ot.radius + 1.5e-9)
+    run_scf(tube, ga, [0.0])  # warm-up (tables, caches)
+    rg = run_scf(tube, ga, SCF_VG)
+    ro = run_scf_oracle(ot, ga.K, SCF_VG, nthreads=threads)
+    dq = max(float(np.max(np.abs(a.Q - b.Q))) for a, b in zip(rg.steps, ro.steps))
+    return {"workload": SCF_WORKLOAD, "gpu_seconds": rg.seconds, "gpu_iterations": [s.iterations for s in rg.steps],
+            "cpu_seconds": ro.seconds, "cpu_iterations": [s.iterations for s in ro.steps], "cpu_cores": threads,
+            "cpu_kind": "port (oracle, O(N) walk; the reference path at Vds=0 has no real-axis walk)",
+            "max_abs_dQ_gpu_vs_cpu": dq, "speedup": ro.seconds / rg.seconds}
+
+
 def ring_positions_nm(unitcells, acc=1.42e-10):
     """Axial ring positions [nm] of a zigzag tube (CNT.cpp:93-132)."""
     y0 = -(unitcells / 2.0) * 3.0 * acc - acc / 2.0
@@ -204,6 +232,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-scf", action="store_true")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis)")
     args = ap.parse_args()
@@ -337,6 +366,7 @@ def main():
                    "sample": "8 of the 4096 energy points (every 512th: 2 contour + 6 real-axis), all 8 modes, "
                              "N=4000, faithful O(N)-per-site contact walk (NEGF_Common.cpp:3418-3426), "
                              f"{threads} threads over energies; {dt:.2f} s"}
+        scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                 "frac": achieved_tf / peak_tf if peak_tf else None,
                 "traffic": prof.get("dram_bytes_per_launch"),
@@ -354,7 +384,7 @@ def main():
                 "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
                            "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu,
+                "roofline": roof, "cpu_baseline": cpu, "scf": scf,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
                         "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},

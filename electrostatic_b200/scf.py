@@ -1,0 +1,129 @@
+"""Self-consistent NEGF-Poisson loop (the transport driver around the engine).
+
+Mirrors c_TransportSolver::Solve (Source/Solver/Transport/Transport.cpp:385-505):
+each iteration computes the site potential from the current input charge
+(the electrostatics stand-in of electrostatics.py replaces MLMG + gather),
+sets U_contact to the end-site potentials (Nanostructure.cpp:500-504), runs the
+NEGF charge pass and one Broyden modified-second step; the loop ends when the
+Broyden max-norm of the iteration's residual is <= Broyden_max_norm, and
+Broyden is reset between bias steps (Reset_ForNextBiasStep,
+Transport.cpp:713-717; Broyden_Parallel_General.cpp:250-355).  Every vector
+stays on the device; per iteration the host reads the two contact potentials
+and the Broyden norm.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+
+@dataclass
+class StepResult:
+    Vg: float
+    iterations: int
+    norm: float
+    Q: np.ndarray
+    U: np.ndarray
+    seconds: float
+
+
+@dataclass
+class SCFResult:
+    steps: list = field(default_factory=list)
+
+    @property
+    def total_iterations(self):
+        return sum(s.iterations for s in self.steps)
+
+    @property
+    def seconds(self):
+        return sum(s.seconds for s in self.steps)
+
+
+def device_view(ptr: int, n: int):
+    """Zero-copy float64 torch view of n doubles of device memory at ptr."""
+    import torch
+
+    class _Array:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (int(ptr), False), "version": 3}
+
+    return torch.as_tensor(_Array(), device="cuda")
+
+
+def run_scf(tube, electro, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
+            initial_charge=0.0, reset_with_previous_charge=False, stream=None):
+    """Bias sweep of self-consistent solves for one tube on the current device."""
+    import torch
+    from .negf import Broyden, compute_charge
+
+    L = _lib.load()
+    N = tube.num_field_sites
+    dev = torch.device("cuda")
+    n_in = torch.full((N,), float(initial_charge), dtype=torch.float64, device=dev)
+    Q = torch.zeros(N, dtype=torch.float64, device=dev)
+    br = Broyden(n_in, max_step=max_step, fraction=fraction, norm_type=norm_type)
+    U_ptr = tube.potential_device_ptr()
+    U_view = device_view(U_ptr, N)
+    s_ptr = None if stream is None else C.c_void_p(stream.cuda_stream)
+    res = SCFResult()
+    for Vg in Vg_list:
+        Kd, U0 = electro.device_operator(Vg)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, nrm = 0, float("inf")
+        while True:
+            if br.step_number > max_step:  # Transport.cpp:389-393
+                raise RuntimeError("Broyden_Step has exceeded the Broyden_Threshold_MaxStep")
+            check(L.negf_affine_potential(C.c_void_p(Kd.data_ptr()), C.c_void_p(U0.data_ptr()),
+                                          C.c_void_p(n_in.data_ptr()), C.c_void_p(U_ptr), N, s_ptr),
+                  "negf_affine_potential")
+            ends = U_view[[0, N - 1]].cpu().numpy()
+            tube.set_potential_device(U_ptr, (float(ends[0]), float(ends[1])), stream=stream)
+            compute_charge([tube], out=Q, stream=stream)
+            nrm = br.step(Q, n_in_out=n_in, stream=stream)
+            it += 1
+            if not (nrm > max_norm):
+                break
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res.steps.append(StepResult(Vg, it, nrm, Q.cpu().numpy().copy(), U_view.cpu().numpy().copy(), dt))
+        br.reset(keep_charge=reset_with_previous_charge, init_value=initial_charge)
+        if reset_with_previous_charge:
+            n_in.copy_(device_view(br.input_device_ptr(), N))
+        else:
+            n_in.fill_(float(initial_charge))
+    br.close()
+    return res
+
+
+def run_scf_oracle(oracle_tube, K, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
+                   initial_charge=0.0, reset_with_previous_charge=False, nthreads=8):
+    """The same loop on the CPU oracle (test infrastructure and CPU baseline)."""
+    from oracle import oracle as O
+
+    N = oracle_tube.N
+    n_in = np.full(N, float(initial_charge))
+    br = O.OracleBroyden(n_in, max_step=max_step, fraction=fraction, norm_type=norm_type)
+    res = SCFResult()
+    for Vg in Vg_list:
+        t0 = time.perf_counter()
+        it, nrm = 0, float("inf")
+        while True:
+            U = -float(Vg) - K @ n_in
+            oracle_tube.set_potential(U, (U[0], U[-1]))
+            Q = oracle_tube.charge(nthreads=nthreads)
+            nrm, n_in, _ = br.step(Q)
+            it += 1
+            if not (nrm > max_norm):
+                break
+        res.steps.append(StepResult(Vg, it, nrm, Q, U, time.perf_counter() - t0))
+        br.reset(keep_charge=reset_with_previous_charge, init_value=initial_charge)
+        if not reset_with_previous_charge:
+            n_in = np.full(N, float(initial_charge))
+    return res
