@@ -25,7 +25,7 @@ EXPORTED = [
     "negf_tube_potential_device_ptr", "negf_tube_set_contact_mu", "negf_tube_energy_points",
     "negf_desc_energy_points", "negf_tube_noneq",
     "negf_tube_total_integration_pts", "negf_tube_set_energy_shard", "negf_shard_range", "negf_compute_charge",
-    "negf_last_stats", "negf_set_timing", "negf_broyden_create", "negf_broyden_destroy", "negf_broyden_set_input",
+    "negf_last_stats", "negf_set_timing", "negf_set_tuning", "negf_broyden_create", "negf_broyden_destroy", "negf_broyden_set_input",
     "negf_broyden_step", "negf_broyden_reset", "negf_broyden_step_number", "negf_broyden_input_device_ptr",
     "negf_affine_potential", "negf_write_step", "negf_last_error", "negf_device_selftest",
     "negf_compute_charge_noalloc",
@@ -117,6 +117,7 @@ def load():
         "negf_compute_charge_noalloc": [C.POINTER(vp), C.c_int, vp, vp],
         "negf_last_stats": [C.POINTER(Stats)],
         "negf_set_timing": [C.c_int],
+        "negf_set_tuning": [C.c_int, C.c_int],
         "negf_broyden_create": [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(vp)],
         "negf_broyden_destroy": [vp],
         "negf_broyden_set_input": [vp, vp, C.c_int, vp],

@@ -987,6 +987,19 @@ int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q
     return NEGF_OK;
 }
 
+int negf_set_tuning(int key, int value) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    Workspace& W = ws();
+    switch (key) {
+        case NEGF_TUNE_PASS2_WARPS_PER_BLOCK:
+            if (value != 1 && value != 2 && value != 4) return fail(NEGF_ERR_ARG, "warps per block must be 1, 2 or 4");
+            W.warps_per_block = value;
+            return NEGF_OK;
+        default:
+            return fail(NEGF_ERR_ARG, "unknown tuning key");
+    }
+}
+
 int negf_set_timing(int enable) {
     std::lock_guard<std::mutex> lk(g_mu);
     ws().timing = enable != 0;

@@ -54,6 +54,10 @@ __device__ __forceinline__ double rcp(double x) {
     const double e = fma(-x, y, 1.0);
     return fma(y, fma(e, e, e), y);
 }
+// Cache hint: bring the line holding p into L1 (every caller passes an
+// address inside its buffer).
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ float rcp(float x) {
     float y;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -278,9 +282,10 @@ struct CkLayout {
 // Q = 1 once per segment keeps |P|, |Q| < (max |alpha|)^kSeg.
 template <typename R>
 struct Proj {
-    R pr, pi, qr, qi;  // P, Q
-    R lam;             // lambda (or rho) at the last renormalisation
-    R H;               // product of h^2 since the last renormalisation
+    R pr, pi, qr, qi;  // P, Q (scaled projective state)
+    R lam;             // lambda (or rho) at the last segment boundary
+    R H;               // product of h^2 since the last segment boundary
+    R rq;              // 1 / |Q|^2 at the last segment boundary
 };
 
 // Linear step with hopping square h2 at a site of potential u (interior
@@ -321,25 +326,33 @@ __device__ __forceinline__ void proj_step_edge(const Chain<R>& c, Proj<R>& p, R 
     p.qi = nqi;
     p.H *= h2;
 }
-// Y = P / Q, lambda *= H / |Q|^2, then (P, Q) = (Y, 1), H = 1.
+// Segment boundary, off the recurrence's critical path: the checkpoint
+// Y = P / Q and lambda from a snapshot of the state; the running state is
+// rescaled by rq = 1 / |Q_b|^2 half a segment later.  With that scaling the
+// telescoped moduli give lambda_{b+K} = lambda_b prod(h^2) rq_b rq_{b+K}.
 template <typename R, bool RA>
-__device__ __forceinline__ void proj_normalise(Proj<R>& p, R& yr, R& yi) {
+__device__ __forceinline__ void proj_boundary(Proj<R>& p, R& yr, R& yi) {
     const R rq = rcp(p.qr * p.qr + p.qi * p.qi);
     yr = (p.pr * p.qr + p.pi * p.qi) * rq;
     yi = (p.pi * p.qr - p.pr * p.qi) * rq;
-    if (RA) p.lam = p.lam * (p.H * rq);
-    p.pr = yr;
-    p.pi = yi;
-    p.qr = 1;
-    p.qi = 0;
+    if (RA) p.lam = p.lam * (p.H * p.rq * rq);
+    p.rq = rq;
     p.H = 1;
 }
+template <typename R>
+__device__ __forceinline__ void proj_scale(Proj<R>& p) {
+    p.pr *= p.rq;
+    p.pi *= p.rq;
+    p.qr *= p.rq;
+    p.qi *= p.rq;
+}
 
-// One block of pass 1: renormalise both sweeps and store their checkpoints,
+// One block of pass 1: checkpoint both sweeps at their segment boundaries,
 // prefetch the potentials of the next block into (nf, nb), then advance the
 // forward sweep through segment blk and the backward sweep through segment
-// nseg-1-blk.
-template <typename R, bool RA>
+// nseg-1-blk.  INTERIOR: the caller guarantees 1 <= blk <= nseg-2 (both
+// segments full, neither holding a contact site).
+template <typename R, bool RA, bool INTERIOR>
 __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<R>& b, int blk, int nseg,
                                             const double* __restrict__ U, R* __restrict__ ck, const R (&uf)[kSeg],
                                             const R (&ub)[kSeg], R (&nf)[kSeg], R (&nb)[kSeg], R hfull) {
@@ -349,10 +362,10 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
     const int fs = blk, bs = nseg - 1 - blk;
     const int f0 = fs * K;                  // forward segment start
     const int be = min(bs * K + K, N) - 1;  // backward segment end
-    R yr, yi, xr, xi;
-    proj_normalise<R, RA>(f, yr, yi);
-    proj_normalise<R, RA>(b, xr, xi);
     {
+        R yr, yi, xr, xi;
+        proj_boundary<R, RA>(f, yr, yi);
+        proj_boundary<R, RA>(b, xr, xi);
         R* p = ck + (size_t)fs * CL::NC * kWarp;
         p[CL::Y * kWarp] = yr;
         p[(CL::Y + 1) * kWarp] = yi;
@@ -362,7 +375,7 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
         q[(CL::X + 1) * kWarp] = xi;
         if (RA) q[CL::RHO * kWarp] = b.lam;
     }
-    if (blk + 1 < nseg) {
+    if (INTERIOR || blk + 1 < nseg) {
         // next forward segment fs+1 and next backward segment bs-1 (full, bs >= 1):
         // 16-byte aligned, inside the padded buffer
         const double2* pf = reinterpret_cast<const double2*>(U + f0 + K);
@@ -376,12 +389,17 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
             nb[K - 2 - 2 * k] = (R)vb.y;
         }
     }
-    const bool interior = (f0 > 0) && (f0 + K < N) && (be < N - 1) && (bs > 0) && (be == bs * K + K - 1);
+    const bool interior =
+        INTERIOR || ((f0 > 0) && (f0 + K < N) && (be < N - 1) && (bs > 0) && (be == bs * K + K - 1));
     if (interior) {
         // forward sites f0 + j (parity of j since f0 is even); backward sites
         // be - j use h_{be-j-1}, parity of j since be - 1 is even.
 #pragma unroll
         for (int j = 0; j < K; ++j) {
+            if (j == K / 2) {
+                proj_scale(f);
+                proj_scale(b);
+            }
             const R h2 = (j & 1) ? c.hg2 : c.hb2;
             proj_step_int(c, f, uf[j], h2);
             proj_step_int(c, b, ub[j], h2);
@@ -392,6 +410,11 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
 #pragma unroll
         for (int j = 0; j < K; ++j) {
             const int n = f0 + j;
+            const int m = be - j;  // backward step at site m gives X_{m-1}
+            if (j == K / 2) {
+                proj_scale(f);
+                proj_scale(b);
+            }
             if (n < N - 1) {
                 const R h2 = (n & 1) ? c.hg2 : c.hb2;
                 if (n == 0)
@@ -399,7 +422,6 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
                 else
                     proj_step(c, f, uf[j], h2);
             }
-            const int m = be - j;  // backward step at site m gives X_{m-1}
             if (m >= bs * K && m >= 1) {
                 const R h2 = ((m - 1) & 1) ? c.hg2 : c.hb2;
                 if (m == N - 1)
@@ -411,19 +433,16 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
     }
 }
 
-// Pass 1: forward (Y, lambda) and backward (X, rho) sweeps run together
-// (they are independent), in projective form, storing the state at every
-// segment start (forward) and segment end (backward).  Block b advances the
-// forward sweep through segment b and the backward sweep through segment
-// nseg-1-b; interior blocks (full segments, no contact site) take a
-// branch-free path with the hopping parity fixed by the unrolled index.
+// Pass 1: lead self-energies (FP64, stored for pass 2), then the forward
+// (Y, lambda) and backward (X, rho) sweeps of one chain run together (they
+// are independent), in projective form, storing the state at every segment
+// start (forward) and segment end (backward).
 template <typename R, bool RA>
-__device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, const ChainRec& cr, const WarpRec& wr,
-                                           double* __restrict__ wscratch, int lane) {
+__device__ __forceinline__ void pass1_chain(const TubeDev* __restrict__ tubes, const ChainRec& cr, int tube,
+                                            double* __restrict__ wscratch, int lane) {
     constexpr int K = kSeg;
     static_assert(K % 2 == 0, "segment length must be even");
-    using CL = CkLayout<RA>;
-    const TubeDev& T = tubes[wr.tube];
+    const TubeDev& T = tubes[tube];
     const int N = T.N;
     const double* __restrict__ U = T.U;
     const bool valid = cr.mode >= 0;
@@ -435,30 +454,38 @@ __device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, co
     wscratch[1 * kWarp + lane] = S0.y;
     wscratch[2 * kWarp + lane] = S1.x;
     wscratch[3 * kWarp + lane] = S1.y;
-    R* __restrict__ ck = reinterpret_cast<R*>(wscratch + 4 * kWarp) + lane;
     const Chain<R> c = make_chain<R, RA>(T, cr, S0.x, S0.y, S1.x, S1.y);
-    const int nseg = (N + K - 1) / K;
-
-    Proj<R> f{0, 0, 1, 0, 1, 1};  // Y_0 = 0, lambda_0 = 1
-    Proj<R> b{0, 0, 1, 0, 1, 1};  // X_{N-1} = 0, rho_{N-1} = 1
-    R hfull = 1;                  // prod of h^2 over a full segment: (beta^2 gamma^2)^(K/2)
+    R* __restrict__ ck = reinterpret_cast<R*>(wscratch + 4 * kWarp) + lane;
+    Proj<R> f{0, 0, 1, 0, 1, 1, 1};  // Y_0 = 0, lambda_0 = 1
+    Proj<R> b{0, 0, 1, 0, 1, 1, 1};  // X_{N-1} = 0, rho_{N-1} = 1
+    R hfull = 1;                     // prod of h^2 over a full segment
 #pragma unroll
     for (int j = 0; j < K / 2; ++j) hfull *= c.hb2 * c.hg2;
+    const int nseg = (N + K - 1) / K;
     // potentials of the first block: forward segment 0, backward segment nseg-1
     // (the buffer has kPadLo zeros before site 0 and kPadHi after site N-1)
     R ua_f[K], ua_b[K], ub_f[K], ub_b[K];
-    {
-        const int be = N - 1;
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-            ua_f[j] = (R)__ldg(U + j);
-            ua_b[j] = (R)__ldg(U + be - j);
-        }
+    for (int j = 0; j < K; ++j) {
+        ua_f[j] = (R)__ldg(U + j);
+        ua_b[j] = (R)__ldg(U + (N - 1) - j);
     }
-    for (int blk = 0; blk < nseg; blk += 2) {
-        pass1_block<R, RA>(c, f, b, blk, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
-        if (blk + 1 >= nseg) break;
-        pass1_block<R, RA>(c, f, b, blk + 1, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+    // Block 0 and block nseg-1 hold the contact sites (and a partial last
+    // segment); blocks 1 .. nseg-2 are interior for both sweeps and run in a
+    // branch-free loop, two blocks per trip with the potential buffers
+    // alternating.
+    pass1_block<R, RA, false>(c, f, b, 0, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+    if (nseg == 1) return;
+    int blk = 1;
+    for (; blk + 2 <= nseg - 1; blk += 2) {
+        pass1_block<R, RA, true>(c, f, b, blk, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+        pass1_block<R, RA, true>(c, f, b, blk + 1, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+    }
+    if (blk < nseg - 1) {
+        pass1_block<R, RA, true>(c, f, b, blk, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+        pass1_block<R, RA, false>(c, f, b, nseg - 1, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+    } else {
+        pass1_block<R, RA, false>(c, f, b, nseg - 1, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
     }
 }
 
@@ -469,7 +496,8 @@ __device__ __forceinline__ void pass1_warp(const TubeDev* __restrict__ tubes, co
 //   G_nn = Q_n S_n / D_n,
 //   |G_nn|^2 lambda_n = lambda_{n0} prod_{n0<=m<n} h_m^2 |S_n|^2 / |D_n|^2,
 //   |G_nn|^2 rho_n    = rho_e prod_{n<=m<e} h_m^2 |Q_n|^2 / |D_n|^2,
-// one reciprocal per site and only short linear dependency chains.
+// with only short linear dependency chains.  D_n does not depend on n inside
+// a segment, so full segments take one reciprocal in all.
 struct CkVals {  // one lane's checkpoint of a segment
     double yr, yi, lam, xr, xi, rho;
 };
@@ -523,23 +551,53 @@ __device__ __forceinline__ void segment_proj(const Chain<double>& c, int n0, con
             if (RA) lm[j + 1] = lm[j] * h2;
         }
     }
+    // Interior segment: D_n is the same at every site of the segment (the
+    // discrete Wronskian: with S_{n-1} = alpha_n S_n - h_n^2 S_{n+1} and
+    // Q_{n+1} = alpha_n Q_n - h_{n-1}^2 Q_{n-1}, D_{n-1} = D_n), so it is
+    // formed once at the segment end, where S = 1 and R = X_e, and folded
+    // into the per-segment coefficients.
+    double cgr = 0.0, cgi = 0.0;  // contour: c conj(D) / |D|^2
+    if (!EDGE) {
+        const double dr = fma(-Rr, qr[K - 1], fma(Ri, qi[K - 1], qr[K]));
+        const double di = fma(-Rr, qi[K - 1], fma(-Ri, qr[K - 1], qi[K]));
+        const double inv = rcp(fma(dr, dr, di * di));
+        if (RA) {
+            const double a = c.k0 * inv, b = c.k1 * inv;
+#pragma unroll
+            for (int j = 0; j < K; ++j) lm[j] *= a;
+            rh *= b;
+        } else {
+            cgr = fma(c.cr, dr, c.ci * di) * inv;
+            cgi = fma(c.ci, dr, -c.cr * di) * inv;
+        }
+    }
 #pragma unroll
     for (int j = K - 1; j >= 0; --j) {
         const int n = n0 + j;
         acc[j] = 0.0;
         if (EDGE && n >= N) continue;
-        // D = S Q_{n+1} - R Q_n
-        const double dr = fma(Sr, qr[j + 1], fma(-Si, qi[j + 1], fma(-Rr, qr[j], Ri * qi[j])));
-        const double di = fma(Sr, qi[j + 1], fma(Si, qr[j + 1], fma(-Rr, qi[j], -Ri * qr[j])));
-        const double inv = rcp(fma(dr, dr, di * di));
         double v;
-        if (RA) {  // real-axis chains carry no contour coefficient (c = 0)
-            const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
-            v = inv * fma(lm[j] * s2, c.k0, rh * q2 * c.k1);
-        } else {  // Im(c T conj(D)) / |D|^2 with T = Q S
-            const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
-            const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
-            v = fma(c.cr, ui, c.ci * ur) * inv;
+        if (!EDGE) {
+            if (RA) {  // |G|^2 (lambda k0 + rho k1) = (lm |S|^2 + rh |Q|^2) with 1/|D|^2 folded in
+                const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
+                v = fma(lm[j], s2, rh * q2);
+            } else {  // Im(c Q S / D)
+                const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
+                v = fma(cgr, ti, cgi * tr);
+            }
+        } else {
+            // D = S Q_{n+1} - R Q_n, per site (the segment may be partial)
+            const double dr = fma(Sr, qr[j + 1], fma(-Si, qi[j + 1], fma(-Rr, qr[j], Ri * qi[j])));
+            const double di = fma(Sr, qi[j + 1], fma(Si, qr[j + 1], fma(-Rr, qi[j], -Ri * qr[j])));
+            const double inv = rcp(fma(dr, dr, di * di));
+            if (RA) {  // real-axis chains carry no contour coefficient (c = 0)
+                const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
+                v = inv * fma(lm[j] * s2, c.k0, rh * q2 * c.k1);
+            } else {  // Im(c T conj(D)) / |D|^2 with T = Q S
+                const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
+                const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
+                v = fma(c.cr, ui, c.ci * ur) * inv;
+            }
         }
         acc[j] = c.valid ? v : 0.0;
         if (j > 0) {  // (R, S) at site n - 1
@@ -581,11 +639,22 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
     const R* __restrict__ ck = reinterpret_cast<const R*>(wscratch + 4 * kWarp) + lane;
     const Chain<R> c = make_chain<R, RA>(T, cr, s0r, s0i, s1r, s1i);
 
+    {
+        // the unit's potentials (at most 256 sites, 17 lines) into L1, one line per lane
+        const int first = su.seg0 * K, last = min(su.seg1 * K, N), off = lane * 16;
+        if (off < last - first + 16) prefetch_l1(U + min(first + off, last - 1));
+    }
     if constexpr (sizeof(R) == 8) {
-        // the next segment's checkpoint is loaded while this one is computed
+        // the next segment's checkpoint is loaded while this one is computed,
+        // the one after next is brought into L1
         CkVals cur = load_ck<RA>(ck + (size_t)su.seg0 * CL::NC * kWarp);
         for (int s = su.seg0; s < su.seg1; ++s) {
             const int n0 = s * K;
+            if (s + 2 < su.seg1) {
+                const R* q = ck + (size_t)(s + 2) * CL::NC * kWarp;
+#pragma unroll
+                for (int k = 0; k < CL::NC; ++k) prefetch_l1(q + k * kWarp);
+            }
             CkVals nxt = cur;
             if (s + 1 < su.seg1) nxt = load_ck<RA>(ck + (size_t)(s + 1) * CL::NC * kWarp);
             double u[K], acc[K];
@@ -643,26 +712,27 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
     }
 }
 
-__global__ void __launch_bounds__(128) rgf_pass1_kernel(const TubeDev* __restrict__ tubes,
-                                                        const ChainRec* __restrict__ chains,
-                                                        const WarpRec* __restrict__ warps, int num_warps,
-                                                        double* __restrict__ scratch) {
+// One warp (32 chains) per block: the latency-bound sweeps spread evenly over the SMs.
+__global__ void __launch_bounds__(32) rgf_pass1_kernel(const TubeDev* __restrict__ tubes,
+                                                       const ChainRec* __restrict__ chains,
+                                                       const WarpRec* __restrict__ warps, int num_warps,
+                                                       double* __restrict__ scratch) {
     const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int w = blockIdx.x;
     if (w >= num_warps) return;
     const WarpRec wr = warps[w];
     const ChainRec c = chains[(size_t)w * kWarp + lane];
     double* ws = scratch + wr.ck_off;
     if (wr.fp32) {
         if (wr.kind == kRealAxis)
-            pass1_warp<float, true>(tubes, c, wr, ws, lane);
+            pass1_chain<float, true>(tubes, c, wr.tube, ws, lane);
         else
-            pass1_warp<float, false>(tubes, c, wr, ws, lane);
+            pass1_chain<float, false>(tubes, c, wr.tube, ws, lane);
     } else {
         if (wr.kind == kRealAxis)
-            pass1_warp<double, true>(tubes, c, wr, ws, lane);
+            pass1_chain<double, true>(tubes, c, wr.tube, ws, lane);
         else
-            pass1_warp<double, false>(tubes, c, wr, ws, lane);
+            pass1_chain<double, false>(tubes, c, wr.tube, ws, lane);
     }
 }
 
@@ -769,16 +839,14 @@ cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const W
                        int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event) {
     if (num_warps <= 0) return cudaSuccess;
     if (warps_per_block < 1 || warps_per_block > 4) warps_per_block = 4;
-    const int threads = warps_per_block * kWarp;
-    (void)threads;
     // pass 1 is latency-bound: one warp per block spreads the chains evenly over the SMs
     rgf_pass1_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
                                                         static_cast<double*>(d_scratch));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (mid_event) cudaEventRecord(mid_event, stream);
-    rgf_pass2_kernel<<<(num_units + 3) / 4, 128, 0, stream>>>(d_tubes, d_chains, d_warps, d_units, num_units,
-                                                               d_partial, static_cast<const double*>(d_scratch));
+    rgf_pass2_kernel<<<(num_units + warps_per_block - 1) / warps_per_block, warps_per_block * kWarp, 0, stream>>>(
+        d_tubes, d_chains, d_warps, d_units, num_units, d_partial, static_cast<const double*>(d_scratch));
     return cudaGetLastError();
 }
 

@@ -172,6 +172,11 @@ typedef struct negf_stats {
     long long checkpoint_bytes;/* scratch bytes written+read by the kernel */
 } negf_stats;
 int negf_last_stats(negf_stats* s);
+/* Launch-shape knobs of negf_compute_charge (results are bitwise identical
+ * for every setting; only speed changes).
+ * NEGF_TUNE_PASS2_WARPS_PER_BLOCK: 1, 2 or 4 (default) warps per pass-2 block. */
+#define NEGF_TUNE_PASS2_WARPS_PER_BLOCK 2
+int negf_set_tuning(int key, int value);
 /* Enable CUDA-event timing of negf_compute_charge (off by default). */
 int negf_set_timing(int enable);
 
