@@ -28,7 +28,9 @@ EXPORTED = [
     "negf_last_stats", "negf_set_timing", "negf_set_tuning", "negf_broyden_create", "negf_broyden_destroy", "negf_broyden_set_input",
     "negf_broyden_step", "negf_broyden_reset", "negf_broyden_step_number", "negf_broyden_input_device_ptr",
     "negf_affine_potential", "negf_write_step", "negf_last_error", "negf_device_selftest",
-    "negf_compute_charge_noalloc",
+    "negf_compute_charge_noalloc", "negf_tube_dos_points", "negf_tube_current_points", "negf_compute_dos",
+    "negf_compute_current", "negf_write_transport_char", "negf_write_current_header", "negf_write_current",
+    "negf_write_integrand",
 ]
 
 
@@ -58,6 +60,7 @@ class TubeDesc(C.Structure):
         ("realaxis_kind", C.c_int),
         ("precision", C.c_int),
         ("mixed_fp64_band", C.c_double),
+        ("flatband_dos_integration_pts", C.c_int),
     ]
 
 
@@ -129,6 +132,14 @@ def load():
         "negf_write_step": [vp, C.c_char_p, dp, dp],
         "negf_last_error": [],
         "negf_device_selftest": [C.c_int, C.c_int, dp, dp],
+        "negf_tube_dos_points": [vp, ip],
+        "negf_tube_current_points": [vp, ip],
+        "negf_compute_dos": [vp, dp, dp, dp, dp, dp, vp, vp],
+        "negf_compute_current": [vp, dp, vp, vp],
+        "negf_write_transport_char": [vp, C.c_char_p, C.c_int, dp, dp, dp, dp],
+        "negf_write_current_header": [C.c_char_p],
+        "negf_write_current": [C.c_char_p, C.c_int, C.c_double, C.c_double, dp, C.c_double, C.c_int, C.c_double],
+        "negf_write_integrand": [vp, C.c_char_p, C.c_int, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -30,6 +30,8 @@ namespace {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kKbEvPerK = 8.617333262e-5;  // Utils/SelectWarpXUtils/WarpXConst.H:61-62
 constexpr double kSpinDegen = 2.0;            // NEGF_Common.H:351
+constexpr double kQe = 1.602176634e-19;       // Utils/SelectWarpXUtils/WarpXConst.H
+constexpr double kHeVperHz = 4.135667696e-15; // Utils/SelectWarpXUtils/WarpXConst.H:33
 
 thread_local std::string g_err;
 
@@ -670,6 +672,117 @@ int compute_rho0(negf_tube* t) {
     return NEGF_OK;
 }
 
+// ------------------------------------------------------------------ transport characteristics
+// DOS energy path (NEGF_Common.cpp:2188-2250): the non-equilibrium paths when
+// biased, else Gauss-Legendre on [Re E_eta, E_rightmost].
+std::vector<Pt> dos_points(const negf_tube& t) {
+    if (t.noneq) return t.noneq_pts;
+    std::vector<Pt> v;
+    gl_path(cplx(t.E_eta.real(), 0.0), t.E_rightmost, t.d.flatband_dos_integration_pts, 0, v);
+    return v;
+}
+
+// One transport run of a tube over energies pts: red[e][6] (see
+// negf::launch_transport) and, when ldos != null, LDOS [e][N].  Every buffer
+// is local to the call (this runs once per bias step, not per SCF iteration).
+int transport_run(negf_tube& t, const std::vector<Pt>& pts, std::vector<double>& red, double* ldos,
+                  cudaStream_t s) {
+    const int P = (int)pts.size(), M = t.d.num_modes, N = t.N;
+    red.assign((size_t)P * 6, 0.0);
+    if (P == 0) return NEGF_OK;
+    std::vector<negf::ChainRec> chains;
+    chains.reserve((size_t)P * M + negf::kWarp);
+    for (int e = 0; e < P; ++e) {
+        const double f0 = fermi(pts[e].E - t.mu[0], t.kT[0]).real();
+        const double f1 = fermi(pts[e].E - t.mu[1], t.kT[1]).real();
+        for (int m = 0; m < M; ++m) {
+            negf::ChainRec c{};
+            c.Er = pts[e].E.real();
+            c.Ei = pts[e].E.imag();
+            c.cr = f0;
+            c.ci = f1;
+            c.b0 = c.b1 = 1.0;
+            c.mode = m;
+            chains.push_back(c);
+        }
+    }
+    while (chains.size() % negf::kWarp) {
+        negf::ChainRec p = chains.back();
+        p.mode = -1;
+        p.cr = p.ci = p.b0 = p.b1 = 0.0;
+        chains.push_back(p);
+    }
+    const int nw = (int)(chains.size() / negf::kWarp);
+    const int nseg = (N + negf::kSeg - 1) / negf::kSeg;
+    const int upw = (nseg + negf::kSegsPerUnit - 1) / negf::kSegsPerUnit;
+    const long long per_warp = negf::rgf_scratch_doubles(N, negf::kRealAxis, 0);
+    std::vector<negf::WarpRec> warps(nw);
+    std::vector<negf::SegUnit> units;
+    for (int w = 0; w < nw; ++w) {
+        warps[w] = negf::WarpRec{};
+        warps[w].tube = 0;
+        warps[w].kind = negf::kRealAxis;
+        warps[w].fp32 = 0;
+        warps[w].ck_off = w * per_warp;
+        for (int s0 = 0; s0 < nseg; s0 += negf::kSegsPerUnit)
+            units.push_back({w, s0, std::min(nseg, s0 + negf::kSegsPerUnit), 0});
+    }
+    const negf::TubeDev td = make_tubedev(t, false);
+    const size_t C = chains.size();
+    DevBuf b_tube, b_chains, b_warps, b_units, b_scratch, b_part, b_cout, b_red, b_site, b_ldos;
+    NEGF_CUDA(b_tube.reserve(sizeof(td)));
+    NEGF_CUDA(b_chains.reserve(C * sizeof(negf::ChainRec)));
+    NEGF_CUDA(b_warps.reserve(warps.size() * sizeof(negf::WarpRec)));
+    NEGF_CUDA(b_units.reserve(units.size() * sizeof(negf::SegUnit)));
+    NEGF_CUDA(b_scratch.reserve((size_t)nw * per_warp * sizeof(double)));
+    NEGF_CUDA(b_part.reserve(units.size() * negf::kWarp * sizeof(double)));
+    NEGF_CUDA(b_cout.reserve(C * 5 * sizeof(double)));
+    NEGF_CUDA(b_red.reserve(red.size() * sizeof(double)));
+    if (ldos) {
+        NEGF_CUDA(b_site.reserve((size_t)N * C * sizeof(double)));
+        NEGF_CUDA(b_ldos.reserve((size_t)P * N * sizeof(double)));
+    }
+    NEGF_CUDA(cudaMemcpyAsync(b_tube.p, &td, sizeof(td), cudaMemcpyHostToDevice, s));
+    NEGF_CUDA(cudaMemcpyAsync(b_chains.p, chains.data(), C * sizeof(negf::ChainRec), cudaMemcpyHostToDevice, s));
+    NEGF_CUDA(cudaMemcpyAsync(b_warps.p, warps.data(), warps.size() * sizeof(negf::WarpRec), cudaMemcpyHostToDevice,
+                              s));
+    NEGF_CUDA(cudaMemcpyAsync(b_units.p, units.data(), units.size() * sizeof(negf::SegUnit),
+                              cudaMemcpyHostToDevice, s));
+    // sites that a chain never reaches keep these zeros (N = 1, 2 probe rules)
+    NEGF_CUDA(cudaMemsetAsync(b_cout.p, 0, C * 5 * sizeof(double), s));
+    NEGF_CUDA(negf::launch_transport(b_tube.as<negf::TubeDev>(), b_chains.as<negf::ChainRec>(),
+                                     b_warps.as<negf::WarpRec>(), nw, b_units.as<negf::SegUnit>(), (int)units.size(),
+                                     b_scratch.p, b_part.as<double>(), b_cout.as<double>(),
+                                     ldos ? b_site.as<double>() : nullptr, (long long)C, P, M, upw,
+                                     b_red.as<double>(), ldos ? b_ldos.as<double>() : nullptr, N, s));
+    NEGF_CUDA(cudaMemcpyAsync(red.data(), b_red.p, red.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (ldos)
+        NEGF_CUDA(cudaMemcpyAsync(ldos, b_ldos.p, (size_t)P * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    NEGF_CUDA(cudaStreamSynchronize(s));
+    return NEGF_OK;
+}
+
+// Compute_Conductance (NEGF_Common.cpp:1873-1928): G_quantum = 1, dF/dE of
+// contact 0 by finite differences with the first spacing deltaE = E_0 - E_1.
+double conductance(const negf_tube& t, const std::vector<double>& E, const double* T, double* C) {
+    const size_t P = E.size();
+    for (size_t i = 0; i < P; ++i) C[i] = 0.0;
+    if (P < 3) return 0.0;
+    std::vector<double> dF(P);
+    const double dE = E[0] - E[1], inv = 1. / (2 * dE);
+    auto F = [&](size_t i) { return fermi(cplx(E[i], 0.0) - t.mu[0], t.kT[0]).real(); };
+    dF[0] = (-3 * F(0) + 4 * F(1) - F(2)) * inv;
+    const size_t n = P - 1;
+    dF[n] = (3 * F(n) - 4 * F(n - 1) + F(n - 2)) * inv;
+    for (size_t i = 1; i < n; ++i) dF[i] = (F(i + 1) - F(i - 1)) * inv;
+    double sum = 0.0;
+    for (size_t i = 0; i < P; ++i) {
+        C[i] = -1.0 * T[i] * dF[i];
+        sum += C[i] * dE;
+    }
+    return sum;
+}
+
 void write_table(FILE* f, const std::vector<double>& pos, const double* v, int n) {
     // Write_Table1D, NEGF_Common.cpp:4221-4254: setprecision(15), setw(35)
     for (int i = 0; i < n; ++i) std::fprintf(f, "%35.15g%35.15g\n", pos[i], v[i]);
@@ -758,6 +871,7 @@ int negf_tube_desc_init(negf_tube_desc* d) {
     d->decimation_layers = 10;
     d->precision = NEGF_PREC_FP64;
     d->mixed_fp64_band = 1e-3;
+    d->flatband_dos_integration_pts = 100;
     return NEGF_OK;
 }
 
@@ -1138,6 +1252,127 @@ int negf_device_selftest(int which, int n, const double* in, double* out) {
 int negf_affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, void* stream) {
     if (!K || !U0 || !Q || !U || n <= 0) return fail(NEGF_ERR_ARG, "bad affine-potential arguments");
     NEGF_CUDA(negf::affine_potential(K, U0, Q, U, n, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+
+// ------------------------------------------------------------------ transport characteristics
+int negf_tube_dos_points(negf_tube* t, int* count) {
+    if (!t || !count) return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    *count = (int)dos_points(*t).size();
+    return NEGF_OK;
+}
+
+int negf_tube_current_points(negf_tube* t, int* count) {
+    if (!t || !count) return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    *count = t->noneq ? (int)t->noneq_pts.size() : 0;
+    return NEGF_OK;
+}
+
+int negf_compute_dos(negf_tube* t, double* E, double* dos, double* transmission, double* conductance_out,
+                     double* total_conductance, double* ldos, void* stream) {
+    if (!t || !E || !dos || !transmission || !conductance_out) return fail(NEGF_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_mu);
+    update_paths(*t);
+    const std::vector<Pt> pts = dos_points(*t);
+    std::vector<double> red;
+    int rc = transport_run(*t, pts, red, ldos, (cudaStream_t)stream);
+    if (rc) return rc;
+    const int P = (int)pts.size();
+    const int apuc = t->atoms_per_ring * t->rings_per_uc;  // CNT.H:52-55
+    std::vector<double> Er(P);
+    for (int e = 0; e < P; ++e) {
+        E[2 * e] = pts[e].E.real();
+        E[2 * e + 1] = pts[e].E.imag();
+        Er[e] = pts[e].E.real();
+        dos[e] = kSpinDegen * (red[6 * e] / (2. * kPi)) / apuc;  // NEGF_Common.cpp:2770-2773
+        transmission[e] = red[6 * e + 1];
+    }
+    const double tot = conductance(*t, Er, transmission, conductance_out);
+    if (total_conductance) *total_conductance = tot;
+    return NEGF_OK;
+}
+
+int negf_compute_current(negf_tube* t, double* current, double* integrand, void* stream) {
+    if (!t || !current) return fail(NEGF_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_mu);
+    update_paths(*t);
+    current[0] = current[1] = 0.0;
+    if (!t->noneq) return NEGF_OK;
+    const std::vector<Pt>& pts = t->noneq_pts;
+    std::vector<double> red;
+    int rc = transport_run(*t, pts, red, nullptr, (cudaStream_t)stream);
+    if (rc) return rc;
+    const int P = (int)pts.size();
+    const double cm = kSpinDegen * kQe / kHeVperHz;  // NEGF_Common.cpp:4576-4577
+    for (int e = 0; e < P; ++e) {
+        // IF at contact k = Gamma_k (f_k - f_k') A^k'_nn (NEGF_Common.cpp:4662-4682)
+        const cplx fk0 = fermi(pts[e].E - t->mu[0], t->kT[0]), fk1 = fermi(pts[e].E - t->mu[1], t->kT[1]);
+        const cplx wJ = pts[e].w * pts[e].J;
+        current[0] += (cm * (fk0 - fk1) * wJ).real() * red[6 * e + 1];
+        current[1] += (cm * (fk1 - fk0) * wJ).real() * red[6 * e + 2];
+        if (integrand)
+            for (int k = 0; k < 3; ++k) integrand[(size_t)k * P + e] = cm * red[6 * e + 3 + k];
+    }
+    return NEGF_OK;
+}
+
+int negf_write_transport_char(negf_tube* t, const char* path, int count, const double* E, const double* dos,
+                              const double* transmission, const double* conductance_in) {
+    if (!t || !path || count < 0 || (count > 0 && (!E || !dos || !transmission || !conductance_in)))
+        return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    FILE* f = std::fopen(path, "w");  // Write_Eql_Characteristics, NEGF_Common.cpp:1931-1975
+    if (!f) return fail(NEGF_ERR_IO, std::string("cannot open ") + path);
+    std::fprintf(f, " E_r, Fermi_Contact1, Fermi_Contact2, DOS_r, Transmission_r, Conductance_r \n");
+    for (int i = 0; i < count; ++i) {
+        const cplx Er(E[2 * i], 0.0);
+        std::fprintf(f, "%20g%20g%20g%35g%35g%35g\n", E[2 * i], fermi(Er - t->mu[0], t->kT[0]).real(),
+                     fermi(Er - t->mu[1], t->kT[1]).real(), dos[i], transmission[i], conductance_in[i]);
+    }
+    std::fclose(f);
+    return NEGF_OK;
+}
+
+int negf_write_current_header(const char* path) {
+    if (!path) return fail(NEGF_ERR_ARG, "null argument");
+    FILE* f = std::fopen(path, "a");  // Define_FileHeaderForCurrent, NEGF_Common.cpp:69-84
+    if (!f) return fail(NEGF_ERR_IO, std::string("cannot open ") + path);
+    std::fprintf(f, "'step', 'Vds' , 'Vgs', ");
+    for (int k = 0; k < 2; ++k) std::fprintf(f, ", 'I at contact_%d',", k + 1);
+    // the reference's literal continues over a backslash-newline: one line with 22 spaces
+    std::fprintf(f, "'Avg_intg_pts', 'Total_Iter', 'Broyden_Fraction', %22s'Broyden_Scalar', "
+                    "'Conductance / (2q^2/h)'\n", "");
+    std::fclose(f);
+    return NEGF_OK;
+}
+
+int negf_write_current(const char* path, int step, double Vds, double Vgs, const double* current,
+                       double avg_intg_pts, int total_iterations, double total_conductance) {
+    if (!path || !current) return fail(NEGF_ERR_ARG, "null argument");
+    FILE* f = std::fopen(path, "a");  // Write_Current, NEGF_Common.cpp:4818-4840
+    if (!f) return fail(NEGF_ERR_IO, std::string("cannot open ") + path);
+    std::fprintf(f, "%10d%15g%15g", step, Vds, Vgs);
+    for (int k = 0; k < 2; ++k) std::fprintf(f, "%20g", current[k]);
+    std::fprintf(f, "%10g%10d%20g\n", avg_intg_pts, total_iterations, total_conductance);
+    std::fclose(f);
+    return NEGF_OK;
+}
+
+int negf_write_integrand(negf_tube* t, const char* path, int count, const double* E, const double* integrand) {
+    if (!t || !path || count < 0 || (count > 0 && (!E || !integrand))) return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    FILE* f = std::fopen(path, "w");  // Write_Integrand, NEGF_Common.cpp:1977-2015
+    if (!f) return fail(NEGF_ERR_IO, std::string("cannot open ") + path);
+    std::fprintf(f, "(E_r-mu_0)/kT Intg_Channel Intg_Source Intg_Drain |F1-F2| E_r\n");
+    for (int e = 0; e < count; ++e) {
+        const cplx Er(E[2 * e], 0.0);
+        const double fd = std::fabs(fermi(Er - t->mu[0], t->kT[0]).real() - fermi(Er - t->mu[1], t->kT[1]).real());
+        std::fprintf(f, "%25.15g%25.15g%25.15g%25.15g%25.15g%25.15g\n", (E[2 * e] - t->mu[0]) / t->kT[0],
+                     integrand[e], integrand[(size_t)count + e], integrand[2 * (size_t)count + e], fd, E[2 * e]);
+    }
+    std::fclose(f);
     return NEGF_OK;
 }
 

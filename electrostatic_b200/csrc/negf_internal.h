@@ -70,6 +70,15 @@ constexpr int kSegsPerUnit = 32;  // segments per pass-2 unit (256 sites)
 // RGF launch: pass 1 (one warp per WarpRec, lane = chain: concurrent forward
 // and backward sweeps storing boundary checkpoints) then pass 2 (one warp per
 // SegUnit: independent segments, per-site contributions into partial rows).
+// Transport characteristics of one tube (DOS, transmission, current
+// integrand probes, optional LDOS): pass 1 on real-axis FP64 chains with
+// b0 = b1 = 1 and (cr, ci) = (Re f_0, Re f_1), then the spectral kernel and
+// the per-energy reductions.  d_red: [num_e][6]; d_ldos: [num_e][N] when
+// d_site (scratch of N x chains doubles, stride site_stride) is given.
+cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
+                             const SegUnit* d_units, int num_units, void* d_scratch, double* d_part,
+                             double* d_chain_out, double* d_site, long long site_stride, int num_e, int M, int upw,
+                             double* d_red, double* d_ldos, int N, cudaStream_t stream);
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
                        int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event);

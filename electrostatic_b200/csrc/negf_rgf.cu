@@ -819,6 +819,164 @@ __global__ void __launch_bounds__(32 * kRowGroups) reduce_kernel(const ReduceTub
     }
 }
 
+
+// ====================================================== transport characteristics
+// Spectral terms of one segment (FP64, per-site D as in edge segments):
+// a_n = deg Gamma_0 |G_n0|^2 and b_n = deg Gamma_1 |G_n,N-1|^2 for chains
+// whose real-axis coefficients are b0 = b1 = 1, so that deg A_nn = a_n + b_n
+// (A = sum_k G Gamma_k G^dagger, NEGF_Common.cpp:2654-2726).
+__device__ __forceinline__ void segment_spectral(const Chain<double>& c, int n0, const CkVals& ckv,
+                                                 const double (&u)[kSeg], double (&a)[kSeg], double (&b)[kSeg]) {
+    constexpr int K = kSeg;
+    const int N = c.N;
+    double pr[K], pi[K], qr[K + 1], qi[K + 1], lm[K];
+    pr[0] = ckv.yr;
+    pi[0] = ckv.yi;
+    qr[0] = 1.0;
+    qi[0] = 0.0;
+    lm[0] = ckv.lam;
+    double Rr = ckv.xr, Ri = ckv.xi, Sr = 1.0, Si = 0.0;
+    double rh = ckv.rho;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const int n = n0 + j;
+        if (n >= N) break;
+        double ar = c.Er - u[j], ai = c.Ei;
+        if (n == 0) {
+            ar -= c.s0r;
+            ai -= c.s0i;
+        }
+        if (n == N - 1) {
+            ar -= c.s1r;
+            ai -= c.s1i;
+        }
+        qr[j + 1] = fma(ar, qr[j], fma(-ai, qi[j], -pr[j]));
+        qi[j + 1] = fma(ar, qi[j], fma(ai, qr[j], -pi[j]));
+        if (j + 1 < K) {
+            const double h2 = (n & 1) ? c.hg2 : c.hb2;
+            pr[j + 1] = h2 * qr[j];
+            pi[j + 1] = h2 * qi[j];
+            lm[j + 1] = lm[j] * h2;
+        }
+    }
+#pragma unroll
+    for (int j = K - 1; j >= 0; --j) {
+        const int n = n0 + j;
+        a[j] = 0.0;
+        b[j] = 0.0;
+        if (n >= N) continue;
+        const double dr = fma(Sr, qr[j + 1], fma(-Si, qi[j + 1], fma(-Rr, qr[j], Ri * qi[j])));
+        const double di = fma(Sr, qi[j + 1], fma(Si, qr[j + 1], fma(-Rr, qi[j], -Ri * qr[j])));
+        const double inv = rcp(fma(dr, dr, di * di));
+        const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
+        a[j] = c.valid ? inv * (lm[j] * s2) * c.k0 : 0.0;
+        b[j] = c.valid ? inv * (rh * q2) * c.k1 : 0.0;
+        if (j > 0) {
+            double ar = c.Er - u[j], ai = c.Ei;
+            if (n == N - 1) {
+                ar -= c.s1r;
+                ai -= c.s1i;
+            }
+            const double h2 = ((n - 1) & 1) ? c.hg2 : c.hb2;
+            const double nrr = h2 * Sr, nri = h2 * Si;
+            const double nsr = fma(ar, Sr, fma(-ai, Si, -Rr));
+            const double nsi = fma(ar, Si, fma(ai, Sr, -Ri));
+            Rr = nrr;
+            Ri = nri;
+            Sr = nsr;
+            Si = nsi;
+            rh *= h2;
+        }
+    }
+}
+
+// One unit (32 segments of one warp's chains) after pass 1 of real-axis FP64
+// chains with b0 = b1 = 1 and (cr, ci) = (Re f_0(E), Re f_1(E)).  Per lane:
+// the sum of deg A_nn over the unit's sites -> part[unit][lane]; per chain
+// (chain_out[chain][5]): deg Gamma_0 Gamma_1 |G_0,N-1|^2 from the source end,
+// the same from the drain end, and deg Re(Gn_nn) = a f_0 + b f_1 at
+// n = N/2, else 0, else N-1 (NEGF_Common.cpp:4684-4714); optionally deg A_nn
+// per site into site_out[n * site_stride + chain].
+__global__ void __launch_bounds__(32) rgf_transport_kernel(const TubeDev* __restrict__ tubes,
+                                                           const ChainRec* __restrict__ chains,
+                                                           const WarpRec* __restrict__ warps,
+                                                           const SegUnit* __restrict__ units, int num_units,
+                                                           const double* __restrict__ scratch, double* __restrict__ part,
+                                                           double* __restrict__ chain_out,
+                                                           double* __restrict__ site_out, long long site_stride) {
+    constexpr int K = kSeg;
+    using CL = CkLayout<true>;
+    const int lane = threadIdx.x & 31;
+    if ((int)blockIdx.x >= num_units) return;
+    const SegUnit su = units[blockIdx.x];
+    const WarpRec wr = warps[su.warp];
+    const long long ci = (long long)su.warp * kWarp + lane;
+    const ChainRec cr = chains[ci];
+    const TubeDev& T = tubes[wr.tube];
+    const int N = T.N;
+    const double* __restrict__ U = T.U;
+    const double* __restrict__ ws = scratch + wr.ck_off;
+    const double s0r = ws[0 * kWarp + lane], s0i = ws[1 * kWarp + lane];
+    const double s1r = ws[2 * kWarp + lane], s1i = ws[3 * kWarp + lane];
+    const Chain<double> c = make_chain<double, true>(T, cr, s0r, s0i, s1r, s1i);
+    const double* __restrict__ ck = ws + 4 * kWarp + lane;
+    const double f0 = cr.cr, f1 = cr.ci;
+    double* out = chain_out + ci * 5;
+    double sum = 0.0;
+    for (int s = su.seg0; s < su.seg1; ++s) {
+        const int n0 = s * K;
+        const CkVals ckv = load_ck<true>(ck + (size_t)s * CL::NC * kWarp);
+        double u[K], a[K], b[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) u[k] = (n0 + k < N) ? __ldg(U + n0 + k) : 0.0;
+        segment_spectral(c, n0, ckv, u, a, b);
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int n = n0 + j;
+            if (n >= N) break;
+            sum += a[j] + b[j];
+            if (site_out) site_out[(long long)n * site_stride + ci] = a[j] + b[j];
+            if (n == 0) out[0] = (-2.0 * s0i) * b[j];
+            if (n == N - 1) out[1] = (-2.0 * s1i) * a[j];
+            const double v = fma(a[j], f0, b[j] * f1);
+            if (n == N / 2)
+                out[2] = v;
+            else if (n == 0)
+                out[3] = v;
+            else if (n == N - 1)
+                out[4] = v;
+        }
+    }
+    part[(long long)blockIdx.x * kWarp + lane] = sum;
+}
+
+// Per energy e (chains e*M .. e*M+M-1, units w*upw .. w*upw+upw-1 of warp
+// w): out[e][6] = (sum deg A_nn over sites, T from the source end, T from the
+// drain end, probe N/2, probe 0, probe N-1), summed over modes in order.
+__global__ void transport_reduce_kernel(const double* __restrict__ part, const double* __restrict__ chain_out,
+                                        int num_e, int M, int upw, double* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= num_e) return;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int m = 0; m < M; ++m) {
+        const long long c = (long long)e * M + m;
+        const long long w = c / kWarp, lane = c % kWarp;
+        for (int j = 0; j < upw; ++j) acc[0] += part[(w * upw + j) * kWarp + lane];
+        for (int k = 0; k < 5; ++k) acc[k + 1] += chain_out[c * 5 + k];
+    }
+    for (int k = 0; k < 6; ++k) out[(long long)e * 6 + k] = acc[k];
+}
+
+// LDOS_n(E_e) = sum_m deg A_nn / 2 pi -> out[e][n].
+__global__ void ldos_reduce_kernel(const double* __restrict__ site, long long stride, int num_e, int M, int N,
+                                   double* __restrict__ out) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)num_e * N) return;
+    const int e = (int)(idx / N), n = (int)(idx % N);
+    double v = 0.0;
+    for (int m = 0; m < M; ++m) v += site[(long long)n * stride + (long long)e * M + m];
+    out[idx] = v / (2.0 * 3.14159265358979323846);
+}
 }  // namespace
 
 long long rgf_scratch_doubles(int N, int kind, int fp32) {
@@ -862,6 +1020,28 @@ cudaError_t launch_reduce(const ReduceTube* d_rt, int num_tubes, int max_N, cons
     dim3 grid((max_N + 31) / 32, num_tubes);
     dim3 block(32, kRowGroups);
     reduce_kernel<<<grid, block, 0, stream>>>(d_rt, d_partial, d_Q);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
+                             const SegUnit* d_units, int num_units, void* d_scratch, double* d_part,
+                             double* d_chain_out, double* d_site, long long site_stride, int num_e, int M, int upw,
+                             double* d_red, double* d_ldos, int N, cudaStream_t stream) {
+    if (num_warps <= 0) return cudaSuccess;
+    rgf_pass1_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
+                                                        static_cast<double*>(d_scratch));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    rgf_transport_kernel<<<num_units, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, d_units, num_units,
+                                                           static_cast<const double*>(d_scratch), d_part,
+                                                           d_chain_out, d_site, site_stride);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    transport_reduce_kernel<<<(num_e + 127) / 128, 128, 0, stream>>>(d_part, d_chain_out, num_e, M, upw, d_red);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !d_site) return e;
+    const long long tot = (long long)num_e * N;
+    ldos_reduce_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(d_site, site_stride, num_e, M, N, d_ldos);
     return cudaGetLastError();
 }
 

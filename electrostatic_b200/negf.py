@@ -50,8 +50,9 @@ class CNT:
     eq_integration_pts, num_noneq_paths, noneq_integration_pts,
     noneq_percent_intercuts, E_valence_min, E_pole_max, E_zPlus_imag,
     Fermi_tail_factors, use_decimation, decimation_max_iter,
-    decimation_layers; plus realaxis_window=(min, max, pts, kind),
-    precision ("fp64" | "mixed") and mixed_fp64_band.
+    decimation_layers, flatband_dos_integration_pts; plus
+    realaxis_window=(min, max, pts, kind), precision ("fp64" | "mixed") and
+    mixed_fp64_band.
     """
 
     def __init__(self, type_id=(17, 0), num_unitcells=100, num_modes=1, acc=1.42e-10, gamma=2.5,
@@ -59,7 +60,7 @@ class CNT:
                  noneq_integration_pts=(100,), noneq_percent_intercuts=None, E_valence_min=-14.0,
                  E_pole_max=10.0, E_zPlus_imag=1e-8, Fermi_tail_factors=(14.0, 14.0), use_decimation=0,
                  decimation_max_iter=30, decimation_layers=10, realaxis_window=None, precision="fp64",
-                 mixed_fp64_band=1e-3):
+                 mixed_fp64_band=1e-3, flatband_dos_integration_pts=100):
         L = _lib.load()
         d = _lib.TubeDesc()
         check(L.negf_tube_desc_init(C.byref(d)), "negf_tube_desc_init")
@@ -93,6 +94,7 @@ class CNT:
             d.realaxis_min, d.realaxis_max, d.realaxis_pts, d.realaxis_kind = float(lo), float(hi), int(pts), int(kind)
         d.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
         d.mixed_fp64_band = float(mixed_fp64_band)
+        d.flatband_dos_integration_pts = int(flatband_dos_integration_pts)
         self.desc = d
         h = C.c_void_p()
         check(L.negf_tube_create(C.byref(d), C.byref(h)), "negf_tube_create")
@@ -195,6 +197,55 @@ class CNT:
     def Compute_InducedCharge(self, out=None, stream=None):
         return compute_charge([self], out=out, stream=stream)
 
+    # --- transport characteristics (PostProcess, Nanostructure.H:134-138)
+    def Compute_DensityOfStates(self, ldos=False, stream=None) -> dict:
+        """Compute_DensityOfStates (NEGF_Common.cpp:2390-2847) on the GPU: dict
+        with E (complex), dos, T, conductance, total_conductance and, with
+        ldos=True, ldos [E][N]."""
+        L = _lib.load()
+        n = C.c_int()
+        check(L.negf_tube_dos_points(self._h, C.byref(n)), "negf_tube_dos_points")
+        P = n.value
+        E = np.zeros(2 * P)
+        dos, T, cond = np.zeros(P), np.zeros(P), np.zeros(P)
+        tot = np.zeros(1)
+        ld = np.zeros(P * self.num_field_sites) if ldos else None
+        check(L.negf_compute_dos(self._h, _dptr(E), _dptr(dos), _dptr(T), _dptr(cond), _dptr(tot),
+                                 None if ld is None else ld.ctypes.data_as(C.c_void_p), _stream(stream)),
+              "negf_compute_dos")
+        out = dict(E=E[0::2] + 1j * E[1::2], dos=dos, T=T, conductance=cond, total_conductance=float(tot[0]))
+        if ldos:
+            out["ldos"] = ld.reshape(P, self.num_field_sites)
+        return out
+
+    def Compute_Current(self, integrand=False, stream=None):
+        """Compute_Current (NEGF_Common.cpp:4321-4816) on the GPU: terminal
+        currents [A] of contacts 0 and 1 and, with integrand=True, the
+        (channel, source, drain) integrand probes [3][P] with their energies."""
+        L = _lib.load()
+        n = C.c_int()
+        check(L.negf_tube_current_points(self._h, C.byref(n)), "negf_tube_current_points")
+        I = np.zeros(2)
+        pr = np.zeros(3 * max(n.value, 1)) if integrand else None
+        check(L.negf_compute_current(self._h, _dptr(I), None if pr is None else pr.ctypes.data_as(C.c_void_p),
+                                     _stream(stream)), "negf_compute_current")
+        if not integrand:
+            return I
+        E = self.energy_points(3)[0] if n.value else np.zeros(0, complex)
+        return I, pr[: 3 * n.value].reshape(3, n.value), E
+
+    def Write_Eql_Characteristics(self, path: str, res: dict):
+        E = np.ascontiguousarray(np.stack([res["E"].real, res["E"].imag], 1).ravel())
+        check(_lib.load().negf_write_transport_char(self._h, path.encode(), len(res["dos"]), _dptr(E),
+                                                    _dptr(res["dos"]), _dptr(res["T"]), _dptr(res["conductance"])),
+              "negf_write_transport_char")
+
+    def Write_Integrand(self, path: str, E, integrand):
+        Eb = np.ascontiguousarray(np.stack([np.real(E), np.imag(E)], 1).ravel())
+        pr = np.ascontiguousarray(integrand, dtype=np.float64)
+        check(_lib.load().negf_write_integrand(self._h, path.encode(), len(E), _dptr(Eb), _dptr(pr)),
+              "negf_write_integrand")
+
     def Write_Data(self, prefix: str, Q, norm=None):
         Q = np.ascontiguousarray(Q, dtype=np.float64)
         nrm = None if norm is None else _dptr(np.ascontiguousarray(norm, dtype=np.float64))
@@ -294,3 +345,17 @@ def affine_potential(K_dev, U0_dev, Q_dev, U_dev, stream=None):
     n = int(U0_dev.shape[0])
     check(_lib.load().negf_affine_potential(_ptr(K_dev), _ptr(U0_dev), _ptr(Q_dev), _ptr(U_dev), n, _stream(stream)),
           "negf_affine_potential")
+
+
+def write_current_header(path: str):
+    """Define_FileHeaderForCurrent (NEGF_Common.cpp:69-84): append the I.dat header."""
+    check(_lib.load().negf_write_current_header(path.encode()), "negf_write_current_header")
+
+
+def write_current(path: str, step: int, Vds: float, Vgs: float, current, avg_intg_pts: float,
+                  total_iterations: int, total_conductance: float):
+    """Write_Current (NEGF_Common.cpp:4818-4840): append one I.dat line."""
+    I = np.ascontiguousarray(current, dtype=np.float64)
+    check(_lib.load().negf_write_current(path.encode(), int(step), float(Vds), float(Vgs), _dptr(I),
+                                         float(avg_intg_pts), int(total_iterations), float(total_conductance)),
+          "negf_write_current")

@@ -74,6 +74,7 @@ typedef struct negf_tube_desc {
     int realaxis_pts, realaxis_kind;
     int precision;                 /* NEGF_PREC_FP64 or NEGF_PREC_MIXED */
     double mixed_fp64_band;        /* mixed mode: points with Im E below this [eV] stay FP64 (1e-3) */
+    int flatband_dos_integration_pts; /* DOS path points at zero bias (NEGF_Common.H:416, 100) */
 } negf_tube_desc;
 
 /* Fill `d` with the reference defaults. */
@@ -179,6 +180,42 @@ int negf_last_stats(negf_stats* s);
 int negf_set_tuning(int key, int value);
 /* Enable CUDA-event timing of negf_compute_charge (off by default). */
 int negf_set_timing(int enable);
+
+/* Transport characteristics (c_NEGF_Common::Compute_DensityOfStates,
+ * NEGF_Common.cpp:2390-2847, and Compute_Current, :4321-4816; called from
+ * c_Nanostructure::PostProcess, Nanostructure.H:134-138).
+ *
+ * DOS path (Update_IntegrationPaths, NEGF_Common.cpp:2188-2250): the
+ * non-equilibrium paths when the contacts are biased, else Gauss-Legendre on
+ * [Re E_eta, E_rightmost] with flatband_dos_integration_pts points.
+ * negf_compute_dos fills, per DOS energy (host arrays of
+ * negf_tube_dos_points() entries): E (re, im interleaved), DOS per unit cell
+ * (spin_degen * sum_sites sum_modes deg A_nn / 2pi / atoms per unit cell),
+ * transmission sum_modes deg Gamma_0 Gamma_1 |G_0,N-1|^2, the conductance
+ * integrand -T dF/dE (G_quantum = 1, Compute_Conductance :1873-1928) and its
+ * total; ldos (optional, [E][N]) = sum_modes deg A_nn / 2pi per site.
+ * negf_compute_current fills the terminal currents [A] of contacts 0 and 1
+ * (2 q/h sum_E Re(w J (f_k - f_k')) T_k(E)) and optionally the integrand
+ * probes [3][P] over the P = negf_tube_current_points() non-equilibrium
+ * energies: 2q/h * sum_modes deg Re(Gn_nn) at n = N/2, 0, N-1 (:4684-4714).
+ * Both run on the GPU and return when the host outputs are written; the
+ * current is zero at zero bias. */
+int negf_tube_dos_points(negf_tube* t, int* count);
+int negf_tube_current_points(negf_tube* t, int* count);
+int negf_compute_dos(negf_tube* t, double* E, double* dos, double* transmission, double* conductance,
+                     double* total_conductance, double* ldos, void* stream);
+int negf_compute_current(negf_tube* t, double* current, double* integrand, void* stream);
+/* Writers with the reference's formats: transport_char.dat
+ * (Write_Eql_Characteristics, NEGF_Common.cpp:1931-1975), the I.dat header
+ * (Define_FileHeaderForCurrent, :69-84) and one appended I.dat line
+ * (Write_Current, :4818-4840), and <step>_integrand.dat (Write_Integrand,
+ * :1977-2015; integrand as returned by negf_compute_current). */
+int negf_write_transport_char(negf_tube* t, const char* path, int count, const double* E, const double* dos,
+                              const double* transmission, const double* conductance);
+int negf_write_current_header(const char* path);
+int negf_write_current(const char* path, int step, double Vds, double Vgs, const double* current,
+                       double avg_intg_pts, int total_iterations, double total_conductance);
+int negf_write_integrand(negf_tube* t, const char* path, int count, const double* E, const double* integrand);
 
 /* Broyden modified-second mixing (Transport.H:203-208):
  * Set_Broyden_Parallel (Broyden_Parallel_General.cpp:68-248),

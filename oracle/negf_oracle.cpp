@@ -36,6 +36,8 @@ namespace {
 constexpr double kPi = 3.14159265358979323846;          // AMReX MathConst::pi
 constexpr double kKbEvPerK = 8.617333262e-5;            // Utils/SelectWarpXUtils/WarpXConst.H:61-62
 constexpr int kSpinDegen = 2;                           // NEGF/NEGF_Common.H:351
+constexpr double kQe = 1.602176634e-19;                  // Utils/SelectWarpXUtils/WarpXConst.H
+constexpr double kHeVperHz = 4.135667696e-15;            // Utils/SelectWarpXUtils/WarpXConst.H:33
 
 // Smith (1962) complex division a / b.
 inline cplx cdiv(cplx a, cplx b) {
@@ -155,6 +157,7 @@ struct Tube {
     int dec_tol_is_int = 1;  // NEGF/NEGF_Common.H:475 stores 1e-5 in an int
     double dec_rel_error = 1e-5;
     int sgf_mode = 0;  // 0 = reference root selection; 1 = (F-S)/D; 2 = (F+S)/D
+    int flatband_dos_pts = 100;  // NEGF/NEGF_Common.H:416
     // explicit real-axis window (noneq always) when rt_pts > 0
     int rt_pts = 0, rt_kind = 0;  // 0 regular (IntegrationPath.cpp:149), 1 GL
     double rt_min = 0.0, rt_max = 0.0;
@@ -522,6 +525,130 @@ std::vector<EPoint> collect(const std::vector<Path>& paths, int kind, const Tube
     return v;
 }
 
+// ---------------------------------------------------------------- transport characteristics
+// DOS energy path (NEGF_Common.cpp:2188-2250): the non-equilibrium paths when
+// biased, else Gauss-Legendre on [Re E_eta, E_rightmost].
+std::vector<Path> dos_paths(const Tube& t) {
+    if (t.noneq) return t.noneq_paths;
+    return {gl_path(cplx(t.E_eta.real(), 0.0), t.E_rightmost, t.flatband_dos_pts, 0)};
+}
+
+// G_{n,k} of contact k by the reference's walk from the contact site
+// (NEGF_Common.cpp:2682-2694).
+cplx contact_walk(const Sweep& s, int N, int kglo, int n) {
+    cplx tmp = cinv(s.alpha[kglo] - s.X[kglo] - s.Y[kglo]);
+    for (int q = kglo; q < n; ++q) tmp = cmul(-s.Xt[q], tmp);
+    for (int q = kglo; q > n; --q) tmp = cmul(-s.Yt[q], tmp);
+    return tmp;
+}
+
+// Compute_DensityOfStates, one energy (NEGF_Common.cpp:2654-2776): per site
+// A_nn = sum_k G_nk Gamma_k G_nk^*, LDOS_n = sum_m deg A_nn / 2 pi; the
+// transmission trace Gamma_0 A_tk[1] with A_tk[1] = G_kk Gamma_1 G_{0,k}^*
+// walked from the drain to site 0 (CT_ID[1] = 0, CNT.cpp:343-344).
+// faithful = 0 replaces the per-site walks by running products.
+void dos_point(const Tube& t, const std::vector<double>& U, cplx E, int faithful, Sweep& s, double* ldos,
+               double& trace0, double& trace1) {
+    const int N = t.N, M = t.nmodes;
+    for (int m = 0; m < M; ++m) {
+        sweep(t, U, E, m, s);
+        const double deg = t.degen[m];
+        cplx Gam[2];
+        for (int k = 0; k < 2; ++k) Gam[k] = cmul(cplx(0.0, 1.0), s.sig[k] - std::conj(s.sig[k]));
+        const int kglo[2] = {0, N - 1};
+        std::vector<cplx> g0, g1;
+        if (!faithful) {
+            g0.resize(N);
+            g1.resize(N);
+            g0[0] = cinv(s.alpha[0] - s.X[0] - s.Y[0]);
+            for (int n = 1; n < N; ++n) g0[n] = cmul(-s.Xt[n - 1], g0[n - 1]);
+            g1[N - 1] = cinv(s.alpha[N - 1] - s.X[N - 1] - s.Y[N - 1]);
+            for (int n = N - 2; n >= 0; --n) g1[n] = cmul(-s.Yt[n + 1], g1[n + 1]);
+        }
+        for (int n = 0; n < N; ++n) {
+            cplx A = 0.0;
+            for (int k = 0; k < 2; ++k) {
+                const cplx g = faithful ? contact_walk(s, N, kglo[k], n) : (k == 0 ? g0[n] : g1[n]);
+                A += cmul(cmul(g, Gam[k]), std::conj(g));
+            }
+            const cplx val = A * deg / (2. * kPi);
+            if (ldos) ldos[n] += val.real();
+            trace0 += val.real();
+        }
+        // A_tk[1] at n = 0
+        const cplx Gkk = cinv(s.alpha[N - 1] - s.X[N - 1] - s.Y[N - 1]);
+        const cplx G0k = faithful ? contact_walk(s, N, N - 1, 0) : g1[0];
+        cplx Akn = cmul(cmul(Gkk, Gam[1]), std::conj(G0k));
+        for (int q = N - 2; q >= 0; --q) Akn = cmul(-s.Yt[q + 1], Akn);
+        trace1 += (cmul(Gam[0], Akn) * deg).real();
+    }
+}
+
+// Compute_Conductance (NEGF_Common.cpp:1873-1928): G_quantum = 1, dF/dE by
+// finite differences with the first grid spacing deltaE = E_0 - E_1.
+double conductance(const Tube& t, const std::vector<cplx>& E, const std::vector<double>& T, std::vector<double>& C) {
+    const size_t P = E.size();
+    C.assign(P, 0.0);
+    if (P < 3) return 0.0;
+    std::vector<double> dF(P, 0.0);
+    const double dE = E[0].real() - E[1].real();
+    const double inv = 1. / (2 * dE);
+    auto F = [&](size_t i) { return fermi(E[i] - t.mu[0], t.kT[0]).real(); };
+    dF[0] = (-3 * F(0) + 4 * F(1) - F(2)) * inv;
+    const size_t n = P - 1;
+    dF[n] = (3 * F(n) - 4 * F(n - 1) + F(n - 2)) * inv;
+    for (size_t i = 1; i < n; ++i) dF[i] = (F(i + 1) - F(i - 1)) * inv;
+    double sum = 0.0;
+    for (size_t i = 0; i < P; ++i) {
+        C[i] = -1.0 * T[i] * dF[i];
+        sum += C[i] * dE;
+    }
+    return sum;
+}
+
+// Compute_Current, one energy of the non-equilibrium paths
+// (NEGF_Common.cpp:4439-4722): at the contact sites IF = Gamma_k f_k A_nn -
+// Gamma_k Gn_nn with Gn_nn = sum_k' A^k'_nn f_k'; integrand probes Gn_nn at
+// n = N/2 (channel), 0 (source), N-1 (drain), as an if / else-if chain.
+void current_point(const Tube& t, const std::vector<double>& U, const EPoint& ep, Sweep& s, double I[2],
+                   double probe[3]) {
+    const int N = t.N, M = t.nmodes;
+    const double cm = kSpinDegen * kQe / kHeVperHz;
+    cplx fk[2];
+    for (int k = 0; k < 2; ++k) fk[k] = fermi(ep.E - t.mu[k], t.kT[k]);
+    const int kglo[2] = {0, N - 1};
+    const int sites[3] = {N / 2, 0, N - 1};
+    for (int m = 0; m < M; ++m) {
+        sweep(t, U, ep.E, m, s);
+        const double deg = t.degen[m];
+        cplx Gam[2];
+        for (int k = 0; k < 2; ++k) Gam[k] = cmul(cplx(0.0, 1.0), s.sig[k] - std::conj(s.sig[k]));
+        for (int i = 0; i < 3; ++i) {
+            const int n = sites[i];
+            if (i == 2 && n == sites[1]) continue;  // N = 1
+            cplx A = 0.0, Gn = 0.0;
+            for (int k = 0; k < 2; ++k) {
+                const cplx g = contact_walk(s, N, kglo[k], n);
+                const cplx Ak = cmul(cmul(g, Gam[k]), std::conj(g));
+                A += Ak;
+                Gn += cmul(Ak, fk[k]);
+            }
+            for (int k = 0; k < 2; ++k)
+                if (n == kglo[k]) {
+                    const cplx IF = cmul(cmul(Gam[k], fk[k]), A) - cmul(Gam[k], Gn);
+                    I[k] += cmul(cmul(cm * IF * deg, ep.w), ep.J).real();
+                }
+            const cplx v = cm * Gn * deg;
+            if (n == N / 2)
+                probe[0] += v.real();
+            else if (n == 0)
+                probe[1] += v.real();
+            else if (n == N - 1)
+                probe[2] += v.real();
+        }
+    }
+}
+
 // ---------------------------------------------------------------- Broyden
 // T/Broyden_Second_Parallel.cpp:9-211 (CPU branch) and
 // T/Broyden_Parallel_General.cpp:68-355 (set-up and reset).
@@ -843,6 +970,79 @@ long long orc_tube_sample(void* h, int faithful, int nthreads, int stride, int o
 }
 
 // ------------------------------------------------------------- Broyden
+// DOS / transmission / conductance over the tube's DOS path.  Returns the
+// number of energies; with E != null writes E (re, im), dos, T, conductance
+// per energy, the total conductance, and optionally LDOS [e][n].
+int orc_tube_dos(void* h, int faithful, int nthreads, double* E, double* dos, double* T, double* cond,
+                 double* total_cond, double* ldos) {
+    Tube* t = static_cast<Tube*>(h);
+    energy_limits(*t);
+    build_eq_noneq_paths(*t);
+    const auto paths = dos_paths(*t);
+    std::vector<cplx> Ev;
+    for (const auto& p : paths)
+        for (auto e : p.E) Ev.push_back(e);
+    const int P = (int)Ev.size();
+    if (!E) return P;
+    const int N = t->N;
+    std::vector<double> tr0(P, 0.0), tr1(P, 0.0);
+    nthreads = std::max(1, std::min(nthreads, P));
+    auto worker = [&](int tid) {
+        Sweep s;
+        for (int e = P * tid / nthreads; e < P * (tid + 1) / nthreads; ++e)
+            dos_point(*t, t->U, Ev[e], faithful, s, ldos ? ldos + (size_t)e * N : nullptr, tr0[e], tr1[e]);
+    };
+    if (ldos) std::fill(ldos, ldos + (size_t)P * N, 0.0);
+    std::vector<std::thread> th;
+    for (int i = 0; i < nthreads; ++i) th.emplace_back(worker, i);
+    for (auto& x : th) x.join();
+    const int apuc = t->atoms_per_ring * t->rings_per_uc;  // CNT.H:52-55
+    std::vector<double> Tv(P), C;
+    for (int e = 0; e < P; ++e) {
+        E[2 * e] = Ev[e].real();
+        E[2 * e + 1] = Ev[e].imag();
+        dos[e] = kSpinDegen * tr0[e] / apuc;
+        T[e] = Tv[e] = tr1[e];
+    }
+    // Compute_Conductance takes the energies as complex numbers with the real part only
+    std::vector<cplx> Er(P);
+    for (int e = 0; e < P; ++e) Er[e] = cplx(Ev[e].real(), 0.0);
+    const double tot = conductance(*t, Er, Tv, C);
+    for (int e = 0; e < P; ++e) cond[e] = C[e];
+    if (total_cond) *total_cond = tot;
+    return P;
+}
+void orc_tube_set_flatband_dos_pts(void* h, int pts) { static_cast<Tube*>(h)->flatband_dos_pts = pts; }
+
+// Terminal currents over the non-equilibrium paths; integrand probes
+// (channel, source, drain) per energy when probes != null ([3][P]).
+int orc_tube_current(void* h, int nthreads, double* I, double* probes) {
+    Tube* t = static_cast<Tube*>(h);
+    energy_limits(*t);
+    build_eq_noneq_paths(*t);
+    const auto pts = collect(t->noneq_paths, 3, *t);
+    const int P = (int)pts.size();
+    I[0] = I[1] = 0.0;
+    if (P == 0) return 0;
+    std::vector<double> Ie(2 * P, 0.0), pr(3 * P, 0.0);
+    nthreads = std::max(1, std::min(nthreads, P));
+    auto worker = [&](int tid) {
+        Sweep s;
+        for (int e = P * tid / nthreads; e < P * (tid + 1) / nthreads; ++e)
+            current_point(*t, t->U, pts[e], s, &Ie[2 * e], &pr[3 * e]);
+    };
+    std::vector<std::thread> th;
+    for (int i = 0; i < nthreads; ++i) th.emplace_back(worker, i);
+    for (auto& x : th) x.join();
+    for (int e = 0; e < P; ++e) {
+        I[0] += Ie[2 * e];
+        I[1] += Ie[2 * e + 1];
+        if (probes)
+            for (int k = 0; k < 3; ++k) probes[(size_t)k * P + e] = pr[3 * e + k];
+    }
+    return P;
+}
+
 void* orc_broyden_new(int S, int maxstep, double fraction, int norm_type, const double* n_in) {
     Broyden* b = new Broyden();
     b->S = S;

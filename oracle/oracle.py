@@ -62,6 +62,10 @@ def lib():
         L.orc_tube_partial.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp]
         L.orc_tube_sample.restype = C.c_longlong
         L.orc_tube_sample.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp]
+        L.orc_tube_dos.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]
+        L.orc_tube_set_flatband_dos_pts.argtypes = [C.c_void_p, C.c_int]
+        L.orc_tube_current.argtypes = [C.c_void_p, C.c_int, _dp, C.c_void_p]
         L.orc_broyden_new.restype = C.c_void_p
         L.orc_broyden_new.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, _dp]
         L.orc_broyden_free.argtypes = [C.c_void_p]
@@ -191,6 +195,39 @@ def _sample(self, stride, offset=0, faithful=True, nthreads=1):
 
 
 OracleTube.sample = _sample
+
+
+def _dos(self, faithful=True, nthreads=1, ldos=False, flatband_pts=None):
+    """Compute_DensityOfStates over the tube's DOS path: dict with E (complex),
+    dos, T, conductance, total_conductance and, if asked, ldos [E][N]."""
+    L = lib()
+    if flatband_pts is not None:
+        L.orc_tube_set_flatband_dos_pts(self._h, int(flatband_pts))
+    P = L.orc_tube_dos(self._h, int(faithful), int(nthreads), None, None, None, None, None, None)
+    E = np.zeros(2 * P)
+    dos, T, cond = np.zeros(P), np.zeros(P), np.zeros(P)
+    tot = np.zeros(1)
+    ld = np.zeros(P * self.N) if ldos else None
+    vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+    L.orc_tube_dos(self._h, int(faithful), int(nthreads), vp(E), vp(dos), vp(T), vp(cond), vp(tot), vp(ld))
+    out = dict(E=E[0::2] + 1j * E[1::2], dos=dos, T=T, conductance=cond, total_conductance=float(tot[0]))
+    if ldos:
+        out["ldos"] = ld.reshape(P, self.N)
+    return out
+
+
+def _current(self, nthreads=1, probes=False):
+    """Compute_Current: (I[2], probes [3][P] or None) over the non-equilibrium paths."""
+    L = lib()
+    I = np.zeros(2)
+    n = len(self.paths(3)[0])
+    pr = np.zeros(3 * max(n, 1)) if probes else None
+    L.orc_tube_current(self._h, int(nthreads), I, None if pr is None else pr.ctypes.data_as(C.c_void_p))
+    return I, (pr[: 3 * n].reshape(3, n) if probes else None)
+
+
+OracleTube.dos = _dos
+OracleTube.current = _current
 
 
 class OracleBroyden:

@@ -12,6 +12,10 @@ read-only mount used when this repository was built).
   negf_python/PointContact/cpp_results/1gpu/{Sigma,DOS,Transmission}
       N=4, 1000 energies on [-1, 1] + 1e-8 i, root (F + S)/D
       (scripts/negf_cpp/spectral_function_1D_pll/Source/main.cpp)
+  negf_python/DOS_Compare/cpp_results/gpu/{LDOS,Transmission}.dat
+      output of the engine's own Compute_DensityOfStates for a (17,0) CNT of
+      one unit cell (N=4), 2 modes, analytic leads, 200 uniform energies on
+      [-1, 1] + 1e-8 i: DOS per unit cell and transmission per energy
 """
 import argparse
 import os
@@ -22,6 +26,7 @@ SETS = {
     "pointcontact_1gpu": "scripts/negf_python/PointContact/cpp_results/1gpu",
 }
 FILES = ["Sigma", "DOS", "Transmission"]
+DOS_COMPARE = ("scripts/negf_python/DOS_Compare/cpp_results/gpu", ["LDOS.dat", "Transmission.dat"])
 
 
 def main():
@@ -35,6 +40,12 @@ def main():
             dst = os.path.join(here, f"{tag}_{f}.txt")
             shutil.copyfile(src, dst)
             print(f"{src} -> {dst}")
+    rel, files = DOS_COMPARE
+    for f in files:
+        src = os.path.join(args.ref, rel, f)
+        dst = os.path.join(here, "dos_compare_gpu_" + f.replace(".dat", ".txt"))
+        shutil.copyfile(src, dst)
+        print(f"{src} -> {dst}")
 
 
 if __name__ == "__main__":

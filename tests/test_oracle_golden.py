@@ -4,6 +4,8 @@ tests/golden/*.txt are the committed outputs of the reference's standalone RGF
 programs (tests/golden/make_golden.py lists their origin).  The files print 6
 significant digits, so the bound is 1e-5 relative.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -16,7 +18,6 @@ GOLDEN = {
 
 
 def _load(tag, name):
-    import os
     p = os.path.join(os.path.dirname(__file__), "golden", f"{tag}_{name}.txt")
     return np.loadtxt(p, skiprows=1)
 
@@ -154,3 +155,62 @@ def test_broyden_oracle_linear_problem(oracle):
     fixed = np.linalg.solve(np.eye(S) - A, b)
     assert it < 2 * S + 5  # Broyden terminates in <= 2S steps on linear maps (exact arithmetic)
     np.testing.assert_allclose(n, fixed, atol=1e-8)
+
+
+def _dos_compare_tube(oracle, faithful):
+    t = oracle.OracleTube(type_id=(17, 0), num_unitcells=1, num_modes=2, contact_mu=(0.0, -1e-4),
+                          realaxis_window=(-1.0, 1.0, 200, 0), E_zPlus_imag=1e-8)
+    t.set_potential(np.zeros(t.N), (0.0, 0.0))
+    return t.dos(faithful=faithful, nthreads=4)
+
+
+@pytest.mark.parametrize("faithful", [True, False])
+def test_dos_transmission_against_reference_output(oracle, faithful):
+    """Compute_DensityOfStates restated (NEGF_Common.cpp:2390-2847) against the
+    reference engine's committed DOS_Compare output: (17,0), N=4, 2 modes,
+    200 uniform energies on [-1, 1] + 1e-8 i (6 printed digits; the gap values
+    near 1e-15 pin the broadening and the lead self-energies)."""
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    gT = np.loadtxt(os.path.join(here, "dos_compare_gpu_Transmission.txt"), skiprows=1)
+    gD = np.loadtxt(os.path.join(here, "dos_compare_gpu_LDOS.txt"), skiprows=1)
+    d = _dos_compare_tube(oracle, faithful)
+    assert np.allclose(d["E"].real, gT[:, 0], rtol=0, atol=1e-6)
+    assert np.max(np.abs(d["T"] - gT[:, 1]) / np.abs(gT[:, 1])) < 1e-5
+    assert np.max(np.abs(d["dos"] - gD[:, 1]) / np.abs(gD[:, 1])) < 1e-5
+
+
+def test_current_against_dense_inverse(oracle):
+    """Terminal current (NEGF_Common.cpp:4321-4816) against a dense-inverse
+    Landauer sum over the same non-equilibrium energy grid."""
+    t = oracle.OracleTube(type_id=(17, 0), num_unitcells=3, num_modes=2, contact_mu=(-0.2, -0.6),
+                          contact_T=(300.0, 300.0), noneq_integration_pts=(40, 30), E_zPlus_imag=1e-6)
+    rng = np.random.default_rng(5)
+    U = 0.1 * rng.standard_normal(t.N)
+    t.set_potential(U, (U[0], U[-1]))
+    I, probes = t.current(nthreads=4, probes=True)
+    E, w, J = t.paths(3)
+    J_, deg, beta, _ = t.modes()
+    kB, q, h = 8.617333262e-5, 1.602176634e-19, 4.135667696e-15
+    kT = kB * 300.0
+    f = lambda x, mu: 1.0 / (np.exp((x - mu) / kT) + 1.0)
+    N, g = t.N, 2.5
+    Iref = 0.0
+    for e in range(len(E)):
+        Te = 0.0
+        for m in range(len(beta)):
+            S = [t.sigma(m, E[e], U[0]), t.sigma(m, E[e], U[-1])]
+            A = np.zeros((N, N), complex)
+            for n in range(N):
+                A[n, n] = E[e] - U[n]
+            for n in range(N - 1):
+                hop = -beta[m] if n % 2 == 0 else -g
+                A[n, n + 1] = A[n + 1, n] = -hop
+            A[0, 0] -= S[0]
+            A[-1, -1] -= S[1]
+            G = np.linalg.inv(A)
+            G0 = [1j * (S[k] - np.conj(S[k])) for k in range(2)]
+            Te += deg[m] * (G0[0] * G0[1] * abs(G[0, N - 1]) ** 2).real
+        Iref += (2 * q / h * (f(E[e], -0.2) - f(E[e], -0.6)) * w[e] * J[e]).real * Te
+    assert abs(I[0] - Iref) / abs(Iref) < 1e-8
+    assert abs(I[1] + Iref) / abs(Iref) < 1e-8
+    assert probes.shape == (3, len(E)) and np.all(np.isfinite(probes))
