@@ -30,7 +30,8 @@ EXPORTED = [
     "negf_affine_potential", "negf_write_step", "negf_last_error", "negf_device_selftest",
     "negf_compute_charge_noalloc", "negf_tube_dos_points", "negf_tube_current_points", "negf_compute_dos",
     "negf_compute_current", "negf_write_transport_char", "negf_write_current_header", "negf_write_current",
-    "negf_write_integrand",
+    "negf_write_integrand", "negf_tube_correct_integration_limits", "negf_tube_noneq_integrand",
+    "negf_tube_noneq_layout",
 ]
 
 
@@ -61,6 +62,11 @@ class TubeDesc(C.Structure):
         ("precision", C.c_int),
         ("mixed_fp64_band", C.c_double),
         ("flatband_dos_integration_pts", C.c_int),
+        ("flag_adaptive_integration_limits", C.c_int),
+        ("integrand_correction_interval", C.c_int),
+        ("kT_window_around_singularity", C.c_double * 2),
+        ("flag_noneq_integration_pts_density", C.c_int),
+        ("noneq_integration_pts_density", C.c_double * NEGF_MAX_NONEQ_PATHS),
     ]
 
 
@@ -140,6 +146,9 @@ def load():
         "negf_write_current_header": [C.c_char_p],
         "negf_write_current": [C.c_char_p, C.c_int, C.c_double, C.c_double, dp, C.c_double, C.c_int, C.c_double],
         "negf_write_integrand": [vp, C.c_char_p, C.c_int, dp, dp],
+        "negf_tube_correct_integration_limits": [vp, vp],
+        "negf_tube_noneq_integrand": [vp, dp, vp],
+        "negf_tube_noneq_layout": [vp, ip, ip, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -173,6 +173,8 @@ struct negf_tube {
     std::vector<cplx> poles;
     int version = 0;
     int shard_rank = 0, shard_world = 1;
+    // adaptive non-equilibrium limits (NEGF_Common.H:453-457)
+    double E_at_max_noneq_integrand = 0.0;
     ~negf_tube() {
         if (d_U_pad) cudaFree(d_U_pad);
         if (d_zero_pad) cudaFree(d_zero_pad);
@@ -682,13 +684,13 @@ std::vector<Pt> dos_points(const negf_tube& t) {
     return v;
 }
 
-// One transport run of a tube over energies pts: red[e][6] (see
+// One transport run of a tube over energies pts: red[e][8] (see
 // negf::launch_transport) and, when ldos != null, LDOS [e][N].  Every buffer
 // is local to the call (this runs once per bias step, not per SCF iteration).
 int transport_run(negf_tube& t, const std::vector<Pt>& pts, std::vector<double>& red, double* ldos,
                   cudaStream_t s) {
     const int P = (int)pts.size(), M = t.d.num_modes, N = t.N;
-    red.assign((size_t)P * 6, 0.0);
+    red.assign((size_t)P * 8, 0.0);
     if (P == 0) return NEGF_OK;
     std::vector<negf::ChainRec> chains;
     chains.reserve((size_t)P * M + negf::kWarp);
@@ -736,7 +738,7 @@ int transport_run(negf_tube& t, const std::vector<Pt>& pts, std::vector<double>&
     NEGF_CUDA(b_units.reserve(units.size() * sizeof(negf::SegUnit)));
     NEGF_CUDA(b_scratch.reserve((size_t)nw * per_warp * sizeof(double)));
     NEGF_CUDA(b_part.reserve(units.size() * negf::kWarp * sizeof(double)));
-    NEGF_CUDA(b_cout.reserve(C * 5 * sizeof(double)));
+    NEGF_CUDA(b_cout.reserve(C * 7 * sizeof(double)));
     NEGF_CUDA(b_red.reserve(red.size() * sizeof(double)));
     if (ldos) {
         NEGF_CUDA(b_site.reserve((size_t)N * C * sizeof(double)));
@@ -749,7 +751,7 @@ int transport_run(negf_tube& t, const std::vector<Pt>& pts, std::vector<double>&
     NEGF_CUDA(cudaMemcpyAsync(b_units.p, units.data(), units.size() * sizeof(negf::SegUnit),
                               cudaMemcpyHostToDevice, s));
     // sites that a chain never reaches keep these zeros (N = 1, 2 probe rules)
-    NEGF_CUDA(cudaMemsetAsync(b_cout.p, 0, C * 5 * sizeof(double), s));
+    NEGF_CUDA(cudaMemsetAsync(b_cout.p, 0, C * 7 * sizeof(double), s));
     NEGF_CUDA(negf::launch_transport(b_tube.as<negf::TubeDev>(), b_chains.as<negf::ChainRec>(),
                                      b_warps.as<negf::WarpRec>(), nw, b_units.as<negf::SegUnit>(), (int)units.size(),
                                      b_scratch.p, b_part.as<double>(), b_cout.as<double>(),
@@ -781,6 +783,67 @@ double conductance(const negf_tube& t, const std::vector<double>& E, const doubl
         sum += C[i] * dE;
     }
     return sum;
+}
+
+// Integrand of Compute_RhoNonEq at the probe sites (NEGF_Common.cpp:3467-3496):
+// Re(-spin/2pi sum_modes deg sum_k A^k_nn f_k) at n = N/2, N/4, 3N/4 over the
+// current non-equilibrium energies -> integrand [3][P].
+int noneq_integrand(negf_tube& t, std::vector<double>& integrand, cudaStream_t s) {
+    const std::vector<Pt>& pts = t.noneq_pts;
+    std::vector<double> red;
+    int rc = transport_run(t, pts, red, nullptr, s);
+    if (rc) return rc;
+    const int P = (int)pts.size();
+    const double c = -1 * kSpinDegen / (2 * kPi);
+    integrand.assign((size_t)3 * P, 0.0);
+    for (int e = 0; e < P; ++e) {
+        integrand[e] = c * red[8 * e + 3];
+        integrand[(size_t)P + e] = c * red[8 * e + 6];
+        integrand[(size_t)2 * P + e] = c * red[8 * e + 7];
+    }
+    return NEGF_OK;
+}
+
+// Find_NonEq_Percent_Intercuts_Adaptively (NEGF_Common.cpp:2062-2185): new
+// intercuts and point counts of 2 or 3 non-equilibrium paths around E* (the
+// energy of the largest |integrand|), in units of kT_0 from mu_0; the point
+// densities per kT are fixed on first use.
+void find_intercuts(negf_tube& t) {
+    negf_tube_desc& d = t.d;
+    const int np = d.num_noneq_paths;
+    const double Es = (t.E_at_max_noneq_integrand - t.mu[0]) / t.kT[0];
+    const double Emin = (t.E_right.real() - t.mu[0]) / t.kT[0];
+    const double Emax = (t.E_rightmost.real() - t.mu[0]) / t.kT[0];
+    double* cut = d.noneq_percent_intercuts;
+    int* pts = d.noneq_integration_pts;
+    double* den = d.noneq_integration_pts_density;
+    if (cut[0] < 0)  // the uniform default, made explicit
+        for (int p = 0; p < np - 1; ++p) cut[p] = (p + 1) * (100. / np);
+    if (np == 3) {
+        if (!d.flag_noneq_integration_pts_density) {
+            den[0] = pts[0] / ((cut[0] / 100.) * (Emax - Emin));
+            den[1] = pts[1] / (((cut[1] - cut[0]) / 100.) * (Emax - Emin));
+            den[2] = pts[2] / (((100. - cut[1]) / 100.) * (Emax - Emin));
+            d.flag_noneq_integration_pts_density = 1;
+        }
+        const double lo = std::max(Es - d.kT_window_around_singularity[0], Emin);
+        const double hi = std::min(Es + d.kT_window_around_singularity[1], Emax);
+        cut[0] = 100 * (lo - Emin) / (Emax - Emin);
+        cut[1] = 100 * (hi - Emin) / (Emax - Emin);
+        pts[0] = (int)(std::round(((lo - Emin) * den[0]) / 2) * 2);
+        pts[1] = (int)(std::round(((hi - lo) * den[1]) / 2) * 2);
+        pts[2] = (int)(std::round(((Emax - hi) * den[2]) / 2) * 2);
+    } else if (np == 2) {
+        if (!d.flag_noneq_integration_pts_density) {
+            den[0] = pts[0] / ((cut[0] / 100.) * (Emax - Emin));
+            den[1] = pts[1] / (((100 - cut[0]) / 100.) * (Emax - Emin));
+            d.flag_noneq_integration_pts_density = 1;
+        }
+        const double hi = Es + d.kT_window_around_singularity[1];
+        cut[0] = 100 * (hi - Emin) / (Emax - Emin);
+        pts[0] = (int)(std::round(((hi - Emin) * den[0]) / 2) * 2);
+        pts[1] = (int)(std::round(((Emax - hi) * den[1]) / 2) * 2);
+    }
 }
 
 void write_table(FILE* f, const std::vector<double>& pos, const double* v, int n) {
@@ -872,6 +935,10 @@ int negf_tube_desc_init(negf_tube_desc* d) {
     d->precision = NEGF_PREC_FP64;
     d->mixed_fp64_band = 1e-3;
     d->flatband_dos_integration_pts = 100;
+    d->flag_adaptive_integration_limits = 0;
+    d->integrand_correction_interval = 500;
+    d->kT_window_around_singularity[0] = d->kT_window_around_singularity[1] = 1.0;
+    d->flag_noneq_integration_pts_density = 0;
     return NEGF_OK;
 }
 
@@ -1286,8 +1353,8 @@ int negf_compute_dos(negf_tube* t, double* E, double* dos, double* transmission,
         E[2 * e] = pts[e].E.real();
         E[2 * e + 1] = pts[e].E.imag();
         Er[e] = pts[e].E.real();
-        dos[e] = kSpinDegen * (red[6 * e] / (2. * kPi)) / apuc;  // NEGF_Common.cpp:2770-2773
-        transmission[e] = red[6 * e + 1];
+        dos[e] = kSpinDegen * (red[8 * e] / (2. * kPi)) / apuc;  // NEGF_Common.cpp:2770-2773
+        transmission[e] = red[8 * e + 1];
     }
     const double tot = conductance(*t, Er, transmission, conductance_out);
     if (total_conductance) *total_conductance = tot;
@@ -1310,11 +1377,58 @@ int negf_compute_current(negf_tube* t, double* current, double* integrand, void*
         // IF at contact k = Gamma_k (f_k - f_k') A^k'_nn (NEGF_Common.cpp:4662-4682)
         const cplx fk0 = fermi(pts[e].E - t->mu[0], t->kT[0]), fk1 = fermi(pts[e].E - t->mu[1], t->kT[1]);
         const cplx wJ = pts[e].w * pts[e].J;
-        current[0] += (cm * (fk0 - fk1) * wJ).real() * red[6 * e + 1];
-        current[1] += (cm * (fk1 - fk0) * wJ).real() * red[6 * e + 2];
+        current[0] += (cm * (fk0 - fk1) * wJ).real() * red[8 * e + 1];
+        current[1] += (cm * (fk1 - fk0) * wJ).real() * red[8 * e + 2];
         if (integrand)
-            for (int k = 0; k < 3; ++k) integrand[(size_t)k * P + e] = cm * red[6 * e + 3 + k];
+            for (int k = 0; k < 3; ++k) integrand[(size_t)k * P + e] = cm * red[8 * e + 3 + k];
     }
+    return NEGF_OK;
+}
+
+int negf_tube_noneq_integrand(negf_tube* t, double* integrand, void* stream) {
+    if (!t || !integrand) return fail(NEGF_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_mu);
+    update_paths(*t);
+    if (!t->noneq) return NEGF_OK;
+    std::vector<double> v;
+    int rc = noneq_integrand(*t, v, (cudaStream_t)stream);
+    if (rc) return rc;
+    std::copy(v.begin(), v.end(), integrand);
+    return NEGF_OK;
+}
+
+int negf_tube_correct_integration_limits(negf_tube* t, void* stream) {
+    if (!t) return fail(NEGF_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_mu);
+    update_paths(*t);  // Generate_NonEq_Paths with the current intercuts
+    if (!t->noneq || t->d.realaxis_pts > 0) return NEGF_OK;
+    std::vector<double> v;
+    int rc = noneq_integrand(*t, v, (cudaStream_t)stream);
+    if (rc) return rc;
+    // the first energy of largest |integrand at N/2| (NEGF_Common.cpp:3527-3542)
+    double mx = 0.0;
+    for (size_t e = 0; e < t->noneq_pts.size(); ++e)
+        if (mx < std::fabs(v[e])) {
+            mx = std::fabs(v[e]);
+            t->E_at_max_noneq_integrand = t->noneq_pts[e].E.real();
+        }
+    find_intercuts(*t);
+    t->limits_dirty = true;  // Generate_NonEq_Paths with the new intercuts
+    update_paths(*t);
+    return NEGF_OK;
+}
+
+int negf_tube_noneq_layout(negf_tube* t, int* num_paths, int* pts, double* intercuts, double* E_at_max) {
+    if (!t) return fail(NEGF_ERR_ARG, "null argument");
+    update_paths(*t);
+    const int np = t->d.num_noneq_paths;
+    if (num_paths) *num_paths = np;
+    for (int p = 0; p < np; ++p) {
+        if (pts) pts[p] = t->d.noneq_integration_pts[p];
+        if (intercuts && p < np - 1)
+            intercuts[p] = t->d.noneq_percent_intercuts[0] < 0 ? (p + 1) * (100. / np) : t->d.noneq_percent_intercuts[p];
+    }
+    if (E_at_max) *E_at_max = t->E_at_max_noneq_integrand;
     return NEGF_OK;
 }
 

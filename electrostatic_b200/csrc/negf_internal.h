@@ -73,7 +73,7 @@ constexpr int kSegsPerUnit = 32;  // segments per pass-2 unit (256 sites)
 // Transport characteristics of one tube (DOS, transmission, current
 // integrand probes, optional LDOS): pass 1 on real-axis FP64 chains with
 // b0 = b1 = 1 and (cr, ci) = (Re f_0, Re f_1), then the spectral kernel and
-// the per-energy reductions.  d_red: [num_e][6]; d_ldos: [num_e][N] when
+// the per-energy reductions.  d_red: [num_e][8]; d_ldos: [num_e][N] when
 // d_site (scratch of N x chains doubles, stride site_stride) is given.
 cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                              const SegUnit* d_units, int num_units, void* d_scratch, double* d_part,

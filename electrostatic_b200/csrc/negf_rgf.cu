@@ -893,10 +893,11 @@ __device__ __forceinline__ void segment_spectral(const Chain<double>& c, int n0,
 // One unit (32 segments of one warp's chains) after pass 1 of real-axis FP64
 // chains with b0 = b1 = 1 and (cr, ci) = (Re f_0(E), Re f_1(E)).  Per lane:
 // the sum of deg A_nn over the unit's sites -> part[unit][lane]; per chain
-// (chain_out[chain][5]): deg Gamma_0 Gamma_1 |G_0,N-1|^2 from the source end,
-// the same from the drain end, and deg Re(Gn_nn) = a f_0 + b f_1 at
-// n = N/2, else 0, else N-1 (NEGF_Common.cpp:4684-4714); optionally deg A_nn
-// per site into site_out[n * site_stride + chain].
+// (chain_out[chain][7]): deg Gamma_0 Gamma_1 |G_0,N-1|^2 from the source end,
+// the same from the drain end, deg Re(Gn_nn) = a f_0 + b f_1 at n = N/2,
+// else 0, else N-1 (the current's probes, NEGF_Common.cpp:4684-4714), and at
+// n = N/4, else 3N/4 after N/2 (the charge integrand's probes, :3467-3496);
+// optionally deg A_nn per site into site_out[n * site_stride + chain].
 __global__ void __launch_bounds__(32) rgf_transport_kernel(const TubeDev* __restrict__ tubes,
                                                            const ChainRec* __restrict__ chains,
                                                            const WarpRec* __restrict__ warps,
@@ -921,7 +922,7 @@ __global__ void __launch_bounds__(32) rgf_transport_kernel(const TubeDev* __rest
     const Chain<double> c = make_chain<double, true>(T, cr, s0r, s0i, s1r, s1i);
     const double* __restrict__ ck = ws + 4 * kWarp + lane;
     const double f0 = cr.cr, f1 = cr.ci;
-    double* out = chain_out + ci * 5;
+    double* out = chain_out + ci * 7;
     double sum = 0.0;
     for (int s = su.seg0; s < su.seg1; ++s) {
         const int n0 = s * K;
@@ -945,26 +946,32 @@ __global__ void __launch_bounds__(32) rgf_transport_kernel(const TubeDev* __rest
                 out[3] = v;
             else if (n == N - 1)
                 out[4] = v;
+            if (n != N / 2) {
+                if (n == N / 4)
+                    out[5] = v;
+                else if (n == (N * 3) / 4)
+                    out[6] = v;
+            }
         }
     }
     part[(long long)blockIdx.x * kWarp + lane] = sum;
 }
 
 // Per energy e (chains e*M .. e*M+M-1, units w*upw .. w*upw+upw-1 of warp
-// w): out[e][6] = (sum deg A_nn over sites, T from the source end, T from the
-// drain end, probe N/2, probe 0, probe N-1), summed over modes in order.
+// w): out[e][8] = (sum deg A_nn over sites, T from the source end, T from the
+// drain end, probes at N/2, 0, N-1, N/4, 3N/4), summed over modes in order.
 __global__ void transport_reduce_kernel(const double* __restrict__ part, const double* __restrict__ chain_out,
                                         int num_e, int M, int upw, double* __restrict__ out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= num_e) return;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int m = 0; m < M; ++m) {
         const long long c = (long long)e * M + m;
         const long long w = c / kWarp, lane = c % kWarp;
         for (int j = 0; j < upw; ++j) acc[0] += part[(w * upw + j) * kWarp + lane];
-        for (int k = 0; k < 5; ++k) acc[k + 1] += chain_out[c * 5 + k];
+        for (int k = 0; k < 7; ++k) acc[k + 1] += chain_out[c * 7 + k];
     }
-    for (int k = 0; k < 6; ++k) out[(long long)e * 6 + k] = acc[k];
+    for (int k = 0; k < 8; ++k) out[(long long)e * 8 + k] = acc[k];
 }
 
 // LDOS_n(E_e) = sum_m deg A_nn / 2 pi -> out[e][n].

@@ -50,7 +50,9 @@ class CNT:
     eq_integration_pts, num_noneq_paths, noneq_integration_pts,
     noneq_percent_intercuts, E_valence_min, E_pole_max, E_zPlus_imag,
     Fermi_tail_factors, use_decimation, decimation_max_iter,
-    decimation_layers, flatband_dos_integration_pts; plus
+    decimation_layers, flatband_dos_integration_pts,
+    flag_adaptive_integration_limits, integrand_correction_interval,
+    kT_window_around_singularity, noneq_integration_pts_density; plus
     realaxis_window=(min, max, pts, kind), precision ("fp64" | "mixed") and
     mixed_fp64_band.
     """
@@ -60,7 +62,9 @@ class CNT:
                  noneq_integration_pts=(100,), noneq_percent_intercuts=None, E_valence_min=-14.0,
                  E_pole_max=10.0, E_zPlus_imag=1e-8, Fermi_tail_factors=(14.0, 14.0), use_decimation=0,
                  decimation_max_iter=30, decimation_layers=10, realaxis_window=None, precision="fp64",
-                 mixed_fp64_band=1e-3, flatband_dos_integration_pts=100):
+                 mixed_fp64_band=1e-3, flatband_dos_integration_pts=100, flag_adaptive_integration_limits=0,
+                 integrand_correction_interval=500, kT_window_around_singularity=(1.0, 1.0),
+                 noneq_integration_pts_density=None):
         L = _lib.load()
         d = _lib.TubeDesc()
         check(L.negf_tube_desc_init(C.byref(d)), "negf_tube_desc_init")
@@ -95,6 +99,13 @@ class CNT:
         d.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
         d.mixed_fp64_band = float(mixed_fp64_band)
         d.flatband_dos_integration_pts = int(flatband_dos_integration_pts)
+        d.flag_adaptive_integration_limits = int(flag_adaptive_integration_limits)
+        d.integrand_correction_interval = int(integrand_correction_interval)
+        d.kT_window_around_singularity[0], d.kT_window_around_singularity[1] = map(float, kT_window_around_singularity)
+        if noneq_integration_pts_density is not None:
+            d.flag_noneq_integration_pts_density = 1
+            for i, v in enumerate(noneq_integration_pts_density):
+                d.noneq_integration_pts_density[i] = float(v)
         self.desc = d
         h = C.c_void_p()
         check(L.negf_tube_create(C.byref(d), C.byref(h)), "negf_tube_create")
@@ -187,12 +198,39 @@ class CNT:
         return v.value
 
     # --- charge
-    def Solve_NEGF(self, U=None, U_contact=None, out=None, stream=None):
+    def Solve_NEGF(self, U=None, U_contact=None, out=None, stream=None, iter=None):
         """Solve_NEGF (NEGF_Common.cpp:1309-1340).  Returns the induced charge
-        per site (numpy) or writes it into the device tensor `out`."""
+        per site (numpy) or writes it into the device tensor `out`.  With
+        flag_adaptive_integration_limits, iteration numbers that are multiples
+        of integrand_correction_interval first correct the non-equilibrium
+        intercuts (:1316-1336)."""
         if U is not None:
             self.set_potential(U, U_contact)
+        d = self.desc
+        if iter is not None and d.flag_adaptive_integration_limits and iter % d.integrand_correction_interval == 0:
+            self.correct_integration_limits(stream=stream)
         return compute_charge([self], out=out, stream=stream)
+
+    def correct_integration_limits(self, stream=None):
+        check(_lib.load().negf_tube_correct_integration_limits(self._h, _stream(stream)),
+              "negf_tube_correct_integration_limits")
+
+    def noneq_integrand(self, stream=None):
+        """Compute_RhoNonEq integrand probes [3][P] (sites N/2, N/4, 3N/4)."""
+        P = len(self.energy_points(3)[0]) if self.noneq() else 0
+        out = np.zeros(3 * max(P, 1))
+        check(_lib.load().negf_tube_noneq_integrand(self._h, _dptr(out), _stream(stream)), "negf_tube_noneq_integrand")
+        return out[: 3 * P].reshape(3, P)
+
+    def noneq_layout(self):
+        """(points per path, intercuts in percent, E* of the last correction)."""
+        n = C.c_int()
+        pts = (C.c_int * _lib.NEGF_MAX_NONEQ_PATHS)()
+        cuts = np.zeros(_lib.NEGF_MAX_NONEQ_PATHS)
+        Es = np.zeros(1)
+        check(_lib.load().negf_tube_noneq_layout(self._h, C.byref(n), pts, _dptr(cuts), _dptr(Es)),
+              "negf_tube_noneq_layout")
+        return np.array(pts[: n.value]), cuts[: max(n.value - 1, 0)].copy(), float(Es[0])
 
     def Compute_InducedCharge(self, out=None, stream=None):
         return compute_charge([self], out=out, stream=stream)

@@ -75,6 +75,13 @@ typedef struct negf_tube_desc {
     int precision;                 /* NEGF_PREC_FP64 or NEGF_PREC_MIXED */
     double mixed_fp64_band;        /* mixed mode: points with Im E below this [eV] stay FP64 (1e-3) */
     int flatband_dos_integration_pts; /* DOS path points at zero bias (NEGF_Common.H:416, 100) */
+    /* Adaptive non-equilibrium limits (Read_AdaptiveIntegrationParams,
+     * NEGF_Common.cpp:524-543; NEGF_Common.H:453-457). */
+    int flag_adaptive_integration_limits;      /* 0 */
+    int integrand_correction_interval;         /* 500 */
+    double kT_window_around_singularity[2];    /* {1, 1} */
+    int flag_noneq_integration_pts_density;    /* 1 when the densities below are given */
+    double noneq_integration_pts_density[NEGF_MAX_NONEQ_PATHS]; /* points per kT of each path */
 } negf_tube_desc;
 
 /* Fill `d` with the reference defaults. */
@@ -205,6 +212,24 @@ int negf_tube_current_points(negf_tube* t, int* count);
 int negf_compute_dos(negf_tube* t, double* E, double* dos, double* transmission, double* conductance,
                      double* total_conductance, double* ldos, void* stream);
 int negf_compute_current(negf_tube* t, double* current, double* integrand, void* stream);
+/* Adaptive non-equilibrium limits.  negf_tube_correct_integration_limits
+ * is Update_IntegrationPaths with flag_correct_integration_limits
+ * (NEGF_Common.cpp:2188-2215): the charge integrand on the current paths
+ * (Compute_RhoNonEq's probe at site N/2, :3467-3542), its largest |value|
+ * fixes E*, and Find_NonEq_Percent_Intercuts_Adaptively (:2062-2185) moves
+ * the intercuts and point counts of 2 or 3 paths to a window of
+ * kT_window_around_singularity around E*.  Solve_NEGF applies it when
+ * flag_adaptive_integration_limits and iter % integrand_correction_interval
+ * == 0 (:1316-1336); the caller owns that schedule.  No effect at zero bias
+ * or with an explicit real-axis window.
+ * negf_tube_noneq_integrand: the charge integrand probes [3][P]
+ * (site N/2, N/4, 3N/4; Re(-spin/2pi sum_modes deg sum_k A^k_nn f_k)) over
+ * the P current non-equilibrium energies.
+ * negf_tube_noneq_layout: current path count, points per path, intercuts
+ * [num_paths - 1] (percent) and E* [eV]. */
+int negf_tube_correct_integration_limits(negf_tube* t, void* stream);
+int negf_tube_noneq_integrand(negf_tube* t, double* integrand, void* stream);
+int negf_tube_noneq_layout(negf_tube* t, int* num_paths, int* pts, double* intercuts, double* E_at_max);
 /* Writers with the reference's formats: transport_char.dat
  * (Write_Eql_Characteristics, NEGF_Common.cpp:1931-1975), the I.dat header
  * (Define_FileHeaderForCurrent, :69-84) and one appended I.dat line

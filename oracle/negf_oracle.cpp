@@ -158,6 +158,11 @@ struct Tube {
     double dec_rel_error = 1e-5;
     int sgf_mode = 0;  // 0 = reference root selection; 1 = (F-S)/D; 2 = (F+S)/D
     int flatband_dos_pts = 100;  // NEGF/NEGF_Common.H:416
+    // adaptive non-equilibrium limits (NEGF/NEGF_Common.H:453-457)
+    double kT_window[2] = {1.0, 1.0};
+    bool has_density = false;
+    std::vector<double> density;
+    double E_at_max = 0.0;
     // explicit real-axis window (noneq always) when rt_pts > 0
     int rt_pts = 0, rt_kind = 0;  // 0 regular (IntegrationPath.cpp:149), 1 GL
     double rt_min = 0.0, rt_max = 0.0;
@@ -649,6 +654,77 @@ void current_point(const Tube& t, const std::vector<double>& U, const EPoint& ep
     }
 }
 
+// ---------------------------------------------------------------- adaptive non-equilibrium limits
+// Integrand probes of Compute_RhoNonEq (NEGF_Common.cpp:3467-3496):
+// Re(c sum_modes deg sum_k A^k_nn f_k), c = -spin/2pi, at n = N/2, else N/4,
+// else 3N/4, with the per-site contact walks.
+void noneq_integrand_point(const Tube& t, const std::vector<double>& U, cplx E, Sweep& s, double out[3]) {
+    const int N = t.N, M = t.nmodes;
+    const double c = -1 * kSpinDegen / (2 * kPi);
+    cplx fk[2];
+    for (int k = 0; k < 2; ++k) fk[k] = fermi(E - t.mu[k], t.kT[k]);
+    const int kglo[2] = {0, N - 1};
+    cplx acc[3] = {0.0, 0.0, 0.0};
+    for (int m = 0; m < M; ++m) {
+        sweep(t, U, E, m, s);
+        const double deg = t.degen[m];
+        cplx Gam[2];
+        for (int k = 0; k < 2; ++k) Gam[k] = cmul(cplx(0.0, 1.0), s.sig[k] - std::conj(s.sig[k]));
+        for (int n = 0; n < N; ++n) {
+            int slot = -1;
+            if (n == N / 2)
+                slot = 0;
+            else if (n == N / 4)
+                slot = 1;
+            else if (n == N * 3 / 4)
+                slot = 2;
+            if (slot < 0) continue;
+            cplx AnF = 0.0;
+            for (int k = 0; k < 2; ++k) {
+                const cplx g = contact_walk(s, N, kglo[k], n);
+                AnF += cmul(cmul(cmul(g, Gam[k]), std::conj(g)), fk[k]);
+            }
+            acc[slot] += c * AnF * deg;
+        }
+    }
+    for (int k = 0; k < 3; ++k) out[k] = acc[k].real();
+}
+
+// Find_NonEq_Percent_Intercuts_Adaptively (NEGF_Common.cpp:2062-2185).
+void find_intercuts(Tube& t) {
+    const int np = (int)t.noneq_pts.size();
+    const double Es = (t.E_at_max - t.mu[0]) / t.kT[0];
+    const double Emin = (t.E_right.real() - t.mu[0]) / t.kT[0];
+    const double Emax = (t.E_rightmost.real() - t.mu[0]) / t.kT[0];
+    std::vector<double>& cut = t.intercuts;
+    std::vector<int>& pts = t.noneq_pts;
+    if (np == 3) {
+        if (!t.has_density) {
+            t.density = {pts[0] / ((cut[0] / 100.) * (Emax - Emin)),
+                         pts[1] / (((cut[1] - cut[0]) / 100.) * (Emax - Emin)),
+                         pts[2] / (((100. - cut[1]) / 100.) * (Emax - Emin))};
+            t.has_density = true;
+        }
+        const double lo = std::max(Es - t.kT_window[0], Emin);
+        const double hi = std::min(Es + t.kT_window[1], Emax);
+        cut[0] = 100 * (lo - Emin) / (Emax - Emin);
+        cut[1] = 100 * (hi - Emin) / (Emax - Emin);
+        pts[0] = (int)(std::round(((lo - Emin) * t.density[0]) / 2) * 2);
+        pts[1] = (int)(std::round(((hi - lo) * t.density[1]) / 2) * 2);
+        pts[2] = (int)(std::round(((Emax - hi) * t.density[2]) / 2) * 2);
+    } else if (np == 2) {
+        if (!t.has_density) {
+            t.density = {pts[0] / ((cut[0] / 100.) * (Emax - Emin)),
+                         pts[1] / (((100 - cut[0]) / 100.) * (Emax - Emin))};
+            t.has_density = true;
+        }
+        const double hi = Es + t.kT_window[1];
+        cut[0] = 100 * (hi - Emin) / (Emax - Emin);
+        pts[0] = (int)(std::round(((hi - Emin) * t.density[0]) / 2) * 2);
+        pts[1] = (int)(std::round(((Emax - hi) * t.density[1]) / 2) * 2);
+    }
+}
+
 // ---------------------------------------------------------------- Broyden
 // T/Broyden_Second_Parallel.cpp:9-211 (CPU branch) and
 // T/Broyden_Parallel_General.cpp:68-355 (set-up and reset).
@@ -1041,6 +1117,68 @@ int orc_tube_current(void* h, int nthreads, double* I, double* probes) {
             for (int k = 0; k < 3; ++k) probes[(size_t)k * P + e] = pr[3 * e + k];
     }
     return P;
+}
+
+// Integrand probes [3][P] of Compute_RhoNonEq over the current non-equilibrium energies.
+int orc_tube_noneq_integrand(void* h, int nthreads, double* out) {
+    Tube* t = static_cast<Tube*>(h);
+    energy_limits(*t);
+    build_eq_noneq_paths(*t);
+    std::vector<cplx> Ev;
+    for (const auto& p : t->noneq_paths)
+        for (auto e : p.E) Ev.push_back(e);
+    const int P = (int)Ev.size();
+    if (!out || P == 0) return P;
+    std::vector<double> v(3 * (size_t)P);
+    nthreads = std::max(1, std::min(nthreads, P));
+    auto worker = [&](int tid) {
+        Sweep s;
+        for (int e = P * tid / nthreads; e < P * (tid + 1) / nthreads; ++e)
+            noneq_integrand_point(*t, t->U, Ev[e], s, &v[3 * (size_t)e]);
+    };
+    std::vector<std::thread> th;
+    for (int i = 0; i < nthreads; ++i) th.emplace_back(worker, i);
+    for (auto& x : th) x.join();
+    for (int e = 0; e < P; ++e)
+        for (int k = 0; k < 3; ++k) out[(size_t)k * P + e] = v[3 * (size_t)e + k];
+    return P;
+}
+
+// Update_IntegrationPaths with flag_correct_integration_limits (NEGF_Common.cpp:2200-2211).
+void orc_tube_set_adaptive(void* h, double win_lo, double win_hi, int n_density, const double* density) {
+    Tube* t = static_cast<Tube*>(h);
+    t->kT_window[0] = win_lo;
+    t->kT_window[1] = win_hi;
+    t->has_density = n_density > 0;
+    t->density.assign(density, density + std::max(0, n_density));
+}
+void orc_tube_correct_limits(void* h, int nthreads) {
+    Tube* t = static_cast<Tube*>(h);
+    energy_limits(*t);
+    build_eq_noneq_paths(*t);
+    if (!t->noneq || t->rt_pts > 0) return;
+    const int P = orc_tube_noneq_integrand(h, 1, nullptr);
+    std::vector<double> v(3 * (size_t)std::max(P, 1));
+    orc_tube_noneq_integrand(h, nthreads, v.data());
+    std::vector<cplx> Ev;
+    for (const auto& p : t->noneq_paths)
+        for (auto e : p.E) Ev.push_back(e);
+    double mx = 0.0;
+    for (int e = 0; e < P; ++e)
+        if (mx < std::fabs(v[e])) {
+            mx = std::fabs(v[e]);
+            t->E_at_max = Ev[e].real();
+        }
+    find_intercuts(*t);
+    build_eq_noneq_paths(*t);
+}
+int orc_tube_noneq_layout(void* h, int* pts, double* cuts, double* E_at_max) {
+    Tube* t = static_cast<Tube*>(h);
+    const int np = (int)t->noneq_pts.size();
+    for (int p = 0; p < np; ++p) pts[p] = t->noneq_pts[p];
+    for (int p = 0; p + 1 < np; ++p) cuts[p] = t->intercuts[p];
+    *E_at_max = t->E_at_max;
+    return np;
 }
 
 void* orc_broyden_new(int S, int maxstep, double fraction, int norm_type, const double* n_in) {

@@ -66,6 +66,10 @@ def lib():
                                    C.c_void_p, C.c_void_p]
         L.orc_tube_set_flatband_dos_pts.argtypes = [C.c_void_p, C.c_int]
         L.orc_tube_current.argtypes = [C.c_void_p, C.c_int, _dp, C.c_void_p]
+        L.orc_tube_noneq_integrand.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_tube_set_adaptive.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]
+        L.orc_tube_correct_limits.argtypes = [C.c_void_p, C.c_int]
+        L.orc_tube_noneq_layout.argtypes = [C.c_void_p, _ip, _dp, _dp]
         L.orc_broyden_new.restype = C.c_void_p
         L.orc_broyden_new.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, _dp]
         L.orc_broyden_free.argtypes = [C.c_void_p]
@@ -226,6 +230,38 @@ def _current(self, nthreads=1, probes=False):
     return I, (pr[: 3 * n].reshape(3, n) if probes else None)
 
 
+def _noneq_integrand(self, nthreads=1):
+    """Compute_RhoNonEq integrand probes [3][P] (site N/2, N/4, 3N/4)."""
+    L = lib()
+    P = L.orc_tube_noneq_integrand(self._h, 1, None)
+    out = np.zeros(3 * max(P, 1))
+    L.orc_tube_noneq_integrand(self._h, int(nthreads), out.ctypes.data_as(C.c_void_p))
+    return out[: 3 * P].reshape(3, P)
+
+
+def _correct_limits(self, nthreads=1, kT_window=(1.0, 1.0), density=None):
+    """One adaptive correction of the non-equilibrium intercuts and points
+    (the window and the optional point densities are fixed on first use)."""
+    L = lib()
+    if not getattr(self, "_adaptive", False) or density is not None:
+        self._dens = np.ascontiguousarray([] if density is None else density, dtype=np.float64)
+        L.orc_tube_set_adaptive(self._h, kT_window[0], kT_window[1], len(self._dens),
+                                self._dens.ctypes.data_as(C.c_void_p) if len(self._dens) else None)
+        self._adaptive = True
+    L.orc_tube_correct_limits(self._h, int(nthreads))
+
+
+def _noneq_layout(self):
+    pts = np.zeros(8, np.int32)
+    cuts = np.zeros(8)
+    Emax = np.zeros(1)
+    n = lib().orc_tube_noneq_layout(self._h, pts, cuts, Emax)
+    return pts[:n].copy(), cuts[: max(n - 1, 0)].copy(), float(Emax[0])
+
+
+OracleTube.noneq_integrand = _noneq_integrand
+OracleTube.correct_limits = _correct_limits
+OracleTube.noneq_layout = _noneq_layout
 OracleTube.dos = _dos
 OracleTube.current = _current
 

@@ -126,3 +126,35 @@ def test_transport_writers(tmp_path):
     rows = np.loadtxt(ip, skiprows=1)
     assert rows.shape == (len(E), 6)
     assert np.allclose(rows[:, 1], probes[0], rtol=1e-14, atol=0)
+
+
+@pytest.mark.parametrize("paths", [2, 3])
+def test_adaptive_intercuts_against_oracle(oracle, paths):
+    """Update_IntegrationPaths with flag_correct_integration_limits: the
+    charge integrand (sites N/2, N/4, 3N/4), E* and the corrected intercuts
+    and point counts match the oracle over two corrections, then the charge."""
+    pts, cuts = ((30, 50), (40.0,)) if paths == 2 else ((20, 40, 20), (30.0, 70.0))
+    kw = dict(type_id=(17, 0), num_unitcells=12, num_modes=2, contact_mu=(0.0, -0.4), contact_T=(300.0, 300.0),
+              noneq_integration_pts=pts, noneq_percent_intercuts=cuts, E_zPlus_imag=1e-6)
+    g, o = _pair(oracle, seed=21, **kw)
+    assert _rel(g.noneq_integrand(), o.noneq_integrand(nthreads=8)) <= TOL
+    for _ in range(2):
+        g.correct_integration_limits()
+        o.correct_limits(nthreads=8)
+        gp, gc, gE = g.noneq_layout()
+        op, oc, oE = o.noneq_layout()
+        assert list(gp) == list(op) and gE == oE
+        assert np.allclose(gc, oc, rtol=0, atol=1e-9)
+    assert _rel(g.Solve_NEGF(), o.charge(nthreads=8)) <= TOL
+
+
+def test_solve_negf_adaptive_schedule():
+    """Solve_NEGF(iter) corrects only on multiples of the interval."""
+    from electrostatic_b200.negf import CNT
+    g = CNT(type_id=(17, 0), num_unitcells=8, num_modes=2, contact_mu=(0.0, -0.4), noneq_integration_pts=(20, 40, 20),
+            noneq_percent_intercuts=(30.0, 70.0), flag_adaptive_integration_limits=1, integrand_correction_interval=3)
+    g.set_potential(np.zeros(g.num_field_sites), (0.0, 0.0))
+    g.Solve_NEGF(iter=1)
+    assert list(g.noneq_layout()[0]) == [20, 40, 20]
+    g.Solve_NEGF(iter=3)
+    assert list(g.noneq_layout()[0]) != [20, 40, 20]
