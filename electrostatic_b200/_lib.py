@@ -31,7 +31,7 @@ EXPORTED = [
     "negf_compute_charge_noalloc", "negf_tube_dos_points", "negf_tube_current_points", "negf_compute_dos",
     "negf_compute_current", "negf_write_transport_char", "negf_write_current_header", "negf_write_current",
     "negf_write_integrand", "negf_tube_correct_integration_limits", "negf_tube_noneq_integrand",
-    "negf_tube_noneq_layout",
+    "negf_tube_noneq_layout", "negf_read_table1d",
 ]
 
 
@@ -149,6 +149,7 @@ def load():
         "negf_tube_correct_integration_limits": [vp, vp],
         "negf_tube_noneq_integrand": [vp, dp, vp],
         "negf_tube_noneq_layout": [vp, ip, ip, dp, dp],
+        "negf_read_table1d": [C.c_char_p, C.c_int, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

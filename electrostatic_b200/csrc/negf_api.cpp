@@ -1490,6 +1490,37 @@ int negf_write_integrand(negf_tube* t, const char* path, int count, const double
     return NEGF_OK;
 }
 
+int negf_read_table1d(const char* filename, int n, double* values) {
+    if (!filename || n < 0 || (n > 0 && !values)) return fail(NEGF_ERR_ARG, "null argument");
+    // Read_Table1D, NEGF_Common.cpp:237-285: header line, then `position value` per line
+    FILE* f = std::fopen(filename, "r");
+    if (!f) return fail(NEGF_ERR_IO, std::string("Failed to read file ") + filename);
+    int lines = 0, c, last = '\n';
+    while ((c = std::fgetc(f)) != EOF) {
+        if (c == '\n') ++lines;
+        last = c;
+    }
+    if (last != '\n') ++lines;  // a final line without a newline still counts
+    if (lines - 1 != n) {
+        std::fclose(f);
+        return fail(NEGF_ERR_IO, "Assert size, " + std::to_string(n) + ", is not equal to the filesize-1, " +
+                                     std::to_string(lines - 1) + " !");
+    }
+    std::rewind(f);
+    while ((c = std::fgetc(f)) != EOF && c != '\n') {
+    }
+    for (int l = 0; l < n; ++l) {
+        double pos, v;
+        if (std::fscanf(f, "%lf %lf", &pos, &v) != 2) {
+            std::fclose(f);
+            return fail(NEGF_ERR_IO, std::string("malformed line ") + std::to_string(l + 2) + " in " + filename);
+        }
+        values[l] = v;
+    }
+    std::fclose(f);
+    return NEGF_OK;
+}
+
 // ------------------------------------------------------------------ output
 int negf_write_step(negf_tube* t, const char* prefix, const double* Q, const double* norm) {
     if (!t || !prefix || !Q) return fail(NEGF_ERR_ARG, "null argument");

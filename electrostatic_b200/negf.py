@@ -397,3 +397,35 @@ def write_current(path: str, step: int, Vds: float, Vgs: float, current, avg_int
     check(_lib.load().negf_write_current(path.encode(), int(step), float(Vds), float(Vgs), _dptr(I),
                                          float(avg_intg_pts), int(total_iterations), float(total_conductance)),
           "negf_write_current")
+
+
+# --- file naming and restart (NEGF_Common.cpp:87-140, 178-285, 565-621)
+NAME_DIGITS = 4  # negf_plt_name_digits, NEGF_Common.H:65
+
+
+def concatenate(root: str, num: int, digits: int = NAME_DIGITS) -> str:
+    """amrex::Concatenate: root followed by num zero-padded to `digits` digits."""
+    return f"{root}{num:0{digits}d}"
+
+
+def step_filename(folder: str, name: str, step: int) -> str:
+    """Set_StepFilenameString: <folder>/<name>/stepNNNN."""
+    return concatenate(f"{folder}/{name}/step", step)
+
+
+def iter_filename(step_prefix: str, it: int) -> str:
+    """Set_IterationFilenameString: <stepNNNN>_iter/iterMMMM."""
+    return concatenate(f"{step_prefix}_iter/iter", it)
+
+
+def restart_charge_filename(folder: str, name: str, restart_step: int) -> str:
+    """Read_AtomLocationAndChargeDistributionFilename with restart: the
+    _Qout.dat of step restart_step - 1."""
+    return step_filename(folder, name, restart_step - 1) + "_Qout.dat"
+
+
+def read_table1d(filename: str, n: int) -> np.ndarray:
+    """Read_Table1D: the value column of a header + n-line table."""
+    out = np.zeros(n)
+    check(_lib.load().negf_read_table1d(filename.encode(), int(n), _dptr(out)), "negf_read_table1d")
+    return out

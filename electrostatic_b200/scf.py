@@ -58,14 +58,23 @@ def device_view(ptr: int, n: int):
 
 def run_scf(tube, electro, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
             initial_charge=0.0, reset_with_previous_charge=False, stream=None):
-    """Bias sweep of self-consistent solves for one tube on the current device."""
+    """Bias sweep of self-consistent solves for one tube on the current device.
+    initial_charge: a value for every site, or the path of a _Qout.dat table
+    (restart, read with Read_Table1D's rules)."""
     import torch
     from .negf import Broyden, compute_charge
+
+    from .negf import read_table1d
 
     L = _lib.load()
     N = tube.num_field_sites
     dev = torch.device("cuda")
-    n_in = torch.full((N,), float(initial_charge), dtype=torch.float64, device=dev)
+    if isinstance(initial_charge, str):
+        # Initialize_ChargeAtFieldSites with a charge table (NEGF_Common.cpp:178-235)
+        n_in = torch.tensor(read_table1d(initial_charge, N), dtype=torch.float64, device=dev)
+        initial_charge = 0.0
+    else:
+        n_in = torch.full((N,), float(initial_charge), dtype=torch.float64, device=dev)
     Q = torch.zeros(N, dtype=torch.float64, device=dev)
     br = Broyden(n_in, max_step=max_step, fraction=fraction, norm_type=norm_type)
     U_ptr = tube.potential_device_ptr()

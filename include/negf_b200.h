@@ -230,6 +230,12 @@ int negf_compute_current(negf_tube* t, double* current, double* integrand, void*
 int negf_tube_correct_integration_limits(negf_tube* t, void* stream);
 int negf_tube_noneq_integrand(negf_tube* t, double* integrand, void* stream);
 int negf_tube_noneq_layout(negf_tube* t, int* num_paths, int* pts, double* intercuts, double* E_at_max);
+/* Read_Table1D (NEGF_Common.cpp:237-285), used to initialise or restart the
+ * charge from a `_Qout.dat` table (Initialize_ChargeAtFieldSites, :178-235;
+ * file naming at :565-621): a header line, then `position value` per line;
+ * the file must hold exactly n + 1 lines (else NEGF_ERR_IO with the
+ * reference's message).  Host only. */
+int negf_read_table1d(const char* filename, int n, double* values);
 /* Writers with the reference's formats: transport_char.dat
  * (Write_Eql_Characteristics, NEGF_Common.cpp:1931-1975), the I.dat header
  * (Define_FileHeaderForCurrent, :69-84) and one appended I.dat line

@@ -142,3 +142,22 @@ def test_poles_count_equilibrium():
     kT = 8.617333262e-5 * 298.0
     assert len(E) == int((3.0 - np.pi * kT) / (2 * np.pi * kT) + 1) == 19
     np.testing.assert_allclose(E.imag, np.pi * kT * (2 * np.arange(len(E)) + 1))
+
+
+def test_read_table1d(negf_lib, tmp_path):
+    """Read_Table1D restated: header + n lines, size assertion, missing file."""
+    from electrostatic_b200 import negf
+    from electrostatic_b200._lib import NEGFError
+    p = tmp_path / "step0003_Qout.dat"
+    vals = np.linspace(-1e-3, 2e-3, 7)
+    with open(p, "w") as f:
+        f.write("'axial location / (nm)', 'Induced charge per site / (e)'\n")
+        for i, v in enumerate(vals):
+            f.write("%35.15g%35.15g\n" % (0.1 * i, v))
+    assert np.array_equal(negf.read_table1d(str(p), 7), vals)
+    with pytest.raises(NEGFError, match="Assert size, 8, is not equal to the filesize-1, 7 !"):
+        negf.read_table1d(str(p), 8)
+    with pytest.raises(NEGFError, match="Failed to read file"):
+        negf.read_table1d(str(tmp_path / "missing.dat"), 7)
+    assert negf.restart_charge_filename("output/negf", "cnt", 4) == "output/negf/cnt/step0003_Qout.dat"
+    assert negf.iter_filename(negf.step_filename("out", "cnt", 1), 12) == "out/cnt/step0001_iter/iter0012"
