@@ -17,6 +17,7 @@ NEGF_PREC_MIXED = 1
 NEGF_NORM_ABSOLUTE = 0
 NEGF_NORM_RELATIVE = 1
 NEGF_MAX_NONEQ_PATHS = 8
+NEGF_PLAN_AUTOTUNE = 1
 
 # Every symbol include/negf_b200.h declares (checked by the CPU test suite).
 EXPORTED = [
@@ -31,7 +32,8 @@ EXPORTED = [
     "negf_compute_charge_noalloc", "negf_tube_dos_points", "negf_tube_current_points", "negf_compute_dos",
     "negf_compute_current", "negf_write_transport_char", "negf_write_current_header", "negf_write_current",
     "negf_write_integrand", "negf_tube_correct_integration_limits", "negf_tube_noneq_integrand",
-    "negf_tube_noneq_layout", "negf_read_table1d",
+    "negf_tube_noneq_layout", "negf_read_table1d", "negf_broyden_step_device", "negf_affine_potential_masked",
+    "negf_charge_plan_create", "negf_charge_plan_launch", "negf_charge_plan_info", "negf_charge_plan_destroy",
 ]
 
 
@@ -150,6 +152,12 @@ def load():
         "negf_tube_noneq_integrand": [vp, dp, vp],
         "negf_tube_noneq_layout": [vp, ip, ip, dp, dp],
         "negf_read_table1d": [C.c_char_p, C.c_int, dp],
+        "negf_broyden_step_device": [vp, vp, C.c_double, vp, vp],
+        "negf_affine_potential_masked": [vp, vp, vp, vp, C.c_int, vp, vp],
+        "negf_charge_plan_create": [C.POINTER(vp), C.c_int, vp, C.c_int, C.POINTER(vp)],
+        "negf_charge_plan_launch": [vp, vp, vp],
+        "negf_charge_plan_info": [vp, ip, ip, dp, C.POINTER(C.c_longlong)],
+        "negf_charge_plan_destroy": [vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -190,7 +190,19 @@ struct negf_broyden {
         double* bufs[] = {dev.n_in, dev.n_prev, dev.F, dev.dF, dev.norm, dev.V, dev.W, dev.c, dev.sum, dev.scal, dev.part};
         for (double* p : bufs)
             if (p) cudaFree(p);
+        if (dev.step_dev) cudaFree(dev.step_dev);
     }
+};
+
+struct negf_charge_plan {
+    std::vector<negf_tube*> tubes;
+    std::vector<int> versions;
+    DevBuf d_tubes, d_chains, d_warps, d_units, d_rts, d_partial, d_scratch;
+    int num_warps = 0, num_units = 0, max_N = 0;
+    int wpb = 4, spu = negf::kSegsPerUnit;
+    double* d_Q = nullptr;
+    long long updates = 0;
+    double tuned_ms = 0.0;
 };
 
 namespace {
@@ -523,7 +535,7 @@ void build_tube_chains(Out<negf::ChainRec>& chains, Out<negf::WarpRec>& warps, T
 // (order[] is caller scratch of passes.size() ints); rts[i] describes pass i.
 void build_table_generic(const TubePass* passes, int num_passes, int* order, Out<negf::ChainRec>& chains,
                          Out<negf::WarpRec>& warps, Out<negf::SegUnit>& units, negf::ReduceTube* rts,
-                         TableCounts& cnt) {
+                         TableCounts& cnt, int segs_per_unit = negf::kSegsPerUnit) {
     cnt = TableCounts();
     for (int i = 0; i < num_passes; ++i) order[i] = i;
     for (int i = 1; i < num_passes; ++i) {  // stable insertion sort by descending N
@@ -554,8 +566,8 @@ void build_table_generic(const TubePass* passes, int num_passes, int* order, Out
             row += N;
             warps.at(w).ck_off = ck;
             ck += negf::rgf_scratch_doubles(N, warps.at(w).kind, warps.at(w).fp32);
-            for (int s0 = 0; s0 < nseg; s0 += negf::kSegsPerUnit)
-                units.push({(int)w, s0, std::min(nseg, s0 + negf::kSegsPerUnit), 0});
+            for (int s0 = 0; s0 < nseg; s0 += segs_per_unit)
+                units.push({(int)w, s0, std::min(nseg, s0 + segs_per_unit), 0});
         }
         rts[oi] = rt;
         cnt.max_N = std::max(cnt.max_N, N);
@@ -1168,6 +1180,158 @@ int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q
     return NEGF_OK;
 }
 
+// ------------------------------------------------------------------ charge plans
+namespace {
+// Tables of a plan for a given number of segments per pass-2 unit.
+int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
+    const int n = (int)p.tubes.size();
+    std::vector<TubePass> passes;
+    std::vector<negf::TubeDev> tdev;
+    long long off = 0;
+    for (int i = 0; i < n; ++i) {
+        passes.push_back({p.tubes[i], i, off, false});
+        negf::TubeDev d = make_tubedev(*p.tubes[i], false);
+        d.uc_from_U = 1;
+        tdev.push_back(d);
+        off += p.tubes[i]->N;
+    }
+    ChainTable ct;
+    Out<negf::ChainRec> oc;
+    oc.vec = &ct.chains;
+    Out<negf::WarpRec> ow;
+    ow.vec = &ct.warps;
+    Out<negf::SegUnit> ou;
+    ou.vec = &ct.units;
+    ct.rts.resize(n);
+    std::vector<int> order(n);
+    TableCounts cnt;
+    build_table_generic(passes.data(), n, order.data(), oc, ow, ou, ct.rts.data(), cnt, spu);
+    p.num_warps = (int)ct.warps.size();
+    p.num_units = (int)ct.units.size();
+    p.max_N = cnt.max_N;
+    p.updates = cnt.updates;
+    p.spu = spu;
+    NEGF_CUDA(p.d_units.reserve(std::max<size_t>(1, ct.units.size()) * sizeof(negf::SegUnit)));
+    if (!ct.units.empty())
+        NEGF_CUDA(cudaMemcpy(p.d_units.p, ct.units.data(), ct.units.size() * sizeof(negf::SegUnit),
+                             cudaMemcpyHostToDevice));
+    if (!upload_all) return NEGF_OK;
+    NEGF_CUDA(p.d_tubes.reserve(tdev.size() * sizeof(negf::TubeDev)));
+    NEGF_CUDA(p.d_chains.reserve(std::max<size_t>(1, ct.chains.size()) * sizeof(negf::ChainRec)));
+    NEGF_CUDA(p.d_warps.reserve(std::max<size_t>(1, ct.warps.size()) * sizeof(negf::WarpRec)));
+    NEGF_CUDA(p.d_rts.reserve(ct.rts.size() * sizeof(negf::ReduceTube)));
+    NEGF_CUDA(p.d_partial.reserve(std::max<long long>(1, cnt.partial_doubles) * sizeof(double)));
+    NEGF_CUDA(p.d_scratch.reserve(std::max<long long>(1, cnt.scratch_doubles) * sizeof(double)));
+    NEGF_CUDA(cudaMemcpy(p.d_tubes.p, tdev.data(), tdev.size() * sizeof(negf::TubeDev), cudaMemcpyHostToDevice));
+    if (!ct.chains.empty())
+        NEGF_CUDA(cudaMemcpy(p.d_chains.p, ct.chains.data(), ct.chains.size() * sizeof(negf::ChainRec),
+                             cudaMemcpyHostToDevice));
+    if (!ct.warps.empty())
+        NEGF_CUDA(cudaMemcpy(p.d_warps.p, ct.warps.data(), ct.warps.size() * sizeof(negf::WarpRec),
+                             cudaMemcpyHostToDevice));
+    for (int i = 0; i < n; ++i) ct.rts[i].rho0 = p.tubes[i]->shard_rank == 0 ? p.tubes[i]->d_rho0 : nullptr;
+    NEGF_CUDA(cudaMemcpy(p.d_rts.p, ct.rts.data(), ct.rts.size() * sizeof(negf::ReduceTube), cudaMemcpyHostToDevice));
+    return NEGF_OK;
+}
+
+cudaError_t plan_launch(const negf_charge_plan& p, const int* skip, cudaStream_t s) {
+    cudaError_t e = negf::launch_rgf(p.d_tubes.as<negf::TubeDev>(), p.d_chains.as<negf::ChainRec>(),
+                                     p.d_warps.as<negf::WarpRec>(), p.num_warps, p.d_units.as<negf::SegUnit>(),
+                                     p.num_units, p.d_partial.as<double>(), p.d_scratch.p, p.wpb, s, nullptr, skip);
+    if (e != cudaSuccess) return e;
+    return negf::launch_reduce(p.d_rts.as<negf::ReduceTube>(), (int)p.tubes.size(), p.max_N,
+                               p.d_partial.as<double>(), p.d_Q, s, skip);
+}
+}  // namespace
+
+int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q, int flags, negf_charge_plan** out) {
+    if (!tubes || num_tubes <= 0 || !d_Q || !out) return fail(NEGF_ERR_ARG, "null argument");
+    *out = nullptr;
+    int rc = require_device();
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::unique_ptr<negf_charge_plan> p(new negf_charge_plan());
+    for (int i = 0; i < num_tubes; ++i) {
+        if (!tubes[i]) return fail(NEGF_ERR_ARG, "null tube in batch");
+        update_paths(*tubes[i]);
+        p->tubes.push_back(tubes[i]);
+        p->versions.push_back(tubes[i]->version);
+    }
+    p->d_Q = d_Q;
+    p->wpb = ws().warps_per_block;
+    rc = plan_tables(*p, negf::kSegsPerUnit, true);
+    if (rc) return rc;
+    if (flags & NEGF_PLAN_AUTOTUNE) {
+        // time every (segments per pass-2 unit, pass-2 warps per block) pair on
+        // this batch; results are identical for all of them
+        cudaEvent_t e0, e1;
+        NEGF_CUDA(cudaEventCreate(&e0));
+        NEGF_CUDA(cudaEventCreate(&e1));
+        double best = 1e300;
+        int best_spu = negf::kSegsPerUnit, best_wpb = p->wpb;
+        for (int spu : {16, 32, 64}) {
+            rc = plan_tables(*p, spu, false);
+            if (rc) break;
+            for (int wpb : {1, 2, 4}) {
+                p->wpb = wpb;
+                cudaError_t e = plan_launch(*p, nullptr, 0);
+                for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+                    if (r == 1) e = cudaEventRecord(e0, 0);
+                    if (e == cudaSuccess) e = plan_launch(*p, nullptr, 0);
+                }
+                if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                if (e != cudaSuccess) {
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    return fail(NEGF_ERR_CUDA, cudaGetErrorString(e));
+                }
+                if (ms / 2 < best) {
+                    best = ms / 2;
+                    best_spu = spu;
+                    best_wpb = wpb;
+                }
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc) return rc;
+        p->wpb = best_wpb;
+        p->tuned_ms = best;
+        rc = plan_tables(*p, best_spu, false);
+        if (rc) return rc;
+    }
+    *out = p.release();
+    return NEGF_OK;
+}
+
+int negf_charge_plan_launch(negf_charge_plan* p, const int* d_skip, void* stream) {
+    if (!p) return fail(NEGF_ERR_ARG, "null plan");
+    for (size_t i = 0; i < p->tubes.size(); ++i)
+        if (p->tubes[i]->version != p->versions[i] || p->tubes[i]->limits_dirty)
+            return fail(NEGF_ERR_STATE, "charge plan is stale: the energy paths of tube " + std::to_string(i) +
+                                            " changed after the plan was made");
+    NEGF_CUDA(plan_launch(*p, d_skip, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+
+int negf_charge_plan_info(const negf_charge_plan* p, int* pass2_warps_per_block, int* segs_per_unit,
+                          double* tuned_ms, long long* updates) {
+    if (!p) return fail(NEGF_ERR_ARG, "null plan");
+    if (pass2_warps_per_block) *pass2_warps_per_block = p->wpb;
+    if (segs_per_unit) *segs_per_unit = p->spu;
+    if (tuned_ms) *tuned_ms = p->tuned_ms;
+    if (updates) *updates = p->updates;
+    return NEGF_OK;
+}
+
+int negf_charge_plan_destroy(negf_charge_plan* p) {
+    delete p;
+    return NEGF_OK;
+}
+
 int negf_set_tuning(int key, int value) {
     std::lock_guard<std::mutex> lk(g_mu);
     Workspace& W = ws();
@@ -1236,6 +1400,9 @@ int negf_broyden_create(int S, int max_step, double fraction, int norm_type, neg
     NEGF_CUDA(cudaMalloc(&d.scal, sizeof(double) * 4));
     NEGF_CUDA(cudaMemset(d.scal, 0, sizeof(double) * 4));
     NEGF_CUDA(cudaMalloc(&d.part, sizeof(double) * 3 * d.nblocks));
+    NEGF_CUDA(cudaMalloc(&d.step_dev, sizeof(int)));
+    const int one = 1;
+    NEGF_CUDA(cudaMemcpy(d.step_dev, &one, sizeof(int), cudaMemcpyHostToDevice));
     *out = b.release();
     return NEGF_OK;
 }
@@ -1265,6 +1432,7 @@ int negf_broyden_step(negf_broyden* b, const double* d_n_out, double* d_n_in_out
     NEGF_CUDA(negf::broyden_norm(b->dev, d_n_out, s));
     NEGF_CUDA(negf::broyden_update(b->dev, b->step - 1, s));
     b->step += 1;
+    NEGF_CUDA(negf::set_int(b->dev.step_dev, b->step, s));
     if (d_n_in_out)
         NEGF_CUDA(cudaMemcpyAsync(d_n_in_out, b->dev.n_in, sizeof(double) * b->dev.S, cudaMemcpyDeviceToDevice, s));
     if (d_norm)
@@ -1288,12 +1456,24 @@ int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void
     NEGF_CUDA(cudaMemsetAsync(d.W, 0, sizeof(double) * (size_t)d.S * d.max_step, s));
     NEGF_CUDA(cudaMemsetAsync(d.c, 0, sizeof(double) * d.max_step, s));
     b->step = 1;
+    NEGF_CUDA(negf::set_int(d.step_dev, 1, s));
     return NEGF_OK;
 }
 
-int negf_broyden_step_number(const negf_broyden* b, int* step) {
+int negf_broyden_step_number(negf_broyden* b, int* step) {
     if (!b || !step) return fail(NEGF_ERR_ARG, "null argument");
+    // device-resident steps advance the device counter only
+    NEGF_CUDA(cudaMemcpy(&b->step, b->dev.step_dev, sizeof(int), cudaMemcpyDeviceToHost));
     *step = b->step;
+    return NEGF_OK;
+}
+
+int negf_broyden_step_device(negf_broyden* b, const double* d_n_out, double max_norm, int* d_flags, void* stream) {
+    if (!b || !d_n_out || !d_flags) return fail(NEGF_ERR_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    NEGF_CUDA(negf::broyden_norm(b->dev, d_n_out, s, d_flags));
+    NEGF_CUDA(negf::broyden_update(b->dev, 0, s, d_flags));
+    NEGF_CUDA(negf::broyden_finish_step(b->dev, max_norm, d_flags, s));
     return NEGF_OK;
 }
 
@@ -1319,6 +1499,13 @@ int negf_device_selftest(int which, int n, const double* in, double* out) {
 int negf_affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, void* stream) {
     if (!K || !U0 || !Q || !U || n <= 0) return fail(NEGF_ERR_ARG, "bad affine-potential arguments");
     NEGF_CUDA(negf::affine_potential(K, U0, Q, U, n, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+
+int negf_affine_potential_masked(const double* K, const double* U0, const double* Q, double* U, int n,
+                                 const int* d_skip, void* stream) {
+    if (!K || !U0 || !Q || !U || n <= 0) return fail(NEGF_ERR_ARG, "bad affine-potential arguments");
+    NEGF_CUDA(negf::affine_potential(K, U0, Q, U, n, (cudaStream_t)stream, d_skip));
     return NEGF_OK;
 }
 

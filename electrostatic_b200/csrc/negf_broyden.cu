@@ -18,6 +18,15 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Device-resident iterations (BroydenDev::step_dev set): the iteration index
+// m = step - 1 is read on the device and `flags` (int[4]: converged,
+// iterations, error, skip) makes every kernel of a finished solve return at
+// entry, so a captured sequence of iterations needs no host round trip.
+__device__ __forceinline__ bool skipped(const int* flags) { return flags && flags[3]; }
+__device__ __forceinline__ int iter_m(const BroydenDev& b, int m_host) {
+    return b.step_dev ? *b.step_dev - 1 : m_host;
+}
+
 // Block reduction of (max, sum, sum) in a fixed order.
 __device__ __forceinline__ void block_reduce3(double& a, double& b, double& c) {
     __shared__ double sh[3][kThreads / 32];
@@ -67,7 +76,8 @@ __device__ __forceinline__ double block_sum(double v) {
 
 // Broyden_Second_Parallel.cpp:243-315: F, |F| (or relative), dF, and the
 // three scalars (max norm, sum of squares, dF^T dF) as block partials.
-__global__ void norm_kernel(BroydenDev b, const double* __restrict__ n_out) {
+__global__ void norm_kernel(BroydenDev b, const double* __restrict__ n_out, const int* flags) {
+    if (skipped(flags)) return;
     double mx = 0.0, s1 = 0.0, s2 = 0.0;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
         const double nin = b.n_in[s], nout = n_out[s];
@@ -97,8 +107,8 @@ __global__ void norm_kernel(BroydenDev b, const double* __restrict__ n_out) {
     }
 }
 
-__global__ void norm_finalize(BroydenDev b) {
-    if (threadIdx.x != 0) return;
+__global__ void norm_finalize(BroydenDev b, const int* flags) {
+    if (threadIdx.x != 0 || skipped(flags)) return;
     double mx = 0.0, s1 = 0.0, s2 = 0.0;
     for (int i = 0; i < b.nblocks; ++i) {
         mx = fmax(mx, b.part[3 * i]);
@@ -110,8 +120,11 @@ __global__ void norm_finalize(BroydenDev b) {
     b.scal[2] = s2;
 }
 
-// c[it] = sum_s V[it][s] x[s] for it = 1..rows (one block per row).
-__global__ void dots_kernel(BroydenDev b, const double* __restrict__ x, int rows) {
+// c[it] = sum_s V[it][s] x[s] for it = 1..rows (one block per row);
+// rows = m - 1 + which with m from the host or the device.
+__global__ void dots_kernel(BroydenDev b, const double* __restrict__ x, int m_host, int which, const int* flags) {
+    if (skipped(flags)) return;
+    const int rows = iter_m(b, m_host) - 1 + which;
     const int it = blockIdx.x + 1;
     if (it > rows) return;
     const double* v = b.V + (size_t)it * b.S;
@@ -122,7 +135,10 @@ __global__ void dots_kernel(BroydenDev b, const double* __restrict__ x, int rows
 }
 
 // Broyden_Second_Parallel.cpp:381-403: sum = W c (it < m), new V and W rows at m.
-__global__ void newrow_kernel(BroydenDev b, int m) {
+__global__ void newrow_kernel(BroydenDev b, int m_host, const int* flags) {
+    if (skipped(flags)) return;
+    const int m = iter_m(b, m_host);
+    if (m <= 0) return;
     const double denom = b.scal[2];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
         double acc = 0.0;
@@ -135,7 +151,9 @@ __global__ void newrow_kernel(BroydenDev b, int m) {
 }
 
 // Broyden_Second_Parallel.cpp:455-481: sum = W c (it <= m), then the new input.
-__global__ void final_kernel(BroydenDev b, int m) {
+__global__ void final_kernel(BroydenDev b, int m_host, const int* flags) {
+    if (skipped(flags)) return;
+    const int m = iter_m(b, m_host);
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
         double acc = 0.0;
         for (int it = 1; it <= m; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
@@ -146,13 +164,34 @@ __global__ void final_kernel(BroydenDev b, int m) {
     }
 }
 
+// End of a device-resident step: the loop predicate of Transport.cpp:385-505
+// (stop when the norm is not above max_norm), the step count, and the
+// MaxStep abort of :389-393 as an error flag for the host.
+__global__ void step_kernel(BroydenDev b, double max_norm, int* flags) {
+    if (flags[3]) return;
+    const double nrm = b.scal[0];
+    flags[1] += 1;
+    const int step = *b.step_dev + 1;
+    *b.step_dev = step;
+    if (!isfinite(nrm))
+        flags[2] = 2;
+    else if (!(nrm > max_norm))
+        flags[0] = 1;
+    else if (step > b.max_step)
+        flags[2] = 1;
+    flags[3] = (flags[0] || flags[2]) ? 1 : 0;
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
 __global__ void set_kernel(double* p, double v, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
 
 // U[i] = U0[i] + sum_j K[i][j] Q[j]: one warp per row, fixed-order lane tree.
 __global__ void affine_kernel(const double* __restrict__ K, const double* __restrict__ U0,
-                              const double* __restrict__ Q, double* __restrict__ U, int n) {
+                              const double* __restrict__ Q, double* __restrict__ U, int n, const int* skip) {
+    if (skip && *skip) return;
     const int lane = threadIdx.x & 31;
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (row >= n) return;
@@ -166,19 +205,38 @@ __global__ void affine_kernel(const double* __restrict__ K, const double* __rest
 
 }  // namespace
 
-cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s) {
-    norm_kernel<<<b.nblocks, kThreads, 0, s>>>(b, n_out);
-    norm_finalize<<<1, 32, 0, s>>>(b);
+cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s, const int* flags) {
+    norm_kernel<<<b.nblocks, kThreads, 0, s>>>(b, n_out, flags);
+    norm_finalize<<<1, 32, 0, s>>>(b, flags);
     return cudaGetLastError();
 }
 
-cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s) {
-    if (m > 0) {
-        if (m - 1 >= 1) dots_kernel<<<m - 1, kThreads, 0, s>>>(b, b.dF, m - 1);
-        newrow_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m);
-        dots_kernel<<<m, kThreads, 0, s>>>(b, b.F, m);
+cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int* flags) {
+    if (b.step_dev && flags) {
+        // device-resident: shapes cover every m up to max_step, rows above m return
+        const int g = b.max_step > 1 ? b.max_step : 1;
+        dots_kernel<<<g, kThreads, 0, s>>>(b, b.dF, 0, 0, flags);
+        newrow_kernel<<<b.nblocks, kThreads, 0, s>>>(b, 0, flags);
+        dots_kernel<<<g, kThreads, 0, s>>>(b, b.F, 0, 1, flags);
+        final_kernel<<<b.nblocks, kThreads, 0, s>>>(b, 0, flags);
+        return cudaGetLastError();
     }
-    final_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m);
+    if (m > 0) {
+        if (m - 1 >= 1) dots_kernel<<<m - 1, kThreads, 0, s>>>(b, b.dF, m, 0, nullptr);
+        newrow_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m, nullptr);
+        dots_kernel<<<m, kThreads, 0, s>>>(b, b.F, m, 1, nullptr);
+    }
+    final_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t broyden_finish_step(const BroydenDev& b, double max_norm, int* flags, cudaStream_t s) {
+    step_kernel<<<1, 1, 0, s>>>(b, max_norm, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t set_int(int* p, int v, cudaStream_t s) {
+    set_int_kernel<<<1, 1, 0, s>>>(p, v);
     return cudaGetLastError();
 }
 
@@ -189,10 +247,11 @@ cudaError_t broyden_set(double* p, double v, int n, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s) {
+cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s,
+                             const int* skip) {
     if (n <= 0) return cudaSuccess;
     const int warps_per_block = 8;
-    affine_kernel<<<(n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, s>>>(K, U0, Q, U, n);
+    affine_kernel<<<(n + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, s>>>(K, U0, Q, U, n, skip);
     return cudaGetLastError();
 }
 

@@ -22,7 +22,8 @@ struct __align__(16) TubeDev {
     int num_modes;
     double gamma;      // hopping [eV]
     double Uc0, Uc1;   // contact potentials [eV]
-    int use_decimation, dec_iters, dec_layers, pad0;
+    int use_decimation, dec_iters, dec_layers;
+    int uc_from_U;     // 1: contact potentials are U[0] and U[N-1] read on the device
     double beta[kMaxModes];
     double degen[kMaxModes];
 };
@@ -79,15 +80,19 @@ cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, c
                              const SegUnit* d_units, int num_units, void* d_scratch, double* d_part,
                              double* d_chain_out, double* d_site, long long site_stride, int num_e, int M, int upw,
                              double* d_red, double* d_ldos, int N, cudaStream_t stream);
+// skip (device int, may be null): when nonzero at launch time every block
+// returns at entry (device-side early exit of a captured SCF iteration).
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
-                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event);
+                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event,
+                       const int* skip = nullptr);
 // Device self-test of numeric primitives: which = 0 FP64 reciprocal,
 // 1 FP32 reciprocal (input/output as doubles), n values, device pointers.
 cudaError_t selftest(int which, int n, const double* d_in, double* d_out, cudaStream_t stream);
 // Per-site reduction (Kahan) of warp rows, minus Rho0 when rho0 != null.
 cudaError_t launch_reduce(const ReduceTube* d_rt, int num_tubes, int max_N, const double* d_partial, double* d_Q,
-                          cudaStream_t stream);
+                          cudaStream_t stream,
+                          const int* skip = nullptr);
 // Scratch elements (doubles, rounded up) needed per warp for a tube of N sites.
 // Scratch of one warp: per-lane lead self-energies (4 x 32 doubles) then the
 // segment checkpoints (Y, lambda at segment starts; X, rho at segment ends).
@@ -131,10 +136,16 @@ struct BroydenDev {
     double* scal;     // [4]: max norm, sum of squares, denominator, spare
     double* part;     // [3 * nblocks] block partials
     int nblocks;
+    int* step_dev;    // device copy of the step counter (read by device-resident steps)
 };
-cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s);
-cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s);
+cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s, const int* flags = nullptr);
+cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int* flags = nullptr);
+// Device-resident step end: flags int[4] = converged, iterations, error
+// (1 MaxStep exceeded, 2 non-finite norm), skip; advances *step_dev.
+cudaError_t broyden_finish_step(const BroydenDev& b, double max_norm, int* flags, cudaStream_t s);
+cudaError_t set_int(int* p, int v, cudaStream_t s);
 cudaError_t broyden_set(double* p, double v, int n, cudaStream_t s);
-cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s);
+cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s,
+                             const int* skip = nullptr);
 
 }  // namespace negf

@@ -448,8 +448,10 @@ __device__ __forceinline__ void pass1_chain(const TubeDev* __restrict__ tubes, c
     const bool valid = cr.mode >= 0;
     const double beta = T.beta[valid ? cr.mode : 0];
     const cd E = {cr.Er, cr.Ei};
-    const cd S0 = sigma_contact(E, T.Uc0, beta, T);
-    const cd S1 = sigma_contact(E, T.Uc1, beta, T);
+    // U_contact = U at the end sites (Nanostructure.cpp:500-504) when read on the device
+    const double Uc0 = T.uc_from_U ? U[0] : T.Uc0, Uc1 = T.uc_from_U ? U[N - 1] : T.Uc1;
+    const cd S0 = sigma_contact(E, Uc0, beta, T);
+    const cd S1 = sigma_contact(E, Uc1, beta, T);
     wscratch[0 * kWarp + lane] = S0.x;
     wscratch[1 * kWarp + lane] = S0.y;
     wscratch[2 * kWarp + lane] = S1.x;
@@ -716,7 +718,8 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
 __global__ void __launch_bounds__(32) rgf_pass1_kernel(const TubeDev* __restrict__ tubes,
                                                        const ChainRec* __restrict__ chains,
                                                        const WarpRec* __restrict__ warps, int num_warps,
-                                                       double* __restrict__ scratch) {
+                                                       double* __restrict__ scratch, const int* __restrict__ skip) {
+    if (skip && *skip) return;
     const int lane = threadIdx.x & 31;
     const int w = blockIdx.x;
     if (w >= num_warps) return;
@@ -741,7 +744,9 @@ __global__ void __launch_bounds__(128) rgf_pass2_kernel(const TubeDev* __restric
                                                         const WarpRec* __restrict__ warps,
                                                         const SegUnit* __restrict__ units, int num_units,
                                                         double* __restrict__ partial,
-                                                        const double* __restrict__ scratch) {
+                                                        const double* __restrict__ scratch,
+                                                        const int* __restrict__ skip) {
+    if (skip && *skip) return;
     const int lane = threadIdx.x & 31;
     const int ui = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (ui >= num_units) return;
@@ -775,7 +780,8 @@ __global__ void selftest_kernel(int which, int n, const double* __restrict__ in,
 constexpr int kRowGroups = 8;
 __global__ void __launch_bounds__(32 * kRowGroups) reduce_kernel(const ReduceTube* __restrict__ rts,
                                                                  const double* __restrict__ partial,
-                                                                 double* __restrict__ Q) {
+                                                                 double* __restrict__ Q, const int* __restrict__ skip) {
+    if (skip && *skip) return;  // uniform over the block
     __shared__ double sh_s[kRowGroups][32], sh_c[kRowGroups][32];
     const ReduceTube r = rts[blockIdx.y];
     const int n = blockIdx.x * 32 + threadIdx.x;
@@ -1001,17 +1007,17 @@ int rgf_kernel_regs() {
 
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
-                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event) {
+                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event, const int* skip) {
     if (num_warps <= 0) return cudaSuccess;
     if (warps_per_block < 1 || warps_per_block > 4) warps_per_block = 4;
     // pass 1 is latency-bound: one warp per block spreads the chains evenly over the SMs
     rgf_pass1_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
-                                                        static_cast<double*>(d_scratch));
+                                                        static_cast<double*>(d_scratch), skip);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (mid_event) cudaEventRecord(mid_event, stream);
     rgf_pass2_kernel<<<(num_units + warps_per_block - 1) / warps_per_block, warps_per_block * kWarp, 0, stream>>>(
-        d_tubes, d_chains, d_warps, d_units, num_units, d_partial, static_cast<const double*>(d_scratch));
+        d_tubes, d_chains, d_warps, d_units, num_units, d_partial, static_cast<const double*>(d_scratch), skip);
     return cudaGetLastError();
 }
 
@@ -1022,11 +1028,11 @@ cudaError_t selftest(int which, int n, const double* d_in, double* d_out, cudaSt
 }
 
 cudaError_t launch_reduce(const ReduceTube* d_rt, int num_tubes, int max_N, const double* d_partial, double* d_Q,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, const int* skip) {
     if (num_tubes <= 0 || max_N <= 0) return cudaSuccess;
     dim3 grid((max_N + 31) / 32, num_tubes);
     dim3 block(32, kRowGroups);
-    reduce_kernel<<<grid, block, 0, stream>>>(d_rt, d_partial, d_Q);
+    reduce_kernel<<<grid, block, 0, stream>>>(d_rt, d_partial, d_Q, skip);
     return cudaGetLastError();
 }
 
@@ -1036,7 +1042,7 @@ cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, c
                              double* d_red, double* d_ldos, int N, cudaStream_t stream) {
     if (num_warps <= 0) return cudaSuccess;
     rgf_pass1_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
-                                                        static_cast<double*>(d_scratch));
+                                                        static_cast<double*>(d_scratch), nullptr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     rgf_transport_kernel<<<num_units, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, d_units, num_units,

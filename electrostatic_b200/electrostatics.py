@@ -59,8 +59,10 @@ class GateAllAround:
         return -float(Vg) - self.K @ np.asarray(Q, dtype=np.float64)
 
     def device_operator(self, Vg, device="cuda"):
-        """(K_dev, U0_dev) for negf_affine_potential: U = U0 + Kd Q with Kd = -K."""
+        """(K_dev, U0_dev) for negf_affine_potential: U = U0 + Kd Q with Kd = -K
+        (Kd is uploaded once and reused)."""
         import torch
-        Kd = torch.tensor(-self.K, dtype=torch.float64, device=device).contiguous()
+        if getattr(self, "_Kd", None) is None or str(self._Kd.device) != str(torch.device(device)):
+            self._Kd = torch.tensor(-self.K, dtype=torch.float64, device=device).contiguous()
         U0 = torch.full((self.N,), -float(Vg), dtype=torch.float64, device=device)
-        return Kd, U0
+        return self._Kd, U0

@@ -361,6 +361,12 @@ class Broyden:
 
     Execute_Broyden_Modified_Second_Algorithm_Parallel = step
 
+    def step_device(self, n_out_dev, max_norm, flags_dev, stream=None):
+        """Device-resident step (capturable): flags_dev int32[4] on the device
+        = converged, steps taken, error, skip."""
+        check(_lib.load().negf_broyden_step_device(self._h, _ptr(n_out_dev), float(max_norm), _ptr(flags_dev),
+                                                   _stream(stream)), "negf_broyden_step_device")
+
     def reset(self, keep_charge=False, init_value=0.0, stream=None):
         check(_lib.load().negf_broyden_reset(self._h, int(bool(keep_charge)), float(init_value), _stream(stream)),
               "negf_broyden_reset")
@@ -429,3 +435,44 @@ def read_table1d(filename: str, n: int) -> np.ndarray:
     out = np.zeros(n)
     check(_lib.load().negf_read_table1d(filename.encode(), int(n), _dptr(out)), "negf_read_table1d")
     return out
+
+
+class ChargePlan:
+    """A batch of tubes with its launch tables on the device: launch() is
+    kernel launches only (capturable in a CUDA graph); the contact potentials
+    follow the end sites of each tube's potential buffer."""
+
+    def __init__(self, tubes: Sequence[CNT], out, autotune=False):
+        L = _lib.load()
+        self.tubes = list(tubes)
+        self.out = out
+        arr = (C.c_void_p * len(tubes))(*[t.handle for t in tubes])
+        h = C.c_void_p()
+        check(L.negf_charge_plan_create(arr, len(tubes), _ptr(out), _lib.NEGF_PLAN_AUTOTUNE if autotune else 0,
+                                        C.byref(h)), "negf_charge_plan_create")
+        self._h = h
+
+    def launch(self, skip=None, stream=None):
+        check(_lib.load().negf_charge_plan_launch(self._h, _ptr(skip), _stream(stream)), "negf_charge_plan_launch")
+
+    def info(self) -> dict:
+        w, s, ms, up = C.c_int(), C.c_int(), C.c_double(), C.c_longlong()
+        check(_lib.load().negf_charge_plan_info(self._h, C.byref(w), C.byref(s), C.byref(ms), C.byref(up)),
+              "negf_charge_plan_info")
+        return dict(pass2_warps_per_block=w.value, segs_per_unit=s.value, tuned_ms=ms.value, updates=up.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().negf_charge_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def affine_potential_masked(K_dev, U0_dev, Q_dev, U_dev, n, skip, stream=None):
+    check(_lib.load().negf_affine_potential_masked(_ptr(K_dev), _ptr(U0_dev), _ptr(Q_dev), _ptr(U_dev), int(n),
+                                                   _ptr(skip), _stream(stream)), "negf_affine_potential_masked")

@@ -136,3 +136,119 @@ def run_scf_oracle(oracle_tube, K, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
         if not reset_with_previous_charge:
             n_in = np.full(N, float(initial_charge))
     return res
+
+
+def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
+                  initial_charge=0.0, reset_with_previous_charge=False, use_graph=True, iters_per_graph=8,
+                  autotune=True):
+    """Self-consistent bias sweep of a batch of tubes with one Broyden over
+    all their sites (the all-tubes n_in of Broyden_Parallel_General.cpp:42-66).
+
+    Each iteration: U_t = U0_t + K_t n_in[t] for every tube (its electrostatics
+    operator), one charge-plan launch for the whole batch, one device-resident
+    Broyden step.  With use_graph, iters_per_graph iterations are captured in
+    one CUDA graph and replayed until the device flags say converged (or
+    failed); the host reads the 4 flag ints once per replay.  Returns an
+    SCFResult plus the plan's schedule."""
+    import torch
+    from .negf import Broyden, ChargePlan, affine_potential_masked
+
+    dev = torch.device("cuda")
+    Ns = [t.num_field_sites for t in tubes]
+    offs = np.concatenate([[0], np.cumsum(Ns)]).astype(int)
+    S = int(offs[-1])
+    stream = torch.cuda.Stream()
+    res = SCFResult()
+    with torch.cuda.stream(stream):
+        Q = torch.zeros(S, dtype=torch.float64, device=dev)
+        n0 = torch.full((S,), float(initial_charge), dtype=torch.float64, device=dev)
+        br = Broyden(n0, max_step=max_step, fraction=fraction, norm_type=norm_type, stream=stream)
+        nin = br.input_device_ptr()
+        ops = []
+        for e in electros:
+            Kd, U0 = e.device_operator(0.0)
+            ops.append((Kd, U0.clone()))
+        U_ptrs = [t.potential_device_ptr() for t in tubes]
+        flags = torch.zeros(4, dtype=torch.int32, device=dev)
+        skip = flags.data_ptr() + 3 * 4
+        # the initial potential (paths do not depend on it; contact potentials are read on the device)
+        for (Kd, U0), t, o, N, Up in zip(ops, tubes, offs, Ns, U_ptrs):
+            affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, None, stream=stream)
+        plan = ChargePlan(tubes, Q, autotune=autotune)
+
+        def body(s):
+            for (Kd, U0), o, N, Up in zip(ops, offs, Ns, U_ptrs):
+                affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip, stream=s)
+            plan.launch(skip=skip, stream=s)
+            br.step_device(Q, max_norm, flags, stream=s)
+
+        graph = None
+        if use_graph:
+            flags[3] = 1  # load every kernel once, all skipped
+            body(stream)
+            stream.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=stream):
+                for _ in range(iters_per_graph):
+                    body(torch.cuda.current_stream())
+        for Vg in Vg_list:
+            for (Kd, U0), e in zip(ops, electros):
+                U0.copy_(e.device_operator(Vg)[1])
+            flags.zero_()
+            stream.synchronize()
+            t0 = time.perf_counter()
+            while True:
+                if graph is not None:
+                    graph.replay()
+                else:
+                    body(stream)
+                f = flags.cpu().numpy()
+                if f[3]:
+                    break
+            dt = time.perf_counter() - t0
+            if f[2] == 1:
+                raise RuntimeError("Broyden_Step has exceeded the Broyden_Threshold_MaxStep")
+            if f[2] == 2:
+                raise RuntimeError("non-finite Broyden norm")
+            U = np.concatenate([device_view(Up, N).cpu().numpy() for Up, N in zip(U_ptrs, Ns)])
+            res.steps.append(StepResult(Vg, int(f[1]), float("nan"), Q.cpu().numpy().copy(), U, dt))
+            br.reset(keep_charge=reset_with_previous_charge, init_value=initial_charge, stream=stream)
+        stream.synchronize()
+    info = plan.info()
+    del graph
+    plan.close()
+    br.close()
+    res.schedule = info
+    return res
+
+
+def run_scf_batch_oracle(oracle_tubes, Ks, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200,
+                         norm_type="absolute", initial_charge=0.0, nthreads=8):
+    """The batched loop on the CPU oracle: one Broyden over all tubes' sites."""
+    from oracle import oracle as O
+
+    Ns = [t.N for t in oracle_tubes]
+    offs = np.concatenate([[0], np.cumsum(Ns)]).astype(int)
+    S = int(offs[-1])
+    n_in = np.full(S, float(initial_charge))
+    br = O.OracleBroyden(n_in, max_step=max_step, fraction=fraction, norm_type=norm_type)
+    res = SCFResult()
+    for Vg in Vg_list:
+        t0 = time.perf_counter()
+        it = 0
+        while True:
+            Q = np.zeros(S)
+            for t, K, a, b in zip(oracle_tubes, Ks, offs[:-1], offs[1:]):
+                U = -float(Vg) - K @ n_in[a:b]
+                t.set_potential(U, (U[0], U[-1]))
+                Q[a:b] = t.charge(nthreads=nthreads)
+            nrm, n_in, _ = br.step(Q)
+            it += 1
+            if not (nrm > max_norm):
+                break
+            if it >= max_step:
+                raise RuntimeError("Broyden_Step has exceeded the Broyden_Threshold_MaxStep")
+        res.steps.append(StepResult(Vg, it, nrm, Q, None, time.perf_counter() - t0))
+        br.reset(keep_charge=False, init_value=initial_charge)
+        n_in = np.full(S, float(initial_charge))
+    return res

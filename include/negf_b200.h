@@ -248,6 +248,25 @@ int negf_write_current(const char* path, int step, double Vds, double Vgs, const
                        double avg_intg_pts, int total_iterations, double total_conductance);
 int negf_write_integrand(negf_tube* t, const char* path, int count, const double* E, const double* integrand);
 
+/* Charge plans: the launch tables of a batch uploaded once, so that
+ * negf_charge_plan_launch is kernel launches only (no allocation, no host
+ * copy, no synchronisation) and can be captured in a CUDA graph.  The
+ * contact potentials are read on the device as U[0] and U[N-1] of each
+ * tube's potential buffer (U_contact = U at the end sites,
+ * Nanostructure.cpp:500-504).  d_Q: device output of sum N doubles (tube
+ * order).  With NEGF_PLAN_AUTOTUNE the pass-2 schedule (segments per unit
+ * 16/32/64 x warps per block 1/2/4) is timed on the batch and the fastest
+ * kept (results are identical for all).  A plan is stale (NEGF_ERR_STATE at
+ * launch) once a tube's energy paths change (contact mu, adaptive limits);
+ * d_skip (device int or null) skips the launch at kernel entry when set. */
+#define NEGF_PLAN_AUTOTUNE 1
+typedef struct negf_charge_plan negf_charge_plan;
+int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q, int flags, negf_charge_plan** plan);
+int negf_charge_plan_launch(negf_charge_plan* plan, const int* d_skip, void* stream);
+int negf_charge_plan_info(const negf_charge_plan* plan, int* pass2_warps_per_block, int* segs_per_unit,
+                          double* tuned_ms, long long* updates);
+int negf_charge_plan_destroy(negf_charge_plan* plan);
+
 /* Broyden modified-second mixing (Transport.H:203-208):
  * Set_Broyden_Parallel (Broyden_Parallel_General.cpp:68-248),
  * Execute_Broyden_Modified_Second_Algorithm_Parallel
@@ -268,7 +287,16 @@ int negf_broyden_step(negf_broyden* b, const double* d_n_out, double* d_n_in_out
  * reset_with_previous_charge_distribution, otherwise n_in = init_value. */
 int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void* stream);
 /* Broyden_Step (1-based). */
-int negf_broyden_step_number(const negf_broyden* b, int* step);
+int negf_broyden_step_number(negf_broyden* b, int* step);
+/* Device-resident Broyden step (no host synchronisation; capturable in a
+ * CUDA graph).  d_flags: int[4] in device memory, zeroed by the caller at
+ * the start of a solve: [0] converged (norm <= max_norm, the loop predicate
+ * of Transport.cpp:385-505), [1] steps taken, [2] error (1: the step count
+ * passed max_step, Transport.cpp:389-393; 2: non-finite norm), [3] skip
+ * (= [0] or [2]).  Once [3] is set, this call and every *_masked / plan
+ * launch given d_flags + 3 returns at kernel entry, so a captured sequence
+ * of iterations stops itself.  The iteration index is read on the device. */
+int negf_broyden_step_device(negf_broyden* b, const double* d_n_out, double max_norm, int* d_flags, void* stream);
 /* Device pointer of the current input charge n_in. */
 int negf_broyden_input_device_ptr(negf_broyden* b, double** d_n_in);
 
@@ -279,6 +307,8 @@ int negf_device_selftest(int which, int n, const double* in, double* out);
 
 /* Affine electrostatics stand-in used by the SCF harness:
  * d_U[i] = d_U0[i] + sum_j K[i*n + j] * d_Q[j]   (all device pointers). */
+int negf_affine_potential_masked(const double* K, const double* U0, const double* Q, double* U, int n,
+                                 const int* d_skip, void* stream);
 int negf_affine_potential(const double* d_K, const double* d_U0, const double* d_Q, double* d_U, int n,
                           void* stream);
 

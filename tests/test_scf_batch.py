@@ -1,0 +1,99 @@
+"""Batched self-consistency on the GPU: charge plans, device-resident Broyden
+steps and CUDA-graph replay, against the host loop and the oracle."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch(oracle=None, modes=(2, 3, 2), cells=(10, 17, 6), chir=(17, 13, 19), mu=(0.0, -0.2), precision="fp64"):
+    from electrostatic_b200.electrostatics import GateAllAround
+    from electrostatic_b200.negf import CNT
+    tubes, oracles, electros = [], [], []
+    for m, uc, ch in zip(modes, cells, chir):
+        kw = dict(type_id=(ch, 0), num_unitcells=uc, num_modes=m, contact_mu=mu, contact_T=(300.0, 300.0),
+                  eq_integration_pts=(16, 16, 24), noneq_integration_pts=(24,), E_zPlus_imag=1e-5, E_pole_max=3.0)
+        t = CNT(precision=precision, **kw)
+        y = t.site_positions()
+        e = GateAllAround(y, r_tube=0.0665e-9 * ch / 17 * 10, r_gate=1.5e-9 + 0.0665e-9 * ch / 17 * 10)
+        tubes.append(t)
+        electros.append(e)
+        if oracle is not None:
+            oracles.append(oracle.OracleTube(**kw))
+    return tubes, electros, oracles
+
+
+def test_plan_matches_compute_charge():
+    import torch
+    from electrostatic_b200.negf import ChargePlan, compute_charge
+    tubes, _, _ = _batch()
+    rng = np.random.default_rng(3)
+    for t in tubes:
+        U = 0.1 * rng.standard_normal(t.num_field_sites)
+        t.set_potential(U, (U[0], U[-1]))
+    S = sum(t.num_field_sites for t in tubes)
+    ref = torch.zeros(S, dtype=torch.float64, device="cuda")
+    compute_charge(tubes, out=ref)
+    for autotune in (False, True):
+        Q = torch.zeros(S, dtype=torch.float64, device="cuda")
+        plan = ChargePlan(tubes, Q, autotune=autotune)
+        plan.launch()
+        torch.cuda.synchronize()
+        assert torch.equal(Q, ref)
+        info = plan.info()
+        assert info["pass2_warps_per_block"] in (1, 2, 4) and info["segs_per_unit"] in (16, 32, 64)
+        plan.close()
+
+
+def test_plan_stale_after_contact_change():
+    import torch
+    from electrostatic_b200._lib import NEGFError
+    from electrostatic_b200.negf import ChargePlan
+    tubes, _, _ = _batch()
+    Q = torch.zeros(sum(t.num_field_sites for t in tubes), dtype=torch.float64, device="cuda")
+    plan = ChargePlan(tubes, Q)
+    tubes[1].set_Contact_Electrochemical_Potential((0.0, -0.3))
+    with pytest.raises(NEGFError, match="stale"):
+        plan.launch()
+
+
+def test_device_broyden_matches_host_steps():
+    import torch
+    from electrostatic_b200.negf import Broyden
+    S = 300
+    rng = np.random.default_rng(9)
+    A = np.eye(S) * 0.5 + 0.01 * rng.standard_normal((S, S))
+    b = rng.standard_normal(S)
+    n0 = torch.zeros(S, dtype=torch.float64, device="cuda")
+    h = Broyden(n0, max_step=50, fraction=0.2)
+    d = Broyden(n0, max_step=50, fraction=0.2)
+    flags = torch.zeros(4, dtype=torch.int32, device="cuda")
+    for _ in range(12):
+        xh = torch.from_numpy(A @ _read(h.input_device_ptr(), S) + b).cuda()
+        h.step(xh)
+        xd = torch.from_numpy(A @ _read(d.input_device_ptr(), S) + b).cuda()
+        d.step_device(xd, 1e-30, flags)
+    torch.cuda.synchronize()
+    assert np.array_equal(_read(h.input_device_ptr(), S), _read(d.input_device_ptr(), S))
+    assert flags.cpu().tolist()[:3] == [0, 12, 0] and d.step_number == 13
+
+
+def _read(ptr, n):
+    from electrostatic_b200.scf import device_view
+    return device_view(ptr, n).cpu().numpy()
+
+
+def test_batch_scf_graph_equals_loop_and_oracle(oracle):
+    from electrostatic_b200.scf import run_scf_batch, run_scf_batch_oracle
+    Vg = [0.0, 0.15]
+    tubes, electros, oracles = _batch(oracle)
+    r_graph = run_scf_batch(tubes, electros, Vg, use_graph=True, iters_per_graph=4)
+    tubes2, electros2, _ = _batch()
+    r_loop = run_scf_batch(tubes2, electros2, Vg, use_graph=False, autotune=False)
+    for a, b in zip(r_graph.steps, r_loop.steps):
+        assert a.iterations == b.iterations
+        assert np.array_equal(a.Q, b.Q)
+    r_o = run_scf_batch_oracle(oracles, [e.K for e in electros], Vg)
+    for a, b in zip(r_graph.steps, r_o.steps):
+        assert a.iterations == b.iterations
+        assert np.max(np.abs(a.Q - b.Q)) <= 1e-8 * np.max(np.abs(b.Q))
