@@ -200,7 +200,7 @@ def scf_measure(threads):
     """Config-1 SCF sweep: device loop (FP64) vs the same loop on the CPU oracle."""
     from electrostatic_b200.electrostatics import GateAllAround
     from electrostatic_b200.negf import CNT
-    from electrostatic_b200.scf import run_scf, run_scf_oracle
+    from electrostatic_b200.scf import run_scf, run_scf_batch, run_scf_oracle
     from oracle import oracle as O
     tube = CNT(**SCF_KW)
     y = tube.site_positions()
@@ -208,12 +208,77 @@ def scf_measure(threads):
     ga = GateAllAround(y, ot.radius, ot.radius + 1.5e-9)
     run_scf(tube, ga, [0.0])  # warm-up (tables, caches)
     rg = run_scf(tube, ga, SCF_VG)
+    rgraph = run_scf_batch([tube], [ga], SCF_VG, use_graph=True, iters_per_graph=8, autotune=False)
     ro = run_scf_oracle(ot, ga.K, SCF_VG, nthreads=threads)
     dq = max(float(np.max(np.abs(a.Q - b.Q))) for a, b in zip(rg.steps, ro.steps))
     return {"workload": SCF_WORKLOAD, "gpu_seconds": rg.seconds, "gpu_iterations": [s.iterations for s in rg.steps],
             "cpu_seconds": ro.seconds, "cpu_iterations": [s.iterations for s in ro.steps], "cpu_cores": threads,
             "cpu_kind": "port (oracle, O(N) walk; the reference path at Vds=0 has no real-axis walk)",
-            "max_abs_dQ_gpu_vs_cpu": dq, "speedup": ro.seconds / rg.seconds}
+            "max_abs_dQ_gpu_vs_cpu": dq, "speedup": ro.seconds / rg.seconds,
+            "gpu_graph_seconds": rgraph.seconds, "gpu_graph_iterations": [s.iterations for s in rgraph.steps],
+            "graph_speedup_vs_cpu": ro.seconds / rgraph.seconds,
+            "max_abs_dQ_graph_vs_loop": max(float(np.max(np.abs(a.Q - b.Q))) for a, b in zip(rgraph.steps, rg.steps))}
+
+
+def config4_measure(torch, passes=5):
+    """Uneven 16-tube batch (seeded): batched charge pass (autotuned plan)
+    throughput and the self-consistent gate sweep replayed as CUDA graphs,
+    in mixed precision and in FP64."""
+    from electrostatic_b200.electrostatics import GateAllAround
+    from electrostatic_b200.negf import CNT, ChargePlan
+    from electrostatic_b200.scf import run_scf_batch
+    from electrostatic_b200.workloads import GATE_SWEEP, SEED_BASE, gate_with_contacts, site_potential, uneven_batch
+    out = {"workload": "16 tubes (13,0)/(17,0)/(19,0), 200-2000 unit cells, 2-10 modes, 512-8192 energies each, "
+                       "Vds 0.4 V, 300 K; gate-all-around stand-in per tube with source/drain electrodes over the first/last "
+                       "min(5 nm, L/10); Vg 0..0.6 V step 0.05, "
+                       "Broyden alpha 0.1 to 1e-6 absolute max-norm; seeded (%d)" % (SEED_BASE + 4)}
+    electros = None
+    Qs = {}
+    for prec in ("mixed", "fp64"):
+        descs = uneven_batch(precision=prec)
+        tubes = [CNT(**d) for d in descs]
+        if electros is None:
+            electros = []
+            for d, t in zip(descs, tubes):
+                R = 1.42e-10 * np.sqrt(3.0) * d["type_id"][0] / (2 * np.pi)  # CNT.cpp:23-41
+                electros.append(gate_with_contacts(t.site_positions(), R))
+        for i, t in enumerate(tubes):
+            U = site_potential(t.site_positions(), SEED_BASE + 4 + 100 * i)
+            t.set_potential(U, (U[0], U[-1]))
+        S = sum(t.num_field_sites for t in tubes)
+        Q = torch.zeros(S, dtype=torch.float64, device="cuda")
+        plan = ChargePlan(tubes, Q, autotune=True)
+        info = plan.info()
+        for _ in range(2):
+            plan.launch()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(passes):
+            plan.launch(stream=torch.cuda.current_stream())
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / passes
+        plan.close()
+        entry = {"updates_per_pass": info["updates"], "ms_per_pass": ms, "updates_per_s": info["updates"] / (ms * 1e-3),
+                 "schedule": {"pass2_warps_per_block": info["pass2_warps_per_block"],
+                              "segs_per_unit": info["segs_per_unit"]}}
+        try:
+            sw = 1e-4 if prec == "mixed" else None
+            r = run_scf_batch(tubes, electros, GATE_SWEEP, use_graph=True, iters_per_graph=4, switch_norm=sw)
+            entry.update({"scf_seconds": r.seconds, "scf_iterations": [s.iterations for s in r.steps]})
+            if sw:
+                entry["switch_norm"] = sw
+                entry["scf_lowprec_iterations"] = [s.lowprec_iterations for s in r.steps]
+            Qs[prec] = [s.Q for s in r.steps]
+        except RuntimeError as e:
+            entry["scf_error"] = str(e)
+        out[prec] = entry
+        del tubes
+    if "mixed" in Qs and "fp64" in Qs:
+        out["mixed_vs_fp64_rel"] = max(float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+                                       for a, b in zip(Qs["mixed"], Qs["fp64"]))
+    return out
 
 
 def ring_positions_nm(unitcells, acc=1.42e-10):
@@ -233,6 +298,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scf", action="store_true")
+    ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis)")
     args = ap.parse_args()
@@ -367,6 +433,7 @@ def main():
                              "N=4000, faithful O(N)-per-site contact walk (NEGF_Common.cpp:3418-3426), "
                              f"{threads} threads over energies; {dt:.2f} s"}
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
+        cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                 "frac": achieved_tf / peak_tf if peak_tf else None,
                 "traffic": prof.get("dram_bytes_per_launch"),
@@ -384,11 +451,11 @@ def main():
                 "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
                            "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu, "scf": scf,
+                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config4": cfg4,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
                         "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},
-                "gpu_launches": 2 * args.steps, "clocks": clk.summary(clk_lo, clk_hi),
+                "gpu_launches": int(st["kernel_launches"]) * args.steps, "clocks": clk.summary(clk_lo, clk_hi),
                 "kernel_ms_per_pass": {"rgf": k_ms, "rgf_pass1": float(np.mean(p1_ms)),
                                        "rgf_pass2": float(np.mean(p2_ms)), "reduce": float(np.mean(red_ms))}}
         print(json.dumps(line), flush=True)

@@ -18,6 +18,7 @@ NEGF_NORM_ABSOLUTE = 0
 NEGF_NORM_RELATIVE = 1
 NEGF_MAX_NONEQ_PATHS = 8
 NEGF_PLAN_AUTOTUNE = 1
+NEGF_PLAN_FP64 = 2
 
 # Every symbol include/negf_b200.h declares (checked by the CPU test suite).
 EXPORTED = [
@@ -34,6 +35,7 @@ EXPORTED = [
     "negf_write_integrand", "negf_tube_correct_integration_limits", "negf_tube_noneq_integrand",
     "negf_tube_noneq_layout", "negf_read_table1d", "negf_broyden_step_device", "negf_affine_potential_masked",
     "negf_charge_plan_create", "negf_charge_plan_launch", "negf_charge_plan_info", "negf_charge_plan_destroy",
+    "negf_broyden_step_device_switch",
 ]
 
 
@@ -153,6 +155,7 @@ def load():
         "negf_tube_noneq_layout": [vp, ip, ip, dp, dp],
         "negf_read_table1d": [C.c_char_p, C.c_int, dp],
         "negf_broyden_step_device": [vp, vp, C.c_double, vp, vp],
+        "negf_broyden_step_device_switch": [vp, vp, C.c_double, C.c_double, vp, vp],
         "negf_affine_potential_masked": [vp, vp, vp, vp, C.c_int, vp, vp],
         "negf_charge_plan_create": [C.POINTER(vp), C.c_int, vp, C.c_int, C.POINTER(vp)],
         "negf_charge_plan_launch": [vp, vp, vp],

@@ -203,6 +203,7 @@ struct negf_charge_plan {
     double* d_Q = nullptr;
     long long updates = 0;
     double tuned_ms = 0.0;
+    bool force_fp64 = false;
 };
 
 namespace {
@@ -492,7 +493,9 @@ void build_tube_chains(Out<negf::ChainRec>& chains, Out<negf::WarpRec>& warps, T
             for (int idx = lo; idx < hi; ++idx) {
                 const Item it = pass_item(t, tp.rho0_pass, idx);
                 if (it.kind != kind) continue;
-                const int want32 = mixed && std::fabs(it.E.imag()) >= band ? 1 : 0;
+                // FP32 recursions only for contour points at least `band` above the real
+                // axis; real-axis chains (running products over the whole tube) stay FP64
+                const int want32 = mixed && it.kind == negf::kContour && std::fabs(it.E.imag()) >= band ? 1 : 0;
                 if (want32 != fp32) continue;
                 for (int m = 0; m < M; ++m) {
                     negf::ChainRec c{};
@@ -1185,6 +1188,12 @@ namespace {
 // Tables of a plan for a given number of segments per pass-2 unit.
 int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
     const int n = (int)p.tubes.size();
+    // an FP64 plan of mixed-precision tubes: their descriptors read as FP64 while the table is built
+    std::vector<int> saved(n);
+    for (int i = 0; i < n; ++i) {
+        saved[i] = p.tubes[i]->d.precision;
+        if (p.force_fp64) p.tubes[i]->d.precision = NEGF_PREC_FP64;
+    }
     std::vector<TubePass> passes;
     std::vector<negf::TubeDev> tdev;
     long long off = 0;
@@ -1206,6 +1215,7 @@ int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
     std::vector<int> order(n);
     TableCounts cnt;
     build_table_generic(passes.data(), n, order.data(), oc, ow, ou, ct.rts.data(), cnt, spu);
+    for (int i = 0; i < n; ++i) p.tubes[i]->d.precision = saved[i];
     p.num_warps = (int)ct.warps.size();
     p.num_units = (int)ct.units.size();
     p.max_N = cnt.max_N;
@@ -1258,6 +1268,7 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
         p->versions.push_back(tubes[i]->version);
     }
     p->d_Q = d_Q;
+    p->force_fp64 = (flags & NEGF_PLAN_FP64) != 0;
     p->wpb = ws().warps_per_block;
     rc = plan_tables(*p, negf::kSegsPerUnit, true);
     if (rc) return rc;
@@ -1473,7 +1484,17 @@ int negf_broyden_step_device(negf_broyden* b, const double* d_n_out, double max_
     cudaStream_t s = (cudaStream_t)stream;
     NEGF_CUDA(negf::broyden_norm(b->dev, d_n_out, s, d_flags));
     NEGF_CUDA(negf::broyden_update(b->dev, 0, s, d_flags));
-    NEGF_CUDA(negf::broyden_finish_step(b->dev, max_norm, d_flags, s));
+    NEGF_CUDA(negf::broyden_finish_step(b->dev, max_norm, 0.0, d_flags, s));
+    return NEGF_OK;
+}
+
+int negf_broyden_step_device_switch(negf_broyden* b, const double* d_n_out, double max_norm, double switch_norm,
+                                    int* d_flags, void* stream) {
+    if (!b || !d_n_out || !d_flags || !(switch_norm > 0)) return fail(NEGF_ERR_ARG, "bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    NEGF_CUDA(negf::broyden_norm(b->dev, d_n_out, s, d_flags));
+    NEGF_CUDA(negf::broyden_update(b->dev, 0, s, d_flags));
+    NEGF_CUDA(negf::broyden_finish_step(b->dev, max_norm, switch_norm, d_flags, s));
     return NEGF_OK;
 }
 

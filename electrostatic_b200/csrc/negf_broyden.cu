@@ -27,13 +27,16 @@ __device__ __forceinline__ int iter_m(const BroydenDev& b, int m_host) {
     return b.step_dev ? *b.step_dev - 1 : m_host;
 }
 
+// max that keeps a NaN (a non-finite residual must not read as converged)
+__device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+
 // Block reduction of (max, sum, sum) in a fixed order.
 __device__ __forceinline__ void block_reduce3(double& a, double& b, double& c) {
     __shared__ double sh[3][kThreads / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
-        a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+        a = nanmax(a, __shfl_xor_sync(0xffffffffu, a, o));
         b += __shfl_xor_sync(0xffffffffu, b, o);
         c += __shfl_xor_sync(0xffffffffu, c, o);
     }
@@ -50,7 +53,7 @@ __device__ __forceinline__ void block_reduce3(double& a, double& b, double& c) {
         c = lane < nw ? sh[2][lane] : 0.0;
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) {
-            a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+            a = nanmax(a, __shfl_xor_sync(0xffffffffu, a, o));
             b += __shfl_xor_sync(0xffffffffu, b, o);
             c += __shfl_xor_sync(0xffffffffu, c, o);
         }
@@ -95,7 +98,7 @@ __global__ void norm_kernel(BroydenDev b, const double* __restrict__ n_out, cons
         b.dF[s] = d;
         b.F[s] = Fc;
         b.sum[s] = 0.0;
-        mx = fmax(mx, nr);
+        mx = nanmax(mx, nr);
         s1 += sq;
         s2 += d * d;
     }
@@ -111,7 +114,7 @@ __global__ void norm_finalize(BroydenDev b, const int* flags) {
     if (threadIdx.x != 0 || skipped(flags)) return;
     double mx = 0.0, s1 = 0.0, s2 = 0.0;
     for (int i = 0; i < b.nblocks; ++i) {
-        mx = fmax(mx, b.part[3 * i]);
+        mx = nanmax(mx, b.part[3 * i]);
         s1 += b.part[3 * i + 1];
         s2 += b.part[3 * i + 2];
     }
@@ -167,19 +170,31 @@ __global__ void final_kernel(BroydenDev b, int m_host, const int* flags) {
 // End of a device-resident step: the loop predicate of Transport.cpp:385-505
 // (stop when the norm is not above max_norm), the step count, and the
 // MaxStep abort of :389-393 as an error flag for the host.
-__global__ void step_kernel(BroydenDev b, double max_norm, int* flags) {
+// switch_norm > 0 (precision switching, flags int[8]): until flags[4] is set
+// the charge came from the low-precision plan; the first norm below
+// switch_norm sets flags[4] and later steps use the FP64 plan, and only an
+// FP64 charge can end the solve.  flags[5] / flags[6] are the skip words of
+// the low-precision and FP64 plans; flags[7] counts low-precision steps.
+__global__ void step_kernel(BroydenDev b, double max_norm, double switch_norm, int* flags) {
     if (flags[3]) return;
     const double nrm = b.scal[0];
     flags[1] += 1;
     const int step = *b.step_dev + 1;
     *b.step_dev = step;
+    const bool fp64_charge = !(switch_norm > 0) || flags[4];
+    if (!fp64_charge) flags[7] += 1;  // steps on a low-precision charge
     if (!isfinite(nrm))
         flags[2] = 2;
-    else if (!(nrm > max_norm))
+    else if (fp64_charge && !(nrm > max_norm))
         flags[0] = 1;
     else if (step > b.max_step)
         flags[2] = 1;
     flags[3] = (flags[0] || flags[2]) ? 1 : 0;
+    if (switch_norm > 0) {
+        if (!flags[4] && nrm < switch_norm) flags[4] = 1;
+        flags[5] = (flags[3] || flags[4]) ? 1 : 0;
+        flags[6] = (flags[3] || !flags[4]) ? 1 : 0;
+    }
 }
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
@@ -230,8 +245,8 @@ cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int
     return cudaGetLastError();
 }
 
-cudaError_t broyden_finish_step(const BroydenDev& b, double max_norm, int* flags, cudaStream_t s) {
-    step_kernel<<<1, 1, 0, s>>>(b, max_norm, flags);
+cudaError_t broyden_finish_step(const BroydenDev& b, double max_norm, double switch_norm, int* flags, cudaStream_t s) {
+    step_kernel<<<1, 1, 0, s>>>(b, max_norm, switch_norm, flags);
     return cudaGetLastError();
 }
 

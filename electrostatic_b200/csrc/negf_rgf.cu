@@ -184,60 +184,6 @@ struct Chain {
     bool valid;
 };
 
-// alpha_n = E - U_n - delta_{n,0} Sigma_0 - delta_{n,N-1} Sigma_1
-template <typename R>
-__device__ __forceinline__ void alpha(const Chain<R>& c, int n, R u, R& ar, R& ai) {
-    ar = c.Er - u;
-    ai = c.Ei;
-    if (n == 0) {
-        ar -= c.s0r;
-        ai -= c.s0i;
-    }
-    if (n == c.N - 1) {
-        ar -= c.s1r;
-        ai -= c.s1i;
-    }
-}
-
-// Forward step at site n (< N-1): Y_{n+1} = h_n^2 / (alpha_n - Y_n), lambda_{n+1}.
-template <typename R, bool RA>
-__device__ __forceinline__ void fwd_step(const Chain<R>& c, int n, R u, R yr, R yi, R l, R& oyr, R& oyi, R& ol) {
-    R ar, ai;
-    alpha(c, n, u, ar, ai);
-    const R dr = ar - yr, di = ai - yi;
-    const R h2 = (n & 1) ? c.hg2 : c.hb2;
-    const R inv = rcp(dr * dr + di * di);
-    const R hi = h2 * inv;
-    oyr = hi * dr;
-    oyi = -hi * di;
-    if (RA) ol = l * hi;
-}
-
-// Backward step at site n (> 0): X_{n-1} = h_{n-1}^2 / (alpha_n - X_n), rho_{n-1}.
-template <typename R, bool RA>
-__device__ __forceinline__ void bwd_step(const Chain<R>& c, int n, R u, R& xr, R& xi, R& rho) {
-    R ar, ai;
-    alpha(c, n, u, ar, ai);
-    const R er = ar - xr, ei = ai - xi;
-    const R h2 = ((n - 1) & 1) ? c.hg2 : c.hb2;
-    const R hi = h2 * rcp(er * er + ei * ei);
-    xr = hi * er;
-    xi = -hi * ei;
-    if (RA) rho = rho * hi;
-}
-
-// Contribution of site n: Im(c G_nn) [+ |G_nn|^2 (lambda k0 + rho k1)].
-template <typename R, bool RA>
-__device__ __forceinline__ double site_value(const Chain<R>& c, int n, R u, R yr, R yi, R l, R xr, R xi, R rho) {
-    R ar, ai;
-    alpha(c, n, u, ar, ai);
-    const R gr = ar - xr - yr, gi = ai - xi - yi;
-    const R ginv = rcp(gr * gr + gi * gi);  // |G_nn|^2
-    double v = c.cr * (double)(-gi * ginv) + c.ci * (double)(gr * ginv);
-    if (RA) v += (double)ginv * ((double)l * c.k0 + (double)rho * c.k1);
-    return c.valid ? v : 0.0;
-}
-
 template <typename R, bool RA>
 __device__ __forceinline__ Chain<R> make_chain(const TubeDev& T, const ChainRec& cr, double s0r, double s0i,
                                                double s1r, double s1i) {
@@ -330,21 +276,34 @@ __device__ __forceinline__ void proj_step_edge(const Chain<R>& c, Proj<R>& p, R 
 // Y = P / Q and lambda from a snapshot of the state; the running state is
 // rescaled by rq = 1 / |Q_b|^2 half a segment later.  With that scaling the
 // telescoped moduli give lambda_{b+K} = lambda_b prod(h^2) rq_b rq_{b+K}.
+// FP32 renormalises at the boundary itself (state := (Y, 1)): the deferred
+// scaling lets |Q| swing to |Q_b|^-2 between boundaries, which can leave the
+// FP32 range when |alpha - Y| is near its floor Im E.
 template <typename R, bool RA>
 __device__ __forceinline__ void proj_boundary(Proj<R>& p, R& yr, R& yi) {
     const R rq = rcp(p.qr * p.qr + p.qi * p.qi);
     yr = (p.pr * p.qr + p.pi * p.qi) * rq;
     yi = (p.pi * p.qr - p.pr * p.qi) * rq;
-    if (RA) p.lam = p.lam * (p.H * p.rq * rq);
-    p.rq = rq;
+    if constexpr (sizeof(R) == 4) {
+        if (RA) p.lam = p.lam * (p.H * rq);
+        p.pr = yr;
+        p.pi = yi;
+        p.qr = 1;
+        p.qi = 0;
+    } else {
+        if (RA) p.lam = p.lam * (p.H * p.rq * rq);
+        p.rq = rq;
+    }
     p.H = 1;
 }
 template <typename R>
 __device__ __forceinline__ void proj_scale(Proj<R>& p) {
-    p.pr *= p.rq;
-    p.pi *= p.rq;
-    p.qr *= p.rq;
-    p.qi *= p.rq;
+    if constexpr (sizeof(R) == 8) {
+        p.pr *= p.rq;
+        p.pi *= p.rq;
+        p.qr *= p.rq;
+        p.qi *= p.rq;
+    }
 }
 
 // One block of pass 1: checkpoint both sweeps at their segment boundaries,
@@ -500,39 +459,40 @@ __device__ __forceinline__ void pass1_chain(const TubeDev* __restrict__ tubes, c
 //   |G_nn|^2 rho_n    = rho_e prod_{n<=m<e} h_m^2 |Q_n|^2 / |D_n|^2,
 // with only short linear dependency chains.  D_n does not depend on n inside
 // a segment, so full segments take one reciprocal in all.
+template <typename R>
 struct CkVals {  // one lane's checkpoint of a segment
-    double yr, yi, lam, xr, xi, rho;
+    R yr, yi, lam, xr, xi, rho;
 };
-template <bool RA>
-__device__ __forceinline__ CkVals load_ck(const double* __restrict__ p) {
+template <typename R, bool RA>
+__device__ __forceinline__ CkVals<R> load_ck(const R* __restrict__ p) {
     using CL = CkLayout<RA>;
-    CkVals v;
+    CkVals<R> v;
     v.yr = p[CL::Y * kWarp];
     v.yi = p[(CL::Y + 1) * kWarp];
-    v.lam = RA ? p[CL::L * kWarp] : 1.0;
+    v.lam = RA ? p[CL::L * kWarp] : (R)1;
     v.xr = p[CL::X * kWarp];
     v.xi = p[(CL::X + 1) * kWarp];
-    v.rho = RA ? p[CL::RHO * kWarp] : 1.0;
+    v.rho = RA ? p[CL::RHO * kWarp] : (R)1;
     return v;
 }
 
-template <bool RA, bool EDGE>
-__device__ __forceinline__ void segment_proj(const Chain<double>& c, int n0, const CkVals& ckv,
-                                             const double (&u)[kSeg], double (&acc)[kSeg]) {
+template <typename R, bool RA, bool EDGE>
+__device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const CkVals<R>& ckv, const R (&u)[kSeg],
+                                             double (&acc)[kSeg]) {
     constexpr int K = kSeg;
     const int N = c.N;
-    double pr[K], pi[K], qr[K + 1], qi[K + 1], lm[K];
+    R pr[K], pi[K], qr[K + 1], qi[K + 1], lm[K];
     pr[0] = ckv.yr;
     pi[0] = ckv.yi;
-    qr[0] = 1.0;
-    qi[0] = 0.0;
+    qr[0] = 1;
+    qi[0] = 0;
     lm[0] = ckv.lam;
-    double Rr = ckv.xr, Ri = ckv.xi, Sr = 1.0, Si = 0.0;
-    double rh = ckv.rho;
+    R Rr = ckv.xr, Ri = ckv.xi, Sr = 1, Si = 0;
+    R rh = ckv.rho;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
         const int n = n0 + j;
-        double ar = c.Er - u[j], ai = c.Ei;
+        R ar = c.Er - u[j], ai = c.Ei;
         if (EDGE) {
             if (n >= N) break;
             if (n == 0) {
@@ -547,7 +507,7 @@ __device__ __forceinline__ void segment_proj(const Chain<double>& c, int n0, con
         qr[j + 1] = fma(ar, qr[j], fma(-ai, qi[j], -pr[j]));
         qi[j + 1] = fma(ar, qi[j], fma(ai, qr[j], -pi[j]));
         if (j + 1 < K) {
-            const double h2 = EDGE ? ((n & 1) ? c.hg2 : c.hb2) : ((j & 1) ? c.hg2 : c.hb2);
+            const R h2 = EDGE ? ((n & 1) ? c.hg2 : c.hb2) : ((j & 1) ? c.hg2 : c.hb2);
             pr[j + 1] = h2 * qr[j];
             pi[j + 1] = h2 * qi[j];
             if (RA) lm[j + 1] = lm[j] * h2;
@@ -558,19 +518,21 @@ __device__ __forceinline__ void segment_proj(const Chain<double>& c, int n0, con
     // Q_{n+1} = alpha_n Q_n - h_{n-1}^2 Q_{n-1}, D_{n-1} = D_n), so it is
     // formed once at the segment end, where S = 1 and R = X_e, and folded
     // into the per-segment coefficients.
-    double cgr = 0.0, cgi = 0.0;  // contour: c conj(D) / |D|^2
+    // D, |D|^2 and the folded coefficients in FP64 once per segment; the
+    // per-site products then run in the chain's precision
+    R cgr = 0, cgi = 0;  // contour: c conj(D) / |D|^2
     if (!EDGE) {
-        const double dr = fma(-Rr, qr[K - 1], fma(Ri, qi[K - 1], qr[K]));
-        const double di = fma(-Rr, qi[K - 1], fma(-Ri, qr[K - 1], qi[K]));
+        const double dr = fma(-(double)Rr, (double)qr[K - 1], fma((double)Ri, (double)qi[K - 1], (double)qr[K]));
+        const double di = fma(-(double)Rr, (double)qi[K - 1], fma(-(double)Ri, (double)qr[K - 1], (double)qi[K]));
         const double inv = rcp(fma(dr, dr, di * di));
         if (RA) {
-            const double a = c.k0 * inv, b = c.k1 * inv;
+            const R fa = (R)(c.k0 * inv), fb = (R)(c.k1 * inv);
 #pragma unroll
-            for (int j = 0; j < K; ++j) lm[j] *= a;
-            rh *= b;
+            for (int j = 0; j < K; ++j) lm[j] *= fa;
+            rh *= fb;
         } else {
-            cgr = fma(c.cr, dr, c.ci * di) * inv;
-            cgi = fma(c.ci, dr, -c.cr * di) * inv;
+            cgr = (R)(fma(c.cr, dr, c.ci * di) * inv);
+            cgi = (R)(fma(c.ci, dr, -c.cr * di) * inv);
         }
     }
 #pragma unroll
@@ -580,40 +542,42 @@ __device__ __forceinline__ void segment_proj(const Chain<double>& c, int n0, con
         if (EDGE && n >= N) continue;
         double v;
         if (!EDGE) {
-            if (RA) {  // |G|^2 (lambda k0 + rho k1) = (lm |S|^2 + rh |Q|^2) with 1/|D|^2 folded in
-                const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
-                v = fma(lm[j], s2, rh * q2);
+            if (RA) {  // |G|^2 (lambda k0 + rho k1) = lm |S|^2 + rh |Q|^2, 1/|D|^2 folded in
+                const R s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
+                v = (double)fma(lm[j], s2, rh * q2);
             } else {  // Im(c Q S / D)
-                const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
-                v = fma(cgr, ti, cgi * tr);
+                const R tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
+                v = (double)fma(cgr, ti, cgi * tr);
             }
         } else {
-            // D = S Q_{n+1} - R Q_n, per site (the segment may be partial)
-            const double dr = fma(Sr, qr[j + 1], fma(-Si, qi[j + 1], fma(-Rr, qr[j], Ri * qi[j])));
-            const double di = fma(Sr, qi[j + 1], fma(Si, qr[j + 1], fma(-Rr, qi[j], -Ri * qr[j])));
+            // D = S Q_{n+1} - R Q_n, per site (the segment may be partial), in FP64
+            const double Sd = Sr, Sid = Si, Rd = Rr, Rid = Ri;
+            const double q1r = qr[j + 1], q1i = qi[j + 1], q0r = qr[j], q0i = qi[j];
+            const double dr = fma(Sd, q1r, fma(-Sid, q1i, fma(-Rd, q0r, Rid * q0i)));
+            const double di = fma(Sd, q1i, fma(Sid, q1r, fma(-Rd, q0i, -Rid * q0r)));
             const double inv = rcp(fma(dr, dr, di * di));
             if (RA) {  // real-axis chains carry no contour coefficient (c = 0)
-                const double s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
-                v = inv * fma(lm[j] * s2, c.k0, rh * q2 * c.k1);
+                const double s2 = fma(Sd, Sd, Sid * Sid), q2 = fma(q0r, q0r, q0i * q0i);
+                v = inv * fma((double)lm[j] * s2, c.k0, (double)rh * q2 * c.k1);
             } else {  // Im(c T conj(D)) / |D|^2 with T = Q S
-                const double tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
+                const double tr = fma(q0r, Sd, -q0i * Sid), ti = fma(q0r, Sid, q0i * Sd);
                 const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
                 v = fma(c.cr, ui, c.ci * ur) * inv;
             }
         }
         acc[j] = c.valid ? v : 0.0;
         if (j > 0) {  // (R, S) at site n - 1
-            double ar = c.Er - u[j], ai = c.Ei;
+            R ar = c.Er - u[j], ai = c.Ei;
             if (EDGE) {
                 if (n == N - 1) {
                     ar -= c.s1r;
                     ai -= c.s1i;
                 }
             }
-            const double h2 = EDGE ? (((n - 1) & 1) ? c.hg2 : c.hb2) : (((j - 1) & 1) ? c.hg2 : c.hb2);
-            const double nrr = h2 * Sr, nri = h2 * Si;
-            const double nsr = fma(ar, Sr, fma(-ai, Si, -Rr));
-            const double nsi = fma(ar, Si, fma(ai, Sr, -Ri));
+            const R h2 = EDGE ? (((n - 1) & 1) ? c.hg2 : c.hb2) : (((j - 1) & 1) ? c.hg2 : c.hb2);
+            const R nrr = h2 * Sr, nri = h2 * Si;
+            const R nsr = fma(ar, Sr, fma(-ai, Si, -Rr));
+            const R nsi = fma(ar, Si, fma(ai, Sr, -Ri));
             Rr = nrr;
             Ri = nri;
             Sr = nsr;
@@ -646,67 +610,36 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
         const int first = su.seg0 * K, last = min(su.seg1 * K, N), off = lane * 16;
         if (off < last - first + 16) prefetch_l1(U + min(first + off, last - 1));
     }
-    if constexpr (sizeof(R) == 8) {
-        // the next segment's checkpoint is loaded while this one is computed,
-        // the one after next is brought into L1
-        CkVals cur = load_ck<RA>(ck + (size_t)su.seg0 * CL::NC * kWarp);
-        for (int s = su.seg0; s < su.seg1; ++s) {
-            const int n0 = s * K;
-            if (s + 2 < su.seg1) {
-                const R* q = ck + (size_t)(s + 2) * CL::NC * kWarp;
-#pragma unroll
-                for (int k = 0; k < CL::NC; ++k) prefetch_l1(q + k * kWarp);
-            }
-            CkVals nxt = cur;
-            if (s + 1 < su.seg1) nxt = load_ck<RA>(ck + (size_t)(s + 1) * CL::NC * kWarp);
-            double u[K], acc[K];
-            const bool interior = n0 > 0 && n0 + K < N;
-            if (interior) {
-                const double2* u2 = reinterpret_cast<const double2*>(U + n0);  // n0 even, U 16-byte aligned
-#pragma unroll
-                for (int k = 0; k < K / 2; ++k) {
-                    const double2 v = __ldg(u2 + k);
-                    u[2 * k] = v.x;
-                    u[2 * k + 1] = v.y;
-                }
-                segment_proj<RA, false>(c, n0, cur, u, acc);
-            } else {
-#pragma unroll
-                for (int k = 0; k < K; ++k) u[k] = (n0 + k < N) ? __ldg(U + n0 + k) : 0.0;
-                segment_proj<RA, true>(c, n0, cur, u, acc);
-            }
-            cur = nxt;
-            const double tot = warp_reduce_scatter<K>(acc, lane);
-            constexpr int shift = (K == 16) ? 1 : 2;
-            const int j = lane >> shift;
-            if ((lane & ((1 << shift) - 1)) == 0 && n0 + j < N) prow[n0 + j] = tot;
-        }
-        return;
-    }
+    // the next segment's checkpoint is loaded while this one is computed,
+    // the one after next is brought into L1
+    CkVals<R> cur = load_ck<R, RA>(ck + (size_t)su.seg0 * CL::NC * kWarp);
     for (int s = su.seg0; s < su.seg1; ++s) {
         const int n0 = s * K;
-        const R* p = ck + (size_t)s * CL::NC * kWarp;
-        R yr[K], yi[K], l[K], u[K];
-        yr[0] = p[CL::Y * kWarp];
-        yi[0] = p[(CL::Y + 1) * kWarp];
-        l[0] = RA ? p[CL::L * kWarp] : (R)1;
-        R xr = p[CL::X * kWarp], xi = p[(CL::X + 1) * kWarp];
-        R rho = RA ? p[CL::RHO * kWarp] : (R)1;
+        if (s + 2 < su.seg1) {
+            const R* q = ck + (size_t)(s + 2) * CL::NC * kWarp;
 #pragma unroll
-        for (int k = 0; k < K; ++k) u[k] = (n0 + k < N) ? (R)__ldg(U + n0 + k) : (R)0;
-#pragma unroll
-        for (int k = 0; k < K - 1; ++k)
-            if (n0 + k < N - 1) fwd_step<R, RA>(c, n0 + k, u[k], yr[k], yi[k], l[k], yr[k + 1], yi[k + 1], l[k + 1]);
-        double acc[K];
-#pragma unroll
-        for (int k = K - 1; k >= 0; --k) {
-            const int n = n0 + k;
-            acc[k] = 0.0;
-            if (n < N) {
-                acc[k] = site_value<R, RA>(c, n, u[k], yr[k], yi[k], l[k], xr, xi, rho);
-                if (k > 0) bwd_step<R, RA>(c, n, u[k], xr, xi, rho);
-            }
+            for (int k = 0; k < CL::NC; ++k) prefetch_l1(q + k * kWarp);
         }
+        CkVals<R> nxt = cur;
+        if (s + 1 < su.seg1) nxt = load_ck<R, RA>(ck + (size_t)(s + 1) * CL::NC * kWarp);
+        R u[K];
+        double acc[K];
+        const bool interior = n0 > 0 && n0 + K < N;
+        if (interior) {
+            const double2* u2 = reinterpret_cast<const double2*>(U + n0);  // n0 even, U 16-byte aligned
+#pragma unroll
+            for (int k = 0; k < K / 2; ++k) {
+                const double2 v = __ldg(u2 + k);
+                u[2 * k] = (R)v.x;
+                u[2 * k + 1] = (R)v.y;
+            }
+            segment_proj<R, RA, false>(c, n0, cur, u, acc);
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; ++k) u[k] = (n0 + k < N) ? (R)__ldg(U + n0 + k) : (R)0;
+            segment_proj<R, RA, true>(c, n0, cur, u, acc);
+        }
+        cur = nxt;
         const double tot = warp_reduce_scatter<K>(acc, lane);
         constexpr int shift = (K == 16) ? 1 : 2;
         const int j = lane >> shift;
@@ -831,7 +764,7 @@ __global__ void __launch_bounds__(32 * kRowGroups) reduce_kernel(const ReduceTub
 // a_n = deg Gamma_0 |G_n0|^2 and b_n = deg Gamma_1 |G_n,N-1|^2 for chains
 // whose real-axis coefficients are b0 = b1 = 1, so that deg A_nn = a_n + b_n
 // (A = sum_k G Gamma_k G^dagger, NEGF_Common.cpp:2654-2726).
-__device__ __forceinline__ void segment_spectral(const Chain<double>& c, int n0, const CkVals& ckv,
+__device__ __forceinline__ void segment_spectral(const Chain<double>& c, int n0, const CkVals<double>& ckv,
                                                  const double (&u)[kSeg], double (&a)[kSeg], double (&b)[kSeg]) {
     constexpr int K = kSeg;
     const int N = c.N;
@@ -932,7 +865,7 @@ __global__ void __launch_bounds__(32) rgf_transport_kernel(const TubeDev* __rest
     double sum = 0.0;
     for (int s = su.seg0; s < su.seg1; ++s) {
         const int n0 = s * K;
-        const CkVals ckv = load_ck<true>(ck + (size_t)s * CL::NC * kWarp);
+        const CkVals<double> ckv = load_ck<double, true>(ck + (size_t)s * CL::NC * kWarp);
         double u[K], a[K], b[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) u[k] = (n0 + k < N) ? __ldg(U + n0 + k) : 0.0;

@@ -361,6 +361,12 @@ class Broyden:
 
     Execute_Broyden_Modified_Second_Algorithm_Parallel = step
 
+    def step_device_switch(self, n_out_dev, max_norm, switch_norm, flags_dev, stream=None):
+        """Device-resident step with precision switching (flags_dev int32[8])."""
+        check(_lib.load().negf_broyden_step_device_switch(self._h, _ptr(n_out_dev), float(max_norm), float(switch_norm),
+                                                          _ptr(flags_dev), _stream(stream)),
+              "negf_broyden_step_device_switch")
+
     def step_device(self, n_out_dev, max_norm, flags_dev, stream=None):
         """Device-resident step (capturable): flags_dev int32[4] on the device
         = converged, steps taken, error, skip."""
@@ -442,14 +448,14 @@ class ChargePlan:
     kernel launches only (capturable in a CUDA graph); the contact potentials
     follow the end sites of each tube's potential buffer."""
 
-    def __init__(self, tubes: Sequence[CNT], out, autotune=False):
+    def __init__(self, tubes: Sequence[CNT], out, autotune=False, fp64=False):
         L = _lib.load()
         self.tubes = list(tubes)
         self.out = out
         arr = (C.c_void_p * len(tubes))(*[t.handle for t in tubes])
         h = C.c_void_p()
-        check(L.negf_charge_plan_create(arr, len(tubes), _ptr(out), _lib.NEGF_PLAN_AUTOTUNE if autotune else 0,
-                                        C.byref(h)), "negf_charge_plan_create")
+        flags = (_lib.NEGF_PLAN_AUTOTUNE if autotune else 0) | (_lib.NEGF_PLAN_FP64 if fp64 else 0)
+        check(L.negf_charge_plan_create(arr, len(tubes), _ptr(out), flags, C.byref(h)), "negf_charge_plan_create")
         self._h = h
 
     def launch(self, skip=None, stream=None):

@@ -113,7 +113,10 @@ def run_scf(tube, electro, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, n
 
 def run_scf_oracle(oracle_tube, K, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
                    initial_charge=0.0, reset_with_previous_charge=False, nthreads=8):
-    """The same loop on the CPU oracle (test infrastructure and CPU baseline)."""
+    """The same loop on the CPU oracle (test infrastructure and CPU baseline).
+    K: the coupling matrix (U = -Vg - K Q) or an electrostatics object with
+    potential(Q, Vg)."""
+    pot = K.potential if hasattr(K, "potential") else (lambda q, vg: -float(vg) - K @ q)
     from oracle import oracle as O
 
     N = oracle_tube.N
@@ -124,7 +127,7 @@ def run_scf_oracle(oracle_tube, K, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
         t0 = time.perf_counter()
         it, nrm = 0, float("inf")
         while True:
-            U = -float(Vg) - K @ n_in
+            U = pot(n_in, Vg)
             oracle_tube.set_potential(U, (U[0], U[-1]))
             Q = oracle_tube.charge(nthreads=nthreads)
             nrm, n_in, _ = br.step(Q)
@@ -140,7 +143,7 @@ def run_scf_oracle(oracle_tube, K, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
 
 def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
                   initial_charge=0.0, reset_with_previous_charge=False, use_graph=True, iters_per_graph=8,
-                  autotune=True):
+                  autotune=True, switch_norm=None):
     """Self-consistent bias sweep of a batch of tubes with one Broyden over
     all their sites (the all-tubes n_in of Broyden_Parallel_General.cpp:42-66).
 
@@ -148,8 +151,11 @@ def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
     operator), one charge-plan launch for the whole batch, one device-resident
     Broyden step.  With use_graph, iters_per_graph iterations are captured in
     one CUDA graph and replayed until the device flags say converged (or
-    failed); the host reads the 4 flag ints once per replay.  Returns an
-    SCFResult plus the plan's schedule."""
+    failed); the host reads the flag ints once per replay.  With switch_norm
+    (mixed-precision tubes), the iterations run on the tubes' own plan until
+    the residual falls below switch_norm and on an FP64 plan from then on;
+    only an FP64 charge ends a solve.  Returns an SCFResult plus the plan's
+    schedule."""
     import torch
     from .negf import Broyden, ChargePlan, affine_potential_masked
 
@@ -169,18 +175,25 @@ def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
             Kd, U0 = e.device_operator(0.0)
             ops.append((Kd, U0.clone()))
         U_ptrs = [t.potential_device_ptr() for t in tubes]
-        flags = torch.zeros(4, dtype=torch.int32, device=dev)
+        flags = torch.zeros(8, dtype=torch.int32, device=dev)
         skip = flags.data_ptr() + 3 * 4
+        switch = switch_norm is not None and switch_norm > 0
         # the initial potential (paths do not depend on it; contact potentials are read on the device)
         for (Kd, U0), t, o, N, Up in zip(ops, tubes, offs, Ns, U_ptrs):
             affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, None, stream=stream)
         plan = ChargePlan(tubes, Q, autotune=autotune)
+        plan64 = ChargePlan(tubes, Q, autotune=autotune, fp64=True) if switch else None
 
         def body(s):
             for (Kd, U0), o, N, Up in zip(ops, offs, Ns, U_ptrs):
                 affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip, stream=s)
-            plan.launch(skip=skip, stream=s)
-            br.step_device(Q, max_norm, flags, stream=s)
+            if switch:
+                plan.launch(skip=flags.data_ptr() + 5 * 4, stream=s)
+                plan64.launch(skip=flags.data_ptr() + 6 * 4, stream=s)
+                br.step_device_switch(Q, max_norm, switch_norm, flags, stream=s)
+            else:
+                plan.launch(skip=skip, stream=s)
+                br.step_device(Q, max_norm, flags, stream=s)
 
         graph = None
         if use_graph:
@@ -195,6 +208,8 @@ def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
             for (Kd, U0), e in zip(ops, electros):
                 U0.copy_(e.device_operator(Vg)[1])
             flags.zero_()
+            if switch:
+                flags[6] = 1  # the FP64 plan waits for the switch
             stream.synchronize()
             t0 = time.perf_counter()
             while True:
@@ -211,12 +226,16 @@ def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
             if f[2] == 2:
                 raise RuntimeError("non-finite Broyden norm")
             U = np.concatenate([device_view(Up, N).cpu().numpy() for Up, N in zip(U_ptrs, Ns)])
-            res.steps.append(StepResult(Vg, int(f[1]), float("nan"), Q.cpu().numpy().copy(), U, dt))
+            st = StepResult(Vg, int(f[1]), float("nan"), Q.cpu().numpy().copy(), U, dt)
+            st.lowprec_iterations = int(f[7])
+            res.steps.append(st)
             br.reset(keep_charge=reset_with_previous_charge, init_value=initial_charge, stream=stream)
         stream.synchronize()
     info = plan.info()
     del graph
     plan.close()
+    if plan64 is not None:
+        plan64.close()
     br.close()
     res.schedule = info
     return res
@@ -224,7 +243,8 @@ def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_ste
 
 def run_scf_batch_oracle(oracle_tubes, Ks, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200,
                          norm_type="absolute", initial_charge=0.0, nthreads=8):
-    """The batched loop on the CPU oracle: one Broyden over all tubes' sites."""
+    """The batched loop on the CPU oracle: one Broyden over all tubes' sites.
+    Ks: per tube a coupling matrix or an electrostatics object."""
     from oracle import oracle as O
 
     Ns = [t.N for t in oracle_tubes]
@@ -239,7 +259,7 @@ def run_scf_batch_oracle(oracle_tubes, Ks, Vg_list, fraction=0.1, max_norm=1e-6,
         while True:
             Q = np.zeros(S)
             for t, K, a, b in zip(oracle_tubes, Ks, offs[:-1], offs[1:]):
-                U = -float(Vg) - K @ n_in[a:b]
+                U = K.potential(n_in[a:b], Vg) if hasattr(K, "potential") else -float(Vg) - K @ n_in[a:b]
                 t.set_potential(U, (U[0], U[-1]))
                 Q[a:b] = t.charge(nthreads=nthreads)
             nrm, n_in, _ = br.step(Q)

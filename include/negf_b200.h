@@ -73,7 +73,8 @@ typedef struct negf_tube_desc {
     double realaxis_min, realaxis_max;
     int realaxis_pts, realaxis_kind;
     int precision;                 /* NEGF_PREC_FP64 or NEGF_PREC_MIXED */
-    double mixed_fp64_band;        /* mixed mode: points with Im E below this [eV] stay FP64 (1e-3) */
+    double mixed_fp64_band;        /* mixed mode: contour points with Im E below this [eV] and every
+                                      real-axis point stay FP64 (1e-3) */
     int flatband_dos_integration_pts; /* DOS path points at zero bias (NEGF_Common.H:416, 100) */
     /* Adaptive non-equilibrium limits (Read_AdaptiveIntegrationParams,
      * NEGF_Common.cpp:524-543; NEGF_Common.H:453-457). */
@@ -260,6 +261,7 @@ int negf_write_integrand(negf_tube* t, const char* path, int count, const double
  * launch) once a tube's energy paths change (contact mu, adaptive limits);
  * d_skip (device int or null) skips the launch at kernel entry when set. */
 #define NEGF_PLAN_AUTOTUNE 1
+#define NEGF_PLAN_FP64 2     /* every chain in FP64 whatever the tubes' precision mode */
 typedef struct negf_charge_plan negf_charge_plan;
 int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q, int flags, negf_charge_plan** plan);
 int negf_charge_plan_launch(negf_charge_plan* plan, const int* d_skip, void* stream);
@@ -297,6 +299,15 @@ int negf_broyden_step_number(negf_broyden* b, int* step);
  * launch given d_flags + 3 returns at kernel entry, so a captured sequence
  * of iterations stops itself.  The iteration index is read on the device. */
 int negf_broyden_step_device(negf_broyden* b, const double* d_n_out, double max_norm, int* d_flags, void* stream);
+/* Precision switching (no counterpart in the reference): d_flags int[8],
+ * initialised by the caller to {0,0,0,0, 0,0,1,0}.  Until the first norm
+ * below switch_norm the charge is taken to come from a low-precision plan
+ * (launched with skip word d_flags + 5); from then on from an FP64 plan
+ * (skip word d_flags + 6), and only an FP64 charge can satisfy max_norm.
+ * [4] is set at the switch; [7] counts the steps taken on low-precision
+ * charges. */
+int negf_broyden_step_device_switch(negf_broyden* b, const double* d_n_out, double max_norm, double switch_norm,
+                                    int* d_flags, void* stream);
 /* Device pointer of the current input charge n_in. */
 int negf_broyden_input_device_ptr(negf_broyden* b, double** d_n_in);
 

@@ -102,6 +102,23 @@ def test_mixed_precision_error_bound(oracle):
     assert _rel(Qg, Qo) <= MIXED_TOL, _rel(Qg, Qo)
 
 
+@pytest.mark.parametrize("cells", [25, 400])
+def test_mixed_precision_broadened_real_axis(oracle, cells):
+    """Broadened real axis (eta = 2 meV): the contour points run in FP32, the
+    real-axis chains (running products over the whole tube) stay FP64."""
+    kw = dict(type_id=(17, 0), num_unitcells=cells, num_modes=3, contact_mu=(0.0, -0.4), contact_T=(300.0, 300.0),
+              eq_integration_pts=(24, 24, 40), noneq_integration_pts=(40, 60, 40),
+              noneq_percent_intercuts=(30.0, 70.0), E_zPlus_imag=2e-3, precision="mixed")
+    g, o = _pair(oracle, seed=13, **kw)
+    Qg = g.Solve_NEGF()
+    from electrostatic_b200.negf import last_stats
+    st = last_stats()
+    assert st["updates_fp32"] == st["contour_updates"] > 0
+    Qo = o.charge(nthreads=8)
+    assert np.all(np.isfinite(Qg))
+    assert _rel(Qg, Qo) <= MIXED_TOL, _rel(Qg, Qo)
+
+
 def test_batch_of_uneven_tubes(oracle):
     from electrostatic_b200.negf import compute_charge
     specs = [

@@ -66,3 +66,21 @@ def test_device_scf_follows_oracle_scf(oracle, keep):
         assert sg.iterations == so.iterations, (sg.iterations, so.iterations)
         np.testing.assert_allclose(sg.Q, so.Q, rtol=0, atol=1e-9)
         np.testing.assert_allclose(sg.U, so.U, rtol=0, atol=1e-9)
+
+
+def test_step_response_properties():
+    """Wall-potential step inside the gate cylinder: s(0) = 1/2, s(dz) + s(-dz) = 1,
+    monotonic, bare step far away, and a contacted stand-in pins the tube ends."""
+    from electrostatic_b200.electrostatics import step_response
+    a, r = 2.17e-9, 0.67e-9
+    dz = np.linspace(-40e-9, 40e-9, 801)
+    s = step_response(dz, r, a)
+    assert abs(s[400] - 0.5) < 1e-12
+    assert np.max(np.abs(s + s[::-1] - 1.0)) < 1e-12
+    assert np.all(np.diff(s) >= -1e-12)
+    assert s[0] < 1e-12 and s[-1] > 1 - 1e-12
+    from electrostatic_b200.workloads import gate_with_contacts
+    y = np.linspace(0, 60, 600)
+    g = gate_with_contacts(y, r, vds=0.4)
+    U = g.external(0.3)
+    assert abs(U[0]) < 1e-3 and abs(U[-1] + 0.4) < 1e-3 and abs(U[300] + 0.3) < 1e-6

@@ -97,3 +97,34 @@ def test_batch_scf_graph_equals_loop_and_oracle(oracle):
     for a, b in zip(r_graph.steps, r_o.steps):
         assert a.iterations == b.iterations
         assert np.max(np.abs(a.Q - b.Q)) <= 1e-8 * np.max(np.abs(b.Q))
+
+
+def test_broyden_non_finite_residual_is_an_error():
+    """A NaN in the NEGF output is never read as convergence."""
+    import torch
+    from electrostatic_b200._lib import NEGFError
+    from electrostatic_b200.negf import Broyden
+    S = 100
+    x = torch.zeros(S, dtype=torch.float64, device="cuda")
+    x[17] = float("nan")
+    h = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"))
+    with pytest.raises(NEGFError, match="non-finite"):
+        h.step(x)
+    d = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"))
+    flags = torch.zeros(4, dtype=torch.int32, device="cuda")
+    d.step_device(x, 1e-6, flags)
+    assert flags.cpu().tolist() == [0, 1, 2, 1]
+
+
+def test_batch_scf_precision_switch_matches_fp64(oracle):
+    """Mixed-precision tubes with the FP64 finish: the converged charge is an
+    FP64 fixed point (same tolerance as the plain FP64 loop)."""
+    from electrostatic_b200.scf import run_scf_batch
+    Vg = [0.1]
+    tubes, electros, _ = _batch(precision="mixed")
+    r_sw = run_scf_batch(tubes, electros, Vg, use_graph=True, iters_per_graph=4, switch_norm=1e-4)
+    tubes2, electros2, _ = _batch()
+    r_64 = run_scf_batch(tubes2, electros2, Vg, use_graph=True, iters_per_graph=4)
+    a, b = r_sw.steps[0], r_64.steps[0]
+    assert 0 < a.lowprec_iterations < a.iterations
+    assert np.max(np.abs(a.Q - b.Q)) < 1e-5
