@@ -281,6 +281,42 @@ def config4_measure(torch, passes=5):
     return out
 
 
+def config3_measure(torch, passes=2):
+    """Real-space ring blocks: (13,0), 600 blocks of 26 atoms, 2048 contour
+    energies + poles, FP64; against the mode-space pass of the same tube with
+    all 7 modes (equal for this ring-uniform potential)."""
+    from electrostatic_b200.negf import CNT, last_stats, set_timing
+    from electrostatic_b200.workloads import SEED_BASE, site_potential
+    kw = dict(type_id=(13, 0), num_unitcells=300, num_modes=7, contact_mu=(-0.8, -0.8), contact_T=(300.0, 300.0),
+              eq_integration_pts=(512, 512, 1024), E_pole_max=3.0, E_zPlus_imag=1e-6)
+    t = CNT(**kw)
+    U = site_potential(t.site_positions(), SEED_BASE + 3)
+    t.set_potential(U, (U[0], U[-1]))
+    Q = torch.zeros(t.num_field_sites, dtype=torch.float64, device="cuda")
+    t.realspace_charge(out=Q)  # warm-up (buffers, lazy loading)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(passes):
+        t.realspace_charge(out=Q)
+    torch.cuda.synchronize()
+    sec = (time.perf_counter() - t0) / passes
+    Qm = t.Solve_NEGF()
+    E = len(t.energy_points(1)[0]) + len(t.energy_points(2)[0])
+    E0 = len(t.energy_points(0)[0])
+    K, n = t.num_field_sites // 2, 26
+    # dense convention: complex GEMM 8n^3, inverse 8n^3; 56 n^3 per block update,
+    # 32 lead iterations x 88 n^3 per contact per energy
+    flops = (E + E0) * (K * 56 * n ** 3 + 2 * 32 * 88 * n ** 3)
+    Qr = Q.cpu().numpy()
+    return {"workload": "(13,0) CNT, 600 blocks of 2 rings (26 atoms), %d contour+pole energies (+%d Rho0), "
+                        "Sancho-Rubio leads (32 iterations), FP64, seeded config-2 ring potential" % (E, E0),
+            "seconds_per_pass": sec, "block_updates_per_s": (E + E0) * K / sec,
+            "achieved_tflops": flops / sec / 1e12, "flops_per_pass": flops,
+            "flop_convention": "dense complex: GEMM 8n^3, inverse 8n^3; 56n^3 per block update, 88n^3 per lead iteration",
+            "path": "negf_rs_compute_charge (FP64 CUDA cores, one warp per energy)",
+            "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm)))}
+
+
 def ring_positions_nm(unitcells, acc=1.42e-10):
     """Axial ring positions [nm] of a zigzag tube (CNT.cpp:93-132)."""
     y0 = -(unitcells / 2.0) * 3.0 * acc - acc / 2.0
@@ -299,6 +335,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-scf", action="store_true")
     ap.add_argument("--no-config4", action="store_true")
+    ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis)")
     args = ap.parse_args()
@@ -434,6 +471,7 @@ def main():
                              f"{threads} threads over energies; {dt:.2f} s"}
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
+        cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch)
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                 "frac": achieved_tf / peak_tf if peak_tf else None,
                 "traffic": prof.get("dram_bytes_per_launch"),
@@ -451,7 +489,7 @@ def main():
                 "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
                            "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config4": cfg4,
+                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config3": cfg3, "config4": cfg4,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
                         "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},

@@ -35,7 +35,7 @@ EXPORTED = [
     "negf_write_integrand", "negf_tube_correct_integration_limits", "negf_tube_noneq_integrand",
     "negf_tube_noneq_layout", "negf_read_table1d", "negf_broyden_step_device", "negf_affine_potential_masked",
     "negf_charge_plan_create", "negf_charge_plan_launch", "negf_charge_plan_info", "negf_charge_plan_destroy",
-    "negf_broyden_step_device_switch",
+    "negf_broyden_step_device_switch", "negf_rs_compute_charge",
 ]
 
 
@@ -156,6 +156,7 @@ def load():
         "negf_read_table1d": [C.c_char_p, C.c_int, dp],
         "negf_broyden_step_device": [vp, vp, C.c_double, vp, vp],
         "negf_broyden_step_device_switch": [vp, vp, C.c_double, C.c_double, vp, vp],
+        "negf_rs_compute_charge": [vp, vp, vp, vp],
         "negf_affine_potential_masked": [vp, vp, vp, vp, C.c_int, vp, vp],
         "negf_charge_plan_create": [C.POINTER(vp), C.c_int, vp, C.c_int, C.POINTER(vp)],
         "negf_charge_plan_launch": [vp, vp, vp],

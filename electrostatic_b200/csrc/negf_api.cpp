@@ -1530,6 +1530,82 @@ int negf_affine_potential_masked(const double* K, const double* U0, const double
     return NEGF_OK;
 }
 
+// ------------------------------------------------------------------ real-space ring blocks
+int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, void* stream) {
+    if (!t || !d_Q) return fail(NEGF_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_mu);
+    update_paths(*t);
+    const int m = t->d.type_id[0];
+    if (t->d.type_id[1] != 0) return fail(NEGF_ERR_ARG, "real-space blocks are built for zigzag (m,0) tubes");
+    if (2 * m > negf::rs_max_atoms_per_block())
+        return fail(NEGF_ERR_ARG, "real-space blocks hold at most " + std::to_string(negf::rs_max_atoms_per_block()) +
+                                      " atoms (m <= 16)");
+    if (t->noneq) return fail(NEGF_ERR_STATE, "the real-space pass covers the equilibrium charge (contour and poles)");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int N = t->N, K = N / 2;
+    // energies: RhoEq contour and poles (coefficients as in the mode-space pass), then Rho0 at U = 0
+    std::vector<double> Er, Ei, cr, ci;
+    const int neq = pass_items(*t, false);
+    for (int idx = 0; idx < neq; ++idx) {
+        const Item it = pass_item(*t, false, idx);
+        Er.push_back(it.E.real());
+        Ei.push_back(it.E.imag());
+        cr.push_back(it.c.real());
+        ci.push_back(it.c.imag());
+    }
+    rho0_paths(*t);
+    const int n0 = pass_items(*t, true);
+    for (int idx = 0; idx < n0; ++idx) {
+        const Item it = pass_item(*t, true, idx);
+        Er.push_back(it.E.real());
+        Ei.push_back(it.E.imag());
+        cr.push_back(it.c.real());
+        ci.push_back(it.c.imag());
+    }
+    const int P = (int)Er.size();
+    const size_t mm = (size_t)m * m;
+    // grow-only buffers kept across calls (serialised by g_mu)
+    static DevBuf bE, bU0, bUa, bCorners, bGL, bRows, bStatus;
+    NEGF_CUDA(bE.reserve(sizeof(double) * 4 * P));
+    NEGF_CUDA(bUa.reserve(sizeof(double) * (size_t)N * m));
+    NEGF_CUDA(bU0.reserve(sizeof(double) * (size_t)N * m));
+    NEGF_CUDA(bCorners.reserve(16 * 2 * mm * P));
+    // both launches (neq contour/pole energies, n0 Rho0 energies) share these buffers
+    const size_t maxe = (size_t)std::max(std::max(neq, n0), 1);
+    NEGF_CUDA(bGL.reserve(16 * mm * K * maxe));
+    NEGF_CUDA(bRows.reserve(sizeof(double) * (size_t)N * maxe));
+    NEGF_CUDA(bStatus.reserve(sizeof(int)));
+    std::vector<double> host(4 * (size_t)P);
+    std::copy(Er.begin(), Er.end(), host.begin());
+    std::copy(Ei.begin(), Ei.end(), host.begin() + P);
+    std::copy(cr.begin(), cr.end(), host.begin() + 2 * P);
+    std::copy(ci.begin(), ci.end(), host.begin() + 3 * P);
+    double* dE = bE.as<double>();
+    NEGF_CUDA(cudaMemcpyAsync(dE, host.data(), sizeof(double) * 4 * P, cudaMemcpyHostToDevice, s));
+    NEGF_CUDA(cudaMemsetAsync(bStatus.p, 0, sizeof(int), s));
+    NEGF_CUDA(cudaMemsetAsync(bU0.p, 0, sizeof(double) * (size_t)N * m, s));
+    const double* Ua = d_Uatoms;
+    if (!Ua) {
+        NEGF_CUDA(negf::rs_expand(t->d_U, N, m, bUa.as<double>(), s));
+        Ua = bUa.as<double>();
+    }
+    const int iters = t->d.decimation_max_iter + 2;
+    if (neq > 0)
+        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, neq, Ua, t->Uc[0],
+                                         t->Uc[1], iters, bCorners.p, bGL.p, bRows.as<double>(), d_Q, 1.0, 0,
+                                         bStatus.as<int>(), s));
+    else
+        NEGF_CUDA(cudaMemsetAsync(d_Q, 0, sizeof(double) * N, s));
+    NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE + neq, dE + P + neq, dE + 2 * P + neq, dE + 3 * P + neq, n0,
+                                     bU0.as<double>(), 0.0, 0.0, iters, bCorners.p, bGL.p, bRows.as<double>(), d_Q,
+                                     -1.0, 1, bStatus.as<int>(), s));
+    int status = 0;
+    NEGF_CUDA(cudaMemcpyAsync(&status, bStatus.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    NEGF_CUDA(cudaStreamSynchronize(s));
+    if (status) return fail(NEGF_ERR_NUMERIC, "zero pivot in a real-space block inversion");
+    return NEGF_OK;
+}
+
 // ------------------------------------------------------------------ transport characteristics
 int negf_tube_dos_points(negf_tube* t, int* count) {
     if (!t || !count) return fail(NEGF_ERR_ARG, "null argument");

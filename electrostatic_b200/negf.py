@@ -235,6 +235,16 @@ class CNT:
     def Compute_InducedCharge(self, out=None, stream=None):
         return compute_charge([self], out=out, stream=stream)
 
+    def realspace_charge(self, out=None, U_atoms=None, stream=None):
+        """Equilibrium charge per ring from the real-space ring-block RGF
+        (zigzag tubes).  U_atoms: optional device tensor [N][m] of per-atom
+        potentials.  Returns numpy unless `out` (device float64) is given."""
+        import torch
+        Q = out if out is not None else torch.zeros(self.num_field_sites, dtype=torch.float64, device="cuda")
+        check(_lib.load().negf_rs_compute_charge(self._h, _ptr(U_atoms), _ptr(Q), _stream(stream)),
+              "negf_rs_compute_charge")
+        return Q if out is not None else Q.cpu().numpy()
+
     # --- transport characteristics (PostProcess, Nanostructure.H:134-138)
     def Compute_DensityOfStates(self, ldos=False, stream=None) -> dict:
         """Compute_DensityOfStates (NEGF_Common.cpp:2390-2847) on the GPU: dict

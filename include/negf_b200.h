@@ -189,6 +189,19 @@ int negf_set_tuning(int key, int value);
 /* Enable CUDA-event timing of negf_compute_charge (off by default). */
 int negf_set_timing(int enable);
 
+/* Real-space ring-block RGF (config shape "(13,0) with 26-atom ring
+ * blocks"; the reference engine is mode space only, so this entry point has
+ * no counterpart there).  Zigzag (m,0) tubes, m <= 16: blocks of two rings
+ * (2m atoms) with the double bond inside a block and the single bond
+ * between blocks, dense 2m x 2m complex FP64 blocks, leads by the Lopez
+ * Sancho-Sancho-Rubio decimation (decimation_max_iter + 2 iterations).
+ * Equilibrium charge per ring into d_Q (device, N doubles): the tube's
+ * contour and pole points with the mode-space coefficients, minus Rho0 at
+ * U = 0.  d_Uatoms (device, [N][m]) gives per-atom potentials; null uses the
+ * tube's ring potential on every atom, in which case the result equals the
+ * mode-space charge with all m//2 + 1 distinct modes.  Synchronous. */
+int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, void* stream);
+
 /* Transport characteristics (c_NEGF_Common::Compute_DensityOfStates,
  * NEGF_Common.cpp:2390-2847, and Compute_Current, :4321-4816; called from
  * c_Nanostructure::PostProcess, Nanostructure.H:134-138).

@@ -725,6 +725,162 @@ void find_intercuts(Tube& t) {
     }
 }
 
+// ---------------------------------------------------------------- real-space ring blocks
+// A zigzag (m,0) tube in real space: blocks of two rings (2m atoms); ring 2k
+// and 2k+1 joined by the double bond (atom j to atoms j and j+1 mod m),
+// ring 2k+1 to ring 2k+2 by the single bond (atom j to atom j); hopping
+// gamma; on-site energy U per atom.  In mode space (Fourier over the ring)
+// the double bond becomes 2 gamma cos(pi J / m) = beta_J and the single bond
+// gamma (CNT.cpp:288-336), so with ring-uniform potentials the block RGF
+// equals the sum over all m mode chains.  Leads: semi-infinite repetitions
+// of one block at the contact potential, surface Green's functions by the
+// Lopez Sancho-Sancho-Rubio decimation (J. Phys. F 15, 851 (1985)).
+using CMat = std::vector<cplx>;  // row-major n x n
+
+// Gauss-Jordan inverse with partial pivoting (returns false when singular).
+bool cinvert(CMat& A, int n) {
+    CMat I(n * n, 0.0);
+    for (int i = 0; i < n; ++i) I[i * n + i] = 1.0;
+    for (int p = 0; p < n; ++p) {
+        int piv = p;
+        double best = std::abs(A[p * n + p]);
+        for (int r = p + 1; r < n; ++r)
+            if (std::abs(A[r * n + p]) > best) {
+                best = std::abs(A[r * n + p]);
+                piv = r;
+            }
+        if (!(best > 0)) return false;
+        if (piv != p)
+            for (int c = 0; c < n; ++c) {
+                std::swap(A[p * n + c], A[piv * n + c]);
+                std::swap(I[p * n + c], I[piv * n + c]);
+            }
+        const cplx inv = cinv(A[p * n + p]);
+        for (int c = 0; c < n; ++c) {
+            A[p * n + c] = cmul(A[p * n + c], inv);
+            I[p * n + c] = cmul(I[p * n + c], inv);
+        }
+        for (int r = 0; r < n; ++r) {
+            if (r == p) continue;
+            const cplx f = A[r * n + p];
+            if (f == cplx(0.0, 0.0)) continue;
+            for (int c = 0; c < n; ++c) {
+                A[r * n + c] -= cmul(f, A[p * n + c]);
+                I[r * n + c] -= cmul(f, I[p * n + c]);
+            }
+        }
+    }
+    A.swap(I);
+    return true;
+}
+CMat cgemm(const CMat& A, const CMat& B, int n) {
+    CMat C(n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < n; ++k) {
+            const cplx a = A[i * n + k];
+            if (a == cplx(0.0, 0.0)) continue;
+            for (int j = 0; j < n; ++j) C[i * n + j] += cmul(a, B[k * n + j]);
+        }
+    return C;
+}
+
+// E - H of one block (2m atoms) with on-site potentials U[2m].
+CMat rs_block(int m, double gamma, cplx E, const double* U) {
+    const int n = 2 * m;
+    CMat A(n * n, 0.0);
+    for (int i = 0; i < n; ++i) A[i * n + i] = E - U[i];
+    for (int j = 0; j < m; ++j) {
+        const int a = j, b1 = m + j, b2 = m + (j + 1) % m;
+        A[a * n + b1] -= gamma;
+        A[b1 * n + a] -= gamma;
+        A[a * n + b2] -= gamma;
+        A[b2 * n + a] -= gamma;
+    }
+    return A;
+}
+
+// Surface Green's function of a semi-infinite lead of blocks at potential
+// Uc.  left = true: the lead extends to the left and its surface block couples
+// to the device through ring b (single bond to the device's ring a); the
+// returned m x m corner is g[b][b].  left = false: lead to the right, corner
+// g[a][a].  Decimation: eps_s += a g b, eps += a g b + b g a, a = a g a,
+// b = b g b, with g = (E - eps)^-1, for `iters` iterations.
+CMat rs_lead_corner(int m, double gamma, cplx E, double Uc, bool left, int iters) {
+    const int n = 2 * m;
+    std::vector<double> U(n, Uc);
+    CMat eps = rs_block(m, gamma, E, U.data());  // holds E - eps
+    CMat eps_s = eps;
+    // tau = H_{i,i+1}: ring b of cell i to ring a of cell i+1, gamma I; in E - H: -gamma
+    CMat tau(n * n, 0.0), taud(n * n, 0.0);
+    for (int j = 0; j < m; ++j) {
+        tau[(m + j) * n + j] = -gamma;
+        taud[j * n + (m + j)] = -gamma;
+    }
+    // the surface that faces the device: left lead -> its last cell couples to the right (alpha = tau^dagger side)
+    CMat al = left ? taud : tau, be = left ? tau : taud;
+    for (int it = 0; it < iters; ++it) {
+        CMat g = eps;
+        cinvert(g, n);
+        const CMat agb = cgemm(cgemm(al, g, n), be, n);
+        const CMat bga = cgemm(cgemm(be, g, n), al, n);
+        for (int i = 0; i < n * n; ++i) {
+            eps_s[i] -= agb[i];
+            eps[i] -= agb[i] + bga[i];
+        }
+        al = cgemm(cgemm(al, g, n), al, n);
+        be = cgemm(cgemm(be, g, n), be, n);
+    }
+    CMat gs = eps_s;
+    cinvert(gs, n);
+    CMat corner(m * m);
+    const int off = left ? m : 0;
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) corner[i * m + j] = gs[(off + i) * n + (off + j)];
+    return corner;
+}
+
+// Block RGF at one energy: the atom diagonal of G_kk for every block
+// (out[k * 2m + i]).  Uatoms: [K][2m].
+void rs_diag(int m, int K, double gamma, cplx E, const double* Uatoms, double Uc0, double Uc1, int iters,
+             std::vector<cplx>& out) {
+    const int n = 2 * m, mm = m * m;
+    const double g2 = gamma * gamma;
+    const CMat sL = rs_lead_corner(m, gamma, E, Uc0, true, iters);
+    const CMat sR = rs_lead_corner(m, gamma, E, Uc1, false, iters);
+    std::vector<CMat> gLbb(K, CMat(mm)), gRaa(K, CMat(mm));
+    for (int k = 0; k < K; ++k) {  // forward: left-connected g_L, corner [b][b]
+        CMat M = rs_block(m, gamma, E, Uatoms + (size_t)k * n);
+        const CMat& c = k == 0 ? sL : gLbb[k - 1];
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) M[i * n + j] -= g2 * c[i * m + j];
+        cinvert(M, n);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) gLbb[k][i * m + j] = M[(m + i) * n + (m + j)];
+    }
+    for (int k = K - 1; k >= 0; --k) {  // backward: right-connected g_R, corner [a][a]
+        CMat M = rs_block(m, gamma, E, Uatoms + (size_t)k * n);
+        const CMat& c = k == K - 1 ? sR : gRaa[k + 1];
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) M[(m + i) * n + (m + j)] -= g2 * c[i * m + j];
+        cinvert(M, n);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) gRaa[k][i * m + j] = M[i * n + j];
+    }
+    out.assign((size_t)K * n, 0.0);
+    for (int k = 0; k < K; ++k) {  // G_kk = (E - H_kk - Sigma_L - Sigma_R)^-1
+        CMat M = rs_block(m, gamma, E, Uatoms + (size_t)k * n);
+        const CMat& cl = k == 0 ? sL : gLbb[k - 1];
+        const CMat& cr = k == K - 1 ? sR : gRaa[k + 1];
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) {
+                M[i * n + j] -= g2 * cl[i * m + j];
+                M[(m + i) * n + (m + j)] -= g2 * cr[i * m + j];
+            }
+        cinvert(M, n);
+        for (int i = 0; i < n; ++i) out[(size_t)k * n + i] = M[i * n + i];
+    }
+}
+
 // ---------------------------------------------------------------- Broyden
 // T/Broyden_Second_Parallel.cpp:9-211 (CPU branch) and
 // T/Broyden_Parallel_General.cpp:68-355 (set-up and reset).
@@ -1179,6 +1335,65 @@ int orc_tube_noneq_layout(void* h, int* pts, double* cuts, double* E_at_max) {
     for (int p = 0; p + 1 < np; ++p) cuts[p] = t->intercuts[p];
     *E_at_max = t->E_at_max;
     return np;
+}
+
+// Real-space equilibrium charge per ring of a zigzag tube over the tube's
+// contour + poles (and Rho0 at U = 0): Q_ring = sum_atoms Im(RhoEq - Rho0)
+// with the same coefficients as the mode-space pass.  Uatoms: [N][m] per-atom
+// potentials (null: ring-uniform from the tube's U).  Returns -1 when biased.
+int orc_tube_rs_charge(void* h, const double* Uatoms, int iters, int nthreads, double* Q) {
+    Tube* t = static_cast<Tube*>(h);
+    energy_limits(*t);
+    build_eq_noneq_paths(*t);
+    if (t->noneq || t->n != 0) return -1;
+    const int m = t->m, N = t->N, K = N / 2, n = 2 * m;
+    std::vector<double> Ua((size_t)N * m), U0((size_t)N * m, 0.0);
+    for (int r = 0; r < N; ++r)
+        for (int j = 0; j < m; ++j) Ua[(size_t)r * m + j] = Uatoms ? Uatoms[(size_t)r * m + j] : t->U[r];
+    // ring r = 2k + (0 | 1) -> block k atoms [0, m) | [m, 2m): same layout as [N][m]
+    auto pts = collect(t->eq_paths, 1, *t);
+    for (auto& p : t->poles) pts.push_back(EPoint{p, 1.0, 1.0, 0.0, 2});
+    Tube t0 = *t;
+    t0.mu[0] = t0.mu[1] = 0.0;
+    t0.rt_pts = 0;
+    energy_limits(t0);
+    build_paths(t0);
+    auto pts0 = collect(t0.rho0_paths, 0, t0);
+    auto run = [&](const std::vector<EPoint>& P, const std::vector<double>& Uv, double Uc0, double Uc1,
+                   std::vector<double>& acc) {
+        acc.assign(N, 0.0);
+        const int T = std::max(1, std::min<int>(nthreads, (int)P.size()));
+        std::vector<std::vector<double>> part(T, std::vector<double>(N, 0.0));
+        auto worker = [&](int tid) {
+            std::vector<cplx> d;
+            for (size_t i = P.size() * tid / T; i < P.size() * (tid + 1) / T; ++i) {
+                const EPoint& ep = P[i];
+                rs_diag(m, K, t->gamma, ep.E, Uv.data(), Uc0, Uc1, iters, d);
+                cplx c;
+                if (ep.kind == 0)
+                    c = cmul((-1 * kSpinDegen / kPi) * ep.w, ep.J);
+                else if (ep.kind == 1)
+                    c = cmul(cmul((-1. * kSpinDegen / kPi) * ep.w, ep.J), ep.f);
+                else
+                    c = cplx(0.0, -2 * t->kT_min * kSpinDegen);
+                for (int r = 0; r < N; ++r) {
+                    cplx s = 0.0;
+                    for (int j = 0; j < m; ++j) s += d[(size_t)(r / 2) * n + (r % 2) * m + j];
+                    part[tid][r] += cmul(c, s).imag();
+                }
+            }
+        };
+        std::vector<std::thread> th;
+        for (int i = 0; i < T; ++i) th.emplace_back(worker, i);
+        for (auto& x : th) x.join();
+        for (int i = 0; i < T; ++i)
+            for (int r = 0; r < N; ++r) acc[r] += part[i][r];
+    };
+    std::vector<double> eq, r0;
+    run(pts, Ua, t->Uc[0], t->Uc[1], eq);
+    run(pts0, U0, 0.0, 0.0, r0);
+    for (int r = 0; r < N; ++r) Q[r] = eq[r] - r0[r];
+    return 0;
 }
 
 void* orc_broyden_new(int S, int maxstep, double fraction, int norm_type, const double* n_in) {

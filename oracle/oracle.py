@@ -70,6 +70,7 @@ def lib():
         L.orc_tube_set_adaptive.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_void_p]
         L.orc_tube_correct_limits.argtypes = [C.c_void_p, C.c_int]
         L.orc_tube_noneq_layout.argtypes = [C.c_void_p, _ip, _dp, _dp]
+        L.orc_tube_rs_charge.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, _dp]
         L.orc_broyden_new.restype = C.c_void_p
         L.orc_broyden_new.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, _dp]
         L.orc_broyden_free.argtypes = [C.c_void_p]
@@ -262,6 +263,20 @@ def _noneq_layout(self):
 OracleTube.noneq_integrand = _noneq_integrand
 OracleTube.correct_limits = _correct_limits
 OracleTube.noneq_layout = _noneq_layout
+def _rs_charge(self, Uatoms=None, iters=32, nthreads=1):
+    """Real-space ring-block equilibrium charge per ring (zigzag tubes)."""
+    Q = np.zeros(self.N)
+    ua = None
+    if Uatoms is not None:
+        self._ua = np.ascontiguousarray(Uatoms, dtype=np.float64)
+        ua = self._ua.ctypes.data_as(C.c_void_p)
+    rc = lib().orc_tube_rs_charge(self._h, ua, int(iters), int(nthreads), Q)
+    if rc != 0:
+        raise ValueError("real-space charge needs a zigzag tube at equilibrium")
+    return Q
+
+
+OracleTube.rs_charge = _rs_charge
 OracleTube.dos = _dos
 OracleTube.current = _current
 
