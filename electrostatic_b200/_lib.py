@@ -35,7 +35,9 @@ EXPORTED = [
     "negf_write_integrand", "negf_tube_correct_integration_limits", "negf_tube_noneq_integrand",
     "negf_tube_noneq_layout", "negf_read_table1d", "negf_broyden_step_device", "negf_affine_potential_masked",
     "negf_charge_plan_create", "negf_charge_plan_launch", "negf_charge_plan_info", "negf_charge_plan_destroy",
-    "negf_broyden_step_device_switch", "negf_rs_compute_charge",
+    "negf_broyden_step_device_switch", "negf_rs_compute_charge", "negf_nn_gemm", "negf_nn_gelu_fwd",
+    "negf_nn_gelu_bwd", "negf_nn_colsum", "negf_nn_cast_bf16", "negf_nn_adam", "negf_nn_rowdot", "negf_nn_outer",
+    "negf_nn_mse",
 ]
 
 
@@ -157,6 +159,17 @@ def load():
         "negf_broyden_step_device": [vp, vp, C.c_double, vp, vp],
         "negf_broyden_step_device_switch": [vp, vp, C.c_double, C.c_double, vp, vp],
         "negf_rs_compute_charge": [vp, vp, vp, vp],
+        "negf_nn_gemm": [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_longlong, vp, C.c_int,
+                         C.c_longlong, vp, C.c_int, C.c_longlong, vp, C.c_int, vp],
+        "negf_nn_gelu_fwd": [C.c_longlong, C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, vp],
+        "negf_nn_gelu_bwd": [C.c_longlong, vp, vp, vp, vp, vp],
+        "negf_nn_colsum": [C.c_longlong, C.c_int, vp, vp, C.c_int, vp],
+        "negf_nn_cast_bf16": [C.c_longlong, vp, vp, vp],
+        "negf_nn_adam": [C.c_longlong, vp, vp, vp, vp, vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                         C.c_float, vp],
+        "negf_nn_rowdot": [C.c_longlong, C.c_int, vp, vp, vp, vp, vp],
+        "negf_nn_outer": [C.c_longlong, C.c_int, vp, vp, vp, vp, vp],
+        "negf_nn_mse": [C.c_longlong, vp, vp, vp, vp, vp],
         "negf_affine_potential_masked": [vp, vp, vp, vp, C.c_int, vp, vp],
         "negf_charge_plan_create": [C.POINTER(vp), C.c_int, vp, C.c_int, C.POINTER(vp)],
         "negf_charge_plan_launch": [vp, vp, vp],

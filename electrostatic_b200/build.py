@@ -19,7 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libnegf_b200.so")
-SOURCES = ["negf_rgf.cu", "negf_broyden.cu", "negf_noalloc.cu", "negf_realspace.cu", "negf_api.cpp"]
+SOURCES = ["negf_rgf.cu", "negf_broyden.cu", "negf_noalloc.cu", "negf_realspace.cu", "negf_surrogate.cu",
+           "negf_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1530,6 +1530,58 @@ int negf_affine_potential_masked(const double* K, const double* U0, const double
     return NEGF_OK;
 }
 
+// ------------------------------------------------------------------ surrogate-model kernels
+int negf_nn_gemm(int a_trans, int b_trans, int M, int N, int K, int batch, const void* A, int lda, long long sA,
+                 const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* C_bf16, int accumulate,
+                 void* stream) {
+    if (!A || !B || !C || M < 0 || N < 0 || K < 0 || batch < 0) return fail(NEGF_ERR_ARG, "bad GEMM arguments");
+    NEGF_CUDA(negf::nn_gemm(a_trans, b_trans, M, N, K, batch, A, lda, sA, B, ldb, sB, C, ldc, sC, C_bf16, accumulate,
+                            (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_gelu_fwd(long long rows, int cols, const float* a, const float* b, const float* bias, float* pre,
+                     float* out, void* out_bf16, int activation, void* stream) {
+    if (!a) return fail(NEGF_ERR_ARG, "null input");
+    NEGF_CUDA(negf::nn_gelu_fwd(rows, cols, a, b, bias, pre, out, out_bf16, activation, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_gelu_bwd(long long n, const float* dy, const float* pre, float* d, void* d_bf16, void* stream) {
+    if (!dy || !pre) return fail(NEGF_ERR_ARG, "null input");
+    NEGF_CUDA(negf::nn_gelu_bwd(n, dy, pre, d, d_bf16, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_colsum(long long rows, int cols, const float* x, float* out, int accumulate, void* stream) {
+    if (!x || !out) return fail(NEGF_ERR_ARG, "null argument");
+    NEGF_CUDA(negf::nn_colsum(rows, cols, x, out, accumulate, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_cast_bf16(long long n, const float* x, void* y, void* stream) {
+    if (!x || !y) return fail(NEGF_ERR_ARG, "null argument");
+    NEGF_CUDA(negf::nn_cast_bf16(n, x, y, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_adam(long long n, float* w, const float* g, float* m, float* v, void* w_bf16, float lr, float beta1,
+                 float beta2, float eps, int step, float weight_decay, void* stream) {
+    if (!w || !g || !m || !v || step < 1) return fail(NEGF_ERR_ARG, "bad Adam arguments");
+    NEGF_CUDA(negf::nn_adam(n, w, g, m, v, w_bf16, lr, beta1, beta2, eps, step, weight_decay, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_rowdot(long long rows, int cols, const float* h, const float* w, const float* b, float* q, void* stream) {
+    if (!h || !w || !q) return fail(NEGF_ERR_ARG, "null argument");
+    NEGF_CUDA(negf::nn_rowdot(rows, cols, h, w, b, q, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_outer(long long rows, int cols, const float* dq, const float* w, float* dh, void* dh_bf16, void* stream) {
+    if (!dq || !w) return fail(NEGF_ERR_ARG, "null argument");
+    NEGF_CUDA(negf::nn_outer(rows, cols, dq, w, dh, dh_bf16, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+int negf_nn_mse(long long n, const float* q, const float* y, float* d, float* partials, void* stream) {
+    if (!q || !y || !d || !partials) return fail(NEGF_ERR_ARG, "null argument");
+    NEGF_CUDA(negf::nn_mse(n, q, y, d, partials, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+
 // ------------------------------------------------------------------ real-space ring blocks
 int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, void* stream) {
     if (!t || !d_Q) return fail(NEGF_ERR_ARG, "null argument");

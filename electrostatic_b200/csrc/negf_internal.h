@@ -92,6 +92,22 @@ cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, co
 cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_t stream);
 int rs_max_atoms_per_block();
 
+// Surrogate-model kernels (negf_surrogate.cu).  BF16 operands as void*.
+cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* A, int lda, long long sA,
+                    const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* Cb, int accumulate,
+                    cudaStream_t s);
+cudaError_t nn_gelu_fwd(long long rows, int cols, const float* a, const float* b, const float* bias, float* pre,
+                        float* out, void* outb, int act, cudaStream_t s);
+cudaError_t nn_gelu_bwd(long long n, const float* dy, const float* pre, float* d, void* db, cudaStream_t s);
+cudaError_t nn_colsum(long long rows, int cols, const float* x, float* out, int accumulate, cudaStream_t s);
+cudaError_t nn_cast_bf16(long long n, const float* x, void* y, cudaStream_t s);
+cudaError_t nn_adam(long long n, float* w, const float* g, float* m, float* v, void* wb, float lr, float b1, float b2,
+                    float eps, int step, float wd, cudaStream_t s);
+cudaError_t nn_rowdot(long long rows, int cols, const float* h, const float* w, const float* b, float* q,
+                      cudaStream_t s);
+cudaError_t nn_outer(long long rows, int cols, const float* dq, const float* w, float* dh, void* dhb, cudaStream_t s);
+cudaError_t nn_mse(long long n, const float* q, const float* y, float* d, float* part, cudaStream_t s);
+
 // skip (device int, may be null): when nonzero at launch time every block
 // returns at entry (device-side early exit of a captured SCF iteration).
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,

@@ -1,0 +1,368 @@
+// Kernels of the surrogate charge model (a 1D Fourier neural operator used
+// to start the self-consistent loop): a BF16 tensor-core GEMM with FP32
+// accumulation and the elementwise / reduction kernels of its training and
+// inference.  The reference engine has no counterpart.
+//
+// GEMM: C[b] (M x N, FP32) = A[b] (M x K) * B[b] (K x N), BF16 operands in any
+// of the four layouts (A row- or column-major, B row- or column-major), with
+// strided batches; optional accumulation into C and an optional BF16 copy of
+// the result.  CTA tile 128 x 128 x 32, 8 warps (2 x 4), warp tile 64 x 32 of
+// mma.sync m16n8k16 (BF16 in, FP32 accumulate).  Tiles go global -> registers
+// -> shared memory (k-contiguous rows, padded to 40 elements so that the
+// fragment loads of a warp hit distinct banks); the next tile is loaded while
+// the current one is multiplied.  Every global access is bounds-checked, so
+// M, N, K need not be tile multiples.
+
+#include <cuda_bf16.h>
+
+#include "negf_internal.h"
+
+namespace negf {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 32, PAD = 40, NT = 256;
+
+__device__ __forceinline__ unsigned pack2(const __nv_bfloat16* p) { return *reinterpret_cast<const unsigned*>(p); }
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Element (m, k) of A and (k, n) of B for the four layouts.
+template <bool AT>
+__device__ __forceinline__ size_t a_off(int m, int k, int lda) {
+    return AT ? (size_t)k * lda + m : (size_t)m * lda + k;
+}
+template <bool BT>
+__device__ __forceinline__ size_t b_off(int k, int n, int ldb) {
+    return BT ? (size_t)n * ldb + k : (size_t)k * ldb + n;
+}
+
+template <bool AT, bool BT>
+__global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
+                                                       int lda, long long sA, const __nv_bfloat16* __restrict__ B,
+                                                       int ldb, long long sB, float* __restrict__ C, int ldc,
+                                                       long long sC, __nv_bfloat16* __restrict__ Cb, int accumulate) {
+    __shared__ __align__(16) __nv_bfloat16 As[2][BM][PAD];
+    __shared__ __align__(16) __nv_bfloat16 Bs[2][BN][PAD];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 2, wn = warp & 3;  // warp tile: rows wm*64, cols wn*32
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const long long bz = blockIdx.z;
+    A += bz * sA;
+    B += bz * sB;
+    C += bz * sC;
+    if (Cb) Cb += bz * sC;
+    const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+
+    // staging: 16 elements of A and 16 of B per thread per k-tile, index i = tid + NT * j
+    __nv_bfloat16 ra[16], rb[16];
+    auto load_tile = [&](int k0) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int i = tid + NT * j;
+            // A: the contiguous dimension varies fastest across threads
+            int m, k;
+            if (AT) {
+                k = i / BM;
+                m = i % BM;
+            } else {
+                m = i / BK;
+                k = i % BK;
+            }
+            const int gm = m0 + m, gk = k0 + k;
+            ra[j] = (gm < M && gk < K) ? A[a_off<AT>(gm, gk, lda)] : zero;
+            int n, kb;
+            if (BT) {
+                n = i / BK;
+                kb = i % BK;
+            } else {
+                kb = i / BN;
+                n = i % BN;
+            }
+            const int gn = n0 + n, gkb = k0 + kb;
+            rb[j] = (gn < N && gkb < K) ? B[b_off<BT>(gkb, gn, ldb)] : zero;
+        }
+    };
+    auto store_tile = [&](int buf) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int i = tid + NT * j;
+            int m, k;
+            if (AT) {
+                k = i / BM;
+                m = i % BM;
+            } else {
+                m = i / BK;
+                k = i % BK;
+            }
+            As[buf][m][k] = ra[j];
+            int n, kb;
+            if (BT) {
+                n = i / BK;
+                kb = i % BK;
+            } else {
+                kb = i / BN;
+                n = i % BN;
+            }
+            Bs[buf][n][kb] = rb[j];
+        }
+    };
+
+    float acc[4][4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
+
+    const int g = lane >> 2, t = lane & 3;
+    const int ktiles = (K + BK - 1) / BK;
+    load_tile(0);
+    store_tile(0);
+    __syncthreads();
+    for (int kt = 0; kt < ktiles; ++kt) {
+        const int buf = kt & 1;
+        if (kt + 1 < ktiles) load_tile((kt + 1) * BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 16) {
+            unsigned af[4][4], bf[4][2];
+#pragma unroll
+            for (int im = 0; im < 4; ++im) {
+                const int r = wm * 64 + im * 16 + g;
+                af[im][0] = pack2(&As[buf][r][kk + 2 * t]);
+                af[im][1] = pack2(&As[buf][r + 8][kk + 2 * t]);
+                af[im][2] = pack2(&As[buf][r][kk + 2 * t + 8]);
+                af[im][3] = pack2(&As[buf][r + 8][kk + 2 * t + 8]);
+            }
+#pragma unroll
+            for (int in = 0; in < 4; ++in) {
+                const int c = wn * 32 + in * 8 + g;
+                bf[in][0] = pack2(&Bs[buf][c][kk + 2 * t]);
+                bf[in][1] = pack2(&Bs[buf][c][kk + 2 * t + 8]);
+            }
+#pragma unroll
+            for (int im = 0; im < 4; ++im)
+#pragma unroll
+                for (int in = 0; in < 4; ++in) mma_bf16(acc[im][in], af[im], bf[in]);
+        }
+        if (kt + 1 < ktiles) {
+            store_tile(buf ^ 1);  // the other buffer: last read one iteration ago, before the barrier below
+        }
+        __syncthreads();
+    }
+    // epilogue: c0,c1 at (row g, cols 2t, 2t+1); c2,c3 at (row g+8, same cols)
+#pragma unroll
+    for (int im = 0; im < 4; ++im)
+#pragma unroll
+        for (int in = 0; in < 4; ++in)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = m0 + wm * 64 + im * 16 + g + 8 * h;
+                if (row >= M) continue;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int col = n0 + wn * 32 + in * 8 + 2 * t + q;
+                    if (col >= N) continue;
+                    float v = acc[im][in][2 * h + q];
+                    float* p = C + (size_t)row * ldc + col;
+                    if (accumulate) v += *p;
+                    *p = v;
+                    if (Cb) Cb[(size_t)row * ldc + col] = __float2bfloat16(v);
+                }
+            }
+}
+
+__device__ __forceinline__ float gelu(float x) {
+    const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+    return 0.5f * x * (1.0f + tanhf(k0 * (x + k1 * x * x * x)));
+}
+__device__ __forceinline__ float gelu_grad(float x) {
+    const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+    const float u = k0 * (x + k1 * x * x * x), th = tanhf(u);
+    return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * k0 * (1.0f + 3.0f * k1 * x * x);
+}
+
+// pre[r][c] = a[r][c] + b[r][c] + bias[c]; out = gelu(pre) (FP32 and BF16)
+__global__ void gelu_fwd_kernel(long long rows, int cols, const float* __restrict__ a, const float* __restrict__ b,
+                                const float* __restrict__ bias, float* __restrict__ pre, float* __restrict__ out,
+                                __nv_bfloat16* __restrict__ outb, int act) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows * cols) return;
+    const int c = (int)(i % cols);
+    const float x = a[i] + (b ? b[i] : 0.0f) + (bias ? bias[c] : 0.0f);
+    if (pre) pre[i] = x;
+    const float y = act ? gelu(x) : x;
+    if (out) out[i] = y;
+    if (outb) outb[i] = __float2bfloat16(y);
+}
+
+// d[i] = dy[i] * gelu'(pre[i]) (FP32 and BF16 copies)
+__global__ void gelu_bwd_kernel(long long n, const float* __restrict__ dy, const float* __restrict__ pre,
+                                float* __restrict__ d, __nv_bfloat16* __restrict__ db) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = dy[i] * gelu_grad(pre[i]);
+    if (d) d[i] = v;
+    if (db) db[i] = __float2bfloat16(v);
+}
+
+// out[c] (+)= sum_r x[r][c], one block per 32 columns, fixed order.
+__global__ void colsum_kernel(long long rows, int cols, const float* __restrict__ x, float* __restrict__ out,
+                              int accumulate) {
+    __shared__ float sh[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    float s = 0.0f;
+    if (c < cols)
+        for (long long r = threadIdx.y; r < rows; r += 8) s += x[r * cols + c];
+    sh[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < cols) {
+        float t = 0.0f;
+        for (int y = 0; y < 8; ++y) t += sh[y][threadIdx.x];
+        out[c] = accumulate ? out[c] + t : t;
+    }
+}
+
+__global__ void cast_bf16_kernel(long long n, const float* __restrict__ x, __nv_bfloat16* __restrict__ y) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = __float2bfloat16(x[i]);
+}
+
+// Adam on FP32 master weights, refreshed BF16 copy.
+__global__ void adam_kernel(long long n, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, __nv_bfloat16* __restrict__ wb, float lr, float b1, float b2,
+                            float eps, float c1, float c2, float wd) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i] + wd * w[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16(wi);
+}
+
+// Per row r: q[r] = sum_c h[r][c] w[c] + b (one warp per row)
+__global__ void rowdot_kernel(long long rows, int cols, const float* __restrict__ h, const float* __restrict__ w,
+                              const float* __restrict__ b, float* __restrict__ q) {
+    const long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    float s = 0.0f;
+    for (int c = lane; c < cols; c += 32) s += h[r * cols + c] * w[c];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) q[r] = s + (b ? *b : 0.0f);
+}
+
+// dh[r][c] = dq[r] * w[c] (FP32 and BF16)
+__global__ void outer_kernel(long long rows, int cols, const float* __restrict__ dq, const float* __restrict__ w,
+                             float* __restrict__ dh, __nv_bfloat16* __restrict__ dhb) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows * cols) return;
+    const float v = dq[i / cols] * w[i % cols];
+    if (dh) dh[i] = v;
+    if (dhb) dhb[i] = __float2bfloat16(v);
+}
+
+// Squared-error loss: d[i] = 2 (q[i] - y[i]) / n; per-block partial sums of (q - y)^2.
+__global__ void mse_kernel(long long n, const float* __restrict__ q, const float* __restrict__ y, float* __restrict__ d,
+                           float* __restrict__ part) {
+    __shared__ float sh[256];
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float e = 0.0f;
+    if (i < n) {
+        const float r = q[i] - y[i];
+        d[i] = 2.0f * r / (float)n;
+        e = r * r;
+    }
+    sh[threadIdx.x] = e;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+}  // namespace
+
+cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* A, int lda, long long sA,
+                    const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* Cb, int accumulate,
+                    cudaStream_t s) {
+    if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return cudaSuccess;
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, batch);
+    const auto* a = static_cast<const __nv_bfloat16*>(A);
+    const auto* b = static_cast<const __nv_bfloat16*>(B);
+    auto* cb = static_cast<__nv_bfloat16*>(Cb);
+    if (!at && !bt)
+        gemm_bf16_kernel<false, false><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+    else if (!at && bt)
+        gemm_bf16_kernel<false, true><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+    else if (at && !bt)
+        gemm_bf16_kernel<true, false><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+    else
+        gemm_bf16_kernel<true, true><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+    return cudaGetLastError();
+}
+
+static unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t nn_gelu_fwd(long long rows, int cols, const float* a, const float* b, const float* bias, float* pre,
+                        float* out, void* outb, int act, cudaStream_t s) {
+    const long long n = rows * cols;
+    if (n <= 0) return cudaSuccess;
+    gelu_fwd_kernel<<<blocks_for(n, 256), 256, 0, s>>>(rows, cols, a, b, bias, pre, out,
+                                                       static_cast<__nv_bfloat16*>(outb), act);
+    return cudaGetLastError();
+}
+cudaError_t nn_gelu_bwd(long long n, const float* dy, const float* pre, float* d, void* db, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    gelu_bwd_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, dy, pre, d, static_cast<__nv_bfloat16*>(db));
+    return cudaGetLastError();
+}
+cudaError_t nn_colsum(long long rows, int cols, const float* x, float* out, int accumulate, cudaStream_t s) {
+    if (cols <= 0) return cudaSuccess;
+    colsum_kernel<<<(cols + 31) / 32, dim3(32, 8), 0, s>>>(rows, cols, x, out, accumulate);
+    return cudaGetLastError();
+}
+cudaError_t nn_cast_bf16(long long n, const float* x, void* y, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    cast_bf16_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, x, static_cast<__nv_bfloat16*>(y));
+    return cudaGetLastError();
+}
+cudaError_t nn_adam(long long n, float* w, const float* g, float* m, float* v, void* wb, float lr, float b1, float b2,
+                    float eps, int step, float wd, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    adam_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, w, g, m, v, static_cast<__nv_bfloat16*>(wb), lr, b1, b2, eps, c1,
+                                                   c2, wd);
+    return cudaGetLastError();
+}
+cudaError_t nn_rowdot(long long rows, int cols, const float* h, const float* w, const float* b, float* q,
+                      cudaStream_t s) {
+    if (rows <= 0) return cudaSuccess;
+    rowdot_kernel<<<blocks_for(rows, 8), 256, 0, s>>>(rows, cols, h, w, b, q);
+    return cudaGetLastError();
+}
+cudaError_t nn_outer(long long rows, int cols, const float* dq, const float* w, float* dh, void* dhb, cudaStream_t s) {
+    const long long n = rows * cols;
+    if (n <= 0) return cudaSuccess;
+    outer_kernel<<<blocks_for(n, 256), 256, 0, s>>>(rows, cols, dq, w, dh, static_cast<__nv_bfloat16*>(dhb));
+    return cudaGetLastError();
+}
+cudaError_t nn_mse(long long n, const float* q, const float* y, float* d, float* part, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    mse_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, q, y, d, part);
+    return cudaGetLastError();
+}
+
+}  // namespace negf

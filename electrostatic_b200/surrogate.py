@@ -1,0 +1,396 @@
+"""Surrogate charge model: a 1D Fourier neural operator for the Broyden start.
+
+Maps the site potential U of a tube (plus the gate and drain biases) to the
+induced charge Q that the NEGF engine would return.  It is trained on (U, Q)
+pairs produced by the engine itself and serves as the initial guess of the
+self-consistent loop; the NEGF engine judges every converged charge.  The
+reference has no counterpart (its loop starts from a constant charge,
+Broyden_Parallel_General.cpp:68-248).
+
+Architecture (channel-last activations, rows = samples x sites):
+  lift      h0 = x W_lift + b_lift,  x = (U, Vg, Vds, site / S)       4 -> 128
+  6 layers  h  = GELU(h W_l + G (R_l * (F h)) + b_l)                 128 -> 128
+            F: real DFT basis of the first 32 frequencies (cos, sin: 64 rows),
+            G: its synthesis basis, R_l: per-frequency 256 x 256 mixing of the
+            (cos, sin) coefficient pair over all channels
+  project   q  = h w_p + b_p                                          128 -> 1
+Every product is a BF16 tensor-core GEMM with FP32 accumulation
+(negf_nn_gemm); GELU, bias, loss, reductions and Adam are the library's own
+kernels; PyTorch only allocates the device buffers.  Master weights and
+optimiser state are FP32, their BF16 copies feed the GEMMs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+WIDTH, MODES, LAYERS, FEAT = 128, 32, 6, 4
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class FourierOperator:
+    """The operator for tubes of S sites.  All state lives on the device."""
+
+    def __init__(self, S: int, seed: int = 0, device: str = "cuda"):
+        import torch
+        self.torch = torch
+        self.S, self.dev = int(S), device
+        g = torch.Generator().manual_seed(seed)
+        W, M = WIDTH, MODES
+        f32 = dict(dtype=torch.float32)
+
+        def init(shape, fan_in):
+            return (torch.randn(*shape, generator=g, **f32) / math.sqrt(fan_in)).to(device)
+
+        self.params = {
+            "W_lift": init((FEAT, W), FEAT),
+            "b_lift": torch.zeros(W, device=device, **f32),
+            "w_p": init((W,), W),
+            "b_p": torch.zeros(1, device=device, **f32),
+        }
+        for l in range(LAYERS):
+            self.params[f"W{l}"] = init((W, W), W)
+            self.params[f"R{l}"] = init((M, 2 * W, 2 * W), 2 * W) * 0.5
+            self.params[f"b{l}"] = torch.zeros(W, device=device, **f32)
+        self.bf = {k: v.to(torch.bfloat16) for k, v in self.params.items()}
+        self.grads = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        self.m = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        self.v = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        self.step = 0
+        # analysis / synthesis bases on the site grid: rows (cos k, sin k), k < 32
+        s = np.arange(self.S)
+        F = np.zeros((2 * M, self.S))
+        for k in range(M):
+            F[2 * k] = np.cos(2 * np.pi * k * s / self.S) * (1.0 if k == 0 else 2.0) / self.S
+            F[2 * k + 1] = np.sin(2 * np.pi * k * s / self.S) * 2.0 / self.S
+        G = np.zeros((self.S, 2 * M))
+        for k in range(M):
+            G[:, 2 * k] = np.cos(2 * np.pi * k * s / self.S)
+            G[:, 2 * k + 1] = np.sin(2 * np.pi * k * s / self.S)
+        self.F = torch.tensor(F, dtype=torch.bfloat16, device=device)
+        self.G = torch.tensor(G, dtype=torch.bfloat16, device=device)
+        self.x_scale = torch.ones(FEAT, device=device)
+        self.q_scale = 1.0
+        self._bufs = {}
+
+    # ------------------------------------------------------------------ helpers
+    def _buf(self, name, shape, dtype=None):
+        t = self.torch
+        dtype = dtype or t.float32
+        key = (name, tuple(shape), dtype)
+        b = self._bufs.get(key)
+        if b is None:
+            b = t.empty(*shape, dtype=dtype, device=self.dev)
+            self._bufs[key] = b
+        return b
+
+    def _gemm(self, at, bt, M, N, K, batch, A, lda, sA, B, ldb, sB, Cf, ldc, sC, Cb=None, acc=0):
+        check(_lib.load().negf_nn_gemm(at, bt, M, N, K, batch, _p(A), lda, sA, _p(B), ldb, sB, _p(Cf), ldc, sC, _p(Cb),
+                                       acc, None), "negf_nn_gemm")
+
+    # ------------------------------------------------------------------ model
+    def features(self, U, Vg, Vds):
+        """x[b][s] = (U, Vg, Vds, s / S) scaled by the stored input scales."""
+        t = self.torch
+        B = U.shape[0]
+        x = t.empty(B, self.S, FEAT, device=self.dev)
+        x[:, :, 0] = U
+        x[:, :, 1] = Vg[:, None]
+        x[:, :, 2] = Vds[:, None]
+        x[:, :, 3] = t.arange(self.S, device=self.dev)[None, :] / self.S
+        return (x / self.x_scale).to(t.bfloat16).reshape(B * self.S, FEAT)
+
+    def forward(self, xb, B, keep=False):
+        """xb: BF16 [B*S][4]; returns q [B*S] (FP32, in units of q_scale)."""
+        t, L = self.torch, _lib.load()
+        S, W, M = self.S, WIDTH, MODES
+        R = B * S
+        cache = {"xb": xb} if keep else None
+        h = self._buf("h0", (R, W))
+        hb = self._buf("h0b", (R, W), t.bfloat16)
+        self._gemm(0, 0, R, W, FEAT, 1, xb, FEAT, 0, self.bf["W_lift"], W, 0, h, W, 0)
+        check(L.negf_nn_gelu_fwd(R, W, _p(h), None, _p(self.params["b_lift"]), None, _p(h), _p(hb), 0, None), "lift")
+        for l in range(LAYERS):
+            s1 = self._buf(f"s1_{l}", (R, W))
+            hat = self._buf(f"hat{l}", (B, 2 * M, W))
+            hatb = self._buf(f"hatb{l}", (B, 2 * M, W), t.bfloat16)
+            z = self._buf(f"z{l}", (B, 2 * M, W))
+            zb = self._buf(f"zb{l}", (B, 2 * M, W), t.bfloat16)
+            s2 = self._buf(f"s2_{l}", (R, W))
+            self._gemm(0, 0, R, W, W, 1, hb, W, 0, self.bf[f"W{l}"], W, 0, s1, W, 0)
+            self._gemm(0, 0, 2 * M, W, S, B, self.F, S, 0, hb, W, S * W, hat, W, 2 * M * W, hatb)
+            # per frequency k: rows b of hat[b][2k:2k+2][:] (256 values) times R[k]
+            self._gemm(0, 0, B, 2 * W, 2 * W, M, hatb, 2 * M * W, 2 * W, self.bf[f"R{l}"], 2 * W, 4 * W * W,
+                       z, 2 * M * W, 2 * W, zb)
+            self._gemm(0, 0, S, W, 2 * M, B, self.G, 2 * M, 0, zb, W, 2 * M * W, s2, W, S * W)
+            pre = self._buf(f"pre{l}", (R, W)) if keep else None
+            hn = self._buf(f"h{l + 1}", (R, W))
+            hnb = self._buf(f"h{l + 1}b", (R, W), t.bfloat16)
+            check(L.negf_nn_gelu_fwd(R, W, _p(s1), _p(s2), _p(self.params[f"b{l}"]), _p(pre), _p(hn), _p(hnb), 1,
+                                     None), "gelu")
+            if keep:
+                cache[l] = (hb, hatb, zb, pre)
+            h, hb = hn, hnb
+        q = self._buf("q", (R,))
+        check(L.negf_nn_rowdot(R, W, _p(h), _p(self.params["w_p"]), _p(self.params["b_p"]), _p(q), None), "proj")
+        if keep:
+            cache["h_last"], cache["h_lastb"] = h, hb
+            self._cache = cache
+        return q
+
+    def backward(self, dq, B):
+        """Gradients of the loss for dq = dL/dq [B*S] (after forward(keep=True))."""
+        t, L = self.torch, _lib.load()
+        S, W, M = self.S, WIDTH, MODES
+        R = B * S
+        c = self._cache
+        gr = self.grads
+        # projection
+        dqb = self._buf("dqb", (R,), t.bfloat16)
+        check(L.negf_nn_cast_bf16(R, _p(dq), _p(dqb), None), "cast")
+        self._gemm(0, 0, 1, W, R, 1, dqb, R, 0, c["h_lastb"], W, 0, gr["w_p"], W, 0)
+        check(L.negf_nn_colsum(R, 1, _p(dq), _p(gr["b_p"]), 0, None), "colsum")
+        dh = self._buf("dh", (R, W))
+        check(L.negf_nn_outer(R, W, _p(dq), _p(self.params["w_p"]), _p(dh), None, None), "outer")
+        for l in reversed(range(LAYERS)):
+            hb, hatb, zb, pre = c[l]
+            dpre = self._buf("dpre", (R, W))
+            dpreb = self._buf("dpreb", (R, W), t.bfloat16)
+            check(L.negf_nn_gelu_bwd(R * W, _p(dh), _p(pre), _p(dpre), _p(dpreb), None), "gelu_bwd")
+            check(L.negf_nn_colsum(R, W, _p(dpre), _p(gr[f"b{l}"]), 0, None), "colsum")
+            # pointwise path: dW = h^T dpre ; dh = dpre W^T
+            self._gemm(1, 0, W, W, R, 1, hb, W, 0, dpreb, W, 0, gr[f"W{l}"], W, 0)
+            dhn = self._buf("dhn", (R, W))
+            self._gemm(0, 1, R, W, W, 1, dpreb, W, 0, self.bf[f"W{l}"], W, 0, dhn, W, 0)
+            # spectral path: dz = G^T dpre ; dR_k = hat_k^T dz_k ; dhat_k = dz_k R_k^T ; dh += F^T dhat
+            dz = self._buf("dz", (B, 2 * M, W))
+            dzb = self._buf("dzb", (B, 2 * M, W), t.bfloat16)
+            self._gemm(1, 0, 2 * M, W, S, B, self.G, 2 * M, 0, dpreb, W, S * W, dz, W, 2 * M * W, dzb)
+            self._gemm(1, 0, 2 * W, 2 * W, B, M, hatb, 2 * M * W, 2 * W, dzb, 2 * M * W, 2 * W, gr[f"R{l}"], 2 * W,
+                       4 * W * W)
+            dhat = self._buf("dhat", (B, 2 * M, W))
+            dhatb = self._buf("dhatb", (B, 2 * M, W), t.bfloat16)
+            self._gemm(0, 1, B, 2 * W, 2 * W, M, dzb, 2 * M * W, 2 * W, self.bf[f"R{l}"], 2 * W, 4 * W * W, dhat,
+                       2 * M * W, 2 * W, dhatb)
+            self._gemm(1, 0, S, W, 2 * M, B, self.F, S, 0, dhatb, W, 2 * M * W, dhn, W, S * W, None, 1)
+            dh, dhn = dhn, dh
+            self._bufs[("dh", (R, W), t.float32)], self._bufs[("dhn", (R, W), t.float32)] = dh, dhn
+        # lift
+        dhb = self._buf("dhb", (R, W), t.bfloat16)
+        check(L.negf_nn_cast_bf16(R * W, _p(dh), _p(dhb), None), "cast")
+        self._gemm(1, 0, FEAT, W, R, 1, c["xb"], FEAT, 0, dhb, W, 0, gr["W_lift"], W, 0)
+        check(L.negf_nn_colsum(R, W, _p(dh), _p(gr["b_lift"]), 0, None), "colsum")
+
+    def adam(self, lr=1e-3, wd=0.0):
+        L = _lib.load()
+        self.step += 1
+        for k, w in self.params.items():
+            check(L.negf_nn_adam(w.numel(), _p(w), _p(self.grads[k]), _p(self.m[k]), _p(self.v[k]), _p(self.bf[k]),
+                                 lr, 0.9, 0.999, 1e-8, self.step, wd, None), "adam")
+
+    def loss_grad(self, q, y):
+        """MSE in units of q_scale; returns (dq, partial sums)."""
+        L = _lib.load()
+        n = q.numel()
+        dq = self._buf("dq", (n,))
+        part = self._buf("part", ((n + 255) // 256,))
+        check(L.negf_nn_mse(n, _p(q), _p(y), _p(dq), _p(part), None), "mse")
+        return dq, part
+
+    # ------------------------------------------------------------------ API
+    def fit(self, U, Vg, Vds, Q, epochs=20, batch=16, lr=2e-3, log=None):
+        """Train on device tensors U [n][S], Vg [n], Vds [n], Q [n][S] (float32)."""
+        t = self.torch
+        n = U.shape[0]
+        self.x_scale = t.tensor([float(U.abs().max()), 1.0, 1.0, 1.0], device=self.dev)
+        self.q_scale = float(Q.abs().max())
+        y_all = (Q / self.q_scale).float()
+        g = t.Generator(device="cpu").manual_seed(1)
+        hist = []
+        t0 = time.perf_counter()
+        steps = epochs * (n // batch)
+        for ep in range(epochs):
+            perm = t.randperm(n, generator=g)
+            tot = 0.0
+            for i in range(n // batch):
+                idx = perm[i * batch:(i + 1) * batch].to(self.dev)
+                xb = self.features(U[idx], Vg[idx], Vds[idx])
+                q = self.forward(xb, batch, keep=True)
+                y = y_all[idx].reshape(-1).contiguous()
+                dq, part = self.loss_grad(q, y)
+                self.backward(dq, batch)
+                frac = (ep * (n // batch) + i) / max(1, steps)
+                self.adam(lr=lr * 0.5 * (1 + math.cos(math.pi * frac)))
+                tot += float(part.sum()) / (batch * self.S)
+            hist.append(tot / (n // batch))
+            if log:
+                log(ep, hist[-1])
+        t.cuda.synchronize()
+        return {"epochs": epochs, "seconds": time.perf_counter() - t0, "loss": hist}
+
+    def predict(self, U, Vg, Vds, batch=16):
+        """Charge [n][S] (float64) for potentials U [n][S]."""
+        t = self.torch
+        n = U.shape[0]
+        out = t.empty(n, self.S, dtype=t.float64, device=self.dev)
+        for i in range(0, n, batch):
+            b = min(batch, n - i)
+            xb = self.features(U[i:i + b], Vg[i:i + b], Vds[i:i + b])
+            q = self.forward(xb, b)
+            out[i:i + b] = (q[: b * self.S].reshape(b, self.S) * self.q_scale).double()
+        return out
+
+
+# ---------------------------------------------------------------------- data
+def tube_kwargs(vds, eta=2e-3, unitcells=1000, modes=8, precision="fp64"):
+    """The (17,0) 4000-site, 8-mode tube with 1024 contour + 3072 real-axis
+    energies on [-1.5, 1.5] eV, contact mu (0, -Vds)."""
+    return dict(type_id=(17, 0), num_unitcells=unitcells, num_modes=modes, contact_mu=(0.0, -float(vds)),
+                contact_T=(300.0, 300.0), eq_integration_pts=(256, 256, 512), E_zPlus_imag=eta,
+                realaxis_window=(-1.5, 1.5, 3072, 0), precision=precision)
+
+
+def generate_pairs(n, seed=20261203 + 5, vds_bins=13, batch_tubes=16, unitcells=1000, modes=8, log=None):
+    """n (U, Vg, Vds, Q) samples of the engine on the tube of tube_kwargs:
+    Vg ~ U(0, 0.8) V, Vds ~ U(0, 0.6) V (rounded to vds_bins levels so that
+    tubes of one level share their energy paths), U = the gate/contact
+    stand-in's external potential (gate Vg, source 0, drain Vds) + the
+    config-2 recipe of 5 seeded Gaussian bumps (amplitudes up to a, a drawn
+    from U(0, 0.4) V per sample; widths U(2, 10) nm).
+    Returns device tensors (float32 U, Vg, Vds; float64 Q) and the seconds
+    the engine spent."""
+    import torch
+    from .negf import CNT, compute_charge
+    from .workloads import gate_with_contacts, site_potential
+    rng = np.random.default_rng(seed)
+    levels = np.linspace(0.0, 0.6, vds_bins)
+    vds = levels[rng.integers(0, vds_bins, n)]
+    vg = rng.uniform(0.0, 0.8, n)
+    U_all = np.zeros((n, 4 * unitcells))
+    Q_all = torch.zeros(n, 4 * unitcells, dtype=torch.float64, device="cuda")
+    engine = 0.0
+    for lv in levels:
+        idx = np.nonzero(vds == lv)[0]
+        if len(idx) == 0:
+            continue
+        tubes = [CNT(**tube_kwargs(lv, unitcells=unitcells, modes=modes)) for _ in range(min(batch_tubes, len(idx)))]
+        y = tubes[0].site_positions()
+        R = 1.42e-10 * np.sqrt(3.0) * 17 / (2 * np.pi)
+        ga = gate_with_contacts(y, R, vds=lv)
+        for c in range(0, len(idx), len(tubes)):
+            part = idx[c:c + len(tubes)]
+            for t, i in zip(tubes, part):
+                amp = rng.uniform(0.0, 0.4)
+                U = ga.external(vg[i]) + site_potential(y, seed + 1000 + int(i), amp=amp, ramp=0.0)
+                U_all[i] = U
+                t.set_potential(U, (U[0], U[-1]))
+            out = torch.empty(sum(t.num_field_sites for t in tubes[:len(part)]), dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            compute_charge(tubes[:len(part)], out=out)
+            torch.cuda.synchronize()
+            engine += time.perf_counter() - t0
+            Q_all[torch.as_tensor(part, device="cuda")] = out.reshape(len(part), -1)
+        if log:
+            log(lv, len(idx))
+        del tubes
+    dev = "cuda"
+    return (torch.tensor(U_all, dtype=torch.float32, device=dev), torch.tensor(vg, dtype=torch.float32, device=dev),
+            torch.tensor(vds, dtype=torch.float32, device=dev), Q_all, engine)
+
+
+# ---------------------------------------------------------------------- SCF
+def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e-6, max_step=200,
+              use_graph=True, iters_per_graph=4, surrogate_norm=1e-6, surrogate_max_step=200):
+    """Gate sweep of one tube, plain or surrogate-started.
+
+    Plain: Broyden from n = 0 with the NEGF charge (device-resident steps,
+    CUDA-graph replay).  Surrogate-started: the same Broyden first converges
+    the loop with the surrogate's charge (to surrogate_norm) and then
+    continues, without a reset, with the NEGF charge; the Broyden history
+    built on the surrogate is the initial inverse Jacobian of the NEGF phase
+    and only an NEGF charge can end the step.  Returns per-step records
+    (NEGF iterations, surrogate iterations, seconds, converged charge)."""
+    import torch
+    from . import negf as ng
+    N = tube.num_field_sites
+    dev = "cuda"
+    stream = torch.cuda.Stream()
+    out = []
+    with torch.cuda.stream(stream):
+        Q = torch.zeros(N, dtype=torch.float64, device=dev)
+        br = ng.Broyden(torch.zeros(N, dtype=torch.float64, device=dev), max_step=max_step, fraction=fraction,
+                        stream=stream)
+        nin = br.input_device_ptr()
+        nin_t = __import__("electrostatic_b200.scf", fromlist=["device_view"]).device_view(nin, N)
+        Kd, U0 = electro.device_operator(0.0)
+        U0 = U0.clone()
+        Up = tube.potential_device_ptr()
+        Uview = __import__("electrostatic_b200.scf", fromlist=["device_view"]).device_view(Up, N)
+        flags = torch.zeros(8, dtype=torch.int32, device=dev)
+        skip = flags.data_ptr() + 12
+        ng.affine_potential_masked(Kd, U0, nin, Up, N, None, stream=stream)
+        plan = ng.ChargePlan([tube], Q)
+
+        def body(s):
+            ng.affine_potential_masked(Kd, U0, nin, Up, N, skip, stream=s)
+            plan.launch(skip=skip, stream=s)
+            br.step_device(Q, max_norm, flags, stream=s)
+
+        graph = None
+        if use_graph:
+            flags[3] = 1
+            body(stream)
+            stream.synchronize()
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=stream):
+                for _ in range(iters_per_graph):
+                    body(torch.cuda.current_stream())
+        for Vg in Vg_list:
+            U0.copy_(electro.device_operator(Vg)[1])
+            flags.zero_()
+            stream.synchronize()
+            t0 = time.perf_counter()
+            sur_it = 0
+            if model is not None:
+                vg_t = torch.tensor([float(Vg)], device=dev)
+                vd_t = torch.tensor([float(Vds)], device=dev)
+                flags_s = torch.zeros(8, dtype=torch.int32, device=dev)
+                while True:
+                    ng.affine_potential_masked(Kd, U0, nin, Up, N, None, stream=stream)
+                    Qs = model.predict(Uview.float()[None, :], vg_t, vd_t, batch=1)[0]
+                    Q.copy_(Qs)
+                    br.step_device(Q, surrogate_norm, flags_s, stream=stream)
+                    sur_it += 1
+                    f = flags_s.cpu().numpy()
+                    if f[3] or sur_it >= surrogate_max_step:
+                        break
+                # continue the same Broyden with the NEGF charge
+            while True:
+                if graph is not None:
+                    graph.replay()
+                else:
+                    body(stream)
+                f = flags.cpu().numpy()
+                if f[3]:
+                    break
+            dt = time.perf_counter() - t0
+            if f[2]:
+                raise RuntimeError("NEGF self-consistency failed (flag %d)" % f[2])
+            out.append(dict(Vg=float(Vg), negf_iterations=int(f[1]), surrogate_iterations=sur_it, seconds=dt,
+                            Q=Q.cpu().numpy().copy()))
+            br.reset(stream=stream)
+        stream.synchronize()
+    del graph
+    plan.close()
+    br.close()
+    return out

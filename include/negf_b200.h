@@ -202,6 +202,36 @@ int negf_set_timing(int enable);
  * mode-space charge with all m//2 + 1 distinct modes.  Synchronous. */
 int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, void* stream);
 
+/* Surrogate-model kernels (no counterpart in the reference): the training
+ * and inference kernels of the neural operator that starts the
+ * self-consistent loop (electrostatic_b200/surrogate.py).  BF16 tensors are
+ * passed as void* (bf16 storage), FP32 as float*; all pointers are device
+ * pointers; launches are asynchronous on `stream`.
+ * negf_nn_gemm: C[b] (M x N, FP32, leading dimension ldc, batch stride sC)
+ * (+)= A[b] (M x K) B[b] (K x N) for b < batch; a_trans = 0: A[m][k] at
+ * A + m lda + k, else at A + k lda + m; b_trans = 0: B[k][n] at B + k ldb + n,
+ * else at B + n ldb + k; tensor-core mma (BF16 in, FP32 accumulate);
+ * C_bf16 (optional) receives a BF16 copy of C.
+ * negf_nn_gelu_fwd: pre = a + b + bias[col] (b, bias optional), out = GELU(pre)
+ * (tanh form) or pre when activation = 0.  negf_nn_gelu_bwd: d = dy GELU'(pre).
+ * negf_nn_colsum: column sums.  negf_nn_adam: Adam with bias correction on
+ * FP32 master weights (+ BF16 copy).  negf_nn_rowdot: q[r] = h[r] . w + *b.
+ * negf_nn_outer: dh[r][c] = dq[r] w[c].  negf_nn_mse: d = 2 (q - y) / n and
+ * per-256-block partial sums of (q - y)^2. */
+int negf_nn_gemm(int a_trans, int b_trans, int M, int N, int K, int batch, const void* A, int lda, long long sA,
+                 const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* C_bf16, int accumulate,
+                 void* stream);
+int negf_nn_gelu_fwd(long long rows, int cols, const float* a, const float* b, const float* bias, float* pre,
+                     float* out, void* out_bf16, int activation, void* stream);
+int negf_nn_gelu_bwd(long long n, const float* dy, const float* pre, float* d, void* d_bf16, void* stream);
+int negf_nn_colsum(long long rows, int cols, const float* x, float* out, int accumulate, void* stream);
+int negf_nn_cast_bf16(long long n, const float* x, void* y, void* stream);
+int negf_nn_adam(long long n, float* w, const float* g, float* m, float* v, void* w_bf16, float lr, float beta1,
+                 float beta2, float eps, int step, float weight_decay, void* stream);
+int negf_nn_rowdot(long long rows, int cols, const float* h, const float* w, const float* b, float* q, void* stream);
+int negf_nn_outer(long long rows, int cols, const float* dq, const float* w, float* dh, void* dh_bf16, void* stream);
+int negf_nn_mse(long long n, const float* q, const float* y, float* d, float* partials, void* stream);
+
 /* Transport characteristics (c_NEGF_Common::Compute_DensityOfStates,
  * NEGF_Common.cpp:2390-2847, and Compute_Current, :4321-4816; called from
  * c_Nanostructure::PostProcess, Nanostructure.H:134-138).

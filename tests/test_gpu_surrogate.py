@@ -1,0 +1,90 @@
+"""Surrogate-model kernels: the BF16 tensor-core GEMM in its four layouts
+against FP32 matmul of the same BF16 values, the hand-written backward pass
+against autograd of the same operator, and a training smoke test."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("at,bt", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K,batch", [(130, 70, 45, 3), (1, 128, 300, 1), (256, 256, 4, 2), (64, 256, 257, 1)])
+def test_gemm_layouts(at, bt, M, N, K, batch):
+    import torch
+    from electrostatic_b200 import _lib
+    L = _lib.load()
+    g = torch.Generator().manual_seed(M * 7 + N + K)
+    A = torch.randn(batch, *((K, M) if at else (M, K)), generator=g).to(torch.bfloat16)
+    B = torch.randn(batch, *((N, K) if bt else (K, N)), generator=g).to(torch.bfloat16)
+    C0 = torch.randn(batch, M, N, generator=g)
+    Af, Bf = A.float(), B.float()
+    ref = (Af.transpose(1, 2) if at else Af) @ (Bf.transpose(1, 2) if bt else Bf) + C0
+    dA, dB, dC = A.cuda(), B.cuda(), C0.cuda().contiguous()
+    dCb = torch.empty(batch, M, N, dtype=torch.bfloat16, device="cuda")
+    lda, ldb = (M if at else K), (K if bt else N)
+    vp = lambda t: __import__("ctypes").c_void_p(t.data_ptr())
+    rc = L.negf_nn_gemm(at, bt, M, N, K, batch, vp(dA), lda, dA[0].numel(), vp(dB), ldb, dB[0].numel(), vp(dC), N,
+                        M * N, vp(dCb), 1, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    out = dC.cpu()
+    assert torch.allclose(out, ref, rtol=1e-5, atol=1e-4 * (1 + ref.abs().max().item()))
+    assert torch.allclose(dCb.float().cpu(), out.to(torch.bfloat16).float())
+
+
+def _torch_reference(model, U, Vg, Vds, y):
+    """The same operator in FP32 autograd (BF16-rounded weights and bases)."""
+    import torch
+    from electrostatic_b200.surrogate import LAYERS
+    P = {k: v.detach().to(torch.bfloat16).float().clone().requires_grad_(True) for k, v in model.params.items()}
+    F, G = model.F.float(), model.G.float()
+    x = model.features(U, Vg, Vds).float()
+    h = x @ P["W_lift"] + P["b_lift"]
+    B, S = U.shape
+    for l in range(LAYERS):
+        s1 = h @ P[f"W{l}"]
+        hb = h.reshape(B, S, -1)
+        hat = torch.einsum("ks,bsc->bkc", F, hb)  # [B][64][W]
+        hk = hat.reshape(B, 32, 2 * hb.shape[-1])
+        z = torch.einsum("bki,kio->bko", hk, P[f"R{l}"]).reshape(B, 64, -1)
+        s2 = torch.einsum("sk,bkc->bsc", G, z).reshape(B * S, -1)
+        h = torch.nn.functional.gelu(s1 + s2 + P[f"b{l}"], approximate="tanh")
+    q = h @ P["w_p"] + P["b_p"]
+    loss = ((q - y) ** 2).mean()
+    loss.backward()
+    return {k: v.grad for k, v in P.items()}, loss.item()
+
+
+def test_backward_matches_autograd():
+    import torch
+    from electrostatic_b200.surrogate import FourierOperator
+    S, B = 256, 2
+    m = FourierOperator(S, seed=3)
+    g = torch.Generator().manual_seed(0)
+    U = (0.3 * torch.randn(B, S, generator=g)).cuda()
+    Vg, Vds = torch.tensor([0.2, 0.5]).cuda(), torch.tensor([0.1, 0.4]).cuda()
+    y = (0.1 * torch.randn(B * S, generator=g)).cuda()
+    ref, _ = _torch_reference(m, U, Vg, Vds, y)
+    q = m.forward(m.features(U, Vg, Vds), B, keep=True)
+    dq, _ = m.loss_grad(q, y)
+    m.backward(dq, B)
+    torch.cuda.synchronize()
+    for k in ("W_lift", "b_lift", "W0", "R0", "b0", "W5", "R5", "w_p", "b_p"):
+        a, r = m.grads[k].cpu().float(), ref[k].cpu().float()
+        rel = (a - r).norm() / max(r.norm().item(), 1e-12)
+        assert rel < 5e-2, (k, float(rel))
+
+
+def test_training_reduces_loss():
+    import torch
+    from electrostatic_b200.surrogate import FourierOperator
+    S, n = 256, 32
+    g = torch.Generator().manual_seed(1)
+    U = (0.3 * torch.randn(n, S, generator=g)).cuda()
+    Vg, Vds = torch.rand(n, generator=g).cuda(), torch.rand(n, generator=g).cuda()
+    Q = (torch.tanh(U) * 0.02 + 0.01 * Vg[:, None]).double()
+    m = FourierOperator(S, seed=5)
+    r = m.fit(U, Vg, Vds, Q, epochs=30, batch=8, lr=2e-3)
+    assert r["loss"][-1] < 0.2 * r["loss"][0]
+    pred = m.predict(U, Vg, Vds)
+    assert pred.shape == Q.shape and torch.isfinite(pred).all()
