@@ -317,6 +317,44 @@ def config3_measure(torch, passes=2):
             "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm)))}
 
 
+def config5_measure(torch, n_pairs=8000, epochs=15):
+    """Surrogate-started self-consistency on the 4000-site, 8-mode (17,0) tube
+    (Vds 0.4 V, gate 0 -> 0.6 V): pairs recorded along plain NEGF solves,
+    BF16 training of the Fourier operator, then plain vs surrogate-started
+    sweeps (NEGF judges every converged charge)."""
+    from electrostatic_b200 import surrogate as S
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import gate_with_contacts
+    t0 = time.perf_counter()
+    U, Vg, Vds, Q, eng = S.generate_scf_pairs(n_pairs)
+    t_data = time.perf_counter() - t0
+    perm = torch.randperm(n_pairs, generator=torch.Generator().manual_seed(0)).cuda()
+    U, Vg, Vds, Q = U[perm], Vg[perm], Vds[perm], Q[perm]
+    ntr = int(0.9 * n_pairs)
+    m = S.FourierOperator(4000, seed=0)
+    r = m.fit(U[:ntr], Vg[:ntr], Vds[:ntr], Q[:ntr], epochs=epochs, batch=16)
+    pred = m.predict(U[ntr:], Vg[ntr:], Vds[ntr:])
+    err = ((pred - Q[ntr:]).abs().max(dim=1).values / Q[ntr:].abs().max(dim=1).values).cpu().numpy()
+    vds = 0.4
+    tube = CNT(**S.tube_kwargs(vds))
+    R = 1.42e-10 * np.sqrt(3.0) * 17 / (2 * np.pi)
+    el = gate_with_contacts(tube.site_positions(), R, vds=vds)
+    vgs = [0.0, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6]
+    S.scf_sweep(tube, el, [0.0], vds)
+    plain = S.scf_sweep(tube, el, vgs, vds)
+    sur = S.scf_sweep(tube, el, vgs, vds, model=m, keep_history=False)
+    return {"workload": "(17,0) N=4000, 8 modes, 1024 contour + 3072 real-axis energies (eta 2 meV), Vds 0.4 V, "
+                        "Vg 0..0.6 V; operator 6 layers x width 128 x 32 frequencies, BF16 weights, FP32 accumulate",
+            "pairs": n_pairs, "data_seconds": t_data, "engine_seconds": eng, "train_seconds": r["seconds"],
+            "epochs": epochs, "final_loss": r["loss"][-1], "test_rel_err_median": float(np.median(err)),
+            "plain": {"iterations": [a["negf_iterations"] for a in plain], "seconds": sum(a["seconds"] for a in plain)},
+            "surrogate_started": {"negf_iterations": [b["negf_iterations"] for b in sur],
+                                  "surrogate_iterations": [b["surrogate_iterations"] for b in sur],
+                                  "used": [b["surrogate_used"] for b in sur],
+                                  "seconds": sum(b["seconds"] for b in sur)},
+            "max_abs_dQ_vs_plain": max(float(np.max(np.abs(a["Q"] - b["Q"]))) for a, b in zip(plain, sur))}
+
+
 def ring_positions_nm(unitcells, acc=1.42e-10):
     """Axial ring positions [nm] of a zigzag tube (CNT.cpp:93-132)."""
     y0 = -(unitcells / 2.0) * 3.0 * acc - acc / 2.0
@@ -336,6 +374,7 @@ def main():
     ap.add_argument("--no-scf", action="store_true")
     ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--no-config3", action="store_true")
+    ap.add_argument("--config5", action="store_true", help="surrogate study (about two minutes, off by default)")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis)")
     args = ap.parse_args()
@@ -472,6 +511,7 @@ def main():
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
         cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch)
+        cfg5 = config5_measure(torch) if (args.config5 and world == 1) else None
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                 "frac": achieved_tf / peak_tf if peak_tf else None,
                 "traffic": prof.get("dram_bytes_per_launch"),
@@ -489,7 +529,7 @@ def main():
                 "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
                            "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config3": cfg3, "config4": cfg4,
+                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config3": cfg3, "config4": cfg4, "config5": cfg5,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
                         "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},

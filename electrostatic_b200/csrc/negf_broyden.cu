@@ -148,7 +148,9 @@ __global__ void newrow_kernel(BroydenDev b, int m_host, const int* flags) {
         for (int it = 1; it <= m - 1; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
         const double dF = b.dF[s];
         const double dn = b.n_in[s] - b.n_prev[s];
-        b.V[(size_t)m * b.S + s] = dF / denom;
+        // a zero step (identical consecutive residuals) adds no direction: the
+        // reference would divide by zero here
+        b.V[(size_t)m * b.S + s] = denom > 0.0 ? dF / denom : 0.0;
         b.W[(size_t)m * b.S + s] = -b.fraction * dF + dn - acc;
     }
 }

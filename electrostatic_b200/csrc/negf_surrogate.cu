@@ -15,6 +15,8 @@
 
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "negf_internal.h"
 
 namespace negf {
@@ -42,20 +44,28 @@ __device__ __forceinline__ size_t b_off(int k, int n, int ldb) {
     return BT ? (size_t)n * ldb + k : (size_t)k * ldb + n;
 }
 
+// splits > 1: blockIdx.z = batch * splits + split; the split covers K
+// elements [split * kchunk, min(K, (split + 1) * kchunk)) and writes its
+// partial product to the workspace (C = workspace, ldc = N, sC = M * N per z),
+// summed by splitk_reduce_kernel in split order.
 template <bool AT, bool BT>
 __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
                                                        int lda, long long sA, const __nv_bfloat16* __restrict__ B,
                                                        int ldb, long long sB, float* __restrict__ C, int ldc,
-                                                       long long sC, __nv_bfloat16* __restrict__ Cb, int accumulate) {
+                                                       long long sC, __nv_bfloat16* __restrict__ Cb, int accumulate,
+                                                       int splits, int kchunk) {
     __shared__ __align__(16) __nv_bfloat16 As[2][BM][PAD];
     __shared__ __align__(16) __nv_bfloat16 Bs[2][BN][PAD];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp >> 2, wn = warp & 3;  // warp tile: rows wm*64, cols wn*32
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-    const long long bz = blockIdx.z;
+    const long long bz = blockIdx.z / splits;
+    const int split = blockIdx.z % splits;
+    const int kbeg = split * kchunk;
+    const int kend = min(K, kbeg + kchunk);
     A += bz * sA;
     B += bz * sB;
-    C += bz * sC;
+    C += splits > 1 ? (long long)blockIdx.z * sC : bz * sC;
     if (Cb) Cb += bz * sC;
     const __nv_bfloat16 zero = __float2bfloat16(0.0f);
 
@@ -75,7 +85,7 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
                 k = i % BK;
             }
             const int gm = m0 + m, gk = k0 + k;
-            ra[j] = (gm < M && gk < K) ? A[a_off<AT>(gm, gk, lda)] : zero;
+            ra[j] = (gm < M && gk < kend) ? A[a_off<AT>(gm, gk, lda)] : zero;
             int n, kb;
             if (BT) {
                 n = i / BK;
@@ -85,7 +95,7 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
                 n = i % BN;
             }
             const int gn = n0 + n, gkb = k0 + kb;
-            rb[j] = (gn < N && gkb < K) ? B[b_off<BT>(gkb, gn, ldb)] : zero;
+            rb[j] = (gn < N && gkb < kend) ? B[b_off<BT>(gkb, gn, ldb)] : zero;
         }
     };
     auto store_tile = [&](int buf) {
@@ -122,13 +132,13 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
             for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
 
     const int g = lane >> 2, t = lane & 3;
-    const int ktiles = (K + BK - 1) / BK;
-    load_tile(0);
+    const int ktiles = (kend - kbeg + BK - 1) / BK;
+    load_tile(kbeg);
     store_tile(0);
     __syncthreads();
     for (int kt = 0; kt < ktiles; ++kt) {
         const int buf = kt & 1;
-        if (kt + 1 < ktiles) load_tile((kt + 1) * BK);
+        if (kt + 1 < ktiles) load_tile(kbeg + (kt + 1) * BK);
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 16) {
             unsigned af[4][4], bf[4][2];
@@ -171,11 +181,32 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
                     if (col >= N) continue;
                     float v = acc[im][in][2 * h + q];
                     float* p = C + (size_t)row * ldc + col;
+                    if (splits > 1) {
+                        *p = v;
+                        continue;
+                    }
                     if (accumulate) v += *p;
                     *p = v;
                     if (Cb) Cb[(size_t)row * ldc + col] = __float2bfloat16(v);
                 }
             }
+}
+
+// C[b][m][n] (+)= sum over splits (in order) of W[b * splits + s][m][n]
+__global__ void splitk_reduce_kernel(int M, int N, int batch, int splits, const float* __restrict__ W,
+                                     float* __restrict__ C, int ldc, long long sC, __nv_bfloat16* __restrict__ Cb,
+                                     int accumulate) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long MN = (long long)M * N;
+    if (i >= MN * batch) return;
+    const long long b = i / MN, r = i % MN;
+    const int m = (int)(r / N), n = (int)(r % N);
+    float v = 0.0f;
+    for (int s = 0; s < splits; ++s) v += W[(b * splits + s) * MN + r];
+    float* p = C + b * sC + (size_t)m * ldc + n;
+    if (accumulate) v += *p;
+    *p = v;
+    if (Cb) Cb[b * sC + (size_t)m * ldc + n] = __float2bfloat16(v);
 }
 
 __device__ __forceinline__ float gelu(float x) {
@@ -299,18 +330,54 @@ cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* 
                     const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* Cb, int accumulate,
                     cudaStream_t s) {
     if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return cudaSuccess;
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, batch);
+    const int tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM) * batch;
+    // split K when the output has too few tiles to fill the GPU (deterministic: partials + ordered sum)
+    int splits = 1;
+    const int kt = (K + BK - 1) / BK;
+    if (tiles < 296 && kt >= 8) splits = std::min(std::min(296 / tiles + 1, kt / 4), 64);
+    if (splits < 1) splits = 1;
+    const int kchunk = ((kt + splits - 1) / splits) * BK;
+    splits = (K + kchunk - 1) / kchunk;
+    static float* ws = nullptr;
+    static size_t ws_bytes = 0;
+    float* out = C;
+    int ldo = ldc;
+    long long so = sC;
+    if (splits > 1) {
+        const size_t need = sizeof(float) * (size_t)M * N * batch * splits;
+        if (need > ws_bytes) {
+            if (ws) cudaFree(ws);
+            ws = nullptr;
+            ws_bytes = 0;
+            cudaError_t e = cudaMalloc(&ws, need);
+            if (e != cudaSuccess) return e;
+            ws_bytes = need;
+        }
+        out = ws;
+        ldo = N;
+        so = (long long)M * N;
+    }
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, batch * splits);
     const auto* a = static_cast<const __nv_bfloat16*>(A);
     const auto* b = static_cast<const __nv_bfloat16*>(B);
-    auto* cb = static_cast<__nv_bfloat16*>(Cb);
+    auto* cb = splits > 1 ? nullptr : static_cast<__nv_bfloat16*>(Cb);
     if (!at && !bt)
-        gemm_bf16_kernel<false, false><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+        gemm_bf16_kernel<false, false><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so, cb,
+                                                           accumulate, splits, kchunk);
     else if (!at && bt)
-        gemm_bf16_kernel<false, true><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+        gemm_bf16_kernel<false, true><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so, cb,
+                                                          accumulate, splits, kchunk);
     else if (at && !bt)
-        gemm_bf16_kernel<true, false><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+        gemm_bf16_kernel<true, false><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so, cb,
+                                                          accumulate, splits, kchunk);
     else
-        gemm_bf16_kernel<true, true><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, C, ldc, sC, cb, accumulate);
+        gemm_bf16_kernel<true, true><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so, cb,
+                                                         accumulate, splits, kchunk);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || splits == 1) return e;
+    const long long n = (long long)M * N * batch;
+    splitk_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(M, N, batch, splits, ws, C, ldc, sC,
+                                                                     static_cast<__nv_bfloat16*>(Cb), accumulate);
     return cudaGetLastError();
 }
 

@@ -93,9 +93,13 @@ class FourierOperator:
             self._bufs[key] = b
         return b
 
+    def _s(self):
+        """The current torch stream (every kernel of the model runs on it)."""
+        return C.c_void_p(self.torch.cuda.current_stream().cuda_stream)
+
     def _gemm(self, at, bt, M, N, K, batch, A, lda, sA, B, ldb, sB, Cf, ldc, sC, Cb=None, acc=0):
         check(_lib.load().negf_nn_gemm(at, bt, M, N, K, batch, _p(A), lda, sA, _p(B), ldb, sB, _p(Cf), ldc, sC, _p(Cb),
-                                       acc, None), "negf_nn_gemm")
+                                       acc, self._s()), "negf_nn_gemm")
 
     # ------------------------------------------------------------------ model
     def features(self, U, Vg, Vds):
@@ -118,7 +122,8 @@ class FourierOperator:
         h = self._buf("h0", (R, W))
         hb = self._buf("h0b", (R, W), t.bfloat16)
         self._gemm(0, 0, R, W, FEAT, 1, xb, FEAT, 0, self.bf["W_lift"], W, 0, h, W, 0)
-        check(L.negf_nn_gelu_fwd(R, W, _p(h), None, _p(self.params["b_lift"]), None, _p(h), _p(hb), 0, None), "lift")
+        check(L.negf_nn_gelu_fwd(R, W, _p(h), None, _p(self.params["b_lift"]), None, _p(h), _p(hb), 0, self._s()),
+              "lift")
         for l in range(LAYERS):
             s1 = self._buf(f"s1_{l}", (R, W))
             hat = self._buf(f"hat{l}", (B, 2 * M, W))
@@ -136,12 +141,12 @@ class FourierOperator:
             hn = self._buf(f"h{l + 1}", (R, W))
             hnb = self._buf(f"h{l + 1}b", (R, W), t.bfloat16)
             check(L.negf_nn_gelu_fwd(R, W, _p(s1), _p(s2), _p(self.params[f"b{l}"]), _p(pre), _p(hn), _p(hnb), 1,
-                                     None), "gelu")
+                                     self._s()), "gelu")
             if keep:
                 cache[l] = (hb, hatb, zb, pre)
             h, hb = hn, hnb
         q = self._buf("q", (R,))
-        check(L.negf_nn_rowdot(R, W, _p(h), _p(self.params["w_p"]), _p(self.params["b_p"]), _p(q), None), "proj")
+        check(L.negf_nn_rowdot(R, W, _p(h), _p(self.params["w_p"]), _p(self.params["b_p"]), _p(q), self._s()), "proj")
         if keep:
             cache["h_last"], cache["h_lastb"] = h, hb
             self._cache = cache
@@ -156,17 +161,17 @@ class FourierOperator:
         gr = self.grads
         # projection
         dqb = self._buf("dqb", (R,), t.bfloat16)
-        check(L.negf_nn_cast_bf16(R, _p(dq), _p(dqb), None), "cast")
+        check(L.negf_nn_cast_bf16(R, _p(dq), _p(dqb), self._s()), "cast")
         self._gemm(0, 0, 1, W, R, 1, dqb, R, 0, c["h_lastb"], W, 0, gr["w_p"], W, 0)
-        check(L.negf_nn_colsum(R, 1, _p(dq), _p(gr["b_p"]), 0, None), "colsum")
+        check(L.negf_nn_colsum(R, 1, _p(dq), _p(gr["b_p"]), 0, self._s()), "colsum")
         dh = self._buf("dh", (R, W))
-        check(L.negf_nn_outer(R, W, _p(dq), _p(self.params["w_p"]), _p(dh), None, None), "outer")
+        check(L.negf_nn_outer(R, W, _p(dq), _p(self.params["w_p"]), _p(dh), None, self._s()), "outer")
         for l in reversed(range(LAYERS)):
             hb, hatb, zb, pre = c[l]
             dpre = self._buf("dpre", (R, W))
             dpreb = self._buf("dpreb", (R, W), t.bfloat16)
-            check(L.negf_nn_gelu_bwd(R * W, _p(dh), _p(pre), _p(dpre), _p(dpreb), None), "gelu_bwd")
-            check(L.negf_nn_colsum(R, W, _p(dpre), _p(gr[f"b{l}"]), 0, None), "colsum")
+            check(L.negf_nn_gelu_bwd(R * W, _p(dh), _p(pre), _p(dpre), _p(dpreb), self._s()), "gelu_bwd")
+            check(L.negf_nn_colsum(R, W, _p(dpre), _p(gr[f"b{l}"]), 0, self._s()), "colsum")
             # pointwise path: dW = h^T dpre ; dh = dpre W^T
             self._gemm(1, 0, W, W, R, 1, hb, W, 0, dpreb, W, 0, gr[f"W{l}"], W, 0)
             dhn = self._buf("dhn", (R, W))
@@ -186,16 +191,16 @@ class FourierOperator:
             self._bufs[("dh", (R, W), t.float32)], self._bufs[("dhn", (R, W), t.float32)] = dh, dhn
         # lift
         dhb = self._buf("dhb", (R, W), t.bfloat16)
-        check(L.negf_nn_cast_bf16(R * W, _p(dh), _p(dhb), None), "cast")
+        check(L.negf_nn_cast_bf16(R * W, _p(dh), _p(dhb), self._s()), "cast")
         self._gemm(1, 0, FEAT, W, R, 1, c["xb"], FEAT, 0, dhb, W, 0, gr["W_lift"], W, 0)
-        check(L.negf_nn_colsum(R, W, _p(dh), _p(gr["b_lift"]), 0, None), "colsum")
+        check(L.negf_nn_colsum(R, W, _p(dh), _p(gr["b_lift"]), 0, self._s()), "colsum")
 
     def adam(self, lr=1e-3, wd=0.0):
         L = _lib.load()
         self.step += 1
         for k, w in self.params.items():
             check(L.negf_nn_adam(w.numel(), _p(w), _p(self.grads[k]), _p(self.m[k]), _p(self.v[k]), _p(self.bf[k]),
-                                 lr, 0.9, 0.999, 1e-8, self.step, wd, None), "adam")
+                                 lr, 0.9, 0.999, 1e-8, self.step, wd, self._s()), "adam")
 
     def loss_grad(self, q, y):
         """MSE in units of q_scale; returns (dq, partial sums)."""
@@ -203,7 +208,7 @@ class FourierOperator:
         n = q.numel()
         dq = self._buf("dq", (n,))
         part = self._buf("part", ((n + 255) // 256,))
-        check(L.negf_nn_mse(n, _p(q), _p(y), _p(dq), _p(part), None), "mse")
+        check(L.negf_nn_mse(n, _p(q), _p(y), _p(dq), _p(part), self._s()), "mse")
         return dq, part
 
     # ------------------------------------------------------------------ API
@@ -236,6 +241,34 @@ class FourierOperator:
                 log(ep, hist[-1])
         t.cuda.synchronize()
         return {"epochs": epochs, "seconds": time.perf_counter() - t0, "loss": hist}
+
+    def bind(self, U_view, Vg, Vds, Q_out):
+        """Fixed buffers for repeated single-sample inference (capturable in a
+        CUDA graph after one call of infer()): U_view (float64 device view of a
+        potential buffer), scalar biases, Q_out (float64 device, S)."""
+        t = self.torch
+        self._bind = dict(U=U_view, Q=Q_out, x=t.empty(1, self.S, FEAT, device=self.dev),
+                          xb=t.empty(self.S, FEAT, dtype=t.bfloat16, device=self.dev))
+        x = self._bind["x"]
+        x[:, :, 1] = float(Vg)
+        x[:, :, 2] = float(Vds)
+        x[:, :, 3] = t.arange(self.S, device=self.dev)[None, :] / self.S
+        x.div_(self.x_scale)
+
+    def set_bias(self, Vg, Vds):
+        x = self._bind["x"]
+        x[:, :, 1] = float(Vg) / float(self.x_scale[1])
+        x[:, :, 2] = float(Vds) / float(self.x_scale[2])
+
+    def infer(self):
+        """Q_out = model(U_view) with the bound buffers (no allocation after the first call)."""
+        b = self._bind
+        b["x"][0, :, 0].copy_(b["U"])
+        b["x"][0, :, 0].div_(self.x_scale[0])
+        b["xb"].copy_(b["x"][0])
+        q = self.forward(b["xb"], 1)
+        b["Q"].copy_(q)
+        b["Q"].mul_(self.q_scale)
 
     def predict(self, U, Vg, Vds, batch=16):
         """Charge [n][S] (float64) for potentials U [n][S]."""
@@ -308,9 +341,69 @@ def generate_pairs(n, seed=20261203 + 5, vds_bins=13, batch_tubes=16, unitcells=
             torch.tensor(vds, dtype=torch.float32, device=dev), Q_all, engine)
 
 
+def generate_scf_pairs(n, seed=20261203 + 5, vds_bins=13, max_iter=60, unitcells=1000, modes=8, log=None):
+    """n (U, Vg, Vds, Q) pairs recorded along plain self-consistent solves of
+    the tube of tube_kwargs inside its gate/contact stand-in at random
+    Vg ~ U(0, 0.8) V and Vds ~ U(0, 0.6) V (vds_bins levels): every NEGF
+    iteration of every solve is one pair, so the pairs cover the potentials
+    that a self-consistent loop visits.  Returns device tensors and the
+    seconds the engine spent."""
+    import torch
+    from .negf import CNT, Broyden, compute_charge
+    from .scf import device_view
+    from .workloads import gate_with_contacts
+    rng = np.random.default_rng(seed)
+    levels = np.linspace(0.0, 0.6, vds_bins)
+    S = 4 * unitcells
+    U_all = torch.zeros(n, S, dtype=torch.float32, device="cuda")
+    Q_all = torch.zeros(n, S, dtype=torch.float64, device="cuda")
+    vg_all = np.zeros(n)
+    vd_all = np.zeros(n)
+    tubes, electros = {}, {}
+    R = 1.42e-10 * np.sqrt(3.0) * 17 / (2 * np.pi)
+    k = 0
+    engine = 0.0
+    Q = torch.zeros(S, dtype=torch.float64, device="cuda")
+    while k < n:
+        lv = float(levels[rng.integers(0, vds_bins)])
+        vg = float(rng.uniform(0.0, 0.8))
+        if lv not in tubes:
+            tubes[lv] = CNT(**tube_kwargs(lv, unitcells=unitcells, modes=modes))
+            electros[lv] = gate_with_contacts(tubes[lv].site_positions(), R, vds=lv)
+        t, el = tubes[lv], electros[lv]
+        Kd, U0 = el.device_operator(vg)
+        Up = t.potential_device_ptr()
+        Uv = device_view(Up, S)
+        br = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"), max_step=max_iter + 2, fraction=0.1)
+        nin = device_view(br.input_device_ptr(), S)
+        for _ in range(max_iter):
+            check(_lib.load().negf_affine_potential(C.c_void_p(Kd.data_ptr()), C.c_void_p(U0.data_ptr()),
+                                                    C.c_void_p(nin.data_ptr()), C.c_void_p(Up), S, None),
+                  "negf_affine_potential")
+            ends = Uv[[0, S - 1]].cpu().numpy()
+            t.set_potential_device(Up, (float(ends[0]), float(ends[1])))
+            t0 = time.perf_counter()
+            compute_charge([t], out=Q)
+            torch.cuda.synchronize()
+            engine += time.perf_counter() - t0
+            if k < n:
+                U_all[k] = Uv.float()
+                Q_all[k] = Q
+                vg_all[k], vd_all[k] = vg, lv
+                k += 1
+            if not (br.step(Q) > 1e-6) or k >= n:
+                break
+        br.close()
+        if log:
+            log(k)
+    dev = "cuda"
+    return (U_all, torch.tensor(vg_all, dtype=torch.float32, device=dev),
+            torch.tensor(vd_all, dtype=torch.float32, device=dev), Q_all, engine)
+
+
 # ---------------------------------------------------------------------- SCF
 def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e-6, max_step=200,
-              use_graph=True, iters_per_graph=4, surrogate_norm=1e-6, surrogate_max_step=200):
+              use_graph=True, iters_per_graph=4, surrogate_norm=1e-3, surrogate_max_step=60, keep_history=True):
     """Gate sweep of one tube, plain or surrogate-started.
 
     Plain: Broyden from n = 0 with the NEGF charge (device-resident steps,
@@ -318,8 +411,11 @@ def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e
     the loop with the surrogate's charge (to surrogate_norm) and then
     continues, without a reset, with the NEGF charge; the Broyden history
     built on the surrogate is the initial inverse Jacobian of the NEGF phase
-    and only an NEGF charge can end the step.  Returns per-step records
-    (NEGF iterations, surrogate iterations, seconds, converged charge)."""
+    (keep_history=False: only the charge is kept) and only an NEGF charge can
+    end the step.  A surrogate phase that does not converge within
+    surrogate_max_step steps (or turns non-finite) is discarded and the step
+    starts plain.  Returns per-step records (NEGF iterations, surrogate
+    iterations, whether the surrogate start was used, seconds, charge)."""
     import torch
     from . import negf as ng
     N = tube.num_field_sites
@@ -328,8 +424,9 @@ def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e
     out = []
     with torch.cuda.stream(stream):
         Q = torch.zeros(N, dtype=torch.float64, device=dev)
-        br = ng.Broyden(torch.zeros(N, dtype=torch.float64, device=dev), max_step=max_step, fraction=fraction,
-                        stream=stream)
+        # history capacity for both phases; the NEGF phase alone stays within max_step
+        br = ng.Broyden(torch.zeros(N, dtype=torch.float64, device=dev), max_step=max_step + surrogate_max_step,
+                        fraction=fraction, stream=stream)
         nin = br.input_device_ptr()
         nin_t = __import__("electrostatic_b200.scf", fromlist=["device_view"]).device_view(nin, N)
         Kd, U0 = electro.device_operator(0.0)
@@ -355,26 +452,49 @@ def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e
             with torch.cuda.graph(graph, stream=stream):
                 for _ in range(iters_per_graph):
                     body(torch.cuda.current_stream())
+        sgraph = None
+        if model is not None:
+            # the surrogate phase: potential -> surrogate charge -> Broyden step, captured
+            Qs = torch.zeros(N, dtype=torch.float64, device=dev)
+            flags_s = torch.zeros(8, dtype=torch.int32, device=dev)
+            model.bind(Uview, 0.0, Vds, Qs)
+
+            def sbody(s):
+                ng.affine_potential_masked(Kd, U0, nin, Up, N, flags_s.data_ptr() + 12, stream=s)
+                model.infer()
+                br.step_device(Qs, surrogate_norm, flags_s, stream=s)
+
+            flags_s[3] = 1
+            sbody(stream)  # allocates the model's buffers outside the capture
+            stream.synchronize()
+            sgraph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(sgraph, stream=stream):
+                for _ in range(iters_per_graph):
+                    sbody(torch.cuda.current_stream())
         for Vg in Vg_list:
             U0.copy_(electro.device_operator(Vg)[1])
             flags.zero_()
             stream.synchronize()
             t0 = time.perf_counter()
             sur_it = 0
+            used = False
             if model is not None:
-                vg_t = torch.tensor([float(Vg)], device=dev)
-                vd_t = torch.tensor([float(Vds)], device=dev)
-                flags_s = torch.zeros(8, dtype=torch.int32, device=dev)
+                model.set_bias(Vg, Vds)
+                flags_s.zero_()
                 while True:
-                    ng.affine_potential_masked(Kd, U0, nin, Up, N, None, stream=stream)
-                    Qs = model.predict(Uview.float()[None, :], vg_t, vd_t, batch=1)[0]
-                    Q.copy_(Qs)
-                    br.step_device(Q, surrogate_norm, flags_s, stream=stream)
-                    sur_it += 1
+                    sgraph.replay()
                     f = flags_s.cpu().numpy()
+                    sur_it = int(f[1])
                     if f[3] or sur_it >= surrogate_max_step:
                         break
-                # continue the same Broyden with the NEGF charge
+                used = bool(f[0]) and not f[2]
+                if not used:  # discard the surrogate phase
+                    br.reset(stream=stream)
+                elif not keep_history:
+                    nkeep = nin_t.clone()
+                    br.reset(stream=stream)
+                    nin_t.copy_(nkeep)
+                # the NEGF phase continues from here
             while True:
                 if graph is not None:
                     graph.replay()
@@ -386,11 +506,12 @@ def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e
             dt = time.perf_counter() - t0
             if f[2]:
                 raise RuntimeError("NEGF self-consistency failed (flag %d)" % f[2])
-            out.append(dict(Vg=float(Vg), negf_iterations=int(f[1]), surrogate_iterations=sur_it, seconds=dt,
-                            Q=Q.cpu().numpy().copy()))
+            out.append(dict(Vg=float(Vg), negf_iterations=int(f[1]), surrogate_iterations=sur_it,
+                            surrogate_used=used, seconds=dt, Q=Q.cpu().numpy().copy()))
             br.reset(stream=stream)
         stream.synchronize()
     del graph
+    del sgraph
     plan.close()
     br.close()
     return out

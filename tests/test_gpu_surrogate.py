@@ -88,3 +88,25 @@ def test_training_reduces_loss():
     assert r["loss"][-1] < 0.2 * r["loss"][0]
     pred = m.predict(U, Vg, Vds)
     assert pred.shape == Q.shape and torch.isfinite(pred).all()
+
+
+def test_surrogate_started_sweep_is_judged_by_negf():
+    """Pipeline on a small tube: pairs from self-consistent solves of the
+    engine, a short training, and a surrogate-started gate sweep whose
+    converged charges are NEGF fixed points (same tolerance as the plain
+    sweep)."""
+    import numpy as np
+    from electrostatic_b200 import surrogate as S
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import gate_with_contacts
+    U, Vg, Vds, Q, _ = S.generate_scf_pairs(96, unitcells=32, modes=2, vds_bins=3)
+    assert U.shape == (96, 128) and np.isfinite(Q.cpu().numpy()).all()
+    m = S.FourierOperator(128, seed=0)
+    m.fit(U, Vg, Vds, Q, epochs=4, batch=8)
+    tube = CNT(**S.tube_kwargs(0.3, unitcells=32, modes=2))
+    R = 1.42e-10 * np.sqrt(3.0) * 17 / (2 * np.pi)
+    el = gate_with_contacts(tube.site_positions(), R, vds=0.3)
+    plain = S.scf_sweep(tube, el, [0.1, 0.3], 0.3)
+    sur = S.scf_sweep(tube, el, [0.1, 0.3], 0.3, model=m, keep_history=False)
+    for a, b in zip(plain, sur):
+        assert np.max(np.abs(a["Q"] - b["Q"])) < 1e-5
