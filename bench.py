@@ -317,6 +317,44 @@ def config3_measure(torch, passes=2):
             "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm)))}
 
 
+def long_tube_measure(torch, reps=10):
+    """Parallel in length: a 64000-site (17,0) tube with 2 modes and 96
+    energies (few chains for a whole GPU), pass-1 sweeps as one piece per
+    chain against the automatic split into pieces; device times by CUDA
+    events of the charge pass."""
+    from electrostatic_b200 import _lib
+    from electrostatic_b200.negf import CNT, last_stats, set_timing
+    from electrostatic_b200.workloads import SEED_BASE, site_potential
+    t = CNT(type_id=(17, 0), num_unitcells=16000, num_modes=2, contact_mu=(0.0, -0.2), contact_T=(300.0, 300.0),
+            eq_integration_pts=(8, 8, 16), noneq_integration_pts=(64,), E_zPlus_imag=1e-3)
+    U = site_potential(t.site_positions(), SEED_BASE + 4)
+    U = 0.5 * (U - U.mean())
+    t.set_potential(U, (U[0], U[-1]))
+    L = _lib.load()
+    set_timing(True)
+    res = {}
+    try:
+        for name, P in (("one_piece", 1), ("automatic", 0)):
+            L.negf_set_tuning(4, P)
+            for _ in range(3):
+                Q = t.Solve_NEGF()
+            ms = []
+            for _ in range(reps):
+                Q = t.Solve_NEGF()
+                ms.append(last_stats()["rgf_kernel_ms"] + last_stats()["reduce_kernel_ms"])
+            st = last_stats()
+            res[name] = {"ms_per_pass": float(np.median(ms)), "pieces": st["pieces"],
+                         "updates_per_s": st["updates"] / (float(np.median(ms)) * 1e-3), "Q": Q}
+    finally:
+        L.negf_set_tuning(4, 0)
+        set_timing(False)
+    Q1, Qa = res["one_piece"].pop("Q"), res["automatic"].pop("Q")
+    return {"workload": "(17,0) CNT, N=64000 sites, 2 modes, 96 energies (contour+poles+real axis), FP64",
+            "one_piece": res["one_piece"], "automatic": res["automatic"],
+            "speedup": res["one_piece"]["ms_per_pass"] / res["automatic"]["ms_per_pass"],
+            "max_rel_automatic_vs_one_piece": float(np.max(np.abs(Qa - Q1)) / np.max(np.abs(Q1)))}
+
+
 def config5_measure(torch, n_pairs=8000, epochs=15):
     """Surrogate-started self-consistency on the 4000-site, 8-mode (17,0) tube
     (Vds 0.4 V, gate 0 -> 0.6 V): pairs recorded along plain NEGF solves,
@@ -374,6 +412,7 @@ def main():
     ap.add_argument("--no-scf", action="store_true")
     ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--no-config3", action="store_true")
+    ap.add_argument("--no-long-tube", action="store_true")
     ap.add_argument("--config5", action="store_true", help="surrogate study (about two minutes, off by default)")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis)")
@@ -511,6 +550,7 @@ def main():
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
         cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch)
+        longt = None if (args.no_long_tube or world > 1) else long_tube_measure(torch)
         cfg5 = config5_measure(torch) if (args.config5 and world == 1) else None
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                 "frac": achieved_tf / peak_tf if peak_tf else None,
@@ -529,7 +569,7 @@ def main():
                 "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
                            "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config3": cfg3, "config4": cfg4, "config5": cfg5,
+                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config3": cfg3, "config4": cfg4, "long_tube": longt, "config5": cfg5,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
                         "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},

@@ -90,6 +90,7 @@ class Stats(C.Structure):
         ("warps", C.c_int),
         ("units", C.c_int),
         ("kernel_launches", C.c_int),
+        ("pieces", C.c_int),
         ("checkpoint_bytes", C.c_longlong),
     ]
 

@@ -210,7 +210,7 @@ namespace {
 
 std::mutex g_mu;
 struct Workspace {
-    DevBuf tubes, chains, warps, rts, units, partial, scratch, qbuf;
+    DevBuf tubes, chains, warps, rts, units, partial, scratch, qbuf, pieces;
     // cached chain table
     std::vector<const negf_tube*> key_tubes;
     std::vector<int> key_versions;
@@ -223,6 +223,7 @@ struct Workspace {
     negf_stats stats{};
     bool stats_pending = false;
     int warps_per_block = 4;
+    int pass1_pieces = 0;  // 0: automatic
 };
 Workspace& ws() {
     static Workspace w;
@@ -534,6 +535,19 @@ void build_tube_chains(Out<negf::ChainRec>& chains, Out<negf::WarpRec>& warps, T
         }
 }
 
+// Streaming multiprocessors of the current device (cached per ordinal).
+int device_sm_count() {
+    static int cache[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cache[dev] = v;
+    }
+    return cache[dev];
+}
+
 // Launch tables of a set of tube passes.  Launch order: longest tubes first
 // (order[] is caller scratch of passes.size() ints); rts[i] describes pass i.
 void build_table_generic(const TubePass* passes, int num_passes, int* order, Out<negf::ChainRec>& chains,
@@ -636,9 +650,21 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
             if (!e) NEGF_CUDA(cudaEventCreate(&e));
         NEGF_CUDA(cudaEventRecord(W.ev[0], stream));
     }
+    // parallel in length when the chains alone cannot fill the GPU: about 8
+    // one-warp blocks per SM, pieces of >= 32 segments, at most 128 pieces
+    // (the prefix over the pieces is sequential per chain)
+    int pieces = W.pass1_pieces;
+    if (pieces == 0) {
+        const int target = 8 * device_sm_count();
+        const int maxp = std::min(128, std::max(1, ((ct.max_N + negf::kSeg - 1) / negf::kSeg) / 32));
+        pieces = nw >= target / 2 ? 1 : std::min(maxp, (target + nw - 1) / std::max(nw, 1));
+    }
+    pieces = std::max(1, pieces);
+    if (pieces > 1) NEGF_CUDA(W.pieces.reserve(sizeof(double) * (size_t)nw * pieces * 24 * negf::kWarp));
     NEGF_CUDA(negf::launch_rgf(W.tubes.as<negf::TubeDev>(), W.chains.as<negf::ChainRec>(), W.warps.as<negf::WarpRec>(),
                                nw, W.units.as<negf::SegUnit>(), (int)ct.units.size(), W.partial.as<double>(),
-                               W.scratch.p, W.warps_per_block, stream, W.timing ? W.ev[3] : nullptr));
+                               W.scratch.p, W.warps_per_block, stream, W.timing ? W.ev[3] : nullptr, nullptr, pieces,
+                               W.pieces.as<double>()));
     if (W.timing) NEGF_CUDA(cudaEventRecord(W.ev[1], stream));
     NEGF_CUDA(negf::launch_reduce(W.rts.as<negf::ReduceTube>(), (int)ct.rts.size(), ct.max_N, W.partial.as<double>(),
                                   d_Q, stream));
@@ -651,7 +677,8 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
     st.realaxis_updates = ct.realaxis_updates;
     st.chains = (int)ct.chains.size();
     st.warps = nw;
-    st.kernel_launches = (nw > 0 ? 2 : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
+    st.kernel_launches = (nw > 0 ? (pieces > 1 ? 4 : 2) : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
+    st.pieces = pieces;
     st.units = (int)ct.units.size();
     st.checkpoint_bytes = 2 * ct.scratch_doubles * 8;
     W.stats_pending = W.timing;
@@ -1350,6 +1377,10 @@ int negf_set_tuning(int key, int value) {
         case NEGF_TUNE_PASS2_WARPS_PER_BLOCK:
             if (value != 1 && value != 2 && value != 4) return fail(NEGF_ERR_ARG, "warps per block must be 1, 2 or 4");
             W.warps_per_block = value;
+            return NEGF_OK;
+        case NEGF_TUNE_PASS1_PIECES:
+            if (value < 0 || value > 4096) return fail(NEGF_ERR_ARG, "pieces must be in [0, 4096] (0: automatic)");
+            W.pass1_pieces = value;
             return NEGF_OK;
         default:
             return fail(NEGF_ERR_ARG, "unknown tuning key");

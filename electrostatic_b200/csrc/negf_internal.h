@@ -113,7 +113,8 @@ cudaError_t nn_mse(long long n, const float* q, const float* y, float* d, float*
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
                        int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event,
-                       const int* skip = nullptr);
+                       const int* skip = nullptr, int pieces = 1, double* d_piece_work = nullptr);
+// pieces > 1 (parallel in length): d_piece_work holds num_warps * pieces * 24 * 32 doubles.
 // Device self-test of numeric primitives: which = 0 FP64 reciprocal,
 // 1 FP32 reciprocal (input/output as doubles), n values, device pointers.
 cudaError_t selftest(int which, int n, const double* d_in, double* d_out, cudaStream_t stream);

@@ -307,18 +307,18 @@ __device__ __forceinline__ void proj_scale(Proj<R>& p) {
 }
 
 // One block of pass 1: checkpoint both sweeps at their segment boundaries,
-// prefetch the potentials of the next block into (nf, nb), then advance the
-// forward sweep through segment blk and the backward sweep through segment
-// nseg-1-blk.  INTERIOR: the caller guarantees 1 <= blk <= nseg-2 (both
-// segments full, neither holding a contact site).
+// prefetch the potentials of the next block (forward segment fs+1, backward
+// segment bs-1) into (nf, nb) when has_next, then advance the forward sweep
+// through segment fs and the backward sweep through segment bs.  INTERIOR:
+// the caller guarantees that both segments are full and hold no contact site
+// and that a next block exists.
 template <typename R, bool RA, bool INTERIOR>
-__device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<R>& b, int blk, int nseg,
+__device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<R>& b, int fs, int bs, bool has_next,
                                             const double* __restrict__ U, R* __restrict__ ck, const R (&uf)[kSeg],
                                             const R (&ub)[kSeg], R (&nf)[kSeg], R (&nb)[kSeg], R hfull) {
     constexpr int K = kSeg;
     using CL = CkLayout<RA>;
     const int N = c.N;
-    const int fs = blk, bs = nseg - 1 - blk;
     const int f0 = fs * K;                  // forward segment start
     const int be = min(bs * K + K, N) - 1;  // backward segment end
     {
@@ -334,7 +334,7 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
         q[(CL::X + 1) * kWarp] = xi;
         if (RA) q[CL::RHO * kWarp] = b.lam;
     }
-    if (INTERIOR || blk + 1 < nseg) {
+    if (INTERIOR || has_next) {
         // next forward segment fs+1 and next backward segment bs-1 (full, bs >= 1):
         // 16-byte aligned, inside the padded buffer
         const double2* pf = reinterpret_cast<const double2*>(U + f0 + K);
@@ -392,61 +392,79 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
     }
 }
 
-// Pass 1: lead self-energies (FP64, stored for pass 2), then the forward
-// (Y, lambda) and backward (X, rho) sweeps of one chain run together (they
-// are independent), in projective form, storing the state at every segment
-// start (forward) and segment end (backward).
+// Initial sweep states of one piece of a chain (FP64): forward (Y, lambda)
+// at the piece's first site, backward (X, rho) at its last site.
+struct PieceState {
+    double yr, yi, lam, xr, xi, rho;
+};
+
+// Pass 1 over segments [s0, s1) of a chain: lead self-energies (FP64; the
+// piece holding site 0 stores them for pass 2), then the forward (Y, lambda)
+// and backward (X, rho) sweeps run together (they are independent), in
+// projective form, from the piece's initial states, storing the state at
+// every segment start (forward) and segment end (backward).  The whole chain
+// is the single piece [0, nseg) with Y_0 = 0, lambda_0 = 1, X_{N-1} = 0,
+// rho_{N-1} = 1.
 template <typename R, bool RA>
 __device__ __forceinline__ void pass1_chain(const TubeDev* __restrict__ tubes, const ChainRec& cr, int tube,
-                                            double* __restrict__ wscratch, int lane) {
+                                            double* __restrict__ wscratch, int lane, int s0, int s1,
+                                            const PieceState& st) {
     constexpr int K = kSeg;
     static_assert(K % 2 == 0, "segment length must be even");
     const TubeDev& T = tubes[tube];
     const int N = T.N;
+    const int nseg = (N + K - 1) / K;
+    if (s1 <= s0) return;
     const double* __restrict__ U = T.U;
     const bool valid = cr.mode >= 0;
     const double beta = T.beta[valid ? cr.mode : 0];
     const cd E = {cr.Er, cr.Ei};
-    // U_contact = U at the end sites (Nanostructure.cpp:500-504) when read on the device
-    const double Uc0 = T.uc_from_U ? U[0] : T.Uc0, Uc1 = T.uc_from_U ? U[N - 1] : T.Uc1;
-    const cd S0 = sigma_contact(E, Uc0, beta, T);
-    const cd S1 = sigma_contact(E, Uc1, beta, T);
-    wscratch[0 * kWarp + lane] = S0.x;
-    wscratch[1 * kWarp + lane] = S0.y;
-    wscratch[2 * kWarp + lane] = S1.x;
-    wscratch[3 * kWarp + lane] = S1.y;
+    cd S0 = {0.0, 0.0}, S1 = {0.0, 0.0};
+    if (s0 == 0 || s1 == nseg) {  // the contact sites lie in the first and the last piece
+        // U_contact = U at the end sites (Nanostructure.cpp:500-504) when read on the device
+        const double Uc0 = T.uc_from_U ? U[0] : T.Uc0, Uc1 = T.uc_from_U ? U[N - 1] : T.Uc1;
+        S0 = sigma_contact(E, Uc0, beta, T);
+        S1 = sigma_contact(E, Uc1, beta, T);
+    }
+    if (s0 == 0) {
+        wscratch[0 * kWarp + lane] = S0.x;
+        wscratch[1 * kWarp + lane] = S0.y;
+        wscratch[2 * kWarp + lane] = S1.x;
+        wscratch[3 * kWarp + lane] = S1.y;
+    }
     const Chain<R> c = make_chain<R, RA>(T, cr, S0.x, S0.y, S1.x, S1.y);
     R* __restrict__ ck = reinterpret_cast<R*>(wscratch + 4 * kWarp) + lane;
-    Proj<R> f{0, 0, 1, 0, 1, 1, 1};  // Y_0 = 0, lambda_0 = 1
-    Proj<R> b{0, 0, 1, 0, 1, 1, 1};  // X_{N-1} = 0, rho_{N-1} = 1
-    R hfull = 1;                     // prod of h^2 over a full segment
+    Proj<R> f{(R)st.yr, (R)st.yi, 1, 0, (R)st.lam, 1, 1};
+    Proj<R> b{(R)st.xr, (R)st.xi, 1, 0, (R)st.rho, 1, 1};
+    R hfull = 1;  // prod of h^2 over a full segment
 #pragma unroll
     for (int j = 0; j < K / 2; ++j) hfull *= c.hb2 * c.hg2;
-    const int nseg = (N + K - 1) / K;
-    // potentials of the first block: forward segment 0, backward segment nseg-1
+    const int nb = s1 - s0;
+    const int e = min(s1 * K, N) - 1;  // the piece's last site
+    // potentials of the first block: forward segment s0, backward segment s1-1
     // (the buffer has kPadLo zeros before site 0 and kPadHi after site N-1)
     R ua_f[K], ua_b[K], ub_f[K], ub_b[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) {
-        ua_f[j] = (R)__ldg(U + j);
-        ua_b[j] = (R)__ldg(U + (N - 1) - j);
+        ua_f[j] = (R)__ldg(U + s0 * K + j);
+        ua_b[j] = (R)__ldg(U + e - j);
     }
-    // Block 0 and block nseg-1 hold the contact sites (and a partial last
-    // segment); blocks 1 .. nseg-2 are interior for both sweeps and run in a
+    // Block k advances forward segment s0+k and backward segment s1-1-k.
+    // Blocks 1 .. nb-2 never touch the contact segments and run in a
     // branch-free loop, two blocks per trip with the potential buffers
-    // alternating.
-    pass1_block<R, RA, false>(c, f, b, 0, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
-    if (nseg == 1) return;
-    int blk = 1;
-    for (; blk + 2 <= nseg - 1; blk += 2) {
-        pass1_block<R, RA, true>(c, f, b, blk, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
-        pass1_block<R, RA, true>(c, f, b, blk + 1, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+    // alternating; the first and last blocks decide at run time.
+    pass1_block<R, RA, false>(c, f, b, s0, s1 - 1, nb > 1, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+    if (nb == 1) return;
+    int k = 1;
+    for (; k + 2 <= nb - 1; k += 2) {
+        pass1_block<R, RA, true>(c, f, b, s0 + k, s1 - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+        pass1_block<R, RA, true>(c, f, b, s0 + k + 1, s1 - 2 - k, true, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
     }
-    if (blk < nseg - 1) {
-        pass1_block<R, RA, true>(c, f, b, blk, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
-        pass1_block<R, RA, false>(c, f, b, nseg - 1, nseg, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+    if (k < nb - 1) {
+        pass1_block<R, RA, true>(c, f, b, s0 + k, s1 - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+        pass1_block<R, RA, false>(c, f, b, s1 - 1, s0, false, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
     } else {
-        pass1_block<R, RA, false>(c, f, b, nseg - 1, nseg, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+        pass1_block<R, RA, false>(c, f, b, s1 - 1, s0, false, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
     }
 }
 
@@ -647,28 +665,251 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
     }
 }
 
-// One warp (32 chains) per block: the latency-bound sweeps spread evenly over the SMs.
+// Segments [s0, s1) of piece p of P on a tube of nseg segments.
+__device__ __forceinline__ void piece_range(int nseg, int P, int p, int& s0, int& s1) {
+    s0 = (int)((long long)p * nseg / P);
+    s1 = (int)((long long)(p + 1) * nseg / P);
+}
+
+// One warp (32 chains, one piece of them) per block: the latency-bound
+// sweeps spread evenly over the SMs.  pieces > 1: block u = warp * pieces +
+// piece, initial states from states[warp][piece][component][lane].
 __global__ void __launch_bounds__(32) rgf_pass1_kernel(const TubeDev* __restrict__ tubes,
                                                        const ChainRec* __restrict__ chains,
                                                        const WarpRec* __restrict__ warps, int num_warps,
-                                                       double* __restrict__ scratch, const int* __restrict__ skip) {
+                                                       double* __restrict__ scratch, const int* __restrict__ skip,
+                                                       int pieces, const double* __restrict__ states) {
     if (skip && *skip) return;
     const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x;
+    const int w = blockIdx.x / pieces, p = blockIdx.x % pieces;
     if (w >= num_warps) return;
     const WarpRec wr = warps[w];
     const ChainRec c = chains[(size_t)w * kWarp + lane];
     double* ws = scratch + wr.ck_off;
+    const int nseg = (tubes[wr.tube].N + kSeg - 1) / kSeg;
+    int s0 = 0, s1 = nseg;
+    PieceState st{0.0, 0.0, 1.0, 0.0, 0.0, 1.0};
+    if (pieces > 1) {
+        piece_range(nseg, pieces, p, s0, s1);
+        const double* q = states + ((size_t)w * pieces + p) * 6 * kWarp + lane;
+        st = PieceState{q[0], q[kWarp], q[2 * kWarp], q[3 * kWarp], q[4 * kWarp], q[5 * kWarp]};
+    }
     if (wr.fp32) {
         if (wr.kind == kRealAxis)
-            pass1_chain<float, true>(tubes, c, wr.tube, ws, lane);
+            pass1_chain<float, true>(tubes, c, wr.tube, ws, lane, s0, s1, st);
         else
-            pass1_chain<float, false>(tubes, c, wr.tube, ws, lane);
+            pass1_chain<float, false>(tubes, c, wr.tube, ws, lane, s0, s1, st);
     } else {
         if (wr.kind == kRealAxis)
-            pass1_chain<double, true>(tubes, c, wr.tube, ws, lane);
+            pass1_chain<double, true>(tubes, c, wr.tube, ws, lane, s0, s1, st);
         else
-            pass1_chain<double, false>(tubes, c, wr.tube, ws, lane);
+            pass1_chain<double, false>(tubes, c, wr.tube, ws, lane, s0, s1, st);
+    }
+}
+
+// 2 x 2 complex matrix, row-major: (a b; c d)
+struct M2 {
+    cd a, b, c, d;
+};
+__device__ __forceinline__ cd cmulz(cd x, cd y) { return {fma(x.x, y.x, -x.y * y.y), fma(x.x, y.y, x.y * y.x)}; }
+// (0 h2; -1 al) * M
+__device__ __forceinline__ M2 step_left(double h2, cd al, const M2& m) {
+    M2 r;
+    r.a = {h2 * m.c.x, h2 * m.c.y};
+    r.b = {h2 * m.d.x, h2 * m.d.y};
+    const cd ac = cmulz(al, m.c), ad = cmulz(al, m.d);
+    r.c = {ac.x - m.a.x, ac.y - m.a.y};
+    r.d = {ad.x - m.b.x, ad.y - m.b.y};
+    return r;
+}
+// Scale m by a power of two so that its largest |re| + |im| lies in [1, 2);
+// the exponent goes to e (exact: no rounding from the rescaling).
+__device__ __forceinline__ void normalise(M2& m, int& e) {
+    const double s = fmax(fmax(fabs(m.a.x) + fabs(m.a.y), fabs(m.b.x) + fabs(m.b.y)),
+                          fmax(fabs(m.c.x) + fabs(m.c.y), fabs(m.d.x) + fabs(m.d.y)));
+    const int be = (int)((__double_as_longlong(s) >> 52) & 0x7ff);  // biased exponent of s
+    if (be == 0 || be == 0x7ff) return;                              // zero, subnormal, inf or NaN: leave as is
+    const double f = __longlong_as_double((long long)(2046 - be) << 52);  // 2^-(be - 1023)
+    m.a = {m.a.x * f, m.a.y * f};
+    m.b = {m.b.x * f, m.b.y * f};
+    m.c = {m.c.x * f, m.c.y * f};
+    m.d = {m.d.x * f, m.d.y * f};
+    e += be - 1023;
+}
+
+// Transfer matrices of one piece of a chain (FP64): forward
+// (P, Q)_{piece end} = Mf (P, Q)_{piece start} with (P, Q) <- (h_n^2 Q,
+// alpha_n Q - P) for every forward step of the piece, and backward
+// (R, S)_{before the piece} = Mb (R, S)_{piece end} with (R, S) <-
+// (h_{m-1}^2 S, alpha_m S - R).  Block k advances the forward product
+// through segment s0+k and the backward one through segment s1-1-k (the two
+// are independent and interleave), with the next block's potentials loaded
+// ahead; both are rescaled by powers of two every segment.
+// out[warp][piece][18][lane]: Mf (8), log2 scale of Mf, Mb (8), log2 scale of Mb.
+__global__ void __launch_bounds__(32) rgf_piece_transfer_kernel(const TubeDev* __restrict__ tubes,
+                                                                const ChainRec* __restrict__ chains,
+                                                                const WarpRec* __restrict__ warps, int num_warps,
+                                                                int pieces, double* __restrict__ out) {
+    constexpr int K = kSeg;
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x / pieces, p = blockIdx.x % pieces;
+    if (w >= num_warps) return;
+    const WarpRec wr = warps[w];
+    const ChainRec cr = chains[(size_t)w * kWarp + lane];
+    const TubeDev& T = tubes[wr.tube];
+    const int N = T.N, nseg = (N + K - 1) / K;
+    int s0, s1;
+    piece_range(nseg, pieces, p, s0, s1);
+    const int nb = s1 - s0;
+    const bool valid = cr.mode >= 0;
+    const double beta = T.beta[valid ? cr.mode : 0];
+    const double hb2 = beta * beta, hg2 = T.gamma * T.gamma;
+    const cd E = {cr.Er, cr.Ei};
+    const double* __restrict__ U = T.U;
+    cd S0 = {0.0, 0.0}, S1 = {0.0, 0.0};
+    if (nb > 0 && (s0 == 0 || s1 == nseg)) {
+        const double Uc0 = T.uc_from_U ? U[0] : T.Uc0, Uc1 = T.uc_from_U ? U[N - 1] : T.Uc1;
+        S0 = sigma_contact(E, Uc0, beta, T);
+        S1 = sigma_contact(E, Uc1, beta, T);
+    }
+    M2 mf{{1.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {1.0, 0.0}}, mb = mf;
+    int ef = 0, eb = 0;
+    double uf[K], ub[K];
+    if (nb > 0) {
+        const int e = min(s1 * K, N) - 1;  // the piece's last site
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            uf[j] = __ldg(U + s0 * K + j);
+            ub[j] = __ldg(U + e - j);
+        }
+    }
+    for (int k = 0; k < nb; ++k) {
+        const int f0 = (s0 + k) * K;
+        const int b0 = (s1 - 1 - k) * K;           // backward segment start
+        const int be = min(b0 + K, N) - 1;         // backward segment end
+        double nf[K], nbk[K];
+        if (k + 1 < nb) {
+            // next forward segment and next backward segment (full): 16-byte
+            // aligned, inside the padded buffer
+            const double2* pf = reinterpret_cast<const double2*>(U + f0 + K);
+            const double2* pb = reinterpret_cast<const double2*>(U + b0 - K);
+#pragma unroll
+            for (int q = 0; q < K / 2; ++q) {
+                const double2 vf = __ldg(pf + q), vb = __ldg(pb + q);
+                nf[2 * q] = vf.x;
+                nf[2 * q + 1] = vf.y;
+                nbk[K - 1 - 2 * q] = vb.x;
+                nbk[K - 2 - 2 * q] = vb.y;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            const int n = f0 + j;
+            if (n < N - 1) {  // forward step at site n
+                cd al = {E.x - uf[j], E.y};
+                if (n == 0) al = {al.x - S0.x, al.y - S0.y};
+                mf = step_left((j & 1) ? hg2 : hb2, al, mf);
+            }
+            const int m = be - j;
+            if (m >= b0 && m >= 1) {  // backward step at site m: M <- S_m M
+                cd al = {E.x - ub[j], E.y};
+                if (m == N - 1) al = {al.x - S1.x, al.y - S1.y};
+                mb = step_left(((m - 1) & 1) ? hg2 : hb2, al, mb);
+            }
+        }
+        normalise(mf, ef);
+        normalise(mb, eb);
+        if (k + 1 < nb) {
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                uf[j] = nf[j];
+                ub[j] = nbk[j];
+            }
+        }
+    }
+    double* o = out + ((size_t)w * pieces + p) * 18 * kWarp + lane;
+    const double v[18] = {mf.a.x, mf.a.y, mf.b.x, mf.b.y, mf.c.x, mf.c.y, mf.d.x, mf.d.y, (double)ef,
+                          mb.a.x, mb.a.y, mb.b.x, mb.b.y, mb.c.x, mb.c.y, mb.d.x, mb.d.y, (double)eb};
+#pragma unroll
+    for (int q = 0; q < 18; ++q) o[q * kWarp] = v[q];
+}
+
+// One transfer matrix applied to the state (Z, 1): the new ratio Z' = top /
+// bottom and log |bottom| (natural log) including the matrix's scale 2^e.
+__device__ __forceinline__ void apply_transfer(const double (&t)[9], cd& Z, double& L) {
+    const cd a = {t[0], t[1]}, b = {t[2], t[3]}, c = {t[4], t[5]}, d = {t[6], t[7]};
+    const cd az = cmulz(a, Z), cz = cmulz(c, Z);
+    const cd top = {az.x + b.x, az.y + b.y}, bot = {cz.x + d.x, cz.y + d.y};
+    const double q2 = bot.x * bot.x + bot.y * bot.y;
+    L += t[8] * 0.69314718055994530942 + 0.5 * log(q2);
+    const double iq = 1.0 / q2;
+    Z = {(top.x * bot.x + top.y * bot.y) * iq, (top.y * bot.x - top.x * bot.y) * iq};
+}
+
+// Per chain: the forward state (Y, lambda) at each piece's first site and the
+// backward state (X, rho) at each piece's last site, from the transfer
+// matrices; lambda_n = prod_{m<n} h_m^2 / |Q_n|^2 with Q_0 = 1, rho_n =
+// prod_{n<=m<N-1} h_m^2 / |S_n|^2 with S_{N-1} = 1, in logarithms.  The
+// forward scan (ascending pieces) and the backward one (descending)
+// interleave, the next matrices loaded ahead.
+__global__ void __launch_bounds__(32) rgf_piece_prefix_kernel(const TubeDev* __restrict__ tubes,
+                                                              const ChainRec* __restrict__ chains,
+                                                              const WarpRec* __restrict__ warps, int num_warps,
+                                                              int pieces, const double* __restrict__ tm,
+                                                              double* __restrict__ states) {
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x;
+    if (w >= num_warps) return;
+    const WarpRec wr = warps[w];
+    const ChainRec cr = chains[(size_t)w * kWarp + lane];
+    const TubeDev& T = tubes[wr.tube];
+    const int N = T.N, nseg = (N + kSeg - 1) / kSeg;
+    const bool valid = cr.mode >= 0;
+    const double beta = T.beta[valid ? cr.mode : 0];
+    const double lhb = log(fmax(beta * beta, 1e-300)), lhg = log(T.gamma * T.gamma);
+    // sum_{m < n} log h_m^2: sites of even index carry beta
+    auto hsum = [&](int n) { return ((n + 1) / 2) * lhb + (n / 2) * lhg; };
+    auto clampexp = [](double x) { return exp(fmin(fmax(x, -700.0), 700.0)); };
+    const double hall = hsum(N - 1);
+    const double* base = tm + (size_t)w * pieces * 18 * kWarp + lane;
+    auto load = [&](int p, int half, double (&t)[9]) {
+        const double* q = base + ((size_t)p * 18 + half * 9) * kWarp;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) t[i] = q[i * kWarp];
+    };
+    cd Y = {0.0, 0.0}, X = {0.0, 0.0};
+    double Lf = 0.0, Lb = 0.0;
+    double tf[9], tb[9];
+    load(0, 0, tf);
+    load(pieces - 1, 1, tb);
+    for (int i = 0; i < pieces; ++i) {
+        const int pf = i, pb = pieces - 1 - i;
+        double nf[9], nb[9];
+        if (i + 1 < pieces) {
+            load(pf + 1, 0, nf);
+            load(pb - 1, 1, nb);
+        }
+        int s0, s1;
+        piece_range(nseg, pieces, pf, s0, s1);
+        double* st = states + ((size_t)w * pieces + pf) * 6 * kWarp + lane;
+        st[0] = Y.x;
+        st[kWarp] = Y.y;
+        st[2 * kWarp] = valid ? clampexp(hsum(s0 * kSeg) - 2.0 * Lf) : 1.0;
+        apply_transfer(tf, Y, Lf);
+        piece_range(nseg, pieces, pb, s0, s1);
+        const int e = min(s1 * kSeg, N) - 1;
+        st = states + ((size_t)w * pieces + pb) * 6 * kWarp + lane;
+        st[3 * kWarp] = X.x;
+        st[4 * kWarp] = X.y;
+        st[5 * kWarp] = valid ? clampexp(hall - hsum(e) - 2.0 * Lb) : 1.0;
+        apply_transfer(tb, X, Lb);
+        if (i + 1 < pieces) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                tf[q] = nf[q];
+                tb[q] = nb[q];
+            }
+        }
     }
 }
 
@@ -940,12 +1181,30 @@ int rgf_kernel_regs() {
 
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
-                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event, const int* skip) {
+                       int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event, const int* skip, int pieces,
+                       double* d_piece_work) {
     if (num_warps <= 0) return cudaSuccess;
     if (warps_per_block < 1 || warps_per_block > 4) warps_per_block = 4;
+    double* states = nullptr;
+    if (pieces > 1) {
+        // parallel in length: transfer matrices per piece, prefix per chain, then the pieces' sweeps
+        double* tm = d_piece_work;
+        states = d_piece_work + (size_t)num_warps * pieces * 18 * kWarp;
+        rgf_piece_transfer_kernel<<<num_warps * pieces, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
+                                                                            pieces, tm);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        rgf_piece_prefix_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps, pieces, tm,
+                                                                 states);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    } else {
+        pieces = 1;
+    }
     // pass 1 is latency-bound: one warp per block spreads the chains evenly over the SMs
-    rgf_pass1_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
-                                                        static_cast<double*>(d_scratch), skip);
+    rgf_pass1_kernel<<<num_warps * pieces, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
+                                                                 static_cast<double*>(d_scratch), skip, pieces,
+                                                                 states);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (mid_event) cudaEventRecord(mid_event, stream);
@@ -975,7 +1234,7 @@ cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, c
                              double* d_red, double* d_ldos, int N, cudaStream_t stream) {
     if (num_warps <= 0) return cudaSuccess;
     rgf_pass1_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
-                                                        static_cast<double*>(d_scratch), nullptr);
+                                                        static_cast<double*>(d_scratch), nullptr, 1, nullptr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     rgf_transport_kernel<<<num_units, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, d_units, num_units,

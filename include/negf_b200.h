@@ -178,13 +178,23 @@ typedef struct negf_stats {
     int warps;                 /* pass-1 warps launched */
     int units;                 /* pass-2 warps (segment groups) launched */
     int kernel_launches;       /* kernels launched by the call */
+    int pieces;                /* pass-1 pieces per chain (parallel in length) */
     long long checkpoint_bytes;/* scratch bytes written+read by the kernel */
 } negf_stats;
 int negf_last_stats(negf_stats* s);
-/* Launch-shape knobs of negf_compute_charge (results are bitwise identical
- * for every setting; only speed changes).
- * NEGF_TUNE_PASS2_WARPS_PER_BLOCK: 1, 2 or 4 (default) warps per pass-2 block. */
+/* Launch-shape knobs of negf_compute_charge.
+ * NEGF_TUNE_PASS2_WARPS_PER_BLOCK: 1, 2 or 4 (default) warps per pass-2
+ *   block; results are bitwise identical for every setting.
+ * NEGF_TUNE_PASS1_PIECES: 0 (default, automatic) or P >= 1: the forward and
+ *   backward sweeps of every chain run as P pieces of the tube in parallel
+ *   ("parallel in length", for long tubes with few energies): 2 x 2 transfer
+ *   matrices of each piece, a prefix over the pieces for their boundary
+ *   states, then the pieces' sweeps.  Automatic: when the chains fill
+ *   fewer than 4 warps per SM, enough pieces for about 8 warps per SM, each
+ *   of >= 32 segments (256 sites), at most 128.  Results agree with P = 1 to
+ *   rounding (relative 1e-10 in the tests, about 1e-12 measured). */
 #define NEGF_TUNE_PASS2_WARPS_PER_BLOCK 2
+#define NEGF_TUNE_PASS1_PIECES 4
 int negf_set_tuning(int key, int value);
 /* Enable CUDA-event timing of negf_compute_charge (off by default). */
 int negf_set_timing(int enable);

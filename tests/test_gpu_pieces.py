@@ -1,0 +1,57 @@
+"""Parallel-in-length pass 1: the sweeps of every chain split into pieces
+(transfer matrices, prefix over the pieces, piece sweeps) give the charge of
+the single sweep."""
+import numpy as np
+import pytest
+
+from test_gpu_parity import CASES, _pair, _rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _with_pieces(tube, P):
+    from electrostatic_b200 import _lib
+    from electrostatic_b200.negf import last_stats
+    L = _lib.load()
+    assert L.negf_set_tuning(4, P) == 0
+    try:
+        Q = tube.Solve_NEGF()
+        return Q, last_stats()
+    finally:
+        L.negf_set_tuning(4, 0)
+
+
+@pytest.mark.parametrize("case", ["equilibrium_poles", "bias_gl_paths", "window_regular"])
+@pytest.mark.parametrize("P", [2, 5, 16])
+def test_pieces_equal_single_sweep(oracle, case, P):
+    g, o = _pair(oracle, seed=41, **CASES[case])
+    Q1, _ = _with_pieces(g, 1)
+    QP, st = _with_pieces(g, P)
+    assert st["pieces"] == P
+    assert _rel(QP, Q1) <= 1e-10, _rel(QP, Q1)
+    assert _rel(QP, o.charge(nthreads=8)) <= 1e-8
+
+
+def test_pieces_mixed_precision_and_decimation(oracle):
+    kw = dict(type_id=(17, 0), num_unitcells=40, num_modes=3, contact_mu=(0.0, -0.3), contact_T=(300.0, 320.0),
+              eq_integration_pts=(24, 24, 40), noneq_integration_pts=(60,), E_zPlus_imag=2e-3, use_decimation=1,
+              precision="mixed")
+    g, o = _pair(oracle, seed=42, **kw)
+    Q1, _ = _with_pieces(g, 1)
+    QP, _ = _with_pieces(g, 7)
+    assert _rel(QP, Q1) <= 1e-6
+    assert _rel(QP, o.charge(nthreads=8)) <= 1e-5
+
+
+def test_long_tube_automatic_pieces():
+    """A 16000-site tube with few energies: the automatic choice splits it."""
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import site_potential
+    g = CNT(type_id=(17, 0), num_unitcells=4000, num_modes=2, contact_mu=(0.0, -0.2), contact_T=(300.0, 300.0),
+            eq_integration_pts=(8, 8, 16), noneq_integration_pts=(32,), E_zPlus_imag=1e-3)
+    U = site_potential(g.site_positions(), 7, amp=0.2, ramp=0.2)
+    g.set_potential(U, (U[0], U[-1]))
+    Qa, st = _with_pieces(g, 0)
+    assert st["pieces"] > 1
+    Q1, _ = _with_pieces(g, 1)
+    assert _rel(Qa, Q1) <= 1e-10, _rel(Qa, Q1)
