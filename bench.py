@@ -303,17 +303,19 @@ def config3_measure(torch, passes=2):
     Qm = t.Solve_NEGF()
     E = len(t.energy_points(1)[0]) + len(t.energy_points(2)[0])
     E0 = len(t.energy_points(0)[0])
-    K, n = t.num_field_sites // 2, 26
-    # dense convention: complex GEMM 8n^3, inverse 8n^3; 56 n^3 per block update,
-    # 32 lead iterations x 88 n^3 per contact per energy
-    flops = (E + E0) * (K * 56 * n ** 3 + 2 * 32 * 88 * n ** 3)
+    K, m = t.num_field_sites // 2, 13
+    # ring-corner algorithm: one m x m inverse (8m^3) and three m x m complex
+    # products (8m^3 each) per block update; the lead decimation (stopped at
+    # convergence, data-dependent) is not counted
+    flops = (E + E0) * K * 32 * m ** 3
     Qr = Q.cpu().numpy()
     return {"workload": "(13,0) CNT, 600 blocks of 2 rings (26 atoms), %d contour+pole energies (+%d Rho0), "
-                        "Sancho-Rubio leads (32 iterations), FP64, seeded config-2 ring potential" % (E, E0),
+                        "Sancho-Rubio leads (at most 32 iterations), FP64, seeded config-2 ring potential" % (E, E0),
             "seconds_per_pass": sec, "block_updates_per_s": (E + E0) * K / sec,
             "achieved_tflops": flops / sec / 1e12, "flops_per_pass": flops,
-            "flop_convention": "dense complex: GEMM 8n^3, inverse 8n^3; 56n^3 per block update, 88n^3 per lead iteration",
-            "path": "negf_rs_compute_charge (FP64 CUDA cores, one warp per energy)",
+            "flop_convention": "ring corners m=13: inverse 8m^3 + three complex products 8m^3 per block update "
+                               "(leads not counted)",
+            "path": "negf_rs_compute_charge (FP64 CUDA cores, one warp per energy, Schur complements on ring corners)",
             "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm)))}
 
 

@@ -1636,27 +1636,27 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
         cr.push_back(it.c.real());
         ci.push_back(it.c.imag());
     }
+    // Rho0 at U = 0 in the same launch, with negated coefficients
     rho0_paths(*t);
     const int n0 = pass_items(*t, true);
     for (int idx = 0; idx < n0; ++idx) {
         const Item it = pass_item(*t, true, idx);
         Er.push_back(it.E.real());
         Ei.push_back(it.E.imag());
-        cr.push_back(it.c.real());
-        ci.push_back(it.c.imag());
+        cr.push_back(-it.c.real());
+        ci.push_back(-it.c.imag());
     }
     const int P = (int)Er.size();
     const size_t mm = (size_t)m * m;
+    const size_t pe = (size_t)std::max(P, 1);
     // grow-only buffers kept across calls (serialised by g_mu)
     static DevBuf bE, bU0, bUa, bCorners, bGL, bRows, bStatus;
-    NEGF_CUDA(bE.reserve(sizeof(double) * 4 * P));
+    NEGF_CUDA(bE.reserve(sizeof(double) * 4 * pe));
     NEGF_CUDA(bUa.reserve(sizeof(double) * (size_t)N * m));
     NEGF_CUDA(bU0.reserve(sizeof(double) * (size_t)N * m));
-    NEGF_CUDA(bCorners.reserve(16 * 2 * mm * P));
-    // both launches (neq contour/pole energies, n0 Rho0 energies) share these buffers
-    const size_t maxe = (size_t)std::max(std::max(neq, n0), 1);
-    NEGF_CUDA(bGL.reserve(16 * mm * K * maxe));
-    NEGF_CUDA(bRows.reserve(sizeof(double) * (size_t)N * maxe));
+    NEGF_CUDA(bCorners.reserve(16 * 2 * mm * pe));
+    NEGF_CUDA(bGL.reserve(16 * mm * K * pe));
+    NEGF_CUDA(bRows.reserve(sizeof(double) * (size_t)N * pe));
     NEGF_CUDA(bStatus.reserve(sizeof(int)));
     std::vector<double> host(4 * (size_t)P);
     std::copy(Er.begin(), Er.end(), host.begin());
@@ -1673,15 +1673,12 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
         Ua = bUa.as<double>();
     }
     const int iters = t->d.decimation_max_iter + 2;
-    if (neq > 0)
-        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, neq, Ua, t->Uc[0],
-                                         t->Uc[1], iters, bCorners.p, bGL.p, bRows.as<double>(), d_Q, 1.0, 0,
-                                         bStatus.as<int>(), s));
+    if (P > 0)
+        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, P, neq, Ua,
+                                         bU0.as<double>(), t->Uc[0], t->Uc[1], iters, bCorners.p, bGL.p,
+                                         bRows.as<double>(), d_Q, bStatus.as<int>(), s));
     else
         NEGF_CUDA(cudaMemsetAsync(d_Q, 0, sizeof(double) * N, s));
-    NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE + neq, dE + P + neq, dE + 2 * P + neq, dE + 3 * P + neq, n0,
-                                     bU0.as<double>(), 0.0, 0.0, iters, bCorners.p, bGL.p, bRows.as<double>(), d_Q,
-                                     -1.0, 1, bStatus.as<int>(), s));
     int status = 0;
     NEGF_CUDA(cudaMemcpyAsync(&status, bStatus.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     NEGF_CUDA(cudaStreamSynchronize(s));

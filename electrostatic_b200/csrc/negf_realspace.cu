@@ -1,319 +1,433 @@
 // Real-space ring-block RGF of a zigzag (m,0) tube (FP64).
 //
-// Blocks of two rings (n = 2m atoms, m <= 16 so that one lane owns one row):
-// rings 2k and 2k+1 are joined by the double bond (atom j to atoms j and
-// j+1 mod m), ring 2k+1 to ring 2k+2 by the single bond (atom j to atom j),
-// hopping gamma; in mode space these are beta_J = 2 gamma cos(pi J/m) and
-// gamma (CNT.cpp:288-336), so a ring-uniform potential reproduces the sum of
-// the m mode chains.  The self-energies of neighbouring blocks and of the
-// leads touch one m x m corner only (gamma^2 g_bb on ring a, gamma^2 g_aa on
-// ring b).
+// Blocks of two rings (2m atoms, m <= 16): ring a = 2k and ring b = 2k+1 are
+// joined by the double bond (atom j of a to atoms j and j+1 mod m of b:
+// E - H has -gamma C with C[j][j] = C[j][j+1] = 1), ring b of block k and
+// ring a of block k+1 by the single bond (atom j to atom j, -gamma I).  In
+// mode space these are beta_J = 2 gamma cos(pi J/m) and gamma
+// (CNT.cpp:288-336), so a ring-uniform potential reproduces the sum of the m
+// mode chains.  The dense 2m x 2m block is
+//     M_k = [[A, -gamma C], [-gamma C^T, D]],
+// A = diag(E - U_a) - Sigma_a, D = diag(E - U_b) - Sigma_b, where the
+// self-energies of the neighbours touch one ring each.  The block algebra
+// works on m x m ring corners with Schur complements instead of 2m x 2m
+// inversions:
+//   forward  (Sigma_b = 0, D diagonal): X_k = g_L[a][a] = S^-1 with
+//            S = A - gamma^2 C D^-1 C^T (C D^-1 C^T has three diagonals);
+//            g_L[b][b] = D^-1 + gamma^2 Y^T X Y and g_L[a][b] = gamma X Y,
+//            Y = C D^-1, follow from X with O(m^2) work; X_k is kept.
+//   backward G_kk = g_L + gamma^2 g_L[:, b] G_{k+1}[a][a] g_L[b, :] gives
+//            G[a][a] = X + gamma^4 X (Y G' Y^T) X  and
+//            tr G[b][b] = tr g_L[b][b] + gamma^2 tr(g_L[b][b] G' g_L[b][b])
+//            with G' = G_{k+1}[a][a]: three m x m products per block.  The
+//            right lead enters through G_K[a][a] = (I - gamma^2 s_R
+//            g_L[b][b])^-1 s_R of its first ring.
+// One block update costs one m x m inversion and three m x m products
+// instead of three 2m x 2m inversions (about 10x fewer operations).
 //
-// Kernels (one warp per energy, rows of the working matrices owned by lanes,
-// column-major shared-memory tiles so that lanes read consecutive words):
-//   rs_lead_kernel   surface Green's functions of the two semi-infinite
-//                    leads by the Lopez Sancho-Sancho-Rubio decimation,
-//                    fixed iteration count -> corners sL[b][b], sR[a][a];
-//   rs_chain_kernel  forward sweep (left-connected g_L, corner [b][b] kept in
-//                    global memory per block), backward sweep (right-connected
-//                    g_R in shared memory) with G_kk = (E - H_kk - S_L - S_R)^-1
-//                    and the ring sums of c G_jj written to the energy's row;
+// Leads: Lopez Sancho-Sancho-Rubio decimation of the two-ring cell in the
+// same corner form.  With s the ring that faces the device and t the other,
+// the coupling alpha between cells lives in the [t][s'] corner A and every
+// update stays in ring corners:
+//   eps[t][t] -= A g[s][s] A^T (also the surface cell), eps[s][s] -= A^T
+//   g[t][t] A, A <- A g[s][t] A,
+// with g the cell inverse through the same Schur complement (two m x m
+// inversions and a few products per iteration).  The iteration stops early
+// once both updates fall below 1e-18 of the energy scale (later ones are
+// smaller still: the decimation converges quadratically).
+//
+// Kernels (one warp per energy; m x m complex tiles in shared memory,
+// row-major, products staged in registers so that outputs may alias inputs):
+//   rs_lead_kernel   both lead corners s_L = g[b][b], s_R = g[a][a];
+//   rs_chain_kernel  forward sweep (X_k to global scratch), backward sweep
+//                    with the ring sums of c G_jj written per energy;
 //   rs_reduce_kernel sum over energies per ring in a fixed order (Kahan).
-// Every inversion is Gauss-Jordan with partial pivoting on the augmented
-// [M | I] tile (n x 2n complex).
+// The energies of the U = 0 pass (Rho0) run in the same launches with
+// negated coefficients, so one reduction gives the induced charge.
+// Inversions: Gauss-Jordan with partial pivoting on [S | I] (lane = column).
 
 #include "negf_internal.h"
 
 namespace negf {
 namespace {
 
-constexpr int kMaxN = 32;
+constexpr int kMaxM = 16;  // atoms per ring: the augmented m x 2m tile has one lane per column
 
-struct cplxd {
+struct __align__(16) cplxd {
     double x, y;
 };
 __device__ __forceinline__ cplxd cmk(double a, double b) { return {a, b}; }
 __device__ __forceinline__ cplxd cadd(cplxd a, cplxd b) { return {a.x + b.x, a.y + b.y}; }
 __device__ __forceinline__ cplxd csub(cplxd a, cplxd b) { return {a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ cplxd cscale(cplxd a, double s) { return {a.x * s, a.y * s}; }
 __device__ __forceinline__ cplxd cmul(cplxd a, cplxd b) { return {fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x)}; }
-// a - f b
-__device__ __forceinline__ cplxd cfnms(cplxd f, cplxd b, cplxd a) {
-    return {fma(-f.x, b.x, fma(f.y, b.y, a.x)), fma(-f.x, b.y, fma(-f.y, b.x, a.y))};
+// acc + a b
+__device__ __forceinline__ cplxd cfma(cplxd a, cplxd b, cplxd acc) {
+    return {fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y))};
 }
-// 1 / b, Smith (1962)
-__device__ __forceinline__ cplxd cinvd(cplxd b) {
-    if (fabs(b.x) >= fabs(b.y)) {
-        const double r = b.y / b.x, d = b.x + r * b.y;
-        return {1.0 / d, -r / d};
-    }
-    const double r = b.x / b.y, d = b.y + r * b.x;
-    return {r / d, -1.0 / d};
+// acc - a b
+__device__ __forceinline__ cplxd cfms(cplxd a, cplxd b, cplxd acc) {
+    return {fma(-a.x, b.x, fma(a.y, b.y, acc.x)), fma(-a.x, b.y, fma(-a.y, b.x, acc.y))};
+}
+__device__ __forceinline__ double cabs1(cplxd a) { return fabs(a.x) + fabs(a.y); }
+// Reciprocal: hardware approximation y0 = rcp.approx.ftz(x) with relative
+// error e = 1 - x y0 (|e| <= 2^-20 or better), corrected by the truncated
+// series 1/x = y0 (1 + e + e^2 + ...) to a relative error of order e^3.
+// Arguments are squared moduli of pivots and of E - U (normal numbers).
+__device__ __forceinline__ double rcp64(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
+}
+// 1 / b = conj(b) / |b|^2
+__device__ __forceinline__ cplxd crcp(cplxd b) {
+    const double q = rcp64(fma(b.x, b.x, b.y * b.y));
+    return {b.x * q, -b.y * q};
 }
 
-// Tile: column-major, leading dimension ld (= n, the block size).
-struct Tile {
+// m x m complex tile, row-major with leading dimension ld
+struct Mat {
     cplxd* a;
     int ld;
-    __device__ cplxd& at(int r, int c) const { return a[c * ld + r]; }
+    __device__ __forceinline__ cplxd& at(int r, int c) const { return a[r * ld + c]; }
 };
 
-// Gauss-Jordan: on entry columns [0, n) hold M, columns [n, 2n) are set to I
-// here; on exit columns [n, 2n) hold M^-1.  Returns false if a pivot is 0.
-__device__ bool gj_invert(Tile T, int n, int lane) {
-    for (int c = 0; c < n; ++c)
-        if (lane < n) T.at(lane, n + c) = cmk(lane == c ? 1.0 : 0.0, 0.0);
+__device__ __forceinline__ int wrap(int i, int m) { return i < 0 ? i + m : (i >= m ? i - m : i); }
+
+// Lane layout of every tile operation: column c = lane & 15, rows h, h + 2,
+// ..., h = lane >> 4 (lanes of a half-warp share the row operands).  The
+// body sees r and c.
+#define RS_FOR_ENTRIES(m, lane, ...)                           \
+    {                                                          \
+        const int c_ = (lane) & 15, h_ = (lane) >> 4;          \
+        if (c_ < (m)) {                                        \
+            _Pragma("unroll") for (int i_ = 0; i_ < 8; ++i_) { \
+                const int r_ = h_ + 2 * i_;                    \
+                if (r_ < (m)) {                                \
+                    const int r = r_, c = c_;                  \
+                    __VA_ARGS__                                \
+                }                                              \
+            }                                                  \
+        }                                                      \
+    }
+
+// C = s op(A) op(B) (+ D when ADD); op = transpose for TA / TB.  C may alias
+// any operand: the products are staged in registers.
+template <bool TA, bool TB, bool ADD>
+__device__ void mm(Mat C, Mat A, Mat B, Mat D, double s, int m, int lane) {
+    const int c = lane & 15, h = lane >> 4;
+    cplxd acc[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i] = cmk(0.0, 0.0);
+    if (c < m) {
+#pragma unroll 2
+        for (int k = 0; k < m; ++k) {
+            const cplxd b = TB ? B.at(c, k) : B.at(k, c);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int r = h + 2 * i;
+                if (r < m) acc[i] = cfma(TA ? A.at(k, r) : A.at(r, k), b, acc[i]);
+            }
+        }
+    }
+    __syncwarp();
+    if (c < m) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int r = h + 2 * i;
+            if (r < m) {
+                cplxd v = cscale(acc[i], s);
+                if (ADD) v = cadd(v, D.at(r, c));
+                C.at(r, c) = v;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// out = S^-1 through the augmented tile aug (m x 2m, ld 2m): Gauss-Jordan
+// with partial pivoting (largest |.|^2 over the rows below, lowest row on
+// ties), lane = column; every lane finds the pivot row itself from the
+// broadcast pivot column.  out may alias S.  Returns false on a zero pivot.
+__device__ bool invert(Mat out, Mat S, cplxd* aug, int m, int lane) {
+    const int n2 = 2 * m;
+    const Mat A{aug, n2};
+    __syncwarp();  // S complete
+    if (lane < n2)
+        for (int r = 0; r < m; ++r) A.at(r, lane) = lane < m ? S.at(r, lane) : cmk(lane - m == r ? 1.0 : 0.0, 0.0);
     __syncwarp();
     bool ok = true;
-    for (int p = 0; p < n; ++p) {
-        // pivot: largest |M[r][p]| over r >= p (lowest row on ties)
-        double v = -1.0;
-        if (lane >= p && lane < n) {
-            const cplxd x = T.at(lane, p);
-            v = x.x * x.x + x.y * x.y;
+    for (int p = 0; p < m; ++p) {
+        double best = -1.0;
+        int idx = p;
+        for (int r = p; r < m; ++r) {
+            const cplxd x = A.at(r, p);
+            const double v = fma(x.x, x.x, x.y * x.y);
+            if (v > best) {
+                best = v;
+                idx = r;
+            }
         }
-        int idx = lane;
+        if (!(best > 0.0)) ok = false;
+        __syncwarp();
+        if (idx != p && lane < n2) {
+            const cplxd t = A.at(p, lane);
+            A.at(p, lane) = A.at(idx, lane);
+            A.at(idx, lane) = t;
+        }
+        __syncwarp();
+        const cplxd rp = lane < n2 ? cmul(A.at(p, lane), crcp(A.at(p, p))) : cmk(0.0, 0.0);
+        // eliminate column p from the other rows, 8 rows at a time: the
+        // multipliers of a chunk are read before any lane updates the chunk
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-            if (ov > v || (ov == v && oi < idx)) {
-                v = ov;
-                idx = oi;
+        for (int r0 = 0; r0 < kMaxM; r0 += 8) {
+            if (r0 >= m) break;
+            cplxd f[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int r = r0 + j;
+                f[j] = (r < m && r != p) ? A.at(r, p) : cmk(0.0, 0.0);
+            }
+            __syncwarp();
+            if (lane < n2) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int r = r0 + j;
+                    if (r < m && r != p) A.at(r, lane) = cfms(f[j], rp, A.at(r, lane));
+                }
             }
         }
-        if (!(v > 0.0)) ok = false;
-        const int piv = idx;
-        if (piv != p) {  // swap rows p and piv, lanes over columns
-            for (int c = lane; c < 2 * n; c += 32) {
-                const cplxd t = T.at(p, c);
-                T.at(p, c) = T.at(piv, c);
-                T.at(piv, c) = t;
-            }
-        }
-        __syncwarp();
-        const cplxd inv = cinvd(T.at(p, p));
-        __syncwarp();
-        for (int c = lane; c < 2 * n; c += 32)
-            if (c > p) T.at(p, c) = cmul(T.at(p, c), inv);
-        if (lane == 0) T.at(p, p) = cmk(1.0, 0.0);
-        __syncwarp();
-        if (lane < n && lane != p) {
-            const cplxd f = T.at(lane, p);
-            for (int c = p + 1; c < 2 * n; ++c) T.at(lane, c) = cfnms(f, T.at(p, c), T.at(lane, c));
-            T.at(lane, p) = cmk(0.0, 0.0);
-        }
+        if (lane < n2) A.at(p, lane) = rp;
         __syncwarp();
     }
+    if (lane >= m && lane < n2)
+        for (int r = 0; r < m; ++r) out.at(r, lane - m) = A.at(r, lane);
+    __syncwarp();
     return ok;
 }
 
-// E - H of one block into columns [0, n) of T (rows = lanes).
-__device__ void build_block(Tile T, int m, double gamma, cplxd E, const double* __restrict__ U, int lane) {
-    const int n = 2 * m;
-    if (lane < n) {
-        for (int c = 0; c < n; ++c) T.at(lane, c) = cmk(0.0, 0.0);
-        T.at(lane, lane) = cmk(E.x - U[lane], E.y);
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ cplxd warp_sum(cplxd v) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
     }
-    __syncwarp();
-    if (lane < m) {  // double bond: ring a atom j <-> ring b atoms j, j+1
-        const int a = lane, b1 = m + lane, b2 = m + (lane + 1) % m;
-        T.at(a, b1).x -= gamma;
-        T.at(b1, a).x -= gamma;
-        T.at(a, b2).x -= gamma;
-        T.at(b2, a).x -= gamma;
-    }
-    __syncwarp();
+    return v;
 }
 
-// C = A B for n x n tiles (columns [0, n)); lane = row of C.
-__device__ void tile_gemm(Tile C, Tile A, Tile B, int n, int lane) {
-    if (lane < n)
-        for (int j = 0; j < n; ++j) {
-            cplxd s = cmk(0.0, 0.0);
-            for (int k = 0; k < n; ++k) s = cadd(s, cmul(A.at(lane, k), B.at(k, j)));
-            C.at(lane, j) = s;
-        }
-    __syncwarp();
-}
-
-
-// Lead kernel: warp w -> energy w / 2, lead w % 2 (0 left, 1 right).
-__global__ void __launch_bounds__(32) rs_lead_kernel(int m, double gamma, const double* __restrict__ Ere,
-                                                     const double* __restrict__ Eim, int num_e, double Uc0, double Uc1,
-                                                     int iters, cplxd* __restrict__ corners, int* __restrict__ status) {
+// Lead kernel: warp w -> energy w / 2, lead w % 2 (0 left: s = ring b, the
+// intra-cell bond from s to t is C^T; 1 right: s = ring a, bond C), the lead
+// cell at the contact potential (0 for the energies e >= num_u, the U = 0
+// pass).  corners[e][side] = g_surface[s][s] (m x m, row-major).
+__global__ void __launch_bounds__(32, 8) rs_lead_kernel(int m, double gamma, const double* __restrict__ Ere,
+                                                        const double* __restrict__ Eim, int num_e, int num_u,
+                                                        double Uc0, double Uc1, int iters,
+                                                        cplxd* __restrict__ corners, int* __restrict__ status) {
     extern __shared__ cplxd sh[];
     const int lane = threadIdx.x;
     const int w = blockIdx.x;
     if (w >= 2 * num_e) return;
     const int e = w / 2, side = w % 2;
-    const bool left = side == 0;
-    const int n = 2 * m;
-    const cplxd E = cmk(Ere[e], Eim[e]);
-    const int sq = n * n;  // one n x n tile; the augmented tile is two
-    Tile aug{sh, n}, eps{sh + 2 * sq, n}, epss{sh + 3 * sq, n}, al{sh + 4 * sq, n}, be{sh + 5 * sq, n},
-        t1{sh + 6 * sq, n}, t2{sh + 7 * sq, n};
-    // eps = eps_s = E - H00 at the contact potential
-    {
-        const double u = left ? Uc0 : Uc1;
-        if (lane < n) {
-            for (int c = 0; c < n; ++c) eps.at(lane, c) = cmk(0.0, 0.0);
-            eps.at(lane, lane) = cmk(E.x - u, E.y);
-        }
-        __syncwarp();
-        if (lane < m) {
-            const int a = lane, b1 = m + lane, b2 = m + (lane + 1) % m;
-            eps.at(a, b1).x -= gamma;
-            eps.at(b1, a).x -= gamma;
-            eps.at(a, b2).x -= gamma;
-            eps.at(b2, a).x -= gamma;
-        }
-        __syncwarp();
-        if (lane < n)
-            for (int c = 0; c < n; ++c) {
-                epss.at(lane, c) = eps.at(lane, c);
-                // tau (ring b of a cell -> ring a of the next): -gamma at (m + j, j); tau^dagger at (j, m + j)
-                const bool tb = (lane >= m && c == lane - m), td = (lane < m && c == lane + m);
-                const cplxd tau = cmk(tb ? -gamma : 0.0, 0.0), taud = cmk(td ? -gamma : 0.0, 0.0);
-                al.at(lane, c) = left ? taud : tau;
-                be.at(lane, c) = left ? tau : taud;
-            }
-        __syncwarp();
-    }
-    bool ok = true;
-    const Tile T0{sh, n};          // columns [0, n) of aug: free once g is formed
-    const Tile g{sh + sq, n};      // columns [n, 2n) of aug: eps^-1 after the inversion
-    for (int it = 0; it < iters; ++it) {
-        if (lane < n)
-            for (int c = 0; c < n; ++c) aug.at(lane, c) = eps.at(lane, c);
-        __syncwarp();
-        ok = gj_invert(aug, n, lane) && ok;
-        tile_gemm(t1, al, g, n, lane);  // a g
-        tile_gemm(t2, t1, be, n, lane);  // a g b
-        if (lane < n)
-            for (int c = 0; c < n; ++c) {
-                epss.at(lane, c) = csub(epss.at(lane, c), t2.at(lane, c));
-                eps.at(lane, c) = csub(eps.at(lane, c), t2.at(lane, c));
-            }
-        __syncwarp();
-        tile_gemm(T0, be, g, n, lane);   // b g
-        tile_gemm(t2, T0, al, n, lane);  // b g a
-        if (lane < n)
-            for (int c = 0; c < n; ++c) eps.at(lane, c) = csub(eps.at(lane, c), t2.at(lane, c));
-        __syncwarp();
-        tile_gemm(t2, t1, al, n, lane);  // a g a
-        tile_gemm(t1, T0, be, n, lane);  // b g b
-        if (lane < n)
-            for (int c = 0; c < n; ++c) {
-                al.at(lane, c) = t2.at(lane, c);
-                be.at(lane, c) = t1.at(lane, c);
-            }
-        __syncwarp();
-    }
-    if (lane < n)
-        for (int c = 0; c < n; ++c) aug.at(lane, c) = epss.at(lane, c);
+    const int dir = side == 0 ? -1 : 1;  // C_st[i][l] != 0 for l in {i, i + dir}
+    const int mm2 = m * m;
+    const Mat Ess{sh, m}, Ett{sh + mm2, m}, Est{sh + 2 * mm2, m}, Al{sh + 3 * mm2, m}, Qi{sh + 4 * mm2, m},
+        Gss{sh + 5 * mm2, m}, V{sh + 6 * mm2, m}, U1{sh + 7 * mm2, m}, P{sh + 8 * mm2, m}, T{sh + 9 * mm2, m};
+    cplxd* aug = sh + 10 * mm2;  // m x 2m
+    const double u = e >= num_u ? 0.0 : (side == 0 ? Uc0 : Uc1);
+    const cplxd eu = cmk(Ere[e] - u, Eim[e]);
+    const double g2 = gamma * gamma;
+    const double tol = 1e-18 * (cabs1(eu) + fabs(gamma));
+    RS_FOR_ENTRIES(m, lane, {
+        const cplxd d = r == c ? eu : cmk(0.0, 0.0);
+        Ess.at(r, c) = d;
+        Ett.at(r, c) = d;
+        Est.at(r, c) = d;
+        Al.at(r, c) = cmk(r == c ? -gamma : 0.0, 0.0);
+    })
     __syncwarp();
-    ok = gj_invert(aug, n, lane) && ok;
-    // corner: left lead -> g[b][b], right lead -> g[a][a]; stored column-major m x m
-    const int off = left ? m : 0;
-    cplxd* out = corners + ((size_t)e * 2 + side) * m * m;
-    if (lane < m)
-        for (int c = 0; c < m; ++c) out[c * m + lane] = aug.at(off + lane, n + off + c);
+    bool ok = true;
+    for (int it = 0; it < iters; ++it) {
+        // cell inverse: Qi = Ett^-1, g[s][s] = (Ess - gamma^2 C Qi C^T)^-1,
+        // V = C Qi, U1 = g[s][s] V (g[s][t] = gamma U1),
+        // g[t][t] = Qi + gamma^2 V^T U1 (kept in Qi)
+        ok = invert(Qi, Ett, aug, m, lane) && ok;
+        RS_FOR_ENTRIES(m, lane, {
+            const int r1 = wrap(r + dir, m), c1 = wrap(c + dir, m);
+            const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
+            Gss.at(r, c) = csub(Ess.at(r, c), cscale(q, g2));
+            V.at(r, c) = cadd(Qi.at(r, c), Qi.at(r1, c));
+        })
+        ok = invert(Gss, Gss, aug, m, lane) && ok;
+        mm<false, false, false>(U1, Gss, V, Gss, 1.0, m, lane);
+        mm<true, false, true>(Qi, V, U1, Qi, g2, m, lane);
+        // eps[t][t] -= A g[s][s] A^T (bulk and surface), eps[s][s] -= A^T g[t][t] A
+        mm<false, false, false>(P, Al, Gss, P, 1.0, m, lane);
+        mm<false, true, false>(T, P, Al, T, 1.0, m, lane);
+        double d1 = 0.0;
+        RS_FOR_ENTRIES(m, lane, {
+            const cplxd t = T.at(r, c);
+            Ett.at(r, c) = csub(Ett.at(r, c), t);
+            Est.at(r, c) = csub(Est.at(r, c), t);
+            d1 = fmax(d1, cabs1(t));
+        })
+        __syncwarp();
+        mm<true, false, false>(P, Al, Qi, P, 1.0, m, lane);
+        mm<false, false, false>(T, P, Al, T, 1.0, m, lane);
+        RS_FOR_ENTRIES(m, lane, {
+            const cplxd t = T.at(r, c);
+            Ess.at(r, c) = csub(Ess.at(r, c), t);
+            d1 = fmax(d1, cabs1(t));
+        })
+        __syncwarp();
+        // A <- A g[s][t] A = gamma A U1 A
+        mm<false, false, false>(P, Al, U1, P, 1.0, m, lane);
+        mm<false, false, false>(Al, P, Al, Al, gamma, m, lane);
+        if (warp_max(d1) <= tol) break;
+    }
+    // surface: g_s[s][s] = ((E - u) I - gamma^2 C Est^-1 C^T)^-1
+    ok = invert(Qi, Est, aug, m, lane) && ok;
+    RS_FOR_ENTRIES(m, lane, {
+        const int r1 = wrap(r + dir, m), c1 = wrap(c + dir, m);
+        const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
+        Gss.at(r, c) = csub(r == c ? eu : cmk(0.0, 0.0), cscale(q, g2));
+    })
+    ok = invert(Gss, Gss, aug, m, lane) && ok;
+    cplxd* out = corners + ((size_t)e * 2 + side) * mm2;
+    for (int i = lane; i < mm2; i += 32) out[i] = Gss.a[i];
     if (!ok && lane == 0) atomicExch(status, 1);
 }
 
-// Chain kernel: warp e -> energy e.  gL: [num_e][K][m*m] scratch; rows:
-// [num_e][N] ring sums of c G_jj (imaginary part).
-__global__ void __launch_bounds__(32) rs_chain_kernel(int m, int K, double gamma, const double* __restrict__ Ere,
-                                                      const double* __restrict__ Eim, const double* __restrict__ cre,
-                                                      const double* __restrict__ cim, int num_e,
-                                                      const double* __restrict__ Uatoms,
-                                                      const cplxd* __restrict__ corners, cplxd* __restrict__ gL,
-                                                      double* __restrict__ rows, int* __restrict__ status) {
+// Chain kernel: warp e -> energy e, atom potentials Uatoms for e < num_u and
+// Uzero after.  gX: [num_e][K][m*m] scratch (X_k); rows: [num_e][N] ring
+// sums Im(c sum_j G_jj).  The potentials of the next block are loaded while
+// the current block is computed.
+__global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double gamma, const double* __restrict__ Ere,
+                                                          const double* __restrict__ Eim,
+                                                          const double* __restrict__ cre,
+                                                          const double* __restrict__ cim, int num_e, int num_u,
+                                                          const double* __restrict__ Uatoms,
+                                                          const double* __restrict__ Uzero,
+                                                          const cplxd* __restrict__ corners, cplxd* __restrict__ gX,
+                                                          double* __restrict__ rows, int* __restrict__ status) {
     extern __shared__ cplxd sh[];
     const int lane = threadIdx.x;
     const int e = blockIdx.x;
     if (e >= num_e) return;
-    const int n = 2 * m, mm = m * m, N = 2 * K;
+    const int mm2 = m * m, N = 2 * K;
     const cplxd E = cmk(Ere[e], Eim[e]);
     const cplxd cc = cmk(cre[e], cim[e]);
-    const double g2 = gamma * gamma;
-    Tile aug{sh, n};
-    cplxd* gR = sh + 2 * n * n;  // m x m corner [a][a] of the right-connected g_R of block k+1
-    const cplxd* sL = corners + (size_t)e * 2 * mm;
-    const cplxd* sR = sL + mm;
-    cplxd* myL = gL + (size_t)e * K * mm;
+    const double g2 = gamma * gamma, g4 = g2 * g2;
+    const double* __restrict__ Ua = e < num_u ? Uatoms : Uzero;
+    const Mat X{sh, m}, Gbb{sh + mm2, m}, Gn{sh + 2 * mm2, m}, Z{sh + 3 * mm2, m}, W{sh + 4 * mm2, m};
+    cplxd* aug = sh + 3 * mm2;  // Z and W (2 m^2) while an inversion runs
+    cplxd* dv = sh + 5 * mm2;   // D^-1 of the current ring b
+    cplxd* da = dv + kMaxM;     // E - U of the current ring a
+    const cplxd* sL = corners + (size_t)e * 2 * mm2;
+    const cplxd* sR = sL + mm2;
+    cplxd* myX = gX + (size_t)e * K * mm2;
     double* row = rows + (size_t)e * N;
     bool ok = true;
-    // forward: g_L[k] corner [b][b]
-    for (int k = 0; k < K; ++k) {
-        build_block(aug, m, gamma, E, Uatoms + (size_t)k * n, lane);
-        const cplxd* c = k == 0 ? sL : myL + (size_t)(k - 1) * mm;
-        if (lane < m)
-            for (int j = 0; j < m; ++j) {
-                const cplxd v = c[j * m + lane];
-                aug.at(lane, j) = cmk(fma(-g2, v.x, aug.at(lane, j).x), fma(-g2, v.y, aug.at(lane, j).y));
-            }
-        __syncwarp();
-        ok = gj_invert(aug, n, lane) && ok;
-        if (lane < m)
-            for (int j = 0; j < m; ++j) myL[(size_t)k * mm + j * m + lane] = aug.at(m + lane, n + m + j);
-        __syncwarp();
-    }
-    // backward: g_R[k] and G_kk
-    for (int k = K - 1; k >= 0; --k) {
-        const cplxd* cr = k == K - 1 ? sR : gR;
-        const cplxd* cl = k == 0 ? sL : myL + (size_t)(k - 1) * mm;
-        // G_kk
-        build_block(aug, m, gamma, E, Uatoms + (size_t)k * n, lane);
-        if (lane < m)
-            for (int j = 0; j < m; ++j) {
-                const cplxd vl = cl[j * m + lane], vr = cr[j * m + lane];
-                cplxd& a = aug.at(lane, j);
-                a = cmk(fma(-g2, vl.x, a.x), fma(-g2, vl.y, a.y));
-                cplxd& b = aug.at(m + lane, m + j);
-                b = cmk(fma(-g2, vr.x, b.x), fma(-g2, vr.y, b.y));
-            }
-        __syncwarp();
-        ok = gj_invert(aug, n, lane) && ok;
-        {
-            // ring sums of the diagonal: lanes [0, m) ring a, [m, 2m) ring b
-            cplxd d = lane < n ? aug.at(lane, n + lane) : cmk(0.0, 0.0);
-            double sa_x = lane < m ? d.x : 0.0, sa_y = lane < m ? d.y : 0.0;
-            double sb_x = (lane >= m && lane < n) ? d.x : 0.0, sb_y = (lane >= m && lane < n) ? d.y : 0.0;
-#pragma unroll
-            for (int o = 16; o >= 1; o >>= 1) {
-                sa_x += __shfl_xor_sync(0xffffffffu, sa_x, o);
-                sa_y += __shfl_xor_sync(0xffffffffu, sa_y, o);
-                sb_x += __shfl_xor_sync(0xffffffffu, sb_x, o);
-                sb_y += __shfl_xor_sync(0xffffffffu, sb_y, o);
-            }
-            if (lane == 0) {
-                row[2 * k] = fma(cc.x, sa_y, cc.y * sa_x);      // Im(c s_a)
-                row[2 * k + 1] = fma(cc.x, sb_y, cc.y * sb_x);  // Im(c s_b)
-            }
+    // lane j < m: potentials of atom j on rings a and b of the next block
+    double ua_n = 0.0, ub_n = 0.0;
+    auto fetch_u = [&](int k) {
+        if (lane < m) {
+            ua_n = __ldg(Ua + (size_t)(2 * k) * m + lane);
+            ub_n = __ldg(Ua + (size_t)(2 * k + 1) * m + lane);
         }
+    };
+    // g_L[b][b] = D^-1 + gamma^2 Y^T X Y into Gbb
+    auto form_gbb = [&]() {
+        RS_FOR_ENTRIES(m, lane, {
+            const int r0 = wrap(r - 1, m), c0 = wrap(c - 1, m);
+            const cplxd q = cadd(cadd(X.at(r, c), X.at(r, c0)), cadd(X.at(r0, c), X.at(r0, c0)));
+            cplxd v = cscale(cmul(cmul(dv[r], dv[c]), q), g2);
+            if (r == c) v = cadd(v, dv[r]);
+            Gbb.at(r, c) = v;
+        })
         __syncwarp();
-        if (k == 0) break;
-        // g_R[k]: corner [a][a] for block k-1
-        build_block(aug, m, gamma, E, Uatoms + (size_t)k * n, lane);
-        if (lane < m)
-            for (int j = 0; j < m; ++j) {
-                const cplxd vr = cr[j * m + lane];
-                cplxd& b = aug.at(m + lane, m + j);
-                b = cmk(fma(-g2, vr.x, b.x), fma(-g2, vr.y, b.y));
-            }
+    };
+    // left lead corner as g_L[b][b] of block -1
+    for (int i = lane; i < mm2; i += 32) Gbb.a[i] = sL[i];
+    fetch_u(0);
+    for (int k = 0; k < K; ++k) {
+        if (lane < m) {
+            dv[lane] = crcp(cmk(E.x - ub_n, E.y));
+            da[lane] = cmk(E.x - ua_n, E.y);
+        }
+        if (k + 1 < K) fetch_u(k + 1);
         __syncwarp();
-        ok = gj_invert(aug, n, lane) && ok;
-        if (lane < m)
-            for (int j = 0; j < m; ++j) gR[j * m + lane] = aug.at(lane, n + j);
+        // S = diag(E - U_a) - gamma^2 g_L[b][b]_{k-1} - gamma^2 C D^-1 C^T
+        RS_FOR_ENTRIES(m, lane, {
+            const int r1 = wrap(r + 1, m), c1 = wrap(c + 1, m);
+            cplxd cd = cmk(0.0, 0.0);
+            if (r == c) cd = cadd(cd, dv[r]);
+            if (r == c1) cd = cadd(cd, dv[r]);
+            if (r1 == c) cd = cadd(cd, dv[r1]);
+            if (r1 == c1) cd = cadd(cd, dv[r1]);
+            cplxd v = cscale(cadd(Gbb.at(r, c), cd), -g2);
+            if (r == c) v = cadd(v, da[r]);
+            X.at(r, c) = v;
+        })
+        ok = invert(X, X, aug, m, lane) && ok;
+        cplxd* dst = myX + (size_t)k * mm2;
+        for (int i = lane; i < mm2; i += 32) dst[i] = X.a[i];
+        form_gbb();
+    }
+    // G_K[a][a] of the right lead's first ring: (I - gamma^2 s_R g_L[b][b])^-1 s_R
+    for (int i = lane; i < mm2; i += 32) X.a[i] = sR[i];
+    __syncwarp();
+    mm<false, false, false>(Gn, X, Gbb, Gn, -g2, m, lane);
+    if (lane < m) Gn.at(lane, lane) = cadd(Gn.at(lane, lane), cmk(1.0, 0.0));
+    ok = invert(Gn, Gn, aug, m, lane) && ok;
+    mm<false, false, false>(Gn, Gn, X, Gn, 1.0, m, lane);
+    fetch_u(K - 1);
+    for (int k = K - 1; k >= 0; --k) {
+        const cplxd* src = myX + (size_t)k * mm2;
+        for (int i = lane; i < mm2; i += 32) X.a[i] = src[i];
+        if (lane < m) dv[lane] = crcp(cmk(E.x - ub_n, E.y));
+        if (k > 0) fetch_u(k - 1);
         __syncwarp();
+        form_gbb();
+        // Z = Y G' Y^T, Y = C D^-1
+        RS_FOR_ENTRIES(m, lane, {
+            const int r1 = wrap(r + 1, m), c1 = wrap(c + 1, m);
+            cplxd v = cmul(cmul(dv[r], dv[c]), Gn.at(r, c));
+            v = cfma(cmul(dv[r], dv[c1]), Gn.at(r, c1), v);
+            v = cfma(cmul(dv[r1], dv[c]), Gn.at(r1, c), v);
+            v = cfma(cmul(dv[r1], dv[c1]), Gn.at(r1, c1), v);
+            Z.at(r, c) = v;
+        })
+        __syncwarp();
+        // tr G[b][b] = tr g_L[b][b] + gamma^2 sum_rc (g_L[b][b] G')[r][c] g_L[b][b][c][r]
+        mm<false, false, false>(W, Gbb, Gn, W, 1.0, m, lane);
+        cplxd tb = cmk(0.0, 0.0);
+        RS_FOR_ENTRIES(m, lane, {
+            tb = cfma(cscale(W.at(r, c), g2), Gbb.at(c, r), tb);
+            if (r == c) tb = cadd(tb, Gbb.at(r, r));
+        })
+        // G[a][a] = X + gamma^4 (X Z) X
+        mm<false, false, false>(Z, X, Z, Z, 1.0, m, lane);
+        mm<false, false, true>(Gn, Z, X, X, g4, m, lane);
+        cplxd ta = cmk(0.0, 0.0);
+        if (lane < m) ta = Gn.at(lane, lane);
+        ta = warp_sum(ta);
+        tb = warp_sum(tb);
+        if (lane == 0) {
+            row[2 * k] = fma(cc.x, ta.y, cc.y * ta.x);      // Im(c tr G[a][a])
+            row[2 * k + 1] = fma(cc.x, tb.y, cc.y * tb.x);  // Im(c tr G[b][b])
+        }
     }
     if (!ok && lane == 0) atomicExch(status, 1);
 }
 
-// Q[r] (+)= sum over energies of rows[e][r], Kahan, energies in order.
-__global__ void rs_reduce_kernel(const double* __restrict__ rows, int num_e, int N, double sign,
-                                 double* __restrict__ Q, int accumulate) {
+// Q[r] = sum over energies of rows[e][r], Kahan, energies in order.
+__global__ void rs_reduce_kernel(const double* __restrict__ rows, int num_e, int N, double* __restrict__ Q) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= N) return;
     double s = 0.0, comp = 0.0;
@@ -323,7 +437,7 @@ __global__ void rs_reduce_kernel(const double* __restrict__ rows, int num_e, int
         comp = (t - s) - y;
         s = t;
     }
-    Q[r] = accumulate ? Q[r] + sign * s : sign * s;
+    Q[r] = s;
 }
 
 // Uatoms[r][j] = U[r] (ring-uniform potential on the atoms).
@@ -331,6 +445,9 @@ __global__ void rs_expand_kernel(const double* __restrict__ U, int N, int m, dou
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < N * m) Ua[i] = U[i / m];
 }
+
+size_t rs_lead_smem_bytes(int m) { return sizeof(cplxd) * 12 * m * m; }
+size_t rs_chain_smem_bytes(int m) { return sizeof(cplxd) * (5 * m * m + 2 * kMaxM); }
 
 }  // namespace
 
@@ -340,35 +457,32 @@ cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_
     return cudaGetLastError();
 }
 
-size_t rs_lead_smem_bytes(int n) { return sizeof(cplxd) * 8 * n * n; }
-size_t rs_chain_smem_bytes(int n) { return sizeof(cplxd) * (2 * n * n + n * n / 4 + 1); }
-int rs_max_atoms_per_block() { return kMaxN; }
+int rs_max_atoms_per_block() { return 2 * kMaxM; }
 
 cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
-                             const double* d_cre, const double* d_cim, int num_e, const double* d_Uatoms, double Uc0,
-                             double Uc1, int lead_iters, void* d_corners, void* d_gL, double* d_rows, double* d_Q,
-                             double sign, int accumulate, int* d_status, cudaStream_t stream) {
+                             const double* d_cre, const double* d_cim, int num_e, int num_u, const double* d_Uatoms,
+                             const double* d_Uzero, double Uc0, double Uc1, int lead_iters, void* d_corners,
+                             void* d_gL, double* d_rows, double* d_Q, int* d_status, cudaStream_t stream) {
     if (num_e <= 0) return cudaSuccess;
-    const int n = 2 * m;
-    if (n > kMaxN) return cudaErrorInvalidValue;
+    if (m < 1 || m > kMaxM || K < 1) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(rs_lead_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)rs_lead_smem_bytes(kMaxN));
+                                         (int)rs_lead_smem_bytes(kMaxM));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(rs_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)rs_chain_smem_bytes(kMaxN));
+                             (int)rs_chain_smem_bytes(kMaxM));
     if (e != cudaSuccess) return e;
-    rs_lead_kernel<<<2 * num_e, 32, rs_lead_smem_bytes(n), stream>>>(m, gamma, d_Ere, d_Eim, num_e, Uc0, Uc1,
-                                                                     lead_iters, static_cast<cplxd*>(d_corners),
+    rs_lead_kernel<<<2 * num_e, 32, rs_lead_smem_bytes(m), stream>>>(m, gamma, d_Ere, d_Eim, num_e, num_u, Uc0,
+                                                                     Uc1, lead_iters, static_cast<cplxd*>(d_corners),
                                                                      d_status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    rs_chain_kernel<<<num_e, 32, rs_chain_smem_bytes(n), stream>>>(
-        m, K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_Uatoms, static_cast<const cplxd*>(d_corners),
-        static_cast<cplxd*>(d_gL), d_rows, d_status);
+    rs_chain_kernel<<<num_e, 32, rs_chain_smem_bytes(m), stream>>>(
+        m, K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, num_u, d_Uatoms, d_Uzero,
+        static_cast<const cplxd*>(d_corners), static_cast<cplxd*>(d_gL), d_rows, d_status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int N = 2 * K;
-    rs_reduce_kernel<<<(N + 127) / 128, 128, 0, stream>>>(d_rows, num_e, N, sign, d_Q, accumulate);
+    rs_reduce_kernel<<<(N + 127) / 128, 128, 0, stream>>>(d_rows, num_e, N, d_Q);
     return cudaGetLastError();
 }
 

@@ -203,8 +203,10 @@ int negf_set_timing(int enable);
  * blocks"; the reference engine is mode space only, so this entry point has
  * no counterpart there).  Zigzag (m,0) tubes, m <= 16: blocks of two rings
  * (2m atoms) with the double bond inside a block and the single bond
- * between blocks, dense 2m x 2m complex FP64 blocks, leads by the Lopez
- * Sancho-Sancho-Rubio decimation (decimation_max_iter + 2 iterations).
+ * between blocks, 2m x 2m complex FP64 blocks handled through Schur
+ * complements on their m x m ring corners, leads by the Lopez
+ * Sancho-Sancho-Rubio decimation (at most decimation_max_iter + 2
+ * iterations, stopped once the updates fall below rounding).
  * Equilibrium charge per ring into d_Q (device, N doubles): the tube's
  * contour and pole points with the mode-space coefficients, minus Rho0 at
  * U = 0.  d_Uatoms (device, [N][m]) gives per-atom potentials; null uses the
