@@ -86,14 +86,15 @@ __device__ __forceinline__ cplxd crcp(cplxd b) {
     return {b.x * q, -b.y * q};
 }
 
-// m x m complex tile, row-major with leading dimension ld
+// Complex tile, row-major with compile-time leading dimension LD
+template <int LD>
 struct Mat {
     cplxd* a;
-    int ld;
-    __device__ __forceinline__ cplxd& at(int r, int c) const { return a[r * ld + c]; }
+    __device__ __forceinline__ cplxd& at(int r, int c) const { return a[r * LD + c]; }
 };
 
-__device__ __forceinline__ int wrap(int i, int m) { return i < 0 ? i + m : (i >= m ? i - m : i); }
+template <int M>
+__device__ __forceinline__ int wrap(int i) { return i < 0 ? i + M : (i >= M ? i - M : i); }
 
 // Lane layout of every tile operation: column c = lane & 15, rows h, h + 2,
 // ..., h = lane >> 4 (lanes of a half-warp share the row operands).  The
@@ -114,14 +115,14 @@ __device__ __forceinline__ int wrap(int i, int m) { return i < 0 ? i + m : (i >=
 
 // C = s op(A) op(B) (+ D when ADD); op = transpose for TA / TB.  C may alias
 // any operand: the products are staged in registers.
-template <bool TA, bool TB, bool ADD>
-__device__ void mm(Mat C, Mat A, Mat B, Mat D, double s, int m, int lane) {
+template <int m, bool TA, bool TB, bool ADD>
+__device__ __forceinline__ void mm(Mat<m> C, Mat<m> A, Mat<m> B, Mat<m> D, double s, int lane) {
     const int c = lane & 15, h = lane >> 4;
     cplxd acc[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) acc[i] = cmk(0.0, 0.0);
     if (c < m) {
-#pragma unroll 2
+#pragma unroll
         for (int k = 0; k < m; ++k) {
             const cplxd b = TB ? B.at(c, k) : B.at(k, c);
 #pragma unroll
@@ -150,17 +151,22 @@ __device__ void mm(Mat C, Mat A, Mat B, Mat D, double s, int m, int lane) {
 // with partial pivoting (largest |.|^2 over the rows below, lowest row on
 // ties), lane = column; every lane finds the pivot row itself from the
 // broadcast pivot column.  out may alias S.  Returns false on a zero pivot.
-__device__ bool invert(Mat out, Mat S, cplxd* aug, int m, int lane) {
-    const int n2 = 2 * m;
-    const Mat A{aug, n2};
+template <int m>
+__device__ __forceinline__ bool invert(Mat<m> out, Mat<m> S, cplxd* aug, int lane) {
+    constexpr int n2 = 2 * m;
+    const Mat<n2> A{aug};
     __syncwarp();  // S complete
-    if (lane < n2)
+    if (lane < n2) {
+#pragma unroll
         for (int r = 0; r < m; ++r) A.at(r, lane) = lane < m ? S.at(r, lane) : cmk(lane - m == r ? 1.0 : 0.0, 0.0);
+    }
     __syncwarp();
     bool ok = true;
+#pragma unroll
     for (int p = 0; p < m; ++p) {
         double best = -1.0;
         int idx = p;
+#pragma unroll
         for (int r = p; r < m; ++r) {
             const cplxd x = A.at(r, p);
             const double v = fma(x.x, x.x, x.y * x.y);
@@ -181,8 +187,7 @@ __device__ bool invert(Mat out, Mat S, cplxd* aug, int m, int lane) {
         // eliminate column p from the other rows, 8 rows at a time: the
         // multipliers of a chunk are read before any lane updates the chunk
 #pragma unroll
-        for (int r0 = 0; r0 < kMaxM; r0 += 8) {
-            if (r0 >= m) break;
+        for (int r0 = 0; r0 < m; r0 += 8) {
             cplxd f[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -201,8 +206,10 @@ __device__ bool invert(Mat out, Mat S, cplxd* aug, int m, int lane) {
         if (lane < n2) A.at(p, lane) = rp;
         __syncwarp();
     }
-    if (lane >= m && lane < n2)
+    if (lane >= m && lane < n2) {
+#pragma unroll
         for (int r = 0; r < m; ++r) out.at(r, lane - m) = A.at(r, lane);
+    }
     __syncwarp();
     return ok;
 }
@@ -225,7 +232,8 @@ __device__ __forceinline__ cplxd warp_sum(cplxd v) {
 // intra-cell bond from s to t is C^T; 1 right: s = ring a, bond C), the lead
 // cell at the contact potential (0 for the energies e >= num_u, the U = 0
 // pass).  corners[e][side] = g_surface[s][s] (m x m, row-major).
-__global__ void __launch_bounds__(32, 8) rs_lead_kernel(int m, double gamma, const double* __restrict__ Ere,
+template <int m>
+__global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const double* __restrict__ Ere,
                                                         const double* __restrict__ Eim, int num_e, int num_u,
                                                         double Uc0, double Uc1, int iters,
                                                         cplxd* __restrict__ corners, int* __restrict__ status) {
@@ -235,9 +243,9 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(int m, double gamma, con
     if (w >= 2 * num_e) return;
     const int e = w / 2, side = w % 2;
     const int dir = side == 0 ? -1 : 1;  // C_st[i][l] != 0 for l in {i, i + dir}
-    const int mm2 = m * m;
-    const Mat Ess{sh, m}, Ett{sh + mm2, m}, Est{sh + 2 * mm2, m}, Al{sh + 3 * mm2, m}, Qi{sh + 4 * mm2, m},
-        Gss{sh + 5 * mm2, m}, V{sh + 6 * mm2, m}, U1{sh + 7 * mm2, m}, P{sh + 8 * mm2, m}, T{sh + 9 * mm2, m};
+    constexpr int mm2 = m * m;
+    const Mat<m> Ess{sh}, Ett{sh + mm2}, Est{sh + 2 * mm2}, Al{sh + 3 * mm2}, Qi{sh + 4 * mm2}, Gss{sh + 5 * mm2},
+        V{sh + 6 * mm2}, U1{sh + 7 * mm2}, P{sh + 8 * mm2}, T{sh + 9 * mm2};
     cplxd* aug = sh + 10 * mm2;  // m x 2m
     const double u = e >= num_u ? 0.0 : (side == 0 ? Uc0 : Uc1);
     const cplxd eu = cmk(Ere[e] - u, Eim[e]);
@@ -256,19 +264,19 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(int m, double gamma, con
         // cell inverse: Qi = Ett^-1, g[s][s] = (Ess - gamma^2 C Qi C^T)^-1,
         // V = C Qi, U1 = g[s][s] V (g[s][t] = gamma U1),
         // g[t][t] = Qi + gamma^2 V^T U1 (kept in Qi)
-        ok = invert(Qi, Ett, aug, m, lane) && ok;
+        ok = invert<m>(Qi, Ett, aug, lane) && ok;
         RS_FOR_ENTRIES(m, lane, {
-            const int r1 = wrap(r + dir, m), c1 = wrap(c + dir, m);
+            const int r1 = wrap<m>(r + dir), c1 = wrap<m>(c + dir);
             const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
             Gss.at(r, c) = csub(Ess.at(r, c), cscale(q, g2));
             V.at(r, c) = cadd(Qi.at(r, c), Qi.at(r1, c));
         })
-        ok = invert(Gss, Gss, aug, m, lane) && ok;
-        mm<false, false, false>(U1, Gss, V, Gss, 1.0, m, lane);
-        mm<true, false, true>(Qi, V, U1, Qi, g2, m, lane);
+        ok = invert<m>(Gss, Gss, aug, lane) && ok;
+        mm<m, false, false, false>(U1, Gss, V, Gss, 1.0, lane);
+        mm<m, true, false, true>(Qi, V, U1, Qi, g2, lane);
         // eps[t][t] -= A g[s][s] A^T (bulk and surface), eps[s][s] -= A^T g[t][t] A
-        mm<false, false, false>(P, Al, Gss, P, 1.0, m, lane);
-        mm<false, true, false>(T, P, Al, T, 1.0, m, lane);
+        mm<m, false, false, false>(P, Al, Gss, P, 1.0, lane);
+        mm<m, false, true, false>(T, P, Al, T, 1.0, lane);
         double d1 = 0.0;
         RS_FOR_ENTRIES(m, lane, {
             const cplxd t = T.at(r, c);
@@ -277,8 +285,8 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(int m, double gamma, con
             d1 = fmax(d1, cabs1(t));
         })
         __syncwarp();
-        mm<true, false, false>(P, Al, Qi, P, 1.0, m, lane);
-        mm<false, false, false>(T, P, Al, T, 1.0, m, lane);
+        mm<m, true, false, false>(P, Al, Qi, P, 1.0, lane);
+        mm<m, false, false, false>(T, P, Al, T, 1.0, lane);
         RS_FOR_ENTRIES(m, lane, {
             const cplxd t = T.at(r, c);
             Ess.at(r, c) = csub(Ess.at(r, c), t);
@@ -286,18 +294,18 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(int m, double gamma, con
         })
         __syncwarp();
         // A <- A g[s][t] A = gamma A U1 A
-        mm<false, false, false>(P, Al, U1, P, 1.0, m, lane);
-        mm<false, false, false>(Al, P, Al, Al, gamma, m, lane);
+        mm<m, false, false, false>(P, Al, U1, P, 1.0, lane);
+        mm<m, false, false, false>(Al, P, Al, Al, gamma, lane);
         if (warp_max(d1) <= tol) break;
     }
     // surface: g_s[s][s] = ((E - u) I - gamma^2 C Est^-1 C^T)^-1
-    ok = invert(Qi, Est, aug, m, lane) && ok;
+    ok = invert<m>(Qi, Est, aug, lane) && ok;
     RS_FOR_ENTRIES(m, lane, {
-        const int r1 = wrap(r + dir, m), c1 = wrap(c + dir, m);
+        const int r1 = wrap<m>(r + dir), c1 = wrap<m>(c + dir);
         const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
         Gss.at(r, c) = csub(r == c ? eu : cmk(0.0, 0.0), cscale(q, g2));
     })
-    ok = invert(Gss, Gss, aug, m, lane) && ok;
+    ok = invert<m>(Gss, Gss, aug, lane) && ok;
     cplxd* out = corners + ((size_t)e * 2 + side) * mm2;
     for (int i = lane; i < mm2; i += 32) out[i] = Gss.a[i];
     if (!ok && lane == 0) atomicExch(status, 1);
@@ -307,7 +315,8 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(int m, double gamma, con
 // Uzero after.  gX: [num_e][K][m*m] scratch (X_k); rows: [num_e][N] ring
 // sums Im(c sum_j G_jj).  The potentials of the next block are loaded while
 // the current block is computed.
-__global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double gamma, const double* __restrict__ Ere,
+template <int m>
+__global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, const double* __restrict__ Ere,
                                                           const double* __restrict__ Eim,
                                                           const double* __restrict__ cre,
                                                           const double* __restrict__ cim, int num_e, int num_u,
@@ -319,12 +328,13 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double g
     const int lane = threadIdx.x;
     const int e = blockIdx.x;
     if (e >= num_e) return;
-    const int mm2 = m * m, N = 2 * K;
+    constexpr int mm2 = m * m;
+    const int N = 2 * K;
     const cplxd E = cmk(Ere[e], Eim[e]);
     const cplxd cc = cmk(cre[e], cim[e]);
     const double g2 = gamma * gamma, g4 = g2 * g2;
     const double* __restrict__ Ua = e < num_u ? Uatoms : Uzero;
-    const Mat X{sh, m}, Gbb{sh + mm2, m}, Gn{sh + 2 * mm2, m}, Z{sh + 3 * mm2, m}, W{sh + 4 * mm2, m};
+    const Mat<m> X{sh}, Gbb{sh + mm2}, Gn{sh + 2 * mm2}, Z{sh + 3 * mm2}, W{sh + 4 * mm2};
     cplxd* aug = sh + 3 * mm2;  // Z and W (2 m^2) while an inversion runs
     cplxd* dv = sh + 5 * mm2;   // D^-1 of the current ring b
     cplxd* da = dv + kMaxM;     // E - U of the current ring a
@@ -344,7 +354,7 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double g
     // g_L[b][b] = D^-1 + gamma^2 Y^T X Y into Gbb
     auto form_gbb = [&]() {
         RS_FOR_ENTRIES(m, lane, {
-            const int r0 = wrap(r - 1, m), c0 = wrap(c - 1, m);
+            const int r0 = wrap<m>(r - 1), c0 = wrap<m>(c - 1);
             const cplxd q = cadd(cadd(X.at(r, c), X.at(r, c0)), cadd(X.at(r0, c), X.at(r0, c0)));
             cplxd v = cscale(cmul(cmul(dv[r], dv[c]), q), g2);
             if (r == c) v = cadd(v, dv[r]);
@@ -364,7 +374,7 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double g
         __syncwarp();
         // S = diag(E - U_a) - gamma^2 g_L[b][b]_{k-1} - gamma^2 C D^-1 C^T
         RS_FOR_ENTRIES(m, lane, {
-            const int r1 = wrap(r + 1, m), c1 = wrap(c + 1, m);
+            const int r1 = wrap<m>(r + 1), c1 = wrap<m>(c + 1);
             cplxd cd = cmk(0.0, 0.0);
             if (r == c) cd = cadd(cd, dv[r]);
             if (r == c1) cd = cadd(cd, dv[r]);
@@ -374,7 +384,7 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double g
             if (r == c) v = cadd(v, da[r]);
             X.at(r, c) = v;
         })
-        ok = invert(X, X, aug, m, lane) && ok;
+        ok = invert<m>(X, X, aug, lane) && ok;
         cplxd* dst = myX + (size_t)k * mm2;
         for (int i = lane; i < mm2; i += 32) dst[i] = X.a[i];
         form_gbb();
@@ -382,10 +392,10 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double g
     // G_K[a][a] of the right lead's first ring: (I - gamma^2 s_R g_L[b][b])^-1 s_R
     for (int i = lane; i < mm2; i += 32) X.a[i] = sR[i];
     __syncwarp();
-    mm<false, false, false>(Gn, X, Gbb, Gn, -g2, m, lane);
+    mm<m, false, false, false>(Gn, X, Gbb, Gn, -g2, lane);
     if (lane < m) Gn.at(lane, lane) = cadd(Gn.at(lane, lane), cmk(1.0, 0.0));
-    ok = invert(Gn, Gn, aug, m, lane) && ok;
-    mm<false, false, false>(Gn, Gn, X, Gn, 1.0, m, lane);
+    ok = invert<m>(Gn, Gn, aug, lane) && ok;
+    mm<m, false, false, false>(Gn, Gn, X, Gn, 1.0, lane);
     fetch_u(K - 1);
     for (int k = K - 1; k >= 0; --k) {
         const cplxd* src = myX + (size_t)k * mm2;
@@ -396,7 +406,7 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double g
         form_gbb();
         // Z = Y G' Y^T, Y = C D^-1
         RS_FOR_ENTRIES(m, lane, {
-            const int r1 = wrap(r + 1, m), c1 = wrap(c + 1, m);
+            const int r1 = wrap<m>(r + 1), c1 = wrap<m>(c + 1);
             cplxd v = cmul(cmul(dv[r], dv[c]), Gn.at(r, c));
             v = cfma(cmul(dv[r], dv[c1]), Gn.at(r, c1), v);
             v = cfma(cmul(dv[r1], dv[c]), Gn.at(r1, c), v);
@@ -405,15 +415,15 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int m, int K, double g
         })
         __syncwarp();
         // tr G[b][b] = tr g_L[b][b] + gamma^2 sum_rc (g_L[b][b] G')[r][c] g_L[b][b][c][r]
-        mm<false, false, false>(W, Gbb, Gn, W, 1.0, m, lane);
+        mm<m, false, false, false>(W, Gbb, Gn, W, 1.0, lane);
         cplxd tb = cmk(0.0, 0.0);
         RS_FOR_ENTRIES(m, lane, {
             tb = cfma(cscale(W.at(r, c), g2), Gbb.at(c, r), tb);
             if (r == c) tb = cadd(tb, Gbb.at(r, r));
         })
         // G[a][a] = X + gamma^4 (X Z) X
-        mm<false, false, false>(Z, X, Z, Z, 1.0, m, lane);
-        mm<false, false, true>(Gn, Z, X, X, g4, m, lane);
+        mm<m, false, false, false>(Z, X, Z, Z, 1.0, lane);
+        mm<m, false, false, true>(Gn, Z, X, X, g4, lane);
         cplxd ta = cmk(0.0, 0.0);
         if (lane < m) ta = Gn.at(lane, lane);
         ta = warp_sum(ta);
@@ -459,31 +469,50 @@ cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_
 
 int rs_max_atoms_per_block() { return 2 * kMaxM; }
 
-cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
-                             const double* d_cre, const double* d_cim, int num_e, int num_u, const double* d_Uatoms,
-                             const double* d_Uzero, double Uc0, double Uc1, int lead_iters, void* d_corners,
-                             void* d_gL, double* d_rows, double* d_Q, int* d_status, cudaStream_t stream) {
-    if (num_e <= 0) return cudaSuccess;
-    if (m < 1 || m > kMaxM || K < 1) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(rs_lead_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)rs_lead_smem_bytes(kMaxM));
+namespace {
+template <int m>
+cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_Eim, const double* d_cre,
+                      const double* d_cim, int num_e, int num_u, const double* d_Uatoms, const double* d_Uzero,
+                      double Uc0, double Uc1, int lead_iters, void* d_corners, void* d_gL, double* d_rows, double* d_Q,
+                      int* d_status, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(rs_lead_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)rs_lead_smem_bytes(m));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(rs_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)rs_chain_smem_bytes(kMaxM));
+    e = cudaFuncSetAttribute(rs_chain_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rs_chain_smem_bytes(m));
     if (e != cudaSuccess) return e;
-    rs_lead_kernel<<<2 * num_e, 32, rs_lead_smem_bytes(m), stream>>>(m, gamma, d_Ere, d_Eim, num_e, num_u, Uc0,
-                                                                     Uc1, lead_iters, static_cast<cplxd*>(d_corners),
-                                                                     d_status);
+    rs_lead_kernel<m><<<2 * num_e, 32, rs_lead_smem_bytes(m), stream>>>(
+        gamma, d_Ere, d_Eim, num_e, num_u, Uc0, Uc1, lead_iters, static_cast<cplxd*>(d_corners), d_status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    rs_chain_kernel<<<num_e, 32, rs_chain_smem_bytes(m), stream>>>(
-        m, K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, num_u, d_Uatoms, d_Uzero,
-        static_cast<const cplxd*>(d_corners), static_cast<cplxd*>(d_gL), d_rows, d_status);
+    rs_chain_kernel<m><<<num_e, 32, rs_chain_smem_bytes(m), stream>>>(
+        K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, num_u, d_Uatoms, d_Uzero, static_cast<const cplxd*>(d_corners),
+        static_cast<cplxd*>(d_gL), d_rows, d_status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int N = 2 * K;
     rs_reduce_kernel<<<(N + 127) / 128, 128, 0, stream>>>(d_rows, num_e, N, d_Q);
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
+                             const double* d_cre, const double* d_cim, int num_e, int num_u, const double* d_Uatoms,
+                             const double* d_Uzero, double Uc0, double Uc1, int lead_iters, void* d_corners,
+                             void* d_gL, double* d_rows, double* d_Q, int* d_status, cudaStream_t stream) {
+    if (num_e <= 0) return cudaSuccess;
+    if (K < 1) return cudaErrorInvalidValue;
+#define RS_CASE(M)                                                                                                 \
+    case M:                                                                                                        \
+        return launch_rs<M>(K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, num_u, d_Uatoms, d_Uzero, Uc0, Uc1,        \
+                            lead_iters, d_corners, d_gL, d_rows, d_Q, d_status, stream);
+    switch (m) {
+        RS_CASE(1) RS_CASE(2) RS_CASE(3) RS_CASE(4) RS_CASE(5) RS_CASE(6) RS_CASE(7) RS_CASE(8)
+        RS_CASE(9) RS_CASE(10) RS_CASE(11) RS_CASE(12) RS_CASE(13) RS_CASE(14) RS_CASE(15) RS_CASE(16)
+        default:
+            return cudaErrorInvalidValue;
+    }
+#undef RS_CASE
 }
 
 }  // namespace negf

@@ -18,9 +18,9 @@ def _eq_kw(m, cells, **extra):
     return kw
 
 
-@pytest.mark.parametrize("m,cells", [(13, 4), (7, 3), (16, 2)])
+@pytest.mark.parametrize("m,cells", [(13, 4), (7, 3), (16, 2), (3, 3), (4, 2), (10, 2), (15, 2)])
 def test_realspace_against_block_oracle(oracle, m, cells):
-    g, o = _pair(oracle, seed=31, **_eq_kw(m, cells))
+    g, o = _pair(oracle, seed=31, **_eq_kw(m, cells, num_modes=1))  # the real-space pass uses every atom
     Qg = g.realspace_charge()
     Qo = o.rs_charge(nthreads=8)
     assert _rel(Qg, Qo) <= TOL, _rel(Qg, Qo)
