@@ -51,7 +51,7 @@
 namespace negf {
 namespace {
 
-constexpr int kMaxM = 16;  // atoms per ring: the augmented m x 2m tile has one lane per column
+constexpr int kMaxM = 16;  // atoms per ring: [S | I] has one lane per column
 
 struct __align__(16) cplxd {
     double x, y;
@@ -147,68 +147,74 @@ __device__ __forceinline__ void mm(Mat<m> C, Mat<m> A, Mat<m> B, Mat<m> D, doubl
     __syncwarp();
 }
 
-// out = S^-1 through the augmented tile aug (m x 2m, ld 2m): Gauss-Jordan
-// with partial pivoting (largest |.|^2 over the rows below, lowest row on
-// ties), lane = column; every lane finds the pivot row itself from the
-// broadcast pivot column.  out may alias S.  Returns false on a zero pivot.
+// out = S^-1 by Gauss-Jordan with partial pivoting (largest |.|^2 over the
+// rows below, lowest row on ties).  Lane c < 2m holds column c of [S | I] in
+// registers; the pivot column reaches every lane through buf (m complex in
+// shared memory), every lane finds the pivot row by a tournament over it,
+// and rows are swapped (a warp-uniform branch) only when the pivot is off
+// the diagonal.  out may alias S.  Returns false on a zero pivot.
 template <int m>
-__device__ __forceinline__ bool invert(Mat<m> out, Mat<m> S, cplxd* aug, int lane) {
+__device__ __forceinline__ bool invert(Mat<m> out, Mat<m> S, cplxd* buf, int lane) {
     constexpr int n2 = 2 * m;
-    const Mat<n2> A{aug};
     __syncwarp();  // S complete
-    if (lane < n2) {
+    cplxd col[m];
 #pragma unroll
-        for (int r = 0; r < m; ++r) A.at(r, lane) = lane < m ? S.at(r, lane) : cmk(lane - m == r ? 1.0 : 0.0, 0.0);
-    }
-    __syncwarp();
+    for (int r = 0; r < m; ++r) col[r] = lane < m ? S.at(r, lane) : cmk(lane - m == r ? 1.0 : 0.0, 0.0);
     bool ok = true;
 #pragma unroll
     for (int p = 0; p < m; ++p) {
-        double best = -1.0;
-        int idx = p;
+        __syncwarp();  // every lane is done with buf (and with S on the first pivot)
+        if (lane == p) {
 #pragma unroll
-        for (int r = p; r < m; ++r) {
-            const cplxd x = A.at(r, p);
-            const double v = fma(x.x, x.x, x.y * x.y);
-            if (v > best) {
-                best = v;
-                idx = r;
-            }
-        }
-        if (!(best > 0.0)) ok = false;
-        __syncwarp();
-        if (idx != p && lane < n2) {
-            const cplxd t = A.at(p, lane);
-            A.at(p, lane) = A.at(idx, lane);
-            A.at(idx, lane) = t;
+            for (int r = 0; r < m; ++r) buf[r] = col[r];
         }
         __syncwarp();
-        const cplxd rp = lane < n2 ? cmul(A.at(p, lane), crcp(A.at(p, p))) : cmk(0.0, 0.0);
-        // eliminate column p from the other rows, 8 rows at a time: the
-        // multipliers of a chunk are read before any lane updates the chunk
+        double bv[m];
+        int bi[m];
 #pragma unroll
-        for (int r0 = 0; r0 < m; r0 += 8) {
-            cplxd f[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int r = r0 + j;
-                f[j] = (r < m && r != p) ? A.at(r, p) : cmk(0.0, 0.0);
+        for (int r = 0; r < m; ++r) {
+            bi[r] = r;
+            bv[r] = -1.0;
+            if (r >= p) {
+                const cplxd x = buf[r];
+                bv[r] = fma(x.x, x.x, x.y * x.y);
             }
-            __syncwarp();
-            if (lane < n2) {
+        }
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int r = r0 + j;
-                    if (r < m && r != p) A.at(r, lane) = cfms(f[j], rp, A.at(r, lane));
+        for (int st = 1; st < m; st *= 2) {
+#pragma unroll
+            for (int r = 0; r + st < m; r += 2 * st) {
+                if (bv[r + st] > bv[r]) {
+                    bv[r] = bv[r + st];
+                    bi[r] = bi[r + st];
                 }
             }
         }
-        if (lane < n2) A.at(p, lane) = rp;
-        __syncwarp();
+        const int idx = bi[0];
+        if (!(bv[0] > 0.0)) ok = false;
+        if (idx != p) {
+#pragma unroll
+            for (int r = p + 1; r < m; ++r) {
+                if (r == idx) {
+                    const cplxd t = col[r];
+                    col[r] = col[p];
+                    col[p] = t;
+                }
+            }
+        }
+        // multiplier of row r after the swap: buf[r], but buf[p] for row idx
+        const cplxd rp = cmul(col[p], crcp(buf[idx]));
+#pragma unroll
+        for (int r = 0; r < m; ++r) {
+            if (r == 8) asm volatile("" ::: "memory");  // two batches of multiplier loads
+            if (r != p) col[r] = cfms(buf[r == idx ? p : r], rp, col[r]);
+        }
+        col[p] = rp;
     }
+    __syncwarp();
     if (lane >= m && lane < n2) {
 #pragma unroll
-        for (int r = 0; r < m; ++r) out.at(r, lane - m) = A.at(r, lane);
+        for (int r = 0; r < m; ++r) out.at(r, lane - m) = col[r];
     }
     __syncwarp();
     return ok;
@@ -246,7 +252,7 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const doub
     constexpr int mm2 = m * m;
     const Mat<m> Ess{sh}, Ett{sh + mm2}, Est{sh + 2 * mm2}, Al{sh + 3 * mm2}, Qi{sh + 4 * mm2}, Gss{sh + 5 * mm2},
         V{sh + 6 * mm2}, U1{sh + 7 * mm2}, P{sh + 8 * mm2}, T{sh + 9 * mm2};
-    cplxd* aug = sh + 10 * mm2;  // m x 2m
+    cplxd* buf = sh + 10 * mm2;  // pivot column
     const double u = e >= num_u ? 0.0 : (side == 0 ? Uc0 : Uc1);
     const cplxd eu = cmk(Ere[e] - u, Eim[e]);
     const double g2 = gamma * gamma;
@@ -264,14 +270,14 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const doub
         // cell inverse: Qi = Ett^-1, g[s][s] = (Ess - gamma^2 C Qi C^T)^-1,
         // V = C Qi, U1 = g[s][s] V (g[s][t] = gamma U1),
         // g[t][t] = Qi + gamma^2 V^T U1 (kept in Qi)
-        ok = invert<m>(Qi, Ett, aug, lane) && ok;
+        ok = invert<m>(Qi, Ett, buf, lane) && ok;
         RS_FOR_ENTRIES(m, lane, {
             const int r1 = wrap<m>(r + dir), c1 = wrap<m>(c + dir);
             const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
             Gss.at(r, c) = csub(Ess.at(r, c), cscale(q, g2));
             V.at(r, c) = cadd(Qi.at(r, c), Qi.at(r1, c));
         })
-        ok = invert<m>(Gss, Gss, aug, lane) && ok;
+        ok = invert<m>(Gss, Gss, buf, lane) && ok;
         mm<m, false, false, false>(U1, Gss, V, Gss, 1.0, lane);
         mm<m, true, false, true>(Qi, V, U1, Qi, g2, lane);
         // eps[t][t] -= A g[s][s] A^T (bulk and surface), eps[s][s] -= A^T g[t][t] A
@@ -299,13 +305,13 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const doub
         if (warp_max(d1) <= tol) break;
     }
     // surface: g_s[s][s] = ((E - u) I - gamma^2 C Est^-1 C^T)^-1
-    ok = invert<m>(Qi, Est, aug, lane) && ok;
+    ok = invert<m>(Qi, Est, buf, lane) && ok;
     RS_FOR_ENTRIES(m, lane, {
         const int r1 = wrap<m>(r + dir), c1 = wrap<m>(c + dir);
         const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
         Gss.at(r, c) = csub(r == c ? eu : cmk(0.0, 0.0), cscale(q, g2));
     })
-    ok = invert<m>(Gss, Gss, aug, lane) && ok;
+    ok = invert<m>(Gss, Gss, buf, lane) && ok;
     cplxd* out = corners + ((size_t)e * 2 + side) * mm2;
     for (int i = lane; i < mm2; i += 32) out[i] = Gss.a[i];
     if (!ok && lane == 0) atomicExch(status, 1);
@@ -335,9 +341,9 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
     const double g2 = gamma * gamma, g4 = g2 * g2;
     const double* __restrict__ Ua = e < num_u ? Uatoms : Uzero;
     const Mat<m> X{sh}, Gbb{sh + mm2}, Gn{sh + 2 * mm2}, Z{sh + 3 * mm2}, W{sh + 4 * mm2};
-    cplxd* aug = sh + 3 * mm2;  // Z and W (2 m^2) while an inversion runs
     cplxd* dv = sh + 5 * mm2;   // D^-1 of the current ring b
     cplxd* da = dv + kMaxM;     // E - U of the current ring a
+    cplxd* buf = da + kMaxM;    // pivot column
     const cplxd* sL = corners + (size_t)e * 2 * mm2;
     const cplxd* sR = sL + mm2;
     cplxd* myX = gX + (size_t)e * K * mm2;
@@ -384,7 +390,7 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
             if (r == c) v = cadd(v, da[r]);
             X.at(r, c) = v;
         })
-        ok = invert<m>(X, X, aug, lane) && ok;
+        ok = invert<m>(X, X, buf, lane) && ok;
         cplxd* dst = myX + (size_t)k * mm2;
         for (int i = lane; i < mm2; i += 32) dst[i] = X.a[i];
         form_gbb();
@@ -394,7 +400,7 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
     __syncwarp();
     mm<m, false, false, false>(Gn, X, Gbb, Gn, -g2, lane);
     if (lane < m) Gn.at(lane, lane) = cadd(Gn.at(lane, lane), cmk(1.0, 0.0));
-    ok = invert<m>(Gn, Gn, aug, lane) && ok;
+    ok = invert<m>(Gn, Gn, buf, lane) && ok;
     mm<m, false, false, false>(Gn, Gn, X, Gn, 1.0, lane);
     fetch_u(K - 1);
     for (int k = K - 1; k >= 0; --k) {
@@ -456,8 +462,8 @@ __global__ void rs_expand_kernel(const double* __restrict__ U, int N, int m, dou
     if (i < N * m) Ua[i] = U[i / m];
 }
 
-size_t rs_lead_smem_bytes(int m) { return sizeof(cplxd) * 12 * m * m; }
-size_t rs_chain_smem_bytes(int m) { return sizeof(cplxd) * (5 * m * m + 2 * kMaxM); }
+size_t rs_lead_smem_bytes(int m) { return sizeof(cplxd) * (10 * m * m + kMaxM); }
+size_t rs_chain_smem_bytes(int m) { return sizeof(cplxd) * (5 * m * m + 3 * kMaxM); }
 
 }  // namespace
 
