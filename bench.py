@@ -301,6 +301,19 @@ def config3_measure(torch, passes=2):
     torch.cuda.synchronize()
     sec = (time.perf_counter() - t0) / passes
     Qm = t.Solve_NEGF()
+    # mixed precision: FP32 chains with tensor-core products away from the real axis
+    tm = CNT(**kw, precision="mixed")
+    tm.set_potential(U, (U[0], U[-1]))
+    Qx = torch.zeros_like(Q)
+    tm.realspace_charge(out=Qx)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(passes):
+        tm.realspace_charge(out=Qx)
+    torch.cuda.synchronize()
+    sec_mixed = (time.perf_counter() - t0) / passes
+    Eall = np.concatenate([t.energy_points(1)[0], t.energy_points(2)[0]])
+    n32 = int(np.sum(np.abs(Eall.imag) >= 1e-3))
     E = len(t.energy_points(1)[0]) + len(t.energy_points(2)[0])
     E0 = len(t.energy_points(0)[0])
     K, m = t.num_field_sites // 2, 13
@@ -316,7 +329,12 @@ def config3_measure(torch, passes=2):
             "flop_convention": "ring corners m=13: inverse 8m^3 + three complex products 8m^3 per block update "
                                "(leads not counted)",
             "path": "negf_rs_compute_charge (FP64 CUDA cores, one warp per energy, Schur complements on ring corners)",
-            "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm)))}
+            "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm))),
+            "mixed": {"seconds_per_pass": sec_mixed, "block_updates_per_s": (E + E0) * K / sec_mixed,
+                      "fp32_energies": n32, "fp64_energies": E + E0 - n32,
+                      "path": "FP32 chains: TF32 tensor-core products (high/remainder split, 3 real products per "
+                              "complex product), FP32 inversion; FP64 leads, Rho0 and near-axis chains",
+                      "max_rel_vs_fp64": float(np.max(np.abs(Qx.cpu().numpy() - Qr)) / np.max(np.abs(Qr)))}}
 
 
 def long_tube_measure(torch, reps=10):

@@ -1626,45 +1626,55 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     if (t->noneq) return fail(NEGF_ERR_STATE, "the real-space pass covers the equilibrium charge (contour and poles)");
     cudaStream_t s = (cudaStream_t)stream;
     const int N = t->N, K = N / 2;
-    // energies: RhoEq contour and poles (coefficients as in the mode-space pass), then Rho0 at U = 0
-    std::vector<double> Er, Ei, cr, ci;
+    // energies: RhoEq contour and poles (coefficients as in the mode-space
+    // pass) and Rho0 at U = 0 with negated coefficients, in one launch.  In
+    // mixed mode the contour and pole points at least mixed_fp64_band above
+    // the real axis run in FP32; the FP64 chains go first in the launch.
+    struct RsE {
+        double Er, Ei, cr, ci;
+        int flags;
+    };
+    std::vector<RsE> e64, e32;
+    const bool mixed = t->d.precision == NEGF_PREC_MIXED;
     const int neq = pass_items(*t, false);
     for (int idx = 0; idx < neq; ++idx) {
         const Item it = pass_item(*t, false, idx);
-        Er.push_back(it.E.real());
-        Ei.push_back(it.E.imag());
-        cr.push_back(it.c.real());
-        ci.push_back(it.c.imag());
+        const bool fp32 = mixed && std::fabs(it.E.imag()) >= t->d.mixed_fp64_band;
+        (fp32 ? e32 : e64).push_back({it.E.real(), it.E.imag(), it.c.real(), it.c.imag(), fp32 ? 1 : 0});
     }
-    // Rho0 at U = 0 in the same launch, with negated coefficients
     rho0_paths(*t);
     const int n0 = pass_items(*t, true);
     for (int idx = 0; idx < n0; ++idx) {
         const Item it = pass_item(*t, true, idx);
-        Er.push_back(it.E.real());
-        Ei.push_back(it.E.imag());
-        cr.push_back(-it.c.real());
-        ci.push_back(-it.c.imag());
+        e64.push_back({it.E.real(), it.E.imag(), -it.c.real(), -it.c.imag(), 2});
     }
-    const int P = (int)Er.size();
+    std::vector<RsE> all(e64);
+    all.insert(all.end(), e32.begin(), e32.end());
+    const int P = (int)all.size();
     const size_t mm = (size_t)m * m;
     const size_t pe = (size_t)std::max(P, 1);
     // grow-only buffers kept across calls (serialised by g_mu)
-    static DevBuf bE, bU0, bUa, bCorners, bGL, bRows, bStatus;
+    static DevBuf bE, bFlags, bU0, bUa, bCorners, bGL, bRows, bStatus;
     NEGF_CUDA(bE.reserve(sizeof(double) * 4 * pe));
+    NEGF_CUDA(bFlags.reserve(sizeof(int) * pe));
     NEGF_CUDA(bUa.reserve(sizeof(double) * (size_t)N * m));
     NEGF_CUDA(bU0.reserve(sizeof(double) * (size_t)N * m));
     NEGF_CUDA(bCorners.reserve(16 * 2 * mm * pe));
     NEGF_CUDA(bGL.reserve(16 * mm * K * pe));
     NEGF_CUDA(bRows.reserve(sizeof(double) * (size_t)N * pe));
     NEGF_CUDA(bStatus.reserve(sizeof(int)));
-    std::vector<double> host(4 * (size_t)P);
-    std::copy(Er.begin(), Er.end(), host.begin());
-    std::copy(Ei.begin(), Ei.end(), host.begin() + P);
-    std::copy(cr.begin(), cr.end(), host.begin() + 2 * P);
-    std::copy(ci.begin(), ci.end(), host.begin() + 3 * P);
+    std::vector<double> host(4 * pe);
+    std::vector<int> hflags(pe, 0);
+    for (int i = 0; i < P; ++i) {
+        host[i] = all[i].Er;
+        host[P + i] = all[i].Ei;
+        host[2 * P + i] = all[i].cr;
+        host[3 * P + i] = all[i].ci;
+        hflags[i] = all[i].flags;
+    }
     double* dE = bE.as<double>();
     NEGF_CUDA(cudaMemcpyAsync(dE, host.data(), sizeof(double) * 4 * P, cudaMemcpyHostToDevice, s));
+    NEGF_CUDA(cudaMemcpyAsync(bFlags.p, hflags.data(), sizeof(int) * P, cudaMemcpyHostToDevice, s));
     NEGF_CUDA(cudaMemsetAsync(bStatus.p, 0, sizeof(int), s));
     NEGF_CUDA(cudaMemsetAsync(bU0.p, 0, sizeof(double) * (size_t)N * m, s));
     const double* Ua = d_Uatoms;
@@ -1674,8 +1684,8 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     }
     const int iters = t->d.decimation_max_iter + 2;
     if (P > 0)
-        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, P, neq, Ua,
-                                         bU0.as<double>(), t->Uc[0], t->Uc[1], iters, bCorners.p, bGL.p,
+        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, P, bFlags.as<int>(),
+                                         Ua, bU0.as<double>(), t->Uc[0], t->Uc[1], iters, bCorners.p, bGL.p,
                                          bRows.as<double>(), d_Q, bStatus.as<int>(), s));
     else
         NEGF_CUDA(cudaMemsetAsync(d_Q, 0, sizeof(double) * N, s));

@@ -81,16 +81,17 @@ cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, c
                              double* d_chain_out, double* d_site, long long site_stride, int num_e, int M, int upw,
                              double* d_red, double* d_ldos, int N, cudaStream_t stream);
 // Real-space ring-block RGF (negf_realspace.cu): leads, chain and reduction
-// for num_e energies with coefficients c, Q[r] = sum_e Im(c sum_atoms G_jj);
-// energies e < num_u see the atom potentials d_Uatoms ([2K][m]) and the
-// contact potentials Uc0, Uc1, the others d_Uzero and 0 (a U = 0 pass with
-// negated c subtracts it).  d_corners: num_e * 2 * m^2 complex, d_gL:
-// num_e * K * m^2 complex, d_rows: num_e * 2K doubles; *d_status set to 1 on
-// a zero pivot.
+// for num_e energies with coefficients c, Q[r] = sum_e Im(c sum_atoms G_jj).
+// d_flags[e]: 1 = chain in FP32 (tensor-core products), 2 = U = 0 pass
+// (d_Uzero on the atoms and 0 at the contacts; with negated c it subtracts
+// Rho0); otherwise the atom potentials d_Uatoms ([2K][m]) and Uc0, Uc1.
+// d_corners: num_e * 2 * m^2 complex, d_gL: num_e * K * m^2 complex,
+// d_rows: num_e * 2K doubles; *d_status set to 1 on a zero pivot.
 cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
-                             const double* d_cre, const double* d_cim, int num_e, int num_u, const double* d_Uatoms,
-                             const double* d_Uzero, double Uc0, double Uc1, int lead_iters, void* d_corners,
-                             void* d_gL, double* d_rows, double* d_Q, int* d_status, cudaStream_t stream);
+                             const double* d_cre, const double* d_cim, int num_e, const int* d_flags,
+                             const double* d_Uatoms, const double* d_Uzero, double Uc0, double Uc1, int lead_iters,
+                             void* d_corners, void* d_gL, double* d_rows, double* d_Q, int* d_status,
+                             cudaStream_t stream);
 cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_t stream);
 int rs_max_atoms_per_block();
 

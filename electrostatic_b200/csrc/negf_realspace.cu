@@ -1,4 +1,4 @@
-// Real-space ring-block RGF of a zigzag (m,0) tube (FP64).
+// Real-space ring-block RGF of a zigzag (m,0) tube (FP64, or mixed FP32/FP64).
 //
 // Blocks of two rings (2m atoms, m <= 16): ring a = 2k and ring b = 2k+1 are
 // joined by the double bond (atom j of a to atoms j and j+1 mod m of b:
@@ -45,6 +45,17 @@
 // The energies of the U = 0 pass (Rho0) run in the same launches with
 // negated coefficients, so one reduction gives the induced charge.
 // Inversions: Gauss-Jordan with partial pivoting on [S | I] (lane = column).
+//
+// Mixed precision: the chain of an energy runs in FP32 when its tube is in
+// mixed mode and the point lies at least mixed_fp64_band above the real axis
+// (the rule of the mode-space pass); the leads, the other energies, the ring
+// sums per energy and their Kahan sum stay FP64.  In FP32 the m x m
+// products run on the tensor cores: mma.sync m16n8k8 TF32 with each operand
+// split into a TF32 high part and a TF32 remainder (three products per
+// pair, about FP32 accuracy) and the complex product in the three-multiply
+// form Re = ArBr - AiBi, Im = (Ar + Ai)(Br + Bi) - ArBr - AiBi; the
+// inversion runs on the FP32 cores.  One launch holds both precisions (the
+// FP64 energies first).
 
 #include "negf_internal.h"
 
@@ -53,44 +64,70 @@ namespace {
 
 constexpr int kMaxM = 16;  // atoms per ring: [S | I] has one lane per column
 
-struct __align__(16) cplxd {
-    double x, y;
+template <typename R>
+struct __align__(2 * sizeof(R)) cplx {
+    R x, y;
 };
-__device__ __forceinline__ cplxd cmk(double a, double b) { return {a, b}; }
-__device__ __forceinline__ cplxd cadd(cplxd a, cplxd b) { return {a.x + b.x, a.y + b.y}; }
-__device__ __forceinline__ cplxd csub(cplxd a, cplxd b) { return {a.x - b.x, a.y - b.y}; }
-__device__ __forceinline__ cplxd cscale(cplxd a, double s) { return {a.x * s, a.y * s}; }
-__device__ __forceinline__ cplxd cmul(cplxd a, cplxd b) { return {fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x)}; }
+using cplxd = cplx<double>;
+using cplxf = cplx<float>;
+template <typename R>
+__device__ __forceinline__ cplx<R> cmk(R a, R b) {
+    return {a, b};
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> cadd(cplx<R> a, cplx<R> b) {
+    return {a.x + b.x, a.y + b.y};
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> csub(cplx<R> a, cplx<R> b) {
+    return {a.x - b.x, a.y - b.y};
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> cscale(cplx<R> a, R s) {
+    return {a.x * s, a.y * s};
+}
+template <typename R>
+__device__ __forceinline__ cplx<R> cmul(cplx<R> a, cplx<R> b) {
+    return {fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x)};
+}
 // acc + a b
-__device__ __forceinline__ cplxd cfma(cplxd a, cplxd b, cplxd acc) {
+template <typename R>
+__device__ __forceinline__ cplx<R> cfma(cplx<R> a, cplx<R> b, cplx<R> acc) {
     return {fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y))};
 }
 // acc - a b
-__device__ __forceinline__ cplxd cfms(cplxd a, cplxd b, cplxd acc) {
+template <typename R>
+__device__ __forceinline__ cplx<R> cfms(cplx<R> a, cplx<R> b, cplx<R> acc) {
     return {fma(-a.x, b.x, fma(a.y, b.y, acc.x)), fma(-a.x, b.y, fma(-a.y, b.x, acc.y))};
 }
 __device__ __forceinline__ double cabs1(cplxd a) { return fabs(a.x) + fabs(a.y); }
 // Reciprocal: hardware approximation y0 = rcp.approx.ftz(x) with relative
 // error e = 1 - x y0 (|e| <= 2^-20 or better), corrected by the truncated
-// series 1/x = y0 (1 + e + e^2 + ...) to a relative error of order e^3.
-// Arguments are squared moduli of pivots and of E - U (normal numbers).
-__device__ __forceinline__ double rcp64(double x) {
+// series 1/x = y0 (1 + e + e^2 + ...) to a relative error of order e^3 (FP64)
+// or e^2 (FP32).  Arguments are squared moduli of pivots and of E - U.
+__device__ __forceinline__ double rcp_r(double x) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     const double e = fma(-x, y, 1.0);
     return fma(y, fma(e, e, e), y);
 }
+__device__ __forceinline__ float rcp_r(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return fmaf(y, fmaf(-x, y, 1.0f), y);
+}
 // 1 / b = conj(b) / |b|^2
-__device__ __forceinline__ cplxd crcp(cplxd b) {
-    const double q = rcp64(fma(b.x, b.x, b.y * b.y));
+template <typename R>
+__device__ __forceinline__ cplx<R> crcp(cplx<R> b) {
+    const R q = rcp_r(fma(b.x, b.x, b.y * b.y));
     return {b.x * q, -b.y * q};
 }
 
 // Complex tile, row-major with compile-time leading dimension LD
-template <int LD>
+template <int LD, typename R>
 struct Mat {
-    cplxd* a;
-    __device__ __forceinline__ cplxd& at(int r, int c) const { return a[r * LD + c]; }
+    cplx<R>* a;
+    __device__ __forceinline__ cplx<R>& at(int r, int c) const { return a[r * LD + c]; }
 };
 
 template <int M>
@@ -116,7 +153,8 @@ __device__ __forceinline__ int wrap(int i) { return i < 0 ? i + M : (i >= M ? i 
 // C = s op(A) op(B) (+ D when ADD); op = transpose for TA / TB.  C may alias
 // any operand: the products are staged in registers.
 template <int m, bool TA, bool TB, bool ADD>
-__device__ __forceinline__ void mm(Mat<m> C, Mat<m> A, Mat<m> B, Mat<m> D, double s, int lane) {
+__device__ __forceinline__ void mm(Mat<m, double> C, Mat<m, double> A, Mat<m, double> B, Mat<m, double> D, double s,
+                                   int lane) {
     const int c = lane & 15, h = lane >> 4;
     cplxd acc[8];
 #pragma unroll
@@ -147,19 +185,102 @@ __device__ __forceinline__ void mm(Mat<m> C, Mat<m> A, Mat<m> B, Mat<m> D, doubl
     __syncwarp();
 }
 
+// TF32 tensor-core product D += A B of a 16 x 8 x 8 tile (mma.sync
+// m16n8k8, FP32 accumulate).  Fragments, g = lane / 4, t = lane % 4:
+// a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g];
+// d = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1].
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+// x = hi + lo with hi the TF32 rounding of x and lo the TF32 rounding of the rest
+__device__ __forceinline__ void split_tf32(float x, unsigned& hi, unsigned& lo) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    const float rest = x - __uint_as_float(hi);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(rest));
+}
+// D += A B in three tensor-core products: lo hi + hi lo + hi hi
+__device__ __forceinline__ void mma3(float (&d)[4], const unsigned (&ah)[4], const unsigned (&al)[4],
+                                     const unsigned (&bh)[2], const unsigned (&bl)[2]) {
+    mma_tf32(d, al, bh);
+    mma_tf32(d, ah, bl);
+    mma_tf32(d, ah, bh);
+}
+
+// C = s op(A) op(B) (+ D when ADD) in FP32 on the tensor cores: the m x m
+// tiles are read as zero-padded 16 x 16 operands, the complex product in
+// the three-multiply form.  C may alias any operand.
+template <int m, bool TA, bool TB, bool ADD>
+__device__ __forceinline__ void mm(Mat<m, float> C, Mat<m, float> A, Mat<m, float> B, Mat<m, float> D, float s,
+                                   int lane) {
+    const int g = lane >> 2, t = lane & 3;
+    float t1[2][4], t2[2][4], t3[2][4];  // Ar Br, Ai Bi, (Ar + Ai)(Br + Bi) per 8-column tile
+#pragma unroll
+    for (int n = 0; n < 2; ++n)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t1[n][q] = t2[n][q] = t3[n][q] = 0.0f;
+#pragma unroll
+    for (int k0 = 0; k0 < m; k0 += 8) {
+        unsigned arh[4], arl[4], aih[4], ail[4], ash[4], asl[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = g + ((q & 1) ? 8 : 0), k = k0 + t + ((q & 2) ? 4 : 0);
+            cplxf v = cmk(0.0f, 0.0f);
+            if (r < m && k < m) v = TA ? A.at(k, r) : A.at(r, k);
+            split_tf32(v.x, arh[q], arl[q]);
+            split_tf32(v.y, aih[q], ail[q]);
+            split_tf32(v.x + v.y, ash[q], asl[q]);
+        }
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+            if (8 * n < m) {
+                unsigned brh[2], brl[2], bih[2], bil[2], bsh[2], bsl[2];
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int k = k0 + t + 4 * q, c = 8 * n + g;
+                    cplxf v = cmk(0.0f, 0.0f);
+                    if (k < m && c < m) v = TB ? B.at(c, k) : B.at(k, c);
+                    split_tf32(v.x, brh[q], brl[q]);
+                    split_tf32(v.y, bih[q], bil[q]);
+                    split_tf32(v.x + v.y, bsh[q], bsl[q]);
+                }
+                mma3(t1[n], arh, arl, brh, brl);
+                mma3(t2[n], aih, ail, bih, bil);
+                mma3(t3[n], ash, asl, bsh, bsl);
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = g + ((q & 2) ? 8 : 0), c = 8 * n + 2 * t + (q & 1);
+            if (r < m && c < m) {
+                cplxf v = cmk((t1[n][q] - t2[n][q]) * s, (t3[n][q] - t1[n][q] - t2[n][q]) * s);
+                if (ADD) v = cadd(v, D.at(r, c));
+                C.at(r, c) = v;
+            }
+        }
+    }
+    __syncwarp();
+}
+
 // out = S^-1 by Gauss-Jordan with partial pivoting (largest |.|^2 over the
 // rows below, lowest row on ties).  Lane c < 2m holds column c of [S | I] in
 // registers; the pivot column reaches every lane through buf (m complex in
 // shared memory), every lane finds the pivot row by a tournament over it,
 // and rows are swapped (a warp-uniform branch) only when the pivot is off
 // the diagonal.  out may alias S.  Returns false on a zero pivot.
-template <int m>
-__device__ __forceinline__ bool invert(Mat<m> out, Mat<m> S, cplxd* buf, int lane) {
+template <int m, typename R>
+__device__ __forceinline__ bool invert(Mat<m, R> out, Mat<m, R> S, cplx<R>* buf, int lane) {
     constexpr int n2 = 2 * m;
     __syncwarp();  // S complete
-    cplxd col[m];
+    cplx<R> col[m];
 #pragma unroll
-    for (int r = 0; r < m; ++r) col[r] = lane < m ? S.at(r, lane) : cmk(lane - m == r ? 1.0 : 0.0, 0.0);
+    for (int r = 0; r < m; ++r) col[r] = lane < m ? S.at(r, lane) : cmk<R>(lane - m == r ? R(1) : R(0), R(0));
     bool ok = true;
 #pragma unroll
     for (int p = 0; p < m; ++p) {
@@ -169,14 +290,14 @@ __device__ __forceinline__ bool invert(Mat<m> out, Mat<m> S, cplxd* buf, int lan
             for (int r = 0; r < m; ++r) buf[r] = col[r];
         }
         __syncwarp();
-        double bv[m];
+        R bv[m];
         int bi[m];
 #pragma unroll
         for (int r = 0; r < m; ++r) {
             bi[r] = r;
-            bv[r] = -1.0;
+            bv[r] = R(-1);
             if (r >= p) {
-                const cplxd x = buf[r];
+                const cplx<R> x = buf[r];
                 bv[r] = fma(x.x, x.x, x.y * x.y);
             }
         }
@@ -191,19 +312,19 @@ __device__ __forceinline__ bool invert(Mat<m> out, Mat<m> S, cplxd* buf, int lan
             }
         }
         const int idx = bi[0];
-        if (!(bv[0] > 0.0)) ok = false;
+        if (!(bv[0] > R(0))) ok = false;
         if (idx != p) {
 #pragma unroll
             for (int r = p + 1; r < m; ++r) {
                 if (r == idx) {
-                    const cplxd t = col[r];
+                    const cplx<R> t = col[r];
                     col[r] = col[p];
                     col[p] = t;
                 }
             }
         }
         // multiplier of row r after the swap: buf[r], but buf[p] for row idx
-        const cplxd rp = cmul(col[p], crcp(buf[idx]));
+        const cplx<R> rp = cmul(col[p], crcp(buf[idx]));
 #pragma unroll
         for (int r = 0; r < m; ++r) {
             if (r == 8) asm volatile("" ::: "memory");  // two batches of multiplier loads
@@ -234,14 +355,19 @@ __device__ __forceinline__ cplxd warp_sum(cplxd v) {
     return v;
 }
 
+// Energy flags: kRsFP32 runs the chain in FP32, kRsZeroU takes U = 0 on the
+// atoms and the contacts (the Rho0 pass).
+constexpr int kRsFP32 = 1, kRsZeroU = 2;
+
 // Lead kernel: warp w -> energy w / 2, lead w % 2 (0 left: s = ring b, the
 // intra-cell bond from s to t is C^T; 1 right: s = ring a, bond C), the lead
-// cell at the contact potential (0 for the energies e >= num_u, the U = 0
-// pass).  corners[e][side] = g_surface[s][s] (m x m, row-major).
+// cell at the contact potential.  corners[e][side] = g_surface[s][s] (m x m,
+// row-major).
 template <int m>
 __global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const double* __restrict__ Ere,
-                                                        const double* __restrict__ Eim, int num_e, int num_u,
-                                                        double Uc0, double Uc1, int iters,
+                                                        const double* __restrict__ Eim, int num_e,
+                                                        const int* __restrict__ flags, double Uc0, double Uc1,
+                                                        int iters,
                                                         cplxd* __restrict__ corners, int* __restrict__ status) {
     extern __shared__ cplxd sh[];
     const int lane = threadIdx.x;
@@ -250,10 +376,10 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const doub
     const int e = w / 2, side = w % 2;
     const int dir = side == 0 ? -1 : 1;  // C_st[i][l] != 0 for l in {i, i + dir}
     constexpr int mm2 = m * m;
-    const Mat<m> Ess{sh}, Ett{sh + mm2}, Est{sh + 2 * mm2}, Al{sh + 3 * mm2}, Qi{sh + 4 * mm2}, Gss{sh + 5 * mm2},
-        V{sh + 6 * mm2}, U1{sh + 7 * mm2}, P{sh + 8 * mm2}, T{sh + 9 * mm2};
+    const Mat<m, double> Ess{sh}, Ett{sh + mm2}, Est{sh + 2 * mm2}, Al{sh + 3 * mm2}, Qi{sh + 4 * mm2},
+        Gss{sh + 5 * mm2}, V{sh + 6 * mm2}, U1{sh + 7 * mm2}, P{sh + 8 * mm2}, T{sh + 9 * mm2};
     cplxd* buf = sh + 10 * mm2;  // pivot column
-    const double u = e >= num_u ? 0.0 : (side == 0 ? Uc0 : Uc1);
+    const double u = (flags[e] & kRsZeroU) ? 0.0 : (side == 0 ? Uc0 : Uc1);
     const cplxd eu = cmk(Ere[e] - u, Eim[e]);
     const double g2 = gamma * gamma;
     const double tol = 1e-18 * (cabs1(eu) + fabs(gamma));
@@ -317,59 +443,44 @@ __global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const doub
     if (!ok && lane == 0) atomicExch(status, 1);
 }
 
-// Chain kernel: warp e -> energy e, atom potentials Uatoms for e < num_u and
-// Uzero after.  gX: [num_e][K][m*m] scratch (X_k); rows: [num_e][N] ring
-// sums Im(c sum_j G_jj).  The potentials of the next block are loaded while
-// the current block is computed.
-template <int m>
-__global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, const double* __restrict__ Ere,
-                                                          const double* __restrict__ Eim,
-                                                          const double* __restrict__ cre,
-                                                          const double* __restrict__ cim, int num_e, int num_u,
-                                                          const double* __restrict__ Uatoms,
-                                                          const double* __restrict__ Uzero,
-                                                          const cplxd* __restrict__ corners, cplxd* __restrict__ gX,
-                                                          double* __restrict__ rows, int* __restrict__ status) {
-    extern __shared__ cplxd sh[];
-    const int lane = threadIdx.x;
-    const int e = blockIdx.x;
-    if (e >= num_e) return;
+// One energy's chain in precision R (warp e): atom potentials Ua, lead
+// corners (FP64, m x m, row-major), scratch myX for X_k (K m^2 complex R),
+// row of 2K ring sums Im(c sum_j G_jj) written in FP64.  The potentials of
+// the next block are loaded while the current block is computed.
+template <int m, typename R>
+__device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, const double* __restrict__ Ua,
+                                         const cplxd* __restrict__ sL, const cplxd* __restrict__ sR,
+                                         cplx<R>* __restrict__ myX, double* __restrict__ row, cplx<R>* sh, int lane) {
+    using C = cplx<R>;
     constexpr int mm2 = m * m;
-    const int N = 2 * K;
-    const cplxd E = cmk(Ere[e], Eim[e]);
-    const cplxd cc = cmk(cre[e], cim[e]);
-    const double g2 = gamma * gamma, g4 = g2 * g2;
-    const double* __restrict__ Ua = e < num_u ? Uatoms : Uzero;
-    const Mat<m> X{sh}, Gbb{sh + mm2}, Gn{sh + 2 * mm2}, Z{sh + 3 * mm2}, W{sh + 4 * mm2};
-    cplxd* dv = sh + 5 * mm2;   // D^-1 of the current ring b
-    cplxd* da = dv + kMaxM;     // E - U of the current ring a
-    cplxd* buf = da + kMaxM;    // pivot column
-    const cplxd* sL = corners + (size_t)e * 2 * mm2;
-    const cplxd* sR = sL + mm2;
-    cplxd* myX = gX + (size_t)e * K * mm2;
-    double* row = rows + (size_t)e * N;
+    const R g2 = gamma * gamma, g4 = g2 * g2;
+    const R zero(0), one(1);
+    const Mat<m, R> X{sh}, Gbb{sh + mm2}, Gn{sh + 2 * mm2}, Z{sh + 3 * mm2}, W{sh + 4 * mm2};
+    C* dv = sh + 5 * mm2;  // D^-1 of the current ring b
+    C* da = dv + kMaxM;    // E - U of the current ring a
+    C* buf = da + kMaxM;   // pivot column
     bool ok = true;
     // lane j < m: potentials of atom j on rings a and b of the next block
-    double ua_n = 0.0, ub_n = 0.0;
+    R ua_n = zero, ub_n = zero;
     auto fetch_u = [&](int k) {
         if (lane < m) {
-            ua_n = __ldg(Ua + (size_t)(2 * k) * m + lane);
-            ub_n = __ldg(Ua + (size_t)(2 * k + 1) * m + lane);
+            ua_n = (R)__ldg(Ua + (size_t)(2 * k) * m + lane);
+            ub_n = (R)__ldg(Ua + (size_t)(2 * k + 1) * m + lane);
         }
     };
     // g_L[b][b] = D^-1 + gamma^2 Y^T X Y into Gbb
     auto form_gbb = [&]() {
         RS_FOR_ENTRIES(m, lane, {
             const int r0 = wrap<m>(r - 1), c0 = wrap<m>(c - 1);
-            const cplxd q = cadd(cadd(X.at(r, c), X.at(r, c0)), cadd(X.at(r0, c), X.at(r0, c0)));
-            cplxd v = cscale(cmul(cmul(dv[r], dv[c]), q), g2);
+            const C q = cadd(cadd(X.at(r, c), X.at(r, c0)), cadd(X.at(r0, c), X.at(r0, c0)));
+            C v = cscale(cmul(cmul(dv[r], dv[c]), q), g2);
             if (r == c) v = cadd(v, dv[r]);
             Gbb.at(r, c) = v;
         })
         __syncwarp();
     };
     // left lead corner as g_L[b][b] of block -1
-    for (int i = lane; i < mm2; i += 32) Gbb.a[i] = sL[i];
+    for (int i = lane; i < mm2; i += 32) Gbb.a[i] = cmk((R)sL[i].x, (R)sL[i].y);
     fetch_u(0);
     for (int k = 0; k < K; ++k) {
         if (lane < m) {
@@ -381,30 +492,30 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
         // S = diag(E - U_a) - gamma^2 g_L[b][b]_{k-1} - gamma^2 C D^-1 C^T
         RS_FOR_ENTRIES(m, lane, {
             const int r1 = wrap<m>(r + 1), c1 = wrap<m>(c + 1);
-            cplxd cd = cmk(0.0, 0.0);
+            C cd = cmk(zero, zero);
             if (r == c) cd = cadd(cd, dv[r]);
             if (r == c1) cd = cadd(cd, dv[r]);
             if (r1 == c) cd = cadd(cd, dv[r1]);
             if (r1 == c1) cd = cadd(cd, dv[r1]);
-            cplxd v = cscale(cadd(Gbb.at(r, c), cd), -g2);
+            C v = cscale(cadd(Gbb.at(r, c), cd), -g2);
             if (r == c) v = cadd(v, da[r]);
             X.at(r, c) = v;
         })
         ok = invert<m>(X, X, buf, lane) && ok;
-        cplxd* dst = myX + (size_t)k * mm2;
+        C* dst = myX + (size_t)k * mm2;
         for (int i = lane; i < mm2; i += 32) dst[i] = X.a[i];
         form_gbb();
     }
     // G_K[a][a] of the right lead's first ring: (I - gamma^2 s_R g_L[b][b])^-1 s_R
-    for (int i = lane; i < mm2; i += 32) X.a[i] = sR[i];
+    for (int i = lane; i < mm2; i += 32) X.a[i] = cmk((R)sR[i].x, (R)sR[i].y);
     __syncwarp();
     mm<m, false, false, false>(Gn, X, Gbb, Gn, -g2, lane);
-    if (lane < m) Gn.at(lane, lane) = cadd(Gn.at(lane, lane), cmk(1.0, 0.0));
+    if (lane < m) Gn.at(lane, lane) = cadd(Gn.at(lane, lane), cmk(one, zero));
     ok = invert<m>(Gn, Gn, buf, lane) && ok;
-    mm<m, false, false, false>(Gn, Gn, X, Gn, 1.0, lane);
+    mm<m, false, false, false>(Gn, Gn, X, Gn, one, lane);
     fetch_u(K - 1);
     for (int k = K - 1; k >= 0; --k) {
-        const cplxd* src = myX + (size_t)k * mm2;
+        const C* src = myX + (size_t)k * mm2;
         for (int i = lane; i < mm2; i += 32) X.a[i] = src[i];
         if (lane < m) dv[lane] = crcp(cmk(E.x - ub_n, E.y));
         if (k > 0) fetch_u(k - 1);
@@ -413,7 +524,7 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
         // Z = Y G' Y^T, Y = C D^-1
         RS_FOR_ENTRIES(m, lane, {
             const int r1 = wrap<m>(r + 1), c1 = wrap<m>(c + 1);
-            cplxd v = cmul(cmul(dv[r], dv[c]), Gn.at(r, c));
+            C v = cmul(cmul(dv[r], dv[c]), Gn.at(r, c));
             v = cfma(cmul(dv[r], dv[c1]), Gn.at(r, c1), v);
             v = cfma(cmul(dv[r1], dv[c]), Gn.at(r1, c), v);
             v = cfma(cmul(dv[r1], dv[c1]), Gn.at(r1, c1), v);
@@ -421,17 +532,18 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
         })
         __syncwarp();
         // tr G[b][b] = tr g_L[b][b] + gamma^2 sum_rc (g_L[b][b] G')[r][c] g_L[b][b][c][r]
-        mm<m, false, false, false>(W, Gbb, Gn, W, 1.0, lane);
+        mm<m, false, false, false>(W, Gbb, Gn, W, one, lane);
         cplxd tb = cmk(0.0, 0.0);
         RS_FOR_ENTRIES(m, lane, {
-            tb = cfma(cscale(W.at(r, c), g2), Gbb.at(c, r), tb);
-            if (r == c) tb = cadd(tb, Gbb.at(r, r));
+            const C w = cmul(cscale(W.at(r, c), g2), Gbb.at(c, r));
+            tb = cadd(tb, cmk((double)w.x, (double)w.y));
+            if (r == c) tb = cadd(tb, cmk((double)Gbb.at(r, r).x, (double)Gbb.at(r, r).y));
         })
         // G[a][a] = X + gamma^4 (X Z) X
-        mm<m, false, false, false>(Z, X, Z, Z, 1.0, lane);
+        mm<m, false, false, false>(Z, X, Z, Z, one, lane);
         mm<m, false, false, true>(Gn, Z, X, X, g4, lane);
         cplxd ta = cmk(0.0, 0.0);
-        if (lane < m) ta = Gn.at(lane, lane);
+        if (lane < m) ta = cmk((double)Gn.at(lane, lane).x, (double)Gn.at(lane, lane).y);
         ta = warp_sum(ta);
         tb = warp_sum(tb);
         if (lane == 0) {
@@ -439,6 +551,41 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
             row[2 * k + 1] = fma(cc.x, tb.y, cc.y * tb.x);  // Im(c tr G[b][b])
         }
     }
+    return ok;
+}
+
+// Chain kernel: warp e -> energy e in the precision and with the potentials
+// its flags give (Uatoms, or Uzero for the U = 0 pass).
+// gX: [num_e][K][m*m] FP64-complex slots (an FP32 chain uses the first half
+// of its slot); rows: [num_e][N].
+template <int m>
+__global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, const double* __restrict__ Ere,
+                                                          const double* __restrict__ Eim,
+                                                          const double* __restrict__ cre,
+                                                          const double* __restrict__ cim, int num_e,
+                                                          const int* __restrict__ flags,
+                                                          const double* __restrict__ Uatoms,
+                                                          const double* __restrict__ Uzero,
+                                                          const cplxd* __restrict__ corners, cplxd* __restrict__ gX,
+                                                          double* __restrict__ rows, int* __restrict__ status) {
+    extern __shared__ cplxd sh[];
+    const int lane = threadIdx.x;
+    const int e = blockIdx.x;
+    if (e >= num_e) return;
+    constexpr int mm2 = m * m;
+    const int fl = flags[e];
+    const double* __restrict__ Ua = (fl & kRsZeroU) ? Uzero : Uatoms;
+    const cplxd* sL = corners + (size_t)e * 2 * mm2;
+    const cplxd* sR = sL + mm2;
+    cplxd* myX = gX + (size_t)e * K * mm2;
+    double* row = rows + (size_t)e * 2 * K;
+    const cplxd cc = cmk(cre[e], cim[e]);
+    bool ok;
+    if (!(fl & kRsFP32))
+        ok = rs_chain<m, double>(K, gamma, cmk(Ere[e], Eim[e]), cc, Ua, sL, sR, myX, row, sh, lane);
+    else
+        ok = rs_chain<m, float>(K, (float)gamma, cmk((float)Ere[e], (float)Eim[e]), cc, Ua, sL, sR,
+                                reinterpret_cast<cplxf*>(myX), row, reinterpret_cast<cplxf*>(sh), lane);
     if (!ok && lane == 0) atomicExch(status, 1);
 }
 
@@ -478,7 +625,8 @@ int rs_max_atoms_per_block() { return 2 * kMaxM; }
 namespace {
 template <int m>
 cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_Eim, const double* d_cre,
-                      const double* d_cim, int num_e, int num_u, const double* d_Uatoms, const double* d_Uzero,
+                      const double* d_cim, int num_e, const int* d_flags, const double* d_Uatoms,
+                      const double* d_Uzero,
                       double Uc0, double Uc1, int lead_iters, void* d_corners, void* d_gL, double* d_rows, double* d_Q,
                       int* d_status, cudaStream_t stream) {
     cudaError_t e = cudaFuncSetAttribute(rs_lead_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -488,11 +636,12 @@ cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_
                              (int)rs_chain_smem_bytes(m));
     if (e != cudaSuccess) return e;
     rs_lead_kernel<m><<<2 * num_e, 32, rs_lead_smem_bytes(m), stream>>>(
-        gamma, d_Ere, d_Eim, num_e, num_u, Uc0, Uc1, lead_iters, static_cast<cplxd*>(d_corners), d_status);
+        gamma, d_Ere, d_Eim, num_e, d_flags, Uc0, Uc1, lead_iters, static_cast<cplxd*>(d_corners), d_status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     rs_chain_kernel<m><<<num_e, 32, rs_chain_smem_bytes(m), stream>>>(
-        K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, num_u, d_Uatoms, d_Uzero, static_cast<const cplxd*>(d_corners),
+        K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_flags, d_Uatoms, d_Uzero,
+        static_cast<const cplxd*>(d_corners),
         static_cast<cplxd*>(d_gL), d_rows, d_status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -503,14 +652,15 @@ cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_
 }  // namespace
 
 cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
-                             const double* d_cre, const double* d_cim, int num_e, int num_u, const double* d_Uatoms,
+                             const double* d_cre, const double* d_cim, int num_e, const int* d_flags,
+                             const double* d_Uatoms,
                              const double* d_Uzero, double Uc0, double Uc1, int lead_iters, void* d_corners,
                              void* d_gL, double* d_rows, double* d_Q, int* d_status, cudaStream_t stream) {
     if (num_e <= 0) return cudaSuccess;
     if (K < 1) return cudaErrorInvalidValue;
 #define RS_CASE(M)                                                                                                 \
     case M:                                                                                                        \
-        return launch_rs<M>(K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, num_u, d_Uatoms, d_Uzero, Uc0, Uc1,        \
+        return launch_rs<M>(K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_flags, d_Uatoms, d_Uzero, Uc0, Uc1,      \
                             lead_iters, d_corners, d_gL, d_rows, d_Q, d_status, stream);
     switch (m) {
         RS_CASE(1) RS_CASE(2) RS_CASE(3) RS_CASE(4) RS_CASE(5) RS_CASE(6) RS_CASE(7) RS_CASE(8)

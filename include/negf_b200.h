@@ -211,7 +211,11 @@ int negf_set_timing(int enable);
  * contour and pole points with the mode-space coefficients, minus Rho0 at
  * U = 0.  d_Uatoms (device, [N][m]) gives per-atom potentials; null uses the
  * tube's ring potential on every atom, in which case the result equals the
- * mode-space charge with all m//2 + 1 distinct modes.  Synchronous. */
+ * mode-space charge with all m//2 + 1 distinct modes.  Tubes in mixed
+ * precision run the contour and pole chains at least mixed_fp64_band above
+ * the real axis in FP32 (m x m products on the tensor cores in TF32 with a
+ * high/remainder split, the complex product in three real products); the
+ * leads, the Rho0 pass and the energy sum stay FP64.  Synchronous. */
 int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, void* stream);
 
 /* Surrogate-model kernels (no counterpart in the reference): the training

@@ -26,6 +26,34 @@ def test_realspace_against_block_oracle(oracle, m, cells):
     assert _rel(Qg, Qo) <= TOL, _rel(Qg, Qo)
 
 
+MIXED_TOL = 1e-5
+
+
+@pytest.mark.parametrize("m,cells", [(13, 6), (8, 4)])
+def test_realspace_mixed_against_block_oracle(oracle, m, cells):
+    """Mixed mode: contour and pole chains at least mixed_fp64_band above the
+    real axis in FP32 with tensor-core products, the rest in FP64."""
+    g, o = _pair(oracle, seed=33, **_eq_kw(m, cells, num_modes=1, precision="mixed"))
+    E = np.concatenate([g.energy_points(1)[0], g.energy_points(2)[0]])
+    assert np.sum(np.abs(E.imag) >= 1e-3) > 0.5 * len(E)  # most chains take the FP32 path
+    Qg = g.realspace_charge()
+    Qo = o.rs_charge(nthreads=8)
+    assert _rel(Qg, Qo) <= MIXED_TOL, _rel(Qg, Qo)
+
+
+def test_realspace_mixed_long_tube_against_fp64():
+    """300 blocks: the FP32 recursion stays within the mixed tolerance of the FP64 pass."""
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import site_potential
+    kw = _eq_kw(13, 150, eq_integration_pts=(64, 64, 96))
+    g64, g32 = CNT(**kw), CNT(**kw, precision="mixed")
+    U = site_potential(g64.site_positions(), 20261203 + 3)
+    for g in (g64, g32):
+        g.set_potential(U, (U[0], U[-1]))
+    Q64, Q32 = g64.realspace_charge(), g32.realspace_charge()
+    assert _rel(Q32, Q64) <= MIXED_TOL, _rel(Q32, Q64)
+
+
 def test_realspace_per_atom_potential(oracle):
     import torch
     g, o = _pair(oracle, seed=32, **_eq_kw(13, 3))
