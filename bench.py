@@ -281,14 +281,16 @@ def config4_measure(torch, passes=5):
     return out
 
 
-def config3_measure(torch, passes=2):
+def config3_measure(torch, passes=2, small=False):
     """Real-space ring blocks: (13,0), 600 blocks of 26 atoms, 2048 contour
-    energies + poles, FP64; against the mode-space pass of the same tube with
-    all 7 modes (equal for this ring-uniform potential)."""
+    energies + poles, FP64 and mixed; against the mode-space pass of the same
+    tube with all 7 modes (equal for this ring-uniform potential).  small:
+    the profiling case, 200 blocks and 256 contour energies."""
     from electrostatic_b200.negf import CNT, last_stats, set_timing
     from electrostatic_b200.workloads import SEED_BASE, site_potential
-    kw = dict(type_id=(13, 0), num_unitcells=300, num_modes=7, contact_mu=(-0.8, -0.8), contact_T=(300.0, 300.0),
-              eq_integration_pts=(512, 512, 1024), E_pole_max=3.0, E_zPlus_imag=1e-6)
+    kw = dict(type_id=(13, 0), num_unitcells=100 if small else 300, num_modes=7, contact_mu=(-0.8, -0.8),
+              contact_T=(300.0, 300.0), eq_integration_pts=(64, 64, 128) if small else (512, 512, 1024),
+              E_pole_max=3.0, E_zPlus_imag=1e-6)
     t = CNT(**kw)
     U = site_potential(t.site_positions(), SEED_BASE + 3)
     t.set_potential(U, (U[0], U[-1]))
@@ -322,8 +324,9 @@ def config3_measure(torch, passes=2):
     # convergence, data-dependent) is not counted
     flops = (E + E0) * K * 32 * m ** 3
     Qr = Q.cpu().numpy()
-    return {"workload": "(13,0) CNT, 600 blocks of 2 rings (26 atoms), %d contour+pole energies (+%d Rho0), "
-                        "Sancho-Rubio leads (at most 32 iterations), FP64, seeded config-2 ring potential" % (E, E0),
+    return {"workload": "(13,0) CNT, %d blocks of 2 rings (26 atoms), %d contour+pole energies (+%d Rho0), "
+                        "Sancho-Rubio leads (at most 32 iterations), FP64, seeded config-2 ring potential"
+                        % (K, E, E0),
             "seconds_per_pass": sec, "block_updates_per_s": (E + E0) * K / sec,
             "achieved_tflops": flops / sec / 1e12, "flops_per_pass": flops,
             "flop_convention": "ring corners m=13: inverse 8m^3 + three complex products 8m^3 per block update "
@@ -435,7 +438,8 @@ def main():
     ap.add_argument("--no-long-tube", action="store_true")
     ap.add_argument("--config5", action="store_true", help="surrogate study (about two minutes, off by default)")
     ap.add_argument("--small", action="store_true",
-                    help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis)")
+                    help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis); "
+                         "real-space case of 200 blocks and 256 contour energies")
     args = ap.parse_args()
     if args.small:
         global EQ_PTS, RT_PTS, WORKLOAD
@@ -569,7 +573,7 @@ def main():
                              f"{threads} threads over energies; {dt:.2f} s"}
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
-        cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch)
+        cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch, small=args.small)
         longt = None if (args.no_long_tube or world > 1) else long_tube_measure(torch)
         cfg5 = config5_measure(torch) if (args.config5 and world == 1) else None
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
