@@ -8,7 +8,9 @@ reference has no counterpart (its loop starts from a constant charge,
 Broyden_Parallel_General.cpp:68-248).
 
 Architecture (channel-last activations, rows = samples x sites):
-  lift      h0 = x W_lift + b_lift,  x = (U, Vg, Vds, site / S)       4 -> 128
+  lift      h0 = x W_lift + b_lift,                                  24 -> 128
+            x = (U at the 17 sites n-8 .. n+8 (0 beyond the ends), Vg, Vds,
+                 n / S, ring parity +-1, exp(-n / 40), exp(-(S-1-n) / 40), 0)
   6 layers  h  = GELU(h W_l + G (R_l * (F h)) + b_l)                 128 -> 128
             F: real DFT basis of the first 32 frequencies (cos, sin: 64 rows),
             G: its synthesis basis, R_l: per-frequency 256 x 256 mixing of the
@@ -30,7 +32,8 @@ import numpy as np
 from . import _lib
 from ._lib import check
 
-WIDTH, MODES, LAYERS, FEAT = 128, 32, 6, 4
+WIDTH, MODES, LAYERS, FEAT = 128, 32, 6, 24
+WIN = 8  # half-width of the potential window of each site
 
 
 def _p(t):
@@ -81,6 +84,19 @@ class FourierOperator:
         self.x_scale = torch.ones(FEAT, device=device)
         self.q_scale = 1.0
         self._bufs = {}
+        # window gather: site n reads U[n + d], d = -WIN..WIN, masked to 0 beyond the ends
+        nw = 2 * WIN + 1
+        j = np.arange(self.S)[:, None] + np.arange(-WIN, WIN + 1)[None, :]
+        self._widx = torch.tensor(np.clip(j, 0, self.S - 1).reshape(-1), dtype=torch.long, device=device)
+        self._wmask = torch.tensor(((j >= 0) & (j < self.S)).astype(np.float32), device=device)
+        # fixed site features: n / S, parity, contact proximity
+        n = np.arange(self.S)
+        fixed = np.zeros((self.S, FEAT - nw - 2), dtype=np.float32)
+        fixed[:, 0] = n / self.S
+        fixed[:, 1] = np.where(n % 2 == 0, 1.0, -1.0)
+        fixed[:, 2] = np.exp(-n / 40.0)
+        fixed[:, 3] = np.exp(-(self.S - 1 - n) / 40.0)
+        self._fixed = torch.tensor(fixed, device=device)
 
     # ------------------------------------------------------------------ helpers
     def _buf(self, name, shape, dtype=None):
@@ -103,15 +119,17 @@ class FourierOperator:
 
     # ------------------------------------------------------------------ model
     def features(self, U, Vg, Vds):
-        """x[b][s] = (U, Vg, Vds, s / S) scaled by the stored input scales."""
+        """x[b][s] (see the module docstring), potentials divided by the stored
+        potential scale, as BF16 rows [B*S][FEAT]."""
         t = self.torch
         B = U.shape[0]
+        nw = 2 * WIN + 1
         x = t.empty(B, self.S, FEAT, device=self.dev)
-        x[:, :, 0] = U
-        x[:, :, 1] = Vg[:, None]
-        x[:, :, 2] = Vds[:, None]
-        x[:, :, 3] = t.arange(self.S, device=self.dev)[None, :] / self.S
-        return (x / self.x_scale).to(t.bfloat16).reshape(B * self.S, FEAT)
+        x[:, :, :nw] = U.float()[:, self._widx].reshape(B, self.S, nw) * (self._wmask / self.x_scale[0])
+        x[:, :, nw] = Vg[:, None]
+        x[:, :, nw + 1] = Vds[:, None]
+        x[:, :, nw + 2:] = self._fixed
+        return x.to(t.bfloat16).reshape(B * self.S, FEAT)
 
     def forward(self, xb, B, keep=False):
         """xb: BF16 [B*S][4]; returns q [B*S] (FP32, in units of q_scale)."""
@@ -216,7 +234,8 @@ class FourierOperator:
         """Train on device tensors U [n][S], Vg [n], Vds [n], Q [n][S] (float32)."""
         t = self.torch
         n = U.shape[0]
-        self.x_scale = t.tensor([float(U.abs().max()), 1.0, 1.0, 1.0], device=self.dev)
+        self.x_scale = t.ones(FEAT, device=self.dev)
+        self.x_scale[0] = float(U.abs().max())
         self.q_scale = float(Q.abs().max())
         y_all = (Q / self.q_scale).float()
         g = t.Generator(device="cpu").manual_seed(1)
@@ -247,25 +266,30 @@ class FourierOperator:
         CUDA graph after one call of infer()): U_view (float64 device view of a
         potential buffer), scalar biases, Q_out (float64 device, S)."""
         t = self.torch
-        self._bind = dict(U=U_view, Q=Q_out, x=t.empty(1, self.S, FEAT, device=self.dev),
-                          xb=t.empty(self.S, FEAT, dtype=t.bfloat16, device=self.dev))
+        nw = 2 * WIN + 1
+        self._bind = dict(U=U_view, Q=Q_out, x=t.empty(self.S, FEAT, device=self.dev),
+                          xb=t.empty(self.S, FEAT, dtype=t.bfloat16, device=self.dev),
+                          win=t.empty(self.S * nw, dtype=t.float64, device=self.dev),
+                          wscale=self._wmask / self.x_scale[0])
         x = self._bind["x"]
-        x[:, :, 1] = float(Vg)
-        x[:, :, 2] = float(Vds)
-        x[:, :, 3] = t.arange(self.S, device=self.dev)[None, :] / self.S
-        x.div_(self.x_scale)
+        x[:, nw + 2:] = self._fixed
+        self.set_bias(Vg, Vds)
 
     def set_bias(self, Vg, Vds):
+        nw = 2 * WIN + 1
         x = self._bind["x"]
-        x[:, :, 1] = float(Vg) / float(self.x_scale[1])
-        x[:, :, 2] = float(Vds) / float(self.x_scale[2])
+        x[:, nw] = float(Vg) / float(self.x_scale[nw])
+        x[:, nw + 1] = float(Vds) / float(self.x_scale[nw + 1])
 
     def infer(self):
         """Q_out = model(U_view) with the bound buffers (no allocation after the first call)."""
+        t = self.torch
         b = self._bind
-        b["x"][0, :, 0].copy_(b["U"])
-        b["x"][0, :, 0].div_(self.x_scale[0])
-        b["xb"].copy_(b["x"][0])
+        nw = 2 * WIN + 1
+        t.index_select(b["U"], 0, self._widx, out=b["win"])
+        b["x"][:, :nw].copy_(b["win"].view(self.S, nw))
+        b["x"][:, :nw].mul_(b["wscale"])
+        b["xb"].copy_(b["x"])
         q = self.forward(b["xb"], 1)
         b["Q"].copy_(q)
         b["Q"].mul_(self.q_scale)
