@@ -546,6 +546,32 @@ def main():
     e2e_value = updates * world * args.steps / (float(e2e_all.item()) * 1e-3)
     assert np.all(np.isfinite(Qh))
 
+    # ---- the same workload in the mixed path (FP32 contour recursions, FP64 elsewhere)
+    mixed = None
+    if args.precision == "fp64" and world == 1:
+        tm = CNT(**tube_kwargs("mixed"))
+        tm.set_potential(U, Uc)
+        Qm = torch.zeros_like(Q)
+        for _ in range(3):
+            compute_charge([tm], out=Qm, stream=stream)
+        nm = min(args.steps, 50)
+        mev = []
+        for i in range(nm):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.zero_()
+            a.record(stream)
+            compute_charge([tm], out=Qm, stream=stream)
+            b.record(stream)
+            mev.append((a, b))
+        torch.cuda.synchronize()
+        sm = last_stats()
+        mms = float(np.mean([a.elapsed_time(b) for a, b in mev]))
+        mixed = {"ms_per_pass": mms, "updates_per_s": sm["updates"] / (mms * 1e-3),
+                 "updates_fp32": sm["updates_fp32"], "updates": sm["updates"],
+                 "rule": "contour chains at least 1e-3 eV above the real axis in FP32 (Kahan FP64 sums); "
+                         "real-axis chains, leads and Rho0 in FP64",
+                 "max_rel_vs_fp64": float((Qm - Q).abs().max() / Q.abs().max())}
+
     # ---- roofline of the dominant kernel (the RGF sweep kernel)
     flops = st["contour_updates"] * FLOP_CONTOUR + st["realaxis_updates"] * FLOP_REALAXIS
     k_ms = float(np.mean(rgf_ms))
@@ -597,7 +623,8 @@ def main():
                 "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
                            "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "config3": cfg3, "config4": cfg4, "long_tube": longt, "config5": cfg5,
+                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "mixed": mixed, "config3": cfg3, "config4": cfg4,
+                "long_tube": longt, "config5": cfg5,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
                         "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},
