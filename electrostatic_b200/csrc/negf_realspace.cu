@@ -44,7 +44,8 @@
 //   rs_reduce_kernel sum over energies per ring in a fixed order (Kahan).
 // The energies of the U = 0 pass (Rho0) run in the same launches with
 // negated coefficients, so one reduction gives the induced charge.
-// Inversions: Gauss-Jordan with partial pivoting on [S | I] (lane = column).
+// Inversions: Gauss-Jordan on [S | I] (lane = column), on the diagonal
+// pivots with a fall-back to partial pivoting when a pivot is small.
 //
 // Mixed precision: the chain of an energy runs in FP32 when its tube is in
 // mixed mode and the point lies at least mixed_fp64_band above the real axis
@@ -268,14 +269,19 @@ __device__ __forceinline__ void mm(Mat<m, float> C, Mat<m, float> A, Mat<m, floa
     __syncwarp();
 }
 
+// max(|Re|, |Im|)
+template <typename R>
+__device__ __forceinline__ R cmaxabs(cplx<R> a) {
+    return fmax(fabs(a.x), fabs(a.y));
+}
+
 // out = S^-1 by Gauss-Jordan with partial pivoting (largest |.|^2 over the
 // rows below, lowest row on ties).  Lane c < 2m holds column c of [S | I] in
 // registers; the pivot column reaches every lane through buf (m complex in
-// shared memory), every lane finds the pivot row by a tournament over it,
-// and rows are swapped (a warp-uniform branch) only when the pivot is off
-// the diagonal.  out may alias S.  Returns false on a zero pivot.
+// shared memory), every lane finds the pivot row by a tournament over it.
+// out may alias S.  Returns false on a zero pivot.
 template <int m, typename R>
-__device__ __forceinline__ bool invert(Mat<m, R> out, Mat<m, R> S, cplx<R>* buf, int lane) {
+__device__ __noinline__ bool invert_pivoted(Mat<m, R> out, Mat<m, R> S, cplx<R>* buf, int lane) {
     constexpr int n2 = 2 * m;
     __syncwarp();  // S complete
     cplx<R> col[m];
@@ -339,6 +345,59 @@ __device__ __forceinline__ bool invert(Mat<m, R> out, Mat<m, R> S, cplx<R>* buf,
     }
     __syncwarp();
     return ok;
+}
+
+// out = S^-1 by Gauss-Jordan on the diagonal pivots, falling back to partial
+// pivoting (invert_pivoted, from S, which stays untouched until the result
+// is written) when any pivot is small: max(|Re|, |Im|) of a pivot below tau
+// (1e-3 in FP64, 1e-2 in FP32) times the largest such value of the entries
+// of S.  For E - H - Sigma with Im E > 0, S is complex symmetric with a
+// positive definite imaginary part, so its leading minors never vanish and
+// the diagonal pivots are the usual case; the search and the row swaps of
+// partial pivoting (about half the cost of the inversion) leave the common
+// path.  Lane c < 2m holds column c of [S | I] in registers, the pivot
+// column reaches every lane through buf.  out may alias S.  Returns false on
+// a zero pivot.
+template <int m, typename R>
+__device__ __forceinline__ bool invert(Mat<m, R> out, Mat<m, R> S, cplx<R>* buf, int lane) {
+    constexpr int n2 = 2 * m;
+    const R tau = sizeof(R) == 8 ? R(1e-3) : R(1e-2);
+    __syncwarp();  // S complete
+    cplx<R> col[m];
+    R smax = R(0), pmin;
+#pragma unroll
+    for (int r = 0; r < m; ++r) {
+        col[r] = lane < m ? S.at(r, lane) : cmk<R>(lane - m == r ? R(1) : R(0), R(0));
+        if (lane < m) smax = fmax(smax, cmaxabs(col[r]));
+    }
+#pragma unroll
+    for (int p = 0; p < m; ++p) {
+        __syncwarp();  // every lane is done with buf
+        if (lane == p) {
+#pragma unroll
+            for (int r = 0; r < m; ++r) buf[r] = col[r];
+        }
+        __syncwarp();
+        const cplx<R> piv = buf[p];
+        pmin = p == 0 ? cmaxabs(piv) : fmin(pmin, cmaxabs(piv));
+        const cplx<R> rp = cmul(col[p], crcp(piv));
+#pragma unroll
+        for (int r = 0; r < m; ++r) {
+            if (r == 8) asm volatile("" ::: "memory");  // two batches of multiplier loads
+            if (r != p) col[r] = cfms(buf[r], rp, col[r]);
+        }
+        col[p] = rp;
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+    if (!(pmin >= tau * smax)) return invert_pivoted<m, R>(out, S, buf, lane);
+    __syncwarp();
+    if (lane >= m && lane < n2) {
+#pragma unroll
+        for (int r = 0; r < m; ++r) out.at(r, lane - m) = col[r];
+    }
+    __syncwarp();
+    return true;
 }
 
 __device__ __forceinline__ double warp_max(double v) {
