@@ -1536,14 +1536,29 @@ int negf_broyden_input_device_ptr(negf_broyden* b, double** p) {
 }
 
 int negf_device_selftest(int which, int n, const double* in, double* out) {
-    if (!in || !out || n <= 0 || which < 0 || which > 1) return fail(NEGF_ERR_ARG, "bad self-test arguments");
+    if (!in || !out || n <= 0 || which < 0 || which > 5) return fail(NEGF_ERR_ARG, "bad self-test arguments");
     int rc = require_device();
     if (rc) return rc;
     DevBuf a, b;
     NEGF_CUDA(a.reserve(sizeof(double) * n));
     NEGF_CUDA(b.reserve(sizeof(double) * n));
     NEGF_CUDA(cudaMemcpy(a.p, in, sizeof(double) * n, cudaMemcpyHostToDevice));
-    NEGF_CUDA(negf::selftest(which, n, a.as<double>(), b.as<double>(), 0));
+    if (which <= 1) {
+        NEGF_CUDA(negf::selftest(which, n, a.as<double>(), b.as<double>(), 0));
+    } else {
+        // in = [m, count, matrices...]; out = [m, count, results...]
+        const int m = (int)in[0], count = (int)in[1];
+        const long long per = (long long)(which >= 4 ? 4 : 2) * m * m;
+        if (m != 4 && m != 13 && m != 16) return fail(NEGF_ERR_ARG, "self-test tiles: m must be 4, 13 or 16");
+        if (count < 1 || 2 + per * count > n || 2 + 2LL * m * m * count > n)
+            return fail(NEGF_ERR_ARG, "self-test tiles: n too small for count matrices");
+        NEGF_CUDA(cudaMemset(b.p, 0, sizeof(double) * n));
+        NEGF_CUDA(negf::rs_selftest(which, m, count, a.as<double>() + 2, b.as<double>() + 2, 0));
+        NEGF_CUDA(cudaMemcpy(out, b.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        out[0] = m;
+        out[1] = count;
+        return NEGF_OK;
+    }
     NEGF_CUDA(cudaMemcpy(out, b.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
     return NEGF_OK;
 }

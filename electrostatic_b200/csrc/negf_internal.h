@@ -93,6 +93,11 @@ cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, co
                              void* d_corners, void* d_gL, double* d_rows, double* d_Q, int* d_status,
                              cudaStream_t stream);
 cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_t stream);
+// Self-test of the real-space tile primitives for m in {4, 13, 16}: which 2 / 3
+// inverts count m x m complex matrices in FP64 / FP32, which 4 / 5 forms
+// count products A B (FP64 CUDA cores / FP32 tensor cores); complex values
+// re/im interleaved, row-major.
+cudaError_t rs_selftest(int which, int m, int count, const double* d_in, double* d_out, cudaStream_t stream);
 int rs_max_atoms_per_block();
 
 // Surrogate-model kernels (negf_surrogate.cu).  BF16 operands as void*.

@@ -648,6 +648,36 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
     if (!ok && lane == 0) atomicExch(status, 1);
 }
 
+// Self-test of the tile primitives: warp w takes matrix w (inversion) or the
+// pair (A, B) w (product) from in (complex, re/im interleaved, row-major
+// m x m, FP64), computes in precision R and writes the m x m result to out.
+template <int m, typename R>
+__global__ void __launch_bounds__(32) rs_selftest_kernel(int product, int count, const double* __restrict__ in,
+                                                         double* __restrict__ out) {
+    __shared__ cplx<R> sh[3 * m * m + kMaxM];
+    const int lane = threadIdx.x, w = blockIdx.x;
+    if (w >= count) return;
+    constexpr int mm2 = m * m;
+    const Mat<m, R> A{sh}, B{sh + mm2}, C{sh + 2 * mm2};
+    cplx<R>* buf = sh + 3 * mm2;
+    const double* src = in + (size_t)w * (product ? 2 : 1) * 2 * mm2;
+    for (int i = lane; i < mm2; i += 32) {
+        A.a[i] = cmk((R)src[2 * i], (R)src[2 * i + 1]);
+        if (product) B.a[i] = cmk((R)src[2 * mm2 + 2 * i], (R)src[2 * mm2 + 2 * i + 1]);
+    }
+    __syncwarp();
+    bool ok = true;
+    if (product)
+        mm<m, false, false, false>(C, A, B, C, R(1), lane);
+    else
+        ok = invert<m>(C, A, buf, lane);
+    double* dst = out + (size_t)w * 2 * mm2;
+    for (int i = lane; i < mm2; i += 32) {
+        dst[2 * i] = ok ? (double)C.a[i].x : NAN;
+        dst[2 * i + 1] = ok ? (double)C.a[i].y : NAN;
+    }
+}
+
 // Q[r] = sum over energies of rows[e][r], Kahan, energies in order.
 __global__ void rs_reduce_kernel(const double* __restrict__ rows, int num_e, int N, double* __restrict__ Q) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -680,6 +710,26 @@ cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_
 }
 
 int rs_max_atoms_per_block() { return 2 * kMaxM; }
+
+cudaError_t rs_selftest(int which, int m, int count, const double* d_in, double* d_out, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    const int product = which >= 4;
+    const bool fp32 = which == 3 || which == 5;
+#define RS_ST(M)                                                                                                   \
+    case M:                                                                                                        \
+        if (fp32)                                                                                                  \
+            rs_selftest_kernel<M, float><<<count, 32, 0, stream>>>(product, count, d_in, d_out);                   \
+        else                                                                                                       \
+            rs_selftest_kernel<M, double><<<count, 32, 0, stream>>>(product, count, d_in, d_out);                  \
+        break;
+    switch (m) {
+        RS_ST(4) RS_ST(13) RS_ST(16)
+        default:
+            return cudaErrorInvalidValue;
+    }
+#undef RS_ST
+    return cudaGetLastError();
+}
 
 namespace {
 template <int m>

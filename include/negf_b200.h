@@ -371,8 +371,12 @@ int negf_broyden_step_device_switch(negf_broyden* b, const double* d_n_out, doub
 int negf_broyden_input_device_ptr(negf_broyden* b, double** d_n_in);
 
 /* Device self-test of the kernels' numeric primitives (no counterpart in the
- * reference): which = 0 FP64 reciprocal, 1 FP32 reciprocal; n host values in,
- * n host values out. */
+ * reference): which = 0 FP64 reciprocal, 1 FP32 reciprocal (n values in, n
+ * out); real-space tile primitives on count m x m complex matrices (m = 4,
+ * 13 or 16; in = [m, count, data], out = [m, count, results], complex values
+ * re/im interleaved, row-major): 2 / 3 inverse in FP64 / FP32 (data: count
+ * matrices; a NaN result marks a zero pivot), 4 / 5 product A B on the FP64
+ * cores / FP32 tensor cores (data: count pairs A, B). */
 int negf_device_selftest(int which, int n, const double* in, double* out);
 
 /* Affine electrostatics stand-in used by the SCF harness:

@@ -90,3 +90,48 @@ def test_realspace_rejections():
     b = CNT(type_id=(13, 0), num_unitcells=2, num_modes=2, contact_mu=(0.0, -0.3))
     with pytest.raises(NEGFError, match="equilibrium"):
         b.realspace_charge()
+
+
+def _tiles(negf_lib, which, m, data, count, out_per):
+    import ctypes as C
+    buf = np.concatenate([[m, count], data.ravel()])
+    out = np.zeros(max(len(buf), 2 + out_per * count))
+    dp = C.POINTER(C.c_double)
+    inp = np.zeros_like(out)
+    inp[: len(buf)] = buf
+    assert negf_lib.negf_device_selftest(which, len(out), inp.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
+    r = out[2: 2 + out_per * count].reshape(count, m, m, 2)
+    return r[..., 0] + 1j * r[..., 1]
+
+
+def _cplx_pack(M):
+    return np.stack([M.real, M.imag], axis=-1)
+
+
+@pytest.mark.parametrize("m", [4, 13, 16])
+def test_tile_inversion_and_products(negf_lib, m):
+    """The chain kernels' m x m primitives: inversion on the diagonal pivots
+    with the partial-pivoting fall-back (FP64 and FP32), products on the FP64
+    cores and on the TF32 tensor cores (three-multiply complex form with
+    high/remainder operand splits), against numpy."""
+    rng = np.random.default_rng(m)
+    n = 24
+    # like E - H - Sigma: complex symmetric, positive definite imaginary part
+    A = rng.standard_normal((n, m, m)) + 1j * rng.standard_normal((n, m, m))
+    A = 0.3 * (A + np.transpose(A, (0, 2, 1)))
+    A += np.eye(m)[None] * (2.0 + 0.5j)
+    # matrices whose diagonal pivots are small: the fall-back must pivot
+    Bp = rng.standard_normal((8, m, m)) + 0.1j * rng.standard_normal((8, m, m))
+    Bp[:, np.arange(m), np.arange(m)] = 1e-5 * (1 + 1j)
+    for which, tol in ((2, 1e-12), (3, 2e-4)):
+        for M in (A, Bp):
+            X = _tiles(negf_lib, which, m, _cplx_pack(M), len(M), 2 * m * m)
+            res = np.abs(M @ X - np.eye(m)[None]).max()
+            cond = max(np.linalg.cond(Mi) for Mi in M)
+            assert res <= tol * max(1.0, cond / 100), (which, res, cond)
+    P = rng.standard_normal((n, 2, m, m)) + 1j * rng.standard_normal((n, 2, m, m))
+    ref = P[:, 0] @ P[:, 1]
+    for which, tol in ((4, 1e-13), (5, 2e-6)):
+        Cg = _tiles(negf_lib, which, m, np.stack([_cplx_pack(P[:, 0]), _cplx_pack(P[:, 1])], axis=1), n, 2 * m * m)
+        err = np.abs(Cg - ref).max() / np.abs(ref).max()
+        assert err <= tol, (which, err)
