@@ -1427,6 +1427,7 @@ int negf_broyden_create(int S, int max_step, double fraction, int norm_type, neg
     d.norm_type = norm_type;
     d.fraction = fraction;
     d.scalar = 1.0;
+    d.base = 0;
     d.nblocks = std::min(1024, (S + 255) / 256);
     double** vec[] = {&d.n_in, &d.n_prev, &d.F, &d.dF, &d.norm, &d.sum};
     for (double** p : vec) {
@@ -1442,9 +1443,9 @@ int negf_broyden_create(int S, int max_step, double fraction, int norm_type, neg
     NEGF_CUDA(cudaMalloc(&d.scal, sizeof(double) * 4));
     NEGF_CUDA(cudaMemset(d.scal, 0, sizeof(double) * 4));
     NEGF_CUDA(cudaMalloc(&d.part, sizeof(double) * 3 * d.nblocks));
-    NEGF_CUDA(cudaMalloc(&d.step_dev, sizeof(int)));
-    const int one = 1;
-    NEGF_CUDA(cudaMemcpy(d.step_dev, &one, sizeof(int), cudaMemcpyHostToDevice));
+    NEGF_CUDA(cudaMalloc(&d.step_dev, 2 * sizeof(int)));
+    const int init[2] = {1, 0};
+    NEGF_CUDA(cudaMemcpy(d.step_dev, init, 2 * sizeof(int), cudaMemcpyHostToDevice));
     *out = b.release();
     return NEGF_OK;
 }
@@ -1467,7 +1468,7 @@ int negf_broyden_step(negf_broyden* b, const double* d_n_out, double* d_n_in_out
     if (!b || !d_n_out) return fail(NEGF_ERR_ARG, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
     if (status) *status = 0;
-    if (b->step > b->dev.max_step) {  // Transport.cpp:389-393
+    if (b->step + b->dev.base > b->dev.max_step) {  // Transport.cpp:389-393 (seeded rows take capacity)
         if (status) *status = 1;
         return fail(NEGF_ERR_STATE, "Broyden_Step has exceeded the Broyden_Threshold_MaxStep");
     }
@@ -1497,8 +1498,30 @@ int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void
     NEGF_CUDA(cudaMemsetAsync(d.V, 0, sizeof(double) * (size_t)d.S * d.max_step, s));
     NEGF_CUDA(cudaMemsetAsync(d.W, 0, sizeof(double) * (size_t)d.S * d.max_step, s));
     NEGF_CUDA(cudaMemsetAsync(d.c, 0, sizeof(double) * d.max_step, s));
+    d.base = 0;
     b->step = 1;
     NEGF_CUDA(negf::set_int(d.step_dev, 1, s));
+    NEGF_CUDA(negf::set_int(d.step_dev + 1, 0, s));
+    return NEGF_OK;
+}
+
+int negf_broyden_set_initial_jacobian(negf_broyden* b, const double* d_V, const double* d_W, int k, void* stream) {
+    if (!b || k < 0 || (k > 0 && (!d_V || !d_W))) return fail(NEGF_ERR_ARG, "bad initial-Jacobian arguments");
+    negf::BroydenDev& d = b->dev;
+    if (k > d.max_step / 2) return fail(NEGF_ERR_ARG, "at most max_step / 2 seeded rows");
+    cudaStream_t s = (cudaStream_t)stream;
+    int step = 0;
+    NEGF_CUDA(cudaMemcpyAsync(&step, d.step_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+    NEGF_CUDA(cudaStreamSynchronize(s));
+    if (step != 1 || b->step != 1)
+        return fail(NEGF_ERR_STATE, "the initial inverse Jacobian is set before the first step (after create or reset)");
+    const size_t bytes = sizeof(double) * (size_t)d.S * k;
+    if (k > 0) {
+        NEGF_CUDA(cudaMemcpyAsync(d.V + d.S, d_V, bytes, cudaMemcpyDeviceToDevice, s));
+        NEGF_CUDA(cudaMemcpyAsync(d.W + d.S, d_W, bytes, cudaMemcpyDeviceToDevice, s));
+    }
+    d.base = k;
+    NEGF_CUDA(negf::set_int(d.step_dev + 1, k, s));
     return NEGF_OK;
 }
 

@@ -26,6 +26,8 @@ __device__ __forceinline__ bool skipped(const int* flags) { return flags && flag
 __device__ __forceinline__ int iter_m(const BroydenDev& b, int m_host) {
     return b.step_dev ? *b.step_dev - 1 : m_host;
 }
+// Seeded rows, read on the device so that captured launches see later seeds.
+__device__ __forceinline__ int seeded(const BroydenDev& b) { return b.step_dev ? b.step_dev[1] : b.base; }
 
 // max that keeps a NaN (a non-finite residual must not read as converged)
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
@@ -124,10 +126,11 @@ __global__ void norm_finalize(BroydenDev b, const int* flags) {
 }
 
 // c[it] = sum_s V[it][s] x[s] for it = 1..rows (one block per row);
-// rows = m - 1 + which with m from the host or the device.
+// rows = seeded + m - 1 + which with m from the host or the device (rows
+// 1..seeded: a seeded initial inverse Jacobian).
 __global__ void dots_kernel(BroydenDev b, const double* __restrict__ x, int m_host, int which, const int* flags) {
     if (skipped(flags)) return;
-    const int rows = iter_m(b, m_host) - 1 + which;
+    const int rows = seeded(b) + iter_m(b, m_host) - 1 + which;
     const int it = blockIdx.x + 1;
     if (it > rows) return;
     const double* v = b.V + (size_t)it * b.S;
@@ -137,31 +140,34 @@ __global__ void dots_kernel(BroydenDev b, const double* __restrict__ x, int m_ho
     if (threadIdx.x == 0) b.c[it] = acc;
 }
 
-// Broyden_Second_Parallel.cpp:381-403: sum = W c (it < m), new V and W rows at m.
+// Broyden_Second_Parallel.cpp:381-403: sum = W c (it < m), new V and W rows at m
+// (after the seeded rows).
 __global__ void newrow_kernel(BroydenDev b, int m_host, const int* flags) {
     if (skipped(flags)) return;
     const int m = iter_m(b, m_host);
     if (m <= 0) return;
+    const int row = seeded(b) + m;
     const double denom = b.scal[2];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
         double acc = 0.0;
-        for (int it = 1; it <= m - 1; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
+        for (int it = 1; it <= row - 1; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
         const double dF = b.dF[s];
         const double dn = b.n_in[s] - b.n_prev[s];
         // a zero step (identical consecutive residuals) adds no direction: the
         // reference would divide by zero here
-        b.V[(size_t)m * b.S + s] = denom > 0.0 ? dF / denom : 0.0;
-        b.W[(size_t)m * b.S + s] = -b.fraction * dF + dn - acc;
+        b.V[(size_t)row * b.S + s] = denom > 0.0 ? dF / denom : 0.0;
+        b.W[(size_t)row * b.S + s] = -b.fraction * dF + dn - acc;
     }
 }
 
-// Broyden_Second_Parallel.cpp:455-481: sum = W c (it <= m), then the new input.
+// Broyden_Second_Parallel.cpp:455-481: sum = W c (it <= m, after the seeded
+// rows), then the new input.
 __global__ void final_kernel(BroydenDev b, int m_host, const int* flags) {
     if (skipped(flags)) return;
-    const int m = iter_m(b, m_host);
+    const int rows = seeded(b) + iter_m(b, m_host);
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
         double acc = 0.0;
-        for (int it = 1; it <= m; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
+        for (int it = 1; it <= rows; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
         b.sum[s] = acc;
         const double prev = b.n_in[s];
         b.n_prev[s] = prev;
@@ -183,13 +189,14 @@ __global__ void step_kernel(BroydenDev b, double max_norm, double switch_norm, i
     flags[1] += 1;
     const int step = *b.step_dev + 1;
     *b.step_dev = step;
+    const int limit = b.max_step - seeded(b);  // seeded rows take history capacity
     const bool fp64_charge = !(switch_norm > 0) || flags[4];
     if (!fp64_charge) flags[7] += 1;  // steps on a low-precision charge
     if (!isfinite(nrm))
         flags[2] = 2;
     else if (fp64_charge && !(nrm > max_norm))
         flags[0] = 1;
-    else if (step > b.max_step)
+    else if (step > limit)
         flags[2] = 1;
     flags[3] = (flags[0] || flags[2]) ? 1 : 0;
     if (switch_norm > 0) {
@@ -239,10 +246,10 @@ cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int
         return cudaGetLastError();
     }
     if (m > 0) {
-        if (m - 1 >= 1) dots_kernel<<<m - 1, kThreads, 0, s>>>(b, b.dF, m, 0, nullptr);
+        if (b.base + m - 1 >= 1) dots_kernel<<<b.base + m - 1, kThreads, 0, s>>>(b, b.dF, m, 0, nullptr);
         newrow_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m, nullptr);
-        dots_kernel<<<m, kThreads, 0, s>>>(b, b.F, m, 1, nullptr);
     }
+    if (b.base + m >= 1) dots_kernel<<<b.base + m, kThreads, 0, s>>>(b, b.F, m, 1, nullptr);
     final_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m, nullptr);
     return cudaGetLastError();
 }

@@ -173,7 +173,9 @@ struct BroydenDev {
     double* scal;     // [4]: max norm, sum of squares, denominator, spare
     double* part;     // [3 * nblocks] block partials
     int nblocks;
-    int* step_dev;    // device copy of the step counter (read by device-resident steps)
+    int* step_dev;    // device int[2]: [0] the step counter (read by device-resident steps),
+                      // [1] rows 1..[1] of V, W hold a seeded initial inverse Jacobian (0: none)
+    int base;         // host copy of step_dev[1]
 };
 cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s, const int* flags = nullptr);
 cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int* flags = nullptr);

@@ -391,6 +391,26 @@ class Broyden:
 
     Reset_Broyden_Parallel = reset
 
+    def set_initial_jacobian(self, V, W, stream=None):
+        """Initial inverse Jacobian G0 = fraction I + sum_j W[j] V[j]^T for the
+        next solve (V, W: device float64 [k][S]); call after create or reset."""
+        k = 0 if V is None else int(V.shape[0])
+        check(_lib.load().negf_broyden_set_initial_jacobian(self._h, _ptr(V), _ptr(W), k, _stream(stream)),
+              "negf_broyden_set_initial_jacobian")
+
+    @staticmethod
+    def secant_rows(dn, dF, fraction=0.1):
+        """Rows (V, W) of the modified-second method for secant pairs
+        dn[j], dF[j] (device float64 [k][S]): V[j] = dF[j] / |dF[j]|^2,
+        W[j] = -fraction dF[j] + dn[j] - sum_{i<j} W[i] (V[i] . dF[j])
+        (Broyden_Second_Parallel.cpp:381-403)."""
+        V = dF / (dF * dF).sum(dim=1, keepdim=True)
+        W = -fraction * dF + dn
+        for j in range(1, dF.shape[0]):
+            c = V[:j] @ dF[j]
+            W[j] -= c @ W[:j]
+        return V, W
+
     @property
     def step_number(self) -> int:
         v = C.c_int()

@@ -426,8 +426,34 @@ def generate_scf_pairs(n, seed=20261203 + 5, vds_bins=13, max_iter=60, unitcells
 
 
 # ---------------------------------------------------------------------- SCF
+def surrogate_secant_rows(model, Kd, U0, n0, Vg, Vds, k, fraction, rel_step=0.02):
+    """Initial inverse-Jacobian rows from the surrogate at the charge n0: k
+    secant pairs of its residual map F_s(n) = n - Q_s(U0 + K n) along the
+    first k cosine modes of the charge (each step sized so that the
+    potential moves by rel_step of its range, above the BF16 input
+    resolution), turned into rows of the modified-second method."""
+    import torch
+    from .negf import Broyden
+    N = n0.numel()
+    K = Kd.view(N, N)
+    s = torch.arange(N, dtype=torch.float64, device=n0.device)
+    D = torch.stack([torch.cos(math.pi * j * (s + 0.5) / N) for j in range(k)])  # [k][N]
+    KD = D @ K.T  # potential change of each unit direction
+    U_base = U0 + K @ n0
+    scale = rel_step * float(U_base.abs().max().clamp_min(1e-12))
+    dn = D * (scale / KD.abs().max(dim=1, keepdim=True).values.clamp_min(1e-300))
+    n_all = torch.cat([n0[None], n0[None] + dn])  # [k+1][N]
+    U_all = U0[None] + n_all @ K.T
+    vg = torch.full((k + 1,), float(Vg), dtype=torch.float32, device=n0.device)
+    vd = torch.full((k + 1,), float(Vds), dtype=torch.float32, device=n0.device)
+    Q = model.predict(U_all.float(), vg, vd, batch=min(16, k + 1))
+    F = n_all - Q
+    return Broyden.secant_rows(dn, F[1:] - F[0][None], fraction=fraction)
+
+
 def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e-6, max_step=200,
-              use_graph=True, iters_per_graph=4, surrogate_norm=1e-3, surrogate_max_step=60, keep_history=True):
+              use_graph=True, iters_per_graph=4, surrogate_norm=1e-3, surrogate_max_step=60, keep_history=True,
+              seed_rows=0):
     """Gate sweep of one tube, plain or surrogate-started.
 
     Plain: Broyden from n = 0 with the NEGF charge (device-resident steps,
@@ -435,8 +461,11 @@ def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e
     the loop with the surrogate's charge (to surrogate_norm) and then
     continues, without a reset, with the NEGF charge; the Broyden history
     built on the surrogate is the initial inverse Jacobian of the NEGF phase
-    (keep_history=False: only the charge is kept) and only an NEGF charge can
-    end the step.  A surrogate phase that does not converge within
+    (keep_history=False: only the charge is kept; seed_rows=k > 0: the NEGF
+    phase starts from the surrogate's charge with k secant rows of the
+    surrogate at that charge as its initial inverse Jacobian,
+    negf_broyden_set_initial_jacobian) and only an NEGF charge can end the
+    step.  A surrogate phase that does not converge within
     surrogate_max_step steps (or turns non-finite) is discarded and the step
     starts plain.  Returns per-step records (NEGF iterations, surrogate
     iterations, whether the surrogate start was used, seconds, charge)."""
@@ -514,6 +543,12 @@ def scf_sweep(tube, electro, Vg_list, Vds, model=None, fraction=0.1, max_norm=1e
                 used = bool(f[0]) and not f[2]
                 if not used:  # discard the surrogate phase
                     br.reset(stream=stream)
+                elif seed_rows > 0:
+                    nkeep = nin_t.clone()
+                    V, W = surrogate_secant_rows(model, Kd, U0, nkeep, Vg, Vds, seed_rows, fraction)
+                    br.reset(stream=stream)
+                    nin_t.copy_(nkeep)
+                    br.set_initial_jacobian(V.contiguous(), W.contiguous(), stream=stream)
                 elif not keep_history:
                     nkeep = nin_t.clone()
                     br.reset(stream=stream)

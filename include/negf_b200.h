@@ -347,6 +347,18 @@ int negf_broyden_step(negf_broyden* b, const double* d_n_out, double* d_n_in_out
 /* Reset for the next bias step; keep_charge mirrors
  * reset_with_previous_charge_distribution, otherwise n_in = init_value. */
 int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void* stream);
+/* Initial inverse Jacobian for the next solve (no counterpart in the
+ * reference, whose loop starts from simple mixing G0 = fraction * I,
+ * Broyden_Parallel_General.cpp:68-248): G0 = fraction * I + sum_j w_j v_j^T
+ * for the k rows d_V[j][S], d_W[j][S] (device), so the first step gives
+ * n_in - scalar * G0 F and later steps add their own rows after these.
+ * Rows built from secant pairs (dn_j, dF_j) of a cheaper model, as the
+ * method builds its own (v = dF/|dF|^2, w = -fraction dF + dn - sum_{i<j}
+ * w_i (v_i . dF)), let a surrogate supply the starting Jacobian.  Call after
+ * create or reset and before the first step; k <= max_step / 2, and the k
+ * rows count against max_step.  A reset clears them.  The row count lives
+ * in device memory, so launches captured earlier see it. */
+int negf_broyden_set_initial_jacobian(negf_broyden* b, const double* d_V, const double* d_W, int k, void* stream);
 /* Broyden_Step (1-based). */
 int negf_broyden_step_number(negf_broyden* b, int* step);
 /* Device-resident Broyden step (no host synchronisation; capturable in a

@@ -78,6 +78,42 @@ def test_device_broyden_matches_host_steps():
     assert flags.cpu().tolist()[:3] == [0, 12, 0] and d.step_number == 13
 
 
+def test_broyden_initial_jacobian_exact_inverse():
+    """Seeded with secant pairs whose residual differences are the unit
+    vectors, G0 is the exact inverse Jacobian of a linear map, so the first
+    step (host or device-resident) lands on the fixed point."""
+    import torch
+    from electrostatic_b200._lib import NEGFError
+    from electrostatic_b200.negf import Broyden
+    S = 16
+    rng = np.random.default_rng(11)
+    A = 0.3 * rng.standard_normal((S, S)) / np.sqrt(S)  # n_out = A n_in + b
+    b = rng.standard_normal(S)
+    J = np.eye(S) - A  # F = n_in - n_out = J n_in - b
+    nstar = np.linalg.solve(J, b)
+    dn = torch.from_numpy(np.linalg.inv(J).T.copy()).cuda()  # dn_j = J^-1 e_j, so dF_j = e_j
+    dF = torch.eye(S, dtype=torch.float64, device="cuda")
+    V, W = Broyden.secant_rows(dn, dF, fraction=0.2)
+    for device in (False, True):
+        br = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"), max_step=40, fraction=0.2)
+        br.set_initial_jacobian(V, W)
+        x = torch.from_numpy(A @ _read(br.input_device_ptr(), S) + b).cuda()
+        if device:
+            flags = torch.zeros(4, dtype=torch.int32, device="cuda")
+            br.step_device(x, 1e-30, flags)
+        else:
+            br.step(x)
+        n1 = _read(br.input_device_ptr(), S)
+        assert np.max(np.abs(n1 - nstar)) <= 1e-10 * np.max(np.abs(nstar))
+        with pytest.raises(NEGFError, match="before the first step"):
+            br.set_initial_jacobian(V, W)
+        br.reset()
+        br.set_initial_jacobian(None, None)  # k = 0: the plain simple-mixing start
+    small = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"), max_step=20, fraction=0.2)
+    with pytest.raises(NEGFError, match="max_step / 2"):
+        small.set_initial_jacobian(V, W)
+
+
 def _read(ptr, n):
     from electrostatic_b200.scf import device_view
     return device_view(ptr, n).cpu().numpy()
