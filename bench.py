@@ -597,10 +597,16 @@ def main():
             t0 = time.perf_counter()
             _, n = ot.sample(512, 0, faithful=True, nthreads=threads)
             dt = time.perf_counter() - t0
+            # one thread (one rank of the reference): energies 0 and 2048 (1 contour + 1 real-axis)
+            t1 = time.perf_counter()
+            _, n1 = ot.sample(2048, 0, faithful=True, nthreads=1)
+            dt1 = time.perf_counter() - t1
             cpu = {"value": n / dt, "unit": "updates/s", "cores": threads, "kind": "port",
                    "sample": "8 of the 4096 energy points (every 512th: 2 contour + 6 real-axis), all 8 modes, "
                              "N=4000, faithful O(N)-per-site contact walk (NEGF_Common.cpp:3418-3426), "
-                             f"{threads} threads over energies; {dt:.2f} s"}
+                             f"{threads} threads over energies; {dt:.2f} s",
+                   "single_thread": {"value": n1 / dt1, "unit": "updates/s", "cores": 1,
+                                     "sample": f"energies 0 and 2048 (1 contour + 1 real-axis), 1 thread; {dt1:.2f} s"}}
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
         cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch, small=args.small)
