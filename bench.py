@@ -223,7 +223,8 @@ def scf_measure(threads):
 def config4_measure(torch, passes=5):
     """Uneven 16-tube batch (seeded): batched charge pass (autotuned plan)
     throughput and the self-consistent gate sweep replayed as CUDA graphs,
-    in mixed precision and in FP64."""
+    in mixed precision (FP32 contour chains; and with the real-axis chains
+    at 2 meV broadening in FP32 too) and in FP64."""
     from electrostatic_b200.electrostatics import GateAllAround
     from electrostatic_b200.negf import CNT, ChargePlan
     from electrostatic_b200.scf import run_scf_batch
@@ -234,8 +235,9 @@ def config4_measure(torch, passes=5):
                        "Broyden alpha 0.1 to 1e-6 absolute max-norm; seeded (%d)" % (SEED_BASE + 4)}
     electros = None
     Qs = {}
-    for prec in ("mixed", "fp64"):
-        descs = uneven_batch(precision=prec)
+    for prec in ("mixed", "mixed_realaxis_fp32", "fp64"):
+        descs = uneven_batch(precision="fp64" if prec == "fp64" else "mixed",
+                             realaxis_fp32=prec == "mixed_realaxis_fp32")
         tubes = [CNT(**d) for d in descs]
         if electros is None:
             electros = []
@@ -264,7 +266,7 @@ def config4_measure(torch, passes=5):
                  "schedule": {"pass2_warps_per_block": info["pass2_warps_per_block"],
                               "segs_per_unit": info["segs_per_unit"]}}
         try:
-            sw = 1e-4 if prec == "mixed" else None
+            sw = 1e-4 if prec != "fp64" else None
             r = run_scf_batch(tubes, electros, GATE_SWEEP, use_graph=True, iters_per_graph=4, switch_norm=sw)
             entry.update({"scf_seconds": r.seconds, "scf_iterations": [s.iterations for s in r.steps]})
             if sw:
@@ -275,9 +277,10 @@ def config4_measure(torch, passes=5):
             entry["scf_error"] = str(e)
         out[prec] = entry
         del tubes
-    if "mixed" in Qs and "fp64" in Qs:
-        out["mixed_vs_fp64_rel"] = max(float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
-                                       for a, b in zip(Qs["mixed"], Qs["fp64"]))
+    for name in ("mixed", "mixed_realaxis_fp32"):
+        if name in Qs and "fp64" in Qs:
+            out[name + "_vs_fp64_rel"] = max(float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+                                             for a, b in zip(Qs[name], Qs["fp64"]))
     return out
 
 

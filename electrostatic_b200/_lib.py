@@ -74,6 +74,7 @@ class TubeDesc(C.Structure):
         ("kT_window_around_singularity", C.c_double * 2),
         ("flag_noneq_integration_pts_density", C.c_int),
         ("noneq_integration_pts_density", C.c_double * NEGF_MAX_NONEQ_PATHS),
+        ("mixed_realaxis_fp32", C.c_int),
     ]
 
 

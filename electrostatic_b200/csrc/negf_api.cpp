@@ -496,7 +496,9 @@ void build_tube_chains(Out<negf::ChainRec>& chains, Out<negf::WarpRec>& warps, T
                 if (it.kind != kind) continue;
                 // FP32 recursions only for contour points at least `band` above the real
                 // axis; real-axis chains (running products over the whole tube) stay FP64
-                const int want32 = mixed && it.kind == negf::kContour && std::fabs(it.E.imag()) >= band ? 1 : 0;
+                // unless mixed_realaxis_fp32 admits those at least `band` above it too
+                const bool kind_ok = it.kind == negf::kContour || t.d.mixed_realaxis_fp32;
+                const int want32 = mixed && kind_ok && std::fabs(it.E.imag()) >= band ? 1 : 0;
                 if (want32 != fp32) continue;
                 for (int m = 0; m < M; ++m) {
                     negf::ChainRec c{};
@@ -976,6 +978,7 @@ int negf_tube_desc_init(negf_tube_desc* d) {
     d->decimation_layers = 10;
     d->precision = NEGF_PREC_FP64;
     d->mixed_fp64_band = 1e-3;
+    d->mixed_realaxis_fp32 = 0;
     d->flatband_dos_integration_pts = 100;
     d->flag_adaptive_integration_limits = 0;
     d->integrand_correction_interval = 500;

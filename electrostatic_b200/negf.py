@@ -53,8 +53,9 @@ class CNT:
     decimation_layers, flatband_dos_integration_pts,
     flag_adaptive_integration_limits, integrand_correction_interval,
     kT_window_around_singularity, noneq_integration_pts_density; plus
-    realaxis_window=(min, max, pts, kind), precision ("fp64" | "mixed") and
-    mixed_fp64_band.
+    realaxis_window=(min, max, pts, kind), precision ("fp64" | "mixed"),
+    mixed_fp64_band and mixed_realaxis_fp32 (mixed mode: real-axis chains at
+    least the band above the axis in FP32 too).
     """
 
     def __init__(self, type_id=(17, 0), num_unitcells=100, num_modes=1, acc=1.42e-10, gamma=2.5,
@@ -64,7 +65,7 @@ class CNT:
                  decimation_max_iter=30, decimation_layers=10, realaxis_window=None, precision="fp64",
                  mixed_fp64_band=1e-3, flatband_dos_integration_pts=100, flag_adaptive_integration_limits=0,
                  integrand_correction_interval=500, kT_window_around_singularity=(1.0, 1.0),
-                 noneq_integration_pts_density=None):
+                 noneq_integration_pts_density=None, mixed_realaxis_fp32=False):
         L = _lib.load()
         d = _lib.TubeDesc()
         check(L.negf_tube_desc_init(C.byref(d)), "negf_tube_desc_init")
@@ -98,6 +99,7 @@ class CNT:
             d.realaxis_min, d.realaxis_max, d.realaxis_pts, d.realaxis_kind = float(lo), float(hi), int(pts), int(kind)
         d.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
         d.mixed_fp64_band = float(mixed_fp64_band)
+        d.mixed_realaxis_fp32 = int(bool(mixed_realaxis_fp32))
         d.flatband_dos_integration_pts = int(flatband_dos_integration_pts)
         d.flag_adaptive_integration_limits = int(flag_adaptive_integration_limits)
         d.integrand_correction_interval = int(integrand_correction_interval)

@@ -38,9 +38,11 @@ def site_potential(y_nm, seed, amp=0.4, ramp=0.5):
     return U + ramp * (y_nm - y_nm[0]) / L
 
 
-def uneven_batch(num_tubes=16, precision="mixed", vds=0.4, seed=SEED_BASE + 4, scale=1.0):
+def uneven_batch(num_tubes=16, precision="mixed", vds=0.4, seed=SEED_BASE + 4, scale=1.0, realaxis_fp32=False):
     """Tube descriptors (CNT keyword dicts) of the uneven batch; `scale`
-    shrinks lengths and energy counts for tests (1.0 = the benchmark)."""
+    shrinks lengths and energy counts for tests (1.0 = the benchmark);
+    realaxis_fp32: mixed mode also runs the real-axis chains (broadening
+    2 meV, above the 1 meV FP64 band) in FP32."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(num_tubes):
@@ -55,7 +57,8 @@ def uneven_batch(num_tubes=16, precision="mixed", vds=0.4, seed=SEED_BASE + 4, s
         ne = (ne_total // 4, ne_total // 2, ne_total - ne_total // 4 - ne_total // 2)
         out.append(dict(type_id=(m, 0), num_unitcells=uc, num_modes=M, contact_mu=(0.0, -float(vds)),
                         contact_T=(300.0, 300.0), eq_integration_pts=eq, noneq_integration_pts=ne,
-                        noneq_percent_intercuts=(30.0, 70.0), E_zPlus_imag=2e-3, precision=precision))
+                        noneq_percent_intercuts=(30.0, 70.0), E_zPlus_imag=2e-3, precision=precision,
+                        mixed_realaxis_fp32=bool(realaxis_fp32)))
     return out
 
 

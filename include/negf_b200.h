@@ -74,7 +74,7 @@ typedef struct negf_tube_desc {
     int realaxis_pts, realaxis_kind;
     int precision;                 /* NEGF_PREC_FP64 or NEGF_PREC_MIXED */
     double mixed_fp64_band;        /* mixed mode: contour points with Im E below this [eV] and every
-                                      real-axis point stay FP64 (1e-3) */
+                                      real-axis point (see mixed_realaxis_fp32) stay FP64 (1e-3) */
     int flatband_dos_integration_pts; /* DOS path points at zero bias (NEGF_Common.H:416, 100) */
     /* Adaptive non-equilibrium limits (Read_AdaptiveIntegrationParams,
      * NEGF_Common.cpp:524-543; NEGF_Common.H:453-457). */
@@ -83,6 +83,10 @@ typedef struct negf_tube_desc {
     double kT_window_around_singularity[2];    /* {1, 1} */
     int flag_noneq_integration_pts_density;    /* 1 when the densities below are given */
     double noneq_integration_pts_density[NEGF_MAX_NONEQ_PATHS]; /* points per kT of each path */
+    /* Mixed mode, no counterpart in the reference: 1 also runs the real-axis
+     * chains at least mixed_fp64_band above the axis (broadening
+     * E_zPlus_imag >= band) in FP32 (0, default: real-axis chains stay FP64). */
+    int mixed_realaxis_fp32;
 } negf_tube_desc;
 
 /* Fill `d` with the reference defaults. */

@@ -33,7 +33,7 @@ def _potential(N, y_nm, seed, amp=0.4):
 def _pair(oracle, seed=0, U=None, Uc=None, **kw):
     from electrostatic_b200.negf import CNT
     g = CNT(**kw)
-    okw = {k: v for k, v in kw.items() if k not in ("precision", "mixed_fp64_band")}
+    okw = {k: v for k, v in kw.items() if k not in ("precision", "mixed_fp64_band", "mixed_realaxis_fp32")}
     if "noneq_percent_intercuts" not in okw:
         okw["noneq_percent_intercuts"] = None
     o = oracle.OracleTube(**okw)
@@ -114,6 +114,23 @@ def test_mixed_precision_broadened_real_axis(oracle, cells):
     from electrostatic_b200.negf import last_stats
     st = last_stats()
     assert st["updates_fp32"] == st["contour_updates"] > 0
+    Qo = o.charge(nthreads=8)
+    assert np.all(np.isfinite(Qg))
+    assert _rel(Qg, Qo) <= MIXED_TOL, _rel(Qg, Qo)
+
+
+@pytest.mark.parametrize("cells", [25, 400])
+def test_mixed_precision_fp32_real_axis(oracle, cells):
+    """mixed_realaxis_fp32: the real-axis chains at eta = 2 meV (above the
+    1 meV band) run in FP32 too, within the mixed tolerance."""
+    kw = dict(type_id=(17, 0), num_unitcells=cells, num_modes=3, contact_mu=(0.0, -0.4), contact_T=(300.0, 300.0),
+              eq_integration_pts=(24, 24, 40), noneq_integration_pts=(40, 60, 40),
+              noneq_percent_intercuts=(30.0, 70.0), E_zPlus_imag=2e-3, precision="mixed", mixed_realaxis_fp32=True)
+    g, o = _pair(oracle, seed=13, **kw)
+    Qg = g.Solve_NEGF()
+    from electrostatic_b200.negf import last_stats
+    st = last_stats()
+    assert st["updates_fp32"] > st["contour_updates"] > 0
     Qo = o.charge(nthreads=8)
     assert np.all(np.isfinite(Qg))
     assert _rel(Qg, Qo) <= MIXED_TOL, _rel(Qg, Qo)
