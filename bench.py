@@ -78,7 +78,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -166,7 +166,9 @@ def run_reference_arm(args, rank, world):
     U = site_potential(y, SEED)
     t.set_potential(U, (U[0], U[-1]))
     threads = len(os.sched_getaffinity(0))
-    stride = 512
+    # 8 energy points per step (about 1 s on 16 threads) for short runs; for
+    # many steps fewer points per step keep the whole run within minutes
+    stride = 512 if args.steps <= 20 else (1024 if args.steps <= 60 else 4096)
     for i in range(args.warmup):
         t.sample(stride, i % stride, faithful=True, nthreads=threads)
     tot_upd, tot_t = 0, 0.0
@@ -176,8 +178,9 @@ def run_reference_arm(args, rank, world):
         tot_t += time.perf_counter() - t0
         tot_upd += n
     v = tot_upd / tot_t
-    sample = (f"every {stride}th of the 4096 energy points per step (8 points incl. contour and real-axis, all 8 "
-              f"modes, N=4000), faithful O(N)-per-site contact walk as in NEGF_Common.cpp:3418-3426")
+    sample = (f"every {stride}th of the 4096 energy points per step ({4096 // stride} point(s), offsets rotating "
+              f"over contour and real-axis points, all 8 modes, N=4000), faithful O(N)-per-site contact walk as in "
+              f"NEGF_Common.cpp:3418-3426")
     line = {"impl": "reference", "metric": "site*energy RGF updates/s", "value": v, "unit": "updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
