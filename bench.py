@@ -169,12 +169,13 @@ def run_reference_arm(args, rank, world):
     # 8 energy points per step (about 1 s on 16 threads) for short runs; for
     # many steps fewer points per step keep the whole run within minutes
     stride = 512 if args.steps <= 20 else (1024 if args.steps <= 60 else 4096)
+    # offsets hop by 1031 (coprime to 4096): the samples mix contour and real-axis points as the grid does
     for i in range(args.warmup):
-        t.sample(stride, i % stride, faithful=True, nthreads=threads)
+        t.sample(stride, (i * 1031) % stride, faithful=True, nthreads=threads)
     tot_upd, tot_t = 0, 0.0
     for i in range(args.steps):
         t0 = time.perf_counter()
-        _, n = t.sample(stride, (args.warmup + i) % stride, faithful=True, nthreads=threads)
+        _, n = t.sample(stride, ((args.warmup + i) * 1031) % stride, faithful=True, nthreads=threads)
         tot_t += time.perf_counter() - t0
         tot_upd += n
     v = tot_upd / tot_t
