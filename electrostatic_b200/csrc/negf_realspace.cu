@@ -678,18 +678,36 @@ __global__ void __launch_bounds__(32) rs_selftest_kernel(int product, int count,
     }
 }
 
-// Q[r] = sum over energies of rows[e][r], Kahan, energies in order.
-__global__ void rs_reduce_kernel(const double* __restrict__ rows, int num_e, int N, double* __restrict__ Q) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= N) return;
+// Q[r] = sum over energies of rows[e][r]: block = 32 rings x kRsGroups
+// energy groups; each thread sums energies g, g + kRsGroups, ... (Kahan),
+// then the groups are combined in a fixed order (deterministic).
+constexpr int kRsGroups = 8;
+__global__ void __launch_bounds__(32 * kRsGroups) rs_reduce_kernel(const double* __restrict__ rows, int num_e, int N,
+                                                                   double* __restrict__ Q) {
+    __shared__ double sh_s[kRsGroups][32], sh_c[kRsGroups][32];
+    const int r = blockIdx.x * 32 + threadIdx.x, g = threadIdx.y;
     double s = 0.0, comp = 0.0;
-    for (int e = 0; e < num_e; ++e) {
-        const double y = rows[(size_t)e * N + r] - comp;
-        const double t = s + y;
-        comp = (t - s) - y;
-        s = t;
+    if (r < N) {
+        for (int e = g; e < num_e; e += kRsGroups) {
+            const double y = rows[(size_t)e * N + r] - comp;
+            const double t = s + y;
+            comp = (t - s) - y;
+            s = t;
+        }
     }
-    Q[r] = s;
+    sh_s[g][threadIdx.x] = s;
+    sh_c[g][threadIdx.x] = comp;
+    __syncthreads();
+    if (g == 0 && r < N) {
+        double tot = 0.0, c = 0.0;
+        for (int i = 0; i < kRsGroups; ++i) {
+            const double y = (sh_s[i][threadIdx.x] - sh_c[i][threadIdx.x]) - c;
+            const double t = tot + y;
+            c = (t - tot) - y;
+            tot = t;
+        }
+        Q[r] = tot;
+    }
 }
 
 // Uatoms[r][j] = U[r] (ring-uniform potential on the atoms).
@@ -755,7 +773,7 @@ cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int N = 2 * K;
-    rs_reduce_kernel<<<(N + 127) / 128, 128, 0, stream>>>(d_rows, num_e, N, d_Q);
+    rs_reduce_kernel<<<(N + 31) / 32, dim3(32, kRsGroups), 0, stream>>>(d_rows, num_e, N, d_Q);
     return cudaGetLastError();
 }
 }  // namespace
