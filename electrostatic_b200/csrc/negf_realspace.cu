@@ -37,7 +37,8 @@
 // smaller still: the decimation converges quadratically).
 //
 // Kernels (one warp per energy; m x m complex tiles in shared memory,
-// row-major, products staged in registers so that outputs may alias inputs):
+// row-major; m x m products on the FP64 tensor cores, mma.sync m8n8k4, with
+// the results staged in registers so that outputs may alias inputs):
 //   rs_lead_kernel   both lead corners s_L = g[b][b], s_R = g[a][a];
 //   rs_chain_kernel  forward sweep (X_k to global scratch), backward sweep
 //                    with the ring sums of c G_jj written per energy;
@@ -151,38 +152,68 @@ __device__ __forceinline__ int wrap(int i) { return i < 0 ? i + M : (i >= M ? i 
         }                                                      \
     }
 
-// C = s op(A) op(B) (+ D when ADD); op = transpose for TA / TB.  C may alias
-// any operand: the products are staged in registers.
+// FP64 tensor-core product D += A B of an 8 x 8 x 4 tile (mma.sync m8n8k4,
+// FP64).  Fragments, g = lane / 4, t = lane % 4: a = A[g][t]; b = B[t][g];
+// d = D[g][2t], D[g][2t+1].
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
+}
+
+// C = s op(A) op(B) (+ D when ADD) in FP64 on the tensor cores: the m x m
+// tiles are read as zero-padded 16 x 16 operands (2 x 2 output tiles of
+// 8 x 8, k in steps of 4), complex products in four real products so that
+// each part keeps the rounding of an FP64 dot product.  C may alias any
+// operand: the products are staged in registers.
 template <int m, bool TA, bool TB, bool ADD>
 __device__ __forceinline__ void mm(Mat<m, double> C, Mat<m, double> A, Mat<m, double> B, Mat<m, double> D, double s,
                                    int lane) {
-    const int c = lane & 15, h = lane >> 4;
-    cplxd acc[8];
+    const int g = lane >> 2, t = lane & 3;
+    constexpr int NT = (m + 7) / 8;  // 8 x 8 output tiles per dimension
+    double cr[NT][NT][2], ci[NT][NT][2];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) acc[i] = cmk(0.0, 0.0);
-    if (c < m) {
+    for (int i = 0; i < NT; ++i)
 #pragma unroll
-        for (int k = 0; k < m; ++k) {
-            const cplxd b = TB ? B.at(c, k) : B.at(k, c);
+        for (int j = 0; j < NT; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int r = h + 2 * i;
-                if (r < m) acc[i] = cfma(TA ? A.at(k, r) : A.at(r, k), b, acc[i]);
+    for (int k0 = 0; k0 < m; k0 += 4) {
+        const int k = k0 + t;
+        cplxd a[NT], b[NT];
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+            const int r = 8 * i + g;
+            a[i] = cmk(0.0, 0.0);
+            if (r < m && k < m) a[i] = TA ? A.at(k, r) : A.at(r, k);
+            b[i] = cmk(0.0, 0.0);
+            if (k < m && r < m) b[i] = TB ? B.at(r, k) : B.at(k, r);  // column 8 i + g of B
+        }
+#pragma unroll
+        for (int i = 0; i < NT; ++i) {
+            const double nai = -a[i].y;
+#pragma unroll
+            for (int j = 0; j < NT; ++j) {
+                dmma(cr[i][j], a[i].x, b[j].x);
+                dmma(cr[i][j], nai, b[j].y);
+                dmma(ci[i][j], a[i].x, b[j].y);
+                dmma(ci[i][j], a[i].y, b[j].x);
             }
         }
     }
     __syncwarp();
-    if (c < m) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int r = h + 2 * i;
-            if (r < m) {
-                cplxd v = cscale(acc[i], s);
-                if (ADD) v = cadd(v, D.at(r, c));
-                C.at(r, c) = v;
+    for (int i = 0; i < NT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int r = 8 * i + g, c = 8 * j + 2 * t + q;
+                if (r < m && c < m) {
+                    cplxd v = cmk(cr[i][j][q] * s, ci[i][j][q] * s);
+                    if (ADD) v = cadd(v, D.at(r, c));
+                    C.at(r, c) = v;
+                }
             }
-        }
-    }
     __syncwarp();
 }
 
