@@ -445,6 +445,20 @@ __device__ __forceinline__ cplxd warp_sum(cplxd v) {
     return v;
 }
 
+// Asynchronous global -> shared copy of one complex value (cp.async, 8 or 16
+// bytes, both addresses aligned to the size) and the wait for all of them.
+template <typename T>
+__device__ __forceinline__ void cp_async(T* smem_dst, const T* gsrc) {
+    static_assert(sizeof(T) == 8 || sizeof(T) == 16, "cp.async copies 8 or 16 bytes here");
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if constexpr (sizeof(T) == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Energy flags: kRsFP32 runs the chain in FP32, kRsZeroU takes U = 0 on the
 // atoms and the contacts (the Rho0 pass).
 constexpr int kRsFP32 = 1, kRsZeroU = 2;
@@ -559,10 +573,10 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
         }
     };
     // g_L[b][b] = D^-1 + gamma^2 Y^T X Y into Gbb
-    auto form_gbb = [&]() {
+    auto form_gbb = [&](Mat<m, R> Xt) {
         RS_FOR_ENTRIES(m, lane, {
             const int r0 = wrap<m>(r - 1), c0 = wrap<m>(c - 1);
-            const C q = cadd(cadd(X.at(r, c), X.at(r, c0)), cadd(X.at(r0, c), X.at(r0, c0)));
+            const C q = cadd(cadd(Xt.at(r, c), Xt.at(r, c0)), cadd(Xt.at(r0, c), Xt.at(r0, c0)));
             C v = cscale(cmul(cmul(dv[r], dv[c]), q), g2);
             if (r == c) v = cadd(v, dv[r]);
             Gbb.at(r, c) = v;
@@ -594,7 +608,7 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
         ok = invert<m>(X, X, buf, lane) && ok;
         C* dst = myX + (size_t)k * mm2;
         for (int i = lane; i < mm2; i += 32) dst[i] = X.a[i];
-        form_gbb();
+        form_gbb(X);
     }
     // G_K[a][a] of the right lead's first ring: (I - gamma^2 s_R g_L[b][b])^-1 s_R
     for (int i = lane; i < mm2; i += 32) X.a[i] = cmk((R)sR[i].x, (R)sR[i].y);
@@ -604,13 +618,20 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
     ok = invert<m>(Gn, Gn, buf, lane) && ok;
     mm<m, false, false, false>(Gn, Gn, X, Gn, one, lane);
     fetch_u(K - 1);
+    // Backward.  X_{k-1} is copied into the tile that held the product W of
+    // step k (free once tr G[b][b] is formed) while the last two products of
+    // step k run; the two tiles swap roles every step.
+    Mat<m, R> Xc = X, Wc = W;
+    {
+        const C* src = myX + (size_t)(K - 1) * mm2;
+        for (int i = lane; i < mm2; i += 32) Xc.a[i] = src[i];
+    }
     for (int k = K - 1; k >= 0; --k) {
-        const C* src = myX + (size_t)k * mm2;
-        for (int i = lane; i < mm2; i += 32) X.a[i] = src[i];
+        cp_async_wait_all();  // X_k (issued during step k + 1) has landed
         if (lane < m) dv[lane] = crcp(cmk(E.x - ub_n, E.y));
         if (k > 0) fetch_u(k - 1);
         __syncwarp();
-        form_gbb();
+        form_gbb(Xc);
         // Z = Y G' Y^T, Y = C D^-1
         RS_FOR_ENTRIES(m, lane, {
             const int r1 = wrap<m>(r + 1), c1 = wrap<m>(c + 1);
@@ -622,16 +643,27 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
         })
         __syncwarp();
         // tr G[b][b] = tr g_L[b][b] + gamma^2 sum_rc (g_L[b][b] G')[r][c] g_L[b][b][c][r]
-        mm<m, false, false, false>(W, Gbb, Gn, W, one, lane);
+        mm<m, false, false, false>(Wc, Gbb, Gn, Wc, one, lane);
         cplxd tb = cmk(0.0, 0.0);
         RS_FOR_ENTRIES(m, lane, {
-            const C w = cmul(cscale(W.at(r, c), g2), Gbb.at(c, r));
+            const C w = cmul(cscale(Wc.at(r, c), g2), Gbb.at(c, r));
             tb = cadd(tb, cmk((double)w.x, (double)w.y));
             if (r == c) tb = cadd(tb, cmk((double)Gbb.at(r, r).x, (double)Gbb.at(r, r).y));
         })
+        __syncwarp();  // every lane is done with Wc
+        if (k > 0) {
+            const C* src = myX + (size_t)(k - 1) * mm2;
+            for (int i = lane; i < mm2; i += 32) cp_async(Wc.a + i, src + i);
+            cp_async_commit();
+        }
         // G[a][a] = X + gamma^4 (X Z) X
-        mm<m, false, false, false>(Z, X, Z, Z, one, lane);
-        mm<m, false, false, true>(Gn, Z, X, X, g4, lane);
+        mm<m, false, false, false>(Z, Xc, Z, Z, one, lane);
+        mm<m, false, false, true>(Gn, Z, Xc, Xc, g4, lane);
+        {
+            const Mat<m, R> tt = Xc;
+            Xc = Wc;
+            Wc = tt;
+        }
         cplxd ta = cmk(0.0, 0.0);
         if (lane < m) ta = cmk((double)Gn.at(lane, lane).x, (double)Gn.at(lane, lane).y);
         ta = warp_sum(ta);
