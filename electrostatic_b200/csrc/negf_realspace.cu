@@ -163,19 +163,21 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
 
 // C = s op(A) op(B) (+ D when ADD) in FP64 on the tensor cores: the m x m
 // tiles are read as zero-padded 16 x 16 operands (2 x 2 output tiles of
-// 8 x 8, k in steps of 4), complex products in four real products so that
-// each part keeps the rounding of an FP64 dot product.  C may alias any
+// 8 x 8, k in steps of 4), complex products in the three-multiply form
+// Re = ArBr - AiBi, Im = (Ar + Ai)(Br + Bi) - ArBr - AiBi.  C may alias any
 // operand: the products are staged in registers.
 template <int m, bool TA, bool TB, bool ADD>
 __device__ __forceinline__ void mm(Mat<m, double> C, Mat<m, double> A, Mat<m, double> B, Mat<m, double> D, double s,
                                    int lane) {
     const int g = lane >> 2, t = lane & 3;
     constexpr int NT = (m + 7) / 8;  // 8 x 8 output tiles per dimension
-    double cr[NT][NT][2], ci[NT][NT][2];
+    double p1[NT][NT][2], p2[NT][NT][2], p3[NT][NT][2];  // Ar Br, Ai Bi, (Ar + Ai)(Br + Bi)
 #pragma unroll
     for (int i = 0; i < NT; ++i)
 #pragma unroll
-        for (int j = 0; j < NT; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) p1[i][j][q] = p2[i][j][q] = p3[i][j][q] = 0.0;
 #pragma unroll
     for (int k0 = 0; k0 < m; k0 += 4) {
         const int k = k0 + t;
@@ -190,13 +192,12 @@ __device__ __forceinline__ void mm(Mat<m, double> C, Mat<m, double> A, Mat<m, do
         }
 #pragma unroll
         for (int i = 0; i < NT; ++i) {
-            const double nai = -a[i].y;
+            const double as = a[i].x + a[i].y;
 #pragma unroll
             for (int j = 0; j < NT; ++j) {
-                dmma(cr[i][j], a[i].x, b[j].x);
-                dmma(cr[i][j], nai, b[j].y);
-                dmma(ci[i][j], a[i].x, b[j].y);
-                dmma(ci[i][j], a[i].y, b[j].x);
+                dmma(p1[i][j], a[i].x, b[j].x);
+                dmma(p2[i][j], a[i].y, b[j].y);
+                dmma(p3[i][j], as, b[j].x + b[j].y);
             }
         }
     }
@@ -209,7 +210,8 @@ __device__ __forceinline__ void mm(Mat<m, double> C, Mat<m, double> A, Mat<m, do
             for (int q = 0; q < 2; ++q) {
                 const int r = 8 * i + g, c = 8 * j + 2 * t + q;
                 if (r < m && c < m) {
-                    cplxd v = cmk(cr[i][j][q] * s, ci[i][j][q] * s);
+                    const double re = p1[i][j][q] - p2[i][j][q], im = p3[i][j][q] - p1[i][j][q] - p2[i][j][q];
+                    cplxd v = cmk(re * s, im * s);
                     if (ADD) v = cadd(v, D.at(r, c));
                     C.at(r, c) = v;
                 }
@@ -632,14 +634,13 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
         if (k > 0) fetch_u(k - 1);
         __syncwarp();
         form_gbb(Xc);
-        // Z = Y G' Y^T, Y = C D^-1
+        // Z = Y G' Y^T = C (D^-1 G' D^-1) C^T, Y = C D^-1: H = D^-1 G' D^-1 in the
+        // free tile Wc, then four neighbours of H per entry
+        RS_FOR_ENTRIES(m, lane, { Wc.at(r, c) = cmul(cmul(dv[r], Gn.at(r, c)), dv[c]); })
+        __syncwarp();
         RS_FOR_ENTRIES(m, lane, {
             const int r1 = wrap<m>(r + 1), c1 = wrap<m>(c + 1);
-            C v = cmul(cmul(dv[r], dv[c]), Gn.at(r, c));
-            v = cfma(cmul(dv[r], dv[c1]), Gn.at(r, c1), v);
-            v = cfma(cmul(dv[r1], dv[c]), Gn.at(r1, c), v);
-            v = cfma(cmul(dv[r1], dv[c1]), Gn.at(r1, c1), v);
-            Z.at(r, c) = v;
+            Z.at(r, c) = cadd(cadd(Wc.at(r, c), Wc.at(r, c1)), cadd(Wc.at(r1, c), Wc.at(r1, c1)));
         })
         __syncwarp();
         // tr G[b][b] = tr g_L[b][b] + gamma^2 sum_rc (g_L[b][b] G')[r][c] g_L[b][b][c][r]
