@@ -329,21 +329,22 @@ def config3_measure(torch, passes=2, small=False):
     # ring-corner algorithm: one m x m inverse (8m^3) and three m x m complex
     # products (8m^3 each) per block update; the lead decimation (stopped at
     # convergence, data-dependent) is not counted
-    flops = (E + E0) * K * 32 * m ** 3
+    flops = E * K * 32 * m ** 3  # timed passes: the tube's Rho0 comes from the warm-up call
     Qr = Q.cpu().numpy()
-    return {"workload": "(13,0) CNT, %d blocks of 2 rings (26 atoms), %d contour+pole energies (+%d Rho0), "
-                        "Sancho-Rubio leads (at most 32 iterations), FP64, seeded config-2 ring potential"
-                        % (K, E, E0),
-            "seconds_per_pass": sec, "block_updates_per_s": (E + E0) * K / sec,
+    return {"workload": "(13,0) CNT, %d blocks of 2 rings (26 atoms), %d contour+pole energies per pass (the "
+                        "%d-energy Rho0 pass at U = 0 runs once per tube, in the warm-up call, as the mode-space "
+                        "Rho0 does at tube creation), Sancho-Rubio leads (at most 32 iterations), FP64, seeded "
+                        "config-2 ring potential" % (K, E, E0),
+            "seconds_per_pass": sec, "block_updates_per_s": E * K / sec,
             "achieved_tflops": flops / sec / 1e12, "flops_per_pass": flops,
             "flop_convention": "ring corners m=13: inverse 8m^3 + three complex products 8m^3 per block update "
                                "(leads not counted)",
             "path": "negf_rs_compute_charge (FP64 CUDA cores, one warp per energy, Schur complements on ring corners)",
             "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm))),
-            "mixed": {"seconds_per_pass": sec_mixed, "block_updates_per_s": (E + E0) * K / sec_mixed,
-                      "fp32_energies": n32, "fp64_energies": E + E0 - n32,
+            "mixed": {"seconds_per_pass": sec_mixed, "block_updates_per_s": E * K / sec_mixed,
+                      "fp32_energies": n32, "fp64_energies": E - n32,
                       "path": "FP32 chains: TF32 tensor-core products (high/remainder split, 3 real products per "
-                              "complex product), FP32 inversion; FP64 leads, Rho0 and near-axis chains",
+                              "complex product), FP32 inversion; FP64 leads and near-axis chains",
                       "max_rel_vs_fp64": float(np.max(np.abs(Qx.cpu().numpy() - Qr)) / np.max(np.abs(Qr)))}}
 
 

@@ -164,6 +164,7 @@ struct negf_tube {
     double* d_U_pad = nullptr;  // kPadLo zeros, N sites, kPadHi zeros
     double* d_zero_pad = nullptr;
     double* d_rho0 = nullptr;
+    double* d_rs_rho0 = nullptr;  // real-space Rho0 per ring (U = 0), made by the first real-space call
     // contacts / limits (NEGF_Common.cpp:1687-1787)
     double mu[2] = {0.0, 0.0}, kT[2] = {0.0, 0.0};
     double kT_min = 0, kT_max = 0, mu_min = 0, mu_max = 0;
@@ -179,6 +180,7 @@ struct negf_tube {
         if (d_U_pad) cudaFree(d_U_pad);
         if (d_zero_pad) cudaFree(d_zero_pad);
         if (d_rho0) cudaFree(d_rho0);
+        if (d_rs_rho0) cudaFree(d_rs_rho0);
     }
 };
 
@@ -1668,14 +1670,17 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     cudaStream_t s = (cudaStream_t)stream;
     const int N = t->N, K = N / 2;
     // energies: RhoEq contour and poles (coefficients as in the mode-space
-    // pass) and Rho0 at U = 0 with negated coefficients, in one launch.  In
-    // mixed mode the contour and pole points at least mixed_fp64_band above
-    // the real axis run in FP32; the FP64 chains go first in the launch.
+    // pass).  In mixed mode the points at least mixed_fp64_band above the
+    // real axis run in FP32; the FP64 chains go first in the launch.  Rho0
+    // (U = 0, FP64) does not depend on the potential: like the mode-space
+    // Rho0 of negf_tube_create (Compute_Rho0 once at initialisation,
+    // NEGF_Common.cpp:1300) it is computed by the first real-space call for
+    // the tube and kept.
     struct RsE {
         double Er, Ei, cr, ci;
         int flags;
     };
-    std::vector<RsE> e64, e32;
+    std::vector<RsE> e64, e32, e0;
     const bool mixed = t->d.precision == NEGF_PREC_MIXED;
     const int neq = pass_items(*t, false);
     for (int idx = 0; idx < neq; ++idx) {
@@ -1683,17 +1688,19 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
         const bool fp32 = mixed && std::fabs(it.E.imag()) >= t->d.mixed_fp64_band;
         (fp32 ? e32 : e64).push_back({it.E.real(), it.E.imag(), it.c.real(), it.c.imag(), fp32 ? 1 : 0});
     }
-    rho0_paths(*t);
-    const int n0 = pass_items(*t, true);
-    for (int idx = 0; idx < n0; ++idx) {
-        const Item it = pass_item(*t, true, idx);
-        e64.push_back({it.E.real(), it.E.imag(), -it.c.real(), -it.c.imag(), 2});
+    if (!t->d_rs_rho0) {
+        rho0_paths(*t);
+        const int n0 = pass_items(*t, true);
+        for (int idx = 0; idx < n0; ++idx) {
+            const Item it = pass_item(*t, true, idx);
+            e0.push_back({it.E.real(), it.E.imag(), it.c.real(), it.c.imag(), 2});
+        }
     }
     std::vector<RsE> all(e64);
     all.insert(all.end(), e32.begin(), e32.end());
-    const int P = (int)all.size();
+    const int P = (int)all.size(), P0 = (int)e0.size();
     const size_t mm = (size_t)m * m;
-    const size_t pe = (size_t)std::max(P, 1);
+    const size_t pe = (size_t)std::max(std::max(P, P0), 1);
     // grow-only buffers kept across calls (serialised by g_mu)
     static DevBuf bE, bFlags, bU0, bUa, bCorners, bGL, bRows, bStatus;
     NEGF_CUDA(bE.reserve(sizeof(double) * 4 * pe));
@@ -1704,32 +1711,47 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     NEGF_CUDA(bGL.reserve(16 * mm * K * pe));
     NEGF_CUDA(bRows.reserve(sizeof(double) * (size_t)N * pe));
     NEGF_CUDA(bStatus.reserve(sizeof(int)));
-    std::vector<double> host(4 * pe);
-    std::vector<int> hflags(pe, 0);
-    for (int i = 0; i < P; ++i) {
-        host[i] = all[i].Er;
-        host[P + i] = all[i].Ei;
-        host[2 * P + i] = all[i].cr;
-        host[3 * P + i] = all[i].ci;
-        hflags[i] = all[i].flags;
-    }
-    double* dE = bE.as<double>();
-    NEGF_CUDA(cudaMemcpyAsync(dE, host.data(), sizeof(double) * 4 * P, cudaMemcpyHostToDevice, s));
-    NEGF_CUDA(cudaMemcpyAsync(bFlags.p, hflags.data(), sizeof(int) * P, cudaMemcpyHostToDevice, s));
     NEGF_CUDA(cudaMemsetAsync(bStatus.p, 0, sizeof(int), s));
-    NEGF_CUDA(cudaMemsetAsync(bU0.p, 0, sizeof(double) * (size_t)N * m, s));
+    const int iters = t->d.decimation_max_iter + 2;
+    double* dE = bE.as<double>();
+    auto upload = [&](const std::vector<RsE>& v, std::vector<double>& host, std::vector<int>& hflags) -> int {
+        const int n = (int)v.size();
+        host.assign(4 * (size_t)std::max(n, 1), 0.0);
+        hflags.assign((size_t)std::max(n, 1), 0);
+        for (int i = 0; i < n; ++i) {
+            host[i] = v[i].Er;
+            host[n + i] = v[i].Ei;
+            host[2 * n + i] = v[i].cr;
+            host[3 * n + i] = v[i].ci;
+            hflags[i] = v[i].flags;
+        }
+        NEGF_CUDA(cudaMemcpyAsync(dE, host.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice, s));
+        NEGF_CUDA(cudaMemcpyAsync(bFlags.p, hflags.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        return NEGF_OK;
+    };
+    std::vector<double> host0, host1;
+    std::vector<int> hflags0, hflags1;
+    if (!t->d_rs_rho0) {
+        double* d_rho = nullptr;
+        NEGF_CUDA(cudaMalloc(&d_rho, sizeof(double) * N));
+        t->d_rs_rho0 = d_rho;
+        NEGF_CUDA(cudaMemsetAsync(bU0.p, 0, sizeof(double) * (size_t)N * m, s));
+        if (int rc = upload(e0, host0, hflags0)) return rc;
+        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P0, dE + 2 * P0, dE + 3 * P0, P0,
+                                         bFlags.as<int>(), bU0.as<double>(), bU0.as<double>(), 0.0, 0.0, iters,
+                                         bCorners.p, bGL.p, bRows.as<double>(), t->d_rs_rho0, nullptr,
+                                         bStatus.as<int>(), s));
+        NEGF_CUDA(cudaStreamSynchronize(s));  // the host energy tables are rewritten below
+    }
     const double* Ua = d_Uatoms;
     if (!Ua) {
         NEGF_CUDA(negf::rs_expand(t->d_U, N, m, bUa.as<double>(), s));
         Ua = bUa.as<double>();
     }
-    const int iters = t->d.decimation_max_iter + 2;
-    if (P > 0)
-        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, P, bFlags.as<int>(),
-                                         Ua, bU0.as<double>(), t->Uc[0], t->Uc[1], iters, bCorners.p, bGL.p,
-                                         bRows.as<double>(), d_Q, bStatus.as<int>(), s));
-    else
-        NEGF_CUDA(cudaMemsetAsync(d_Q, 0, sizeof(double) * N, s));
+    if (int rc = upload(all, host1, hflags1)) return rc;
+    NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, P, bFlags.as<int>(), Ua,
+                                     bU0.as<double>(), t->Uc[0], t->Uc[1], iters, bCorners.p, bGL.p,
+                                     bRows.as<double>(), d_Q, t->d_rs_rho0, bStatus.as<int>(), s));
     int status = 0;
     NEGF_CUDA(cudaMemcpyAsync(&status, bStatus.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     NEGF_CUDA(cudaStreamSynchronize(s));

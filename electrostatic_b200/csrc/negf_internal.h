@@ -81,7 +81,8 @@ cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, c
                              double* d_chain_out, double* d_site, long long site_stride, int num_e, int M, int upw,
                              double* d_red, double* d_ldos, int N, cudaStream_t stream);
 // Real-space ring-block RGF (negf_realspace.cu): leads, chain and reduction
-// for num_e energies with coefficients c, Q[r] = sum_e Im(c sum_atoms G_jj).
+// for num_e >= 0 energies with coefficients c, Q[r] = sum_e Im(c sum_atoms
+// G_jj) - d_sub[r] (d_sub may be null).
 // d_flags[e]: 1 = chain in FP32 (tensor-core products), 2 = U = 0 pass
 // (d_Uzero on the atoms and 0 at the contacts; with negated c it subtracts
 // Rho0); otherwise the atom potentials d_Uatoms ([2K][m]) and Uc0, Uc1.
@@ -90,8 +91,8 @@ cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, c
 cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
                              const double* d_cre, const double* d_cim, int num_e, const int* d_flags,
                              const double* d_Uatoms, const double* d_Uzero, double Uc0, double Uc1, int lead_iters,
-                             void* d_corners, void* d_gL, double* d_rows, double* d_Q, int* d_status,
-                             cudaStream_t stream);
+                             void* d_corners, void* d_gL, double* d_rows, double* d_Q, const double* d_sub,
+                             int* d_status, cudaStream_t stream);
 cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_t stream);
 // Self-test of the real-space tile primitives for m in {4, 13, 16}: which 2 / 3
 // inverts count m x m complex matrices in FP64 / FP32, which 4 / 5 forms

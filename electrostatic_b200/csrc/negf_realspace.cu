@@ -742,11 +742,12 @@ __global__ void __launch_bounds__(32) rs_selftest_kernel(int product, int count,
     }
 }
 
-// Q[r] = sum over energies of rows[e][r]: block = 32 rings x kRsGroups
+// Q[r] = sum over energies of rows[e][r] (minus sub[r]): block = 32 rings x kRsGroups
 // energy groups; each thread sums energies g, g + kRsGroups, ... (Kahan),
 // then the groups are combined in a fixed order (deterministic).
 constexpr int kRsGroups = 8;
 __global__ void __launch_bounds__(32 * kRsGroups) rs_reduce_kernel(const double* __restrict__ rows, int num_e, int N,
+                                                                   const double* __restrict__ sub,
                                                                    double* __restrict__ Q) {
     __shared__ double sh_s[kRsGroups][32], sh_c[kRsGroups][32];
     const int r = blockIdx.x * 32 + threadIdx.x, g = threadIdx.y;
@@ -770,7 +771,7 @@ __global__ void __launch_bounds__(32 * kRsGroups) rs_reduce_kernel(const double*
             c = (t - tot) - y;
             tot = t;
         }
-        Q[r] = tot;
+        Q[r] = sub ? tot - sub[r] : tot;
     }
 }
 
@@ -819,25 +820,26 @@ cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_
                       const double* d_cim, int num_e, const int* d_flags, const double* d_Uatoms,
                       const double* d_Uzero,
                       double Uc0, double Uc1, int lead_iters, void* d_corners, void* d_gL, double* d_rows, double* d_Q,
-                      int* d_status, cudaStream_t stream) {
+                      const double* d_sub, int* d_status, cudaStream_t stream) {
     cudaError_t e = cudaFuncSetAttribute(rs_lead_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)rs_lead_smem_bytes(m));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(rs_chain_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)rs_chain_smem_bytes(m));
     if (e != cudaSuccess) return e;
-    rs_lead_kernel<m><<<2 * num_e, 32, rs_lead_smem_bytes(m), stream>>>(
-        gamma, d_Ere, d_Eim, num_e, d_flags, Uc0, Uc1, lead_iters, static_cast<cplxd*>(d_corners), d_status);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    rs_chain_kernel<m><<<num_e, 32, rs_chain_smem_bytes(m), stream>>>(
-        K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_flags, d_Uatoms, d_Uzero,
-        static_cast<const cplxd*>(d_corners),
-        static_cast<cplxd*>(d_gL), d_rows, d_status);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    if (num_e > 0) {
+        rs_lead_kernel<m><<<2 * num_e, 32, rs_lead_smem_bytes(m), stream>>>(
+            gamma, d_Ere, d_Eim, num_e, d_flags, Uc0, Uc1, lead_iters, static_cast<cplxd*>(d_corners), d_status);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        rs_chain_kernel<m><<<num_e, 32, rs_chain_smem_bytes(m), stream>>>(
+            K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_flags, d_Uatoms, d_Uzero,
+            static_cast<const cplxd*>(d_corners), static_cast<cplxd*>(d_gL), d_rows, d_status);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     const int N = 2 * K;
-    rs_reduce_kernel<<<(N + 31) / 32, dim3(32, kRsGroups), 0, stream>>>(d_rows, num_e, N, d_Q);
+    rs_reduce_kernel<<<(N + 31) / 32, dim3(32, kRsGroups), 0, stream>>>(d_rows, num_e, N, d_sub, d_Q);
     return cudaGetLastError();
 }
 }  // namespace
@@ -846,13 +848,13 @@ cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, co
                              const double* d_cre, const double* d_cim, int num_e, const int* d_flags,
                              const double* d_Uatoms,
                              const double* d_Uzero, double Uc0, double Uc1, int lead_iters, void* d_corners,
-                             void* d_gL, double* d_rows, double* d_Q, int* d_status, cudaStream_t stream) {
-    if (num_e <= 0) return cudaSuccess;
-    if (K < 1) return cudaErrorInvalidValue;
+                             void* d_gL, double* d_rows, double* d_Q, const double* d_sub, int* d_status,
+                             cudaStream_t stream) {
+    if (num_e < 0 || K < 1) return cudaErrorInvalidValue;
 #define RS_CASE(M)                                                                                                 \
     case M:                                                                                                        \
         return launch_rs<M>(K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_flags, d_Uatoms, d_Uzero, Uc0, Uc1,      \
-                            lead_iters, d_corners, d_gL, d_rows, d_Q, d_status, stream);
+                            lead_iters, d_corners, d_gL, d_rows, d_Q, d_sub, d_status, stream);
     switch (m) {
         RS_CASE(1) RS_CASE(2) RS_CASE(3) RS_CASE(4) RS_CASE(5) RS_CASE(6) RS_CASE(7) RS_CASE(8)
         RS_CASE(9) RS_CASE(10) RS_CASE(11) RS_CASE(12) RS_CASE(13) RS_CASE(14) RS_CASE(15) RS_CASE(16)

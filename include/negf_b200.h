@@ -219,7 +219,9 @@ int negf_set_timing(int enable);
  * precision run the contour and pole chains at least mixed_fp64_band above
  * the real axis in FP32 (m x m products on the tensor cores in TF32 with a
  * high/remainder split, the complex product in three real products); the
- * leads, the Rho0 pass and the energy sum stay FP64.  Synchronous. */
+ * leads, the Rho0 pass and the energy sum stay FP64.  The Rho0 pass (U = 0)
+ * does not depend on the potential: the first call for a tube computes it
+ * and later calls reuse it.  Synchronous. */
 int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, void* stream);
 
 /* Surrogate-model kernels (no counterpart in the reference): the training

@@ -24,6 +24,8 @@ def test_realspace_against_block_oracle(oracle, m, cells):
     Qg = g.realspace_charge()
     Qo = o.rs_charge(nthreads=8)
     assert _rel(Qg, Qo) <= TOL, _rel(Qg, Qo)
+    # the second call reuses the tube's Rho0 (computed by the first): the same charge
+    assert np.array_equal(g.realspace_charge(), Qg)
 
 
 MIXED_TOL = 1e-5
