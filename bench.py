@@ -10,9 +10,11 @@ Workload (one step = one full induced-charge pass over resident inputs):
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp64|mixed]
 
-Multi-GPU (torchrun, one rank per GPU): every rank integrates its own tube
-(independent objects, weak scaling, no collective in the data path); the step
-time is the max over ranks.
+Multi-GPU (torchrun, one rank per GPU): the ranks split the one tube's energy
+points into contiguous shards (negf_tube_set_energy_shard; Rho0 subtracted on
+rank 0 only) and sum their partial site charges with one NCCL all-reduce of
+N doubles per pass, inside the timed region: the total work is fixed as the
+GPU count grows (strong scaling).  The step time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -39,28 +41,24 @@ TEMP = (300.0, 300.0)
 SEED = 20261203 + 2
 FLOP_CONTOUR = 53  # per contour update: forward 15 + backward 15 + G_nn 15 + accumulate 8
 FLOP_REALAXIS = 76  # + two running products 12, two |G|^2 Gamma f terms 8, accumulate 3
+MIXED_RULE = ("FP32 recursions for contour/pole chains at least 1e-3 eV above the real axis (Kahan FP64 "
+              "sums); real-axis chains, chains within 1e-3 eV of a lead band edge, leads and Rho0 in FP64")
 WORKLOAD = (f"mode-space RGF induced-charge pass: (17,0) CNT N={4 * N_UNITCELLS} sites, M={N_MODES} modes, "
             f"E={sum(EQ_PTS) + RT_PTS} energies ({sum(EQ_PTS)} contour GL + {RT_PTS} real-axis uniform on "
             f"[-1.5,1.5] eV, eta={ETA} eV), mu=(0,-0.5) eV, 300 K")
 
 
 def tube_kwargs(precision="fp64"):
-    return dict(type_id=(17, 0), num_unitcells=N_UNITCELLS, num_modes=N_MODES, contact_mu=MU, contact_T=TEMP,
-                eq_integration_pts=EQ_PTS, E_zPlus_imag=ETA, realaxis_window=(-1.5, 1.5, RT_PTS, 0),
-                precision=precision)
+    from electrostatic_b200.workloads import config2_kwargs
+    kw = config2_kwargs(precision, small=RT_PTS != 3072)
+    assert kw["num_unitcells"] == N_UNITCELLS and kw["num_modes"] == N_MODES and kw["eq_integration_pts"] == EQ_PTS
+    return kw
 
 
 def site_potential(y_nm, seed):
     """Seeded sum of 5 Gaussian bumps + linear ramp 0-0.5 V (as U in eV = -phi)."""
-    rng = np.random.default_rng(seed)
-    L = y_nm[-1] - y_nm[0]
-    U = np.zeros_like(y_nm)
-    for _ in range(5):
-        A = rng.uniform(-0.4, 0.4)
-        w = rng.uniform(2.0, 10.0)
-        c = rng.uniform(0.0, L)
-        U += A * np.exp(-((y_nm - y_nm[0] - c) ** 2) / (2 * w * w))
-    return U + 0.5 * (y_nm - y_nm[0]) / L
+    from electrostatic_b200.workloads import site_potential as sp
+    return sp(y_nm, seed)
 
 
 class ClockSampler:
@@ -204,7 +202,8 @@ def scf_measure(threads):
     """Config-1 SCF sweep: device loop (FP64) vs the same loop on the CPU oracle."""
     from electrostatic_b200.electrostatics import GateAllAround
     from electrostatic_b200.negf import CNT
-    from electrostatic_b200.scf import run_scf, run_scf_batch, run_scf_oracle
+    from electrostatic_b200.scf import run_scf, run_scf_batch
+    from oracle.scf_oracle import run_scf_oracle
     from oracle import oracle as O
     tube = CNT(**SCF_KW)
     y = tube.site_positions()
@@ -483,9 +482,11 @@ def main():
 
     tube = CNT(**tube_kwargs(args.precision))
     y = tube.site_positions()
-    U = site_potential(y, SEED + rank)
+    U = site_potential(y, SEED)
     Uc = (U[0], U[-1])
     tube.set_potential(U, Uc)
+    if world > 1:
+        tube.set_energy_shard(rank, world)  # contiguous energy ranges; Rho0 on rank 0 only
     N = tube.num_field_sites
     Q = torch.zeros(N, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
@@ -497,12 +498,24 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    def charge_pass(out):
+        """One step: this rank's energy shard, then (N > 1) the sum of the
+        partial site charges over the ranks (NCCL, N doubles)."""
+        compute_charge([tube], out=out, stream=stream)
+        if dist is not None:
+            dist.all_reduce(out)
+
     clk = ClockSampler(local).__enter__()
     # ---- warm-up
     for _ in range(args.warmup):
-        compute_charge([tube], out=Q, stream=stream)
+        charge_pass(Q)
     torch.cuda.synchronize()
     clk.wait_first()
+    # updates of the whole tube (every rank's shard)
+    upd = torch.tensor([float(last_stats()["updates"])], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(upd)
+    updates = int(upd.item())
 
     # ---- timed: K passes over resident inputs, L2 flushed between passes
     set_timing(True)
@@ -513,7 +526,7 @@ def main():
     for i in range(args.steps):
         flush.zero_()
         ev[i][0].record(stream)
-        compute_charge([tube], out=Q, stream=stream)
+        charge_pass(Q)
         ev[i][1].record(stream)
         st = last_stats()  # waits for this pass's kernel events
         rgf_ms.append(st["rgf_kernel_ms"])
@@ -522,7 +535,6 @@ def main():
         p2_ms.append(st["pass2_kernel_ms"])
     barrier()
     clk_hi = clk.mark() + 1
-    clk.__exit__()
     set_timing(False)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     t_local = float(np.sum(step_ms))
@@ -530,10 +542,11 @@ def main():
     if dist is not None:
         dist.all_reduce(t_all, op=dist.ReduceOp.MAX)
     t_max = float(t_all.item())
-    updates = st["updates"]
-    value = updates * world * args.steps / (t_max * 1e-3)
+    value = updates * args.steps / (t_max * 1e-3)
+    Q_dev = Q.cpu().numpy()
 
-    # ---- end to end through the C-ABI with host buffers (H2D of U, D2H of Q)
+    # ---- end to end through the public API with host buffers: H2D of U
+    # (negf_tube_set_potential), the charge pass, and D2H of Q
     U_pinned = torch.from_numpy(U).pin_memory()
     Uh = U_pinned.numpy()
     e2e_ev = []
@@ -543,7 +556,11 @@ def main():
         flush.zero_()
         s.record(stream)
         tube.set_potential(Uh, Uc)
-        Qh = compute_charge([tube], stream=stream)
+        if dist is None:
+            Qh = compute_charge([tube], stream=stream)  # host Q through the C-ABI
+        else:
+            charge_pass(Q)
+            Qh = Q.cpu().numpy()
         e.record(stream)
         e2e_ev.append((s, e))
     barrier()
@@ -551,11 +568,12 @@ def main():
     e2e_all = torch.tensor([e2e_local], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(e2e_all, op=dist.ReduceOp.MAX)
-    e2e_value = updates * world * args.steps / (float(e2e_all.item()) * 1e-3)
+    e2e_value = updates * args.steps / (float(e2e_all.item()) * 1e-3)
     assert np.all(np.isfinite(Qh))
 
-    # ---- the same workload in the mixed path (FP32 contour recursions, FP64 elsewhere)
+    # ---- the same workload in the mixed path
     mixed = None
+    Q_mixed = None
     if args.precision == "fp64" and world == 1:
         tm = CNT(**tube_kwargs("mixed"))
         tm.set_potential(U, Uc)
@@ -574,11 +592,12 @@ def main():
         torch.cuda.synchronize()
         sm = last_stats()
         mms = float(np.mean([a.elapsed_time(b) for a, b in mev]))
+        Q_mixed = Qm.cpu().numpy()
         mixed = {"ms_per_pass": mms, "updates_per_s": sm["updates"] / (mms * 1e-3),
+                 "speedup_vs_fp64": (t_max / args.steps) / mms,
                  "updates_fp32": sm["updates_fp32"], "updates": sm["updates"],
-                 "rule": "contour chains at least 1e-3 eV above the real axis in FP32 (Kahan FP64 sums); "
-                         "real-axis chains, leads and Rho0 in FP64",
-                 "max_rel_vs_fp64": float((Qm - Q).abs().max() / Q.abs().max())}
+                 "rule": MIXED_RULE,
+                 "max_rel_vs_fp64": float(np.max(np.abs(Q_mixed - Q_dev)) / np.max(np.abs(Q_dev)))}
 
     # ---- roofline of the dominant kernel (the RGF sweep kernel)
     flops = st["contour_updates"] * FLOP_CONTOUR + st["realaxis_updates"] * FLOP_REALAXIS
@@ -594,6 +613,7 @@ def main():
     line = None
     if rank == 0:
         cpu = None
+        parity = None
         if not args.no_cpu_baseline and world == 1:
             from oracle import oracle as O
             O.build()
@@ -615,11 +635,23 @@ def main():
                              f"{threads} threads over energies; {dt:.2f} s",
                    "single_thread": {"value": n1 / dt1, "unit": "updates/s", "cores": 1,
                                      "sample": f"energies 0 and 2048 (1 contour + 1 real-axis), 1 thread; {dt1:.2f} s"}}
+            # the oracle as the checker: the whole workload (all 4096 energies, O(N) sweeps), outside the timing
+            t2 = time.perf_counter()
+            Qo = ot.charge(nthreads=threads)
+            dto = time.perf_counter() - t2
+            qmax = float(np.max(np.abs(Qo)))
+            parity = {"oracle": f"FP64 CPU restatement, whole config-2 pass, {threads} threads, {dto:.1f} s",
+                      "fp64_max_rel_vs_oracle": float(np.max(np.abs(Q_dev - Qo)) / qmax),
+                      "e2e_max_rel_vs_oracle": float(np.max(np.abs(Qh - Qo)) / qmax),
+                      "bars": {"fp64": 1e-8, "mixed": 1e-5}}
+            if Q_mixed is not None:
+                parity["mixed_max_rel_vs_oracle"] = float(np.max(np.abs(Q_mixed - Qo)) / qmax)
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
         cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch, small=args.small)
         longt = None if (args.no_long_tube or world > 1) else long_tube_measure(torch)
         cfg5 = config5_measure(torch) if (args.config5 and world == 1) else None
+        clk.__exit__()
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                 "frac": achieved_tf / peak_tf if peak_tf else None,
                 "traffic": prof.get("dram_bytes_per_launch"),
@@ -629,23 +661,32 @@ def main():
                                    f"{FLOP_CONTOUR}/contour update, {FLOP_REALAXIS}/real-axis update",
                 "hbm": {"scratch_bytes_per_launch": st["checkpoint_bytes"], "achieved_gbs": scratch_gbs,
                         "peak_gbs": hbm_peak, "frac": scratch_gbs / hbm_peak}}
+        clocks = clk.summary()
+        clocks["window"] = "whole GPU phase of the run (warm-up through the last measurement)"
+        clocks["timed_region"] = clk.summary(clk_lo, clk_hi)
         line = {"metric": "site*energy RGF updates/s", "value": value, "unit": "updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded potential; no dataset)",
                 "config": {"workload": WORKLOAD, "precision": args.precision, "updates_per_pass": updates,
-                           "updates_fp32": st["updates_fp32"], "parallelism": f"{world} independent tubes",
+                           "updates_fp32": st["updates_fp32"],
+                           "parallelism": ("one tube on one GPU" if world == 1 else
+                                           f"energy shards of one tube over {world} GPUs, one NCCL all-reduce of "
+                                           f"{N} doubles per pass"),
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu, "scf": scf, "mixed": mixed, "config3": cfg3, "config4": cfg4,
-                "long_tube": longt, "config5": cfg5,
+                "roofline": roof, "cpu_baseline": cpu, "parity": parity, "scf": scf, "mixed": mixed,
+                "config3": cfg3, "config4": cfg4, "long_tube": longt, "config5": cfg5,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,
-                        "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)"},
-                "gpu_launches": int(st["kernel_launches"]) * args.steps, "clocks": clk.summary(clk_lo, clk_hi),
+                        "path": "negf_tube_set_potential (host U) + negf_compute_charge (host Q)" if world == 1 else
+                                "negf_tube_set_potential (host U) + negf_compute_charge + NCCL all-reduce + D2H of Q"},
+                "gpu_launches": int(st["kernel_launches"]) * args.steps, "clocks": clocks,
                 "kernel_ms_per_pass": {"rgf": k_ms, "rgf_pass1": float(np.mean(p1_ms)),
                                        "rgf_pass2": float(np.mean(p2_ms)), "reduce": float(np.mean(red_ms))}}
         print(json.dumps(line), flush=True)
+    else:
+        clk.__exit__()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -14,6 +14,8 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -173,6 +175,7 @@ struct negf_tube {
     std::vector<Pt> eq_pts, noneq_pts, rho0_pts;
     std::vector<cplx> poles;
     int version = 0;
+    long long serial = 0;  // unique per tube of the process (keys the cached launch tables)
     int shard_rank = 0, shard_world = 1;
     // adaptive non-equilibrium limits (NEGF_Common.H:453-457)
     double E_at_max_noneq_integrand = 0.0;
@@ -211,25 +214,95 @@ struct negf_charge_plan {
 namespace {
 
 std::mutex g_mu;
+
+// Device buffers and the cached launch table of the charge calls made on one
+// (device, stream) pair.  Calls on the same stream are ordered by the stream;
+// calls on different streams or devices get different workspaces, so their
+// kernels never share scratch.  A workspace is reused only after the last
+// kernel of its previous call (event `done`), which also orders a stream
+// handle that the runtime hands out again after the caller destroyed the
+// stream it first named.
 struct Workspace {
+    int device = 0;
+    cudaStream_t stream = nullptr;
     DevBuf tubes, chains, warps, rts, units, partial, scratch, qbuf, pieces;
+    // real-space pass (negf_rs_compute_charge)
+    DevBuf rsE, rsFlags, rsU0, rsUa, rsCorners, rsGL, rsRows, rsStatus;
     // cached chain table
-    std::vector<const negf_tube*> key_tubes;
+    std::vector<long long> key_serials;
     std::vector<int> key_versions;
-    std::vector<int> key_shard;
     ChainTable table;
     bool table_valid = false;
-    // stats / timing
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // timing of the last call
+    cudaEvent_t done = nullptr;                                 // end of the last call's kernels
+    bool used = false;
+    ~Workspace() {
+        // buffers belong to `device`; free them with it current
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && cur != device) cudaSetDevice(device);
+        for (cudaEvent_t& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (done) cudaEventDestroy(done);
+        DevBuf* bufs[] = {&tubes, &chains, &warps,  &rts,   &units,  &partial,   &scratch, &qbuf,
+                          &pieces, &rsE,  &rsFlags, &rsU0, &rsUa, &rsCorners, &rsGL,    &rsRows, &rsStatus};
+        for (DevBuf* b : bufs) {
+            if (b->p) cudaFree(b->p);
+            b->p = nullptr;
+        }
+        if (cur >= 0 && cur != device) cudaSetDevice(cur);
+    }
+};
+
+// Process-wide settings and the statistics of the last charge call.
+struct Settings {
     bool timing = false;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    negf_stats stats{};
-    bool stats_pending = false;
     int warps_per_block = 4;
     int pass1_pieces = 0;  // 0: automatic
+    negf_stats stats{};
+    Workspace* stats_ws = nullptr;  // workspace whose events time the last call (when timing)
 };
-Workspace& ws() {
-    static Workspace w;
-    return w;
+Settings& settings() {
+    static Settings s;
+    return s;
+}
+
+struct WsKey {
+    int device;
+    cudaStream_t stream;
+    bool operator<(const WsKey& o) const {
+        return device != o.device ? device < o.device : std::less<cudaStream_t>()(stream, o.stream);
+    }
+};
+
+// Workspace of the current device and `stream` (callers hold g_mu); waits on
+// the stream for the previous call that used it.
+int get_workspace(cudaStream_t stream, Workspace** out) {
+    static std::map<WsKey, std::unique_ptr<Workspace>> all;
+    int dev = 0;
+    NEGF_CUDA(cudaGetDevice(&dev));
+    std::unique_ptr<Workspace>& w = all[WsKey{dev, stream}];
+    if (!w) {
+        w.reset(new Workspace());
+        w->device = dev;
+        w->stream = stream;
+        NEGF_CUDA(cudaEventCreateWithFlags(&w->done, cudaEventDisableTiming));
+    }
+    if (w->used) NEGF_CUDA(cudaStreamWaitEvent(stream, w->done, 0));
+    *out = w.get();
+    return NEGF_OK;
+}
+
+// Every tube of a batch must live on the current device (its buffers were
+// allocated there by negf_tube_create).
+int check_batch_device(negf_tube* const* tubes, int num_tubes) {
+    int dev = 0;
+    NEGF_CUDA(cudaGetDevice(&dev));
+    for (int i = 0; i < num_tubes; ++i)
+        if (tubes[i] && tubes[i]->device != dev)
+            return fail(NEGF_ERR_ARG, "tube " + std::to_string(i) + " lives on device " +
+                                          std::to_string(tubes[i]->device) + " but device " + std::to_string(dev) +
+                                          " is current: every tube of a call must be on the current device");
+    return NEGF_OK;
 }
 
 int require_device() {
@@ -479,6 +552,24 @@ Item pass_item(const negf_tube& t, bool rho0_pass, int idx) {
             negf::kRealAxis};
 }
 
+// Whether Re E lies within `band` of a band edge of mode m in either lead.
+// A lead of mode m is the chain with alternating hoppings beta_m and gamma at
+// the contact potential U_c, whose bands are |E - U_c| in
+// [| |beta_m| - gamma |, |beta_m| + gamma]; at the edges the surface Green's
+// function has its square-root singularity and the group velocity vanishes,
+// so mixed mode keeps real-axis chains there in FP64 (contour chains sit at
+// least the band above the axis, hence at least that far from every edge).
+// The contact potentials are the host values of the last
+// negf_tube_set_potential[_device] (for a charge plan: at its creation).
+bool near_lead_band_edge(const negf_tube& t, int m, cplx E, double band) {
+    const double b = std::fabs(t.beta[m]), g = std::fabs(t.d.gamma);
+    const double edges[4] = {std::fabs(b - g), b + g, -std::fabs(b - g), -(b + g)};
+    for (int c = 0; c < 2; ++c)
+        for (double e : edges)
+            if (std::fabs(E.real() - t.Uc[c] - e) < band) return true;
+    return false;
+}
+
 // Chains of one tube, grouped by (kind, precision) with each group padded
 // to whole warps (padding lanes: mode -1, zero coefficients).
 void build_tube_chains(Out<negf::ChainRec>& chains, Out<negf::WarpRec>& warps, TableCounts& cnt, const TubePass& tp) {
@@ -500,9 +591,13 @@ void build_tube_chains(Out<negf::ChainRec>& chains, Out<negf::WarpRec>& warps, T
                 // axis; real-axis chains (running products over the whole tube) stay FP64
                 // unless mixed_realaxis_fp32 admits those at least `band` above it too
                 const bool kind_ok = it.kind == negf::kContour || t.d.mixed_realaxis_fp32;
-                const int want32 = mixed && kind_ok && std::fabs(it.E.imag()) >= band ? 1 : 0;
-                if (want32 != fp32) continue;
+                const bool axis_ok = mixed && kind_ok && std::fabs(it.E.imag()) >= band;
+                if (!axis_ok && fp32) continue;
                 for (int m = 0; m < M; ++m) {
+                    // real-axis chains also not within `band` of a band edge of the mode's leads
+                    const bool edge = it.kind == negf::kRealAxis && near_lead_band_edge(t, m, it.E, band);
+                    const int want32 = axis_ok && !edge ? 1 : 0;
+                    if (want32 != fp32) continue;
                     negf::ChainRec c{};
                     c.Er = it.E.real();
                     c.Ei = it.E.imag();
@@ -618,9 +713,9 @@ void build_table(ChainTable& ct, const std::vector<TubePass>& passes) {
     ct.max_N = cnt.max_N;
 }
 
-int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<negf::TubeDev>& tdev, bool rebuild,
-                      double* d_Q, cudaStream_t stream) {
-    Workspace& W = ws();
+int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const std::vector<negf::TubeDev>& tdev,
+                      bool rebuild, double* d_Q, cudaStream_t stream) {
+    Settings& G = settings();
     ChainTable& ct = W.table;
     if (rebuild) {
         build_table(ct, passes);
@@ -649,7 +744,7 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
     NEGF_CUDA(cudaMemcpyAsync(W.tubes.p, tdev.data(), tdev.size() * sizeof(negf::TubeDev), cudaMemcpyHostToDevice,
                               stream));
     const int nw = (int)ct.warps.size();
-    if (W.timing) {
+    if (G.timing) {
         for (auto& e : W.ev)
             if (!e) NEGF_CUDA(cudaEventCreate(&e));
         NEGF_CUDA(cudaEventRecord(W.ev[0], stream));
@@ -657,7 +752,7 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
     // parallel in length when the chains alone cannot fill the GPU: about 8
     // one-warp blocks per SM, pieces of >= 32 segments, at most 128 pieces
     // (the prefix over the pieces is sequential per chain)
-    int pieces = W.pass1_pieces;
+    int pieces = G.pass1_pieces;
     if (pieces == 0) {
         const int target = 8 * device_sm_count();
         const int maxp = std::min(128, std::max(1, ((ct.max_N + negf::kSeg - 1) / negf::kSeg) / 32));
@@ -667,13 +762,15 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
     if (pieces > 1) NEGF_CUDA(W.pieces.reserve(sizeof(double) * (size_t)nw * pieces * 24 * negf::kWarp));
     NEGF_CUDA(negf::launch_rgf(W.tubes.as<negf::TubeDev>(), W.chains.as<negf::ChainRec>(), W.warps.as<negf::WarpRec>(),
                                nw, W.units.as<negf::SegUnit>(), (int)ct.units.size(), W.partial.as<double>(),
-                               W.scratch.p, W.warps_per_block, stream, W.timing ? W.ev[3] : nullptr, nullptr, pieces,
+                               W.scratch.p, G.warps_per_block, stream, G.timing ? W.ev[3] : nullptr, nullptr, pieces,
                                W.pieces.as<double>()));
-    if (W.timing) NEGF_CUDA(cudaEventRecord(W.ev[1], stream));
+    if (G.timing) NEGF_CUDA(cudaEventRecord(W.ev[1], stream));
     NEGF_CUDA(negf::launch_reduce(W.rts.as<negf::ReduceTube>(), (int)ct.rts.size(), ct.max_N, W.partial.as<double>(),
                                   d_Q, stream));
-    if (W.timing) NEGF_CUDA(cudaEventRecord(W.ev[2], stream));
-    negf_stats& st = W.stats;
+    if (G.timing) NEGF_CUDA(cudaEventRecord(W.ev[2], stream));
+    NEGF_CUDA(cudaEventRecord(W.done, stream));
+    W.used = true;
+    negf_stats& st = G.stats;
     st = negf_stats{};
     st.updates = ct.updates;
     st.updates_fp32 = ct.updates_fp32;
@@ -685,7 +782,7 @@ int upload_and_launch(const std::vector<TubePass>& passes, const std::vector<neg
     st.pieces = pieces;
     st.units = (int)ct.units.size();
     st.checkpoint_bytes = 2 * ct.scratch_doubles * 8;
-    W.stats_pending = W.timing;
+    G.stats_ws = G.timing ? &W : nullptr;
     return NEGF_OK;
 }
 
@@ -707,16 +804,25 @@ negf::TubeDev make_tubedev(const negf_tube& t, bool rho0_pass) {
     return d;
 }
 
+// Contact potentials; in mixed precision the chain table depends on them
+// (the band-edge rule), so a change marks it for rebuilding.
+void set_contacts(negf_tube& t, const double Uc[2]) {
+    if (t.d.precision == NEGF_PREC_MIXED && (t.Uc[0] != Uc[0] || t.Uc[1] != Uc[1])) t.version++;
+    t.Uc[0] = Uc[0];
+    t.Uc[1] = Uc[1];
+}
+
 int compute_rho0(negf_tube* t) {
-    Workspace& W = ws();
+    Workspace* W = nullptr;
+    if (int rc = get_workspace(nullptr, &W)) return rc;
     rho0_paths(*t);
     std::vector<TubePass> passes{{t, 0, 0, true}};
     std::vector<negf::TubeDev> tdev{make_tubedev(*t, true)};
-    W.table_valid = false;
-    int rc = upload_and_launch(passes, tdev, true, t->d_rho0, 0);
-    W.table_valid = false;
+    W->table_valid = false;
+    int rc = upload_and_launch(*W, passes, tdev, true, t->d_rho0, nullptr);
+    W->table_valid = false;
     if (rc != NEGF_OK) return rc;
-    NEGF_CUDA(cudaStreamSynchronize(0));
+    NEGF_CUDA(cudaStreamSynchronize(nullptr));
     return NEGF_OK;
 }
 
@@ -907,9 +1013,14 @@ int report(int code, const char* msg) { return fail(code, msg); }
 // Plans one charge launch into caller-provided fixed arrays (no allocation).
 // Requires every tube's energy paths to be current (they are rebuilt by
 // negf_tube_create / negf_tube_set_contact_mu).
+std::unique_lock<std::mutex> api_lock() { return std::unique_lock<std::mutex>(g_mu); }
+
 int plan_charge_fixed(negf_tube* const* tubes, int num_tubes, FixedPlan& fp) {
     constexpr int kMaxPlanTubes = 64;
     if (!tubes || num_tubes <= 0) return fail(NEGF_ERR_ARG, "null or empty tube batch");
+    for (int i = 0; i < num_tubes; ++i)
+        if (!tubes[i]) return fail(NEGF_ERR_ARG, "null tube in batch");
+    if (int rc = check_batch_device(tubes, num_tubes)) return rc;
     if (num_tubes > kMaxPlanTubes || num_tubes > fp.tube_cap)
         return fail(NEGF_ERR_ARG, "too many tubes for the allocation-free entry point (max " +
                                       std::to_string(std::min(kMaxPlanTubes, fp.tube_cap)) + ")");
@@ -918,7 +1029,6 @@ int plan_charge_fixed(negf_tube* const* tubes, int num_tubes, FixedPlan& fp) {
     long long off = 0;
     for (int i = 0; i < num_tubes; ++i) {
         const negf_tube* t = tubes[i];
-        if (!t) return fail(NEGF_ERR_ARG, "null tube in batch");
         if (t->limits_dirty) return fail(NEGF_ERR_STATE, "tube energy paths are not current");
         passes[i] = {t, i, off, false};
         fp.tubes[i] = make_tubedev(*t, false);
@@ -1011,6 +1121,10 @@ int negf_tube_create(const negf_tube_desc* d, negf_tube** out) {
     rc = setup_material(*t);
     if (rc) return rc;
     cudaGetDevice(&t->device);
+    {
+        static std::atomic<long long> next_serial{1};
+        t->serial = next_serial++;
+    }
     t->mu[0] = d->contact_mu[0];
     t->mu[1] = d->contact_mu[1];
     // zero padding on both sides lets the kernels load whole segments of U
@@ -1037,8 +1151,7 @@ int negf_tube_create(const negf_tube_desc* d, negf_tube** out) {
 int negf_tube_destroy(negf_tube* t) {
     if (t) {
         std::lock_guard<std::mutex> lk(g_mu);
-        ws().table_valid = false;
-        delete t;
+        delete t;  // cached launch tables are keyed by tube serials, never reused
     }
     return NEGF_OK;
 }
@@ -1074,8 +1187,7 @@ int negf_tube_set_potential(negf_tube* t, const double* U, int n, const double U
         if (!std::isfinite(U[i])) return fail(NEGF_ERR_NUMERIC, "non-finite potential at site " + std::to_string(i));
     if (!std::isfinite(Uc[0]) || !std::isfinite(Uc[1])) return fail(NEGF_ERR_NUMERIC, "non-finite contact potential");
     NEGF_CUDA(cudaMemcpy(t->d_U, U, sizeof(double) * n, cudaMemcpyHostToDevice));
-    t->Uc[0] = Uc[0];
-    t->Uc[1] = Uc[1];
+    set_contacts(*t, Uc);
     return NEGF_OK;
 }
 
@@ -1085,8 +1197,7 @@ int negf_tube_set_potential_device(negf_tube* t, const double* dU, int n, const 
     if (!std::isfinite(Uc[0]) || !std::isfinite(Uc[1])) return fail(NEGF_ERR_NUMERIC, "non-finite contact potential");
     if (dU != t->d_U)
         NEGF_CUDA(cudaMemcpyAsync(t->d_U, dU, sizeof(double) * n, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
-    t->Uc[0] = Uc[0];
-    t->Uc[1] = Uc[1];
+    set_contacts(*t, Uc);
     return NEGF_OK;
 }
 
@@ -1180,36 +1291,44 @@ int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q
     if (!tubes || num_tubes <= 0 || !Q) return fail(NEGF_ERR_ARG, "null argument");
     cudaStream_t s = (cudaStream_t)stream;
     std::lock_guard<std::mutex> lk(g_mu);
-    Workspace& W = ws();
+    for (int i = 0; i < num_tubes; ++i)
+        if (!tubes[i]) return fail(NEGF_ERR_ARG, "null tube in batch");
+    if (int rc = check_batch_device(tubes, num_tubes)) return rc;
+    Workspace* Wp = nullptr;
+    if (int rc = get_workspace(s, &Wp)) return rc;
+    Workspace& W = *Wp;
     std::vector<TubePass> passes;
     std::vector<negf::TubeDev> tdev;
     long long off = 0;
-    bool same = W.table_valid && W.key_tubes.size() == (size_t)num_tubes;
+    bool same = W.table_valid && W.key_serials.size() == (size_t)num_tubes;
     for (int i = 0; i < num_tubes; ++i) {
         negf_tube* t = tubes[i];
-        if (!t) return fail(NEGF_ERR_ARG, "null tube in batch");
         update_paths(*t);
         passes.push_back({t, i, off, false});
         tdev.push_back(make_tubedev(*t, false));
         off += t->N;
-        if (same && (W.key_tubes[i] != t || W.key_versions[i] != t->version)) same = false;
+        if (same && (W.key_serials[i] != t->serial || W.key_versions[i] != t->version)) same = false;
     }
     double* dQ = Q;
     if (!q_on_device) {
         NEGF_CUDA(W.qbuf.reserve(sizeof(double) * off));
         dQ = W.qbuf.as<double>();
     }
-    int rc = upload_and_launch(passes, tdev, !same, dQ, s);
+    int rc = upload_and_launch(W, passes, tdev, !same, dQ, s);
     if (rc) {
         W.table_valid = false;
         return rc;
     }
-    W.key_tubes.assign(tubes, tubes + num_tubes);
+    W.key_serials.clear();
     W.key_versions.clear();
-    for (int i = 0; i < num_tubes; ++i) W.key_versions.push_back(tubes[i]->version);
+    for (int i = 0; i < num_tubes; ++i) {
+        W.key_serials.push_back(tubes[i]->serial);
+        W.key_versions.push_back(tubes[i]->version);
+    }
     W.table_valid = true;
     if (!q_on_device) {
         NEGF_CUDA(cudaMemcpyAsync(Q, dQ, sizeof(double) * off, cudaMemcpyDeviceToHost, s));
+        NEGF_CUDA(cudaEventRecord(W.done, s));  // the next call may rewrite qbuf only after this copy
         NEGF_CUDA(cudaStreamSynchronize(s));
     }
     return NEGF_OK;
@@ -1293,15 +1412,17 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(g_mu);
     std::unique_ptr<negf_charge_plan> p(new negf_charge_plan());
-    for (int i = 0; i < num_tubes; ++i) {
+    for (int i = 0; i < num_tubes; ++i)
         if (!tubes[i]) return fail(NEGF_ERR_ARG, "null tube in batch");
+    if (int rc2 = check_batch_device(tubes, num_tubes)) return rc2;
+    for (int i = 0; i < num_tubes; ++i) {
         update_paths(*tubes[i]);
         p->tubes.push_back(tubes[i]);
         p->versions.push_back(tubes[i]->version);
     }
     p->d_Q = d_Q;
     p->force_fp64 = (flags & NEGF_PLAN_FP64) != 0;
-    p->wpb = ws().warps_per_block;
+    p->wpb = settings().warps_per_block;
     rc = plan_tables(*p, negf::kSegsPerUnit, true);
     if (rc) return rc;
     if (flags & NEGF_PLAN_AUTOTUNE) {
@@ -1377,15 +1498,15 @@ int negf_charge_plan_destroy(negf_charge_plan* p) {
 
 int negf_set_tuning(int key, int value) {
     std::lock_guard<std::mutex> lk(g_mu);
-    Workspace& W = ws();
+    Settings& G = settings();
     switch (key) {
         case NEGF_TUNE_PASS2_WARPS_PER_BLOCK:
             if (value != 1 && value != 2 && value != 4) return fail(NEGF_ERR_ARG, "warps per block must be 1, 2 or 4");
-            W.warps_per_block = value;
+            G.warps_per_block = value;
             return NEGF_OK;
         case NEGF_TUNE_PASS1_PIECES:
             if (value < 0 || value > 4096) return fail(NEGF_ERR_ARG, "pieces must be in [0, 4096] (0: automatic)");
-            W.pass1_pieces = value;
+            G.pass1_pieces = value;
             return NEGF_OK;
         default:
             return fail(NEGF_ERR_ARG, "unknown tuning key");
@@ -1394,27 +1515,27 @@ int negf_set_tuning(int key, int value) {
 
 int negf_set_timing(int enable) {
     std::lock_guard<std::mutex> lk(g_mu);
-    ws().timing = enable != 0;
+    settings().timing = enable != 0;
     return NEGF_OK;
 }
 
 int negf_last_stats(negf_stats* s) {
     if (!s) return fail(NEGF_ERR_ARG, "null argument");
     std::lock_guard<std::mutex> lk(g_mu);
-    Workspace& W = ws();
-    if (W.stats_pending) {
-        NEGF_CUDA(cudaEventSynchronize(W.ev[2]));
+    Settings& G = settings();
+    if (Workspace* W = G.stats_ws) {
+        NEGF_CUDA(cudaEventSynchronize(W->ev[2]));
         float a = 0, b = 0, p1 = 0;
-        NEGF_CUDA(cudaEventElapsedTime(&a, W.ev[0], W.ev[1]));
-        NEGF_CUDA(cudaEventElapsedTime(&b, W.ev[1], W.ev[2]));
-        NEGF_CUDA(cudaEventElapsedTime(&p1, W.ev[0], W.ev[3]));
-        W.stats.rgf_kernel_ms = a;
-        W.stats.pass1_kernel_ms = p1;
-        W.stats.pass2_kernel_ms = a - p1;
-        W.stats.reduce_kernel_ms = b;
-        W.stats_pending = false;
+        NEGF_CUDA(cudaEventElapsedTime(&a, W->ev[0], W->ev[1]));
+        NEGF_CUDA(cudaEventElapsedTime(&b, W->ev[1], W->ev[2]));
+        NEGF_CUDA(cudaEventElapsedTime(&p1, W->ev[0], W->ev[3]));
+        G.stats.rgf_kernel_ms = a;
+        G.stats.pass1_kernel_ms = p1;
+        G.stats.pass2_kernel_ms = a - p1;
+        G.stats.reduce_kernel_ms = b;
+        G.stats_ws = nullptr;
     }
-    *s = W.stats;
+    *s = G.stats;
     return NEGF_OK;
 }
 
@@ -1701,8 +1822,12 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     const int P = (int)all.size(), P0 = (int)e0.size();
     const size_t mm = (size_t)m * m;
     const size_t pe = (size_t)std::max(std::max(P, P0), 1);
-    // grow-only buffers kept across calls (serialised by g_mu)
-    static DevBuf bE, bFlags, bU0, bUa, bCorners, bGL, bRows, bStatus;
+    // grow-only buffers of this (device, stream) kept across calls
+    if (int rc = check_batch_device(&t, 1)) return rc;
+    Workspace* Wp = nullptr;
+    if (int rc = get_workspace(s, &Wp)) return rc;
+    DevBuf &bE = Wp->rsE, &bFlags = Wp->rsFlags, &bU0 = Wp->rsU0, &bUa = Wp->rsUa, &bCorners = Wp->rsCorners,
+           &bGL = Wp->rsGL, &bRows = Wp->rsRows, &bStatus = Wp->rsStatus;
     NEGF_CUDA(bE.reserve(sizeof(double) * 4 * pe));
     NEGF_CUDA(bFlags.reserve(sizeof(int) * pe));
     NEGF_CUDA(bUa.reserve(sizeof(double) * (size_t)N * m));
@@ -1754,6 +1879,8 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
                                      bRows.as<double>(), d_Q, t->d_rs_rho0, bStatus.as<int>(), s));
     int status = 0;
     NEGF_CUDA(cudaMemcpyAsync(&status, bStatus.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    NEGF_CUDA(cudaEventRecord(Wp->done, s));
+    Wp->used = true;
     NEGF_CUDA(cudaStreamSynchronize(s));
     if (status) return fail(NEGF_ERR_NUMERIC, "zero pivot in a real-space block inversion");
     return NEGF_OK;

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 namespace negf {
 
@@ -155,6 +156,11 @@ struct FixedPlan {
 }  // namespace negf
 struct negf_tube;
 namespace negf {
+// Lock of the host layer: held by every entry point that reads or writes tube
+// state or shared host tables.
+std::unique_lock<std::mutex> api_lock();
+// Callers hold api_lock().  Fails with NEGF_ERR_ARG when a tube is not on the
+// current device or the tables overflow the fixed arrays.
 int plan_charge_fixed(negf_tube* const* tubes, int num_tubes, FixedPlan& fp);
 int report(int code, const char* msg);  // sets negf_last_error, returns code
 

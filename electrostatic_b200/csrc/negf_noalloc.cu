@@ -1,11 +1,10 @@
 // Allocation-free induced-charge entry point.
 //
 // Some callers cannot allocate device memory at the point where they need
-// the charge: code running while a stream is being captured into a CUDA
-// graph, applications whose memory is handed out by their own pool and
-// forbid the runtime allocator, or drop-in plugins that must not grow the
-// footprint of the host program between its own allocations.  For them,
-// negf_compute_charge_noalloc() runs the same RGF kernels as
+// the charge: applications whose device memory is handed out by their own
+// pool and that forbid the runtime allocator, or drop-in plugins that must not
+// grow the footprint of the host program between its own allocations.  For
+// them, negf_compute_charge_noalloc() runs the same RGF kernels as
 // negf_compute_charge(), but every buffer of a call -- the launch tables,
 // the per-warp partial rows and the segment checkpoints -- lives in one
 // file-scope device array of kScratchBytes (32 MiB).  Every GPU that loads
@@ -15,6 +14,7 @@
 //   * the charge output is a device pointer supplied by the caller;
 //   * problems whose tables and scratch exceed the array are rejected with
 //     NEGF_ERR_ARG and a message giving the bytes needed;
+//   * every tube of a call must live on the current device (NEGF_ERR_ARG);
 //   * the first call on a device looks up the array's device address (a
 //     set-up step); make that first call before any stream capture;
 //   * all calls share the array, so calls whose work overlaps on the GPU
@@ -80,6 +80,10 @@ int scratch_address(unsigned char** out) {
 extern "C" int negf_compute_charge_noalloc(negf_tube* const* tubes, int num_tubes, double* d_Q, void* stream) {
     using namespace negf;
     if (!d_Q) return report(NEGF_ERR_ARG, "null charge output (a device pointer is required)");
+    // the host tables below are shared: planning and their upload run under
+    // the host layer's lock (a pageable-memory copy has consumed its source
+    // when cudaMemcpyAsync returns)
+    std::unique_lock<std::mutex> lk = api_lock();
     FixedPlan fp{};
     fp.tubes = h_tubes;
     fp.rts = h_rts;

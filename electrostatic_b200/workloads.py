@@ -65,6 +65,27 @@ def uneven_batch(num_tubes=16, precision="mixed", vds=0.4, seed=SEED_BASE + 4, s
 GATE_SWEEP = [round(0.05 * i, 2) for i in range(13)]  # 0 -> 0.6 V
 
 
+def config2_kwargs(precision="fp64", small=False):
+    """Batched mode-space benchmark tube (config id 2): (17,0), 1000 unit
+    cells (N = 4000), 8 modes, 1024 equilibrium-contour points (256 + 256
+    line, 512 arc) + 3072 real-axis points uniform on [-1.5, 1.5] eV with
+    eta = 1e-4 eV, contacts mu = (0, -0.5) eV at 300 K.  small: a quarter of
+    the energies (the profiling case)."""
+    eq, rt = ((64, 64, 128), 768) if small else ((256, 256, 512), 3072)
+    return dict(type_id=(17, 0), num_unitcells=1000, num_modes=8, contact_mu=(0.0, -0.5), contact_T=(300.0, 300.0),
+                eq_integration_pts=eq, E_zPlus_imag=1e-4, realaxis_window=(-1.5, 1.5, rt, 0), precision=precision)
+
+
+def config3_kwargs(precision="fp64", small=False):
+    """Real-space benchmark tube (config id 3): (13,0), 300 unit cells = 600
+    ring blocks of 26 atoms, 2048 equilibrium-contour points (512 + 512
+    line, 1024 arc) plus the Matsubara poles up to 3 eV, mu = -0.8 eV at
+    300 K.  small: 200 blocks and 256 contour points (the profiling case)."""
+    return dict(type_id=(13, 0), num_unitcells=100 if small else 300, num_modes=7, contact_mu=(-0.8, -0.8),
+                contact_T=(300.0, 300.0), eq_integration_pts=(64, 64, 128) if small else (512, 512, 1024),
+                E_pole_max=3.0, E_zPlus_imag=1e-6, precision=precision)
+
+
 def gate_with_contacts(y_nm, r_tube, vds=0.4, gate_gap=1.5e-9, contact_nm=5.0):
     """Gate-all-around stand-in of a batch tube: gate radius r_tube + 1.5 nm,
     source (0 V) and drain (Vds) electrodes over the first and last

@@ -14,6 +14,11 @@
  *     as documented per argument; sizes are element counts.
  *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
  *   - one handle is not thread-safe; distinct handles are independent.
+ *     Charge calls keep their device scratch per (device, stream): calls
+ *     on different streams or devices never share scratch, and calls on one
+ *     stream reuse it in stream order.  Each stream's scratch is held until
+ *     the process exits (it grows to the largest problem seen on it).
+ *   - every tube of a call must live on the current device (NEGF_ERR_ARG).
  *   - reductions are deterministic: the same inputs give bitwise-identical
  *     charge on the same GPU and launch configuration.
  *   - the library has no CPU fallback: every compute call needs a CUDA
@@ -155,16 +160,20 @@ int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q
 
 /* Allocation-free variant of negf_compute_charge -- no counterpart in the
  * reference.  For callers that cannot allocate device memory when they need
- * the charge (work recorded while a stream is captured, applications whose
- * device memory comes from their own pool, plugins that must not grow the
- * host program's footprint).  It runs the same kernels, but keeps the launch
+ * the charge: applications whose device memory comes from their own pool
+ * and that forbid the runtime allocator, and plugins that must not grow the
+ * host program's footprint.  It runs the same kernels, but keeps the launch
  * tables, partial rows and checkpoints in one static device array of 32 MiB
  * that every GPU loading this library holds until exit; it calls no
  * cudaMalloc/cudaFree.  d_Q is a device pointer.  Problems that need more
- * than 32 MiB of scratch are rejected with NEGF_ERR_ARG.  The first call on
- * a device looks up the array's address (set-up), so make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller. */
+ * than 32 MiB of scratch, or more than 64 tubes, are rejected with
+ * NEGF_ERR_ARG, as are tubes that do not live on the current device.
+ * NEGF_ERR_STATE marks a tube whose energy paths are stale; the public calls
+ * that change paths (negf_tube_set_contact_mu,
+ * negf_tube_correct_integration_limits) rebuild them before returning.  The
+ * first call on a device looks up the array's address (set-up), so make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
 int negf_compute_charge_noalloc(negf_tube* const* tubes, int num_tubes, double* d_Q, void* stream);
 
 /* Per-call timing and work counters of the last negf_compute_charge

@@ -3,8 +3,10 @@
 The reference ships three standalone RGF programs whose outputs are committed
 in its tree.  This script copies the numeric tables (data only, no source)
 into ``tests/golden/`` so that the tests can run where the reference tree is
-absent.  It reads the reference checkout given by ``--ref`` (default: the
-read-only mount used when this repository was built).
+absent.  It reads the reference checkout given by ``--ref`` or, failing that,
+by the ELEQTRONEX_REFERENCE environment variable; there is no default path.
+
+    python tests/golden/make_golden.py --ref <path of the reference checkout>
 
   decimation_technique/Exec/output/{Sigma,DOS,Transmission}
       N=4, 10 energies on [-6, 0] + 1e-8 i, beta = 2*2.5*cos(6 pi/17),
@@ -31,8 +33,11 @@ DOS_COMPARE = ("scripts/negf_python/DOS_Compare/cpp_results/gpu", ["LDOS.dat", "
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("ELEQTRONEX_REFERENCE"),
+                    help="reference checkout (default: $ELEQTRONEX_REFERENCE)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("give the reference checkout with --ref or ELEQTRONEX_REFERENCE")
     here = os.path.dirname(os.path.abspath(__file__))
     for tag, rel in SETS.items():
         for f in FILES:

@@ -136,6 +136,38 @@ def test_mixed_precision_fp32_real_axis(oracle, cells):
     assert _rel(Qg, Qo) <= MIXED_TOL, _rel(Qg, Qo)
 
 
+def test_mixed_precision_band_edge_chains_stay_fp64(oracle):
+    """A real-axis grid point on a lead band edge of mode 0: that chain stays
+    FP64 in mixed mode (its other modes, and every chain further than the
+    1 meV band from every edge, run in FP32), and the charge stays within the
+    mixed tolerance of the FP64 oracle."""
+    from electrostatic_b200.negf import CNT, last_stats
+    base = dict(type_id=(17, 0), num_unitcells=60, num_modes=3, contact_mu=(0.05, -0.05), contact_T=(300.0, 300.0),
+                eq_integration_pts=(16, 16, 24), E_zPlus_imag=2e-3)
+    probe = CNT(**base)
+    _, _, beta = probe.modes()
+    gamma = 2.5
+    edge = abs(abs(beta[0]) - gamma)  # inner band edge of mode 0 (contact potential 0)
+    pts, half = 101, 0.075  # spacing 1.5 meV: only the centre point lies within 1 meV of the edge
+    kw = dict(base, realaxis_window=(edge - half, edge + half, pts, 0), precision="mixed", mixed_realaxis_fp32=True)
+    y = probe.site_positions()
+    U = 0.15 * np.exp(-((y - y.mean()) ** 2) / 20.0)
+    U[0] = U[-1] = 0.0
+    g, o = _pair(oracle, U=U, Uc=(0.0, 0.0), **kw)
+    Qg = g.Solve_NEGF()
+    st = last_stats()
+    E = np.linspace(edge - half, edge + half, pts)
+    edges = [e for b in beta for e in (abs(abs(b) - gamma), abs(b) + gamma, -abs(abs(b) - gamma), -(abs(b) + gamma))]
+    near = sum(1 for x in E for m, b in enumerate(beta)
+               if any(abs(x - e) < 1e-3 for e in (abs(abs(b) - gamma), abs(b) + gamma, -abs(abs(b) - gamma),
+                                                   -(abs(b) + gamma))))
+    assert near >= 1 and any(abs(E[pts // 2] - e) < 1e-12 for e in edges)
+    n_real32 = (pts * len(beta) - near) * g.num_field_sites
+    assert st["updates_fp32"] == st["contour_updates"] + n_real32, (st, near)
+    Qo = o.charge(nthreads=8)
+    assert _rel(Qg, Qo) <= MIXED_TOL, _rel(Qg, Qo)
+
+
 def test_batch_of_uneven_tubes(oracle):
     from electrostatic_b200.negf import compute_charge
     specs = [

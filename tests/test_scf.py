@@ -38,7 +38,7 @@ SMALL = dict(type_id=(17, 0), num_unitcells=10, num_modes=2, contact_mu=(-1.0, -
 
 def test_oracle_scf_converges(oracle):
     from electrostatic_b200.electrostatics import ring_coupling_matrix
-    from electrostatic_b200.scf import run_scf_oracle
+    from oracle.scf_oracle import run_scf_oracle
     t = oracle.OracleTube(**SMALL)
     K = ring_coupling_matrix(_ring_y(10), t.radius, t.radius + 1.5e-9)
     res = run_scf_oracle(t, K, [0.0, 0.2], nthreads=4)
@@ -53,7 +53,8 @@ def test_oracle_scf_converges(oracle):
 def test_device_scf_follows_oracle_scf(oracle, keep):
     from electrostatic_b200.electrostatics import GateAllAround
     from electrostatic_b200.negf import CNT
-    from electrostatic_b200.scf import run_scf, run_scf_oracle
+    from electrostatic_b200.scf import run_scf
+    from oracle.scf_oracle import run_scf_oracle
     g = CNT(**SMALL)
     y = g.site_positions()
     np.testing.assert_allclose(y, _ring_y(10), rtol=1e-12)

@@ -120,7 +120,8 @@ def _read(ptr, n):
 
 
 def test_batch_scf_graph_equals_loop_and_oracle(oracle):
-    from electrostatic_b200.scf import run_scf_batch, run_scf_batch_oracle
+    from electrostatic_b200.scf import run_scf_batch
+    from oracle.scf_oracle import run_scf_batch_oracle
     Vg = [0.0, 0.15]
     tubes, electros, oracles = _batch(oracle)
     r_graph = run_scf_batch(tubes, electros, Vg, use_graph=True, iters_per_graph=4)
