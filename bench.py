@@ -599,6 +599,31 @@ def main():
                  "rule": MIXED_RULE,
                  "max_rel_vs_fp64": float(np.max(np.abs(Q_mixed - Q_dev)) / np.max(np.abs(Q_dev)))}
 
+    # ---- both RGF schedules on the same tube (kernel time per pass, CUDA events)
+    schedules = None
+    if world == 1:
+        from electrostatic_b200.negf import SCHEDULE_FUSED, SCHEDULE_TWO_PASS, TUNE_SCHEDULE, set_tuning
+        schedules = {"chosen": {1: "two_pass", 2: "fused"}.get(st["schedule"], "?")}
+        set_timing(True)
+        try:
+            for name, v in (("fused", SCHEDULE_FUSED), ("two_pass", SCHEDULE_TWO_PASS)):
+                set_tuning(TUNE_SCHEDULE, v)
+                Qs = torch.zeros_like(Q)
+                for _ in range(3):
+                    compute_charge([tube], out=Qs, stream=stream)
+                kms = []
+                for _ in range(min(args.steps, 30)):
+                    flush.zero_()
+                    compute_charge([tube], out=Qs, stream=stream)
+                    kms.append(last_stats()["rgf_kernel_ms"])
+                ss = last_stats()
+                schedules[name] = {"rgf_kernel_ms": float(np.mean(kms)), "kernel_launches": ss["kernel_launches"],
+                                   "checkpoint_bytes": ss["checkpoint_bytes"],
+                                   "max_rel_vs_timed": float((Qs - Q).abs().max() / Q.abs().max())}
+        finally:
+            set_tuning(TUNE_SCHEDULE, 0)
+            set_timing(False)
+
     # ---- roofline of the dominant kernel (the RGF sweep kernel)
     flops = st["contour_updates"] * FLOP_CONTOUR + st["realaxis_updates"] * FLOP_REALAXIS
     k_ms = float(np.mean(rgf_ms))
@@ -675,7 +700,8 @@ def main():
                                            f"energy shards of one tube over {world} GPUs, one NCCL all-reduce of "
                                            f"{N} doubles per pass"),
                            "l2": "flushed between passes (256 MiB write), flush outside the per-pass events"},
-                "roofline": roof, "cpu_baseline": cpu, "parity": parity, "scf": scf, "mixed": mixed,
+                "roofline": roof, "cpu_baseline": cpu, "parity": parity, "schedules": schedules, "scf": scf,
+                "mixed": mixed,
                 "config3": cfg3, "config4": cfg4, "long_tube": longt, "config5": cfg5,
                 "e2e": {"value": e2e_value, "unit": "updates/s", "h2d_bytes_per_step": 8 * N + 16,
                         "d2h_bytes_per_step": 8 * N,

@@ -94,6 +94,7 @@ class Stats(C.Structure):
         ("kernel_launches", C.c_int),
         ("pieces", C.c_int),
         ("checkpoint_bytes", C.c_longlong),
+        ("schedule", C.c_int),
     ]
 
 

@@ -205,6 +205,7 @@ struct negf_charge_plan {
     DevBuf d_tubes, d_chains, d_warps, d_units, d_rts, d_partial, d_scratch;
     int num_warps = 0, num_units = 0, max_N = 0;
     int wpb = 4, spu = negf::kSegsPerUnit;
+    int schedule = 0;  // negf::kScheduleTwoPass or kScheduleFused
     double* d_Q = nullptr;
     long long updates = 0;
     double tuned_ms = 0.0;
@@ -258,6 +259,7 @@ struct Settings {
     bool timing = false;
     int warps_per_block = 4;
     int pass1_pieces = 0;  // 0: automatic
+    int schedule = 0;      // 0: automatic, else NEGF_SCHEDULE_*
     negf_stats stats{};
     Workspace* stats_ws = nullptr;  // workspace whose events time the last call (when timing)
 };
@@ -647,6 +649,32 @@ int device_sm_count() {
     return cache[dev];
 }
 
+// RGF schedule of a launch of nw warps (NEGF_TUNE_SCHEDULE): fused when the
+// sweeps run as one piece and the warps fill at least one per SM
+// sub-partition (4 per SM), else two-pass (its segment tiles spread few
+// chains over the whole GPU).
+int choose_schedule(int setting, int nw, int pieces) {
+    if (pieces > 1) return negf::kScheduleTwoPass;
+    if (setting == NEGF_SCHEDULE_FUSED) return negf::kScheduleFused;
+    if (setting == NEGF_SCHEDULE_TWO_PASS) return negf::kScheduleTwoPass;
+    return nw >= 4 * device_sm_count() ? negf::kScheduleFused : negf::kScheduleTwoPass;
+}
+
+// Checkpoint bytes written + read by one launch: two-pass stores both sweeps'
+// states at every segment (pass 1 writes, pass 2 reads); the fused schedule
+// stores one record per segment ((Y, lambda) or (X, rho); (Y) or (X) on
+// contour chains).
+long long checkpoint_traffic(const std::vector<negf::WarpRec>& warps, const std::vector<negf::TubeDev>& tdev,
+                             long long scratch_doubles, int schedule) {
+    if (schedule != negf::kScheduleFused) return 2 * scratch_doubles * 8;
+    long long b = 0;
+    for (const negf::WarpRec& w : warps) {
+        const long long nseg = (tdev[w.tube].N + negf::kSeg - 1) / negf::kSeg;
+        b += nseg * (w.kind == negf::kRealAxis ? 3 : 2) * negf::kWarp * (w.fp32 ? 4 : 8);
+    }
+    return 2 * b;
+}
+
 // Launch tables of a set of tube passes.  Launch order: longest tubes first
 // (order[] is caller scratch of passes.size() ints); rts[i] describes pass i.
 void build_table_generic(const TubePass* passes, int num_passes, int* order, Out<negf::ChainRec>& chains,
@@ -759,11 +787,13 @@ int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const s
         pieces = nw >= target / 2 ? 1 : std::min(maxp, (target + nw - 1) / std::max(nw, 1));
     }
     pieces = std::max(1, pieces);
+    const int schedule = choose_schedule(G.schedule, nw, pieces);
+    if (schedule == negf::kScheduleFused) pieces = 1;
     if (pieces > 1) NEGF_CUDA(W.pieces.reserve(sizeof(double) * (size_t)nw * pieces * 24 * negf::kWarp));
     NEGF_CUDA(negf::launch_rgf(W.tubes.as<negf::TubeDev>(), W.chains.as<negf::ChainRec>(), W.warps.as<negf::WarpRec>(),
                                nw, W.units.as<negf::SegUnit>(), (int)ct.units.size(), W.partial.as<double>(),
                                W.scratch.p, G.warps_per_block, stream, G.timing ? W.ev[3] : nullptr, nullptr, pieces,
-                               W.pieces.as<double>()));
+                               W.pieces.as<double>(), schedule));
     if (G.timing) NEGF_CUDA(cudaEventRecord(W.ev[1], stream));
     NEGF_CUDA(negf::launch_reduce(W.rts.as<negf::ReduceTube>(), (int)ct.rts.size(), ct.max_N, W.partial.as<double>(),
                                   d_Q, stream));
@@ -778,10 +808,12 @@ int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const s
     st.realaxis_updates = ct.realaxis_updates;
     st.chains = (int)ct.chains.size();
     st.warps = nw;
-    st.kernel_launches = (nw > 0 ? (pieces > 1 ? 4 : 2) : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
+    const bool fused = schedule == negf::kScheduleFused;
+    st.kernel_launches = (nw > 0 ? (fused ? 1 : pieces > 1 ? 4 : 2) : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
     st.pieces = pieces;
-    st.units = (int)ct.units.size();
-    st.checkpoint_bytes = 2 * ct.scratch_doubles * 8;
+    st.units = fused ? 0 : (int)ct.units.size();
+    st.checkpoint_bytes = checkpoint_traffic(ct.warps, tdev, ct.scratch_doubles, schedule);
+    st.schedule = fused ? NEGF_SCHEDULE_FUSED : NEGF_SCHEDULE_TWO_PASS;
     G.stats_ws = G.timing ? &W : nullptr;
     return NEGF_OK;
 }
@@ -1398,7 +1430,8 @@ int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
 cudaError_t plan_launch(const negf_charge_plan& p, const int* skip, cudaStream_t s) {
     cudaError_t e = negf::launch_rgf(p.d_tubes.as<negf::TubeDev>(), p.d_chains.as<negf::ChainRec>(),
                                      p.d_warps.as<negf::WarpRec>(), p.num_warps, p.d_units.as<negf::SegUnit>(),
-                                     p.num_units, p.d_partial.as<double>(), p.d_scratch.p, p.wpb, s, nullptr, skip);
+                                     p.num_units, p.d_partial.as<double>(), p.d_scratch.p, p.wpb, s, nullptr, skip, 1,
+                                     nullptr, p.schedule);
     if (e != cudaSuccess) return e;
     return negf::launch_reduce(p.d_rts.as<negf::ReduceTube>(), (int)p.tubes.size(), p.max_N,
                                p.d_partial.as<double>(), p.d_Q, s, skip);
@@ -1425,9 +1458,10 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
     p->wpb = settings().warps_per_block;
     rc = plan_tables(*p, negf::kSegsPerUnit, true);
     if (rc) return rc;
+    p->schedule = choose_schedule(settings().schedule, p->num_warps, 1);
     if (flags & NEGF_PLAN_AUTOTUNE) {
-        // time every (segments per pass-2 unit, pass-2 warps per block) pair on
-        // this batch; results are identical for all of them
+        // time the fused schedule (wpb 0 below) and every two-pass shape
+        // (segments per pass-2 unit x pass-2 warps per block) on this batch
         cudaEvent_t e0, e1;
         NEGF_CUDA(cudaEventCreate(&e0));
         NEGF_CUDA(cudaEventCreate(&e1));
@@ -1436,8 +1470,10 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
         for (int spu : {16, 32, 64}) {
             rc = plan_tables(*p, spu, false);
             if (rc) break;
-            for (int wpb : {1, 2, 4}) {
-                p->wpb = wpb;
+            for (int wpb : {0, 1, 2, 4}) {
+                if (wpb == 0 && spu != 16) continue;  // the fused schedule has no segment units
+                p->wpb = wpb == 0 ? 4 : wpb;
+                p->schedule = wpb == 0 ? negf::kScheduleFused : negf::kScheduleTwoPass;
                 cudaError_t e = plan_launch(*p, nullptr, 0);
                 for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
                     if (r == 1) e = cudaEventRecord(e0, 0);
@@ -1462,7 +1498,8 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (rc) return rc;
-        p->wpb = best_wpb;
+        p->schedule = best_wpb == 0 ? negf::kScheduleFused : negf::kScheduleTwoPass;
+        p->wpb = best_wpb == 0 ? 4 : best_wpb;
         p->tuned_ms = best;
         rc = plan_tables(*p, best_spu, false);
         if (rc) return rc;
@@ -1484,7 +1521,7 @@ int negf_charge_plan_launch(negf_charge_plan* p, const int* d_skip, void* stream
 int negf_charge_plan_info(const negf_charge_plan* p, int* pass2_warps_per_block, int* segs_per_unit,
                           double* tuned_ms, long long* updates) {
     if (!p) return fail(NEGF_ERR_ARG, "null plan");
-    if (pass2_warps_per_block) *pass2_warps_per_block = p->wpb;
+    if (pass2_warps_per_block) *pass2_warps_per_block = p->schedule == negf::kScheduleFused ? 0 : p->wpb;
     if (segs_per_unit) *segs_per_unit = p->spu;
     if (tuned_ms) *tuned_ms = p->tuned_ms;
     if (updates) *updates = p->updates;
@@ -1507,6 +1544,11 @@ int negf_set_tuning(int key, int value) {
         case NEGF_TUNE_PASS1_PIECES:
             if (value < 0 || value > 4096) return fail(NEGF_ERR_ARG, "pieces must be in [0, 4096] (0: automatic)");
             G.pass1_pieces = value;
+            return NEGF_OK;
+        case NEGF_TUNE_SCHEDULE:
+            if (value != 0 && value != NEGF_SCHEDULE_TWO_PASS && value != NEGF_SCHEDULE_FUSED)
+                return fail(NEGF_ERR_ARG, "schedule must be 0 (automatic), NEGF_SCHEDULE_TWO_PASS or NEGF_SCHEDULE_FUSED");
+            G.schedule = value;
             return NEGF_OK;
         default:
             return fail(NEGF_ERR_ARG, "unknown tuning key");

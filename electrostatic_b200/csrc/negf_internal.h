@@ -118,12 +118,21 @@ cudaError_t nn_rowdot(long long rows, int cols, const float* h, const float* w, 
 cudaError_t nn_outer(long long rows, int cols, const float* dq, const float* w, float* dh, void* dhb, cudaStream_t s);
 cudaError_t nn_mse(long long n, const float* q, const float* y, float* d, float* part, cudaStream_t s);
 
+// RGF schedules.  Two-pass: pass 1 (one warp per 32 chains, both sweeps,
+// checkpoints at every segment) then pass 2 (one warp per group of segments:
+// segment-parallel tiles).  Fused: one kernel, one warp per 32 whole chains,
+// meet-in-the-middle sweeps (fewer operations and half the checkpoint bytes;
+// it needs enough warps to fill the GPU).  Results agree to rounding.
+constexpr int kScheduleTwoPass = 0;
+constexpr int kScheduleFused = 1;
 // skip (device int, may be null): when nonzero at launch time every block
 // returns at entry (device-side early exit of a captured SCF iteration).
+// The fused schedule runs with pieces == 1 only (else the two-pass one runs).
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
                        int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event,
-                       const int* skip = nullptr, int pieces = 1, double* d_piece_work = nullptr);
+                       const int* skip = nullptr, int pieces = 1, double* d_piece_work = nullptr,
+                       int schedule = kScheduleTwoPass);
 // pieces > 1 (parallel in length): d_piece_work holds num_warps * pieces * 24 * 32 doubles.
 // Device self-test of numeric primitives: which = 0 FP64 reciprocal,
 // 1 FP32 reciprocal (input/output as doubles), n values, device pointers.

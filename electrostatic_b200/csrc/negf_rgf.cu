@@ -312,7 +312,15 @@ __device__ __forceinline__ void proj_scale(Proj<R>& p) {
 // through segment fs and the backward sweep through segment bs.  INTERIOR:
 // the caller guarantees that both segments are full and hold no contact site
 // and that a next block exists.
-template <typename R, bool RA, bool INTERIOR>
+// Checkpoint record of the fused schedule: one per segment, (Y, lambda) at
+// the start of a segment the forward sweep crosses first, (X, rho) at the end
+// of one the backward sweep crosses first.
+template <bool RA>
+struct CkCompact {
+    static constexpr int NC = RA ? 3 : 2;
+};
+
+template <typename R, bool RA, bool INTERIOR, bool COMPACT = false>
 __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<R>& b, int fs, int bs, bool has_next,
                                             const double* __restrict__ U, R* __restrict__ ck, const R (&uf)[kSeg],
                                             const R (&ub)[kSeg], R (&nf)[kSeg], R (&nb)[kSeg], R hfull) {
@@ -325,14 +333,26 @@ __device__ __forceinline__ void pass1_block(const Chain<R>& c, Proj<R>& f, Proj<
         R yr, yi, xr, xi;
         proj_boundary<R, RA>(f, yr, yi);
         proj_boundary<R, RA>(b, xr, xi);
-        R* p = ck + (size_t)fs * CL::NC * kWarp;
-        p[CL::Y * kWarp] = yr;
-        p[(CL::Y + 1) * kWarp] = yi;
-        if (RA) p[CL::L * kWarp] = f.lam;
-        R* q = ck + (size_t)bs * CL::NC * kWarp;
-        q[CL::X * kWarp] = xr;
-        q[(CL::X + 1) * kWarp] = xi;
-        if (RA) q[CL::RHO * kWarp] = b.lam;
+        if (COMPACT) {
+            constexpr int NC = CkCompact<RA>::NC;
+            R* p = ck + (size_t)fs * NC * kWarp;
+            p[0] = yr;
+            p[kWarp] = yi;
+            if (RA) p[2 * kWarp] = f.lam;
+            R* q = ck + (size_t)bs * NC * kWarp;
+            q[0] = xr;
+            q[kWarp] = xi;
+            if (RA) q[2 * kWarp] = b.lam;
+        } else {
+            R* p = ck + (size_t)fs * CL::NC * kWarp;
+            p[CL::Y * kWarp] = yr;
+            p[(CL::Y + 1) * kWarp] = yi;
+            if (RA) p[CL::L * kWarp] = f.lam;
+            R* q = ck + (size_t)bs * CL::NC * kWarp;
+            q[CL::X * kWarp] = xr;
+            q[(CL::X + 1) * kWarp] = xi;
+            if (RA) q[CL::RHO * kWarp] = b.lam;
+        }
     }
     if (INTERIOR || has_next) {
         // next forward segment fs+1 and next backward segment bs-1 (full, bs >= 1):
@@ -494,9 +514,15 @@ __device__ __forceinline__ CkVals<R> load_ck(const R* __restrict__ p) {
     return v;
 }
 
-template <typename R, bool RA, bool EDGE>
+// Sweep state at a segment boundary (normalised: (Y, 1) with lambda).
+template <typename R>
+struct Bnd {
+    R yr, yi, lam;
+};
+
+template <typename R, bool RA, bool EDGE, bool NEXT = false>
 __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const CkVals<R>& ckv, const R (&u)[kSeg],
-                                             double (&acc)[kSeg]) {
+                                             double (&acc)[kSeg], Bnd<R>* next = nullptr) {
     constexpr int K = kSeg;
     const int N = c.N;
     R pr[K], pi[K], qr[K + 1], qi[K + 1], lm[K];
@@ -530,6 +556,17 @@ __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const Ck
             pi[j + 1] = h2 * qi[j];
             if (RA) lm[j + 1] = lm[j] * h2;
         }
+    }
+    if constexpr (NEXT) {
+        // forward state at the next segment start (interior segments, K even:
+        // the last hopping of the segment is gamma): Y = h^2 Q_{K-1} / Q_K,
+        // lambda = lambda_{n0} prod h^2 / |Q_K|^2 with Q_{n0} = 1
+        static_assert(!EDGE, "next boundary of interior segments only");
+        const R rq = rcp(fma(qr[K], qr[K], qi[K] * qi[K]));
+        const R tr = fma(qr[K - 1], qr[K], qi[K - 1] * qi[K]), ti = fma(qi[K - 1], qr[K], -qr[K - 1] * qi[K]);
+        next->yr = c.hg2 * tr * rq;
+        next->yi = c.hg2 * ti * rq;
+        next->lam = RA ? lm[K - 1] * c.hg2 * rq : (R)1;
     }
     // Interior segment: D_n is the same at every site of the segment (the
     // discrete Wronskian: with S_{n-1} = alpha_n S_n - h_n^2 S_{n+1} and
@@ -662,6 +699,197 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
         constexpr int shift = (K == 16) ? 1 : 2;
         const int j = lane >> shift;
         if ((lane & ((1 << shift) - 1)) == 0 && n0 + j < N) prow[n0 + j] = tot;
+    }
+}
+
+// K forward projective steps through an interior segment from the
+// normalised state (Y, 1), lambda: the normalised state at the next segment
+// start.  The same routine advances the backward sweep when given the
+// segment's potentials in reverse order (the hopping parities of an aligned
+// segment read the same both ways).
+template <typename R, bool RA>
+__device__ __forceinline__ Bnd<R> sweep_segment(const Chain<R>& c, const Bnd<R>& in, const R (&u)[kSeg]) {
+    constexpr int K = kSeg;
+    R pr = in.yr, pi = in.yi, qr = 1, qi = 0, H = 1;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const R h2 = (j & 1) ? c.hg2 : c.hb2;
+        const R ar = c.Er - u[j];
+        const R nqr = fma(ar, qr, fma(-c.Ei, qi, -pr));
+        const R nqi = fma(ar, qi, fma(c.Ei, qr, -pi));
+        pr = h2 * qr;
+        pi = h2 * qi;
+        qr = nqr;
+        qi = nqi;
+        H *= h2;
+    }
+    // Y = h^2 Q_{K-1} / Q_K (pr, pi = h^2 Q_{K-1}), lambda * prod h^2 / |Q_K|^2
+    const R rq = rcp(fma(qr, qr, qi * qi));
+    Bnd<R> o;
+    o.yr = fma(pr, qr, pi * qi) * rq;
+    o.yi = fma(pi, qr, -pr * qi) * rq;
+    o.lam = RA ? in.lam * H * rq : (R)1;
+    return o;
+}
+
+// Sum of a segment's per-lane contributions over the warp, one coalesced
+// row-segment write (sites n0 .. n0 + K - 1 below N).
+__device__ __forceinline__ void write_segment(double (&acc)[kSeg], int n0, int N, double* __restrict__ prow,
+                                              int lane) {
+    const double tot = warp_reduce_scatter<kSeg>(acc, lane);
+    const int j = lane >> 2;
+    if ((lane & 3) == 0 && n0 + j < N) prow[n0 + j] = tot;
+}
+
+template <typename R>
+__device__ __forceinline__ void load_seg(const double* __restrict__ U, int n0, R (&u)[kSeg]) {
+    const double2* u2 = reinterpret_cast<const double2*>(U + n0);  // n0 even, U 16-byte aligned
+#pragma unroll
+    for (int k = 0; k < kSeg / 2; ++k) {
+        const double2 v = __ldg(u2 + k);
+        u[2 * k] = (R)v.x;
+        u[2 * k + 1] = (R)v.y;
+    }
+}
+template <typename R>
+__device__ __forceinline__ void load_seg_reversed(const double* __restrict__ U, int n0, R (&u)[kSeg]) {
+    const double2* u2 = reinterpret_cast<const double2*>(U + n0);
+#pragma unroll
+    for (int k = 0; k < kSeg / 2; ++k) {
+        const double2 v = __ldg(u2 + k);
+        u[kSeg - 1 - 2 * k] = (R)v.x;
+        u[kSeg - 2 - 2 * k] = (R)v.y;
+    }
+}
+template <typename R>
+__device__ __forceinline__ void load_seg_edge(const double* __restrict__ U, int n0, int N, R (&u)[kSeg]) {
+#pragma unroll
+    for (int k = 0; k < kSeg; ++k) u[k] = (n0 + k < N) ? (R)__ldg(U + n0 + k) : (R)0;
+}
+
+// Fused schedule: one warp carries 32 whole chains.  With A = nseg / 2,
+// phase A runs the forward sweep through segments [0, A) and the backward
+// sweep through [nseg - A, nseg) together (as pass 1), each storing its own
+// boundary record at those segments only.  The middle segment of an odd
+// count is then integrated from both live states.  Phase B continues each
+// sweep into the other half: the forward sweep forms the contributions of
+// segment s from its live state at the segment start and the backward record
+// at the segment end (the segment recompute of pass 2, whose forward part is
+// now the sweep itself), the backward sweep does the mirror image on the
+// segment read in reverse.  Every site is crossed twice instead of three
+// times, each record is written once and read once, and no second kernel
+// runs.  The contact segments take the per-site (edge) form.
+template <typename R, bool RA>
+__device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, const ChainRec& cr, int tube,
+                                            R* __restrict__ ck_warp, double* __restrict__ prow, int lane) {
+    constexpr int K = kSeg;
+    constexpr int NC = CkCompact<RA>::NC;
+    const TubeDev& T = tubes[tube];
+    const int N = T.N;
+    const int nseg = (N + K - 1) / K;
+    const double* __restrict__ U = T.U;
+    const bool valid = cr.mode >= 0;
+    const double beta = T.beta[valid ? cr.mode : 0];
+    const cd E = {cr.Er, cr.Ei};
+    // U_contact = U at the end sites (Nanostructure.cpp:500-504) when read on the device
+    const double Uc0 = T.uc_from_U ? U[0] : T.Uc0, Uc1 = T.uc_from_U ? U[N - 1] : T.Uc1;
+    const cd S0 = sigma_contact(E, Uc0, beta, T);
+    const cd S1 = sigma_contact(E, Uc1, beta, T);
+    const Chain<R> c = make_chain<R, RA>(T, cr, S0.x, S0.y, S1.x, S1.y);
+    Chain<R> crev = c;  // the chain read from the drain end: the two contacts' roles swap
+    crev.k0 = c.k1;
+    crev.k1 = c.k0;
+    R* __restrict__ ck = ck_warp + lane;
+    auto rec = [&](int seg) -> Bnd<R> {
+        const R* p = ck + (size_t)seg * NC * kWarp;
+        return {p[0], p[kWarp], RA ? p[2 * kWarp] : (R)1};
+    };
+    const int A = nseg / 2;
+    Proj<R> f{0, 0, 1, 0, 1, 1, 1};  // Y_0 = 0, lambda_0 = 1
+    Proj<R> b{0, 0, 1, 0, 1, 1, 1};  // X_{N-1} = 0, rho_{N-1} = 1
+    // ---- phase A
+    if (A > 0) {
+        R hfull = 1;  // prod of h^2 over a full segment
+#pragma unroll
+        for (int j = 0; j < K / 2; ++j) hfull *= c.hb2 * c.hg2;
+        R ua_f[K], ua_b[K], ub_f[K], ub_b[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            ua_f[j] = (R)__ldg(U + j);
+            ua_b[j] = (R)__ldg(U + N - 1 - j);  // kPadLo zeros before site 0 cover N < K
+        }
+        pass1_block<R, RA, false, true>(c, f, b, 0, nseg - 1, A > 1, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+        int k = 1;
+        for (; k + 2 <= A; k += 2) {
+            pass1_block<R, RA, true, true>(c, f, b, k, nseg - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+            pass1_block<R, RA, true, true>(c, f, b, k + 1, nseg - 2 - k, true, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+        }
+        if (k < A) pass1_block<R, RA, true, true>(c, f, b, k, nseg - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+    }
+    Bnd<R> fw, bw;  // forward state at the start of segment nseg - A - (nseg odd), backward at the end of segment A - 1 + (nseg odd)
+    proj_boundary<R, RA>(f, fw.yr, fw.yi);
+    fw.lam = f.lam;
+    proj_boundary<R, RA>(b, bw.yr, bw.yi);
+    bw.lam = b.lam;
+    // ---- middle segment of an odd count, from both live states
+    if (nseg & 1) {
+        const int n0 = A * K;
+        const CkVals<R> v{fw.yr, fw.yi, fw.lam, bw.yr, bw.yi, bw.lam};
+        double acc[K];
+        R u[K];
+        if (nseg == 1) {
+            load_seg_edge(U, 0, N, u);
+            segment_proj<R, RA, true>(c, 0, v, u, acc);
+            write_segment(acc, 0, N, prow, lane);
+            return;
+        }
+        load_seg(U, n0, u);
+        Bnd<R> nf;
+        segment_proj<R, RA, false, true>(c, n0, v, u, acc, &nf);
+        write_segment(acc, n0, N, prow, lane);
+        R ur[K];
+        load_seg_reversed(U, n0, ur);
+        bw = sweep_segment<R, RA>(c, bw, ur);  // X and rho at the end of segment A - 1
+        fw = nf;                               // Y and lambda at the start of segment A + 1
+    }
+    // ---- phase B: forward through [nseg - A, nseg), backward through [0, A) downwards
+    for (int k = 0; k < A; ++k) {
+        const int sf = nseg - A + k, sb = A - 1 - k;
+        const bool last = k == A - 1;  // the contact segments nseg - 1 and 0
+        {
+            const int n0 = sf * K;
+            const Bnd<R> x = rec(sf);
+            const CkVals<R> v{fw.yr, fw.yi, fw.lam, x.yr, x.yi, x.lam};
+            double acc[K];
+            R u[K];
+            if (!last) {
+                load_seg(U, n0, u);
+                segment_proj<R, RA, false, true>(c, n0, v, u, acc, &fw);
+            } else {
+                load_seg_edge(U, n0, N, u);
+                segment_proj<R, RA, true>(c, n0, v, u, acc);
+            }
+            write_segment(acc, n0, N, prow, lane);
+        }
+        {
+            const int n0 = sb * K;
+            const Bnd<R> y = rec(sb);
+            double acc[K];
+            R u[K];
+            if (!last) {
+                load_seg_reversed(U, n0, u);
+                const CkVals<R> v{bw.yr, bw.yi, bw.lam, y.yr, y.yi, y.lam};
+                double accr[K];
+                segment_proj<R, RA, false, true>(crev, n0, v, u, accr, &bw);
+#pragma unroll
+                for (int j = 0; j < K; ++j) acc[j] = accr[K - 1 - j];
+            } else {
+                load_seg_edge(U, n0, N, u);
+                const CkVals<R> v{y.yr, y.yi, y.lam, bw.yr, bw.yi, bw.lam};
+                segment_proj<R, RA, true>(c, n0, v, u, acc);
+            }
+            write_segment(acc, n0, N, prow, lane);
+        }
     }
 }
 
@@ -910,6 +1138,34 @@ __global__ void __launch_bounds__(32) rgf_piece_prefix_kernel(const TubeDev* __r
                 tb[q] = nb[q];
             }
         }
+    }
+}
+
+// Fused schedule: one warp (32 whole chains) per block; records in the
+// warp's scratch, per-site sums into the warp's partial row.
+__global__ void __launch_bounds__(32) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
+                                                       const ChainRec* __restrict__ chains,
+                                                       const WarpRec* __restrict__ warps, int num_warps,
+                                                       double* __restrict__ partial, double* __restrict__ scratch,
+                                                       const int* __restrict__ skip) {
+    if (skip && *skip) return;
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x;
+    if (w >= num_warps) return;
+    const WarpRec wr = warps[w];
+    const ChainRec c = chains[(size_t)w * kWarp + lane];
+    double* ws = scratch + wr.ck_off;
+    double* prow = partial + wr.row_off;
+    if (wr.fp32) {
+        if (wr.kind == kRealAxis)
+            fused_chain<float, true>(tubes, c, wr.tube, reinterpret_cast<float*>(ws), prow, lane);
+        else
+            fused_chain<float, false>(tubes, c, wr.tube, reinterpret_cast<float*>(ws), prow, lane);
+    } else {
+        if (wr.kind == kRealAxis)
+            fused_chain<double, true>(tubes, c, wr.tube, ws, prow, lane);
+        else
+            fused_chain<double, false>(tubes, c, wr.tube, ws, prow, lane);
     }
 }
 
@@ -1182,8 +1438,16 @@ int rgf_kernel_regs() {
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
                        int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event, const int* skip, int pieces,
-                       double* d_piece_work) {
+                       double* d_piece_work, int schedule) {
     if (num_warps <= 0) return cudaSuccess;
+    if (schedule == kScheduleFused && pieces <= 1) {
+        // one warp per block: whole chains spread evenly over the SMs
+        rgf_fused_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps, d_partial,
+                                                           static_cast<double*>(d_scratch), skip);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess && mid_event) e = cudaEventRecord(mid_event, stream);
+        return e;
+    }
     if (warps_per_block < 1 || warps_per_block > 4) warps_per_block = 4;
     double* states = nullptr;
     if (pieces > 1) {

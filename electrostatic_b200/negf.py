@@ -330,6 +330,17 @@ def set_timing(enable: bool):
     check(_lib.load().negf_set_timing(int(bool(enable))), "negf_set_timing")
 
 
+TUNE_PASS2_WARPS_PER_BLOCK = 2
+TUNE_PASS1_PIECES = 4
+TUNE_SCHEDULE = 6
+SCHEDULE_AUTO, SCHEDULE_TWO_PASS, SCHEDULE_FUSED = 0, 1, 2
+
+
+def set_tuning(key: int, value: int):
+    """negf_set_tuning: launch-shape knobs of the charge calls (TUNE_* keys)."""
+    check(_lib.load().negf_set_tuning(int(key), int(value)), "negf_set_tuning")
+
+
 def shard_range(num_points: int, rank: int, world: int):
     lo, hi = C.c_int(), C.c_int()
     check(_lib.load().negf_shard_range(int(num_points), int(rank), int(world), C.byref(lo), C.byref(hi)),

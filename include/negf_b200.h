@@ -193,6 +193,7 @@ typedef struct negf_stats {
     int kernel_launches;       /* kernels launched by the call */
     int pieces;                /* pass-1 pieces per chain (parallel in length) */
     long long checkpoint_bytes;/* scratch bytes written+read by the kernel */
+    int schedule;              /* NEGF_SCHEDULE_TWO_PASS or NEGF_SCHEDULE_FUSED */
 } negf_stats;
 int negf_last_stats(negf_stats* s);
 /* Launch-shape knobs of negf_compute_charge.
@@ -205,9 +206,23 @@ int negf_last_stats(negf_stats* s);
  *   states, then the pieces' sweeps.  Automatic: when the chains fill
  *   fewer than 4 warps per SM, enough pieces for about 8 warps per SM, each
  *   of >= 32 segments (256 sites), at most 128.  Results agree with P = 1 to
- *   rounding (relative 1e-10 in the tests, about 1e-12 measured). */
+ *   rounding (relative 1e-10 in the tests, about 1e-12 measured).
+ * NEGF_TUNE_SCHEDULE: 0 (default, automatic), NEGF_SCHEDULE_TWO_PASS or
+ *   NEGF_SCHEDULE_FUSED.  Two-pass: pass 1 runs both sweeps of every chain
+ *   and checkpoints them at every 8-site segment, pass 2 integrates the
+ *   segments in parallel tiles (parallelism for few chains).  Fused: one
+ *   kernel; the forward sweep crosses the first half of the tube and the
+ *   backward sweep the second, each storing its own checkpoints, then each
+ *   continues into the other half and integrates the segments it crosses
+ *   (every site crossed twice instead of three times, half the checkpoint
+ *   bytes; needs enough chains to fill the GPU).  Automatic: fused when the
+ *   chains fill at least one warp per SM sub-partition and the sweeps run as
+ *   one piece.  Results agree to rounding. */
 #define NEGF_TUNE_PASS2_WARPS_PER_BLOCK 2
 #define NEGF_TUNE_PASS1_PIECES 4
+#define NEGF_TUNE_SCHEDULE 6
+#define NEGF_SCHEDULE_TWO_PASS 1
+#define NEGF_SCHEDULE_FUSED 2
 int negf_set_tuning(int key, int value);
 /* Enable CUDA-event timing of negf_compute_charge (off by default). */
 int negf_set_timing(int enable);
@@ -329,9 +344,13 @@ int negf_write_integrand(negf_tube* t, const char* path, int count, const double
  * contact potentials are read on the device as U[0] and U[N-1] of each
  * tube's potential buffer (U_contact = U at the end sites,
  * Nanostructure.cpp:500-504).  d_Q: device output of sum N doubles (tube
- * order).  With NEGF_PLAN_AUTOTUNE the pass-2 schedule (segments per unit
- * 16/32/64 x warps per block 1/2/4) is timed on the batch and the fastest
- * kept (results are identical for all).  A plan is stale (NEGF_ERR_STATE at
+ * order).  With NEGF_PLAN_AUTOTUNE the fused (warp per chain) schedule and
+ * every two-pass (segment tile) schedule -- segments per unit 16/32/64 x
+ * pass-2 warps per block 1/2/4 -- are timed on the batch and the fastest is
+ * kept (results agree to rounding; bitwise within the two-pass shapes).
+ * Without it the schedule follows NEGF_TUNE_SCHEDULE's automatic rule.
+ * negf_charge_plan_info's *pass2_warps_per_block is 0 when the fused
+ * schedule was chosen.  A plan is stale (NEGF_ERR_STATE at
  * launch) once a tube's energy paths change (contact mu, adaptive limits);
  * d_skip (device int or null) skips the launch at kernel entry when set. */
 #define NEGF_PLAN_AUTOTUNE 1
