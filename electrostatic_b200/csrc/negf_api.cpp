@@ -781,6 +781,7 @@ int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const s
     // one-warp blocks per SM, pieces of >= 32 segments, at most 128 pieces
     // (the prefix over the pieces is sequential per chain)
     int pieces = G.pass1_pieces;
+    if (pieces == 0 && G.schedule == NEGF_SCHEDULE_FUSED) pieces = 1;  // an explicit fused request wins
     if (pieces == 0) {
         const int target = 8 * device_sm_count();
         const int maxp = std::min(128, std::max(1, ((ct.max_N + negf::kSeg - 1) / negf::kSeg) / 32));

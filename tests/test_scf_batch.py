@@ -34,14 +34,20 @@ def test_plan_matches_compute_charge():
     S = sum(t.num_field_sites for t in tubes)
     ref = torch.zeros(S, dtype=torch.float64, device="cuda")
     compute_charge(tubes, out=ref)
+    from electrostatic_b200.negf import last_stats
+    ref_schedule = last_stats()["schedule"]  # 1 two-pass, 2 fused
     for autotune in (False, True):
         Q = torch.zeros(S, dtype=torch.float64, device="cuda")
         plan = ChargePlan(tubes, Q, autotune=autotune)
         plan.launch()
         torch.cuda.synchronize()
-        assert torch.equal(Q, ref)
         info = plan.info()
-        assert info["pass2_warps_per_block"] in (1, 2, 4) and info["segs_per_unit"] in (16, 32, 64)
+        fused = info["pass2_warps_per_block"] == 0
+        if fused == (ref_schedule == 2):
+            assert torch.equal(Q, ref)  # same schedule: bitwise
+        else:  # the autotuner chose the other schedule: equal to rounding
+            assert float((Q - ref).abs().max() / ref.abs().max()) <= 1e-11
+        assert info["pass2_warps_per_block"] in (0, 1, 2, 4) and info["segs_per_unit"] in (16, 32, 64)
         plan.close()
 
 
