@@ -448,6 +448,8 @@ def main():
     ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--no-long-tube", action="store_true")
     ap.add_argument("--config5", action="store_true", help="surrogate study (about two minutes, off by default)")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "two_pass"],
+                    help="RGF schedule of the timed passes (automatic by default)")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis); "
                          "real-space case of 200 blocks and 256 contour energies")
@@ -478,7 +480,8 @@ def main():
 
     from electrostatic_b200 import build
     build.build()
-    from electrostatic_b200.negf import CNT, compute_charge, last_stats, set_timing
+    from electrostatic_b200.negf import CNT, TUNE_SCHEDULE, compute_charge, last_stats, set_timing, set_tuning
+    set_tuning(TUNE_SCHEDULE, {"auto": 0, "two_pass": 1, "fused": 2}[args.schedule])
 
     tube = CNT(**tube_kwargs(args.precision))
     y = tube.site_positions()
@@ -602,7 +605,7 @@ def main():
     # ---- both RGF schedules on the same tube (kernel time per pass, CUDA events)
     schedules = None
     if world == 1:
-        from electrostatic_b200.negf import SCHEDULE_FUSED, SCHEDULE_TWO_PASS, TUNE_SCHEDULE, set_tuning
+        from electrostatic_b200.negf import SCHEDULE_FUSED, SCHEDULE_TWO_PASS
         schedules = {"chosen": {1: "two_pass", 2: "fused"}.get(st["schedule"], "?")}
         set_timing(True)
         try:
@@ -621,7 +624,7 @@ def main():
                                    "checkpoint_bytes": ss["checkpoint_bytes"],
                                    "max_rel_vs_timed": float((Qs - Q).abs().max() / Q.abs().max())}
         finally:
-            set_tuning(TUNE_SCHEDULE, 0)
+            set_tuning(TUNE_SCHEDULE, {"auto": 0, "two_pass": 1, "fused": 2}[args.schedule])
             set_timing(False)
 
     # ---- roofline of the dominant kernel (the RGF sweep kernel)

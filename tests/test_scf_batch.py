@@ -130,7 +130,7 @@ def test_batch_scf_graph_equals_loop_and_oracle(oracle):
     from oracle.scf_oracle import run_scf_batch_oracle
     Vg = [0.0, 0.15]
     tubes, electros, oracles = _batch(oracle)
-    r_graph = run_scf_batch(tubes, electros, Vg, use_graph=True, iters_per_graph=4)
+    r_graph = run_scf_batch(tubes, electros, Vg, use_graph=True, iters_per_graph=4, autotune=False)
     tubes2, electros2, _ = _batch()
     r_loop = run_scf_batch(tubes2, electros2, Vg, use_graph=False, autotune=False)
     for a, b in zip(r_graph.steps, r_loop.steps):
