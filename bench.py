@@ -385,46 +385,101 @@ def long_tube_measure(torch, reps=10):
             "max_rel_automatic_vs_one_piece": float(np.max(np.abs(Qa - Q1)) / np.max(np.abs(Q1)))}
 
 
-def config5_measure(torch, n_pairs=8000, epochs=20):
-    """Surrogate-started self-consistency on the 4000-site, 8-mode (17,0) tube
-    (Vds 0.4 V, gate 0 -> 0.6 V): pairs recorded along plain NEGF solves,
-    BF16 training of the Fourier operator, then plain vs surrogate-started
-    sweeps (NEGF judges every converged charge)."""
-    from electrostatic_b200 import surrogate as S
+def config5_measure(torch, n_pairs=20000, epochs=20, oracle_check=True):
+    """Surrogate-assisted self-consistency on the config-4 tube set (16
+    tubes): one Fourier operator for the whole set (6 layers, width 128, 32
+    frequencies, BF16 weights, FP32 accumulation) trained on n_pairs (U, Q)
+    pairs from the engine; then the Vds = 0.4 V gate sweep 0 -> 0.6 V twice:
+    plain (FP64 tubes, Broyden alpha 0.1 from zero charge at every gate
+    point, the reference's defaults) and surrogate-started (mixed-precision
+    tubes; surrogate charge as the start, surrogate Jacobian for the initial
+    inverse Jacobian, FP64 finish).  Per-step times exclude the one-off
+    plans and graph captures of both sweeps; data generation and training
+    are reported separately."""
     from electrostatic_b200.negf import CNT
-    from electrostatic_b200.workloads import gate_with_contacts
-    t0 = time.perf_counter()
-    U, Vg, Vds, Q, eng = S.generate_scf_pairs(n_pairs)
-    t_data = time.perf_counter() - t0
-    perm = torch.randperm(n_pairs, generator=torch.Generator().manual_seed(0)).cuda()
-    U, Vg, Vds, Q = U[perm], Vg[perm], Vds[perm], Q[perm]
-    ntr = int(0.9 * n_pairs)
-    m = S.FourierOperator(4000, seed=0)
-    r = m.fit(U[:ntr], Vg[:ntr], Vds[:ntr], Q[:ntr], epochs=epochs, batch=16)
-    pred = m.predict(U[ntr:], Vg[ntr:], Vds[ntr:])
-    qmax = Q[ntr:].abs().max(dim=1).values
-    err = ((pred - Q[ntr:]).abs().max(dim=1).values / qmax).cpu().numpy()
-    rms = ((pred - Q[ntr:]).pow(2).mean(dim=1).sqrt() / qmax).cpu().numpy()
+    from electrostatic_b200.scf import run_scf_batch
+    from electrostatic_b200.surrogate_set import (TubeSetOperator, generate_set_pairs, set_scf_sweep,
+                                                  tube_descriptor)
+    from electrostatic_b200.workloads import GATE_SWEEP, gate_with_contacts, uneven_batch
+    descs = uneven_batch(precision="fp64")
     vds = 0.4
-    tube = CNT(**S.tube_kwargs(vds))
-    R = 1.42e-10 * np.sqrt(3.0) * 17 / (2 * np.pi)
-    el = gate_with_contacts(tube.site_positions(), R, vds=vds)
-    vgs = [0.0, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6]
-    S.scf_sweep(tube, el, [0.0], vds)
-    plain = S.scf_sweep(tube, el, vgs, vds)
-    sur = S.scf_sweep(tube, el, vgs, vds, model=m, keep_history=False)
-    return {"workload": "(17,0) N=4000, 8 modes, 1024 contour + 3072 real-axis energies (eta 2 meV), Vds 0.4 V, "
-                        "Vg 0..0.6 V; operator 6 layers x width 128 x 32 frequencies, 17-site potential window per "
-                        "site, BF16 weights, FP32 accumulate",
-            "pairs": n_pairs, "data_seconds": t_data, "engine_seconds": eng, "train_seconds": r["seconds"],
-            "epochs": epochs, "final_loss": r["loss"][-1], "test_rel_err_median": float(np.median(err)),
-            "test_rms_rel_err_median": float(np.median(rms)),
-            "plain": {"iterations": [a["negf_iterations"] for a in plain], "seconds": sum(a["seconds"] for a in plain)},
-            "surrogate_started": {"negf_iterations": [b["negf_iterations"] for b in sur],
-                                  "surrogate_iterations": [b["surrogate_iterations"] for b in sur],
-                                  "used": [b["surrogate_used"] for b in sur],
-                                  "seconds": sum(b["seconds"] for b in sur)},
-            "max_abs_dQ_vs_plain": max(float(np.max(np.abs(a["Q"] - b["Q"]))) for a, b in zip(plain, sur))}
+
+    def make(lv, precision="fp64", realaxis_fp32=False):
+        return [CNT(**dict(d, contact_mu=(0.0, -float(lv)), precision=precision, mixed_realaxis_fp32=realaxis_fp32))
+                for d in descs]
+
+    tubes64 = make(vds)
+    electros = []
+    for d, t in zip(descs, tubes64):
+        R = 1.42e-10 * np.sqrt(3.0) * d["type_id"][0] / (2 * np.pi)  # CNT.cpp:23-41
+        electros.append(gate_with_contacts(t.site_positions(), R, vds=vds))
+    t0 = time.perf_counter()
+    U, Vg, Vds, tid, Q, eng = generate_set_pairs(make, electros, n_pairs)
+    t_data = time.perf_counter() - t0
+    for e in electros:
+        e.Vds = vds
+    model = TubeSetOperator([tube_descriptor(t) for t in tubes64], seed=0)
+    perm = torch.randperm(n_pairs, generator=torch.Generator().manual_seed(0)).cuda()
+    U, Vg, Vds, tid, Q = U[perm], Vg[perm], Vds[perm], tid[perm], Q[perm]
+    ntr = int(0.9 * n_pairs)
+    fit = model.fit_set(U[:ntr], Vg[:ntr], Vds[:ntr], tid[:ntr], Q[:ntr], epochs=epochs, batch=16)
+    pred = model.predict_set(U[ntr:], Vg[ntr:], Vds[ntr:], tid[ntr:])
+    qt = Q[ntr:].double()
+    qmax = qt.abs().max(dim=1).values.clamp_min(1e-30)
+    err = ((pred - qt).abs().max(dim=1).values / qmax).cpu().numpy()
+    rms = ((pred - qt).pow(2).sum(dim=1) / model._mask_set[tid[ntr:]].sum(dim=1)).sqrt().div(qmax).cpu().numpy()
+    del U, Q, pred, qt
+    torch.cuda.empty_cache()
+    # plain FP64 sweep (warm-up on one gate point first: plans, graphs, lazy loading)
+    run_scf_batch(tubes64, electros, [0.0], use_graph=True, iters_per_graph=4)
+    plain = run_scf_batch(tubes64, electros, GATE_SWEEP, use_graph=True, iters_per_graph=4)
+    # surrogate-started, mixed precision (contour and real-axis chains in FP32 at 2 meV broadening)
+    tubesmx = make(vds, precision="mixed", realaxis_fp32=True)
+    set_scf_sweep(tubesmx, electros, [0.0], model)  # warm-up
+    sur, alpha, lam, t_setup = set_scf_sweep(tubesmx, electros, GATE_SWEEP, model)
+    t_plain = sum(s_.seconds for s_ in plain.steps)
+    t_sur = sum(r["seconds"] for r in sur)
+    dq = max(float(np.max(np.abs(r["Q"] - s_.Q))) / float(np.max(np.abs(s_.Q))) for r, s_ in zip(sur, plain.steps))
+    res = {"workload": "config-4 tube set (16 tubes), Vds 0.4 V, Vg 0..0.6 V step 0.05, 1e-6 absolute max-norm; "
+                       "operator 6 layers x width 128 x 32 frequencies on a %d-site canvas, BF16 weights, FP32 "
+                       "accumulation" % model.S,
+           "pairs": n_pairs, "data_seconds": t_data, "engine_seconds": eng, "train_seconds": fit["seconds"],
+           "epochs": epochs, "final_loss": fit["loss"][-1], "test_rel_err_median": float(np.median(err)),
+           "test_rel_err_p90": float(np.percentile(err, 90)), "test_rms_rel_err_median": float(np.median(rms)),
+           "plain": {"iterations": [s_.iterations for s_ in plain.steps], "seconds": t_plain,
+                     "method": "FP64 tubes, Broyden alpha 0.1, n = 0 at every gate point (reference defaults)"},
+           "surrogate_started": {"negf_iterations": [r["negf_iterations"] for r in sur],
+                                 "fp32_iterations": [r["lowprec_iterations"] for r in sur],
+                                 "surrogate_iterations": [r["surrogate_iterations"] for r in sur],
+                                 "used": [r["surrogate_used"] for r in sur], "seconds": t_sur,
+                                 "fraction": alpha, "lambda_max": lam, "setup_seconds_excluded": t_setup,
+                                 "method": "mixed-precision tubes (FP32 contour and real-axis chains, FP64 finish "
+                                           "below 1e-5); start = surrogate self-consistent charge; initial inverse "
+                                           "Jacobian = surrogate secant rows (first gate point), carried NEGF rows "
+                                           "after, fraction 2/(1+lambda_max) of the surrogate Jacobian"},
+           "speedup": t_plain / t_sur, "max_rel_dQ_vs_plain_fp64": dq}
+    if oracle_check:
+        # the FP64 oracle's charge at the converged potential of the last gate point (fixed-point check)
+        from oracle import oracle as O
+        O.build()
+        threads = len(os.sched_getaffinity(0))
+        r = sur[-1]
+        n_conv = r["n_in"]
+        offs = np.concatenate([[0], np.cumsum([t.num_field_sites for t in tubesmx])]).astype(int)
+        worst, t1 = 0.0, time.perf_counter()
+        qmx = float(np.max(np.abs(n_conv)))
+        for d, e, a, b in zip(descs, electros, offs[:-1], offs[1:]):
+            kw = {k: v for k, v in d.items() if k not in ("precision", "mixed_realaxis_fp32")}
+            ot = O.OracleTube(**dict(kw, contact_mu=(0.0, -vds)))
+            Uc = e.potential(n_conv[a:b], GATE_SWEEP[-1])
+            ot.set_potential(Uc, (Uc[0], Uc[-1]))
+            worst = max(worst, float(np.max(np.abs(ot.charge(nthreads=threads) - n_conv[a:b]))))
+        res["oracle_fixed_point"] = {"Vg": GATE_SWEEP[-1], "max_abs_Qoracle_minus_n": worst,
+                                     "relative": worst / qmx, "seconds": time.perf_counter() - t1,
+                                     "check": "|Q_oracle(U(n)) - n| of the surrogate sweep's converged charge n"}
+    for t in tubes64 + tubesmx:
+        t.close()
+    return res
 
 
 def ring_positions_nm(unitcells, acc=1.42e-10):
@@ -447,7 +502,7 @@ def main():
     ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--no-long-tube", action="store_true")
-    ap.add_argument("--config5", action="store_true", help="surrogate study (about two minutes, off by default)")
+    ap.add_argument("--config5", action="store_true", help="surrogate-assisted sweep of the config-4 set")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "two_pass"],
                     help="RGF schedule of the timed passes (automatic by default)")
     ap.add_argument("--small", action="store_true",

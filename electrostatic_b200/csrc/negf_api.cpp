@@ -1694,6 +1694,37 @@ int negf_broyden_set_initial_jacobian(negf_broyden* b, const double* d_V, const 
     return NEGF_OK;
 }
 
+int negf_broyden_restart(negf_broyden* b, int keep_rows, void* stream) {
+    if (!b || keep_rows < 0) return fail(NEGF_ERR_ARG, "bad restart arguments");
+    negf::BroydenDev& d = b->dev;
+    cudaStream_t s = (cudaStream_t)stream;
+    int st[2] = {1, 0};
+    NEGF_CUDA(cudaMemcpyAsync(st, d.step_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    NEGF_CUDA(cudaStreamSynchronize(s));
+    // rows 1 .. base are seeds, the solve added one row per step after its first
+    const int rows = st[1] + std::max(0, st[0] - 2);
+    const int keep = std::min(std::min(rows, keep_rows), d.max_step / 2);
+    NEGF_CUDA(negf::broyden_shift_rows(d, rows - keep, keep, s));
+    d.base = keep;
+    b->step = 1;
+    NEGF_CUDA(negf::set_int(d.step_dev, 1, s));
+    NEGF_CUDA(negf::set_int(d.step_dev + 1, keep, s));
+    return NEGF_OK;
+}
+
+int negf_broyden_history(negf_broyden* b, double** d_V, double** d_W, int* rows, void* stream) {
+    if (!b || !d_V || !d_W || !rows) return fail(NEGF_ERR_ARG, "null argument");
+    negf::BroydenDev& d = b->dev;
+    cudaStream_t s = (cudaStream_t)stream;
+    int st[2] = {1, 0};
+    NEGF_CUDA(cudaMemcpyAsync(st, d.step_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    NEGF_CUDA(cudaStreamSynchronize(s));
+    *rows = st[1] + std::max(0, st[0] - 2);
+    *d_V = d.V + d.S;  // row 1
+    *d_W = d.W + d.S;
+    return NEGF_OK;
+}
+
 int negf_broyden_step_number(negf_broyden* b, int* step) {
     if (!b || !step) return fail(NEGF_ERR_ARG, "null argument");
     // device-resident steps advance the device counter only

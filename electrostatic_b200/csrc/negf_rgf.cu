@@ -520,19 +520,27 @@ struct Bnd {
     R yr, yi, lam;
 };
 
+// State of one segment between its forward part (recompute of (P, Q) from
+// the start record, D and the folded coefficients) and its backward part
+// (walk of (R, S) from the end record with the site contributions).
+template <typename R>
+struct SegWork {
+    R qr[kSeg + 1], qi[kSeg + 1], lm[kSeg];
+    R Rr, Ri, rh, cgr, cgi;
+};
+
 template <typename R, bool RA, bool EDGE, bool NEXT = false>
-__device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const CkVals<R>& ckv, const R (&u)[kSeg],
-                                             double (&acc)[kSeg], Bnd<R>* next = nullptr) {
+__device__ __forceinline__ void seg_fwd(const Chain<R>& c, int n0, const CkVals<R>& ckv, const R (&u)[kSeg],
+                                        SegWork<R>& w, Bnd<R>* next = nullptr) {
     constexpr int K = kSeg;
     const int N = c.N;
-    R pr[K], pi[K], qr[K + 1], qi[K + 1], lm[K];
-    pr[0] = ckv.yr;
-    pi[0] = ckv.yi;
-    qr[0] = 1;
-    qi[0] = 0;
-    lm[0] = ckv.lam;
-    R Rr = ckv.xr, Ri = ckv.xi, Sr = 1, Si = 0;
-    R rh = ckv.rho;
+    R pr = ckv.yr, pi = ckv.yi;
+    w.qr[0] = 1;
+    w.qi[0] = 0;
+    w.lm[0] = ckv.lam;
+    w.Rr = ckv.xr;
+    w.Ri = ckv.xi;
+    w.rh = ckv.rho;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
         const int n = n0 + j;
@@ -548,13 +556,13 @@ __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const Ck
                 ai -= c.s1i;
             }
         }
-        qr[j + 1] = fma(ar, qr[j], fma(-ai, qi[j], -pr[j]));
-        qi[j + 1] = fma(ar, qi[j], fma(ai, qr[j], -pi[j]));
+        w.qr[j + 1] = fma(ar, w.qr[j], fma(-ai, w.qi[j], -pr));
+        w.qi[j + 1] = fma(ar, w.qi[j], fma(ai, w.qr[j], -pi));
         if (j + 1 < K) {
             const R h2 = EDGE ? ((n & 1) ? c.hg2 : c.hb2) : ((j & 1) ? c.hg2 : c.hb2);
-            pr[j + 1] = h2 * qr[j];
-            pi[j + 1] = h2 * qi[j];
-            if (RA) lm[j + 1] = lm[j] * h2;
+            pr = h2 * w.qr[j];
+            pi = h2 * w.qi[j];
+            if (RA) w.lm[j + 1] = w.lm[j] * h2;
         }
     }
     if constexpr (NEXT) {
@@ -562,11 +570,12 @@ __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const Ck
         // the last hopping of the segment is gamma): Y = h^2 Q_{K-1} / Q_K,
         // lambda = lambda_{n0} prod h^2 / |Q_K|^2 with Q_{n0} = 1
         static_assert(!EDGE, "next boundary of interior segments only");
-        const R rq = rcp(fma(qr[K], qr[K], qi[K] * qi[K]));
-        const R tr = fma(qr[K - 1], qr[K], qi[K - 1] * qi[K]), ti = fma(qi[K - 1], qr[K], -qr[K - 1] * qi[K]);
+        const R rq = rcp(fma(w.qr[K], w.qr[K], w.qi[K] * w.qi[K]));
+        const R tr = fma(w.qr[K - 1], w.qr[K], w.qi[K - 1] * w.qi[K]);
+        const R ti = fma(w.qi[K - 1], w.qr[K], -w.qr[K - 1] * w.qi[K]);
         next->yr = c.hg2 * tr * rq;
         next->yi = c.hg2 * ti * rq;
-        next->lam = RA ? lm[K - 1] * c.hg2 * rq : (R)1;
+        next->lam = RA ? w.lm[K - 1] * c.hg2 * rq : (R)1;
     }
     // Interior segment: D_n is the same at every site of the segment (the
     // discrete Wronskian: with S_{n-1} = alpha_n S_n - h_n^2 S_{n+1} and
@@ -575,21 +584,32 @@ __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const Ck
     // into the per-segment coefficients.
     // D, |D|^2 and the folded coefficients in FP64 once per segment; the
     // per-site products then run in the chain's precision
-    R cgr = 0, cgi = 0;  // contour: c conj(D) / |D|^2
+    w.cgr = 0;
+    w.cgi = 0;  // contour: c conj(D) / |D|^2
     if (!EDGE) {
-        const double dr = fma(-(double)Rr, (double)qr[K - 1], fma((double)Ri, (double)qi[K - 1], (double)qr[K]));
-        const double di = fma(-(double)Rr, (double)qi[K - 1], fma(-(double)Ri, (double)qr[K - 1], (double)qi[K]));
+        const double dr =
+            fma(-(double)w.Rr, (double)w.qr[K - 1], fma((double)w.Ri, (double)w.qi[K - 1], (double)w.qr[K]));
+        const double di =
+            fma(-(double)w.Rr, (double)w.qi[K - 1], fma(-(double)w.Ri, (double)w.qr[K - 1], (double)w.qi[K]));
         const double inv = rcp(fma(dr, dr, di * di));
         if (RA) {
             const R fa = (R)(c.k0 * inv), fb = (R)(c.k1 * inv);
 #pragma unroll
-            for (int j = 0; j < K; ++j) lm[j] *= fa;
-            rh *= fb;
+            for (int j = 0; j < K; ++j) w.lm[j] *= fa;
+            w.rh *= fb;
         } else {
-            cgr = (R)(fma(c.cr, dr, c.ci * di) * inv);
-            cgi = (R)(fma(c.ci, dr, -c.cr * di) * inv);
+            w.cgr = (R)(fma(c.cr, dr, c.ci * di) * inv);
+            w.cgi = (R)(fma(c.ci, dr, -c.cr * di) * inv);
         }
     }
+}
+
+template <typename R, bool RA, bool EDGE>
+__device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[kSeg], SegWork<R>& w,
+                                        double (&acc)[kSeg]) {
+    constexpr int K = kSeg;
+    const int N = c.N;
+    R Rr = w.Rr, Ri = w.Ri, Sr = 1, Si = 0, rh = w.rh;
 #pragma unroll
     for (int j = K - 1; j >= 0; --j) {
         const int n = n0 + j;
@@ -598,22 +618,22 @@ __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const Ck
         double v;
         if (!EDGE) {
             if (RA) {  // |G|^2 (lambda k0 + rho k1) = lm |S|^2 + rh |Q|^2, 1/|D|^2 folded in
-                const R s2 = fma(Sr, Sr, Si * Si), q2 = fma(qr[j], qr[j], qi[j] * qi[j]);
-                v = (double)fma(lm[j], s2, rh * q2);
+                const R s2 = fma(Sr, Sr, Si * Si), q2 = fma(w.qr[j], w.qr[j], w.qi[j] * w.qi[j]);
+                v = (double)fma(w.lm[j], s2, rh * q2);
             } else {  // Im(c Q S / D)
-                const R tr = fma(qr[j], Sr, -qi[j] * Si), ti = fma(qr[j], Si, qi[j] * Sr);
-                v = (double)fma(cgr, ti, cgi * tr);
+                const R tr = fma(w.qr[j], Sr, -w.qi[j] * Si), ti = fma(w.qr[j], Si, w.qi[j] * Sr);
+                v = (double)fma(w.cgr, ti, w.cgi * tr);
             }
         } else {
             // D = S Q_{n+1} - R Q_n, per site (the segment may be partial), in FP64
             const double Sd = Sr, Sid = Si, Rd = Rr, Rid = Ri;
-            const double q1r = qr[j + 1], q1i = qi[j + 1], q0r = qr[j], q0i = qi[j];
+            const double q1r = w.qr[j + 1], q1i = w.qi[j + 1], q0r = w.qr[j], q0i = w.qi[j];
             const double dr = fma(Sd, q1r, fma(-Sid, q1i, fma(-Rd, q0r, Rid * q0i)));
             const double di = fma(Sd, q1i, fma(Sid, q1r, fma(-Rd, q0i, -Rid * q0r)));
             const double inv = rcp(fma(dr, dr, di * di));
             if (RA) {  // real-axis chains carry no contour coefficient (c = 0)
                 const double s2 = fma(Sd, Sd, Sid * Sid), q2 = fma(q0r, q0r, q0i * q0i);
-                v = inv * fma((double)lm[j] * s2, c.k0, (double)rh * q2 * c.k1);
+                v = inv * fma((double)w.lm[j] * s2, c.k0, (double)rh * q2 * c.k1);
             } else {  // Im(c T conj(D)) / |D|^2 with T = Q S
                 const double tr = fma(q0r, Sd, -q0i * Sid), ti = fma(q0r, Sid, q0i * Sd);
                 const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
@@ -640,6 +660,14 @@ __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const Ck
             if (RA) rh *= h2;
         }
     }
+}
+
+template <typename R, bool RA, bool EDGE, bool NEXT = false>
+__device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const CkVals<R>& ckv, const R (&u)[kSeg],
+                                             double (&acc)[kSeg], Bnd<R>* next = nullptr) {
+    SegWork<R> w;
+    seg_fwd<R, RA, EDGE, NEXT>(c, n0, ckv, u, w, next);
+    seg_bwd<R, RA, EDGE>(c, n0, u, w, acc);
 }
 
 // Pass 2: segments [seg0, seg1) of one warp's chains.  Per segment: forward
@@ -852,44 +880,65 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
         bw = sweep_segment<R, RA>(c, bw, ur);  // X and rho at the end of segment A - 1
         fw = nf;                               // Y and lambda at the start of segment A + 1
     }
-    // ---- phase B: forward through [nseg - A, nseg), backward through [0, A) downwards
+    // ---- phase B: forward through [nseg - A, nseg), backward through [0, A) downwards.
+    // The records of iteration k + 1 are loaded into registers during
+    // iteration k and those of k + 2 brought into L1 (they were written long
+    // before and sit in DRAM); interior iterations issue the forward parts of
+    // both directions' segments before their backward parts, two independent
+    // dependency chains.
+    auto prefetch_rec = [&](int k) {
+        if (k < A) {
+            const R* pf = ck + (size_t)(nseg - A + k) * NC * kWarp;
+            const R* pb = ck + (size_t)(A - 1 - k) * NC * kWarp;
+#pragma unroll
+            for (int q = 0; q < NC; ++q) {
+                prefetch_l1(pf + q * kWarp);
+                prefetch_l1(pb + q * kWarp);
+            }
+        }
+    };
+    Bnd<R> xn = {0, 0, 1}, yn = {0, 0, 1};
+    if (A > 0) {
+        xn = rec(nseg - A);
+        yn = rec(A - 1);
+    }
+    prefetch_rec(1);
     for (int k = 0; k < A; ++k) {
         const int sf = nseg - A + k, sb = A - 1 - k;
+        const int nf = sf * K, nb = sb * K;
         const bool last = k == A - 1;  // the contact segments nseg - 1 and 0
-        {
-            const int n0 = sf * K;
-            const Bnd<R> x = rec(sf);
-            const CkVals<R> v{fw.yr, fw.yi, fw.lam, x.yr, x.yi, x.lam};
-            double acc[K];
-            R u[K];
-            if (!last) {
-                load_seg(U, n0, u);
-                segment_proj<R, RA, false, true>(c, n0, v, u, acc, &fw);
-            } else {
-                load_seg_edge(U, n0, N, u);
-                segment_proj<R, RA, true>(c, n0, v, u, acc);
-            }
-            write_segment(acc, n0, N, prow, lane);
+        const Bnd<R> x = xn, y = yn;
+        if (!last) {
+            xn = rec(sf + 1);
+            yn = rec(sb - 1);
         }
-        {
-            const int n0 = sb * K;
-            const Bnd<R> y = rec(sb);
-            double acc[K];
-            R u[K];
-            if (!last) {
-                load_seg_reversed(U, n0, u);
-                const CkVals<R> v{bw.yr, bw.yi, bw.lam, y.yr, y.yi, y.lam};
-                double accr[K];
-                segment_proj<R, RA, false, true>(crev, n0, v, u, accr, &bw);
+        prefetch_rec(k + 2);
+        double accf[K], accb[K];
+        if (!last) {
+            R uf[K], ub[K];
+            load_seg(U, nf, uf);
+            load_seg_reversed(U, nb, ub);
+            const CkVals<R> vf{fw.yr, fw.yi, fw.lam, x.yr, x.yi, x.lam};
+            const CkVals<R> vb{bw.yr, bw.yi, bw.lam, y.yr, y.yi, y.lam};
+            SegWork<R> wf, wb;
+            seg_fwd<R, RA, false, true>(c, nf, vf, uf, wf, &fw);
+            seg_fwd<R, RA, false, true>(crev, nb, vb, ub, wb, &bw);
+            double accr[K];
+            seg_bwd<R, RA, false>(c, nf, uf, wf, accf);
+            seg_bwd<R, RA, false>(crev, nb, ub, wb, accr);
 #pragma unroll
-                for (int j = 0; j < K; ++j) acc[j] = accr[K - 1 - j];
-            } else {
-                load_seg_edge(U, n0, N, u);
-                const CkVals<R> v{y.yr, y.yi, y.lam, bw.yr, bw.yi, bw.lam};
-                segment_proj<R, RA, true>(c, n0, v, u, acc);
-            }
-            write_segment(acc, n0, N, prow, lane);
+            for (int j = 0; j < K; ++j) accb[j] = accr[K - 1 - j];
+        } else {
+            R uf[K], ub[K];
+            load_seg_edge(U, nf, N, uf);
+            load_seg_edge(U, nb, N, ub);
+            const CkVals<R> vf{fw.yr, fw.yi, fw.lam, x.yr, x.yi, x.lam};
+            const CkVals<R> vb{y.yr, y.yi, y.lam, bw.yr, bw.yi, bw.lam};
+            segment_proj<R, RA, true>(c, nf, vf, uf, accf);
+            segment_proj<R, RA, true>(c, nb, vb, ub, accb);
         }
+        write_segment(accf, nf, N, prow, lane);
+        write_segment(accb, nb, N, prow, lane);
     }
 }
 

@@ -404,6 +404,21 @@ class Broyden:
 
     Reset_Broyden_Parallel = reset
 
+    def history(self, stream=None):
+        """(V, W, rows): zero-copy device views [rows][S] of the secant rows held now."""
+        from .scf import device_view
+        v, w, r = C.c_void_p(), C.c_void_p(), C.c_int()
+        check(_lib.load().negf_broyden_history(self._h, C.byref(v), C.byref(w), C.byref(r), _stream(stream)),
+              "negf_broyden_history")
+        S = self.S
+        return device_view(v.value, r.value * S).view(r.value, S), device_view(w.value, r.value * S).view(r.value, S), \
+            r.value
+
+    def restart(self, keep_rows=100, stream=None):
+        """Next solve with the secant rows so far (at most keep_rows, the most
+        recent) as its initial inverse Jacobian; n_in stays."""
+        check(_lib.load().negf_broyden_restart(self._h, int(keep_rows), _stream(stream)), "negf_broyden_restart")
+
     def set_initial_jacobian(self, V, W, stream=None):
         """Initial inverse Jacobian G0 = fraction I + sum_j W[j] V[j]^T for the
         next solve (V, W: device float64 [k][S]); call after create or reset."""

@@ -43,10 +43,11 @@ def _p(t):
 class FourierOperator:
     """The operator for tubes of S sites.  All state lives on the device."""
 
-    def __init__(self, S: int, seed: int = 0, device: str = "cuda"):
+    def __init__(self, S: int, seed: int = 0, device: str = "cuda", feat: int = FEAT):
         import torch
         self.torch = torch
         self.S, self.dev = int(S), device
+        self.feat = int(feat)
         g = torch.Generator().manual_seed(seed)
         W, M = WIDTH, MODES
         f32 = dict(dtype=torch.float32)
@@ -55,7 +56,7 @@ class FourierOperator:
             return (torch.randn(*shape, generator=g, **f32) / math.sqrt(fan_in)).to(device)
 
         self.params = {
-            "W_lift": init((FEAT, W), FEAT),
+            "W_lift": init((self.feat, W), self.feat),
             "b_lift": torch.zeros(W, device=device, **f32),
             "w_p": init((W,), W),
             "b_p": torch.zeros(1, device=device, **f32),
@@ -81,7 +82,7 @@ class FourierOperator:
             G[:, 2 * k + 1] = np.sin(2 * np.pi * k * s / self.S)
         self.F = torch.tensor(F, dtype=torch.bfloat16, device=device)
         self.G = torch.tensor(G, dtype=torch.bfloat16, device=device)
-        self.x_scale = torch.ones(FEAT, device=device)
+        self.x_scale = torch.ones(self.feat, device=device)
         self.q_scale = 1.0
         self._bufs = {}
         # window gather: site n reads U[n + d], d = -WIN..WIN, masked to 0 beyond the ends
@@ -91,7 +92,7 @@ class FourierOperator:
         self._wmask = torch.tensor(((j >= 0) & (j < self.S)).astype(np.float32), device=device)
         # fixed site features: n / S, parity, contact proximity
         n = np.arange(self.S)
-        fixed = np.zeros((self.S, FEAT - nw - 2), dtype=np.float32)
+        fixed = np.zeros((self.S, self.feat - nw - 2), dtype=np.float32)
         fixed[:, 0] = n / self.S
         fixed[:, 1] = np.where(n % 2 == 0, 1.0, -1.0)
         fixed[:, 2] = np.exp(-n / 40.0)
@@ -120,16 +121,16 @@ class FourierOperator:
     # ------------------------------------------------------------------ model
     def features(self, U, Vg, Vds):
         """x[b][s] (see the module docstring), potentials divided by the stored
-        potential scale, as BF16 rows [B*S][FEAT]."""
+        potential scale, as BF16 rows [B*S][self.feat]."""
         t = self.torch
         B = U.shape[0]
         nw = 2 * WIN + 1
-        x = t.empty(B, self.S, FEAT, device=self.dev)
+        x = t.empty(B, self.S, self.feat, device=self.dev)
         x[:, :, :nw] = U.float()[:, self._widx].reshape(B, self.S, nw) * (self._wmask / self.x_scale[0])
         x[:, :, nw] = Vg[:, None]
         x[:, :, nw + 1] = Vds[:, None]
         x[:, :, nw + 2:] = self._fixed
-        return x.to(t.bfloat16).reshape(B * self.S, FEAT)
+        return x.to(t.bfloat16).reshape(B * self.S, self.feat)
 
     def forward(self, xb, B, keep=False):
         """xb: BF16 [B*S][4]; returns q [B*S] (FP32, in units of q_scale)."""
@@ -139,7 +140,7 @@ class FourierOperator:
         cache = {"xb": xb} if keep else None
         h = self._buf("h0", (R, W))
         hb = self._buf("h0b", (R, W), t.bfloat16)
-        self._gemm(0, 0, R, W, FEAT, 1, xb, FEAT, 0, self.bf["W_lift"], W, 0, h, W, 0)
+        self._gemm(0, 0, R, W, self.feat, 1, xb, self.feat, 0, self.bf["W_lift"], W, 0, h, W, 0)
         check(L.negf_nn_gelu_fwd(R, W, _p(h), None, _p(self.params["b_lift"]), None, _p(h), _p(hb), 0, self._s()),
               "lift")
         for l in range(LAYERS):
@@ -210,7 +211,7 @@ class FourierOperator:
         # lift
         dhb = self._buf("dhb", (R, W), t.bfloat16)
         check(L.negf_nn_cast_bf16(R * W, _p(dh), _p(dhb), self._s()), "cast")
-        self._gemm(1, 0, FEAT, W, R, 1, c["xb"], FEAT, 0, dhb, W, 0, gr["W_lift"], W, 0)
+        self._gemm(1, 0, self.feat, W, R, 1, c["xb"], self.feat, 0, dhb, W, 0, gr["W_lift"], W, 0)
         check(L.negf_nn_colsum(R, W, _p(dh), _p(gr["b_lift"]), 0, self._s()), "colsum")
 
     def adam(self, lr=1e-3, wd=0.0):
@@ -234,7 +235,7 @@ class FourierOperator:
         """Train on device tensors U [n][S], Vg [n], Vds [n], Q [n][S] (float32)."""
         t = self.torch
         n = U.shape[0]
-        self.x_scale = t.ones(FEAT, device=self.dev)
+        self.x_scale = t.ones(self.feat, device=self.dev)
         self.x_scale[0] = float(U.abs().max())
         self.q_scale = float(Q.abs().max())
         y_all = (Q / self.q_scale).float()
@@ -267,8 +268,8 @@ class FourierOperator:
         potential buffer), scalar biases, Q_out (float64 device, S)."""
         t = self.torch
         nw = 2 * WIN + 1
-        self._bind = dict(U=U_view, Q=Q_out, x=t.empty(self.S, FEAT, device=self.dev),
-                          xb=t.empty(self.S, FEAT, dtype=t.bfloat16, device=self.dev),
+        self._bind = dict(U=U_view, Q=Q_out, x=t.empty(self.S, self.feat, device=self.dev),
+                          xb=t.empty(self.S, self.feat, dtype=t.bfloat16, device=self.dev),
                           win=t.empty(self.S * nw, dtype=t.float64, device=self.dev),
                           wscale=self._wmask / self.x_scale[0])
         x = self._bind["x"]

@@ -1,0 +1,467 @@
+"""Surrogate over a set of tubes: one Fourier neural operator for every tube of
+an uneven batch, and the surrogate-started self-consistent gate sweep.
+
+The operator of surrogate.py maps a fixed-length potential to the induced
+charge.  Here one operator serves the whole batch (tubes of 800-8000 sites,
+chiralities (13,0), (17,0), (19,0), 2-10 modes): every tube sits on a canvas
+of S sites (its own sites first, padding after), and per-site descriptors tell
+the operator which tube it reads.  One inference is then one batch of
+canvases, a fixed set of launches whatever the tube count.
+
+Features per site (FEAT_SET = 32):
+  0..16  U at sites n-8 .. n+8 of the tube (indices clamped to the tube: the
+         leads continue at the end-site potential), divided by the potential
+         scale
+  17, 18 Vg, Vds
+  19..31 n / N, ring parity +-1, exp(-n / 40), exp(-(N-1-n) / 40), inside
+         mask, chirality one-hot (13, 17, 19), modes / 10, inner band edge of
+         the lowest and of the highest kept mode / gamma, channels / 20, N / S
+
+Training pairs come from the engine itself (negf_compute_charge on the whole
+batch): half along self-consistent gate solves at random (Vg, Vds), half from
+the config-2 recipe of random potentials (external potential of the gate and
+contacts plus 5 seeded Gaussian bumps).  The loss is the mean square error
+over the tubes' own sites (padding is masked out).
+
+The sweep (set_scf_sweep) follows scf.run_scf_batch -- one Broyden over all
+the tubes' sites, iterations replayed as CUDA graphs -- and adds the
+surrogate: per gate step, (1) the surrogate phase solves the loop with the
+surrogate's charge (its own Broyden, continued from the previous gate step);
+(2) the NEGF phase starts from that charge; its initial inverse Jacobian is
+the surrogate phase's secant rows at the first gate step and the NEGF
+phase's own rows carried from the previous gate step afterwards
+(negf_broyden_restart), with the scalar part fraction * I set from the
+surrogate's Jacobian (largest eigenvalue of I - dQ_s/dn by power iteration:
+fraction = 2 / (1 + lambda_max)).  The NEGF phase runs the mixed-precision
+plan until the residual falls below switch_norm and the FP64 plan after; only
+an FP64 NEGF charge ends a solve (the engine judges every converged charge).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+from .surrogate import WIN, FourierOperator
+
+FEAT_SET = 32
+
+
+def tube_descriptor(tube):
+    """Per-tube constants of the features (from the engine's mode table)."""
+    J, deg, beta = tube.modes()
+    gamma = float(tube.desc.gamma)
+    edges = np.abs(np.abs(beta) - gamma) / gamma
+    return dict(N=tube.num_field_sites, m=int(tube.desc.type_id[0]), M=len(beta), edge_lo=float(edges.min()),
+                edge_hi=float(edges.max()), channels=int(np.sum(deg)))
+
+
+class TubeSetOperator(FourierOperator):
+    """The Fourier operator on a canvas of S sites for a fixed set of tubes."""
+
+    def __init__(self, descriptors, S=None, seed=0, device="cuda"):
+        import torch
+        nmax = max(d["N"] for d in descriptors)
+        S = int(S or ((nmax + 255) // 256) * 256)
+        super().__init__(S, seed=seed, device=device, feat=FEAT_SET)
+        self.desc = list(descriptors)
+        T = len(self.desc)
+        nw = 2 * WIN + 1
+        fixed = np.zeros((T, S, FEAT_SET - nw - 2), dtype=np.float32)
+        widx = np.zeros((T, S, nw), dtype=np.int64)
+        mask = np.zeros((T, S), dtype=np.float32)
+        n = np.arange(S)
+        for t, d in enumerate(self.desc):
+            N = d["N"]
+            inside = n < N
+            fixed[t, :, 0] = np.where(inside, n / N, 0.0)
+            fixed[t, :, 1] = np.where(n % 2 == 0, 1.0, -1.0)
+            fixed[t, :, 2] = np.exp(-n / 40.0)
+            fixed[t, :, 3] = np.where(inside, np.exp(-np.clip(N - 1 - n, 0, None) / 40.0), 0.0)
+            fixed[t, :, 4] = inside
+            fixed[t, :, 5 + {13: 0, 17: 1, 19: 2}.get(d["m"], 1)] = 1.0
+            fixed[t, :, 8] = d["M"] / 10.0
+            fixed[t, :, 9] = d["edge_lo"]
+            fixed[t, :, 10] = d["edge_hi"]
+            fixed[t, :, 11] = d["channels"] / 20.0
+            fixed[t, :, 12] = N / S
+            widx[t] = np.clip(n[:, None] + np.arange(-WIN, WIN + 1)[None, :], 0, N - 1)
+            mask[t] = inside
+        self._fixed_set = torch.tensor(fixed, device=device)
+        self._widx_set = torch.tensor(widx.reshape(T, S * nw), device=device)
+        self._mask_set = torch.tensor(mask, device=device)
+        self.Ns = [d["N"] for d in self.desc]
+        self.offs = np.concatenate([[0], np.cumsum(self.Ns)]).astype(np.int64)
+
+    # ------------------------------------------------------------------ features
+    def features_set(self, U, Vg, Vds, tid):
+        """U: canvas potentials [B][S] (float32; a tube's sites first), Vg,
+        Vds [B], tid [B] tube indices -> BF16 rows [B*S][FEAT_SET]."""
+        t = self.torch
+        B = U.shape[0]
+        nw = 2 * WIN + 1
+        x = t.empty(B, self.S, FEAT_SET, device=self.dev)
+        win = t.gather(U.float(), 1, self._widx_set[tid]).view(B, self.S, nw)
+        x[:, :, :nw] = win / self.x_scale[0]
+        x[:, :, nw] = (Vg.float() / self.x_scale[nw])[:, None]
+        x[:, :, nw + 1] = (Vds.float() / self.x_scale[nw + 1])[:, None]
+        x[:, :, nw + 2:] = self._fixed_set[tid]
+        return x.to(t.bfloat16).reshape(B * self.S, FEAT_SET)
+
+    # ------------------------------------------------------------------ training
+    def fit_set(self, U, Vg, Vds, tid, Q, epochs=20, batch=16, lr=2e-3, log=None):
+        """Train on canvas tensors U, Q [n][S] (float32), Vg, Vds [n], tid [n];
+        the loss covers every tube's own sites only."""
+        t = self.torch
+        n = U.shape[0]
+        nw = 2 * WIN + 1
+        self.x_scale = t.ones(FEAT_SET, device=self.dev)
+        self.x_scale[0] = float(U.abs().max())
+        self.x_scale[nw] = max(float(Vg.abs().max()), 1e-3)
+        self.x_scale[nw + 1] = max(float(Vds.abs().max()), 1e-3)
+        self.q_scale = float(Q.abs().max())
+        g = t.Generator(device="cpu").manual_seed(1)
+        hist = []
+        t0 = time.perf_counter()
+        steps = epochs * (n // batch)
+        for ep in range(epochs):
+            perm = t.randperm(n, generator=g)
+            tot, cnt = 0.0, 0.0
+            for i in range(n // batch):
+                idx = perm[i * batch:(i + 1) * batch].to(self.dev)
+                ti = tid[idx]
+                xb = self.features_set(U[idx], Vg[idx], Vds[idx], ti)
+                q = self.forward(xb, batch, keep=True)
+                m = self._mask_set[ti].reshape(-1)
+                q.mul_(m)
+                y = (Q[idx].reshape(-1) / self.q_scale).float().mul_(m)
+                dq, part = self.loss_grad(q, y)
+                dq.mul_(m)
+                self.backward(dq, batch)
+                frac = (ep * (n // batch) + i) / max(1, steps)
+                self.adam(lr=lr * 0.5 * (1 + math.cos(math.pi * frac)))
+                tot += float(part.sum())
+                cnt += float(m.sum())
+            hist.append(tot / max(cnt, 1.0))
+            if log:
+                log(ep, hist[-1])
+        t.cuda.synchronize()
+        return {"epochs": epochs, "seconds": time.perf_counter() - t0, "loss": hist}
+
+    def predict_set(self, U, Vg, Vds, tid, batch=16):
+        """Charge canvases [n][S] (float64) for canvas potentials U [n][S]."""
+        t = self.torch
+        n = U.shape[0]
+        out = t.empty(n, self.S, dtype=t.float64, device=self.dev)
+        for i in range(0, n, batch):
+            b = min(batch, n - i)
+            xb = self.features_set(U[i:i + b], Vg[i:i + b], Vds[i:i + b], tid[i:i + b])
+            q = self.forward(xb, b)
+            out[i:i + b] = (q[: b * self.S].reshape(b, self.S) * self.q_scale).double()
+        return out * self._mask_set[tid].double()
+
+    # ------------------------------------------------------------------ bound inference over the set
+    def bind_set(self, Ucat, Qcat, Vg, Vds):
+        """Fixed buffers for repeated inference over the whole set (capturable
+        after one call of infer_set): Ucat, Qcat float64 device vectors of the
+        concatenated tubes' sites (tube order as the descriptors)."""
+        t = self.torch
+        T, S, nw = len(self.desc), self.S, 2 * WIN + 1
+        # window index of every canvas site into Ucat, output index of every tube site into the canvas
+        wi = self._widx_set.view(T, S, nw) + t.tensor(self.offs[:-1], device=self.dev).view(T, 1, 1)
+        qi = np.concatenate([t_ * S + np.arange(N) for t_, N in enumerate(self.Ns)])
+        self._bs = dict(U=Ucat, Q=Qcat, widx=wi.reshape(-1).contiguous(), qidx=t.tensor(qi, device=self.dev),
+                        win=t.empty(T * S * nw, dtype=t.float64, device=self.dev),
+                        x=t.empty(T, S, FEAT_SET, device=self.dev),
+                        xb=t.empty(T * S, FEAT_SET, dtype=t.bfloat16, device=self.dev),
+                        qd=t.empty(T * S, dtype=t.float64, device=self.dev))
+        x = self._bs["x"]
+        x[:, :, nw + 2:] = self._fixed_set
+        self.set_bias_set(Vg, Vds)
+
+    def set_bias_set(self, Vg, Vds):
+        nw = 2 * WIN + 1
+        x = self._bs["x"]
+        x[:, :, nw] = float(Vg) / float(self.x_scale[nw])
+        x[:, :, nw + 1] = float(Vds) / float(self.x_scale[nw + 1])
+
+    def infer_set(self):
+        """Qcat = model(Ucat) over all tubes (no allocation after the first call)."""
+        t = self.torch
+        b = self._bs
+        T, S, nw = len(self.desc), self.S, 2 * WIN + 1
+        t.index_select(b["U"], 0, b["widx"], out=b["win"])
+        b["x"][:, :, :nw].copy_(b["win"].view(T, S, nw))
+        b["x"][:, :, :nw].div_(self.x_scale[0])
+        b["xb"].copy_(b["x"].view(T * S, FEAT_SET))
+        q = self.forward(b["xb"], T)
+        b["qd"].copy_(q)
+        t.index_select(b["qd"], 0, b["qidx"], out=b["Q"])
+        b["Q"].mul_(self.q_scale)
+
+
+# ---------------------------------------------------------------------- data
+def generate_set_pairs(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bins=13, scf_fraction=0.5,
+                       max_iter=40, S=None, log=None):
+    """n_pairs (canvas U, Vg, Vds, tube id, canvas Q) from the engine over the
+    tube set: half recorded along self-consistent solves of the whole set at
+    random gate Vg ~ U(0, 0.8) V and drain Vds ~ U(0, 0.6) V (vds_bins
+    levels: the tubes of one level share their energy paths), half from
+    random potentials of the config-2 recipe (the gate/contact stand-in's
+    external potential plus 5 seeded Gaussian bumps of amplitude up to a,
+    a ~ U(0, 0.4) V).  make_tubes(vds) returns the set's tubes at that drain
+    bias.  Returns device tensors and the seconds the engine spent."""
+    import torch
+    from .negf import Broyden, affine_potential_masked, compute_charge
+    from .scf import device_view
+    from .workloads import site_potential
+    rng = np.random.default_rng(seed)
+    levels = np.linspace(0.0, 0.6, vds_bins)
+    cache = {}
+    T = len(electros)
+    dev = "cuda"
+
+    def tubes_at(lv):
+        if lv not in cache:
+            cache[lv] = make_tubes(lv)
+        return cache[lv]
+
+    Ns = [e.N for e in electros]
+    S = int(S or ((max(Ns) + 255) // 256) * 256)
+    offs = np.concatenate([[0], np.cumsum(Ns)]).astype(np.int64)
+    Stot = int(offs[-1])
+    U_all = torch.zeros(n_pairs, S, dtype=torch.float32, device=dev)
+    Q_all = torch.zeros(n_pairs, S, dtype=torch.float32, device=dev)
+    vg_all = np.zeros(n_pairs)
+    vd_all = np.zeros(n_pairs)
+    tid_all = np.zeros(n_pairs, dtype=np.int64)
+    Qcat = torch.zeros(Stot, dtype=torch.float64, device=dev)
+    k = 0
+    engine = 0.0
+
+    def record(tubes, vg, lv):
+        nonlocal k
+        for t_, tube in enumerate(tubes):
+            if k >= n_pairs:
+                return
+            N = Ns[t_]
+            U_all[k, :N] = device_view(tube.potential_device_ptr(), N).float()
+            Q_all[k, :N] = Qcat[offs[t_]:offs[t_ + 1]].float()
+            vg_all[k], vd_all[k], tid_all[k] = vg, lv, t_
+            k += 1
+
+    def charge(tubes):
+        nonlocal engine
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        compute_charge(tubes, out=Qcat)
+        torch.cuda.synchronize()
+        engine += time.perf_counter() - t0
+
+    n_scf = int(n_pairs * scf_fraction)
+    while k < n_scf:  # pairs along self-consistent solves
+        lv = float(levels[rng.integers(0, vds_bins)])
+        vg = float(rng.uniform(0.0, 0.8))
+        tubes = tubes_at(lv)
+        ops = []
+        for e in electros:
+            e.Vds = lv
+            Kd, U0 = e.device_operator(vg)
+            ops.append((Kd, U0))
+        br = Broyden(torch.zeros(Stot, dtype=torch.float64, device=dev), max_step=max_iter + 2, fraction=0.1)
+        nin = br.input_device_ptr()
+        for _ in range(max_iter):
+            for (Kd, U0), o, tube, N in zip(ops, offs, tubes, Ns):
+                affine_potential_masked(Kd, U0, nin + 8 * int(o), tube.potential_device_ptr(), N, None)
+                U = device_view(tube.potential_device_ptr(), N)
+                ends = U[[0, N - 1]].cpu().numpy()
+                tube.set_potential_device(tube.potential_device_ptr(), (float(ends[0]), float(ends[1])))
+            charge(tubes)
+            record(tubes, vg, lv)
+            if not (br.step(Qcat) > 1e-6) or k >= n_scf:
+                break
+        br.close()
+        if log:
+            log("scf", k)
+    while k < n_pairs:  # random potentials of the config-2 recipe
+        lv = float(levels[rng.integers(0, vds_bins)])
+        vg = float(rng.uniform(0.0, 0.8))
+        tubes = tubes_at(lv)
+        for t_, (tube, e) in enumerate(zip(tubes, electros)):
+            e.Vds = lv
+            amp = rng.uniform(0.0, 0.4)
+            U = e.external(vg) + site_potential(e.y_nm, int(rng.integers(1 << 30)), amp=amp, ramp=0.0)
+            tube.set_potential(U, (U[0], U[-1]))
+        charge(tubes)
+        record(tubes, vg, lv)
+        if log:
+            log("random", k)
+    for tubes in cache.values():
+        for tube in tubes:
+            tube.close()
+    return (U_all, torch.tensor(vg_all, dtype=torch.float32, device=dev),
+            torch.tensor(vd_all, dtype=torch.float32, device=dev), torch.tensor(tid_all, device=dev), Q_all, engine)
+
+
+# ---------------------------------------------------------------------- SCF
+def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6, max_step=200, switch_norm=1e-5,
+                  surrogate_norm=1e-6, surrogate_max_step=60, keep_rows=80, iters_per_graph=4, power_iters=6,
+                  autotune=True):
+    """Surrogate-started gate sweep of a tube set (module docstring).  Tubes
+    in mixed precision run the NEGF phase on their own plan until the
+    residual falls below switch_norm, then on an FP64 plan.  fraction: the
+    scalar part of the initial inverse Jacobian (None: from the surrogate's
+    Jacobian).  Returns per-step records, the chosen fraction and the
+    one-off set-up seconds (plans, graphs; outside the per-step times)."""
+    import torch
+    from . import negf as ng
+    from .scf import device_view
+    dev = "cuda"
+    Ns = [t.num_field_sites for t in tubes]
+    offs = np.concatenate([[0], np.cumsum(Ns)]).astype(np.int64)
+    S = int(offs[-1])
+    stream = torch.cuda.Stream()
+    t_setup = time.perf_counter()
+    out = []
+    with torch.cuda.stream(stream):
+        Q = torch.zeros(S, dtype=torch.float64, device=dev)
+        Qs = torch.zeros(S, dtype=torch.float64, device=dev)
+        Ucat = torch.zeros(S, dtype=torch.float64, device=dev)
+        ops = []
+        for e in electros:
+            Kd, U0 = e.device_operator(Vg_list[0])
+            ops.append((Kd, U0.clone()))
+        U_ptrs = [t.potential_device_ptr() for t in tubes]
+        model.bind_set(Ucat, Qs, Vg_list[0], electros[0].Vds)
+        # surrogate-phase residual map F_s(n) = n - Q_s(U0 + K n) for the power iteration
+        ncur = torch.zeros(S, dtype=torch.float64, device=dev)
+
+        def F_s(n):
+            for (Kd, U0), o, N in zip(ops, offs, Ns):
+                ng.affine_potential_masked(Kd, U0, n.data_ptr() + 8 * int(o), Ucat.data_ptr() + 8 * int(o), N, None,
+                                           stream=stream)
+            model.infer_set()
+            return n - Qs
+
+        F_s(ncur)  # allocates the model's inference buffers
+        stream.synchronize()
+        t_setup = time.perf_counter() - t_setup
+        # ---- timed from here: the scalar part of G0 from the surrogate's Jacobian
+        t0 = time.perf_counter()
+        alpha = fraction
+        lam = None
+        if alpha is None:
+            g = torch.Generator(device="cpu").manual_seed(0)
+            v = torch.randn(S, generator=g, dtype=torch.float64).to(dev)
+            v /= v.norm()
+            F0 = F_s(ncur).clone()
+            eps = 1e-2 * float(model.q_scale)
+            for _ in range(power_iters):
+                w = (F_s(ncur + eps * v) - F0) / eps
+                lam = float(w.norm())
+                v = w / lam
+            alpha = float(min(1.0, max(0.1, 2.0 / (1.0 + lam))))
+        t_alpha = time.perf_counter() - t0
+        t_setup2 = time.perf_counter()
+        brn = ng.Broyden(torch.zeros(S, dtype=torch.float64, device=dev), max_step=max_step, fraction=alpha,
+                         stream=stream)
+        brs = ng.Broyden(torch.zeros(S, dtype=torch.float64, device=dev), max_step=max_step, fraction=alpha,
+                         stream=stream)
+        nin = brn.input_device_ptr()
+        nin_s = brs.input_device_ptr()
+        nin_t = device_view(nin, S)
+        nin_s_t = device_view(nin_s, S)
+        flags = torch.zeros(8, dtype=torch.int32, device=dev)
+        flags_s = torch.zeros(8, dtype=torch.int32, device=dev)
+        skip = flags.data_ptr() + 12
+        switch = switch_norm is not None and switch_norm > 0 and any(t.desc.precision == 1 for t in tubes)
+        for (Kd, U0), o, N, Up in zip(ops, offs, Ns, U_ptrs):
+            ng.affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, None, stream=stream)
+        plan = ng.ChargePlan(tubes, Q, autotune=autotune)
+        plan64 = ng.ChargePlan(tubes, Q, autotune=autotune, fp64=True) if switch else None
+
+        def body(s):
+            for (Kd, U0), o, N, Up in zip(ops, offs, Ns, U_ptrs):
+                ng.affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip, stream=s)
+            if switch:
+                plan.launch(skip=flags.data_ptr() + 5 * 4, stream=s)
+                plan64.launch(skip=flags.data_ptr() + 6 * 4, stream=s)
+                brn.step_device_switch(Q, max_norm, switch_norm, flags, stream=s)
+            else:
+                plan.launch(skip=skip, stream=s)
+                brn.step_device(Q, max_norm, flags, stream=s)
+
+        def sbody(s):
+            sk = flags_s.data_ptr() + 12
+            for (Kd, U0), o, N in zip(ops, offs, Ns):
+                ng.affine_potential_masked(Kd, U0, nin_s + 8 * int(o), Ucat.data_ptr() + 8 * int(o), N, sk, stream=s)
+            model.infer_set()
+            brs.step_device(Qs, surrogate_norm, flags_s, stream=s)
+
+        flags[3] = 1
+        flags_s[3] = 1
+        body(stream)
+        sbody(stream)
+        stream.synchronize()
+        graph, sgraph = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            for _ in range(iters_per_graph):
+                body(torch.cuda.current_stream())
+        with torch.cuda.graph(sgraph, stream=stream):
+            for _ in range(iters_per_graph):
+                sbody(torch.cuda.current_stream())
+        stream.synchronize()
+        t_setup += time.perf_counter() - t_setup2
+        for step, Vg in enumerate(Vg_list):
+            t0 = time.perf_counter()
+            for (Kd, U0), e in zip(ops, electros):
+                U0.copy_(e.device_operator(Vg)[1])
+            model.set_bias_set(Vg, electros[0].Vds)
+            # (1) surrogate phase, continued from the previous gate step
+            if step > 0:
+                brs.restart(keep_rows=keep_rows, stream=stream)
+            flags_s.zero_()
+            while True:
+                sgraph.replay()
+                fs = flags_s.cpu().numpy()
+                if fs[3] or fs[1] >= surrogate_max_step:
+                    break
+            sur_it = int(fs[1])
+            used = bool(fs[0]) and not fs[2]
+            # (2) NEGF phase from the surrogate's charge
+            if step == 0:
+                if used:
+                    V, W, rows = brs.history(stream=stream)
+                    k = min(rows, max_step // 2)
+                    brn.set_initial_jacobian(V[rows - k:].contiguous() if k else None,
+                                             W[rows - k:].contiguous() if k else None, stream=stream)
+            else:
+                brn.restart(keep_rows=keep_rows, stream=stream)
+            if used:
+                nin_t.copy_(nin_s_t)
+            flags.zero_()
+            if switch:
+                flags[6] = 1
+            while True:
+                graph.replay()
+                f = flags.cpu().numpy()
+                if f[3]:
+                    break
+            dt = time.perf_counter() - t0 + (t_alpha if step == 0 else 0.0)
+            if f[2]:
+                raise RuntimeError("NEGF self-consistency failed (flag %d) at Vg = %g" % (f[2], Vg))
+            out.append(dict(Vg=float(Vg), negf_iterations=int(f[1]), lowprec_iterations=int(f[7]),
+                            surrogate_iterations=sur_it, surrogate_used=used, seconds=dt, Q=Q.cpu().numpy().copy(),
+                            n_in=nin_t.cpu().numpy().copy()))
+        stream.synchronize()
+    del graph, sgraph
+    plan.close()
+    if plan64 is not None:
+        plan64.close()
+    brn.close()
+    brs.close()
+    return out, alpha, lam, t_setup

@@ -393,6 +393,21 @@ int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void
  * rows count against max_step.  A reset clears them.  The row count lives
  * in device memory, so launches captured earlier see it. */
 int negf_broyden_set_initial_jacobian(negf_broyden* b, const double* d_V, const double* d_W, int k, void* stream);
+/* Start the next solve keeping the secant rows of the solves so far as its
+ * initial inverse Jacobian (no counterpart in the reference, whose
+ * Reset_Broyden_Parallel clears them, Broyden_Parallel_General.cpp:250-355):
+ * the next step is step 1 and G0 = fraction * I + sum_j w_j v_j^T over the
+ * most recent min(keep_rows, max_step / 2) rows (older rows are dropped).
+ * Along a bias sweep the Jacobian changes little from one bias point to the
+ * next, so the rows carry over.  n_in stays (set a new start with
+ * negf_broyden_set_input); the kept rows count against max_step.
+ * Synchronises `stream` (it reads the step counters). */
+int negf_broyden_restart(negf_broyden* b, int keep_rows, void* stream);
+/* The secant rows held now (seeded rows first): device pointers of rows
+ * 1 .. *rows of V and W ([rows][S] each, valid until the next step, reset or
+ * restart), e.g. to seed another Broyden with negf_broyden_set_initial_jacobian
+ * (no counterpart in the reference).  Synchronises `stream`. */
+int negf_broyden_history(negf_broyden* b, double** d_V, double** d_W, int* rows, void* stream);
 /* Broyden_Step (1-based). */
 int negf_broyden_step_number(negf_broyden* b, int* step);
 /* Device-resident Broyden step (no host synchronisation; capturable in a

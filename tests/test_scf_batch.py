@@ -120,6 +120,53 @@ def test_broyden_initial_jacobian_exact_inverse():
         small.set_initial_jacobian(V, W)
 
 
+def _np_broyden(n, F_of, steps, alpha, W=None, V=None):
+    """Modified-second Broyden in numpy (Broyden_Second_Parallel.cpp:9-211)
+    starting from secant rows W, V; returns the iterates and the rows."""
+    W, V = list(W or []), list(V or [])
+    Fp = npv = None
+    out = []
+    for _ in range(steps):
+        F = F_of(n)
+        if Fp is not None:
+            dF = F - Fp
+            s = sum(w * (v @ dF) for w, v in zip(W, V)) if W else 0.0
+            W.append(-alpha * dF + (n - npv) - s)
+            V.append(dF / (dF @ dF))
+        step = alpha * F + (sum(w * (v @ F) for w, v in zip(W, V)) if W else 0.0)
+        Fp, npv = F, n.copy()
+        n = n - step
+        out.append(n.copy())
+    return out, W, V
+
+
+@pytest.mark.parametrize("keep", [100, 3, 0])
+def test_broyden_restart_carries_rows(keep):
+    """negf_broyden_restart: a second solve (another linear map, as at the next
+    bias point) starts from the first solve's secant rows (the most recent
+    `keep`), matching the numpy twin step by step."""
+    import torch
+    from electrostatic_b200.negf import Broyden
+    S = 24
+    rng = np.random.default_rng(7)
+    A1 = 0.5 * rng.standard_normal((S, S)) / np.sqrt(S)
+    A2 = A1 + 0.05 * rng.standard_normal((S, S)) / np.sqrt(S)
+    b1, b2 = rng.standard_normal(S), rng.standard_normal(S)
+    alpha = 0.3
+    n0 = np.zeros(S)
+    it1, W, V = _np_broyden(n0, lambda n: n - (A1 @ n + b1), 6, alpha)
+    W, V = (W[len(W) - keep:], V[len(V) - keep:]) if keep else ([], [])
+    it2, _, _ = _np_broyden(it1[-1], lambda n: n - (A2 @ n + b2), 5, alpha, W, V)
+    br = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"), max_step=60, fraction=alpha)
+    for A, b, ref in ((A1, b1, it1), (A2, b2, it2)):
+        for k in range(len(ref)):
+            x = torch.from_numpy(A @ _read(br.input_device_ptr(), S) + b).cuda()
+            br.step(x)
+            np.testing.assert_allclose(_read(br.input_device_ptr(), S), ref[k], rtol=1e-9, atol=1e-12)
+        br.restart(keep_rows=keep)
+        assert br.step_number == 1
+
+
 def _read(ptr, n):
     from electrostatic_b200.scf import device_view
     return device_view(ptr, n).cpu().numpy()
