@@ -42,6 +42,72 @@ def _stream(stream):
     return C.c_void_p(stream.cuda_stream)
 
 
+def tube_desc(type_id=(17, 0), num_unitcells=100, num_modes=1, acc=1.42e-10, gamma=2.5,
+              contact_T=(298.0, 298.0), contact_mu=(0.0, 0.0), eq_integration_pts=(30, 30, 30),
+              noneq_integration_pts=(100,), noneq_percent_intercuts=None, E_valence_min=-14.0,
+              E_pole_max=10.0, E_zPlus_imag=1e-8, Fermi_tail_factors=(14.0, 14.0), use_decimation=0,
+              decimation_max_iter=30, decimation_layers=10, realaxis_window=None, precision="fp64",
+              mixed_fp64_band=1e-3, flatband_dos_integration_pts=100, flag_adaptive_integration_limits=0,
+              integrand_correction_interval=500, kT_window_around_singularity=(1.0, 1.0),
+              noneq_integration_pts_density=None, mixed_realaxis_fp32=False):
+    """negf_tube_desc of the keyword arguments of CNT (host only; no device needed)."""
+    L = _lib.load()
+    d = _lib.TubeDesc()
+    check(L.negf_tube_desc_init(C.byref(d)), "negf_tube_desc_init")
+    d.type_id[0], d.type_id[1] = int(type_id[0]), int(type_id[1])
+    d.num_unitcells = int(num_unitcells)
+    d.num_modes = int(num_modes)
+    d.acc = float(acc)
+    d.gamma = float(gamma)
+    d.contact_T[0], d.contact_T[1] = map(float, contact_T)
+    d.contact_mu[0], d.contact_mu[1] = map(float, contact_mu)
+    for i in range(3):
+        d.eq_integration_pts[i] = int(eq_integration_pts[i])
+    ne = list(noneq_integration_pts)
+    d.num_noneq_paths = len(ne)
+    for i, v in enumerate(ne):
+        d.noneq_integration_pts[i] = int(v)
+    if noneq_percent_intercuts is None:
+        d.noneq_percent_intercuts[0] = -1.0
+    else:
+        for i, v in enumerate(noneq_percent_intercuts):
+            d.noneq_percent_intercuts[i] = float(v)
+    d.E_valence_min = float(E_valence_min)
+    d.E_pole_max = float(E_pole_max)
+    d.E_zPlus_imag = float(E_zPlus_imag)
+    d.Fermi_tail_factors[0], d.Fermi_tail_factors[1] = map(float, Fermi_tail_factors)
+    d.use_decimation = int(use_decimation)
+    d.decimation_max_iter = int(decimation_max_iter)
+    d.decimation_layers = int(decimation_layers)
+    if realaxis_window is not None:
+        lo, hi, pts, kind = realaxis_window
+        d.realaxis_min, d.realaxis_max, d.realaxis_pts, d.realaxis_kind = float(lo), float(hi), int(pts), int(kind)
+    d.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
+    d.mixed_fp64_band = float(mixed_fp64_band)
+    d.mixed_realaxis_fp32 = int(bool(mixed_realaxis_fp32))
+    d.flatband_dos_integration_pts = int(flatband_dos_integration_pts)
+    d.flag_adaptive_integration_limits = int(flag_adaptive_integration_limits)
+    d.integrand_correction_interval = int(integrand_correction_interval)
+    d.kT_window_around_singularity[0], d.kT_window_around_singularity[1] = map(float, kT_window_around_singularity)
+    if noneq_integration_pts_density is not None:
+        d.flag_noneq_integration_pts_density = 1
+        for i, v in enumerate(noneq_integration_pts_density):
+            d.noneq_integration_pts_density[i] = float(v)
+    return d
+
+
+def desc_energy_points(desc, kind: int):
+    """Energy-point tables of a descriptor (host only): kind 0 Rho0, 1 RhoEq
+    contour, 2 poles, 3 NonEq -> (E, w, J) complex arrays."""
+    L = _lib.load()
+    n = C.c_int()
+    check(L.negf_desc_energy_points(C.byref(desc), int(kind), None, C.byref(n)), "negf_desc_energy_points")
+    buf = np.zeros(6 * max(n.value, 1))
+    check(L.negf_desc_energy_points(C.byref(desc), int(kind), _dptr(buf), C.byref(n)), "negf_desc_energy_points")
+    b = buf[: 6 * n.value].reshape(-1, 6)
+    return b[:, 0] + 1j * b[:, 1], b[:, 2] + 1j * b[:, 3], b[:, 4] + 1j * b[:, 5]
+
+
 class CNT:
     """Mode-space zigzag carbon nanotube (c_CNT) on the GPU.
 
@@ -66,56 +132,39 @@ class CNT:
                  mixed_fp64_band=1e-3, flatband_dos_integration_pts=100, flag_adaptive_integration_limits=0,
                  integrand_correction_interval=500, kT_window_around_singularity=(1.0, 1.0),
                  noneq_integration_pts_density=None, mixed_realaxis_fp32=False):
-        L = _lib.load()
-        d = _lib.TubeDesc()
-        check(L.negf_tube_desc_init(C.byref(d)), "negf_tube_desc_init")
-        d.type_id[0], d.type_id[1] = int(type_id[0]), int(type_id[1])
-        d.num_unitcells = int(num_unitcells)
-        d.num_modes = int(num_modes)
-        d.acc = float(acc)
-        d.gamma = float(gamma)
-        d.contact_T[0], d.contact_T[1] = map(float, contact_T)
-        d.contact_mu[0], d.contact_mu[1] = map(float, contact_mu)
-        for i in range(3):
-            d.eq_integration_pts[i] = int(eq_integration_pts[i])
-        ne = list(noneq_integration_pts)
-        d.num_noneq_paths = len(ne)
-        for i, v in enumerate(ne):
-            d.noneq_integration_pts[i] = int(v)
-        if noneq_percent_intercuts is None:
-            d.noneq_percent_intercuts[0] = -1.0
-        else:
-            for i, v in enumerate(noneq_percent_intercuts):
-                d.noneq_percent_intercuts[i] = float(v)
-        d.E_valence_min = float(E_valence_min)
-        d.E_pole_max = float(E_pole_max)
-        d.E_zPlus_imag = float(E_zPlus_imag)
-        d.Fermi_tail_factors[0], d.Fermi_tail_factors[1] = map(float, Fermi_tail_factors)
-        d.use_decimation = int(use_decimation)
-        d.decimation_max_iter = int(decimation_max_iter)
-        d.decimation_layers = int(decimation_layers)
-        if realaxis_window is not None:
-            lo, hi, pts, kind = realaxis_window
-            d.realaxis_min, d.realaxis_max, d.realaxis_pts, d.realaxis_kind = float(lo), float(hi), int(pts), int(kind)
-        d.precision = {"fp64": _lib.NEGF_PREC_FP64, "mixed": _lib.NEGF_PREC_MIXED}[precision]
-        d.mixed_fp64_band = float(mixed_fp64_band)
-        d.mixed_realaxis_fp32 = int(bool(mixed_realaxis_fp32))
-        d.flatband_dos_integration_pts = int(flatband_dos_integration_pts)
-        d.flag_adaptive_integration_limits = int(flag_adaptive_integration_limits)
-        d.integrand_correction_interval = int(integrand_correction_interval)
-        d.kT_window_around_singularity[0], d.kT_window_around_singularity[1] = map(float, kT_window_around_singularity)
-        if noneq_integration_pts_density is not None:
-            d.flag_noneq_integration_pts_density = 1
-            for i, v in enumerate(noneq_integration_pts_density):
-                d.noneq_integration_pts_density[i] = float(v)
+        d = tube_desc(type_id=type_id, num_unitcells=num_unitcells, num_modes=num_modes, acc=acc, gamma=gamma,
+                      contact_T=contact_T, contact_mu=contact_mu, eq_integration_pts=eq_integration_pts,
+                      noneq_integration_pts=noneq_integration_pts, noneq_percent_intercuts=noneq_percent_intercuts,
+                      E_valence_min=E_valence_min, E_pole_max=E_pole_max, E_zPlus_imag=E_zPlus_imag,
+                      Fermi_tail_factors=Fermi_tail_factors, use_decimation=use_decimation,
+                      decimation_max_iter=decimation_max_iter, decimation_layers=decimation_layers,
+                      realaxis_window=realaxis_window, precision=precision, mixed_fp64_band=mixed_fp64_band,
+                      flatband_dos_integration_pts=flatband_dos_integration_pts,
+                      flag_adaptive_integration_limits=flag_adaptive_integration_limits,
+                      integrand_correction_interval=integrand_correction_interval,
+                      kT_window_around_singularity=kT_window_around_singularity,
+                      noneq_integration_pts_density=noneq_integration_pts_density,
+                      mixed_realaxis_fp32=mixed_realaxis_fp32)
         self.desc = d
         h = C.c_void_p()
+        L = _lib.load()
         check(L.negf_tube_create(C.byref(d), C.byref(h)), "negf_tube_create")
         self._h = h
         n = C.c_int()
         check(L.negf_tube_num_sites(h, C.byref(n)), "negf_tube_num_sites")
         self.num_field_sites = n.value
         self.U_contact = (0.0, 0.0)
+
+    @classmethod
+    def from_deck(cls, deck, name: str, **overrides):
+        """The nanostructure `name` of a ParmParse-format deck (inputs.Deck or
+        a file path): NS_default / CNT_default layered under the name's keys."""
+        from .inputs import Deck
+        if isinstance(deck, str):
+            deck = Deck.from_file(deck)
+        kw = deck.tube_kwargs(name)
+        kw.update(overrides)
+        return cls(**kw)
 
     def close(self):
         if getattr(self, "_h", None):
