@@ -631,7 +631,7 @@ def main():
 
     # ---- the same workload in the mixed path
     mixed = None
-    Q_mixed = None
+    Q_mixed = Q_mixed_all = None
     if args.precision == "fp64" and world == 1:
         tm = CNT(**tube_kwargs("mixed"))
         tm.set_potential(U, Uc)
@@ -656,6 +656,31 @@ def main():
                  "updates_fp32": sm["updates_fp32"], "updates": sm["updates"],
                  "rule": MIXED_RULE,
                  "max_rel_vs_fp64": float(np.max(np.abs(Q_mixed - Q_dev)) / np.max(np.abs(Q_dev)))}
+        # opt-in outside that rule: the band lowered to the 1e-4 eV broadening, so the
+        # real-axis chains run in FP32 as well (all but the lead band-edge chains)
+        ta = CNT(**dict(tube_kwargs("mixed"), mixed_fp64_band=ETA, mixed_realaxis_fp32=True))
+        ta.set_potential(U, Uc)
+        for _ in range(3):
+            compute_charge([ta], out=Qm, stream=stream)
+        mev = []
+        for i in range(nm):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.zero_()
+            a.record(stream)
+            compute_charge([ta], out=Qm, stream=stream)
+            b.record(stream)
+            mev.append((a, b))
+        torch.cuda.synchronize()
+        sa = last_stats()
+        ams = float(np.mean([a.elapsed_time(b) for a, b in mev]))
+        Q_mixed_all = Qm.cpu().numpy()
+        mixed["realaxis_fp32_opt_in"] = {
+            "ms_per_pass": ams, "speedup_vs_fp64": (t_max / args.steps) / ams, "updates_fp32": sa["updates_fp32"],
+            "rule": "mixed_fp64_band = 1e-4 eV (the broadening) and mixed_realaxis_fp32: every chain in FP32 but "
+                    "those within 1e-4 eV of a lead band edge (outside the 1e-3 eV FP64 band of the design rule)",
+            "max_rel_vs_fp64": float(np.max(np.abs(Q_mixed_all - Q_dev)) / np.max(np.abs(Q_dev)))}
+        ta.close()
+        tm.close()
 
     # ---- both RGF schedules on the same tube (kernel time per pass, CUDA events)
     schedules = None
@@ -729,6 +754,7 @@ def main():
                       "bars": {"fp64": 1e-8, "mixed": 1e-5}}
             if Q_mixed is not None:
                 parity["mixed_max_rel_vs_oracle"] = float(np.max(np.abs(Q_mixed - Qo)) / qmax)
+                parity["mixed_realaxis_fp32_opt_in_max_rel_vs_oracle"] = float(np.max(np.abs(Q_mixed_all - Qo)) / qmax)
         scf = None if (args.no_scf or world > 1) else scf_measure(len(os.sched_getaffinity(0)))
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
         cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch, small=args.small)
