@@ -1701,10 +1701,12 @@ int negf_broyden_restart(negf_broyden* b, int keep_rows, void* stream) {
     int st[2] = {1, 0};
     NEGF_CUDA(cudaMemcpyAsync(st, d.step_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     NEGF_CUDA(cudaStreamSynchronize(s));
-    // rows 1 .. base are seeds, the solve added one row per step after its first
+    // rows 1 .. base are seeds, the solve added one row per step after its first.
+    // Every row is a correction on top of the rows before it, so a subset that
+    // drops the oldest rows is no consistent inverse Jacobian: keep all of them,
+    // or none once they exceed the limit.
     const int rows = st[1] + std::max(0, st[0] - 2);
-    const int keep = std::min(std::min(rows, keep_rows), d.max_step / 2);
-    NEGF_CUDA(negf::broyden_shift_rows(d, rows - keep, keep, s));
+    const int keep = rows <= std::min(keep_rows, d.max_step / 2) ? rows : 0;
     d.base = keep;
     b->step = 1;
     NEGF_CUDA(negf::set_int(d.step_dev, 1, s));

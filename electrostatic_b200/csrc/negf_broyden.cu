@@ -206,15 +206,6 @@ __global__ void step_kernel(BroydenDev b, double max_norm, double switch_norm, i
     }
 }
 
-// Rows from + 1 .. from + count of V and W move to rows 1 .. count (ascending:
-// a source row is read before any write reaches it).
-__global__ void shift_rows_kernel(double* V, double* W, int S, int from, int count) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x)
-        for (int r = 1; r <= count; ++r) {
-            V[(size_t)r * S + s] = V[(size_t)(r + from) * S + s];
-            W[(size_t)r * S + s] = W[(size_t)(r + from) * S + s];
-        }
-}
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
 __global__ void set_kernel(double* p, double v, int n) {
@@ -265,12 +256,6 @@ cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int
 
 cudaError_t broyden_finish_step(const BroydenDev& b, double max_norm, double switch_norm, int* flags, cudaStream_t s) {
     step_kernel<<<1, 1, 0, s>>>(b, max_norm, switch_norm, flags);
-    return cudaGetLastError();
-}
-
-cudaError_t broyden_shift_rows(const BroydenDev& b, int from, int count, cudaStream_t s) {
-    if (from <= 0 || count <= 0) return cudaSuccess;
-    shift_rows_kernel<<<b.nblocks, kThreads, 0, s>>>(b.V, b.W, b.S, from, count);
     return cudaGetLastError();
 }
 

@@ -198,8 +198,6 @@ cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int
 // Device-resident step end: flags int[4] = converged, iterations, error
 // (1 MaxStep exceeded, 2 non-finite norm), skip; advances *step_dev.
 cudaError_t broyden_finish_step(const BroydenDev& b, double max_norm, double switch_norm, int* flags, cudaStream_t s);
-// Rows from + 1 .. from + count of V and W become rows 1 .. count.
-cudaError_t broyden_shift_rows(const BroydenDev& b, int from, int count, cudaStream_t s);
 cudaError_t set_int(int* p, int v, cudaStream_t s);
 cudaError_t broyden_set(double* p, double v, int n, cudaStream_t s);
 cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s,

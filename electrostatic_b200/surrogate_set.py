@@ -359,8 +359,11 @@ def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6,
             v = torch.randn(S, generator=g, dtype=torch.float64).to(dev)
             v /= v.norm()
             F0 = F_s(ncur).clone()
-            eps = 1e-2 * float(model.q_scale)
+            # the surrogate reads BF16 potentials (about 2e-3 V resolution here): size each
+            # step so that the potential moves by about 0.02 V
+            kmax = max(float(Kd.abs().sum(dim=1).max()) for Kd, _ in ops)
             for _ in range(power_iters):
+                eps = 0.02 / (kmax * float(v.abs().max()))
                 w = (F_s(ncur + eps * v) - F0) / eps
                 lam = float(w.norm())
                 v = w / lam

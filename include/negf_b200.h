@@ -396,11 +396,13 @@ int negf_broyden_set_initial_jacobian(negf_broyden* b, const double* d_V, const 
 /* Start the next solve keeping the secant rows of the solves so far as its
  * initial inverse Jacobian (no counterpart in the reference, whose
  * Reset_Broyden_Parallel clears them, Broyden_Parallel_General.cpp:250-355):
- * the next step is step 1 and G0 = fraction * I + sum_j w_j v_j^T over the
- * most recent min(keep_rows, max_step / 2) rows (older rows are dropped).
- * Along a bias sweep the Jacobian changes little from one bias point to the
- * next, so the rows carry over.  n_in stays (set a new start with
- * negf_broyden_set_input); the kept rows count against max_step.
+ * the next step is step 1 and G0 = fraction * I + sum_j w_j v_j^T over all
+ * rows held, if there are at most min(keep_rows, max_step / 2) of them, else
+ * over none (each row corrects the rows before it, so dropping the oldest
+ * rows would leave no consistent inverse Jacobian).  Along a bias sweep the
+ * Jacobian changes little from one bias point to the next, so the rows carry
+ * over.  n_in stays (set a new start with negf_broyden_set_input); the kept
+ * rows count against max_step.
  * Synchronises `stream` (it reads the step counters). */
 int negf_broyden_restart(negf_broyden* b, int keep_rows, void* stream);
 /* The secant rows held now (seeded rows first): device pointers of rows
