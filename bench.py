@@ -385,7 +385,7 @@ def long_tube_measure(torch, reps=10):
             "max_rel_automatic_vs_one_piece": float(np.max(np.abs(Qa - Q1)) / np.max(np.abs(Q1)))}
 
 
-def config5_measure(torch, n_pairs=20000, epochs=20, oracle_check=True):
+def config5_measure(torch, n_pairs=12000, epochs=10, oracle_check=True):
     """Surrogate-assisted self-consistency on the config-4 tube set (16
     tubes): one Fourier operator for the whole set (6 layers, width 128, 32
     frequencies, BF16 weights, FP32 accumulation) trained on n_pairs (U, Q)
@@ -433,11 +433,17 @@ def config5_measure(torch, n_pairs=20000, epochs=20, oracle_check=True):
     # plain FP64 sweep (warm-up on one gate point first: plans, graphs, lazy loading)
     run_scf_batch(tubes64, electros, [0.0], use_graph=True, iters_per_graph=4)
     plain = run_scf_batch(tubes64, electros, GATE_SWEEP, use_graph=True, iters_per_graph=4)
+    # the same with the charge carried between gate points (the validation decks'
+    # reset_with_previous_charge_distribution = 1)
+    cont = run_scf_batch(tubes64, electros, GATE_SWEEP, use_graph=True, iters_per_graph=4,
+                         reset_with_previous_charge=True)
     # surrogate-started, mixed precision (contour and real-axis chains in FP32 at 2 meV broadening)
     tubesmx = make(vds, precision="mixed", realaxis_fp32=True)
     set_scf_sweep(tubesmx, electros, [0.0], model)  # warm-up
     sur, alpha, lam, t_setup = set_scf_sweep(tubesmx, electros, GATE_SWEEP, model)
+    sur_c, _, _, _ = set_scf_sweep(tubesmx, electros, GATE_SWEEP, model, carry_rows=True)
     t_plain = sum(s_.seconds for s_ in plain.steps)
+    t_cont = sum(s_.seconds for s_ in cont.steps)
     t_sur = sum(r["seconds"] for r in sur)
     dq = max(float(np.max(np.abs(r["Q"] - s_.Q))) / float(np.max(np.abs(s_.Q))) for r, s_ in zip(sur, plain.steps))
     res = {"workload": "config-4 tube set (16 tubes), Vds 0.4 V, Vg 0..0.6 V step 0.05, 1e-6 absolute max-norm; "
@@ -457,7 +463,14 @@ def config5_measure(torch, n_pairs=20000, epochs=20, oracle_check=True):
                                            "below 1e-5); start = surrogate self-consistent charge; initial inverse "
                                            "Jacobian = surrogate secant rows (first gate point), carried NEGF rows "
                                            "after, fraction 2/(1+lambda_max) of the surrogate Jacobian"},
-           "speedup": t_plain / t_sur, "max_rel_dQ_vs_plain_fp64": dq}
+           "plain_continuation": {"iterations": [s_.iterations for s_ in cont.steps], "seconds": t_cont,
+                                  "method": "as plain, n_in carried from the previous gate point"},
+           "surrogate_carry_rows": {"negf_iterations": [r["negf_iterations"] for r in sur_c],
+                                    "seconds": sum(r["seconds"] for r in sur_c),
+                                    "method": "as surrogate_started, but the NEGF secant rows of the previous "
+                                              "gate points (negf_broyden_restart) instead of the surrogate's"},
+           "speedup": t_plain / t_sur, "speedup_vs_plain_continuation": t_cont / t_sur,
+           "max_rel_dQ_vs_plain_fp64": dq}
     if oracle_check:
         # the FP64 oracle's charge at the converged potential of the last gate point (fixed-point check)
         from oracle import oracle as O

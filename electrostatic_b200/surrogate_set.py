@@ -113,7 +113,7 @@ class TubeSetOperator(FourierOperator):
         return x.to(t.bfloat16).reshape(B * self.S, FEAT_SET)
 
     # ------------------------------------------------------------------ training
-    def fit_set(self, U, Vg, Vds, tid, Q, epochs=20, batch=16, lr=2e-3, log=None):
+    def fit_set(self, U, Vg, Vds, tid, Q, epochs=20, batch=32, lr=2e-3, log=None):
         """Train on canvas tensors U, Q [n][S] (float32), Vg, Vds [n], tid [n];
         the loss covers every tube's own sites only."""
         t = self.torch
@@ -130,7 +130,8 @@ class TubeSetOperator(FourierOperator):
         steps = epochs * (n // batch)
         for ep in range(epochs):
             perm = t.randperm(n, generator=g)
-            tot, cnt = 0.0, 0.0
+            tot = t.zeros((), dtype=t.float64, device=self.dev)
+            cnt = t.zeros((), dtype=t.float64, device=self.dev)
             for i in range(n // batch):
                 idx = perm[i * batch:(i + 1) * batch].to(self.dev)
                 ti = tid[idx]
@@ -144,9 +145,9 @@ class TubeSetOperator(FourierOperator):
                 self.backward(dq, batch)
                 frac = (ep * (n // batch) + i) / max(1, steps)
                 self.adam(lr=lr * 0.5 * (1 + math.cos(math.pi * frac)))
-                tot += float(part.sum())
-                cnt += float(m.sum())
-            hist.append(tot / max(cnt, 1.0))
+                tot += part.sum()
+                cnt += m.sum()
+            hist.append(float(tot) / max(float(cnt), 1.0))
             if log:
                 log(ep, hist[-1])
         t.cuda.synchronize()
@@ -309,8 +310,8 @@ def generate_set_pairs(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bin
 
 # ---------------------------------------------------------------------- SCF
 def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6, max_step=200, switch_norm=1e-5,
-                  surrogate_norm=1e-6, surrogate_max_step=60, keep_rows=80, iters_per_graph=4, power_iters=6,
-                  autotune=True):
+                  surrogate_norm=1e-6, surrogate_max_step=60, seed_rows=True, carry_rows=False, iters_per_graph=4,
+                  power_iters=6, autotune=True):
     """Surrogate-started gate sweep of a tube set (module docstring).  Tubes
     in mixed precision run the NEGF phase on their own plan until the
     residual falls below switch_norm, then on an FP64 plan.  fraction: the
@@ -424,9 +425,9 @@ def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6,
             for (Kd, U0), e in zip(ops, electros):
                 U0.copy_(e.device_operator(Vg)[1])
             model.set_bias_set(Vg, electros[0].Vds)
-            # (1) surrogate phase, continued from the previous gate step
-            if step > 0:
-                brs.restart(keep_rows=keep_rows, stream=stream)
+            # (1) surrogate phase: a fresh Broyden solve with the surrogate's charge,
+            # continued from the surrogate's previous fixed point
+            brs.reset(keep_charge=True, stream=stream)
             flags_s.zero_()
             while True:
                 sgraph.replay()
@@ -435,17 +436,19 @@ def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6,
                     break
             sur_it = int(fs[1])
             used = bool(fs[0]) and not fs[2]
-            # (2) NEGF phase from the surrogate's charge
-            if step == 0:
-                if used:
-                    V, W, rows = brs.history(stream=stream)
-                    k = min(rows, max_step // 2)
-                    brn.set_initial_jacobian(V[rows - k:].contiguous() if k else None,
-                                             W[rows - k:].contiguous() if k else None, stream=stream)
+            # (2) NEGF phase from the surrogate's charge (else from the previous NEGF
+            # charge); initial inverse Jacobian: the surrogate solve's secant rows, or
+            # the NEGF rows of the previous gate points (carry_rows)
+            if carry_rows and step > 0:
+                brn.restart(keep_rows=max_step // 2, stream=stream)
             else:
-                brn.restart(keep_rows=keep_rows, stream=stream)
+                brn.reset(keep_charge=True, stream=stream)
             if used:
                 nin_t.copy_(nin_s_t)
+                if seed_rows and not (carry_rows and step > 0):
+                    V, W, rows = brs.history(stream=stream)
+                    if 0 < rows <= max_step // 2:
+                        brn.set_initial_jacobian(V.contiguous(), W.contiguous(), stream=stream)
             flags.zero_()
             if switch:
                 flags[6] = 1
