@@ -144,6 +144,8 @@ struct ChainTable {
     std::vector<negf::WarpRec> warps;
     std::vector<negf::ReduceTube> rts;
     std::vector<negf::SegUnit> units;
+    std::vector<int> order;  // fused schedule: FP64 warps, then FP32 warps
+    int n64 = 0, n32 = 0;
     long long partial_doubles = 0, scratch_doubles = 0;
     long long updates = 0, updates_fp32 = 0, contour_updates = 0, realaxis_updates = 0;
     int max_N = 0;
@@ -202,8 +204,16 @@ struct negf_broyden {
 struct negf_charge_plan {
     std::vector<negf_tube*> tubes;
     std::vector<int> versions;
-    DevBuf d_tubes, d_chains, d_warps, d_units, d_rts, d_partial, d_scratch;
+    DevBuf d_tubes, d_chains, d_warps, d_units, d_rts, d_partial, d_scratch, d_order;
     int num_warps = 0, num_units = 0, max_N = 0;
+    int n64 = 0, n32 = 0;  // fused schedule: FP64 / FP32 warps in d_order
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    ~negf_charge_plan() {
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
+    }
     int wpb = 4, spu = negf::kSegsPerUnit;
     int schedule = 0;  // negf::kScheduleTwoPass or kScheduleFused
     double* d_Q = nullptr;
@@ -226,7 +236,9 @@ std::mutex g_mu;
 struct Workspace {
     int device = 0;
     cudaStream_t stream = nullptr;
-    DevBuf tubes, chains, warps, rts, units, partial, scratch, qbuf, pieces;
+    DevBuf tubes, chains, warps, rts, units, partial, scratch, qbuf, pieces, order;
+    cudaStream_t side = nullptr;                 // the FP32 warps of the fused schedule
+    cudaEvent_t fork = nullptr, join = nullptr;  // around them
     // real-space pass (negf_rs_compute_charge)
     DevBuf rsE, rsFlags, rsU0, rsUa, rsCorners, rsGL, rsRows, rsStatus;
     // cached chain table
@@ -244,8 +256,11 @@ struct Workspace {
         for (cudaEvent_t& e : ev)
             if (e) cudaEventDestroy(e);
         if (done) cudaEventDestroy(done);
-        DevBuf* bufs[] = {&tubes, &chains, &warps,  &rts,   &units,  &partial,   &scratch, &qbuf,
-                          &pieces, &rsE,  &rsFlags, &rsU0, &rsUa, &rsCorners, &rsGL,    &rsRows, &rsStatus};
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
+        DevBuf* bufs[] = {&tubes, &chains, &warps, &rts,  &units, &partial,   &scratch, &qbuf,   &pieces,
+                          &order, &rsE,    &rsFlags, &rsU0, &rsUa, &rsCorners, &rsGL,    &rsRows, &rsStatus};
         for (DevBuf* b : bufs) {
             if (b->p) cudaFree(b->p);
             b->p = nullptr;
@@ -288,6 +303,9 @@ int get_workspace(cudaStream_t stream, Workspace** out) {
         w->device = dev;
         w->stream = stream;
         NEGF_CUDA(cudaEventCreateWithFlags(&w->done, cudaEventDisableTiming));
+        NEGF_CUDA(cudaEventCreateWithFlags(&w->fork, cudaEventDisableTiming));
+        NEGF_CUDA(cudaEventCreateWithFlags(&w->join, cudaEventDisableTiming));
+        NEGF_CUDA(cudaStreamCreateWithFlags(&w->side, cudaStreamNonBlocking));
     }
     if (w->used) NEGF_CUDA(cudaStreamWaitEvent(stream, w->done, 0));
     *out = w.get();
@@ -720,6 +738,17 @@ void build_table_generic(const TubePass* passes, int num_passes, int* order, Out
     cnt.scratch_doubles = ck;
 }
 
+// Warp order of the fused schedule (FP64 warps first, then FP32 warps).
+void fused_order(ChainTable& ct) {
+    ct.order.clear();
+    for (int pass = 0; pass < 2; ++pass)
+        for (size_t w = 0; w < ct.warps.size(); ++w)
+            if (ct.warps[w].fp32 == pass) ct.order.push_back((int)w);
+    ct.n32 = 0;
+    for (const negf::WarpRec& w : ct.warps) ct.n32 += w.fp32 ? 1 : 0;
+    ct.n64 = (int)ct.warps.size() - ct.n32;
+}
+
 void build_table(ChainTable& ct, const std::vector<TubePass>& passes) {
     ct = ChainTable();
     Out<negf::ChainRec> oc;
@@ -739,6 +768,7 @@ void build_table(ChainTable& ct, const std::vector<TubePass>& passes) {
     ct.partial_doubles = cnt.partial_doubles;
     ct.scratch_doubles = cnt.scratch_doubles;
     ct.max_N = cnt.max_N;
+    fused_order(ct);
 }
 
 int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const std::vector<negf::TubeDev>& tdev,
@@ -761,6 +791,10 @@ int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const s
                                       cudaMemcpyHostToDevice, stream));
         if (!ct.units.empty())
             NEGF_CUDA(cudaMemcpyAsync(W.units.p, ct.units.data(), ct.units.size() * sizeof(negf::SegUnit),
+                                      cudaMemcpyHostToDevice, stream));
+        NEGF_CUDA(W.order.reserve(std::max<size_t>(1, ct.order.size()) * sizeof(int)));
+        if (!ct.order.empty())
+            NEGF_CUDA(cudaMemcpyAsync(W.order.p, ct.order.data(), ct.order.size() * sizeof(int),
                                       cudaMemcpyHostToDevice, stream));
     }
     // the reduce table carries device pointers that can change (rho0 of a rebuilt tube)
@@ -791,10 +825,11 @@ int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const s
     const int schedule = choose_schedule(G.schedule, nw, pieces);
     if (schedule == negf::kScheduleFused) pieces = 1;
     if (pieces > 1) NEGF_CUDA(W.pieces.reserve(sizeof(double) * (size_t)nw * pieces * 24 * negf::kWarp));
+    const negf::FusedOrder fo{W.order.as<int>(), ct.n64, ct.n32, W.side, W.fork, W.join};
     NEGF_CUDA(negf::launch_rgf(W.tubes.as<negf::TubeDev>(), W.chains.as<negf::ChainRec>(), W.warps.as<negf::WarpRec>(),
                                nw, W.units.as<negf::SegUnit>(), (int)ct.units.size(), W.partial.as<double>(),
                                W.scratch.p, G.warps_per_block, stream, G.timing ? W.ev[3] : nullptr, nullptr, pieces,
-                               W.pieces.as<double>(), schedule));
+                               W.pieces.as<double>(), schedule, &fo));
     if (G.timing) NEGF_CUDA(cudaEventRecord(W.ev[1], stream));
     NEGF_CUDA(negf::launch_reduce(W.rts.as<negf::ReduceTube>(), (int)ct.rts.size(), ct.max_N, W.partial.as<double>(),
                                   d_Q, stream));
@@ -810,7 +845,9 @@ int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const s
     st.chains = (int)ct.chains.size();
     st.warps = nw;
     const bool fused = schedule == negf::kScheduleFused;
-    st.kernel_launches = (nw > 0 ? (fused ? 1 : pieces > 1 ? 4 : 2) : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
+    const int fused_kernels = (ct.n64 > 0 ? 1 : 0) + (ct.n32 > 0 ? 1 : 0);
+    st.kernel_launches =
+        (nw > 0 ? (fused ? fused_kernels : pieces > 1 ? 4 : 2) : 0) + (ct.max_N > 0 && !ct.rts.empty() ? 1 : 0);
     st.pieces = pieces;
     st.units = fused ? 0 : (int)ct.units.size();
     st.checkpoint_bytes = checkpoint_traffic(ct.warps, tdev, ct.scratch_doubles, schedule);
@@ -1400,6 +1437,9 @@ int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
     TableCounts cnt;
     build_table_generic(passes.data(), n, order.data(), oc, ow, ou, ct.rts.data(), cnt, spu);
     for (int i = 0; i < n; ++i) p.tubes[i]->d.precision = saved[i];
+    fused_order(ct);
+    p.n64 = ct.n64;
+    p.n32 = ct.n32;
     p.num_warps = (int)ct.warps.size();
     p.num_units = (int)ct.units.size();
     p.max_N = cnt.max_N;
@@ -1410,6 +1450,9 @@ int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
         NEGF_CUDA(cudaMemcpy(p.d_units.p, ct.units.data(), ct.units.size() * sizeof(negf::SegUnit),
                              cudaMemcpyHostToDevice));
     if (!upload_all) return NEGF_OK;
+    NEGF_CUDA(p.d_order.reserve(std::max<size_t>(1, ct.order.size()) * sizeof(int)));
+    if (!ct.order.empty())
+        NEGF_CUDA(cudaMemcpy(p.d_order.p, ct.order.data(), ct.order.size() * sizeof(int), cudaMemcpyHostToDevice));
     NEGF_CUDA(p.d_tubes.reserve(tdev.size() * sizeof(negf::TubeDev)));
     NEGF_CUDA(p.d_chains.reserve(std::max<size_t>(1, ct.chains.size()) * sizeof(negf::ChainRec)));
     NEGF_CUDA(p.d_warps.reserve(std::max<size_t>(1, ct.warps.size()) * sizeof(negf::WarpRec)));
@@ -1429,10 +1472,11 @@ int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
 }
 
 cudaError_t plan_launch(const negf_charge_plan& p, const int* skip, cudaStream_t s) {
+    const negf::FusedOrder fo{p.d_order.as<int>(), p.n64, p.n32, p.side, p.fork, p.join};
     cudaError_t e = negf::launch_rgf(p.d_tubes.as<negf::TubeDev>(), p.d_chains.as<negf::ChainRec>(),
                                      p.d_warps.as<negf::WarpRec>(), p.num_warps, p.d_units.as<negf::SegUnit>(),
                                      p.num_units, p.d_partial.as<double>(), p.d_scratch.p, p.wpb, s, nullptr, skip, 1,
-                                     nullptr, p.schedule);
+                                     nullptr, p.schedule, &fo);
     if (e != cudaSuccess) return e;
     return negf::launch_reduce(p.d_rts.as<negf::ReduceTube>(), (int)p.tubes.size(), p.max_N,
                                p.d_partial.as<double>(), p.d_Q, s, skip);
@@ -1456,6 +1500,9 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
     }
     p->d_Q = d_Q;
     p->force_fp64 = (flags & NEGF_PLAN_FP64) != 0;
+    NEGF_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
+    NEGF_CUDA(cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming));
+    NEGF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
     p->wpb = settings().warps_per_block;
     rc = plan_tables(*p, negf::kSegsPerUnit, true);
     if (rc) return rc;

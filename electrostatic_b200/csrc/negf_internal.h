@@ -128,11 +128,21 @@ constexpr int kScheduleFused = 1;
 // skip (device int, may be null): when nonzero at launch time every block
 // returns at entry (device-side early exit of a captured SCF iteration).
 // The fused schedule runs with pieces == 1 only (else the two-pass one runs).
+// Warp order of the fused schedule: order[0 .. n64) are the FP64 warps,
+// order[n64 .. n64 + n32) the FP32 ones (device array); the FP32 kernel runs
+// on `side` between the events fork (recorded on the main stream) and join
+// (waited by the main stream) when both kinds exist.
+struct FusedOrder {
+    const int* order;
+    int n64, n32;
+    cudaStream_t side;
+    cudaEvent_t fork, join;
+};
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
                        int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event,
                        const int* skip = nullptr, int pieces = 1, double* d_piece_work = nullptr,
-                       int schedule = kScheduleTwoPass);
+                       int schedule = kScheduleTwoPass, const FusedOrder* fo = nullptr);
 // pieces > 1 (parallel in length): d_piece_work holds num_warps * pieces * 24 * 32 doubles.
 // Device self-test of numeric primitives: which = 0 FP64 reciprocal,
 // 1 FP32 reciprocal (input/output as doubles), n values, device pointers.

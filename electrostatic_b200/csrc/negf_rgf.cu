@@ -1191,31 +1191,27 @@ __global__ void __launch_bounds__(32) rgf_piece_prefix_kernel(const TubeDev* __r
 }
 
 // Fused schedule: one warp (32 whole chains) per block; records in the
-// warp's scratch, per-site sums into the warp's partial row.
+// warp's scratch, per-site sums into the warp's partial row.  One
+// instantiation per precision (FP32 chains need far fewer registers, so more
+// of their warps stay resident); block b takes warp order[b].
+template <typename R>
 __global__ void __launch_bounds__(32) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
                                                        const ChainRec* __restrict__ chains,
-                                                       const WarpRec* __restrict__ warps, int num_warps,
-                                                       double* __restrict__ partial, double* __restrict__ scratch,
-                                                       const int* __restrict__ skip) {
+                                                       const WarpRec* __restrict__ warps, const int* __restrict__ order,
+                                                       int count, double* __restrict__ partial,
+                                                       double* __restrict__ scratch, const int* __restrict__ skip) {
     if (skip && *skip) return;
     const int lane = threadIdx.x & 31;
-    const int w = blockIdx.x;
-    if (w >= num_warps) return;
+    if ((int)blockIdx.x >= count) return;
+    const int w = order[blockIdx.x];
     const WarpRec wr = warps[w];
     const ChainRec c = chains[(size_t)w * kWarp + lane];
     double* ws = scratch + wr.ck_off;
     double* prow = partial + wr.row_off;
-    if (wr.fp32) {
-        if (wr.kind == kRealAxis)
-            fused_chain<float, true>(tubes, c, wr.tube, reinterpret_cast<float*>(ws), prow, lane);
-        else
-            fused_chain<float, false>(tubes, c, wr.tube, reinterpret_cast<float*>(ws), prow, lane);
-    } else {
-        if (wr.kind == kRealAxis)
-            fused_chain<double, true>(tubes, c, wr.tube, ws, prow, lane);
-        else
-            fused_chain<double, false>(tubes, c, wr.tube, ws, prow, lane);
-    }
+    if (wr.kind == kRealAxis)
+        fused_chain<R, true>(tubes, c, wr.tube, reinterpret_cast<R*>(ws), prow, lane);
+    else
+        fused_chain<R, false>(tubes, c, wr.tube, reinterpret_cast<R*>(ws), prow, lane);
 }
 
 __global__ void __launch_bounds__(128) rgf_pass2_kernel(const TubeDev* __restrict__ tubes,
@@ -1487,14 +1483,35 @@ int rgf_kernel_regs() {
 cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const WarpRec* d_warps, int num_warps,
                        const SegUnit* d_units, int num_units, double* d_partial, void* d_scratch,
                        int warps_per_block, cudaStream_t stream, cudaEvent_t mid_event, const int* skip, int pieces,
-                       double* d_piece_work, int schedule) {
+                       double* d_piece_work, int schedule, const FusedOrder* fo) {
     if (num_warps <= 0) return cudaSuccess;
-    if (schedule == kScheduleFused && pieces <= 1) {
-        // one warp per block: whole chains spread evenly over the SMs
-        rgf_fused_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps, d_partial,
-                                                           static_cast<double*>(d_scratch), skip);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess && mid_event) e = cudaEventRecord(mid_event, stream);
+    if (schedule == kScheduleFused && pieces <= 1 && fo && fo->order) {
+        // one warp per block: whole chains spread evenly over the SMs; the FP32
+        // warps run on the side stream alongside the FP64 ones when both exist
+        double* scr = static_cast<double*>(d_scratch);
+        const bool fork = fo->n64 > 0 && fo->n32 > 0 && fo->side && fo->fork && fo->join;
+        cudaError_t e = cudaSuccess;
+        if (fork) {
+            e = cudaEventRecord(fo->fork, stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(fo->side, fo->fork, 0);
+            if (e != cudaSuccess) return e;
+        }
+        if (fo->n64 > 0)
+            rgf_fused_kernel<double><<<fo->n64, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, fo->order, fo->n64,
+                                                                    d_partial, scr, skip);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (fo->n32 > 0)
+            rgf_fused_kernel<float><<<fo->n32, kWarp, 0, fork ? fo->side : stream>>>(
+                d_tubes, d_chains, d_warps, fo->order + fo->n64, fo->n32, d_partial, scr, skip);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (fork) {
+            e = cudaEventRecord(fo->join, fo->side);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, fo->join, 0);
+            if (e != cudaSuccess) return e;
+        }
+        if (mid_event) e = cudaEventRecord(mid_event, stream);
         return e;
     }
     if (warps_per_block < 1 || warps_per_block > 4) warps_per_block = 4;
