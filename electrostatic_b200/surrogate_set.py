@@ -25,16 +25,20 @@ over the tubes' own sites (padding is masked out).
 
 The sweep (set_scf_sweep) follows scf.run_scf_batch -- one Broyden over all
 the tubes' sites, iterations replayed as CUDA graphs -- and adds the
-surrogate: per gate step, (1) the surrogate phase solves the loop with the
-surrogate's charge (its own Broyden, continued from the previous gate step);
-(2) the NEGF phase starts from that charge; its initial inverse Jacobian is
-the surrogate phase's secant rows at the first gate step and the NEGF
-phase's own rows carried from the previous gate step afterwards
-(negf_broyden_restart), with the scalar part fraction * I set from the
-surrogate's Jacobian (largest eigenvalue of I - dQ_s/dn by power iteration:
-fraction = 2 / (1 + lambda_max)).  The NEGF phase runs the mixed-precision
-plan until the residual falls below switch_norm and the FP64 plan after; only
-an FP64 NEGF charge ends a solve (the engine judges every converged charge).
+surrogate: per gate point, (1) the surrogate phase solves the loop with the
+surrogate's charge (a fresh Broyden solve started from the surrogate's
+previous fixed point, to the surrogate's own residual floor); (2) the NEGF
+phase starts from that charge with the surrogate solve's secant rows as its
+initial inverse Jacobian (negf_broyden_set_initial_jacobian; carry_rows
+carries the NEGF rows of the previous gate points instead,
+negf_broyden_restart), the scalar part fraction * I set from the surrogate's
+Jacobian (largest eigenvalue of I - dQ_s/dn by power iteration: fraction =
+2 / (1 + lambda_max), the optimal Richardson step for a spectrum in
+[1, lambda_max]).  The NEGF phase runs the mixed-precision plan until the
+residual falls below switch_norm and the FP64 plan after; only an FP64 NEGF
+charge ends a solve (the engine judges every converged charge).  A surrogate
+phase that does not converge is not used: the NEGF phase then starts from the
+previous gate point's charge.
 """
 from __future__ import annotations
 
@@ -113,7 +117,7 @@ class TubeSetOperator(FourierOperator):
         return x.to(t.bfloat16).reshape(B * self.S, FEAT_SET)
 
     # ------------------------------------------------------------------ training
-    def fit_set(self, U, Vg, Vds, tid, Q, epochs=20, batch=32, lr=2e-3, log=None):
+    def fit_set(self, U, Vg, Vds, tid, Q, epochs=20, batch=64, lr=2e-3, log=None):
         """Train on canvas tensors U, Q [n][S] (float32), Vg, Vds [n], tid [n];
         the loss covers every tube's own sites only."""
         t = self.torch
@@ -123,7 +127,11 @@ class TubeSetOperator(FourierOperator):
         self.x_scale[0] = float(U.abs().max())
         self.x_scale[nw] = max(float(Vg.abs().max()), 1e-3)
         self.x_scale[nw + 1] = max(float(Vds.abs().max()), 1e-3)
-        self.q_scale = float(Q.abs().max())
+        # per-tube output scales: the tubes' charges differ by their channel counts
+        qs = t.zeros(len(self.desc), device=self.dev)
+        qs.scatter_reduce_(0, tid, Q.abs().amax(dim=1).float(), reduce="amax")
+        self.qs_t = qs.clamp_min(1e-12)
+        self.q_scale = float(self.qs_t.max())
         g = t.Generator(device="cpu").manual_seed(1)
         hist = []
         t0 = time.perf_counter()
@@ -139,7 +147,7 @@ class TubeSetOperator(FourierOperator):
                 q = self.forward(xb, batch, keep=True)
                 m = self._mask_set[ti].reshape(-1)
                 q.mul_(m)
-                y = (Q[idx].reshape(-1) / self.q_scale).float().mul_(m)
+                y = (Q[idx] / self.qs_t[ti][:, None]).reshape(-1).float().mul_(m)
                 dq, part = self.loss_grad(q, y)
                 dq.mul_(m)
                 self.backward(dq, batch)
@@ -162,7 +170,7 @@ class TubeSetOperator(FourierOperator):
             b = min(batch, n - i)
             xb = self.features_set(U[i:i + b], Vg[i:i + b], Vds[i:i + b], tid[i:i + b])
             q = self.forward(xb, b)
-            out[i:i + b] = (q[: b * self.S].reshape(b, self.S) * self.q_scale).double()
+            out[i:i + b] = (q[: b * self.S].reshape(b, self.S) * self.qs_t[tid[i:i + b]][:, None]).double()
         return out * self._mask_set[tid].double()
 
     # ------------------------------------------------------------------ bound inference over the set
@@ -179,7 +187,8 @@ class TubeSetOperator(FourierOperator):
                         win=t.empty(T * S * nw, dtype=t.float64, device=self.dev),
                         x=t.empty(T, S, FEAT_SET, device=self.dev),
                         xb=t.empty(T * S, FEAT_SET, dtype=t.bfloat16, device=self.dev),
-                        qd=t.empty(T * S, dtype=t.float64, device=self.dev))
+                        qd=t.empty(T * S, dtype=t.float64, device=self.dev),
+                        qscale=self.qs_t.double().repeat_interleave(S).contiguous())
         x = self._bs["x"]
         x[:, :, nw + 2:] = self._fixed_set
         self.set_bias_set(Vg, Vds)
@@ -201,8 +210,8 @@ class TubeSetOperator(FourierOperator):
         b["xb"].copy_(b["x"].view(T * S, FEAT_SET))
         q = self.forward(b["xb"], T)
         b["qd"].copy_(q)
+        b["qd"].mul_(b["qscale"])
         t.index_select(b["qd"], 0, b["qidx"], out=b["Q"])
-        b["Q"].mul_(self.q_scale)
 
 
 # ---------------------------------------------------------------------- data
@@ -310,7 +319,7 @@ def generate_set_pairs(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bin
 
 # ---------------------------------------------------------------------- SCF
 def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6, max_step=200, switch_norm=1e-5,
-                  surrogate_norm=1e-6, surrogate_max_step=60, seed_rows=True, carry_rows=False, iters_per_graph=4,
+                  surrogate_norm=None, surrogate_max_step=60, seed_rows=True, carry_rows=False, iters_per_graph=4,
                   power_iters=6, autotune=True):
     """Surrogate-started gate sweep of a tube set (module docstring).  Tubes
     in mixed precision run the NEGF phase on their own plan until the
@@ -327,6 +336,8 @@ def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6,
     S = int(offs[-1])
     stream = torch.cuda.Stream()
     t_setup = time.perf_counter()
+    if surrogate_norm is None:  # the surrogate's own residual floor: BF16 inputs, ~0.2% of its charge scale
+        surrogate_norm = 2e-3 * float(model.q_scale)
     out = []
     with torch.cuda.stream(stream):
         Q = torch.zeros(S, dtype=torch.float64, device=dev)
