@@ -385,20 +385,22 @@ def long_tube_measure(torch, reps=10):
             "max_rel_automatic_vs_one_piece": float(np.max(np.abs(Qa - Q1)) / np.max(np.abs(Q1)))}
 
 
-def config5_measure(torch, n_pairs=12000, epochs=10, oracle_check=True):
+def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True, ablation=True):
     """Surrogate-assisted self-consistency on the config-4 tube set (16
     tubes): one Fourier operator for the whole set (6 layers, width 128, 32
-    frequencies, BF16 weights, FP32 accumulation) trained on n_pairs (U, Q)
-    pairs from the engine; then the Vds = 0.4 V gate sweep 0 -> 0.6 V twice:
-    plain (FP64 tubes, Broyden alpha 0.1 from zero charge at every gate
-    point, the reference's defaults) and surrogate-started (mixed-precision
-    tubes; surrogate charge as the start, surrogate Jacobian for the initial
-    inverse Jacobian, FP64 finish).  Per-step times exclude the one-off
-    plans and graph captures of both sweeps; data generation and training
-    are reported separately."""
+    frequencies, BF16 weights, FP32 accumulation) trained on n_pairs
+    (external potential, self-consistent charge) pairs that the engine's own
+    batched solves produce; then the Vds = 0.4 V gate sweep 0 -> 0.6 V:
+    plain (FP64 tubes, one Broyden over the set with fraction 0.1 from zero
+    charge at every gate point: the reference's defaults) and
+    surrogate-started (mixed-precision tubes, one inference per gate point as
+    the start, fraction from the surrogate's Jacobian, one secant update per
+    tube, FP64 finish).  Per-step times exclude the one-off plans and graph
+    captures of both sweeps; data generation and training are reported
+    separately."""
     from electrostatic_b200.negf import CNT
     from electrostatic_b200.scf import run_scf_batch
-    from electrostatic_b200.surrogate_set import (TubeSetOperator, generate_set_pairs, set_scf_sweep,
+    from electrostatic_b200.surrogate_set import (TubeSetOperator, fixed_point_sweep, generate_fixed_points,
                                                   tube_descriptor)
     from electrostatic_b200.workloads import GATE_SWEEP, gate_with_contacts, uneven_batch
     descs = uneven_batch(precision="fp64")
@@ -414,15 +416,13 @@ def config5_measure(torch, n_pairs=12000, epochs=10, oracle_check=True):
         R = 1.42e-10 * np.sqrt(3.0) * d["type_id"][0] / (2 * np.pi)  # CNT.cpp:23-41
         electros.append(gate_with_contacts(t.site_positions(), R, vds=vds))
     t0 = time.perf_counter()
-    U, Vg, Vds, tid, Q, eng = generate_set_pairs(make, electros, n_pairs)
+    U, Vg, Vds, tid, Q, eng, data_iters = generate_fixed_points(make, electros, n_pairs)
     t_data = time.perf_counter() - t0
     for e in electros:
         e.Vds = vds
     model = TubeSetOperator([tube_descriptor(t) for t in tubes64], seed=0)
-    perm = torch.randperm(n_pairs, generator=torch.Generator().manual_seed(0)).cuda()
-    U, Vg, Vds, tid, Q = U[perm], Vg[perm], Vds[perm], tid[perm], Q[perm]
     ntr = int(0.9 * n_pairs)
-    fit = model.fit_set(U[:ntr], Vg[:ntr], Vds[:ntr], tid[:ntr], Q[:ntr], epochs=epochs, batch=16)
+    fit = model.fit_set(U[:ntr], Vg[:ntr], Vds[:ntr], tid[:ntr], Q[:ntr], epochs=epochs, batch=batch)
     pred = model.predict_set(U[ntr:], Vg[ntr:], Vds[ntr:], tid[ntr:])
     qt = Q[ntr:].double()
     qmax = qt.abs().max(dim=1).values.clamp_min(1e-30)
@@ -439,38 +439,41 @@ def config5_measure(torch, n_pairs=12000, epochs=10, oracle_check=True):
                          reset_with_previous_charge=True)
     # surrogate-started, mixed precision (contour and real-axis chains in FP32 at 2 meV broadening)
     tubesmx = make(vds, precision="mixed", realaxis_fp32=True)
-    set_scf_sweep(tubesmx, electros, [0.0], model)  # warm-up
-    sur, alpha, lam, t_setup = set_scf_sweep(tubesmx, electros, GATE_SWEEP, model)
-    sur_c, _, _, _ = set_scf_sweep(tubesmx, electros, GATE_SWEEP, model, carry_rows=True)
+    fixed_point_sweep(tubesmx, electros, [0.0], model)  # warm-up
+    sur, alpha, lam, t_setup = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model)
     t_plain = sum(s_.seconds for s_ in plain.steps)
     t_cont = sum(s_.seconds for s_ in cont.steps)
     t_sur = sum(r["seconds"] for r in sur)
-    dq = max(float(np.max(np.abs(r["Q"] - s_.Q))) / float(np.max(np.abs(s_.Q))) for r, s_ in zip(sur, plain.steps))
+    qref = [s_.Q for s_ in plain.steps]
+    dq = max(float(np.max(np.abs(r["Q"] - q))) / float(np.max(np.abs(q))) for r, q in zip(sur, qref))
+    start_err = [float(np.max(np.abs(r["start"] - q)) / np.max(np.abs(q))) for r, q in zip(sur, qref)]
     res = {"workload": "config-4 tube set (16 tubes), Vds 0.4 V, Vg 0..0.6 V step 0.05, 1e-6 absolute max-norm; "
                        "operator 6 layers x width 128 x 32 frequencies on a %d-site canvas, BF16 weights, FP32 "
-                       "accumulation" % model.S,
-           "pairs": n_pairs, "data_seconds": t_data, "engine_seconds": eng, "train_seconds": fit["seconds"],
-           "epochs": epochs, "final_loss": fit["loss"][-1], "test_rel_err_median": float(np.median(err)),
+                       "accumulation, trained on self-consistent fixed points" % model.S,
+           "pairs": n_pairs, "data_seconds": t_data, "data_solve_seconds": eng,
+           "data_mean_iterations": float(np.mean(data_iters)), "train_seconds": fit["seconds"], "epochs": epochs,
+           "batch": batch, "final_loss": fit["loss"][-1], "test_rel_err_median": float(np.median(err)),
            "test_rel_err_p90": float(np.percentile(err, 90)), "test_rms_rel_err_median": float(np.median(rms)),
            "plain": {"iterations": [s_.iterations for s_ in plain.steps], "seconds": t_plain,
-                     "method": "FP64 tubes, Broyden alpha 0.1, n = 0 at every gate point (reference defaults)"},
+                     "method": "FP64 tubes, one Broyden over the set, fraction 0.1, n = 0 at every gate point "
+                               "(reference defaults)"},
            "surrogate_started": {"negf_iterations": [r["negf_iterations"] for r in sur],
-                                 "fp32_iterations": [r["lowprec_iterations"] for r in sur],
-                                 "surrogate_iterations": [r["surrogate_iterations"] for r in sur],
-                                 "used": [r["surrogate_used"] for r in sur], "seconds": t_sur,
-                                 "fraction": alpha, "lambda_max": lam, "setup_seconds_excluded": t_setup,
+                                 "fp32_iterations": [r["lowprec_iterations"] for r in sur], "seconds": t_sur,
+                                 "start_rel_err": start_err, "fraction": alpha, "lambda_max": lam,
+                                 "setup_seconds_excluded": t_setup,
                                  "method": "mixed-precision tubes (FP32 contour and real-axis chains, FP64 finish "
-                                           "below 1e-5); start = surrogate self-consistent charge; initial inverse "
-                                           "Jacobian = surrogate secant rows (first gate point), carried NEGF rows "
-                                           "after, fraction 2/(1+lambda_max) of the surrogate Jacobian"},
+                                           "below 1e-5); start = one surrogate inference; initial inverse Jacobian "
+                                           "fraction * I with fraction = 2 / (2 + lambda_max) from the surrogate's "
+                                           "Jacobian; one secant update per tube"},
            "plain_continuation": {"iterations": [s_.iterations for s_ in cont.steps], "seconds": t_cont,
                                   "method": "as plain, n_in carried from the previous gate point"},
-           "surrogate_carry_rows": {"negf_iterations": [r["negf_iterations"] for r in sur_c],
-                                    "seconds": sum(r["seconds"] for r in sur_c),
-                                    "method": "as surrogate_started, but the NEGF secant rows of the previous "
-                                              "gate points (negf_broyden_restart) instead of the surrogate's"},
            "speedup": t_plain / t_sur, "speedup_vs_plain_continuation": t_cont / t_sur,
            "max_rel_dQ_vs_plain_fp64": dq}
+    if ablation:
+        # the same solver (mixed, segments, the surrogate's fraction) from zero charge: the start's share
+        nos, _, _, _ = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, fraction=alpha, use_surrogate=False)
+        res["same_solver_zero_start"] = {"negf_iterations": [r["negf_iterations"] for r in nos],
+                                         "seconds": sum(r["seconds"] for r in nos)}
     if oracle_check:
         # the FP64 oracle's charge at the converged potential of the last gate point (fixed-point check)
         from oracle import oracle as O

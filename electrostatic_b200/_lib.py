@@ -29,7 +29,7 @@ EXPORTED = [
     "negf_tube_total_integration_pts", "negf_tube_set_energy_shard", "negf_shard_range", "negf_compute_charge",
     "negf_last_stats", "negf_set_timing", "negf_set_tuning", "negf_broyden_create", "negf_broyden_destroy", "negf_broyden_set_input",
     "negf_broyden_step", "negf_broyden_reset", "negf_broyden_step_number", "negf_broyden_input_device_ptr",
-    "negf_broyden_set_initial_jacobian", "negf_broyden_restart", "negf_broyden_history",
+    "negf_broyden_set_initial_jacobian", "negf_broyden_restart", "negf_broyden_history", "negf_broyden_set_segments",
     "negf_affine_potential", "negf_write_step", "negf_last_error", "negf_device_selftest",
     "negf_compute_charge_noalloc", "negf_tube_dos_points", "negf_tube_current_points", "negf_compute_dos",
     "negf_compute_current", "negf_write_transport_char", "negf_write_current_header", "negf_write_current",
@@ -144,6 +144,7 @@ def load():
         "negf_broyden_reset": [vp, C.c_int, C.c_double, vp],
         "negf_broyden_set_initial_jacobian": [vp, vp, vp, C.c_int, vp],
         "negf_broyden_restart": [vp, C.c_int, vp],
+        "negf_broyden_set_segments": [vp, C.c_int, ip, vp],
         "negf_broyden_history": [vp, C.POINTER(vp), C.POINTER(vp), ip, vp],
         "negf_broyden_step_number": [vp, ip],
         "negf_broyden_input_device_ptr": [vp, C.POINTER(vp)],

@@ -194,10 +194,13 @@ struct negf_broyden {
     int step = 1;
     int device = 0;
     ~negf_broyden() {
-        double* bufs[] = {dev.n_in, dev.n_prev, dev.F, dev.dF, dev.norm, dev.V, dev.W, dev.c, dev.sum, dev.scal, dev.part};
+        double* bufs[] = {dev.n_in, dev.n_prev, dev.F, dev.dF, dev.norm, dev.V, dev.W, dev.c, dev.sum, dev.scal, dev.part,
+                          dev.dd};
         for (double* p : bufs)
             if (p) cudaFree(p);
         if (dev.step_dev) cudaFree(dev.step_dev);
+        if (dev.seg_off) cudaFree(dev.seg_off);
+        if (dev.seg_of) cudaFree(dev.seg_of);
     }
 };
 
@@ -1644,6 +1647,7 @@ int negf_broyden_create(int S, int max_step, double fraction, int norm_type, neg
     d.fraction = fraction;
     d.scalar = 1.0;
     d.base = 0;
+    d.nseg = 1;
     d.nblocks = std::min(1024, (S + 255) / 256);
     double** vec[] = {&d.n_in, &d.n_prev, &d.F, &d.dF, &d.norm, &d.sum};
     for (double** p : vec) {
@@ -1713,7 +1717,7 @@ int negf_broyden_reset(negf_broyden* b, int keep_charge, double init_value, void
     for (double* p : vec) NEGF_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * d.S, s));
     NEGF_CUDA(cudaMemsetAsync(d.V, 0, sizeof(double) * (size_t)d.S * d.max_step, s));
     NEGF_CUDA(cudaMemsetAsync(d.W, 0, sizeof(double) * (size_t)d.S * d.max_step, s));
-    NEGF_CUDA(cudaMemsetAsync(d.c, 0, sizeof(double) * d.max_step, s));
+    NEGF_CUDA(cudaMemsetAsync(d.c, 0, sizeof(double) * d.max_step * d.nseg, s));
     d.base = 0;
     b->step = 1;
     NEGF_CUDA(negf::set_int(d.step_dev, 1, s));
@@ -1738,6 +1742,52 @@ int negf_broyden_set_initial_jacobian(negf_broyden* b, const double* d_V, const 
     }
     d.base = k;
     NEGF_CUDA(negf::set_int(d.step_dev + 1, k, s));
+    return NEGF_OK;
+}
+
+int negf_broyden_set_segments(negf_broyden* b, int nseg, const int* offsets, void* stream) {
+    if (!b || nseg < 1 || (nseg > 1 && !offsets)) return fail(NEGF_ERR_ARG, "bad segment arguments");
+    negf::BroydenDev& d = b->dev;
+    std::vector<int> off(nseg + 1), of;
+    if (nseg > 1) {
+        for (int g = 0; g <= nseg; ++g) off[g] = offsets[g];
+        if (off[0] != 0 || off[nseg] != d.S) return fail(NEGF_ERR_ARG, "segment offsets must run from 0 to S");
+        for (int g = 0; g < nseg; ++g)
+            if (off[g + 1] <= off[g]) return fail(NEGF_ERR_ARG, "segment offsets must increase");
+        of.resize(d.S);
+        for (int g = 0; g < nseg; ++g)
+            for (int i = off[g]; i < off[g + 1]; ++i) of[i] = g;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    int step = 0;
+    NEGF_CUDA(cudaMemcpyAsync(&step, d.step_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+    NEGF_CUDA(cudaStreamSynchronize(s));
+    if (step != 1 || b->step != 1 || d.base != 0)
+        return fail(NEGF_ERR_STATE, "segments are set before the first step and before seeding (after create or reset)");
+    double* c = nullptr;
+    double* dd = nullptr;
+    int* seg_off = nullptr;
+    int* seg_of = nullptr;
+    NEGF_CUDA(cudaMalloc(&c, sizeof(double) * (size_t)d.max_step * nseg));
+    NEGF_CUDA(cudaMemset(c, 0, sizeof(double) * (size_t)d.max_step * nseg));
+    if (nseg > 1) {
+        NEGF_CUDA(cudaMalloc(&dd, sizeof(double) * nseg));
+        NEGF_CUDA(cudaMalloc(&seg_off, sizeof(int) * (nseg + 1)));
+        NEGF_CUDA(cudaMalloc(&seg_of, sizeof(int) * d.S));
+        NEGF_CUDA(cudaMemcpy(seg_off, off.data(), sizeof(int) * (nseg + 1), cudaMemcpyHostToDevice));
+        NEGF_CUDA(cudaMemcpy(seg_of, of.data(), sizeof(int) * d.S, cudaMemcpyHostToDevice));
+    }
+    // the old buffers may still be read by work queued on other streams
+    NEGF_CUDA(cudaDeviceSynchronize());
+    cudaFree(d.c);
+    if (d.dd) cudaFree(d.dd);
+    if (d.seg_off) cudaFree(d.seg_off);
+    if (d.seg_of) cudaFree(d.seg_of);
+    d.c = c;
+    d.dd = dd;
+    d.seg_off = seg_off;
+    d.seg_of = seg_of;
+    d.nseg = nseg;
     return NEGF_OK;
 }
 

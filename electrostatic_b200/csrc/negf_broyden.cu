@@ -127,17 +127,30 @@ __global__ void norm_finalize(BroydenDev b, const int* flags) {
 
 // c[it] = sum_s V[it][s] x[s] for it = 1..rows (one block per row);
 // rows = seeded + m - 1 + which with m from the host or the device (rows
-// 1..seeded: a seeded initial inverse Jacobian).
+// 1..seeded: a seeded initial inverse Jacobian).  With segments the sum runs
+// over each segment's sites separately (blockIdx.y = segment, c[it][g]).
 __global__ void dots_kernel(BroydenDev b, const double* __restrict__ x, int m_host, int which, const int* flags) {
     if (skipped(flags)) return;
     const int rows = seeded(b) + iter_m(b, m_host) - 1 + which;
     const int it = blockIdx.x + 1;
     if (it > rows) return;
+    const int g = blockIdx.y;
+    const int lo = b.nseg > 1 ? b.seg_off[g] : 0, hi = b.nseg > 1 ? b.seg_off[g + 1] : b.S;
     const double* v = b.V + (size_t)it * b.S;
     double acc = 0.0;
-    for (int s = threadIdx.x; s < b.S; s += blockDim.x) acc += v[s] * x[s];
+    for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) acc += v[s] * x[s];
     acc = block_sum(acc);
-    if (threadIdx.x == 0) b.c[it] = acc;
+    if (threadIdx.x == 0) b.c[(size_t)it * b.nseg + g] = acc;
+}
+
+// Per-segment dF^T dF (the denominators of the new V row when segmented).
+__global__ void segsq_kernel(BroydenDev b, int m_host, const int* flags) {
+    if (skipped(flags) || iter_m(b, m_host) <= 0) return;
+    const int g = blockIdx.x;
+    double acc = 0.0;
+    for (int s = b.seg_off[g] + threadIdx.x; s < b.seg_off[g + 1]; s += blockDim.x) acc += b.dF[s] * b.dF[s];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) b.dd[g] = acc;
 }
 
 // Broyden_Second_Parallel.cpp:381-403: sum = W c (it < m), new V and W rows at m
@@ -147,10 +160,11 @@ __global__ void newrow_kernel(BroydenDev b, int m_host, const int* flags) {
     const int m = iter_m(b, m_host);
     if (m <= 0) return;
     const int row = seeded(b) + m;
-    const double denom = b.scal[2];
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
+        const int g = b.nseg > 1 ? b.seg_of[s] : 0;
+        const double denom = b.nseg > 1 ? b.dd[g] : b.scal[2];
         double acc = 0.0;
-        for (int it = 1; it <= row - 1; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
+        for (int it = 1; it <= row - 1; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[(size_t)it * b.nseg + g];
         const double dF = b.dF[s];
         const double dn = b.n_in[s] - b.n_prev[s];
         // a zero step (identical consecutive residuals) adds no direction: the
@@ -166,8 +180,9 @@ __global__ void final_kernel(BroydenDev b, int m_host, const int* flags) {
     if (skipped(flags)) return;
     const int rows = seeded(b) + iter_m(b, m_host);
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < b.S; s += gridDim.x * blockDim.x) {
+        const int g = b.nseg > 1 ? b.seg_of[s] : 0;
         double acc = 0.0;
-        for (int it = 1; it <= rows; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[it];
+        for (int it = 1; it <= rows; ++it) acc += b.W[(size_t)it * b.S + s] * b.c[(size_t)it * b.nseg + g];
         b.sum[s] = acc;
         const double prev = b.n_in[s];
         b.n_prev[s] = prev;
@@ -238,18 +253,20 @@ cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t 
 cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int* flags) {
     if (b.step_dev && flags) {
         // device-resident: shapes cover every m up to max_step, rows above m return
-        const int g = b.max_step > 1 ? b.max_step : 1;
+        const dim3 g(b.max_step > 1 ? b.max_step : 1, b.nseg);
         dots_kernel<<<g, kThreads, 0, s>>>(b, b.dF, 0, 0, flags);
+        if (b.nseg > 1) segsq_kernel<<<b.nseg, kThreads, 0, s>>>(b, 0, flags);
         newrow_kernel<<<b.nblocks, kThreads, 0, s>>>(b, 0, flags);
         dots_kernel<<<g, kThreads, 0, s>>>(b, b.F, 0, 1, flags);
         final_kernel<<<b.nblocks, kThreads, 0, s>>>(b, 0, flags);
         return cudaGetLastError();
     }
     if (m > 0) {
-        if (b.base + m - 1 >= 1) dots_kernel<<<b.base + m - 1, kThreads, 0, s>>>(b, b.dF, m, 0, nullptr);
+        if (b.base + m - 1 >= 1) dots_kernel<<<dim3(b.base + m - 1, b.nseg), kThreads, 0, s>>>(b, b.dF, m, 0, nullptr);
+        if (b.nseg > 1) segsq_kernel<<<b.nseg, kThreads, 0, s>>>(b, m, nullptr);
         newrow_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m, nullptr);
     }
-    if (b.base + m >= 1) dots_kernel<<<b.base + m, kThreads, 0, s>>>(b, b.F, m, 1, nullptr);
+    if (b.base + m >= 1) dots_kernel<<<dim3(b.base + m, b.nseg), kThreads, 0, s>>>(b, b.F, m, 1, nullptr);
     final_kernel<<<b.nblocks, kThreads, 0, s>>>(b, m, nullptr);
     return cudaGetLastError();
 }

@@ -194,7 +194,7 @@ struct BroydenDev {
     double* norm;
     double* V;        // [max_step][S] (row it = V^T column it)
     double* W;        // [max_step][S]
-    double* c;        // [max_step]
+    double* c;        // [max_step][nseg]
     double* sum;      // [S]
     double* scal;     // [4]: max norm, sum of squares, denominator, spare
     double* part;     // [3 * nblocks] block partials
@@ -202,6 +202,12 @@ struct BroydenDev {
     int* step_dev;    // device int[2]: [0] the step counter (read by device-resident steps),
                       // [1] rows 1..[1] of V, W hold a seeded initial inverse Jacobian (0: none)
     int base;         // host copy of step_dev[1]
+    // Segments (per-tube Broyden): the dot products of the secant update run
+    // over each segment's sites separately; nseg == 1 is one Broyden over all sites.
+    int nseg;
+    int* seg_off;     // device int[nseg + 1] (nseg > 1)
+    int* seg_of;      // device int[S]: segment of each site (nseg > 1)
+    double* dd;       // [nseg]: per-segment dF^T dF
 };
 cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s, const int* flags = nullptr);
 cudaError_t broyden_update(const BroydenDev& b, int m, cudaStream_t s, const int* flags = nullptr);

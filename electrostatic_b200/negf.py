@@ -468,6 +468,15 @@ class Broyden:
         recent) as its initial inverse Jacobian; n_in stays."""
         check(_lib.load().negf_broyden_restart(self._h, int(keep_rows), _stream(stream)), "negf_broyden_restart")
 
+    def set_segments(self, offsets, stream=None):
+        """Per-segment secant updates (one Broyden per segment, e.g. per tube)
+        for offsets [0, ..., num_sites]; [0, num_sites] is the whole-vector
+        update.  Call after create or reset, before seeding and stepping."""
+        off = np.ascontiguousarray(offsets, dtype=np.int32)
+        check(_lib.load().negf_broyden_set_segments(self._h, len(off) - 1,
+                                                    off.ctypes.data_as(C.POINTER(C.c_int)), _stream(stream)),
+              "negf_broyden_set_segments")
+
     def set_initial_jacobian(self, V, W, stream=None):
         """Initial inverse Jacobian G0 = fraction I + sum_j W[j] V[j]^T for the
         next solve (V, W: device float64 [k][S]); call after create or reset."""

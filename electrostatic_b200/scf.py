@@ -111,101 +111,154 @@ def run_scf(tube, electro, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, n
     return res
 
 
-def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
-                  initial_charge=0.0, reset_with_previous_charge=False, use_graph=True, iters_per_graph=8,
-                  autotune=True, switch_norm=None):
-    """Self-consistent bias sweep of a batch of tubes with one Broyden over
-    all their sites (the all-tubes n_in of Broyden_Parallel_General.cpp:42-66).
+class BatchSCF:
+    """One self-consistent solver over a batch of tubes, kept between solves.
 
     Each iteration: U_t = U0_t + K_t n_in[t] for every tube (its electrostatics
     operator), one charge-plan launch for the whole batch, one device-resident
-    Broyden step.  With use_graph, iters_per_graph iterations are captured in
-    one CUDA graph and replayed until the device flags say converged (or
-    failed); the host reads the flag ints once per replay.  With switch_norm
-    (mixed-precision tubes), the iterations run on the tubes' own plan until
-    the residual falls below switch_norm and on an FP64 plan from then on;
-    only an FP64 charge ends a solve.  Returns an SCFResult plus the plan's
-    schedule."""
-    import torch
-    from .negf import Broyden, ChargePlan, affine_potential_masked
+    Broyden step over all the tubes' sites (the all-tubes n_in of
+    Broyden_Parallel_General.cpp:42-66).  With use_graph, iters_per_graph
+    iterations are captured in one CUDA graph and replayed until the device
+    flags say converged (or failed); the host reads the flag ints once per
+    replay.  With switch_norm (mixed-precision tubes), the iterations run on
+    the tubes' own plan until the residual falls below switch_norm and on an
+    FP64 plan from then on; only an FP64 charge ends a solve.  segments: one
+    secant update per tube (negf_broyden_set_segments) instead of one over the
+    whole batch.  Every solve runs on the solver's own stream."""
 
-    dev = torch.device("cuda")
-    Ns = [t.num_field_sites for t in tubes]
-    offs = np.concatenate([[0], np.cumsum(Ns)]).astype(int)
-    S = int(offs[-1])
-    stream = torch.cuda.Stream()
-    res = SCFResult()
-    with torch.cuda.stream(stream):
-        Q = torch.zeros(S, dtype=torch.float64, device=dev)
-        n0 = torch.full((S,), float(initial_charge), dtype=torch.float64, device=dev)
-        br = Broyden(n0, max_step=max_step, fraction=fraction, norm_type=norm_type, stream=stream)
-        nin = br.input_device_ptr()
-        ops = []
-        for e in electros:
-            Kd, U0 = e.device_operator(0.0)
-            ops.append((Kd, U0.clone()))
-        U_ptrs = [t.potential_device_ptr() for t in tubes]
-        flags = torch.zeros(8, dtype=torch.int32, device=dev)
-        skip = flags.data_ptr() + 3 * 4
-        switch = switch_norm is not None and switch_norm > 0
-        # the initial potential (paths do not depend on it; contact potentials are read on the device)
-        for (Kd, U0), t, o, N, Up in zip(ops, tubes, offs, Ns, U_ptrs):
-            affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, None, stream=stream)
-        plan = ChargePlan(tubes, Q, autotune=autotune)
-        plan64 = ChargePlan(tubes, Q, autotune=autotune, fp64=True) if switch else None
+    def __init__(self, tubes, electros, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
+                 initial_charge=0.0, use_graph=True, iters_per_graph=8, autotune=True, switch_norm=None,
+                 segments=False):
+        import torch
+        from .negf import Broyden, ChargePlan, affine_potential_masked
 
-        def body(s):
-            for (Kd, U0), o, N, Up in zip(ops, offs, Ns, U_ptrs):
-                affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip, stream=s)
-            if switch:
-                plan.launch(skip=flags.data_ptr() + 5 * 4, stream=s)
-                plan64.launch(skip=flags.data_ptr() + 6 * 4, stream=s)
-                br.step_device_switch(Q, max_norm, switch_norm, flags, stream=s)
-            else:
-                plan.launch(skip=skip, stream=s)
-                br.step_device(Q, max_norm, flags, stream=s)
+        dev = torch.device("cuda")
+        self.tubes, self.electros = list(tubes), list(electros)
+        self.Ns = [t.num_field_sites for t in tubes]
+        self.offs = np.concatenate([[0], np.cumsum(self.Ns)]).astype(int)
+        S = self.S = int(self.offs[-1])
+        self.stream = stream = torch.cuda.Stream()
+        self.initial_charge = float(initial_charge)
+        with torch.cuda.stream(stream):
+            self.Q = Q = torch.zeros(S, dtype=torch.float64, device=dev)
+            n0 = torch.full((S,), self.initial_charge, dtype=torch.float64, device=dev)
+            self.br = br = Broyden(n0, max_step=max_step, fraction=fraction, norm_type=norm_type, stream=stream)
+            if segments and len(tubes) > 1:
+                br.set_segments(self.offs, stream=stream)
+            nin = br.input_device_ptr()
+            self.n_in = device_view(nin, S)
+            self.ops = ops = []
+            for e in electros:
+                Kd, U0 = e.device_operator(0.0)
+                ops.append((Kd, U0.clone()))
+            self.U_ptrs = U_ptrs = [t.potential_device_ptr() for t in tubes]
+            self.flags = flags = torch.zeros(8, dtype=torch.int32, device=dev)
+            skip = flags.data_ptr() + 3 * 4
+            self.switch = switch = switch_norm is not None and switch_norm > 0
+            # the initial potential (paths do not depend on it; contact potentials are read on the device)
+            for (Kd, U0), o, N, Up in zip(ops, self.offs, self.Ns, U_ptrs):
+                affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, None, stream=stream)
+            self.plan = plan = ChargePlan(tubes, Q, autotune=autotune)
+            self.plan64 = plan64 = ChargePlan(tubes, Q, autotune=autotune, fp64=True) if switch else None
 
-        graph = None
-        if use_graph:
-            flags[3] = 1  # load every kernel once, all skipped
-            body(stream)
-            stream.synchronize()
-            graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph, stream=stream):
-                for _ in range(iters_per_graph):
-                    body(torch.cuda.current_stream())
-        for Vg in Vg_list:
-            for (Kd, U0), e in zip(ops, electros):
-                U0.copy_(e.device_operator(Vg)[1])
-            flags.zero_()
-            if switch:
-                flags[6] = 1  # the FP64 plan waits for the switch
-            stream.synchronize()
-            t0 = time.perf_counter()
-            while True:
-                if graph is not None:
-                    graph.replay()
+            def body(s):
+                for (Kd, U0), o, N, Up in zip(ops, self.offs, self.Ns, U_ptrs):
+                    affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip, stream=s)
+                if switch:
+                    plan.launch(skip=flags.data_ptr() + 5 * 4, stream=s)
+                    plan64.launch(skip=flags.data_ptr() + 6 * 4, stream=s)
+                    br.step_device_switch(Q, max_norm, switch_norm, flags, stream=s)
                 else:
-                    body(stream)
-                f = flags.cpu().numpy()
+                    plan.launch(skip=skip, stream=s)
+                    br.step_device(Q, max_norm, flags, stream=s)
+
+            self._body = body
+            self.graph = None
+            if use_graph:
+                flags[3] = 1  # load every kernel once, all skipped
+                body(stream)
+                stream.synchronize()
+                self.graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(self.graph, stream=stream):
+                    for _ in range(iters_per_graph):
+                        body(torch.cuda.current_stream())
+            stream.synchronize()
+
+    def set_external(self, Vg=None, U0=None):
+        """The external potential of the next solve: the electrostatics' at
+        gate voltage Vg, or U0 (one host array per tube)."""
+        import torch
+        with torch.cuda.stream(self.stream):
+            for t_, ((Kd, U0d), e) in enumerate(zip(self.ops, self.electros)):
+                if U0 is None:
+                    U0d.copy_(e.device_operator(Vg)[1])
+                else:
+                    U0d.copy_(torch.as_tensor(np.asarray(U0[t_], dtype=np.float64)), non_blocking=False)
+
+    def solve(self):
+        """Iterate to convergence from the current n_in; returns (steps,
+        low-precision steps).  Raises on MaxStep or a non-finite norm."""
+        import torch
+        with torch.cuda.stream(self.stream):
+            self.flags.zero_()
+            if self.switch:
+                self.flags[6] = 1  # the FP64 plan waits for the switch
+            while True:
+                if self.graph is not None:
+                    self.graph.replay()
+                else:
+                    self._body(self.stream)
+                f = self.flags.cpu().numpy()
                 if f[3]:
                     break
-            dt = time.perf_counter() - t0
-            if f[2] == 1:
-                raise RuntimeError("Broyden_Step has exceeded the Broyden_Threshold_MaxStep")
-            if f[2] == 2:
-                raise RuntimeError("non-finite Broyden norm")
-            U = np.concatenate([device_view(Up, N).cpu().numpy() for Up, N in zip(U_ptrs, Ns)])
-            st = StepResult(Vg, int(f[1]), float("nan"), Q.cpu().numpy().copy(), U, dt)
-            st.lowprec_iterations = int(f[7])
-            res.steps.append(st)
-            br.reset(keep_charge=reset_with_previous_charge, init_value=initial_charge, stream=stream)
-        stream.synchronize()
-    info = plan.info()
-    del graph
-    plan.close()
-    if plan64 is not None:
-        plan64.close()
-    br.close()
+        if f[2] == 1:
+            raise RuntimeError("Broyden_Step has exceeded the Broyden_Threshold_MaxStep")
+        if f[2] == 2:
+            raise RuntimeError("non-finite Broyden norm")
+        return int(f[1]), int(f[7])
+
+    def reset(self, keep_charge=False, init_value=None):
+        """Reset_ForNextBiasStep: clear the secant rows; n_in stays (keep_charge)
+        or becomes init_value (default: the initial charge)."""
+        v = self.initial_charge if init_value is None else float(init_value)
+        self.br.reset(keep_charge=keep_charge, init_value=v, stream=self.stream)
+
+    def potentials(self):
+        return np.concatenate([device_view(Up, N).cpu().numpy() for Up, N in zip(self.U_ptrs, self.Ns)])
+
+    def close(self):
+        self.stream.synchronize()
+        self.graph = None
+        self.plan.close()
+        if self.plan64 is not None:
+            self.plan64.close()
+        self.br.close()
+
+
+def run_scf_batch(tubes, electros, Vg_list, fraction=0.1, max_norm=1e-6, max_step=200, norm_type="absolute",
+                  initial_charge=0.0, reset_with_previous_charge=False, use_graph=True, iters_per_graph=8,
+                  autotune=True, switch_norm=None, segments=False):
+    """Self-consistent bias sweep of a batch of tubes (BatchSCF) with one
+    Broyden over all their sites, reset between bias points
+    (Reset_ForNextBiasStep, Transport.cpp:713-717).  Returns an SCFResult
+    plus the plan's schedule."""
+    import torch
+    scf = BatchSCF(tubes, electros, fraction=fraction, max_norm=max_norm, max_step=max_step, norm_type=norm_type,
+                   initial_charge=initial_charge, use_graph=use_graph, iters_per_graph=iters_per_graph,
+                   autotune=autotune, switch_norm=switch_norm, segments=segments)
+    res = SCFResult()
+    for Vg in Vg_list:
+        scf.set_external(Vg=Vg)
+        scf.stream.synchronize()
+        t0 = time.perf_counter()
+        it, low = scf.solve()
+        dt = time.perf_counter() - t0
+        with torch.cuda.stream(scf.stream):
+            st = StepResult(Vg, it, float("nan"), scf.Q.cpu().numpy().copy(), scf.potentials(), dt)
+        st.lowprec_iterations = low
+        res.steps.append(st)
+        scf.reset(keep_charge=reset_with_previous_charge)
+    info = scf.plan.info()
+    scf.close()
     res.schedule = info
     return res

@@ -1,44 +1,51 @@
 """Surrogate over a set of tubes: one Fourier neural operator for every tube of
-an uneven batch, and the surrogate-started self-consistent gate sweep.
+an uneven batch, trained on the batch's self-consistent fixed points, and the
+surrogate-started gate sweep.
 
-The operator of surrogate.py maps a fixed-length potential to the induced
-charge.  Here one operator serves the whole batch (tubes of 800-8000 sites,
-chiralities (13,0), (17,0), (19,0), 2-10 modes): every tube sits on a canvas
-of S sites (its own sites first, padding after), and per-site descriptors tell
-the operator which tube it reads.  One inference is then one batch of
-canvases, a fixed set of launches whatever the tube count.
+The operator of surrogate.py maps a fixed-length potential to a charge.  Here
+one operator serves the whole batch (tubes of 800-8000 sites, chiralities
+(13,0), (17,0), (19,0), 2-10 modes): every tube sits on a canvas of S sites
+(its own sites first, padding after), and per-site descriptors tell the
+operator which tube it reads.  One inference is one batch of canvases, a
+fixed set of launches whatever the tube count.
+
+What it maps: the EXTERNAL site potential U_ext of a tube (the gate and
+contact electrodes' potential with no charge on the tube) plus (Vg, Vds) to
+the tube's self-consistent charge n* (the fixed point n* = Q(U_ext + K n*) of
+the NEGF-Poisson loop).  One inference is then the Broyden start of a bias
+point; no surrogate loop runs.
 
 Features per site (FEAT_SET = 32):
-  0..16  U at sites n-8 .. n+8 of the tube (indices clamped to the tube: the
-         leads continue at the end-site potential), divided by the potential
-         scale
+  0..16  U_ext at sites n-8 .. n+8 of the tube (indices clamped to the tube:
+         the leads continue at the end-site potential), divided by the
+         potential scale
   17, 18 Vg, Vds
   19..31 n / N, ring parity +-1, exp(-n / 40), exp(-(N-1-n) / 40), inside
          mask, chirality one-hot (13, 17, 19), modes / 10, inner band edge of
          the lowest and of the highest kept mode / gamma, channels / 20, N / S
 
-Training pairs come from the engine itself (negf_compute_charge on the whole
-batch): half along self-consistent gate solves at random (Vg, Vds), half from
-the config-2 recipe of random potentials (external potential of the gate and
-contacts plus 5 seeded Gaussian bumps).  The loss is the mean square error
-over the tubes' own sites (padding is masked out).
+Training pairs come from the engine itself (generate_fixed_points): batched
+self-consistent solves of the whole set at random drain biases Vds ~ U(0,
+0.6) V (vds_bins levels: the tubes of one level share their energy paths)
+and per-tube gate voltages Vg ~ U(0, 0.8) V; in a bump_fraction of the solves
+the external potential also carries 5 seeded Gaussian bumps (the config-2
+recipe of random potentials), so the operator sees more than the
+two-parameter family of a gate sweep.  The loss is the mean square error over
+the tubes' own sites (padding masked out), per tube relative to its largest
+charge.
 
-The sweep (set_scf_sweep) follows scf.run_scf_batch -- one Broyden over all
-the tubes' sites, iterations replayed as CUDA graphs -- and adds the
-surrogate: per gate point, (1) the surrogate phase solves the loop with the
-surrogate's charge (a fresh Broyden solve started from the surrogate's
-previous fixed point, to the surrogate's own residual floor); (2) the NEGF
-phase starts from that charge with the surrogate solve's secant rows as its
-initial inverse Jacobian (negf_broyden_set_initial_jacobian; carry_rows
-carries the NEGF rows of the previous gate points instead,
-negf_broyden_restart), the scalar part fraction * I set from the surrogate's
-Jacobian (largest eigenvalue of I - dQ_s/dn by power iteration: fraction =
-2 / (1 + lambda_max), the optimal Richardson step for a spectrum in
-[1, lambda_max]).  The NEGF phase runs the mixed-precision plan until the
-residual falls below switch_norm and the FP64 plan after; only an FP64 NEGF
-charge ends a solve (the engine judges every converged charge).  A surrogate
-phase that does not converge is not used: the NEGF phase then starts from the
-previous gate point's charge.
+The sweep (fixed_point_sweep): per gate point, one inference gives the
+start, and a BatchSCF solve -- mixed-precision plan until the residual falls
+below switch_norm, the FP64 plan after, one secant update per tube
+(segments) -- converges it; only an FP64 NEGF charge ends a solve (the engine
+judges every converged charge).  The initial inverse Jacobian is
+fraction * I with fraction from the surrogate's Jacobian: the fixed-point
+map's derivative J = dn*/dU_ext = (I - chi K)^-1 chi gives J K = (I - chi
+K)^-1 chi K, whose eigenvalues are -lambda / (1 + lambda) for the
+eigenvalues 1 + lambda of the loop's Jacobian I - chi K; the largest
+|mu| by power iteration gives lambda_max = |mu| / (1 - |mu|) and
+fraction = 2 / (2 + lambda_max), the Richardson step for a spectrum in
+[1, 1 + lambda_max].
 """
 from __future__ import annotations
 
@@ -215,270 +222,163 @@ class TubeSetOperator(FourierOperator):
 
 
 # ---------------------------------------------------------------------- data
-def generate_set_pairs(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bins=13, scf_fraction=0.5,
-                       max_iter=40, S=None, log=None):
-    """n_pairs (canvas U, Vg, Vds, tube id, canvas Q) from the engine over the
-    tube set: half recorded along self-consistent solves of the whole set at
-    random gate Vg ~ U(0, 0.8) V and drain Vds ~ U(0, 0.6) V (vds_bins
-    levels: the tubes of one level share their energy paths), half from
-    random potentials of the config-2 recipe (the gate/contact stand-in's
-    external potential plus 5 seeded Gaussian bumps of amplitude up to a,
-    a ~ U(0, 0.4) V).  make_tubes(vds) returns the set's tubes at that drain
-    bias.  Returns device tensors and the seconds the engine spent."""
+def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bins=13, bump_fraction=0.5,
+                          bump_amp=0.2, tol=3e-6, fraction=0.3, S=None, log=None):
+    """n_pairs (canvas U_ext, Vg, Vds, tube id, canvas n*) from batched
+    self-consistent solves of the tube set (module docstring): per solve every
+    tube gets its own gate voltage, the drain bias is one of vds_bins levels
+    in [0, 0.6] V; solves to a max-norm residual of tol.  make_tubes(vds)
+    returns the set's tubes at that drain bias.  Returns device tensors, the
+    seconds of the solves and their iteration counts."""
     import torch
-    from .negf import Broyden, affine_potential_masked, compute_charge
-    from .scf import device_view
+    from .scf import BatchSCF
     from .workloads import site_potential
     rng = np.random.default_rng(seed)
     levels = np.linspace(0.0, 0.6, vds_bins)
-    cache = {}
     T = len(electros)
     dev = "cuda"
-
-    def tubes_at(lv):
-        if lv not in cache:
-            cache[lv] = make_tubes(lv)
-        return cache[lv]
-
     Ns = [e.N for e in electros]
     S = int(S or ((max(Ns) + 255) // 256) * 256)
-    offs = np.concatenate([[0], np.cumsum(Ns)]).astype(np.int64)
-    Stot = int(offs[-1])
-    U_all = torch.zeros(n_pairs, S, dtype=torch.float32, device=dev)
-    Q_all = torch.zeros(n_pairs, S, dtype=torch.float32, device=dev)
-    vg_all = np.zeros(n_pairs)
-    vd_all = np.zeros(n_pairs)
-    tid_all = np.zeros(n_pairs, dtype=np.int64)
-    Qcat = torch.zeros(Stot, dtype=torch.float64, device=dev)
+    n_solves = -(-n_pairs // T)
+    per_level = [n_solves // vds_bins + (1 if i < n_solves % vds_bins else 0) for i in range(vds_bins)]
+    U_all = torch.zeros(n_solves * T, S, dtype=torch.float32, device=dev)
+    Q_all = torch.zeros(n_solves * T, S, dtype=torch.float32, device=dev)
+    vg_all = np.zeros(n_solves * T)
+    vd_all = np.zeros(n_solves * T)
+    tid_all = np.tile(np.arange(T), n_solves)
     k = 0
-    engine = 0.0
-
-    def record(tubes, vg, lv):
-        nonlocal k
-        for t_, tube in enumerate(tubes):
-            if k >= n_pairs:
-                return
-            N = Ns[t_]
-            U_all[k, :N] = device_view(tube.potential_device_ptr(), N).float()
-            Q_all[k, :N] = Qcat[offs[t_]:offs[t_ + 1]].float()
-            vg_all[k], vd_all[k], tid_all[k] = vg, lv, t_
-            k += 1
-
-    def charge(tubes):
-        nonlocal engine
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        compute_charge(tubes, out=Qcat)
-        torch.cuda.synchronize()
-        engine += time.perf_counter() - t0
-
-    n_scf = int(n_pairs * scf_fraction)
-    while k < n_scf:  # pairs along self-consistent solves
-        lv = float(levels[rng.integers(0, vds_bins)])
-        vg = float(rng.uniform(0.0, 0.8))
-        tubes = tubes_at(lv)
-        ops = []
+    seconds, iters = 0.0, []
+    for lv, count in zip(levels, per_level):
+        if count == 0:
+            continue
+        lv = float(lv)
         for e in electros:
             e.Vds = lv
-            Kd, U0 = e.device_operator(vg)
-            ops.append((Kd, U0))
-        br = Broyden(torch.zeros(Stot, dtype=torch.float64, device=dev), max_step=max_iter + 2, fraction=0.1)
-        nin = br.input_device_ptr()
-        for _ in range(max_iter):
-            for (Kd, U0), o, tube, N in zip(ops, offs, tubes, Ns):
-                affine_potential_masked(Kd, U0, nin + 8 * int(o), tube.potential_device_ptr(), N, None)
-                U = device_view(tube.potential_device_ptr(), N)
-                ends = U[[0, N - 1]].cpu().numpy()
-                tube.set_potential_device(tube.potential_device_ptr(), (float(ends[0]), float(ends[1])))
-            charge(tubes)
-            record(tubes, vg, lv)
-            if not (br.step(Qcat) > 1e-6) or k >= n_scf:
-                break
-        br.close()
-        if log:
-            log("scf", k)
-    while k < n_pairs:  # random potentials of the config-2 recipe
-        lv = float(levels[rng.integers(0, vds_bins)])
-        vg = float(rng.uniform(0.0, 0.8))
-        tubes = tubes_at(lv)
-        for t_, (tube, e) in enumerate(zip(tubes, electros)):
-            e.Vds = lv
-            amp = rng.uniform(0.0, 0.4)
-            U = e.external(vg) + site_potential(e.y_nm, int(rng.integers(1 << 30)), amp=amp, ramp=0.0)
-            tube.set_potential(U, (U[0], U[-1]))
-        charge(tubes)
-        record(tubes, vg, lv)
-        if log:
-            log("random", k)
-    for tubes in cache.values():
+        tubes = make_tubes(lv)
+        scf = BatchSCF(tubes, electros, fraction=fraction, max_norm=tol, iters_per_graph=4, segments=True)
+        for _ in range(count):
+            U0 = []
+            for t_, e in enumerate(electros):
+                vg = float(rng.uniform(0.0, 0.8))
+                u = e.external(vg)
+                if rng.uniform() < bump_fraction:
+                    u = u + site_potential(e.y_nm, int(rng.integers(1 << 30)), amp=float(rng.uniform(0.0, bump_amp)),
+                                           ramp=0.0)
+                U0.append(u)
+                U_all[k + t_, :Ns[t_]] = torch.as_tensor(u, dtype=torch.float32, device=dev)
+                vg_all[k + t_], vd_all[k + t_] = vg, lv
+            scf.set_external(U0=U0)
+            scf.reset(keep_charge=False)
+            scf.stream.synchronize()
+            t0 = time.perf_counter()
+            it, _ = scf.solve()
+            scf.stream.synchronize()
+            seconds += time.perf_counter() - t0
+            iters.append(it)
+            for t_ in range(T):
+                Q_all[k + t_, :Ns[t_]] = scf.n_in[scf.offs[t_]:scf.offs[t_ + 1]].float()
+            k += T
+            if log:
+                log(lv, k, it)
+        scf.close()
         for tube in tubes:
             tube.close()
-    return (U_all, torch.tensor(vg_all, dtype=torch.float32, device=dev),
-            torch.tensor(vd_all, dtype=torch.float32, device=dev), torch.tensor(tid_all, device=dev), Q_all, engine)
+    order = torch.tensor(rng.permutation(k)[:n_pairs], device=dev)
+    return (U_all[order], torch.tensor(vg_all, dtype=torch.float32, device=dev)[order],
+            torch.tensor(vd_all, dtype=torch.float32, device=dev)[order], torch.tensor(tid_all, device=dev)[order],
+            Q_all[order], seconds, iters)
 
 
 # ---------------------------------------------------------------------- SCF
-def set_scf_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6, max_step=200, switch_norm=1e-5,
-                  surrogate_norm=None, surrogate_max_step=60, seed_rows=True, carry_rows=False, iters_per_graph=4,
-                  power_iters=6, autotune=True):
+def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6, max_step=200,
+                      switch_norm=1e-5, segments=True, iters_per_graph=4, power_iters=6, autotune=True,
+                      use_surrogate=True):
     """Surrogate-started gate sweep of a tube set (module docstring).  Tubes
-    in mixed precision run the NEGF phase on their own plan until the
-    residual falls below switch_norm, then on an FP64 plan.  fraction: the
-    scalar part of the initial inverse Jacobian (None: from the surrogate's
-    Jacobian).  Returns per-step records, the chosen fraction and the
+    in mixed precision run on their own plan until the residual falls below
+    switch_norm, then on an FP64 plan.  fraction: the scalar initial inverse
+    Jacobian (None: from the surrogate's Jacobian).  use_surrogate=False
+    starts every point from zero charge (the same solver without the
+    surrogate).  Returns per-step records, the fraction, lambda_max and the
     one-off set-up seconds (plans, graphs; outside the per-step times)."""
     import torch
     from . import negf as ng
-    from .scf import device_view
+    from .scf import BatchSCF
     dev = "cuda"
     Ns = [t.num_field_sites for t in tubes]
     offs = np.concatenate([[0], np.cumsum(Ns)]).astype(np.int64)
     S = int(offs[-1])
     stream = torch.cuda.Stream()
+    vds = float(electros[0].Vds)
     t_setup = time.perf_counter()
-    if surrogate_norm is None:  # the surrogate's own residual floor: BF16 inputs, ~0.2% of its charge scale
-        surrogate_norm = 2e-3 * float(model.q_scale)
-    out = []
     with torch.cuda.stream(stream):
-        Q = torch.zeros(S, dtype=torch.float64, device=dev)
-        Qs = torch.zeros(S, dtype=torch.float64, device=dev)
         Ucat = torch.zeros(S, dtype=torch.float64, device=dev)
-        ops = []
-        for e in electros:
-            Kd, U0 = e.device_operator(Vg_list[0])
-            ops.append((Kd, U0.clone()))
-        U_ptrs = [t.potential_device_ptr() for t in tubes]
-        model.bind_set(Ucat, Qs, Vg_list[0], electros[0].Vds)
-        # surrogate-phase residual map F_s(n) = n - Q_s(U0 + K n) for the power iteration
-        ncur = torch.zeros(S, dtype=torch.float64, device=dev)
+        Qs = torch.zeros(S, dtype=torch.float64, device=dev)
+        zero = torch.zeros(max(Ns), dtype=torch.float64, device=dev)
+        Kds = [e.device_operator(Vg_list[0])[0] for e in electros]
+        model.bind_set(Ucat, Qs, Vg_list[0], vds)
 
-        def F_s(n):
-            for (Kd, U0), o, N in zip(ops, offs, Ns):
-                ng.affine_potential_masked(Kd, U0, n.data_ptr() + 8 * int(o), Ucat.data_ptr() + 8 * int(o), N, None,
-                                           stream=stream)
-            model.infer_set()
-            return n - Qs
+        def external(Vg):
+            for e, o, N in zip(electros, offs, Ns):
+                Ucat[int(o):int(o) + N].copy_(e.device_operator(Vg)[1])
 
-        F_s(ncur)  # allocates the model's inference buffers
+        external(Vg_list[0])
+        model.infer_set()  # allocates the model's inference buffers
         stream.synchronize()
-        t_setup = time.perf_counter() - t_setup
-        # ---- timed from here: the scalar part of G0 from the surrogate's Jacobian
-        t0 = time.perf_counter()
-        alpha = fraction
-        lam = None
+    t_setup = time.perf_counter() - t_setup
+    # ---- timed: the scalar initial inverse Jacobian from the surrogate's Jacobian (power iteration on J K)
+    t0 = time.perf_counter()
+    alpha, lam = fraction, None
+    with torch.cuda.stream(stream):
         if alpha is None:
             g = torch.Generator(device="cpu").manual_seed(0)
             v = torch.randn(S, generator=g, dtype=torch.float64).to(dev)
             v /= v.norm()
-            F0 = F_s(ncur).clone()
-            # the surrogate reads BF16 potentials (about 2e-3 V resolution here): size each
-            # step so that the potential moves by about 0.02 V
-            kmax = max(float(Kd.abs().sum(dim=1).max()) for Kd, _ in ops)
-            for _ in range(power_iters):
-                eps = 0.02 / (kmax * float(v.abs().max()))
-                w = (F_s(ncur + eps * v) - F0) / eps
-                lam = float(w.norm())
-                v = w / lam
-            alpha = float(min(1.0, max(0.1, 2.0 / (1.0 + lam))))
-        t_alpha = time.perf_counter() - t0
-        t_setup2 = time.perf_counter()
-        brn = ng.Broyden(torch.zeros(S, dtype=torch.float64, device=dev), max_step=max_step, fraction=alpha,
-                         stream=stream)
-        brs = ng.Broyden(torch.zeros(S, dtype=torch.float64, device=dev), max_step=max_step, fraction=alpha,
-                         stream=stream)
-        nin = brn.input_device_ptr()
-        nin_s = brs.input_device_ptr()
-        nin_t = device_view(nin, S)
-        nin_s_t = device_view(nin_s, S)
-        flags = torch.zeros(8, dtype=torch.int32, device=dev)
-        flags_s = torch.zeros(8, dtype=torch.int32, device=dev)
-        skip = flags.data_ptr() + 12
-        switch = switch_norm is not None and switch_norm > 0 and any(t.desc.precision == 1 for t in tubes)
-        for (Kd, U0), o, N, Up in zip(ops, offs, Ns, U_ptrs):
-            ng.affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, None, stream=stream)
-        plan = ng.ChargePlan(tubes, Q, autotune=autotune)
-        plan64 = ng.ChargePlan(tubes, Q, autotune=autotune, fp64=True) if switch else None
-
-        def body(s):
-            for (Kd, U0), o, N, Up in zip(ops, offs, Ns, U_ptrs):
-                ng.affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip, stream=s)
-            if switch:
-                plan.launch(skip=flags.data_ptr() + 5 * 4, stream=s)
-                plan64.launch(skip=flags.data_ptr() + 6 * 4, stream=s)
-                brn.step_device_switch(Q, max_norm, switch_norm, flags, stream=s)
-            else:
-                plan.launch(skip=skip, stream=s)
-                brn.step_device(Q, max_norm, flags, stream=s)
-
-        def sbody(s):
-            sk = flags_s.data_ptr() + 12
-            for (Kd, U0), o, N in zip(ops, offs, Ns):
-                ng.affine_potential_masked(Kd, U0, nin_s + 8 * int(o), Ucat.data_ptr() + 8 * int(o), N, sk, stream=s)
+            U0 = Ucat.clone()
             model.infer_set()
-            brs.step_device(Qs, surrogate_norm, flags_s, stream=s)
-
-        flags[3] = 1
-        flags_s[3] = 1
-        body(stream)
-        sbody(stream)
+            q0 = Qs.clone()
+            Kv = torch.empty(S, dtype=torch.float64, device=dev)
+            mu = 0.0
+            for _ in range(power_iters):
+                for Kd, o, N in zip(Kds, offs, Ns):
+                    ng.affine_potential_masked(Kd, zero, v.data_ptr() + 8 * int(o), Kv.data_ptr() + 8 * int(o), N,
+                                               None, stream=stream)
+                # the operator reads BF16 potentials: move them by about 0.02 V
+                eps = 0.02 / float(Kv.abs().max())
+                torch.add(U0, Kv, alpha=eps, out=Ucat)
+                model.infer_set()
+                w = (Qs - q0) / eps
+                mu = float(w.norm())
+                v = w / mu
+            Ucat.copy_(U0)
+            mu = min(mu, 0.95)
+            lam = mu / (1.0 - mu)
+            alpha = float(min(0.5, max(0.1, 2.0 / (2.0 + lam))))
         stream.synchronize()
-        graph, sgraph = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph, stream=stream):
-            for _ in range(iters_per_graph):
-                body(torch.cuda.current_stream())
-        with torch.cuda.graph(sgraph, stream=stream):
-            for _ in range(iters_per_graph):
-                sbody(torch.cuda.current_stream())
+    t_alpha = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    switch = switch_norm if any(t.desc.precision == 1 for t in tubes) else None
+    scf = BatchSCF(tubes, electros, fraction=alpha, max_norm=max_norm, max_step=max_step,
+                   iters_per_graph=iters_per_graph, autotune=autotune, switch_norm=switch, segments=segments)
+    t_setup += time.perf_counter() - t1
+    out = []
+    for step, Vg in enumerate(Vg_list):
         stream.synchronize()
-        t_setup += time.perf_counter() - t_setup2
-        for step, Vg in enumerate(Vg_list):
-            t0 = time.perf_counter()
-            for (Kd, U0), e in zip(ops, electros):
-                U0.copy_(e.device_operator(Vg)[1])
-            model.set_bias_set(Vg, electros[0].Vds)
-            # (1) surrogate phase: a fresh Broyden solve with the surrogate's charge,
-            # continued from the surrogate's previous fixed point
-            brs.reset(keep_charge=True, stream=stream)
-            flags_s.zero_()
-            while True:
-                sgraph.replay()
-                fs = flags_s.cpu().numpy()
-                if fs[3] or fs[1] >= surrogate_max_step:
-                    break
-            sur_it = int(fs[1])
-            used = bool(fs[0]) and not fs[2]
-            # (2) NEGF phase from the surrogate's charge (else from the previous NEGF
-            # charge); initial inverse Jacobian: the surrogate solve's secant rows, or
-            # the NEGF rows of the previous gate points (carry_rows)
-            if carry_rows and step > 0:
-                brn.restart(keep_rows=max_step // 2, stream=stream)
-            else:
-                brn.reset(keep_charge=True, stream=stream)
-            if used:
-                nin_t.copy_(nin_s_t)
-                if seed_rows and not (carry_rows and step > 0):
-                    V, W, rows = brs.history(stream=stream)
-                    if 0 < rows <= max_step // 2:
-                        brn.set_initial_jacobian(V.contiguous(), W.contiguous(), stream=stream)
-            flags.zero_()
-            if switch:
-                flags[6] = 1
-            while True:
-                graph.replay()
-                f = flags.cpu().numpy()
-                if f[3]:
-                    break
-            dt = time.perf_counter() - t0 + (t_alpha if step == 0 else 0.0)
-            if f[2]:
-                raise RuntimeError("NEGF self-consistency failed (flag %d) at Vg = %g" % (f[2], Vg))
-            out.append(dict(Vg=float(Vg), negf_iterations=int(f[1]), lowprec_iterations=int(f[7]),
-                            surrogate_iterations=sur_it, surrogate_used=used, seconds=dt, Q=Q.cpu().numpy().copy(),
-                            n_in=nin_t.cpu().numpy().copy()))
-        stream.synchronize()
-    del graph, sgraph
-    plan.close()
-    if plan64 is not None:
-        plan64.close()
-    brn.close()
-    brs.close()
+        scf.stream.synchronize()
+        t0 = time.perf_counter()
+        scf.set_external(Vg=Vg)
+        scf.reset(keep_charge=use_surrogate, init_value=0.0)
+        if use_surrogate:
+            with torch.cuda.stream(scf.stream):
+                external(Vg)
+                model.set_bias_set(Vg, vds)
+                model.infer_set()
+                scf.n_in.copy_(Qs)
+        it, low = scf.solve()
+        scf.stream.synchronize()
+        dt = time.perf_counter() - t0 + (t_alpha if step == 0 else 0.0)
+        with torch.cuda.stream(scf.stream):
+            start = Qs.cpu().numpy().copy() if use_surrogate else np.zeros(S)
+            out.append(dict(Vg=float(Vg), negf_iterations=it, lowprec_iterations=low, seconds=dt,
+                            Q=scf.Q.cpu().numpy().copy(), n_in=scf.n_in.cpu().numpy().copy(), start=start))
+    scf.close()
     return out, alpha, lam, t_setup

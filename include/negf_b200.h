@@ -405,6 +405,19 @@ int negf_broyden_set_initial_jacobian(negf_broyden* b, const double* d_V, const 
  * rows count against max_step.
  * Synchronises `stream` (it reads the step counters). */
 int negf_broyden_restart(negf_broyden* b, int keep_rows, void* stream);
+/* Per-segment secant updates (no counterpart in the reference, whose one
+ * Broyden mixes the sites of all nanostructures with whole-vector dot
+ * products, Broyden_Second_Parallel.cpp:213-486): the sites split into nseg
+ * segments, offsets[0] = 0 < offsets[1] < ... < offsets[nseg] = num_sites
+ * (host array), and every dot product of the update (V^T dF, V^T F and the
+ * dF^T dF of a new row) runs over each segment's sites separately.  The
+ * update is then block diagonal: nseg independent Broyden mixers in one
+ * set of launches, which suits a batch of tubes whose potentials do not
+ * couple (one segment per tube).  The norm and the stopping rule stay over
+ * all sites.  nseg = 1 restores the whole-vector update.  Call after create
+ * or reset, before seeding rows and before the first step; the setting
+ * survives resets and restarts.  Synchronises the device. */
+int negf_broyden_set_segments(negf_broyden* b, int nseg, const int* offsets, void* stream);
 /* The secant rows held now (seeded rows first): device pointers of rows
  * 1 .. *rows of V and W ([rows][S] each, valid until the next step, reset or
  * restart), e.g. to seed another Broyden with negf_broyden_set_initial_jacobian

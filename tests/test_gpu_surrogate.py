@@ -110,3 +110,47 @@ def test_surrogate_started_sweep_is_judged_by_negf():
     sur = S.scf_sweep(tube, el, [0.1, 0.3], 0.3, model=m, keep_history=False)
     for a, b in zip(plain, sur):
         assert np.max(np.abs(a["Q"] - b["Q"])) < 1e-5
+
+
+def test_fixed_point_surrogate_set_sweep():
+    """Tube-set pipeline on three small tubes: fixed-point pairs from batched
+    self-consistent solves (per-tube secant updates), a short training, and a
+    surrogate-started mixed-precision sweep whose converged charges are NEGF
+    fixed points of the FP64 plain sweep (same 1e-6 residual; the mixed
+    precision's own error stays below 1e-5 of the charge)."""
+    import numpy as np
+    from electrostatic_b200.electrostatics import GateAllAround
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.scf import run_scf_batch
+    from electrostatic_b200.surrogate_set import (TubeSetOperator, fixed_point_sweep, generate_fixed_points,
+                                                  tube_descriptor)
+    specs = [((17, 0), 24, 2), ((13, 0), 40, 3), ((19, 0), 16, 2)]
+
+    def make(lv, precision="fp64"):
+        return [CNT(type_id=ch, num_unitcells=uc, num_modes=m, contact_mu=(0.0, -float(lv)), contact_T=(300.0, 300.0),
+                    eq_integration_pts=(16, 16, 24), noneq_integration_pts=(32,), E_zPlus_imag=2e-3, E_pole_max=3.0,
+                    precision=precision, mixed_realaxis_fp32=precision == "mixed") for ch, uc, m in specs]
+
+    tubes = make(0.2)
+    electros = [GateAllAround(t.site_positions(), 0.0665e-9 * ch[0] / 17 * 10,
+                              1.5e-9 + 0.0665e-9 * ch[0] / 17 * 10, contact_length=1e-9, Vds=0.2)
+                for t, (ch, _, _) in zip(tubes, specs)]
+    U, Vg, Vds, tid, Q, secs, its = generate_fixed_points(make, electros, 96, vds_bins=2)
+    assert U.shape[0] == 96 and np.isfinite(Q.cpu().numpy()).all() and secs > 0 and len(its) == 32
+    for e in electros:
+        e.Vds = 0.2
+    model = TubeSetOperator([tube_descriptor(t) for t in tubes], seed=0)
+    model.fit_set(U, Vg, Vds, tid, Q, epochs=3, batch=16)
+    plain = run_scf_batch(tubes, electros, [0.1, 0.3], use_graph=True, iters_per_graph=4)
+    mixed = make(0.2, "mixed")
+    out, alpha, lam, _ = fixed_point_sweep(mixed, electros, [0.1, 0.3], model)
+    assert 0.1 <= alpha <= 0.5 and lam is not None
+    for r, p in zip(out, plain.steps):
+        assert r["negf_iterations"] > 0
+        assert np.max(np.abs(r["Q"] - p.Q)) <= 1e-5 * np.max(np.abs(p.Q)) + 2e-6
+    # segments with the plain solver's settings: the same fixed points
+    seg = run_scf_batch(make(0.2), electros, [0.1, 0.3], use_graph=True, iters_per_graph=4, segments=True)
+    for a, b in zip(seg.steps, plain.steps):
+        assert np.max(np.abs(a.Q - b.Q)) <= 2e-6
+    for t in tubes + mixed:
+        t.close()

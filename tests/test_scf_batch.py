@@ -120,20 +120,29 @@ def test_broyden_initial_jacobian_exact_inverse():
         small.set_initial_jacobian(V, W)
 
 
-def _np_broyden(n, F_of, steps, alpha, W=None, V=None):
+def _np_broyden(n, F_of, steps, alpha, W=None, V=None, offsets=None):
     """Modified-second Broyden in numpy (Broyden_Second_Parallel.cpp:9-211)
-    starting from secant rows W, V; returns the iterates and the rows."""
+    starting from secant rows W, V; returns the iterates and the rows.
+    offsets: per-segment dot products (the segmented update)."""
     W, V = list(W or []), list(V or [])
     Fp = npv = None
     out = []
+    off = [0, len(n)] if offsets is None else list(offsets)
+
+    def dot(a, b):  # per-segment a.b broadcast over the segment's sites
+        r = np.empty(len(a))
+        for lo, hi in zip(off[:-1], off[1:]):
+            r[lo:hi] = a[lo:hi] @ b[lo:hi]
+        return r
+
     for _ in range(steps):
         F = F_of(n)
         if Fp is not None:
             dF = F - Fp
-            s = sum(w * (v @ dF) for w, v in zip(W, V)) if W else 0.0
+            s = sum(w * dot(v, dF) for w, v in zip(W, V)) if W else 0.0
             W.append(-alpha * dF + (n - npv) - s)
-            V.append(dF / (dF @ dF))
-        step = alpha * F + (sum(w * (v @ F) for w, v in zip(W, V)) if W else 0.0)
+            V.append(dF / dot(dF, dF))
+        step = alpha * F + (sum(w * dot(v, F) for w, v in zip(W, V)) if W else 0.0)
         Fp, npv = F, n.copy()
         n = n - step
         out.append(n.copy())
@@ -165,6 +174,47 @@ def test_broyden_restart_carries_rows(keep):
             np.testing.assert_allclose(_read(br.input_device_ptr(), S), ref[k], rtol=1e-9, atol=1e-12)
         br.restart(keep_rows=keep)
         assert br.step_number == 1
+
+
+@pytest.mark.parametrize("device_steps", [False, True])
+def test_broyden_segments_match_numpy(device_steps):
+    """negf_broyden_set_segments: per-segment secant updates on a block-diagonal
+    linear map (three segments of uneven length) match the numpy twin step by
+    step, through host steps and device-resident steps alike; one segment
+    [0, S] is the whole-vector update bit for bit."""
+    import torch
+    from electrostatic_b200.negf import Broyden
+    off = [0, 7, 20, 33]
+    S = off[-1]
+    rng = np.random.default_rng(11)
+    A = np.zeros((S, S))
+    for lo, hi in zip(off[:-1], off[1:]):
+        A[lo:hi, lo:hi] = 0.6 * rng.standard_normal((hi - lo, hi - lo)) / np.sqrt(hi - lo)
+    b = rng.standard_normal(S)
+    alpha = 0.3
+    ref, _, _ = _np_broyden(np.zeros(S), lambda n: n - (A @ n + b), 8, alpha, offsets=off)
+    br = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"), max_step=40, fraction=alpha)
+    br.set_segments(off)
+    flags = torch.zeros(4, dtype=torch.int32, device="cuda")
+    for k in range(len(ref)):
+        x = torch.from_numpy(A @ _read(br.input_device_ptr(), S) + b).cuda()
+        if device_steps:
+            br.step_device(x, 0.0, flags)
+        else:
+            br.step(x)
+        np.testing.assert_allclose(_read(br.input_device_ptr(), S), ref[k], rtol=1e-9, atol=1e-12)
+    # one segment: bitwise the default update
+    runs = []
+    for segs in (None, [0, S]):
+        br2 = Broyden(torch.zeros(S, dtype=torch.float64, device="cuda"), max_step=40, fraction=alpha)
+        if segs is not None:
+            br2.set_segments(segs)
+        for k in range(6):
+            br2.step(torch.from_numpy(A @ _read(br2.input_device_ptr(), S) + b).cuda())
+        runs.append(_read(br2.input_device_ptr(), S))
+        br2.close()
+    assert np.array_equal(runs[0], runs[1])
+    br.close()
 
 
 def _read(ptr, n):
