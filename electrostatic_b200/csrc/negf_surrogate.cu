@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdint>
 
 #include "negf_internal.h"
 
@@ -69,9 +70,30 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
     if (Cb) Cb += bz * sC;
     const __nv_bfloat16 zero = __float2bfloat16(0.0f);
 
-    // staging: 16 elements of A and 16 of B per thread per k-tile, index i = tid + NT * j
+    // staging: 16 elements of A and 16 of B per thread per k-tile.  Tiles that
+    // lie inside the matrix with 16-byte aligned rows go through two 16-byte
+    // vector loads per operand (fast path); edge tiles through bounds-checked
+    // element loads, index i = tid + NT * j.
+    const bool alignA = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda % 8 == 0);
+    const bool alignB = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb % 8 == 0);
     __nv_bfloat16 ra[16], rb[16];
+    uint4 va[2], vb[2];
+    bool fa = false, fb = false;
     auto load_tile = [&](int k0) {
+        fa = alignA && m0 + BM <= M && k0 + BK <= kend;
+        fb = alignB && n0 + BN <= N && k0 + BK <= kend;
+        if (fa) {
+            const uint4* p = AT ? reinterpret_cast<const uint4*>(A + (size_t)(k0 + (tid >> 3)) * lda + m0 + (tid & 7) * 16)
+                                : reinterpret_cast<const uint4*>(A + (size_t)(m0 + (tid >> 1)) * lda + k0 + (tid & 1) * 16);
+            va[0] = p[0];
+            va[1] = p[1];
+        }
+        if (fb) {
+            const uint4* p = BT ? reinterpret_cast<const uint4*>(B + (size_t)(n0 + (tid >> 1)) * ldb + k0 + (tid & 1) * 16)
+                                : reinterpret_cast<const uint4*>(B + (size_t)(k0 + (tid >> 3)) * ldb + n0 + (tid & 7) * 16);
+            vb[0] = p[0];
+            vb[1] = p[1];
+        }
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int i = tid + NT * j;
@@ -85,7 +107,7 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
                 k = i % BK;
             }
             const int gm = m0 + m, gk = k0 + k;
-            ra[j] = (gm < M && gk < kend) ? A[a_off<AT>(gm, gk, lda)] : zero;
+            if (!fa) ra[j] = (gm < M && gk < kend) ? A[a_off<AT>(gm, gk, lda)] : zero;
             int n, kb;
             if (BT) {
                 n = i / BK;
@@ -95,31 +117,59 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
                 n = i % BN;
             }
             const int gn = n0 + n, gkb = k0 + kb;
-            rb[j] = (gn < N && gkb < kend) ? B[b_off<BT>(gkb, gn, ldb)] : zero;
+            if (!fb) rb[j] = (gn < N && gkb < kend) ? B[b_off<BT>(gkb, gn, ldb)] : zero;
         }
     };
     auto store_tile = [&](int buf) {
+        if (fa) {
+            if (AT) {  // 16 consecutive m of one k: transpose into the k-contiguous rows
+                const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(va);
+                const int k = tid >> 3, mh = (tid & 7) * 16;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) As[buf][mh + q][k] = e[q];
+            } else {
+                const int m = tid >> 1, kh = (tid & 1) * 16;
+                *reinterpret_cast<uint4*>(&As[buf][m][kh]) = va[0];
+                *reinterpret_cast<uint4*>(&As[buf][m][kh + 8]) = va[1];
+            }
+        }
+        if (fb) {
+            if (BT) {
+                const int n = tid >> 1, kh = (tid & 1) * 16;
+                *reinterpret_cast<uint4*>(&Bs[buf][n][kh]) = vb[0];
+                *reinterpret_cast<uint4*>(&Bs[buf][n][kh + 8]) = vb[1];
+            } else {
+                const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(vb);
+                const int k = tid >> 3, nh = (tid & 7) * 16;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) Bs[buf][nh + q][k] = e[q];
+            }
+        }
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int i = tid + NT * j;
-            int m, k;
-            if (AT) {
-                k = i / BM;
-                m = i % BM;
-            } else {
-                m = i / BK;
-                k = i % BK;
+            if (!fa) {
+                int m, k;
+                if (AT) {
+                    k = i / BM;
+                    m = i % BM;
+                } else {
+                    m = i / BK;
+                    k = i % BK;
+                }
+                As[buf][m][k] = ra[j];
             }
-            As[buf][m][k] = ra[j];
-            int n, kb;
-            if (BT) {
-                n = i / BK;
-                kb = i % BK;
-            } else {
-                kb = i / BN;
-                n = i % BN;
+            if (!fb) {
+                int n, kb;
+                if (BT) {
+                    n = i / BK;
+                    kb = i % BK;
+                } else {
+                    kb = i / BN;
+                    n = i % BN;
+                }
+                Bs[buf][n][kb] = rb[j];
             }
-            Bs[buf][n][kb] = rb[j];
         }
     };
 

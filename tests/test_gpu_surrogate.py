@@ -8,7 +8,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("at,bt", [(0, 0), (0, 1), (1, 0), (1, 1)])
-@pytest.mark.parametrize("M,N,K,batch", [(130, 70, 45, 3), (1, 128, 300, 1), (256, 256, 4, 2), (64, 256, 257, 1)])
+@pytest.mark.parametrize("M,N,K,batch", [(130, 70, 45, 3), (1, 128, 300, 1), (256, 256, 4, 2), (64, 256, 257, 1),
+                                         (200, 136, 160, 2), (128, 128, 2048, 1)])
 def test_gemm_layouts(at, bt, M, N, K, batch):
     import torch
     from electrostatic_b200 import _lib
