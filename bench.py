@@ -385,19 +385,24 @@ def long_tube_measure(torch, reps=10):
             "max_rel_automatic_vs_one_piece": float(np.max(np.abs(Qa - Q1)) / np.max(np.abs(Q1)))}
 
 
-def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True, ablation=True):
+# config 5 in the default run: fewer training pairs and epochs than the stated 20k / 20
+CONFIG5_COMPACT = dict(n_pairs=6000, epochs=12)
+
+
+def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True, ablation=True,
+                    keep_arrays=False):
     """Surrogate-assisted self-consistency on the config-4 tube set (16
-    tubes): one Fourier operator for the whole set (6 layers, width 128, 32
-    frequencies, BF16 weights, FP32 accumulation) trained on n_pairs
-    (external potential, self-consistent charge) pairs that the engine's own
-    batched solves produce; then the Vds = 0.4 V gate sweep 0 -> 0.6 V:
-    plain (FP64 tubes, one Broyden over the set with fraction 0.1 from zero
-    charge at every gate point: the reference's defaults) and
-    surrogate-started (mixed-precision tubes, one inference per gate point as
-    the start, fraction from the surrogate's Jacobian, one secant update per
-    tube, FP64 finish).  Per-step times exclude the one-off plans and graph
-    captures of both sweeps; data generation and training are reported
-    separately."""
+    tubes): one neural operator for the whole set (6 layers, width 128, 64
+    cosine modes of each tube's length, BF16 weights, FP32 accumulation)
+    trained on n_pairs (external potential, self-consistent charge) pairs
+    that the engine's own batched solves produce; then the Vds = 0.4 V gate
+    sweep 0 -> 0.6 V: plain (FP64 tubes, one Broyden over the set with
+    fraction 0.1 from zero charge at every gate point: the reference's
+    defaults) and surrogate-started (mixed-precision tubes, start from the
+    operator, fraction from the operator's Jacobian, one secant update per
+    tube, FP64 finish), with the same solver from other starts beside it.
+    Per-step times exclude the one-off plans and graph captures of every
+    sweep; data generation and training are reported separately."""
     from electrostatic_b200.negf import CNT
     from electrostatic_b200.scf import run_scf_batch
     from electrostatic_b200.surrogate_set import (TubeSetOperator, fixed_point_sweep, generate_fixed_points,
@@ -440,40 +445,53 @@ def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True
     # surrogate-started, mixed precision (contour and real-axis chains in FP32 at 2 meV broadening)
     tubesmx = make(vds, precision="mixed", realaxis_fp32=True)
     fixed_point_sweep(tubesmx, electros, [0.0], model)  # warm-up
-    sur, alpha, lam, t_setup = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model)
+    sur, alpha, lam, t_setup = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, start="difference")
     t_plain = sum(s_.seconds for s_ in plain.steps)
     t_cont = sum(s_.seconds for s_ in cont.steps)
     t_sur = sum(r["seconds"] for r in sur)
     qref = [s_.Q for s_ in plain.steps]
     dq = max(float(np.max(np.abs(r["Q"] - q))) / float(np.max(np.abs(q))) for r, q in zip(sur, qref))
-    start_err = [float(np.max(np.abs(r["start"] - q)) / np.max(np.abs(q))) for r, q in zip(sur, qref)]
+
+    def rel(a, q):
+        return float(np.max(np.abs(a - q)) / np.max(np.abs(q)))
+
     res = {"workload": "config-4 tube set (16 tubes), Vds 0.4 V, Vg 0..0.6 V step 0.05, 1e-6 absolute max-norm; "
-                       "operator 6 layers x width 128 x 32 frequencies on a %d-site canvas, BF16 weights, FP32 "
-                       "accumulation, trained on self-consistent fixed points" % model.S,
+                       "operator 6 layers x width 128 x 64 cosine modes of each tube's length (32 mixing pairs), "
+                       "BF16 weights, FP32 accumulation, trained on self-consistent fixed points",
            "pairs": n_pairs, "data_seconds": t_data, "data_solve_seconds": eng,
-           "data_mean_iterations": float(np.mean(data_iters)), "train_seconds": fit["seconds"], "epochs": epochs,
-           "batch": batch, "final_loss": fit["loss"][-1], "test_rel_err_median": float(np.median(err)),
-           "test_rel_err_p90": float(np.percentile(err, 90)), "test_rms_rel_err_median": float(np.median(rms)),
+           "data_mean_iterations": float(np.mean([i for i in data_iters if i > 0])),
+           "data_failed_solves": int(sum(1 for i in data_iters if i < 0)), "train_seconds": fit["seconds"],
+           "epochs": epochs, "batch": batch, "final_loss": fit["loss"][-1],
+           "test_rel_err_median": float(np.median(err)), "test_rel_err_p90": float(np.percentile(err, 90)),
+           "test_rms_rel_err_median": float(np.median(rms)),
            "plain": {"iterations": [s_.iterations for s_ in plain.steps], "seconds": t_plain,
                      "method": "FP64 tubes, one Broyden over the set, fraction 0.1, n = 0 at every gate point "
                                "(reference defaults)"},
-           "surrogate_started": {"negf_iterations": [r["negf_iterations"] for r in sur],
-                                 "fp32_iterations": [r["lowprec_iterations"] for r in sur], "seconds": t_sur,
-                                 "start_rel_err": start_err, "fraction": alpha, "lambda_max": lam,
-                                 "setup_seconds_excluded": t_setup,
-                                 "method": "mixed-precision tubes (FP32 contour and real-axis chains, FP64 finish "
-                                           "below 1e-5); start = one surrogate inference; initial inverse Jacobian "
-                                           "fraction * I with fraction = 2 / (2 + lambda_max) from the surrogate's "
-                                           "Jacobian; one secant update per tube"},
            "plain_continuation": {"iterations": [s_.iterations for s_ in cont.steps], "seconds": t_cont,
                                   "method": "as plain, n_in carried from the previous gate point"},
+           "surrogate_started": {"negf_iterations": [r["negf_iterations"] for r in sur],
+                                 "fp32_iterations": [r["lowprec_iterations"] for r in sur], "seconds": t_sur,
+                                 "start_rel_err": [rel(r["start"], q) for r, q in zip(sur, qref)],
+                                 "surrogate_rel_err": [rel(r["surrogate"], q) for r, q in zip(sur, qref)],
+                                 "fraction": alpha, "lambda_max": lam, "setup_seconds_excluded": t_setup,
+                                 "method": "mixed-precision tubes (FP32 contour and real-axis chains, FP64 finish "
+                                           "below 1e-5); start = previous converged charge + the operator's change "
+                                           "between the gate points (the operator's charge at the first); initial "
+                                           "inverse Jacobian fraction * I, fraction = 2 / (2 + lambda_max) from the "
+                                           "surrogate's Jacobian (at most 0.2); one secant update per tube"},
            "speedup": t_plain / t_sur, "speedup_vs_plain_continuation": t_cont / t_sur,
            "max_rel_dQ_vs_plain_fp64": dq}
     if ablation:
-        # the same solver (mixed, segments, the surrogate's fraction) from zero charge: the start's share
-        nos, _, _, _ = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, fraction=alpha, use_surrogate=False)
-        res["same_solver_zero_start"] = {"negf_iterations": [r["negf_iterations"] for r in nos],
-                                         "seconds": sum(r["seconds"] for r in nos)}
+        # the same solver with other starts: the operator's charge alone, the previous
+        # converged charge, zero
+        for mode in ("surrogate", "continuation", "zero"):
+            o, _, _, _ = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, fraction=alpha, start=mode)
+            res["same_solver_start_" + mode] = {"negf_iterations": [r["negf_iterations"] for r in o],
+                                                "seconds": sum(r["seconds"] for r in o),
+                                                "start_rel_err": [rel(r["start"], q) for r, q in zip(o, qref)]}
+    if keep_arrays:
+        res["_arrays"] = {"plain_Q": np.array(qref), "surrogate": np.array([r["surrogate"] for r in sur]),
+                          "start": np.array([r["start"] for r in sur]), "n_conv": np.array([r["n_in"] for r in sur])}
     if oracle_check:
         # the FP64 oracle's charge at the converged potential of the last gate point (fixed-point check)
         from oracle import oracle as O
@@ -518,7 +536,10 @@ def main():
     ap.add_argument("--no-config4", action="store_true")
     ap.add_argument("--no-config3", action="store_true")
     ap.add_argument("--no-long-tube", action="store_true")
-    ap.add_argument("--config5", action="store_true", help="surrogate-assisted sweep of the config-4 set")
+    ap.add_argument("--config5", action="store_true",
+                    help="surrogate-assisted sweep of the config-4 set at the stated size (20k pairs, 20 epochs); "
+                         "without it the default run measures the compact variant")
+    ap.add_argument("--no-config5", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "fused", "two_pass"],
                     help="RGF schedule of the timed passes (automatic by default)")
     ap.add_argument("--small", action="store_true",
@@ -775,7 +796,11 @@ def main():
         cfg4 = None if (args.no_config4 or world > 1) else config4_measure(torch)
         cfg3 = None if (args.no_config3 or world > 1) else config3_measure(torch, small=args.small)
         longt = None if (args.no_long_tube or world > 1) else long_tube_measure(torch)
-        cfg5 = config5_measure(torch) if (args.config5 and world == 1) else None
+        cfg5 = None
+        if world == 1 and not args.no_config5:
+            cfg5 = config5_measure(torch, **({} if args.config5 else CONFIG5_COMPACT))
+            cfg5["size"] = "stated (20k pairs, 20 epochs)" if args.config5 else "compact (%d pairs, %d epochs)" % (
+                CONFIG5_COMPACT["n_pairs"], CONFIG5_COMPACT["epochs"])
         clk.__exit__()
         roof = {"bound": "fp64", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                 "frac": achieved_tf / peak_tf if peak_tf else None,

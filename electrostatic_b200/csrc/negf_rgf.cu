@@ -1192,10 +1192,12 @@ __global__ void __launch_bounds__(32) rgf_piece_prefix_kernel(const TubeDev* __r
 
 // Fused schedule: one warp (32 whole chains) per block; records in the
 // warp's scratch, per-site sums into the warp's partial row.  One
-// instantiation per precision (FP32 chains need far fewer registers, so more
-// of their warps stay resident); block b takes warp order[b].
+// instantiation per precision; block b takes warp order[b].  The FP32
+// instantiation is held to 128 registers (16 resident warps per SM, no
+// spills) to hide the latency of its dependent recurrences; FP64 needs
+// about 240 and spills below that.
 template <typename R>
-__global__ void __launch_bounds__(32) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
+__global__ void __launch_bounds__(32, (sizeof(R) == 4 ? 16 : 1)) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
                                                        const ChainRec* __restrict__ chains,
                                                        const WarpRec* __restrict__ warps, const int* __restrict__ order,
                                                        int count, double* __restrict__ partial,

@@ -186,12 +186,15 @@ class BatchSCF:
 
     def set_external(self, Vg=None, U0=None):
         """The external potential of the next solve: the electrostatics' at
-        gate voltage Vg, or U0 (one host array per tube)."""
+        gate voltage Vg, or U0 (one array per tube: host arrays, or float64
+        device tensors copied on the solver's stream)."""
         import torch
         with torch.cuda.stream(self.stream):
             for t_, ((Kd, U0d), e) in enumerate(zip(self.ops, self.electros)):
                 if U0 is None:
                     U0d.copy_(e.device_operator(Vg)[1])
+                elif isinstance(U0[t_], torch.Tensor):
+                    U0d.copy_(U0[t_])
                 else:
                     U0d.copy_(torch.as_tensor(np.asarray(U0[t_], dtype=np.float64)), non_blocking=False)
 

@@ -82,6 +82,8 @@ class FourierOperator:
             G[:, 2 * k + 1] = np.sin(2 * np.pi * k * s / self.S)
         self.F = torch.tensor(F, dtype=torch.bfloat16, device=device)
         self.G = torch.tensor(G, dtype=torch.bfloat16, device=device)
+        # per-sample bases (Fb [B][2M][S], Gb [B][S][2M]) replace F and G when set
+        self._basis = None
         self.x_scale = torch.ones(self.feat, device=device)
         self.q_scale = 1.0
         self._bufs = {}
@@ -113,6 +115,13 @@ class FourierOperator:
     def _s(self):
         """The current torch stream (every kernel of the model runs on it)."""
         return C.c_void_p(self.torch.cuda.current_stream().cuda_stream)
+
+    def _bases(self):
+        """Analysis and synthesis bases with their batch strides (0: shared)."""
+        if self._basis is None:
+            return self.F, 0, self.G, 0
+        n = 2 * MODES * self.S
+        return self._basis[0], n, self._basis[1], n
 
     def _gemm(self, at, bt, M, N, K, batch, A, lda, sA, B, ldb, sB, Cf, ldc, sC, Cb=None, acc=0):
         check(_lib.load().negf_nn_gemm(at, bt, M, N, K, batch, _p(A), lda, sA, _p(B), ldb, sB, _p(Cf), ldc, sC, _p(Cb),
@@ -151,11 +160,12 @@ class FourierOperator:
             zb = self._buf(f"zb{l}", (B, 2 * M, W), t.bfloat16)
             s2 = self._buf(f"s2_{l}", (R, W))
             self._gemm(0, 0, R, W, W, 1, hb, W, 0, self.bf[f"W{l}"], W, 0, s1, W, 0)
-            self._gemm(0, 0, 2 * M, W, S, B, self.F, S, 0, hb, W, S * W, hat, W, 2 * M * W, hatb)
+            Fa, sF, Ga, sG = self._bases()
+            self._gemm(0, 0, 2 * M, W, S, B, Fa, S, sF, hb, W, S * W, hat, W, 2 * M * W, hatb)
             # per frequency k: rows b of hat[b][2k:2k+2][:] (256 values) times R[k]
             self._gemm(0, 0, B, 2 * W, 2 * W, M, hatb, 2 * M * W, 2 * W, self.bf[f"R{l}"], 2 * W, 4 * W * W,
                        z, 2 * M * W, 2 * W, zb)
-            self._gemm(0, 0, S, W, 2 * M, B, self.G, 2 * M, 0, zb, W, 2 * M * W, s2, W, S * W)
+            self._gemm(0, 0, S, W, 2 * M, B, Ga, 2 * M, sG, zb, W, 2 * M * W, s2, W, S * W)
             pre = self._buf(f"pre{l}", (R, W)) if keep else None
             hn = self._buf(f"h{l + 1}", (R, W))
             hnb = self._buf(f"h{l + 1}b", (R, W), t.bfloat16)
@@ -198,14 +208,15 @@ class FourierOperator:
             # spectral path: dz = G^T dpre ; dR_k = hat_k^T dz_k ; dhat_k = dz_k R_k^T ; dh += F^T dhat
             dz = self._buf("dz", (B, 2 * M, W))
             dzb = self._buf("dzb", (B, 2 * M, W), t.bfloat16)
-            self._gemm(1, 0, 2 * M, W, S, B, self.G, 2 * M, 0, dpreb, W, S * W, dz, W, 2 * M * W, dzb)
+            Fa, sF, Ga, sG = self._bases()
+            self._gemm(1, 0, 2 * M, W, S, B, Ga, 2 * M, sG, dpreb, W, S * W, dz, W, 2 * M * W, dzb)
             self._gemm(1, 0, 2 * W, 2 * W, B, M, hatb, 2 * M * W, 2 * W, dzb, 2 * M * W, 2 * W, gr[f"R{l}"], 2 * W,
                        4 * W * W)
             dhat = self._buf("dhat", (B, 2 * M, W))
             dhatb = self._buf("dhatb", (B, 2 * M, W), t.bfloat16)
             self._gemm(0, 1, B, 2 * W, 2 * W, M, dzb, 2 * M * W, 2 * W, self.bf[f"R{l}"], 2 * W, 4 * W * W, dhat,
                        2 * M * W, 2 * W, dhatb)
-            self._gemm(1, 0, S, W, 2 * M, B, self.F, S, 0, dhatb, W, 2 * M * W, dhn, W, S * W, None, 1)
+            self._gemm(1, 0, S, W, 2 * M, B, Fa, S, sF, dhatb, W, 2 * M * W, dhn, W, S * W, None, 1)
             dh, dhn = dhn, dh
             self._bufs[("dh", (R, W), t.float32)], self._bufs[("dhn", (R, W), t.float32)] = dh, dhn
         # lift

@@ -34,8 +34,15 @@ two-parameter family of a gate sweep.  The loss is the mean square error over
 the tubes' own sites (padding masked out), per tube relative to its largest
 charge.
 
+Spectral path: instead of the shared canvas-length Fourier basis of
+surrogate.py, every tube gets the first 64 cosine (DCT-II) modes of its own
+length (pairs of modes share one mixing matrix, as the (cos, sin) pairs do
+there), so short and long tubes are resolved alike.
+
 The sweep (fixed_point_sweep): per gate point, one inference gives the
-start, and a BatchSCF solve -- mixed-precision plan until the residual falls
+start -- by default the previous gate point's converged charge plus the
+operator's change between the two gate points, which cancels the part of
+the operator's error that varies slowly with the bias -- and a BatchSCF solve -- mixed-precision plan until the residual falls
 below switch_norm, the FP64 plan after, one secant update per tube
 (segments) -- converges it; only an FP64 NEGF charge ends a solve (the engine
 judges every converged charge).  The initial inverse Jacobian is
@@ -57,7 +64,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check
-from .surrogate import WIN, FourierOperator
+from .surrogate import MODES, WIN, FourierOperator
 
 FEAT_SET = 32
 
@@ -102,6 +109,20 @@ class TubeSetOperator(FourierOperator):
             fixed[t, :, 12] = N / S
             widx[t] = np.clip(n[:, None] + np.arange(-WIN, WIN + 1)[None, :], 0, N - 1)
             mask[t] = inside
+        # per-tube spectral bases: the first 2 * MODES cosine (DCT-II) modes of the
+        # tube's own length, so that every tube, short or long, gets the same
+        # resolution (a shared canvas-length basis would give an 800-site tube
+        # only a few modes); pairs of modes (2j, 2j + 1) share one mixing matrix
+        Fa = np.zeros((T, 2 * MODES, S), dtype=np.float32)
+        Ga = np.zeros((T, S, 2 * MODES), dtype=np.float32)
+        for t, d in enumerate(self.desc):
+            N = d["N"]
+            k = np.arange(2 * MODES)[:, None]
+            c = np.cos(np.pi * k * (np.arange(N)[None, :] + 0.5) / N)
+            Fa[t, :, :N] = c * np.where(k == 0, 1.0, 2.0) / N
+            Ga[t, :N, :] = c.T
+        self.F_all = torch.tensor(Fa, dtype=torch.bfloat16, device=device)
+        self.G_all = torch.tensor(Ga, dtype=torch.bfloat16, device=device)
         self._fixed_set = torch.tensor(fixed, device=device)
         self._widx_set = torch.tensor(widx.reshape(T, S * nw), device=device)
         self._mask_set = torch.tensor(mask, device=device)
@@ -151,6 +172,7 @@ class TubeSetOperator(FourierOperator):
                 idx = perm[i * batch:(i + 1) * batch].to(self.dev)
                 ti = tid[idx]
                 xb = self.features_set(U[idx], Vg[idx], Vds[idx], ti)
+                self._basis = (self.F_all[ti], self.G_all[ti])
                 q = self.forward(xb, batch, keep=True)
                 m = self._mask_set[ti].reshape(-1)
                 q.mul_(m)
@@ -166,6 +188,7 @@ class TubeSetOperator(FourierOperator):
             if log:
                 log(ep, hist[-1])
         t.cuda.synchronize()
+        self._basis = None
         return {"epochs": epochs, "seconds": time.perf_counter() - t0, "loss": hist}
 
     def predict_set(self, U, Vg, Vds, tid, batch=16):
@@ -176,7 +199,9 @@ class TubeSetOperator(FourierOperator):
         for i in range(0, n, batch):
             b = min(batch, n - i)
             xb = self.features_set(U[i:i + b], Vg[i:i + b], Vds[i:i + b], tid[i:i + b])
+            self._basis = (self.F_all[tid[i:i + b]], self.G_all[tid[i:i + b]])
             q = self.forward(xb, b)
+            self._basis = None
             out[i:i + b] = (q[: b * self.S].reshape(b, self.S) * self.qs_t[tid[i:i + b]][:, None]).double()
         return out * self._mask_set[tid].double()
 
@@ -215,7 +240,9 @@ class TubeSetOperator(FourierOperator):
         b["x"][:, :, :nw].copy_(b["win"].view(T, S, nw))
         b["x"][:, :, :nw].div_(self.x_scale[0])
         b["xb"].copy_(b["x"].view(T * S, FEAT_SET))
+        self._basis = (self.F_all, self.G_all)
         q = self.forward(b["xb"], T)
+        self._basis = None
         b["qd"].copy_(q)
         b["qd"].mul_(b["qscale"])
         t.index_select(b["qd"], 0, b["qidx"], out=b["Q"])
@@ -223,13 +250,14 @@ class TubeSetOperator(FourierOperator):
 
 # ---------------------------------------------------------------------- data
 def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bins=13, bump_fraction=0.5,
-                          bump_amp=0.2, tol=3e-6, fraction=0.3, S=None, log=None):
+                          bump_amp=0.2, tol=3e-6, fraction=0.15, max_step=300, S=None, log=None):
     """n_pairs (canvas U_ext, Vg, Vds, tube id, canvas n*) from batched
     self-consistent solves of the tube set (module docstring): per solve every
     tube gets its own gate voltage, the drain bias is one of vds_bins levels
-    in [0, 0.6] V; solves to a max-norm residual of tol.  make_tubes(vds)
-    returns the set's tubes at that drain bias.  Returns device tensors, the
-    seconds of the solves and their iteration counts."""
+    in [0, 0.6] V; solves to a max-norm residual of tol (a solve that passes
+    max_step is dropped and drawn again).  make_tubes(vds) returns the set's
+    tubes at that drain bias.  Returns device tensors, the seconds of the
+    solves and their iteration counts (dropped solves as -1)."""
     import torch
     from .scf import BatchSCF
     from .workloads import site_potential
@@ -255,8 +283,10 @@ def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_
         for e in electros:
             e.Vds = lv
         tubes = make_tubes(lv)
-        scf = BatchSCF(tubes, electros, fraction=fraction, max_norm=tol, iters_per_graph=4, segments=True)
-        for _ in range(count):
+        scf = BatchSCF(tubes, electros, fraction=fraction, max_norm=tol, max_step=max_step, iters_per_graph=4,
+                       segments=True)
+        done = 0
+        while done < count:
             U0 = []
             for t_, e in enumerate(electros):
                 vg = float(rng.uniform(0.0, 0.8))
@@ -271,10 +301,18 @@ def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_
             scf.reset(keep_charge=False)
             scf.stream.synchronize()
             t0 = time.perf_counter()
-            it, _ = scf.solve()
+            try:
+                it, _ = scf.solve()
+            except RuntimeError:
+                it = -1
             scf.stream.synchronize()
             seconds += time.perf_counter() - t0
             iters.append(it)
+            if it < 0:
+                if iters.count(-1) > max(4, n_solves // 10):
+                    raise RuntimeError("too many training solves failed to converge")
+                continue
+            done += 1
             for t_ in range(T):
                 Q_all[k + t_, :Ns[t_]] = scf.n_in[scf.offs[t_]:scf.offs[t_ + 1]].float()
             k += T
@@ -290,16 +328,25 @@ def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_
 
 
 # ---------------------------------------------------------------------- SCF
-def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1e-6, max_step=200,
-                      switch_norm=1e-5, segments=True, iters_per_graph=4, power_iters=6, autotune=True,
-                      use_surrogate=True):
+START_MODES = ("surrogate", "difference", "continuation", "zero")
+
+
+def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_fraction=0.2, max_norm=1e-6,
+                      max_step=200, switch_norm=1e-5, segments=True, iters_per_graph=4, power_iters=6,
+                      autotune=True, start="difference"):
     """Surrogate-started gate sweep of a tube set (module docstring).  Tubes
     in mixed precision run on their own plan until the residual falls below
     switch_norm, then on an FP64 plan.  fraction: the scalar initial inverse
-    Jacobian (None: from the surrogate's Jacobian).  use_surrogate=False
-    starts every point from zero charge (the same solver without the
-    surrogate).  Returns per-step records, the fraction, lambda_max and the
-    one-off set-up seconds (plans, graphs; outside the per-step times)."""
+    Jacobian (None: 2 / (2 + lambda_max) from the surrogate's Jacobian, at
+    most max_fraction).  start: "surrogate" (the operator's charge),
+    "difference" (the previous gate point's converged charge plus the
+    operator's change between the two gate points; the operator's charge at
+    the first point), "continuation" (the previous converged charge; zero at
+    the first point) or "zero".  Returns per-step records, the fraction,
+    lambda_max and the one-off set-up seconds (plans, graphs; outside the
+    per-step times)."""
+    if start not in START_MODES:
+        raise ValueError(f"start must be one of {START_MODES}")
     import torch
     from . import negf as ng
     from .scf import BatchSCF
@@ -316,10 +363,14 @@ def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1
         zero = torch.zeros(max(Ns), dtype=torch.float64, device=dev)
         Kds = [e.device_operator(Vg_list[0])[0] for e in electros]
         model.bind_set(Ucat, Qs, Vg_list[0], vds)
+        # the external potential is affine in Vg: U_ext(Vg) = A + Vg B, formed on the device
+        A = torch.tensor(np.concatenate([e.external(0.0) for e in electros]), dtype=torch.float64, device=dev)
+        B = torch.tensor(np.concatenate([e.external(1.0) - e.external(0.0) for e in electros]),
+                         dtype=torch.float64, device=dev)
+        views = [Ucat[int(o):int(o) + N] for o, N in zip(offs, Ns)]
 
         def external(Vg):
-            for e, o, N in zip(electros, offs, Ns):
-                Ucat[int(o):int(o) + N].copy_(e.device_operator(Vg)[1])
+            torch.add(A, B, alpha=float(Vg), out=Ucat)
 
         external(Vg_list[0])
         model.infer_set()  # allocates the model's inference buffers
@@ -352,7 +403,7 @@ def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1
             Ucat.copy_(U0)
             mu = min(mu, 0.95)
             lam = mu / (1.0 - mu)
-            alpha = float(min(0.5, max(0.1, 2.0 / (2.0 + lam))))
+            alpha = float(min(max_fraction, max(0.05, 2.0 / (2.0 + lam))))
         stream.synchronize()
     t_alpha = time.perf_counter() - t0
     t1 = time.perf_counter()
@@ -361,24 +412,40 @@ def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_norm=1
                    iters_per_graph=iters_per_graph, autotune=autotune, switch_norm=switch, segments=segments)
     t_setup += time.perf_counter() - t1
     out = []
+    with torch.cuda.stream(scf.stream):
+        q_prev = torch.zeros(S, dtype=torch.float64, device=dev)
+        n0 = torch.zeros(S, dtype=torch.float64, device=dev)
     for step, Vg in enumerate(Vg_list):
-        stream.synchronize()
+        # the bias point's external potential (the electrostatics' part, untimed as in run_scf_batch)
+        with torch.cuda.stream(scf.stream):
+            external(Vg)
+        scf.set_external(U0=views)
         scf.stream.synchronize()
         t0 = time.perf_counter()
-        scf.set_external(Vg=Vg)
-        scf.reset(keep_charge=use_surrogate, init_value=0.0)
-        if use_surrogate:
-            with torch.cuda.stream(scf.stream):
-                external(Vg)
+        with torch.cuda.stream(scf.stream):
+            first = step == 0
+            if start in ("surrogate", "difference"):
                 model.set_bias_set(Vg, vds)
                 model.infer_set()
-                scf.n_in.copy_(Qs)
+            if start == "surrogate" or (start == "difference" and first):
+                n0.copy_(Qs)
+            elif start == "difference":
+                n0.add_(Qs).sub_(q_prev)  # n0 holds the previous converged charge
+            elif start == "zero" or first:
+                n0.zero_()
+            if start == "difference":
+                q_prev.copy_(Qs)
+            scf.reset(keep_charge=True)
+            scf.n_in.copy_(n0)
         it, low = scf.solve()
         scf.stream.synchronize()
         dt = time.perf_counter() - t0 + (t_alpha if step == 0 else 0.0)
         with torch.cuda.stream(scf.stream):
-            start = Qs.cpu().numpy().copy() if use_surrogate else np.zeros(S)
-            out.append(dict(Vg=float(Vg), negf_iterations=it, lowprec_iterations=low, seconds=dt,
-                            Q=scf.Q.cpu().numpy().copy(), n_in=scf.n_in.cpu().numpy().copy(), start=start))
+            rec = dict(Vg=float(Vg), negf_iterations=it, lowprec_iterations=low, seconds=dt,
+                       Q=scf.Q.cpu().numpy().copy(), n_in=scf.n_in.cpu().numpy().copy(), start=n0.cpu().numpy().copy())
+            if start in ("surrogate", "difference"):
+                rec["surrogate"] = Qs.cpu().numpy().copy()
+            out.append(rec)
+            n0.copy_(scf.n_in)  # the converged charge: the next point's continuation
     scf.close()
     return out, alpha, lam, t_setup
