@@ -153,17 +153,19 @@ __device__ cd sigma_contact(cd E, double Uc, double beta, const TubeDev& T) {
 }
 
 // Butterfly reduce-scatter of K per-lane values over the 32 lanes: returns
-// the sum over lanes of element j = lane >> (5 - log2 K).  Fixed order.
-template <int K>
-__device__ __forceinline__ double warp_reduce_scatter(double (&a)[K], int lane) {
+// the sum over lanes of element j = lane >> (5 - log2 K).  Fixed order, in
+// the chains' precision (FP32 chains sum their 32 lanes in FP32; the rows
+// are added up in FP64 afterwards).
+template <int K, typename T>
+__device__ __forceinline__ T warp_reduce_scatter(T (&a)[K], int lane) {
     static_assert(K == 8 || K == 16, "K");
 #pragma unroll
     for (int half = K / 2, bit = 16; half >= 1; half >>= 1, bit >>= 1) {
         const bool up = (lane & bit) != 0;
 #pragma unroll
         for (int i = 0; i < half; ++i) {
-            const double send = up ? a[i] : a[i + half];
-            const double keep = up ? a[i + half] : a[i];
+            const T send = up ? a[i] : a[i + half];
+            const T keep = up ? a[i + half] : a[i];
             a[i] = keep + __shfl_xor_sync(kFull, send, bit);
         }
     }
@@ -606,25 +608,27 @@ __device__ __forceinline__ void seg_fwd(const Chain<R>& c, int n0, const CkVals<
 
 template <typename R, bool RA, bool EDGE>
 __device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[kSeg], SegWork<R>& w,
-                                        double (&acc)[kSeg]) {
+                                        R (&acc)[kSeg]) {
     constexpr int K = kSeg;
     const int N = c.N;
     R Rr = w.Rr, Ri = w.Ri, Sr = 1, Si = 0, rh = w.rh;
 #pragma unroll
     for (int j = K - 1; j >= 0; --j) {
         const int n = n0 + j;
-        acc[j] = 0.0;
+        acc[j] = 0;
         if (EDGE && n >= N) continue;
-        double v;
         if (!EDGE) {
+            R v;
             if (RA) {  // |G|^2 (lambda k0 + rho k1) = lm |S|^2 + rh |Q|^2, 1/|D|^2 folded in
                 const R s2 = fma(Sr, Sr, Si * Si), q2 = fma(w.qr[j], w.qr[j], w.qi[j] * w.qi[j]);
-                v = (double)fma(w.lm[j], s2, rh * q2);
+                v = fma(w.lm[j], s2, rh * q2);
             } else {  // Im(c Q S / D)
                 const R tr = fma(w.qr[j], Sr, -w.qi[j] * Si), ti = fma(w.qr[j], Si, w.qi[j] * Sr);
-                v = (double)fma(w.cgr, ti, w.cgi * tr);
+                v = fma(w.cgr, ti, w.cgi * tr);
             }
+            acc[j] = c.valid ? v : (R)0;
         } else {
+            double v;
             // D = S Q_{n+1} - R Q_n, per site (the segment may be partial), in FP64
             const double Sd = Sr, Sid = Si, Rd = Rr, Rid = Ri;
             const double q1r = w.qr[j + 1], q1i = w.qi[j + 1], q0r = w.qr[j], q0i = w.qi[j];
@@ -639,8 +643,8 @@ __device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[
                 const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
                 v = fma(c.cr, ui, c.ci * ur) * inv;
             }
+            acc[j] = c.valid ? (R)v : (R)0;
         }
-        acc[j] = c.valid ? v : 0.0;
         if (j > 0) {  // (R, S) at site n - 1
             R ar = c.Er - u[j], ai = c.Ei;
             if (EDGE) {
@@ -664,7 +668,7 @@ __device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[
 
 template <typename R, bool RA, bool EDGE, bool NEXT = false>
 __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const CkVals<R>& ckv, const R (&u)[kSeg],
-                                             double (&acc)[kSeg], Bnd<R>* next = nullptr) {
+                                             R (&acc)[kSeg], Bnd<R>* next = nullptr) {
     SegWork<R> w;
     seg_fwd<R, RA, EDGE, NEXT>(c, n0, ckv, u, w, next);
     seg_bwd<R, RA, EDGE>(c, n0, u, w, acc);
@@ -706,7 +710,7 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
         CkVals<R> nxt = cur;
         if (s + 1 < su.seg1) nxt = load_ck<R, RA>(ck + (size_t)(s + 1) * CL::NC * kWarp);
         R u[K];
-        double acc[K];
+        R acc[K];
         const bool interior = n0 > 0 && n0 + K < N;
         if (interior) {
             const double2* u2 = reinterpret_cast<const double2*>(U + n0);  // n0 even, U 16-byte aligned
@@ -723,7 +727,7 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
             segment_proj<R, RA, true>(c, n0, cur, u, acc);
         }
         cur = nxt;
-        const double tot = warp_reduce_scatter<K>(acc, lane);
+        const double tot = (double)warp_reduce_scatter<K>(acc, lane);
         constexpr int shift = (K == 16) ? 1 : 2;
         const int j = lane >> shift;
         if ((lane & ((1 << shift) - 1)) == 0 && n0 + j < N) prow[n0 + j] = tot;
@@ -762,9 +766,9 @@ __device__ __forceinline__ Bnd<R> sweep_segment(const Chain<R>& c, const Bnd<R>&
 
 // Sum of a segment's per-lane contributions over the warp, one coalesced
 // row-segment write (sites n0 .. n0 + K - 1 below N).
-__device__ __forceinline__ void write_segment(double (&acc)[kSeg], int n0, int N, double* __restrict__ prow,
-                                              int lane) {
-    const double tot = warp_reduce_scatter<kSeg>(acc, lane);
+template <typename T>
+__device__ __forceinline__ void write_segment(T (&acc)[kSeg], int n0, int N, double* __restrict__ prow, int lane) {
+    const double tot = (double)warp_reduce_scatter<kSeg>(acc, lane);
     const int j = lane >> 2;
     if ((lane & 3) == 0 && n0 + j < N) prow[n0 + j] = tot;
 }
@@ -863,7 +867,7 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
     if (nseg & 1) {
         const int n0 = A * K;
         const CkVals<R> v{fw.yr, fw.yi, fw.lam, bw.yr, bw.yi, bw.lam};
-        double acc[K];
+        R acc[K];
         R u[K];
         if (nseg == 1) {
             load_seg_edge(U, 0, N, u);
@@ -913,7 +917,7 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
             yn = rec(sb - 1);
         }
         prefetch_rec(k + 2);
-        double accf[K], accb[K];
+        R accf[K], accb[K];
         if (!last) {
             R uf[K], ub[K];
             load_seg(U, nf, uf);
@@ -923,7 +927,7 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
             SegWork<R> wf, wb;
             seg_fwd<R, RA, false, true>(c, nf, vf, uf, wf, &fw);
             seg_fwd<R, RA, false, true>(crev, nb, vb, ub, wb, &bw);
-            double accr[K];
+            R accr[K];
             seg_bwd<R, RA, false>(c, nf, uf, wf, accf);
             seg_bwd<R, RA, false>(crev, nb, ub, wb, accr);
 #pragma unroll
