@@ -445,7 +445,7 @@ def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True
     # surrogate-started, mixed precision (contour and real-axis chains in FP32 at 2 meV broadening)
     tubesmx = make(vds, precision="mixed", realaxis_fp32=True)
     fixed_point_sweep(tubesmx, electros, [0.0], model)  # warm-up
-    sur, alpha, lam, t_setup = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, start="difference")
+    sur, alpha, lam, t_setup = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model)
     t_plain = sum(s_.seconds for s_ in plain.steps)
     t_cont = sum(s_.seconds for s_ in cont.steps)
     t_sur = sum(r["seconds"] for r in sur)
@@ -475,20 +475,23 @@ def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True
                                  "surrogate_rel_err": [rel(r["surrogate"], q) for r, q in zip(sur, qref)],
                                  "fraction": alpha, "lambda_max": lam, "setup_seconds_excluded": t_setup,
                                  "method": "mixed-precision tubes (FP32 contour and real-axis chains, FP64 finish "
-                                           "below 1e-5); start = previous converged charge + the operator's change "
-                                           "between the gate points (the operator's charge at the first); initial "
-                                           "inverse Jacobian fraction * I, fraction = 2 / (2 + lambda_max) from the "
-                                           "surrogate's Jacobian (at most 0.2); one secant update per tube"},
+                                           "below 3e-6); start = linear extrapolation of the previous two converged "
+                                           "charges plus the operator's second difference (the operator's change at "
+                                           "the second gate point, its charge at the first); initial inverse "
+                                           "Jacobian 0.2 * I; one secant update per tube"},
            "speedup": t_plain / t_sur, "speedup_vs_plain_continuation": t_cont / t_sur,
            "max_rel_dQ_vs_plain_fp64": dq}
     if ablation:
-        # the same solver with other starts: the operator's charge alone, the previous
-        # converged charge, zero
-        for mode in ("surrogate", "continuation", "zero"):
-            o, _, _, _ = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, fraction=alpha, start=mode)
-            res["same_solver_start_" + mode] = {"negf_iterations": [r["negf_iterations"] for r in o],
-                                                "seconds": sum(r["seconds"] for r in o),
-                                                "start_rel_err": [rel(r["start"], q) for r, q in zip(o, qref)]}
+        # the same solver with other starts (with and without the operator), with the secant
+        # rows carried between gate points, and with the fraction from the operator's Jacobian
+        variants = [(m, dict(start=m)) for m in ("difference", "surrogate", "extrapolation", "continuation", "zero")]
+        variants += [("extrapolated_carry_rows", dict(carry_rows=True)),
+                     ("extrapolated_fraction_from_operator", dict(fraction=None))]
+        for name, kw in variants:
+            o, a_, l_, _ = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, **kw)
+            res["same_solver_" + name] = {"negf_iterations": [r["negf_iterations"] for r in o],
+                                          "seconds": sum(r["seconds"] for r in o), "fraction": a_, "lambda_max": l_,
+                                          "start_rel_err": [rel(r["start"], q) for r, q in zip(o, qref)]}
     if keep_arrays:
         res["_arrays"] = {"plain_Q": np.array(qref), "surrogate": np.array([r["surrogate"] for r in sur]),
                           "start": np.array([r["start"] for r in sur]), "n_conv": np.array([r["n_in"] for r in sur])}

@@ -15,14 +15,17 @@ the tube's self-consistent charge n* (the fixed point n* = Q(U_ext + K n*) of
 the NEGF-Poisson loop).  One inference is then the Broyden start of a bias
 point; no surrogate loop runs.
 
-Features per site (FEAT_SET = 32):
+Features per site (FEAT_SET = 40):
   0..16  U_ext at sites n-8 .. n+8 of the tube (indices clamped to the tube:
          the leads continue at the end-site potential), divided by the
          potential scale
   17, 18 Vg, Vds
-  19..31 n / N, ring parity +-1, exp(-n / 40), exp(-(N-1-n) / 40), inside
+  19..39 n / N, ring parity +-1, exp(-n / 40), exp(-(N-1-n) / 40), inside
          mask, chirality one-hot (13, 17, 19), modes / 10, inner band edge of
-         the lowest and of the highest kept mode / gamma, channels / 20, N / S
+         the lowest and of the highest kept mode / gamma, channels / 20, N / S,
+         exp(-n / 3), exp(-(N-1-n) / 3), exp(-n / 12), exp(-(N-1-n) / 12),
+         end-site indicators (n = 0, n = N-1), two zeros (the end sites carry
+         the largest charges: the leads attach there)
 
 Training pairs come from the engine itself (generate_fixed_points): batched
 self-consistent solves of the whole set at random drain biases Vds ~ U(0,
@@ -66,7 +69,7 @@ from . import _lib
 from ._lib import check
 from .surrogate import MODES, WIN, FourierOperator
 
-FEAT_SET = 32
+FEAT_SET = 40
 
 
 def tube_descriptor(tube):
@@ -107,6 +110,13 @@ class TubeSetOperator(FourierOperator):
             fixed[t, :, 10] = d["edge_hi"]
             fixed[t, :, 11] = d["channels"] / 20.0
             fixed[t, :, 12] = N / S
+            tail = np.clip(N - 1 - n, 0, None)
+            fixed[t, :, 13] = np.exp(-n / 3.0)
+            fixed[t, :, 14] = np.where(inside, np.exp(-tail / 3.0), 0.0)
+            fixed[t, :, 15] = np.exp(-n / 12.0)
+            fixed[t, :, 16] = np.where(inside, np.exp(-tail / 12.0), 0.0)
+            fixed[t, 0, 17] = 1.0
+            fixed[t, N - 1, 18] = 1.0
             widx[t] = np.clip(n[:, None] + np.arange(-WIN, WIN + 1)[None, :], 0, N - 1)
             mask[t] = inside
         # per-tube spectral bases: the first 2 * MODES cosine (DCT-II) modes of the
@@ -249,12 +259,14 @@ class TubeSetOperator(FourierOperator):
 
 
 # ---------------------------------------------------------------------- data
-def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bins=13, bump_fraction=0.5,
-                          bump_amp=0.2, tol=3e-6, fraction=0.15, max_step=300, S=None, log=None):
+def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_bins=13, vds_max=0.6,
+                          vg_max=0.8, bump_fraction=0.5, bump_amp=0.2, tol=3e-6, fraction=0.15, max_step=300, S=None,
+                          log=None):
     """n_pairs (canvas U_ext, Vg, Vds, tube id, canvas n*) from batched
     self-consistent solves of the tube set (module docstring): per solve every
-    tube gets its own gate voltage, the drain bias is one of vds_bins levels
-    in [0, 0.6] V; solves to a max-norm residual of tol (a solve that passes
+    tube gets its own gate voltage in [0, vg_max] V, the drain bias is one of
+    vds_bins levels in [0, vds_max] V; solves to a max-norm residual of tol
+    with per-tube secant updates at the given fraction (a solve that passes
     max_step is dropped and drawn again).  make_tubes(vds) returns the set's
     tubes at that drain bias.  Returns device tensors, the seconds of the
     solves and their iteration counts (dropped solves as -1)."""
@@ -262,7 +274,7 @@ def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_
     from .scf import BatchSCF
     from .workloads import site_potential
     rng = np.random.default_rng(seed)
-    levels = np.linspace(0.0, 0.6, vds_bins)
+    levels = np.linspace(0.0, vds_max, vds_bins)
     T = len(electros)
     dev = "cuda"
     Ns = [e.N for e in electros]
@@ -289,7 +301,7 @@ def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_
         while done < count:
             U0 = []
             for t_, e in enumerate(electros):
-                vg = float(rng.uniform(0.0, 0.8))
+                vg = float(rng.uniform(0.0, vg_max))
                 u = e.external(vg)
                 if rng.uniform() < bump_fraction:
                     u = u + site_potential(e.y_nm, int(rng.integers(1 << 30)), amp=float(rng.uniform(0.0, bump_amp)),
@@ -328,23 +340,32 @@ def generate_fixed_points(make_tubes, electros, n_pairs, seed=20261203 + 5, vds_
 
 
 # ---------------------------------------------------------------------- SCF
-START_MODES = ("surrogate", "difference", "continuation", "zero")
+START_MODES = ("extrapolated", "difference", "surrogate", "extrapolation", "continuation", "zero")
 
 
-def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_fraction=0.2, max_norm=1e-6,
-                      max_step=200, switch_norm=1e-5, segments=True, iters_per_graph=4, power_iters=6,
-                      autotune=True, start="difference"):
+def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=0.2, max_fraction=0.2, max_norm=1e-6,
+                      max_step=200, switch_norm=3e-6, segments=True, carry_rows=False, iters_per_graph=4,
+                      power_iters=6, autotune=True, start="extrapolated"):
     """Surrogate-started gate sweep of a tube set (module docstring).  Tubes
     in mixed precision run on their own plan until the residual falls below
     switch_norm, then on an FP64 plan.  fraction: the scalar initial inverse
     Jacobian (None: 2 / (2 + lambda_max) from the surrogate's Jacobian, at
-    most max_fraction).  start: "surrogate" (the operator's charge),
-    "difference" (the previous gate point's converged charge plus the
-    operator's change between the two gate points; the operator's charge at
-    the first point), "continuation" (the previous converged charge; zero at
-    the first point) or "zero".  Returns per-step records, the fraction,
-    lambda_max and the one-off set-up seconds (plans, graphs; outside the
-    per-step times)."""
+    most max_fraction).  start, with n_k the converged charge and S_k the
+    operator's charge at gate point k:
+      "extrapolated"  2 n_{k-1} - n_{k-2} + (S_k - 2 S_{k-1} + S_{k-2}): the
+                      linear extrapolation of the converged charges plus the
+                      operator's curvature ("difference" at k = 1, S_0 at 0);
+      "difference"    n_{k-1} + S_k - S_{k-1} (S_0 at k = 0);
+      "surrogate"     S_k;
+      "extrapolation" 2 n_{k-1} - n_{k-2} without the operator (n_0 at k = 1,
+                      zero at k = 0);
+      "continuation"  n_{k-1} (zero at k = 0);
+      "zero".
+    carry_rows: start each gate point from the previous points' secant rows
+    (negf_broyden_restart; all of them while they fit in max_step / 2, else
+    none).  Returns per-step records, the fraction, lambda_max (None unless
+    fraction is None) and the one-off set-up seconds (plans, graphs; outside
+    the per-step times)."""
     if start not in START_MODES:
         raise ValueError(f"start must be one of {START_MODES}")
     import torch
@@ -412,8 +433,12 @@ def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_fracti
                    iters_per_graph=iters_per_graph, autotune=autotune, switch_norm=switch, segments=segments)
     t_setup += time.perf_counter() - t1
     out = []
+    uses_model = start in ("extrapolated", "difference", "surrogate")
     with torch.cuda.stream(scf.stream):
-        q_prev = torch.zeros(S, dtype=torch.float64, device=dev)
+        s1 = torch.zeros(S, dtype=torch.float64, device=dev)  # S_{k-1}
+        s2 = torch.zeros(S, dtype=torch.float64, device=dev)  # S_{k-2}
+        m1 = torch.zeros(S, dtype=torch.float64, device=dev)  # n_{k-1}
+        m2 = torch.zeros(S, dtype=torch.float64, device=dev)  # n_{k-2}
         n0 = torch.zeros(S, dtype=torch.float64, device=dev)
     for step, Vg in enumerate(Vg_list):
         # the bias point's external potential (the electrostatics' part, untimed as in run_scf_batch)
@@ -423,19 +448,32 @@ def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_fracti
         scf.stream.synchronize()
         t0 = time.perf_counter()
         with torch.cuda.stream(scf.stream):
-            first = step == 0
-            if start in ("surrogate", "difference"):
+            if uses_model:
                 model.set_bias_set(Vg, vds)
                 model.infer_set()
-            if start == "surrogate" or (start == "difference" and first):
-                n0.copy_(Qs)
-            elif start == "difference":
-                n0.add_(Qs).sub_(q_prev)  # n0 holds the previous converged charge
-            elif start == "zero" or first:
+            k = step
+            if start == "zero" or (k == 0 and not uses_model):
                 n0.zero_()
-            if start == "difference":
-                q_prev.copy_(Qs)
-            scf.reset(keep_charge=True)
+            elif start == "surrogate" or k == 0:
+                n0.copy_(Qs)
+            elif start == "continuation" or (start == "extrapolation" and k == 1):
+                n0.copy_(m1)
+            elif start == "difference" or (start == "extrapolated" and k == 1):
+                torch.add(m1, Qs, out=n0)
+                n0.sub_(s1)
+            elif start == "extrapolation":
+                torch.mul(m1, 2.0, out=n0)
+                n0.sub_(m2)
+            else:  # extrapolated, k >= 2
+                torch.mul(m1, 2.0, out=n0)
+                n0.sub_(m2).add_(Qs).sub_(s1, alpha=2.0).add_(s2)
+            if uses_model:
+                s2.copy_(s1)
+                s1.copy_(Qs)
+            if carry_rows and k > 0:
+                scf.br.restart(keep_rows=max_step // 2, stream=scf.stream)
+            else:
+                scf.reset(keep_charge=True)
             scf.n_in.copy_(n0)
         it, low = scf.solve()
         scf.stream.synchronize()
@@ -443,9 +481,10 @@ def fixed_point_sweep(tubes, electros, Vg_list, model, fraction=None, max_fracti
         with torch.cuda.stream(scf.stream):
             rec = dict(Vg=float(Vg), negf_iterations=it, lowprec_iterations=low, seconds=dt,
                        Q=scf.Q.cpu().numpy().copy(), n_in=scf.n_in.cpu().numpy().copy(), start=n0.cpu().numpy().copy())
-            if start in ("surrogate", "difference"):
+            if uses_model:
                 rec["surrogate"] = Qs.cpu().numpy().copy()
             out.append(rec)
-            n0.copy_(scf.n_in)  # the converged charge: the next point's continuation
+            m2.copy_(m1)
+            m1.copy_(scf.n_in)  # the converged charge
     scf.close()
     return out, alpha, lam, t_setup

@@ -136,23 +136,26 @@ def test_fixed_point_surrogate_set_sweep():
     electros = [GateAllAround(t.site_positions(), 0.0665e-9 * ch[0] / 17 * 10,
                               1.5e-9 + 0.0665e-9 * ch[0] / 17 * 10, contact_length=1e-9, Vds=0.2)
                 for t, (ch, _, _) in zip(tubes, specs)]
-    U, Vg, Vds, tid, Q, secs, its = generate_fixed_points(make, electros, 96, vds_bins=2)
+    U, Vg, Vds, tid, Q, secs, its = generate_fixed_points(make, electros, 96, vds_bins=2, vds_max=0.3, vg_max=0.4,
+                                                          fraction=0.1, bump_amp=0.1)
     assert U.shape[0] == 96 and np.isfinite(Q.cpu().numpy()).all() and secs > 0
     assert len([i for i in its if i > 0]) == 32
     for e in electros:
         e.Vds = 0.2
     model = TubeSetOperator([tube_descriptor(t) for t in tubes], seed=0)
     model.fit_set(U, Vg, Vds, tid, Q, epochs=3, batch=16)
-    plain = run_scf_batch(tubes, electros, [0.1, 0.3], use_graph=True, iters_per_graph=4)
     mixed = make(0.2, "mixed")
-    for start in ("difference", "surrogate", "continuation", "zero"):
-        out, alpha, lam, _ = fixed_point_sweep(mixed, electros, [0.1, 0.3], model, start=start)
-        assert 0.05 <= alpha <= 0.2 and lam is not None
+    vg = [0.1, 0.2, 0.3]
+    plain = run_scf_batch(tubes, electros, vg, use_graph=True, iters_per_graph=4)
+    for start in ("extrapolated", "difference", "surrogate", "extrapolation", "continuation", "zero"):
+        out, alpha, lam, _ = fixed_point_sweep(mixed, electros, vg, model, start=start,
+                                               fraction=None if start == "surrogate" else 0.2)
+        assert 0.05 <= alpha <= 0.2 and (lam is not None) == (start == "surrogate")
         for r, p in zip(out, plain.steps):
             assert r["negf_iterations"] > 0
             assert np.max(np.abs(r["Q"] - p.Q)) <= 1e-5 * np.max(np.abs(p.Q)) + 2e-6
     # segments with the plain solver's settings: the same fixed points
-    seg = run_scf_batch(make(0.2), electros, [0.1, 0.3], use_graph=True, iters_per_graph=4, segments=True)
+    seg = run_scf_batch(make(0.2), electros, vg, use_graph=True, iters_per_graph=4, segments=True)
     for a, b in zip(seg.steps, plain.steps):
         assert np.max(np.abs(a.Q - b.Q)) <= 2e-6
     for t in tubes + mixed:
