@@ -129,15 +129,15 @@ def test_fixed_point_surrogate_set_sweep():
 
     def make(lv, precision="fp64"):
         return [CNT(type_id=ch, num_unitcells=uc, num_modes=m, contact_mu=(0.0, -float(lv)), contact_T=(300.0, 300.0),
-                    eq_integration_pts=(16, 16, 24), noneq_integration_pts=(32,), E_zPlus_imag=2e-3, E_pole_max=3.0,
+                    eq_integration_pts=(24, 24, 32), noneq_integration_pts=(64,), E_zPlus_imag=2e-3, E_pole_max=3.0,
                     precision=precision, mixed_realaxis_fp32=precision == "mixed") for ch, uc, m in specs]
 
     tubes = make(0.2)
     electros = [GateAllAround(t.site_positions(), 0.0665e-9 * ch[0] / 17 * 10,
                               1.5e-9 + 0.0665e-9 * ch[0] / 17 * 10, contact_length=1e-9, Vds=0.2)
                 for t, (ch, _, _) in zip(tubes, specs)]
-    U, Vg, Vds, tid, Q, secs, its = generate_fixed_points(make, electros, 96, vds_bins=2, vds_max=0.3, vg_max=0.4,
-                                                          fraction=0.1, bump_amp=0.1)
+    U, Vg, Vds, tid, Q, secs, its = generate_fixed_points(make, electros, 96, vds_bins=2, vds_max=0.2, vg_max=0.3,
+                                                          fraction=0.1, bump_amp=0.05, tol=1e-5)
     assert U.shape[0] == 96 and np.isfinite(Q.cpu().numpy()).all() and secs > 0
     assert len([i for i in its if i > 0]) == 32
     for e in electros:
