@@ -36,6 +36,8 @@
 // butterfly reduce-scatter and written as one coalesced row segment; a third
 // kernel sums the rows per site in a fixed order (deterministic).
 
+#include <type_traits>
+
 #include "negf_internal.h"
 
 namespace negf {
@@ -799,6 +801,211 @@ __device__ __forceinline__ void load_seg_edge(const double* __restrict__ U, int 
     for (int k = 0; k < kSeg; ++k) u[k] = (n0 + k < N) ? (R)__ldg(U + n0 + k) : (R)0;
 }
 
+// ---- Packed FP32 pairs (sm_100 FFMA2 / FMUL2 / FADD2).  The fused schedule
+// runs two independent recurrences per chain side by side -- the forward
+// sweep and the backward sweep (the chain read from the drain end) -- with
+// the same operations on different data, so an FP32 chain carries both in
+// one float2: .x forward, .y backward, and every step of the interior loops
+// issues one packed instruction for the two.  The states keep -P (and -R)
+// so that no step needs a negation: with a = E - U and the hopping square h2,
+//   Q' = a Q - i Ei Q ... written out: qr' = a qr - Ei qi - pr,
+//   qi' = a qi + Ei qr - pi, and -P' = -h2 Q.
+struct F2 {
+    float2 v;
+};
+__device__ __forceinline__ F2 f2(float x, float y) { return {make_float2(x, y)}; }
+__device__ __forceinline__ F2 f2b(float x) { return {make_float2(x, x)}; }
+__device__ __forceinline__ F2 add2(F2 a, F2 b) { return {__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) { return {__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+
+// -U of an aligned interior segment (forward order) and of another read in
+// reverse, as pairs: mu[j] = (-U[nf + j], -U[nb + K - 1 - j]).
+__device__ __forceinline__ void load_seg_pair(const double* __restrict__ U, int nf, int nb, F2 (&mu)[kSeg]) {
+#pragma unroll
+    for (int k = 0; k < kSeg / 2; ++k) {
+        // nf, nb and K even, U 16-byte aligned
+        const double2 va = __ldg(reinterpret_cast<const double2*>(U + nf + 2 * k));
+        const double2 vb = __ldg(reinterpret_cast<const double2*>(U + nb + kSeg - 2 - 2 * k));
+        mu[2 * k] = f2(-(float)va.x, -(float)vb.y);
+        mu[2 * k + 1] = f2(-(float)va.y, -(float)vb.x);
+    }
+}
+
+// Pass-1 state of both sweeps of a chain: -P, Q, lambda and the product of
+// h^2 since the last boundary, per direction.
+struct Proj2 {
+    F2 mpr, mpi, qr, qi, lam, H;
+};
+
+// One interior block of phase A for an FP32 chain (pass1_block with
+// INTERIOR and COMPACT, both sweeps packed): boundary records of the forward
+// sweep at segment fs and of the backward sweep at segment bs, the next
+// block's potentials into mun, then K packed steps over whole segments
+// (the product of h^2 at the next boundary is hfull for each direction).
+template <bool RA>
+__device__ __forceinline__ void pass1_interior2(const Chain<float>& c, Proj2& p, int fs, int bs,
+                                                const double* __restrict__ U, float* __restrict__ ck,
+                                                const F2 (&mu)[kSeg], F2 (&mun)[kSeg], float hfull) {
+    constexpr int K = kSeg;
+    constexpr int NC = CkCompact<RA>::NC;
+    {
+        // boundary (per direction, as proj_boundary's FP32 form): Y = P / Q, state := (Y, 1)
+        const float q2x = fmaf(p.qr.v.x, p.qr.v.x, p.qi.v.x * p.qi.v.x);
+        const float q2y = fmaf(p.qr.v.y, p.qr.v.y, p.qi.v.y * p.qi.v.y);
+        const F2 rq = f2(rcp(q2x), rcp(q2y));
+        // P = -mP: Y = P conj(Q) / |Q|^2
+        const F2 tr = fma2(p.mpr, p.qr, mul2(p.mpi, p.qi));  // -(pr qr + pi qi)
+        const F2 ti = fma2(p.mpi, p.qr, mul2(f2(-p.mpr.v.x, -p.mpr.v.y), p.qi));  // -(pi qr - pr qi)
+        const F2 myr = mul2(tr, rq), myi = mul2(ti, rq);  // -Y
+        if (RA) p.lam = mul2(p.lam, mul2(p.H, rq));
+        p.H = f2b(hfull);
+        float* pf = ck + (size_t)fs * NC * kWarp;
+        pf[0] = -myr.v.x;
+        pf[kWarp] = -myi.v.x;
+        if (RA) pf[2 * kWarp] = p.lam.v.x;
+        float* pb = ck + (size_t)bs * NC * kWarp;
+        pb[0] = -myr.v.y;
+        pb[kWarp] = -myi.v.y;
+        if (RA) pb[2 * kWarp] = p.lam.v.y;
+        p.mpr = myr;
+        p.mpi = myi;
+        p.qr = f2b(1.0f);
+        p.qi = f2b(0.0f);
+    }
+    load_seg_pair(U, fs * K + K, (bs - 1) * K, mun);
+    const F2 Er = f2b(c.Er), Ei = f2b(c.Ei), mEi = f2b(-c.Ei);
+    const F2 mhb = f2b(-c.hb2), mhg = f2b(-c.hg2);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const F2 mh2 = (j & 1) ? mhg : mhb;
+        const F2 ar = add2(Er, mu[j]);
+        const F2 nqr = fma2(ar, p.qr, fma2(mEi, p.qi, p.mpr));
+        const F2 nqi = fma2(ar, p.qi, fma2(Ei, p.qr, p.mpi));
+        p.mpr = mul2(mh2, p.qr);
+        p.mpi = mul2(mh2, p.qi);
+        p.qr = nqr;
+        p.qi = nqi;
+    }
+}
+
+// Phase-B segment pair of an FP32 chain: the forward sweep's interior segment
+// at nf (chain c, live state vf, backward record at its end) and the
+// backward sweep's at nb read in reverse (chain cr with the contacts'
+// roles swapped, live state vb, forward record at its start), as seg_fwd
+// (with the next boundary) followed by seg_bwd for each, packed.  Returns
+// the contributions of both (accb in reversed site order) and the live
+// states at the next segments.
+template <bool RA>
+__device__ __forceinline__ void segment_pair2(const Chain<float>& c, const Chain<float>& cr,
+                                              const CkVals<float>& vf, const CkVals<float>& vb,
+                                              const F2 (&mu)[kSeg], float (&accf)[kSeg], float (&accr)[kSeg],
+                                              Bnd<float>& nf, Bnd<float>& nb) {
+    constexpr int K = kSeg;
+    const F2 Er = f2b(c.Er), Ei = f2b(c.Ei), mEi = f2b(-c.Ei);
+    const F2 hb = f2b(c.hb2), hg = f2b(c.hg2), mhb = f2b(-c.hb2), mhg = f2b(-c.hg2);
+    F2 qr[K + 1], qi[K + 1], lm[K];
+    // forward recompute of Q from (Y, 1) at the segment start
+    F2 mpr = f2(-vf.yr, -vb.yr), mpi = f2(-vf.yi, -vb.yi);
+    qr[0] = f2b(1.0f);
+    qi[0] = f2b(0.0f);
+    lm[0] = f2(vf.lam, vb.lam);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        const F2 ar = add2(Er, mu[j]);
+        qr[j + 1] = fma2(ar, qr[j], fma2(mEi, qi[j], mpr));
+        qi[j + 1] = fma2(ar, qi[j], fma2(Ei, qr[j], mpi));
+        if (j + 1 < K) {
+            const F2 mh2 = (j & 1) ? mhg : mhb;
+            mpr = mul2(mh2, qr[j]);
+            mpi = mul2(mh2, qi[j]);
+            if (RA) lm[j + 1] = mul2(lm[j], (j & 1) ? hg : hb);
+        }
+    }
+    // next boundary per direction: Y = h^2 Q_{K-1} conj(Q_K) / |Q_K|^2 (the last hopping is gamma)
+    {
+        const float ax = fmaf(qr[K].v.x, qr[K].v.x, qi[K].v.x * qi[K].v.x);
+        const float ay = fmaf(qr[K].v.y, qr[K].v.y, qi[K].v.y * qi[K].v.y);
+        const F2 rq = f2(rcp(ax), rcp(ay));
+        const F2 tr = fma2(qr[K - 1], qr[K], mul2(qi[K - 1], qi[K]));
+        const F2 ti = fma2(qi[K - 1], qr[K], mul2(f2(-qr[K - 1].v.x, -qr[K - 1].v.y), qi[K]));
+        const F2 g = mul2(hg, rq);
+        const F2 yr = mul2(tr, g), yi = mul2(ti, g);
+        nf.yr = yr.v.x;
+        nf.yi = yi.v.x;
+        nb.yr = yr.v.y;
+        nb.yi = yi.v.y;
+        if (RA) {
+            const F2 l = mul2(lm[K - 1], g);
+            nf.lam = l.v.x;
+            nb.lam = l.v.y;
+        } else {
+            nf.lam = 1.0f;
+            nb.lam = 1.0f;
+        }
+    }
+    // D = S_e Q_{K} - R_e Q_{K-1} with S_e = 1, R_e = X_e, in FP64 once per segment and direction,
+    // folded into the per-site coefficients
+    F2 rh = f2(vf.rho, vb.rho), cg_r = f2b(0.0f), cg_i = f2b(0.0f), mcg_i = f2b(0.0f);
+    {
+        double dr[2], di[2];
+        const float Rr[2] = {vf.xr, vb.xr}, Ri[2] = {vf.xi, vb.xi};
+        const float q1r[2] = {qr[K].v.x, qr[K].v.y}, q1i[2] = {qi[K].v.x, qi[K].v.y};
+        const float q0r[2] = {qr[K - 1].v.x, qr[K - 1].v.y}, q0i[2] = {qi[K - 1].v.x, qi[K - 1].v.y};
+        float fa[2], fb[2], gr[2], gi[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const Chain<float>& ch = h ? cr : c;
+            dr[h] = fma(-(double)Rr[h], (double)q0r[h], fma((double)Ri[h], (double)q0i[h], (double)q1r[h]));
+            di[h] = fma(-(double)Rr[h], (double)q0i[h], fma(-(double)Ri[h], (double)q0r[h], (double)q1i[h]));
+            const double inv = rcp(fma(dr[h], dr[h], di[h] * di[h]));
+            if (RA) {
+                fa[h] = (float)(ch.k0 * inv);
+                fb[h] = (float)(ch.k1 * inv);
+            } else {
+                gr[h] = (float)(fma(ch.cr, dr[h], ch.ci * di[h]) * inv);
+                gi[h] = (float)(fma(ch.ci, dr[h], -ch.cr * di[h]) * inv);
+            }
+        }
+        if (RA) {
+            const F2 f = f2(fa[0], fa[1]);
+#pragma unroll
+            for (int j = 0; j < K; ++j) lm[j] = mul2(lm[j], f);
+            rh = mul2(rh, f2(fb[0], fb[1]));
+        } else {
+            cg_r = f2(gr[0], gr[1]);
+            cg_i = f2(gi[0], gi[1]);
+            mcg_i = f2(-gi[0], -gi[1]);
+        }
+    }
+    // backward walk of (R, S) from (X_e, 1) with the site contributions
+    F2 mRr = f2(-vf.xr, -vb.xr), mRi = f2(-vf.xi, -vb.xi), Sr = f2b(1.0f), Si = f2b(0.0f);
+#pragma unroll
+    for (int j = K - 1; j >= 0; --j) {
+        F2 v;
+        if (RA) {  // lm |S|^2 + rh |Q|^2 (1/|D|^2 folded in)
+            const F2 s2 = fma2(Sr, Sr, mul2(Si, Si)), q2 = fma2(qr[j], qr[j], mul2(qi[j], qi[j]));
+            v = fma2(lm[j], s2, mul2(rh, q2));
+        } else {  // Im(c Q S / D) = qr (cg_r Si + cg_i Sr) + qi (cg_r Sr - cg_i Si)
+            const F2 a = fma2(cg_r, Si, mul2(cg_i, Sr)), b = fma2(cg_r, Sr, mul2(mcg_i, Si));
+            v = fma2(qr[j], a, mul2(qi[j], b));
+        }
+        accf[j] = c.valid ? v.v.x : 0.0f;
+        accr[j] = c.valid ? v.v.y : 0.0f;
+        if (j > 0) {
+            const F2 ar = add2(Er, mu[j]);
+            const F2 mh2 = ((j - 1) & 1) ? mhg : mhb;
+            const F2 nsr = fma2(ar, Sr, fma2(mEi, Si, mRr));
+            const F2 nsi = fma2(ar, Si, fma2(Ei, Sr, mRi));
+            mRr = mul2(mh2, Sr);
+            mRi = mul2(mh2, Si);
+            Sr = nsr;
+            Si = nsi;
+            if (RA) rh = mul2(rh, ((j - 1) & 1) ? hg : hb);
+        }
+    }
+}
+
 // Fused schedule: one warp carries 32 whole chains.  With A = nseg / 2,
 // phase A runs the forward sweep through segments [0, A) and the backward
 // sweep through [nseg - A, nseg) together (as pass 1), each storing its own
@@ -851,12 +1058,48 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
             ua_b[j] = (R)__ldg(U + N - 1 - j);  // kPadLo zeros before site 0 cover N < K
         }
         pass1_block<R, RA, false, true>(c, f, b, 0, nseg - 1, A > 1, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
-        int k = 1;
-        for (; k + 2 <= A; k += 2) {
-            pass1_block<R, RA, true, true>(c, f, b, k, nseg - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
-            pass1_block<R, RA, true, true>(c, f, b, k + 1, nseg - 2 - k, true, U, ck, ua_f, ua_b, ub_f, ub_b, hfull);
+        if constexpr (std::is_same<R, float>::value) {
+            // interior blocks with both sweeps packed (FFMA2)
+            if (A > 1) {
+                Proj2 p2;
+                p2.mpr = f2(-f.pr, -b.pr);
+                p2.mpi = f2(-f.pi, -b.pi);
+                p2.qr = f2(f.qr, b.qr);
+                p2.qi = f2(f.qi, b.qi);
+                p2.lam = f2(f.lam, b.lam);
+                p2.H = f2(f.H, b.H);
+                F2 m0[K], m1[K];
+#pragma unroll
+                for (int j = 0; j < K; ++j) m0[j] = f2(-ub_f[j], -ub_b[j]);
+                int k = 1;
+                for (; k + 2 <= A; k += 2) {
+                    pass1_interior2<RA>(c, p2, k, nseg - 1 - k, U, ck, m0, m1, hfull);
+                    pass1_interior2<RA>(c, p2, k + 1, nseg - 2 - k, U, ck, m1, m0, hfull);
+                }
+                if (k < A) pass1_interior2<RA>(c, p2, k, nseg - 1 - k, U, ck, m0, m1, hfull);
+                f.pr = -p2.mpr.v.x;
+                f.pi = -p2.mpi.v.x;
+                f.qr = p2.qr.v.x;
+                f.qi = p2.qi.v.x;
+                f.lam = p2.lam.v.x;
+                f.H = p2.H.v.x;
+                b.pr = -p2.mpr.v.y;
+                b.pi = -p2.mpi.v.y;
+                b.qr = p2.qr.v.y;
+                b.qi = p2.qi.v.y;
+                b.lam = p2.lam.v.y;
+                b.H = p2.H.v.y;
+            }
+        } else {
+            int k = 1;
+            for (; k + 2 <= A; k += 2) {
+                pass1_block<R, RA, true, true>(c, f, b, k, nseg - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
+                pass1_block<R, RA, true, true>(c, f, b, k + 1, nseg - 2 - k, true, U, ck, ua_f, ua_b, ub_f, ub_b,
+                                               hfull);
+            }
+            if (k < A)
+                pass1_block<R, RA, true, true>(c, f, b, k, nseg - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
         }
-        if (k < A) pass1_block<R, RA, true, true>(c, f, b, k, nseg - 1 - k, true, U, ck, ub_f, ub_b, ua_f, ua_b, hfull);
     }
     Bnd<R> fw, bw;  // forward state at the start of segment nseg - A - (nseg odd), backward at the end of segment A - 1 + (nseg odd)
     proj_boundary<R, RA>(f, fw.yr, fw.yi);
@@ -919,17 +1162,23 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
         prefetch_rec(k + 2);
         R accf[K], accb[K];
         if (!last) {
-            R uf[K], ub[K];
-            load_seg(U, nf, uf);
-            load_seg_reversed(U, nb, ub);
             const CkVals<R> vf{fw.yr, fw.yi, fw.lam, x.yr, x.yi, x.lam};
             const CkVals<R> vb{bw.yr, bw.yi, bw.lam, y.yr, y.yi, y.lam};
-            SegWork<R> wf, wb;
-            seg_fwd<R, RA, false, true>(c, nf, vf, uf, wf, &fw);
-            seg_fwd<R, RA, false, true>(crev, nb, vb, ub, wb, &bw);
             R accr[K];
-            seg_bwd<R, RA, false>(c, nf, uf, wf, accf);
-            seg_bwd<R, RA, false>(crev, nb, ub, wb, accr);
+            if constexpr (std::is_same<R, float>::value) {
+                F2 mu[K];
+                load_seg_pair(U, nf, nb, mu);
+                segment_pair2<RA>(c, crev, vf, vb, mu, accf, accr, fw, bw);
+            } else {
+                R uf[K], ub[K];
+                load_seg(U, nf, uf);
+                load_seg_reversed(U, nb, ub);
+                SegWork<R> wf, wb;
+                seg_fwd<R, RA, false, true>(c, nf, vf, uf, wf, &fw);
+                seg_fwd<R, RA, false, true>(crev, nb, vb, ub, wb, &bw);
+                seg_bwd<R, RA, false>(c, nf, uf, wf, accf);
+                seg_bwd<R, RA, false>(crev, nb, ub, wb, accr);
+            }
 #pragma unroll
             for (int j = 0; j < K; ++j) accb[j] = accr[K - 1 - j];
         } else {
@@ -1197,11 +1446,15 @@ __global__ void __launch_bounds__(32) rgf_piece_prefix_kernel(const TubeDev* __r
 // Fused schedule: one warp (32 whole chains) per block; records in the
 // warp's scratch, per-site sums into the warp's partial row.  One
 // instantiation per precision; block b takes warp order[b].  The FP32
-// instantiation is held to 128 registers (16 resident warps per SM, no
-// spills) to hide the latency of its dependent recurrences; FP64 needs
-// about 240 and spills below that.
+// instantiation (both sweeps packed) is held to NEGF_FP32_MIN_BLOCKS
+// resident warps per SM (12: about 160 registers, no spills) to hide the
+// latency of its dependent recurrences; FP64 needs about 240 registers and
+// spills below that.
+#ifndef NEGF_FP32_MIN_BLOCKS
+#define NEGF_FP32_MIN_BLOCKS 12
+#endif
 template <typename R>
-__global__ void __launch_bounds__(32, (sizeof(R) == 4 ? 16 : 1)) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
+__global__ void __launch_bounds__(32, (sizeof(R) == 4 ? NEGF_FP32_MIN_BLOCKS : 1)) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
                                                        const ChainRec* __restrict__ chains,
                                                        const WarpRec* __restrict__ warps, const int* __restrict__ order,
                                                        int count, double* __restrict__ partial,
