@@ -278,6 +278,7 @@ struct Settings {
     int warps_per_block = 4;
     int pass1_pieces = 0;  // 0: automatic
     int schedule = 0;      // 0: automatic, else NEGF_SCHEDULE_*
+    int nn_gemm = 0;       // 0: default (tcgen05), else NEGF_NN_GEMM_*
     negf_stats stats{};
     Workspace* stats_ws = nullptr;  // workspace whose events time the last call (when timing)
 };
@@ -1601,6 +1602,11 @@ int negf_set_tuning(int key, int value) {
                 return fail(NEGF_ERR_ARG, "schedule must be 0 (automatic), NEGF_SCHEDULE_TWO_PASS or NEGF_SCHEDULE_FUSED");
             G.schedule = value;
             return NEGF_OK;
+        case NEGF_TUNE_NN_GEMM:
+            if (value != 0 && value != NEGF_NN_GEMM_TCGEN05 && value != NEGF_NN_GEMM_MMA_SYNC)
+                return fail(NEGF_ERR_ARG, "GEMM path must be 0 (default), NEGF_NN_GEMM_TCGEN05 or NEGF_NN_GEMM_MMA_SYNC");
+            G.nn_gemm = value;
+            return NEGF_OK;
         default:
             return fail(NEGF_ERR_ARG, "unknown tuning key");
     }
@@ -1903,8 +1909,13 @@ int negf_nn_gemm(int a_trans, int b_trans, int M, int N, int K, int batch, const
                  const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* C_bf16, int accumulate,
                  void* stream) {
     if (!A || !B || !C || M < 0 || N < 0 || K < 0 || batch < 0) return fail(NEGF_ERR_ARG, "bad GEMM arguments");
+    int path;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        path = settings().nn_gemm == NEGF_NN_GEMM_MMA_SYNC ? negf::kNnGemmMmaSync : negf::kNnGemmTcgen05;
+    }
     NEGF_CUDA(negf::nn_gemm(a_trans, b_trans, M, N, K, batch, A, lda, sA, B, ldb, sB, C, ldc, sC, C_bf16, accumulate,
-                            (cudaStream_t)stream));
+                            (cudaStream_t)stream, path));
     return NEGF_OK;
 }
 int negf_nn_gelu_fwd(long long rows, int cols, const float* a, const float* b, const float* bias, float* pre,

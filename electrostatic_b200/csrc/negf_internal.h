@@ -103,9 +103,11 @@ cudaError_t rs_selftest(int which, int m, int count, const double* d_in, double*
 int rs_max_atoms_per_block();
 
 // Surrogate-model kernels (negf_surrogate.cu).  BF16 operands as void*.
+// path: kNnGemmTcgen05 (5th-generation tensor cores, tensor-memory accumulator) or kNnGemmMmaSync
+constexpr int kNnGemmTcgen05 = 1, kNnGemmMmaSync = 2;
 cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* A, int lda, long long sA,
                     const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* Cb, int accumulate,
-                    cudaStream_t s);
+                    cudaStream_t s, int path = kNnGemmTcgen05);
 cudaError_t nn_gelu_fwd(long long rows, int cols, const float* a, const float* b, const float* bias, float* pre,
                         float* out, void* outb, int act, cudaStream_t s);
 cudaError_t nn_gelu_bwd(long long n, const float* dy, const float* pre, float* d, void* db, cudaStream_t s);

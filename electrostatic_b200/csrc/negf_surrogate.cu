@@ -242,6 +242,246 @@ __global__ void __launch_bounds__(NT) gemm_bf16_kernel(int M, int N, int K, cons
             }
 }
 
+// ---------------------------------------------------------------------------
+// The same GEMM on the 5th-generation tensor cores (tcgen05).  One CTA of 128
+// threads computes a 128 x 128 tile of C with the FP32 accumulator in tensor
+// memory: per k-tile of 64, the four warps stage the A and B tiles in shared
+// memory in the UMMA canonical no-swizzle layout (8 x 16-byte core matrices),
+// thread 0 issues four tcgen05.mma (M 128, N 128, K 16, BF16 in, FP32 out)
+// and commits them to an mbarrier, and the next k-tile is staged in the other
+// buffer while they run.  Operands whose contiguous dimension is K use the
+// K-major descriptor, the others the MN-major one, so every staged chunk is
+// one 16-byte store.  The epilogue reads the accumulator with tcgen05.ld (warp
+// w owns rows 32w .. 32w + 31) and writes C as the mma.sync kernel does
+// (bounds, accumulation, BF16 copy, split-K partials).
+// Descriptor encodings (sm_100 UMMA):
+//   shared-memory descriptor: start >> 4 in bits [0,14), leading byte offset
+//   (between the two 8-element K groups of one K-16 step) >> 4 in [16,30),
+//   stride byte offset (between 8-row MN groups) >> 4 in [32,46), version 1
+//   in [46,48), layout 0 (no swizzle) in [61,64);
+//   instruction descriptor (kind::f16): D F32 (1 << 4), A BF16 (1 << 7),
+//   B BF16 (1 << 10), A MN-major (1 << 15), B MN-major (1 << 16), N >> 3 in
+//   [17,23), M >> 4 in [24,29).
+// Waits are bounded: a wait that runs out sets tc_error and the CTA writes
+// NaN into its tile instead of results.
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 64, TC_NT = 128;
+constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 2;            // one operand tile per stage (16 KB)
+constexpr int TC_SMEM = 2 * 2 * TC_TILE_BYTES + 64;         // 2 stages x (A, B) + barriers and the TMEM address
+constexpr uint32_t TC_SBO = (TC_BK / 8) * 128;              // bytes between 8-row MN groups
+constexpr uint32_t TC_LBO = 128;                            // bytes between 8-element K groups
+constexpr long long TC_SPIN_LIMIT = 1LL << 28;
+
+__device__ int tc_error;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((TC_LBO >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((TC_SBO >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+template <bool AMN, bool BMN>
+__device__ __forceinline__ uint32_t umma_idesc() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((AMN ? 1u : 0u) << 15) | ((BMN ? 1u : 0u) << 16) |
+           ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < TC_SPIN_LIMIT; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Stage one 128 x 64 operand tile (rows = the M or N dimension) into shared
+// memory.  KCONTIG: the operand's contiguous dimension is K (element (r, k) at
+// P[r * ld + k]), else it is the row dimension (element (r, k) at P[k * ld + r]).
+// 1024 chunks of 8 contiguous elements, 8 per thread; a chunk inside the
+// matrix with a 16-byte aligned address is one vector load, the rest are
+// bounds-checked element loads (zero outside).
+template <bool KCONTIG>
+__device__ __forceinline__ void tc_load(const __nv_bfloat16* __restrict__ P, int ld, int r0, int rows, int k0,
+                                        int kend, bool aligned, int tid, uint4 (&v)[8]) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int c = tid + TC_NT * i;
+        int r, k;
+        if (KCONTIG) {
+            r = c >> 3;
+            k = (c & 7) * 8;
+        } else {
+            k = c >> 4;
+            r = (c & 15) * 8;
+        }
+        const int gr = r0 + r, gk = k0 + k;
+        const bool full = KCONTIG ? (gr < rows && gk + 8 <= kend) : (gk < kend && gr + 8 <= rows);
+        if (full && aligned) {
+            const __nv_bfloat16* src = KCONTIG ? P + (size_t)gr * ld + gk : P + (size_t)gk * ld + gr;
+            v[i] = *reinterpret_cast<const uint4*>(src);
+        } else {
+            __align__(16) __nv_bfloat16 e[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int rr = KCONTIG ? gr : gr + q, kk = KCONTIG ? gk + q : gk;
+                e[q] = (rr < rows && kk < kend) ? P[KCONTIG ? (size_t)rr * ld + kk : (size_t)kk * ld + rr]
+                                                : __float2bfloat16(0.0f);
+            }
+            v[i] = *reinterpret_cast<const uint4*>(e);
+        }
+    }
+}
+template <bool KCONTIG>
+__device__ __forceinline__ void tc_store(unsigned char* tile, int tid, const uint4 (&v)[8]) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int c = tid + TC_NT * i;
+        uint32_t off;
+        if (KCONTIG) {  // K-major core matrix: row r % 8, 16 bytes of K
+            const int r = c >> 3, kg = c & 7;
+            off = (r >> 3) * TC_SBO + kg * TC_LBO + (r & 7) * 16;
+        } else {  // MN-major core matrix: row k % 8, 16 bytes of MN
+            const int k = c >> 4, rg = c & 15;
+            off = rg * TC_SBO + (k >> 3) * TC_LBO + (k & 7) * 16;
+        }
+        *reinterpret_cast<uint4*>(tile + off) = v[i];
+    }
+}
+
+template <bool AT, bool BT>
+__global__ void __launch_bounds__(TC_NT) gemm_tc_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
+                                                        int lda, long long sA, const __nv_bfloat16* __restrict__ B,
+                                                        int ldb, long long sB, float* __restrict__ C, int ldc,
+                                                        long long sC, __nv_bfloat16* __restrict__ Cb, int accumulate,
+                                                        int splits, int kchunk) {
+    // A (M x K): K contiguous unless AT; B (K x N): N contiguous unless BT
+    constexpr bool AK = !AT, BK_ = BT;
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    unsigned char* tiles = tc_smem;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + 4 * TC_TILE_BYTES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + 4 * TC_TILE_BYTES + 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+    const long long bz = blockIdx.z / splits;
+    const int split = blockIdx.z % splits;
+    const int kbeg = split * kchunk;
+    const int kend = min(K, kbeg + kchunk);
+    A += bz * sA;
+    B += bz * sB;
+    C += splits > 1 ? (long long)blockIdx.z * sC : bz * sC;
+    if (Cb) Cb += bz * sC;
+    const bool alignA = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda % 8 == 0);
+    const bool alignB = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb % 8 == 0);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TC_BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+
+    const int ktiles = (kend - kbeg + TC_BK - 1) / TC_BK;
+    uint32_t phase[2] = {0u, 0u};
+    bool ok = true;
+    for (int kt = 0; kt < ktiles && ok; ++kt) {
+        const int s = kt & 1;
+        const int k0 = kbeg + kt * TC_BK;
+        uint4 va[8], vb[8];
+        tc_load<AK>(A, lda, m0, M, k0, kend, alignA, tid, va);
+        tc_load<BK_>(B, ldb, n0, N, k0, kend, alignB, tid, vb);
+        if (kt >= 2) {  // the MMAs of k-tile kt - 2 read this buffer
+            ok = mbar_wait(smem_u32(&bars[s]), phase[s]);
+            phase[s] ^= 1u;
+        }
+        unsigned char* ta = tiles + (2 * s) * TC_TILE_BYTES;
+        unsigned char* tb = tiles + (2 * s + 1) * TC_TILE_BYTES;
+        tc_store<AK>(ta, tid, va);
+        tc_store<BK_>(tb, tid, vb);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (!__syncthreads_and(ok)) {
+            ok = false;
+            break;
+        }
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t idesc = umma_idesc<!AK, !BK_>();
+#pragma unroll
+            for (int ks = 0; ks < TC_BK / 16; ++ks) {
+                const uint64_t da = umma_desc(smem_u32(ta) + ks * 2 * TC_LBO);
+                const uint64_t db = umma_desc(smem_u32(tb) + ks * 2 * TC_LBO);
+                const uint32_t acc = (kt > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&bars[s]))
+                         : "memory");
+        }
+    }
+    if (ok && ktiles > 0) {  // the last commit covers every MMA issued before it
+        const int sl = (ktiles - 1) & 1;
+        ok = mbar_wait(smem_u32(&bars[sl]), phase[sl]);
+    }
+    ok = __syncthreads_and(ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok && tid == 0) atomicExch(&tc_error, 1);
+    // epilogue: warp w reads accumulator rows 32w .. 32w + 31 (its TMEM lanes), 16 columns at a time
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+        uint32_t r[16];
+        if (ktiles > 0) {
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) r[q] = 0u;
+        }
+        if (row >= M) continue;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int col = n0 + c0 + q;
+            if (col >= N) continue;
+            float v = ok ? __uint_as_float(r[q]) : __int_as_float(0x7fc00000);
+            float* p = C + (size_t)row * ldc + col;
+            if (splits > 1) {
+                *p = v;
+                continue;
+            }
+            if (accumulate) v += *p;
+            *p = v;
+            if (Cb) Cb[(size_t)row * ldc + col] = __float2bfloat16(v);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+}
+
 // C[b][m][n] (+)= sum over splits (in order) of W[b * splits + s][m][n]
 __global__ void splitk_reduce_kernel(int M, int N, int batch, int splits, const float* __restrict__ W,
                                      float* __restrict__ C, int ldc, long long sC, __nv_bfloat16* __restrict__ Cb,
@@ -378,7 +618,7 @@ __global__ void mse_kernel(long long n, const float* __restrict__ q, const float
 
 cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* A, int lda, long long sA,
                     const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* Cb, int accumulate,
-                    cudaStream_t s) {
+                    cudaStream_t s, int path) {
     if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return cudaSuccess;
     const int tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM) * batch;
     // split K when the output has too few tiles to fill the GPU (deterministic: partials + ordered sum)
@@ -411,7 +651,29 @@ cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* 
     const auto* a = static_cast<const __nv_bfloat16*>(A);
     const auto* b = static_cast<const __nv_bfloat16*>(B);
     auto* cb = splits > 1 ? nullptr : static_cast<__nv_bfloat16*>(Cb);
-    if (!at && !bt)
+    if (path != kNnGemmMmaSync) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaFuncSetAttribute(gemm_tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+            cudaFuncSetAttribute(gemm_tc_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+            cudaFuncSetAttribute(gemm_tc_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+            cudaFuncSetAttribute(gemm_tc_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+            attr_set = true;
+        }
+        static_assert(TC_BM == BM && TC_BN == BN, "the two GEMM paths share the tiling of C");
+        if (!at && !bt)
+            gemm_tc_kernel<false, false><<<grid, TC_NT, TC_SMEM, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so,
+                                                                      cb, accumulate, splits, kchunk);
+        else if (!at && bt)
+            gemm_tc_kernel<false, true><<<grid, TC_NT, TC_SMEM, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so,
+                                                                     cb, accumulate, splits, kchunk);
+        else if (at && !bt)
+            gemm_tc_kernel<true, false><<<grid, TC_NT, TC_SMEM, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so,
+                                                                     cb, accumulate, splits, kchunk);
+        else
+            gemm_tc_kernel<true, true><<<grid, TC_NT, TC_SMEM, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so,
+                                                                    cb, accumulate, splits, kchunk);
+    } else if (!at && !bt)
         gemm_bf16_kernel<false, false><<<grid, NT, 0, s>>>(M, N, K, a, lda, sA, b, ldb, sB, out, ldo, so, cb,
                                                            accumulate, splits, kchunk);
     else if (!at && bt)

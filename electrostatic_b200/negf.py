@@ -382,7 +382,9 @@ def set_timing(enable: bool):
 TUNE_PASS2_WARPS_PER_BLOCK = 2
 TUNE_PASS1_PIECES = 4
 TUNE_SCHEDULE = 6
+TUNE_NN_GEMM = 7
 SCHEDULE_AUTO, SCHEDULE_TWO_PASS, SCHEDULE_FUSED = 0, 1, 2
+NN_GEMM_DEFAULT, NN_GEMM_TCGEN05, NN_GEMM_MMA_SYNC = 0, 1, 2
 
 
 def set_tuning(key: int, value: int):

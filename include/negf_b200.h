@@ -221,8 +221,16 @@ int negf_last_stats(negf_stats* s);
 #define NEGF_TUNE_PASS2_WARPS_PER_BLOCK 2
 #define NEGF_TUNE_PASS1_PIECES 4
 #define NEGF_TUNE_SCHEDULE 6
+#define NEGF_TUNE_NN_GEMM 7
 #define NEGF_SCHEDULE_TWO_PASS 1
 #define NEGF_SCHEDULE_FUSED 2
+/* NEGF_TUNE_NN_GEMM: the tensor-core path of negf_nn_gemm: 0 (default) or
+ * NEGF_NN_GEMM_TCGEN05, the 5th-generation tensor cores (tcgen05.mma with
+ * the accumulator in tensor memory), or NEGF_NN_GEMM_MMA_SYNC, warp-level
+ * mma.sync tiles.  Both compute the same BF16 x BF16 -> FP32 products; the
+ * summation order inside a K-16 step may differ. */
+#define NEGF_NN_GEMM_TCGEN05 1
+#define NEGF_NN_GEMM_MMA_SYNC 2
 int negf_set_tuning(int key, int value);
 /* Enable CUDA-event timing of negf_compute_charge (off by default). */
 int negf_set_timing(int enable);

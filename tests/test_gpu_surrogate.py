@@ -7,13 +7,16 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("path", [1, 2])  # tcgen05, mma.sync
 @pytest.mark.parametrize("at,bt", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("M,N,K,batch", [(130, 70, 45, 3), (1, 128, 300, 1), (256, 256, 4, 2), (64, 256, 257, 1),
-                                         (200, 136, 160, 2), (128, 128, 2048, 1)])
-def test_gemm_layouts(at, bt, M, N, K, batch):
+                                         (200, 136, 160, 2), (128, 128, 2048, 1), (384, 256, 512, 2)])
+def test_gemm_layouts(at, bt, M, N, K, batch, path):
     import torch
     from electrostatic_b200 import _lib
+    from electrostatic_b200.negf import TUNE_NN_GEMM, set_tuning
     L = _lib.load()
+    set_tuning(TUNE_NN_GEMM, path)
     g = torch.Generator().manual_seed(M * 7 + N + K)
     A = torch.randn(batch, *((K, M) if at else (M, K)), generator=g).to(torch.bfloat16)
     B = torch.randn(batch, *((N, K) if bt else (K, N)), generator=g).to(torch.bfloat16)
@@ -29,6 +32,7 @@ def test_gemm_layouts(at, bt, M, N, K, batch):
     assert rc == 0
     torch.cuda.synchronize()
     out = dC.cpu()
+    set_tuning(TUNE_NN_GEMM, 0)
     assert torch.allclose(out, ref, rtol=1e-5, atol=1e-4 * (1 + ref.abs().max().item()))
     assert torch.allclose(dCb.float().cpu(), out.to(torch.bfloat16).float())
 
