@@ -287,6 +287,106 @@ def config4_measure(torch, passes=5):
     return out
 
 
+def config4_pass_only(prec, ntubes, passes, warmup):
+    """Profiling case: the charge pass of the first ntubes tubes of the
+    config-4 batch (seeded potentials as in config4_measure), one plan without
+    autotuning, warm-up then CUDA-event timing; prints one JSON line with the
+    error against the FP64 pass of the same potentials."""
+    import torch
+    from electrostatic_b200 import build
+    from electrostatic_b200.negf import CNT, ChargePlan
+    from electrostatic_b200.workloads import SEED_BASE, site_potential, uneven_batch
+    build.build()
+
+    def batch(p):
+        descs = uneven_batch(precision="fp64" if p == "fp64" else "mixed",
+                             realaxis_fp32=p == "mixed_realaxis_fp32")[:ntubes]
+        tubes = [CNT(**d) for d in descs]
+        for i, t in enumerate(tubes):
+            U = site_potential(t.site_positions(), SEED_BASE + 4 + 100 * i)
+            t.set_potential(U, (U[0], U[-1]))
+        Q = torch.zeros(sum(t.num_field_sites for t in tubes), dtype=torch.float64, device="cuda")
+        return tubes, Q, ChargePlan(tubes, Q, autotune=False)
+
+    tubes, Q, plan = batch(prec)
+    s = torch.cuda.current_stream()
+    for _ in range(max(1, warmup)):
+        plan.launch(stream=s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(passes):
+        plan.launch(stream=s)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / passes
+    info = plan.info()
+    out = {"config4_pass": prec, "tubes": ntubes, "ms_per_pass": ms, "updates": info["updates"],
+           "updates_per_s": info["updates"] / (ms * 1e-3)}
+    if prec != "fp64":
+        t64, Q64, p64 = batch("fp64")
+        p64.launch(stream=s)
+        torch.cuda.synchronize()
+        out["max_rel_vs_fp64"] = float((Q - Q64).abs().max() / Q64.abs().max())
+        p64.close()
+        for t in t64:
+            t.close()
+    plan.close()
+    for t in tubes:
+        t.close()
+    print(json.dumps(out))
+
+
+def surrogate_gemm_only(reps, warmup):
+    """Profiling case: the BF16 GEMMs of one training step of the tube-set
+    operator (batch 64 on the 7424-site canvas) through negf_nn_gemm, on the
+    tcgen05 path and on the mma.sync path; one JSON line per shape."""
+    import ctypes as C
+    import torch
+    from electrostatic_b200 import _lib, build
+    from electrostatic_b200.negf import TUNE_NN_GEMM, set_tuning
+    build.build()
+    L = _lib.load()
+    vp = lambda t: C.c_void_p(t.data_ptr())
+    R, S = 64 * 7424, 7424
+    shapes = [("pointwise h W: R x 128 x 128", 0, 0, R, 128, 128, 1),
+              ("spectral analysis F h: 64 x 128 x S, batch 64", 0, 0, 64, 128, S, 64),
+              ("synthesis G z: S x 128 x 64, batch 64", 0, 0, S, 128, 64, 64),
+              ("weight gradient h^T d: 128 x 128 x R", 1, 0, 128, 128, R, 1)]
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for name, at, bt, M, N, K, batch in shapes:
+        A = torch.randn(batch, *((K, M) if at else (M, K)), device="cuda", generator=g).to(torch.bfloat16)
+        B = torch.randn(batch, *((N, K) if bt else (K, N)), device="cuda", generator=g).to(torch.bfloat16)
+        Cm = torch.zeros(batch, M, N, device="cuda")
+        lda, ldb = (M if at else K), (K if bt else N)
+        res = {"shape": name}
+        outs = []
+        for path, key in ((1, "tcgen05"), (2, "mma_sync")):
+            set_tuning(TUNE_NN_GEMM, path)
+
+            def f():
+                rc = L.negf_nn_gemm(at, bt, M, N, K, batch, vp(A), lda, A[0].numel(), vp(B), ldb, B[0].numel(),
+                                    vp(Cm), N, M * N, None, 0, None)
+                if rc != 0:
+                    raise RuntimeError(L.negf_last_error().decode())
+
+            for _ in range(max(1, warmup)):
+                f()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(reps):
+                f()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            res[key] = {"ms": ms, "tflops": 2.0 * M * N * K * batch / ms / 1e9}
+            outs.append(Cm.clone())
+        set_tuning(TUNE_NN_GEMM, 0)
+        res["max_abs_diff_paths"] = float((outs[0] - outs[1]).abs().max())
+        print(json.dumps(res))
+
+
 def config3_measure(torch, passes=2, small=False):
     """Real-space ring blocks: (13,0), 600 blocks of 26 atoms, 2048 contour
     energies + poles, FP64 and mixed; against the mode-space pass of the same
@@ -552,6 +652,11 @@ def main():
     ap.add_argument("--small", action="store_true",
                     help="profiling case: same tube, E = 1024 (256 contour + 768 real-axis); "
                          "real-space case of 200 blocks and 256 contour energies")
+    ap.add_argument("--config4-pass", default=None, choices=["fp64", "mixed", "mixed_realaxis_fp32"],
+                    help="profiling case: only the config-4 batch charge pass in this precision (one JSON line)")
+    ap.add_argument("--tubes", type=int, default=16, help="with --config4-pass: the first TUBES tubes of the batch")
+    ap.add_argument("--surrogate-gemm", action="store_true",
+                    help="profiling case: negf_nn_gemm on the surrogate's shapes, both tensor-core paths")
     args = ap.parse_args()
     if args.small:
         global EQ_PTS, RT_PTS, WORKLOAD
@@ -566,6 +671,12 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.config4_pass:
+        config4_pass_only(args.config4_pass, args.tubes, args.steps, args.warmup)
+        return
+    if args.surrogate_gemm:
+        surrogate_gemm_only(args.steps, args.warmup)
         return
 
     import torch

@@ -378,6 +378,9 @@ __global__ void __launch_bounds__(TC_NT) gemm_tc_kernel(int M, int N, int K, con
     if (Cb) Cb += bz * sC;
     const bool alignA = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda % 8 == 0);
     const bool alignB = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb % 8 == 0);
+    // vector epilogue: rows of C (and of its BF16 copy) 16-byte aligned at every 16th column
+    const bool vec_c = ((reinterpret_cast<uintptr_t>(C) & 15) == 0) && (ldc % 8 == 0) &&
+                       (splits > 1 || !Cb || (reinterpret_cast<uintptr_t>(Cb) & 15) == 0);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -462,6 +465,36 @@ __global__ void __launch_bounds__(TC_NT) gemm_tc_kernel(int M, int N, int K, con
             for (int q = 0; q < 16; ++q) r[q] = 0u;
         }
         if (row >= M) continue;
+        const int col0 = n0 + c0;
+        if (ok && col0 + 16 <= N && vec_c) {
+            // 16 consecutive columns of one row: four 16-byte stores (whole sectors)
+            float* p = C + (size_t)row * ldc + col0;
+            float v[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+            if (splits == 1 && accumulate) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 o = reinterpret_cast<const float4*>(p)[q];
+                    v[4 * q] += o.x;
+                    v[4 * q + 1] += o.y;
+                    v[4 * q + 2] += o.z;
+                    v[4 * q + 3] += o.w;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            if (splits == 1 && Cb) {
+                __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) hb[q] = __float2bfloat16(v[q]);
+                uint4* pb = reinterpret_cast<uint4*>(Cb + (size_t)row * ldc + col0);
+                pb[0] = reinterpret_cast<const uint4*>(hb)[0];
+                pb[1] = reinterpret_cast<const uint4*>(hb)[1];
+            }
+            continue;
+        }
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
             const int col = n0 + c0 + q;
