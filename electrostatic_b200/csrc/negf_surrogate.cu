@@ -300,6 +300,23 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
+// Chunk c (0 .. 1023) of a 128 x 64 operand tile: 8 contiguous elements
+// starting at row r, column k.  A warp's 32 chunks cover 8 consecutive
+// core-matrix rows x 4 consecutive 16-byte columns, so its global loads are
+// 64-byte runs and its 16-byte shared stores hit 8 distinct bank groups
+// (no conflicts in the no-swizzle core-matrix layout).
+template <bool KCONTIG>
+__device__ __forceinline__ void tc_chunk(int c, int& r, int& k) {
+    const int lo = c & 7, mid = (c >> 3) & 3, rest = c >> 5;
+    if (KCONTIG) {  // core rows are rows r; 8 K-groups of 8
+        r = (rest & 15) * 8 + lo;
+        k = ((rest >> 4) * 4 + mid) * 8;
+    } else {  // core rows are k; 16 row-groups of 8
+        k = (rest >> 2) * 8 + lo;
+        r = ((rest & 3) * 4 + mid) * 8;
+    }
+}
+
 // Stage one 128 x 64 operand tile (rows = the M or N dimension) into shared
 // memory.  KCONTIG: the operand's contiguous dimension is K (element (r, k) at
 // P[r * ld + k]), else it is the row dimension (element (r, k) at P[k * ld + r]).
@@ -313,13 +330,7 @@ __device__ __forceinline__ void tc_load(const __nv_bfloat16* __restrict__ P, int
     for (int i = 0; i < 8; ++i) {
         const int c = tid + TC_NT * i;
         int r, k;
-        if (KCONTIG) {
-            r = c >> 3;
-            k = (c & 7) * 8;
-        } else {
-            k = c >> 4;
-            r = (c & 15) * 8;
-        }
+        tc_chunk<KCONTIG>(c, r, k);
         const int gr = r0 + r, gk = k0 + k;
         const bool full = KCONTIG ? (gr < rows && gk + 8 <= kend) : (gk < kend && gr + 8 <= rows);
         if (full && aligned) {
@@ -342,14 +353,13 @@ __device__ __forceinline__ void tc_store(unsigned char* tile, int tid, const uin
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int c = tid + TC_NT * i;
+        int r, k;
+        tc_chunk<KCONTIG>(c, r, k);
         uint32_t off;
-        if (KCONTIG) {  // K-major core matrix: row r % 8, 16 bytes of K
-            const int r = c >> 3, kg = c & 7;
-            off = (r >> 3) * TC_SBO + kg * TC_LBO + (r & 7) * 16;
-        } else {  // MN-major core matrix: row k % 8, 16 bytes of MN
-            const int k = c >> 4, rg = c & 15;
-            off = rg * TC_SBO + (k >> 3) * TC_LBO + (k & 7) * 16;
-        }
+        if (KCONTIG)  // K-major core matrix: row r % 8, 16 bytes of K
+            off = (r >> 3) * TC_SBO + (k >> 3) * TC_LBO + (r & 7) * 16;
+        else  // MN-major core matrix: row k % 8, 16 bytes of MN
+            off = (r >> 3) * TC_SBO + (k >> 3) * TC_LBO + (k & 7) * 16;
         *reinterpret_cast<uint4*>(tile + off) = v[i];
     }
 }
