@@ -586,7 +586,9 @@ def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True
         # rows carried between gate points, and with the fraction from the operator's Jacobian
         variants = [(m, dict(start=m)) for m in ("difference", "surrogate", "extrapolation", "continuation", "zero")]
         variants += [("extrapolated_carry_rows", dict(carry_rows=True)),
-                     ("extrapolated_fraction_from_operator", dict(fraction=None))]
+                     ("extrapolated_fraction_from_operator", dict(fraction=None)),
+                     ("extrapolated_fraction_0.15", dict(fraction=0.15)),
+                     ("extrapolated_fraction_0.25", dict(fraction=0.25, max_fraction=0.25))]
         for name, kw in variants:
             try:
                 o, a_, l_, _ = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, **kw)
