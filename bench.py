@@ -287,7 +287,7 @@ def config4_measure(torch, passes=5):
     return out
 
 
-def config4_pass_only(prec, ntubes, passes, warmup):
+def config4_pass_only(prec, ntubes, passes, warmup, autotune=False):
     """Profiling case: the charge pass of the first ntubes tubes of the
     config-4 batch (seeded potentials as in config4_measure), one plan without
     autotuning, warm-up then CUDA-event timing; prints one JSON line with the
@@ -306,7 +306,7 @@ def config4_pass_only(prec, ntubes, passes, warmup):
             U = site_potential(t.site_positions(), SEED_BASE + 4 + 100 * i)
             t.set_potential(U, (U[0], U[-1]))
         Q = torch.zeros(sum(t.num_field_sites for t in tubes), dtype=torch.float64, device="cuda")
-        return tubes, Q, ChargePlan(tubes, Q, autotune=False)
+        return tubes, Q, ChargePlan(tubes, Q, autotune=autotune and p == prec)
 
     tubes, Q, plan = batch(prec)
     s = torch.cuda.current_stream()
@@ -321,8 +321,10 @@ def config4_pass_only(prec, ntubes, passes, warmup):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / passes
     info = plan.info()
-    out = {"config4_pass": prec, "tubes": ntubes, "ms_per_pass": ms, "updates": info["updates"],
-           "updates_per_s": info["updates"] / (ms * 1e-3)}
+    out = {"config4_pass": prec, "tubes": ntubes, "autotune": bool(autotune), "ms_per_pass": ms,
+           "updates": info["updates"], "updates_per_s": info["updates"] / (ms * 1e-3),
+           "schedule": {"pass2_warps_per_block": info["pass2_warps_per_block"],
+                        "segs_per_unit": info["segs_per_unit"], "tuned_ms": info["tuned_ms"]}}
     if prec != "fp64":
         t64, Q64, p64 = batch("fp64")
         p64.launch(stream=s)
@@ -589,9 +591,14 @@ def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True
                      ("extrapolated_fraction_from_operator", dict(fraction=None)),
                      ("extrapolated_fraction_0.15", dict(fraction=0.15)),
                      ("extrapolated_fraction_0.25", dict(fraction=0.25, max_fraction=0.25))]
+        # the design rule's mixed mode (real-axis chains in FP64, contour chains in FP32)
+        tubesrule = make(vds, precision="mixed")
+        variants.append(("extrapolated_realaxis_fp64", dict(tubes=tubesrule)))
         for name, kw in variants:
+            kw = dict(kw)
+            tset = kw.pop("tubes", tubesmx)
             try:
-                o, a_, l_, _ = fixed_point_sweep(tubesmx, electros, GATE_SWEEP, model, **kw)
+                o, a_, l_, _ = fixed_point_sweep(tset, electros, GATE_SWEEP, model, **kw)
             except RuntimeError as e:  # a variant that does not converge is reported, not fatal
                 res["same_solver_" + name] = {"error": str(e)}
                 continue
@@ -609,9 +616,10 @@ def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True
         r = sur[-1]
         n_conv = r["n_in"]
         offs = np.concatenate([[0], np.cumsum([t.num_field_sites for t in tubesmx])]).astype(int)
-        worst, worst_mx, t1 = 0.0, 0.0, time.perf_counter()
+        worst, worst_mx, worst_rule, t1 = 0.0, 0.0, 0.0, time.perf_counter()
         qmx = float(np.max(np.abs(n_conv)))
-        for d, e, a, b, tm in zip(descs, electros, offs[:-1], offs[1:], tubesmx):
+        rule = tubesrule if ablation else [None] * len(descs)
+        for d, e, a, b, tm, tr in zip(descs, electros, offs[:-1], offs[1:], tubesmx, rule):
             kw = {k: v for k, v in d.items() if k not in ("precision", "mixed_realaxis_fp32")}
             ot = O.OracleTube(**dict(kw, contact_mu=(0.0, -vds)))
             Uc = e.potential(n_conv[a:b], GATE_SWEEP[-1])
@@ -621,16 +629,20 @@ def config5_measure(torch, n_pairs=20000, epochs=20, batch=64, oracle_check=True
             # the mixed-precision engine's charge at the same potential against the oracle's
             qm = tm.Solve_NEGF(Uc, (Uc[0], Uc[-1]))
             worst_mx = max(worst_mx, float(np.max(np.abs(qm - qo))))
+            if tr is not None:
+                worst_rule = max(worst_rule, float(np.max(np.abs(tr.Solve_NEGF(Uc, (Uc[0], Uc[-1])) - qo))))
         res["oracle_fixed_point"] = {"Vg": GATE_SWEEP[-1], "max_abs_Qoracle_minus_n": worst,
                                      "relative": worst / qmx, "residual_bar_abs": 1e-6,
                                      "within_residual_bar": bool(worst <= 1e-6),
                                      "mixed_charge_max_rel_vs_oracle": worst_mx / qmx,
+                                     "mixed_realaxis_fp64_charge_max_rel_vs_oracle": (worst_rule / qmx
+                                                                                      if ablation else None),
                                      "seconds": time.perf_counter() - t1,
                                      "check": "|Q_oracle(U(n)) - n| of the surrogate sweep's converged charge n (the "
                                               "FP64 oracle's residual of the fixed point; the loop's bar is 1e-6 "
                                               "absolute), and the mixed-precision engine's charge at U(n) against "
                                               "the oracle's"}
-    for t in tubes64 + tubesmx:
+    for t in tubes64 + tubesmx + (tubesrule if ablation else []):
         t.close()
     return res
 
@@ -667,6 +679,7 @@ def main():
     ap.add_argument("--config4-pass", default=None, choices=["fp64", "mixed", "mixed_realaxis_fp32"],
                     help="profiling case: only the config-4 batch charge pass in this precision (one JSON line)")
     ap.add_argument("--tubes", type=int, default=16, help="with --config4-pass: the first TUBES tubes of the batch")
+    ap.add_argument("--autotune", action="store_true", help="with --config4-pass: an autotuned plan")
     ap.add_argument("--surrogate-gemm", action="store_true",
                     help="profiling case: negf_nn_gemm on the surrogate's shapes, both tensor-core paths")
     args = ap.parse_args()
@@ -685,7 +698,7 @@ def main():
         run_reference_arm(args, rank, world)
         return
     if args.config4_pass:
-        config4_pass_only(args.config4_pass, args.tubes, args.steps, args.warmup)
+        config4_pass_only(args.config4_pass, args.tubes, args.steps, args.warmup, args.autotune)
         return
     if args.surrogate_gemm:
         surrogate_gemm_only(args.steps, args.warmup)
