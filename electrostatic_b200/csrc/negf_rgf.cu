@@ -1453,8 +1453,11 @@ __global__ void __launch_bounds__(32) rgf_piece_prefix_kernel(const TubeDev* __r
 #ifndef NEGF_FP32_MIN_BLOCKS
 #define NEGF_FP32_MIN_BLOCKS 12
 #endif
+#ifndef NEGF_FP64_MIN_BLOCKS
+#define NEGF_FP64_MIN_BLOCKS 1
+#endif
 template <typename R>
-__global__ void __launch_bounds__(32, (sizeof(R) == 4 ? NEGF_FP32_MIN_BLOCKS : 1)) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
+__global__ void __launch_bounds__(32, (sizeof(R) == 4 ? NEGF_FP32_MIN_BLOCKS : NEGF_FP64_MIN_BLOCKS)) rgf_fused_kernel(const TubeDev* __restrict__ tubes,
                                                        const ChainRec* __restrict__ chains,
                                                        const WarpRec* __restrict__ warps, const int* __restrict__ order,
                                                        int count, double* __restrict__ partial,
