@@ -1603,8 +1603,10 @@ int negf_set_tuning(int key, int value) {
             G.schedule = value;
             return NEGF_OK;
         case NEGF_TUNE_NN_GEMM:
-            if (value != 0 && value != NEGF_NN_GEMM_TCGEN05 && value != NEGF_NN_GEMM_MMA_SYNC)
-                return fail(NEGF_ERR_ARG, "GEMM path must be 0 (default), NEGF_NN_GEMM_TCGEN05 or NEGF_NN_GEMM_MMA_SYNC");
+            if (value != 0 && value != NEGF_NN_GEMM_TCGEN05 && value != NEGF_NN_GEMM_MMA_SYNC &&
+                value != NEGF_NN_GEMM_TCGEN05_STAGED)
+                return fail(NEGF_ERR_ARG, "GEMM path must be 0 (default), NEGF_NN_GEMM_TCGEN05, "
+                                          "NEGF_NN_GEMM_TCGEN05_STAGED or NEGF_NN_GEMM_MMA_SYNC");
             G.nn_gemm = value;
             return NEGF_OK;
         default:
@@ -1912,7 +1914,10 @@ int negf_nn_gemm(int a_trans, int b_trans, int M, int N, int K, int batch, const
     int path;
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        path = settings().nn_gemm == NEGF_NN_GEMM_MMA_SYNC ? negf::kNnGemmMmaSync : negf::kNnGemmTcgen05;
+        const int v = settings().nn_gemm;
+        path = v == NEGF_NN_GEMM_MMA_SYNC ? negf::kNnGemmMmaSync
+               : v == NEGF_NN_GEMM_TCGEN05_STAGED ? negf::kNnGemmTcgen05Staged
+                                                  : negf::kNnGemmTcgen05;
     }
     NEGF_CUDA(negf::nn_gemm(a_trans, b_trans, M, N, K, batch, A, lda, sA, B, ldb, sB, C, ldc, sC, C_bf16, accumulate,
                             (cudaStream_t)stream, path));

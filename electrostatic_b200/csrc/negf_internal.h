@@ -103,8 +103,9 @@ cudaError_t rs_selftest(int which, int m, int count, const double* d_in, double*
 int rs_max_atoms_per_block();
 
 // Surrogate-model kernels (negf_surrogate.cu).  BF16 operands as void*.
-// path: kNnGemmTcgen05 (5th-generation tensor cores, tensor-memory accumulator) or kNnGemmMmaSync
-constexpr int kNnGemmTcgen05 = 1, kNnGemmMmaSync = 2;
+// path: kNnGemmTcgen05 (5th-generation tensor cores, tensor-memory accumulator; operands by TMA where
+// they can be described, else register-staged), kNnGemmTcgen05Staged (register-staged only) or kNnGemmMmaSync
+constexpr int kNnGemmTcgen05 = 1, kNnGemmMmaSync = 2, kNnGemmTcgen05Staged = 3;
 cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* A, int lda, long long sA,
                     const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* Cb, int accumulate,
                     cudaStream_t s, int path = kNnGemmTcgen05);

@@ -13,6 +13,7 @@
 // the current one is multiplied.  Every global access is bounds-checked, so
 // M, N, K need not be tile multiples.
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -364,6 +365,57 @@ __device__ __forceinline__ void tc_store(unsigned char* tile, int tid, const uin
     }
 }
 
+// Epilogue of both tcgen05 kernels: 16 accumulator columns of one row of C
+// (bounds, accumulation, BF16 copy, split-K partials; NaN when a wait ran out).
+__device__ __forceinline__ void tc_write16(float* __restrict__ C, int ldc, __nv_bfloat16* __restrict__ Cb, int row,
+                                           int col0, int M, int N, const uint32_t (&r)[16], bool ok, bool vec_c,
+                                           int splits, int accumulate) {
+    if (row >= M) return;
+    if (ok && col0 + 16 <= N && vec_c) {
+        // 16 consecutive columns of one row: four 16-byte stores (whole sectors)
+        float* p = C + (size_t)row * ldc + col0;
+        float v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+        if (splits == 1 && accumulate) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 o = reinterpret_cast<const float4*>(p)[q];
+                v[4 * q] += o.x;
+                v[4 * q + 1] += o.y;
+                v[4 * q + 2] += o.z;
+                v[4 * q + 3] += o.w;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        if (splits == 1 && Cb) {
+            __align__(16) __nv_bfloat16 hb[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) hb[q] = __float2bfloat16(v[q]);
+            uint4* pb = reinterpret_cast<uint4*>(Cb + (size_t)row * ldc + col0);
+            pb[0] = reinterpret_cast<const uint4*>(hb)[0];
+            pb[1] = reinterpret_cast<const uint4*>(hb)[1];
+        }
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int col = col0 + q;
+        if (col >= N) continue;
+        float v = ok ? __uint_as_float(r[q]) : __int_as_float(0x7fc00000);
+        float* p = C + (size_t)row * ldc + col;
+        if (splits > 1) {
+            *p = v;
+            continue;
+        }
+        if (accumulate) v += *p;
+        *p = v;
+        if (Cb) Cb[(size_t)row * ldc + col] = __float2bfloat16(v);
+    }
+}
+
 template <bool AT, bool BT>
 __global__ void __launch_bounds__(TC_NT) gemm_tc_kernel(int M, int N, int K, const __nv_bfloat16* __restrict__ A,
                                                         int lda, long long sA, const __nv_bfloat16* __restrict__ B,
@@ -474,51 +526,169 @@ __global__ void __launch_bounds__(TC_NT) gemm_tc_kernel(int M, int N, int K, con
 #pragma unroll
             for (int q = 0; q < 16; ++q) r[q] = 0u;
         }
-        if (row >= M) continue;
-        const int col0 = n0 + c0;
-        if (ok && col0 + 16 <= N && vec_c) {
-            // 16 consecutive columns of one row: four 16-byte stores (whole sectors)
-            float* p = C + (size_t)row * ldc + col0;
-            float v[16];
-#pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
-            if (splits == 1 && accumulate) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float4 o = reinterpret_cast<const float4*>(p)[q];
-                    v[4 * q] += o.x;
-                    v[4 * q + 1] += o.y;
-                    v[4 * q + 2] += o.z;
-                    v[4 * q + 3] += o.w;
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-            if (splits == 1 && Cb) {
-                __align__(16) __nv_bfloat16 hb[16];
-#pragma unroll
-                for (int q = 0; q < 16; ++q) hb[q] = __float2bfloat16(v[q]);
-                uint4* pb = reinterpret_cast<uint4*>(Cb + (size_t)row * ldc + col0);
-                pb[0] = reinterpret_cast<const uint4*>(hb)[0];
-                pb[1] = reinterpret_cast<const uint4*>(hb)[1];
-            }
-            continue;
+        tc_write16(C, ldc, Cb, row, n0 + c0, M, N, r, ok, vec_c, splits, accumulate);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN));
+}
+
+// ---------------------------------------------------------------------------
+// The tcgen05 GEMM fed by the Tensor Memory Accelerator.  Same tile and
+// accumulator as gemm_tc_kernel, but the operand tiles arrive by
+// cp.async.bulk.tensor (one elected thread issues them) into the 128-byte
+// swizzled UMMA layout, through a ring of TMA_STAGES k-tile buffers with a
+// "full" mbarrier (transaction bytes) and an "empty" mbarrier (the commit of
+// the MMAs that read the buffer) per stage: warp 0 produces, warp 1 issues
+// the MMAs, all four warps run the epilogue.  Tiles past the matrix edges
+// arrive zero-filled (out-of-bounds fill), so edge tiles need no special path.
+//   K-major operand (K contiguous): one box of 64 K x 128 rows per stage,
+//   rows of 128 bytes, 8-row swizzle atoms 1024 bytes apart (SBO); a K-16
+//   step advances the descriptor's start by 32 bytes inside the atom.
+//   MN-major operand (M or N contiguous): two boxes of 64 MN x 64 K, rows
+//   (one K each) of 128 bytes; 8-row K groups 1024 bytes apart (SBO), the two
+//   64-wide MN halves 8 KB apart (LBO); a K-16 step advances 2048 bytes.
+// Descriptor layout type 2 = 128-byte swizzle (bits [61,64)).
+constexpr int TMA_STAGES = 4;
+constexpr int TMA_SMEM = TMA_STAGES * 2 * TC_TILE_BYTES + 1024 + 128;  // ring + alignment slack + barriers
+
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                            int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+template <bool AK, bool BKC>
+__global__ void __launch_bounds__(TC_NT) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                         const __grid_constant__ CUtensorMap tmB, int M, int N,
+                                                         int K, float* __restrict__ C, int ldc, long long sC,
+                                                         __nv_bfloat16* __restrict__ Cb, int accumulate, int splits,
+                                                         int kchunk, int a_batched, int b_batched) {
+    extern __shared__ unsigned char tma_smem_raw[];
+    // 1024-byte aligned ring (the swizzle atoms' alignment)
+    const uint32_t raw = smem_u32(tma_smem_raw);
+    const uint32_t ring = (raw + 1023u) & ~1023u;
+    unsigned char* ring_ptr = tma_smem_raw + (ring - raw);
+    uint64_t* full = reinterpret_cast<uint64_t*>(ring_ptr + TMA_STAGES * 2 * TC_TILE_BYTES);
+    uint64_t* empty = full + TMA_STAGES;
+    uint64_t* done = empty + TMA_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+    const int bz = blockIdx.z / splits;
+    const int split = blockIdx.z % splits;
+    const int kbeg = split * kchunk;
+    const int kend = min(K, kbeg + kchunk);
+    C += splits > 1 ? (long long)blockIdx.z * sC : (long long)bz * sC;
+    if (Cb) Cb += (long long)bz * sC;
+    const bool vec_c = ((reinterpret_cast<uintptr_t>(C) & 15) == 0) && (ldc % 8 == 0) &&
+                       (splits > 1 || !Cb || (reinterpret_cast<uintptr_t>(Cb) & 15) == 0);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TC_BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 32) {
+        for (int i = 0; i < TMA_STAGES; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[i])));
         }
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-            const int col = n0 + c0 + q;
-            if (col >= N) continue;
-            float v = ok ? __uint_as_float(r[q]) : __int_as_float(0x7fc00000);
-            float* p = C + (size_t)row * ldc + col;
-            if (splits > 1) {
-                *p = v;
-                continue;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(done)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+    const int ktiles = (kend - kbeg + TC_BK - 1) / TC_BK;
+    const int za = a_batched ? bz : 0, zb = b_batched ? bz : 0;
+    bool ok = true;
+
+    if (tid == 0) {  // producer
+        for (int kt = 0; kt < ktiles && ok; ++kt) {
+            const int s = kt % TMA_STAGES;
+            if (kt >= TMA_STAGES) ok = mbar_wait(smem_u32(&empty[s]), (uint32_t)((kt / TMA_STAGES - 1) & 1));
+            if (!ok) break;
+            const uint32_t bar = smem_u32(&full[s]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(2 * TC_TILE_BYTES)
+                         : "memory");
+            const uint32_t ta = ring + (2 * s) * TC_TILE_BYTES, tb = ring + (2 * s + 1) * TC_TILE_BYTES;
+            const int k0 = kbeg + kt * TC_BK;
+            if (AK) {
+                tma_load_3d(ta, &tmA, bar, k0, m0, za);
+            } else {
+                tma_load_3d(ta, &tmA, bar, m0, k0, za);
+                tma_load_3d(ta + TC_TILE_BYTES / 2, &tmA, bar, m0 + 64, k0, za);
             }
-            if (accumulate) v += *p;
-            *p = v;
-            if (Cb) Cb[(size_t)row * ldc + col] = __float2bfloat16(v);
+            if (BKC) {
+                tma_load_3d(tb, &tmB, bar, k0, n0, zb);
+            } else {
+                tma_load_3d(tb, &tmB, bar, n0, k0, zb);
+                tma_load_3d(tb + TC_TILE_BYTES / 2, &tmB, bar, n0 + 64, k0, zb);
+            }
         }
+    } else if (tid == 32) {  // MMA issuer
+        const uint32_t idesc = umma_idesc<!AK, !BKC>();
+        for (int kt = 0; kt < ktiles && ok; ++kt) {
+            const int s = kt % TMA_STAGES;
+            ok = mbar_wait(smem_u32(&full[s]), (uint32_t)((kt / TMA_STAGES) & 1));
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t ta = ring + (2 * s) * TC_TILE_BYTES, tb = ring + (2 * s + 1) * TC_TILE_BYTES;
+#pragma unroll
+            for (int ks = 0; ks < TC_BK / 16; ++ks) {
+                const uint64_t da = AK ? umma_desc_sw128(ta + ks * 32, 16, 1024)
+                                       : umma_desc_sw128(ta + ks * 2048, TC_TILE_BYTES / 2, 1024);
+                const uint64_t db = BKC ? umma_desc_sw128(tb + ks * 32, 16, 1024)
+                                        : umma_desc_sw128(tb + ks * 2048, TC_TILE_BYTES / 2, 1024);
+                const uint32_t acc = (kt > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&empty[s]))
+                         : "memory");
+        }
+        if (ok && ktiles > 0)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(done))
+                         : "memory");
+    }
+    ok = __syncthreads_and(ok) != 0;
+    if (ok && ktiles > 0) ok = mbar_wait(smem_u32(done), 0u);
+    ok = __syncthreads_and(ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok && tid == 0) atomicExch(&tc_error, 1);
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+        uint32_t r[16];
+        if (ktiles > 0) {
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+                "%14, %15}, [%16];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) r[q] = 0u;
+        }
+        tc_write16(C, ldc, Cb, row, n0 + c0, M, N, r, ok, vec_c, splits, accumulate);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -659,17 +829,81 @@ __global__ void mse_kernel(long long n, const float* __restrict__ q, const float
 
 }  // namespace
 
+// Tensor maps of the TMA path.  An operand is described as a 3-d tensor
+// (contiguous dimension, the other matrix dimension, batch) with 128-byte
+// swizzle; boxes of 64 x 128 (K contiguous) or 64 x 64 (M or N contiguous).
+// cudaErrorNotSupported: the operand's layout cannot be described (16-byte
+// alignment of the base and the leading dimension, batches that overlap) and
+// the caller takes the register-staged kernel.
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiled encode_tiled() {
+    static EncodeTiled fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+// inner: the contiguous extent, outer: the other extent, ld: elements between
+// rows of outer, sb: elements between batches (0: shared by every batch)
+static bool make_map(CUtensorMap* m, const __nv_bfloat16* base, long long inner, long long outer, int ld, long long sb,
+                     int batch, bool k_contig, int* batched) {
+    EncodeTiled enc = encode_tiled();
+    if (!enc) return false;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || ld % 8 != 0 || ld < inner) return false;
+    const bool use_batch = batch > 1 && sb != 0;
+    if (use_batch && (sb % 8 != 0 || sb < (long long)ld * outer)) return false;
+    *batched = use_batch ? 1 : 0;
+    const cuuint64_t dims[3] = {(cuuint64_t)inner, (cuuint64_t)outer, (cuuint64_t)(use_batch ? batch : 1)};
+    const cuuint64_t strides[2] = {(cuuint64_t)ld * 2, (cuuint64_t)(use_batch ? sb : (long long)ld * outer) * 2};
+    const cuuint32_t box[3] = {64, (cuuint32_t)(k_contig ? 128 : 64), 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+template <bool AK, bool BKC>
+static cudaError_t launch_tma(int M, int N, int K, int batch, const __nv_bfloat16* a, int lda, long long sA,
+                              const __nv_bfloat16* b, int ldb, long long sB, float* out, int ldo, long long so,
+                              __nv_bfloat16* cb, int accumulate, int splits, int kchunk, dim3 grid, cudaStream_t s) {
+    CUtensorMap ta, tb;
+    int ab = 0, bb = 0;
+    // A (M x K): K contiguous when AK; B (K x N): K contiguous when BKC
+    if (!make_map(&ta, a, AK ? K : M, AK ? M : K, lda, sA, batch, AK, &ab)) return cudaErrorNotSupported;
+    if (!make_map(&tb, b, BKC ? K : N, BKC ? N : K, ldb, sB, batch, BKC, &bb)) return cudaErrorNotSupported;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(gemm_tma_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
+        cudaFuncSetAttribute(gemm_tma_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
+        cudaFuncSetAttribute(gemm_tma_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
+        cudaFuncSetAttribute(gemm_tma_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
+        attr = true;
+    }
+    gemm_tma_kernel<AK, BKC><<<grid, TC_NT, TMA_SMEM, s>>>(ta, tb, M, N, K, out, ldo, so, cb, accumulate, splits,
+                                                          kchunk, ab, bb);
+    return cudaGetLastError();
+}
+
 cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* A, int lda, long long sA,
                     const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* Cb, int accumulate,
                     cudaStream_t s, int path) {
     if (M <= 0 || N <= 0 || K <= 0 || batch <= 0) return cudaSuccess;
     const int tiles = ((N + BN - 1) / BN) * ((M + BM - 1) / BM) * batch;
     // split K when the output has too few tiles to fill the GPU (deterministic: partials + ordered sum)
+    // (k-chunks in whole 64-element tiles, so that a tensor-core k-tile never straddles two splits)
+    const int kg = path == kNnGemmMmaSync ? BK : TC_BK;
     int splits = 1;
-    const int kt = (K + BK - 1) / BK;
+    const int kt = (K + kg - 1) / kg;
     if (tiles < 296 && kt >= 8) splits = std::min(std::min(296 / tiles + 1, kt / 4), 64);
     if (splits < 1) splits = 1;
-    const int kchunk = ((kt + splits - 1) / splits) * BK;
+    const int kchunk = ((kt + splits - 1) / splits) * kg;
     splits = (K + kchunk - 1) / kchunk;
     static float* ws = nullptr;
     static size_t ws_bytes = 0;
@@ -694,6 +928,31 @@ cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* 
     const auto* a = static_cast<const __nv_bfloat16*>(A);
     const auto* b = static_cast<const __nv_bfloat16*>(B);
     auto* cb = splits > 1 ? nullptr : static_cast<__nv_bfloat16*>(Cb);
+    if (path != kNnGemmMmaSync && path != kNnGemmTcgen05Staged) {
+        cudaError_t e = cudaErrorNotSupported;
+        if (at == 0 && bt == 0)
+            e = launch_tma<true, false>(M, N, K, batch, a, lda, sA, b, ldb, sB, out, ldo, so, cb, accumulate, splits,
+                                        kchunk, grid, s);
+        else if (at == 0 && bt == 1)
+            e = launch_tma<true, true>(M, N, K, batch, a, lda, sA, b, ldb, sB, out, ldo, so, cb, accumulate, splits,
+                                       kchunk, grid, s);
+        else if (at == 1 && bt == 0)
+            e = launch_tma<false, false>(M, N, K, batch, a, lda, sA, b, ldb, sB, out, ldo, so, cb, accumulate, splits,
+                                         kchunk, grid, s);
+        else
+            e = launch_tma<false, true>(M, N, K, batch, a, lda, sA, b, ldb, sB, out, ldo, so, cb, accumulate, splits,
+                                        kchunk, grid, s);
+        if (e == cudaSuccess) {
+            if (splits == 1) return cudaSuccess;
+            const long long n = (long long)M * N * batch;
+            splitk_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(M, N, batch, splits, ws, C, ldc, sC,
+                                                                             static_cast<__nv_bfloat16*>(Cb),
+                                                                             accumulate);
+            return cudaGetLastError();
+        }
+        if (e != cudaErrorNotSupported) return e;
+        // operands TMA cannot describe: the register-staged tcgen05 kernel
+    }
     if (path != kNnGemmMmaSync) {
         static bool attr_set = false;
         if (!attr_set) {

@@ -384,7 +384,7 @@ TUNE_PASS1_PIECES = 4
 TUNE_SCHEDULE = 6
 TUNE_NN_GEMM = 7
 SCHEDULE_AUTO, SCHEDULE_TWO_PASS, SCHEDULE_FUSED = 0, 1, 2
-NN_GEMM_DEFAULT, NN_GEMM_TCGEN05, NN_GEMM_MMA_SYNC = 0, 1, 2
+NN_GEMM_DEFAULT, NN_GEMM_TCGEN05, NN_GEMM_MMA_SYNC, NN_GEMM_TCGEN05_STAGED = 0, 1, 2, 3
 
 
 def set_tuning(key: int, value: int):

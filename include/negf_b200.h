@@ -226,11 +226,16 @@ int negf_last_stats(negf_stats* s);
 #define NEGF_SCHEDULE_FUSED 2
 /* NEGF_TUNE_NN_GEMM: the tensor-core path of negf_nn_gemm: 0 (default) or
  * NEGF_NN_GEMM_TCGEN05, the 5th-generation tensor cores (tcgen05.mma with
- * the accumulator in tensor memory), or NEGF_NN_GEMM_MMA_SYNC, warp-level
- * mma.sync tiles.  Both compute the same BF16 x BF16 -> FP32 products; the
- * summation order inside a K-16 step may differ. */
+ * the accumulator in tensor memory) fed by the Tensor Memory Accelerator
+ * where the operands allow it (16-byte aligned base and leading dimension,
+ * non-overlapping batches), else by register-staged loads;
+ * NEGF_NN_GEMM_TCGEN05_STAGED, the register-staged tcgen05 kernel only; or
+ * NEGF_NN_GEMM_MMA_SYNC, warp-level mma.sync tiles.  All compute the same
+ * BF16 x BF16 -> FP32 products; the summation order inside a K-16 step may
+ * differ. */
 #define NEGF_NN_GEMM_TCGEN05 1
 #define NEGF_NN_GEMM_MMA_SYNC 2
+#define NEGF_NN_GEMM_TCGEN05_STAGED 3
 int negf_set_tuning(int key, int value);
 /* Enable CUDA-event timing of negf_compute_charge (off by default). */
 int negf_set_timing(int enable);

@@ -7,7 +7,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("path", [1, 2])  # tcgen05, mma.sync
+@pytest.mark.parametrize("path", [1, 2, 3])  # tcgen05 (TMA where possible), mma.sync, tcgen05 register-staged
 @pytest.mark.parametrize("at,bt", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("M,N,K,batch", [(130, 70, 45, 3), (1, 128, 300, 1), (256, 256, 4, 2), (64, 256, 257, 1),
                                          (200, 136, 160, 2), (128, 128, 2048, 1), (384, 256, 512, 2)])
