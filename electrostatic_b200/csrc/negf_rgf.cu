@@ -154,6 +154,15 @@ __device__ cd sigma_contact(cd E, double Uc, double beta, const TubeDev& T) {
     return cscale(T.gamma * T.gamma, g);
 }
 
+// Accumulator of the per-site contributions before the 32-lane sum: the
+// chains' precision when NEGF_FP32_LANE_SUMS is set (FP32 chains then sum
+// their lanes in FP32, half the shuffles), else FP64 for every chain.
+#ifndef NEGF_FP32_LANE_SUMS
+#define NEGF_FP32_LANE_SUMS 1
+#endif
+template <typename R>
+using AccOf = typename std::conditional<(NEGF_FP32_LANE_SUMS != 0) || (sizeof(R) == 8), R, double>::type;
+
 // Butterfly reduce-scatter of K per-lane values over the 32 lanes: returns
 // the sum over lanes of element j = lane >> (5 - log2 K).  Fixed order, in
 // the chains' precision (FP32 chains sum their 32 lanes in FP32; the rows
@@ -610,7 +619,7 @@ __device__ __forceinline__ void seg_fwd(const Chain<R>& c, int n0, const CkVals<
 
 template <typename R, bool RA, bool EDGE>
 __device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[kSeg], SegWork<R>& w,
-                                        R (&acc)[kSeg]) {
+                                        AccOf<R> (&acc)[kSeg]) {
     constexpr int K = kSeg;
     const int N = c.N;
     R Rr = w.Rr, Ri = w.Ri, Sr = 1, Si = 0, rh = w.rh;
@@ -628,7 +637,7 @@ __device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[
                 const R tr = fma(w.qr[j], Sr, -w.qi[j] * Si), ti = fma(w.qr[j], Si, w.qi[j] * Sr);
                 v = fma(w.cgr, ti, w.cgi * tr);
             }
-            acc[j] = c.valid ? v : (R)0;
+            acc[j] = c.valid ? (AccOf<R>)v : (AccOf<R>)0;
         } else {
             double v;
             // D = S Q_{n+1} - R Q_n, per site (the segment may be partial), in FP64
@@ -645,7 +654,7 @@ __device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[
                 const double ur = fma(tr, dr, ti * di), ui = fma(ti, dr, -tr * di);
                 v = fma(c.cr, ui, c.ci * ur) * inv;
             }
-            acc[j] = c.valid ? (R)v : (R)0;
+            acc[j] = c.valid ? (AccOf<R>)v : (AccOf<R>)0;
         }
         if (j > 0) {  // (R, S) at site n - 1
             R ar = c.Er - u[j], ai = c.Ei;
@@ -670,7 +679,7 @@ __device__ __forceinline__ void seg_bwd(const Chain<R>& c, int n0, const R (&u)[
 
 template <typename R, bool RA, bool EDGE, bool NEXT = false>
 __device__ __forceinline__ void segment_proj(const Chain<R>& c, int n0, const CkVals<R>& ckv, const R (&u)[kSeg],
-                                             R (&acc)[kSeg], Bnd<R>* next = nullptr) {
+                                             AccOf<R> (&acc)[kSeg], Bnd<R>* next = nullptr) {
     SegWork<R> w;
     seg_fwd<R, RA, EDGE, NEXT>(c, n0, ckv, u, w, next);
     seg_bwd<R, RA, EDGE>(c, n0, u, w, acc);
@@ -712,7 +721,7 @@ __device__ __forceinline__ void pass2_unit(const TubeDev* __restrict__ tubes, co
         CkVals<R> nxt = cur;
         if (s + 1 < su.seg1) nxt = load_ck<R, RA>(ck + (size_t)(s + 1) * CL::NC * kWarp);
         R u[K];
-        R acc[K];
+        AccOf<R> acc[K];
         const bool interior = n0 > 0 && n0 + K < N;
         if (interior) {
             const double2* u2 = reinterpret_cast<const double2*>(U + n0);  // n0 even, U 16-byte aligned
@@ -899,7 +908,8 @@ __device__ __forceinline__ void pass1_interior2(const Chain<float>& c, Proj2& p,
 template <bool RA>
 __device__ __forceinline__ void segment_pair2(const Chain<float>& c, const Chain<float>& cr,
                                               const CkVals<float>& vf, const CkVals<float>& vb,
-                                              const F2 (&mu)[kSeg], float (&accf)[kSeg], float (&accr)[kSeg],
+                                              const F2 (&mu)[kSeg], AccOf<float> (&accf)[kSeg],
+                                              AccOf<float> (&accr)[kSeg],
                                               Bnd<float>& nf, Bnd<float>& nb) {
     constexpr int K = kSeg;
     const F2 Er = f2b(c.Er), Ei = f2b(c.Ei), mEi = f2b(-c.Ei);
@@ -1110,7 +1120,7 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
     if (nseg & 1) {
         const int n0 = A * K;
         const CkVals<R> v{fw.yr, fw.yi, fw.lam, bw.yr, bw.yi, bw.lam};
-        R acc[K];
+        AccOf<R> acc[K];
         R u[K];
         if (nseg == 1) {
             load_seg_edge(U, 0, N, u);
@@ -1160,11 +1170,11 @@ __device__ __forceinline__ void fused_chain(const TubeDev* __restrict__ tubes, c
             yn = rec(sb - 1);
         }
         prefetch_rec(k + 2);
-        R accf[K], accb[K];
+        AccOf<R> accf[K], accb[K];
         if (!last) {
             const CkVals<R> vf{fw.yr, fw.yi, fw.lam, x.yr, x.yi, x.lam};
             const CkVals<R> vb{bw.yr, bw.yi, bw.lam, y.yr, y.yi, y.lam};
-            R accr[K];
+            AccOf<R> accr[K];
             if constexpr (std::is_same<R, float>::value) {
                 F2 mu[K];
                 load_seg_pair(U, nf, nb, mu);
