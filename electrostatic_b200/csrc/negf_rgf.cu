@@ -154,11 +154,13 @@ __device__ cd sigma_contact(cd E, double Uc, double beta, const TubeDev& T) {
     return cscale(T.gamma * T.gamma, g);
 }
 
-// Accumulator of the per-site contributions before the 32-lane sum: the
-// chains' precision when NEGF_FP32_LANE_SUMS is set (FP32 chains then sum
-// their lanes in FP32, half the shuffles), else FP64 for every chain.
+// Accumulator of the per-site contributions before the 32-lane sum: FP64 for
+// every chain (default), or the chains' precision when NEGF_FP32_LANE_SUMS is
+// set (FP32 chains then sum their lanes in FP32: half the shuffles, about 5%
+// faster, but at a biased self-consistent state of the 16-tube batch the
+// mixed charge moved from 1.65e-5 to 2.6e-5 of the FP64 one).
 #ifndef NEGF_FP32_LANE_SUMS
-#define NEGF_FP32_LANE_SUMS 1
+#define NEGF_FP32_LANE_SUMS 0
 #endif
 template <typename R>
 using AccOf = typename std::conditional<(NEGF_FP32_LANE_SUMS != 0) || (sizeof(R) == 8), R, double>::type;

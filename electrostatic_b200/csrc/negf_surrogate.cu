@@ -549,8 +549,8 @@ __global__ void __launch_bounds__(TC_NT) gemm_tc_kernel(int M, int N, int K, con
 //   (one K each) of 128 bytes; 8-row K groups 1024 bytes apart (SBO), the two
 //   64-wide MN halves 8 KB apart (LBO); a K-16 step advances 2048 bytes.
 // Descriptor layout type 2 = 128-byte swizzle (bits [61,64)).
-constexpr int TMA_STAGES = 4;
-constexpr int TMA_SMEM = TMA_STAGES * 2 * TC_TILE_BYTES + 1024 + 128;  // ring + alignment slack + barriers
+// ring of ST stages + alignment slack + barriers; 4 stages for long K, 2 (three CTAs per SM) for K <= 128
+constexpr int tma_smem(int st) { return st * 2 * TC_TILE_BYTES + 1024 + 128; }
 
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
@@ -565,7 +565,7 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-template <bool AK, bool BKC>
+template <bool AK, bool BKC, int TMA_STAGES>
 __global__ void __launch_bounds__(TC_NT) gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                          const __grid_constant__ CUtensorMap tmB, int M, int N,
                                                          int K, float* __restrict__ C, int ldc, long long sC,
@@ -869,8 +869,8 @@ static bool make_map(CUtensorMap* m, const __nv_bfloat16* base, long long inner,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
-template <bool AK, bool BKC>
-static cudaError_t launch_tma(int M, int N, int K, int batch, const __nv_bfloat16* a, int lda, long long sA,
+template <bool AK, bool BKC, int ST>
+static cudaError_t launch_tma_st(int M, int N, int K, int batch, const __nv_bfloat16* a, int lda, long long sA,
                               const __nv_bfloat16* b, int ldb, long long sB, float* out, int ldo, long long so,
                               __nv_bfloat16* cb, int accumulate, int splits, int kchunk, dim3 grid, cudaStream_t s) {
     CUtensorMap ta, tb;
@@ -880,15 +880,22 @@ static cudaError_t launch_tma(int M, int N, int K, int batch, const __nv_bfloat1
     if (!make_map(&tb, b, BKC ? K : N, BKC ? N : K, ldb, sB, batch, BKC, &bb)) return cudaErrorNotSupported;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(gemm_tma_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
-        cudaFuncSetAttribute(gemm_tma_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
-        cudaFuncSetAttribute(gemm_tma_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
-        cudaFuncSetAttribute(gemm_tma_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TMA_SMEM);
+        cudaFuncSetAttribute(gemm_tma_kernel<AK, BKC, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem(ST));
         attr = true;
     }
-    gemm_tma_kernel<AK, BKC><<<grid, TC_NT, TMA_SMEM, s>>>(ta, tb, M, N, K, out, ldo, so, cb, accumulate, splits,
-                                                          kchunk, ab, bb);
+    gemm_tma_kernel<AK, BKC, ST><<<grid, TC_NT, tma_smem(ST), s>>>(ta, tb, M, N, K, out, ldo, so, cb, accumulate,
+                                                                  splits, kchunk, ab, bb);
     return cudaGetLastError();
+}
+template <bool AK, bool BKC>
+static cudaError_t launch_tma(int M, int N, int K, int batch, const __nv_bfloat16* a, int lda, long long sA,
+                              const __nv_bfloat16* b, int ldb, long long sB, float* out, int ldo, long long so,
+                              __nv_bfloat16* cb, int accumulate, int splits, int kchunk, dim3 grid, cudaStream_t s) {
+    if (std::min(K, kchunk) <= 2 * TC_BK)
+        return launch_tma_st<AK, BKC, 2>(M, N, K, batch, a, lda, sA, b, ldb, sB, out, ldo, so, cb, accumulate, splits,
+                                         kchunk, grid, s);
+    return launch_tma_st<AK, BKC, 4>(M, N, K, batch, a, lda, sA, b, ldb, sB, out, ldo, so, cb, accumulate, splits,
+                                     kchunk, grid, s);
 }
 
 cudaError_t nn_gemm(int at, int bt, int M, int N, int K, int batch, const void* A, int lda, long long sA,
