@@ -1525,8 +1525,10 @@ __global__ void selftest_kernel(int which, int n, const double* __restrict__ in,
 // Q[q_off + n] = sum_w partial[row_base + w N + n] - rho0[n].
 // Block = 32 sites x kRowGroups row groups; each thread sums rows
 // g, g + kRowGroups, ... with Kahan compensation, then the row groups are
-// combined in a fixed order (deterministic).
-constexpr int kRowGroups = 8;
+// combined in a fixed order (deterministic).  32 row groups: a 4000-site tube
+// gives 125 blocks of 32 warps, enough loads in flight to stream the rows
+// at HBM rate.
+constexpr int kRowGroups = 32;
 __global__ void __launch_bounds__(32 * kRowGroups) reduce_kernel(const ReduceTube* __restrict__ rts,
                                                                  const double* __restrict__ partial,
                                                                  double* __restrict__ Q, const int* __restrict__ skip) {
