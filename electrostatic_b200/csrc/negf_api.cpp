@@ -1906,6 +1906,14 @@ int negf_affine_potential_masked(const double* K, const double* U0, const double
     return NEGF_OK;
 }
 
+int negf_affine_potential_toeplitz(const double* tab, int ntab, const int* idx, const double* U0, const double* Q,
+                                   double* U, int n, const int* d_skip, void* stream) {
+    if (!tab || ntab <= 0 || !idx || !U0 || !Q || !U || n <= 0)
+        return fail(NEGF_ERR_ARG, "bad affine-potential arguments");
+    NEGF_CUDA(negf::affine_toeplitz(tab, ntab, idx, U0, Q, U, n, (cudaStream_t)stream, d_skip));
+    return NEGF_OK;
+}
+
 // ------------------------------------------------------------------ surrogate-model kernels
 int negf_nn_gemm(int a_trans, int b_trans, int M, int N, int K, int batch, const void* A, int lda, long long sA,
                  const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* C_bf16, int accumulate,

@@ -242,7 +242,52 @@ __global__ void affine_kernel(const double* __restrict__ K, const double* __rest
     if (lane == 0) U[row] = U0[row] + acc;
 }
 
+// U[i] = U0[i] + sum_j tab[|idx[i] - idx[j]|] Q[j]: the same operator for a
+// kernel that depends on the lattice distance only (a ring lattice: zigzag
+// tubes), read from a table instead of an n x n matrix.  One warp per row;
+// the block stages idx and Q in shared memory in chunks of 1024 sites, and
+// consecutive sites give consecutive table entries (coalesced gathers).
+constexpr int kToeChunk = 1024;
+__global__ void __launch_bounds__(256) toeplitz_kernel(const double* __restrict__ tab, int ntab,
+                                                       const int* __restrict__ idx, const double* __restrict__ U0,
+                                                       const double* __restrict__ Q, double* __restrict__ U, int n,
+                                                       const int* skip) {
+    if (skip && *skip) return;
+    __shared__ double sq[kToeChunk];
+    __shared__ int si[kToeChunk];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int row = blockIdx.x * (blockDim.x >> 5) + wib;
+    const int ir = row < n ? idx[row] : 0;
+    double acc = 0.0;
+    for (int c0 = 0; c0 < n; c0 += kToeChunk) {
+        const int cn = min(kToeChunk, n - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cn; t += blockDim.x) {
+            sq[t] = Q[c0 + t];
+            si[t] = idx[c0 + t];
+        }
+        __syncthreads();
+        if (row < n) {
+            for (int t = lane; t < cn; t += 32) {
+                int d = ir - si[t];
+                d = d < 0 ? -d : d;
+                acc = fma(d < ntab ? __ldg(tab + d) : 0.0, sq[t], acc);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (row < n && lane == 0) U[row] = U0[row] + acc;
+}
+
 }  // namespace
+
+cudaError_t affine_toeplitz(const double* tab, int ntab, const int* idx, const double* U0, const double* Q, double* U,
+                            int n, cudaStream_t s, const int* skip) {
+    if (n <= 0) return cudaSuccess;
+    toeplitz_kernel<<<(n + 7) / 8, 256, 0, s>>>(tab, ntab, idx, U0, Q, U, n, skip);
+    return cudaGetLastError();
+}
 
 cudaError_t broyden_norm(const BroydenDev& b, const double* n_out, cudaStream_t s, const int* flags) {
     norm_kernel<<<b.nblocks, kThreads, 0, s>>>(b, n_out, flags);

@@ -221,5 +221,7 @@ cudaError_t set_int(int* p, int v, cudaStream_t s);
 cudaError_t broyden_set(double* p, double v, int n, cudaStream_t s);
 cudaError_t affine_potential(const double* K, const double* U0, const double* Q, double* U, int n, cudaStream_t s,
                              const int* skip = nullptr);
+cudaError_t affine_toeplitz(const double* tab, int ntab, const int* idx, const double* U0, const double* Q, double* U,
+                            int n, cudaStream_t s, const int* skip = nullptr);
 
 }  // namespace negf

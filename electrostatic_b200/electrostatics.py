@@ -153,6 +153,19 @@ class GateAllAround:
     def potential(self, Q, Vg):
         return self.external(Vg) - self.K @ np.asarray(Q, dtype=np.float64)
 
+    def device_toeplitz(self, device="cuda"):
+        """(tab_dev, idx_dev) for negf_affine_potential_toeplitz when the rings
+        sit on a lattice (zigzag tubes): Kd[i][j] = tab[|idx[i] - idx[j]|] with
+        Kd = -K; None otherwise."""
+        if self._idx is None:
+            return None
+        import torch
+        if getattr(self, "_toe", None) is None or str(self._toe[0].device) != str(torch.device(device)):
+            idx = torch.tensor(self._idx - self._idx.min(), dtype=torch.int32, device=device)
+            tab = torch.tensor(-self._table, dtype=torch.float64, device=device)
+            self._toe = (tab, idx)
+        return self._toe
+
     def device_operator(self, Vg, device="cuda"):
         """(K_dev, U0_dev) for negf_affine_potential: U = U0 + Kd Q with Kd = -K
         (Kd is built once on the device and reused)."""

@@ -599,6 +599,13 @@ class ChargePlan:
             pass
 
 
+def affine_potential_toeplitz(tab_dev, idx_dev, U0_dev, Q_dev, U_dev, n, skip, stream=None):
+    """U = U0 + K Q with K[i][j] = tab[|idx[i] - idx[j]|] (negf_affine_potential_toeplitz)."""
+    check(_lib.load().negf_affine_potential_toeplitz(_ptr(tab_dev), int(tab_dev.numel()), _ptr(idx_dev), _ptr(U0_dev),
+                                                     _ptr(Q_dev), _ptr(U_dev), int(n), _ptr(skip), _stream(stream)),
+          "negf_affine_potential_toeplitz")
+
+
 def affine_potential_masked(K_dev, U0_dev, Q_dev, U_dev, n, skip, stream=None):
     check(_lib.load().negf_affine_potential_masked(_ptr(K_dev), _ptr(U0_dev), _ptr(Q_dev), _ptr(U_dev), int(n),
                                                    _ptr(skip), _stream(stream)), "negf_affine_potential_masked")

@@ -130,7 +130,7 @@ class BatchSCF:
                  initial_charge=0.0, use_graph=True, iters_per_graph=8, autotune=True, switch_norm=None,
                  segments=False):
         import torch
-        from .negf import Broyden, ChargePlan, affine_potential_masked
+        from .negf import Broyden, ChargePlan, affine_potential_masked, affine_potential_toeplitz
 
         dev = torch.device("cuda")
         self.tubes, self.electros = list(tubes), list(electros)
@@ -151,19 +151,29 @@ class BatchSCF:
             for e in electros:
                 Kd, U0 = e.device_operator(0.0)
                 ops.append((Kd, U0.clone()))
+            # lattice-distance kernels (every zigzag tube of the gate-all-around stand-in) are
+            # applied from their table instead of the n x n matrix
+            toes = [e.device_toeplitz() if hasattr(e, "device_toeplitz") else None for e in electros]
+
+            def potential(i, q_ptr, u_ptr, skip_ptr, s):
+                Kd, U0 = ops[i]
+                if toes[i] is not None:
+                    affine_potential_toeplitz(toes[i][0], toes[i][1], U0, q_ptr, u_ptr, self.Ns[i], skip_ptr, stream=s)
+                else:
+                    affine_potential_masked(Kd, U0, q_ptr, u_ptr, self.Ns[i], skip_ptr, stream=s)
             self.U_ptrs = U_ptrs = [t.potential_device_ptr() for t in tubes]
             self.flags = flags = torch.zeros(8, dtype=torch.int32, device=dev)
             skip = flags.data_ptr() + 3 * 4
             self.switch = switch = switch_norm is not None and switch_norm > 0
             # the initial potential (paths do not depend on it; contact potentials are read on the device)
-            for (Kd, U0), o, N, Up in zip(ops, self.offs, self.Ns, U_ptrs):
-                affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, None, stream=stream)
+            for i, (o, Up) in enumerate(zip(self.offs, U_ptrs)):
+                potential(i, nin + 8 * int(o), Up, None, stream)
             self.plan = plan = ChargePlan(tubes, Q, autotune=autotune)
             self.plan64 = plan64 = ChargePlan(tubes, Q, autotune=autotune, fp64=True) if switch else None
 
             def body(s):
-                for (Kd, U0), o, N, Up in zip(ops, self.offs, self.Ns, U_ptrs):
-                    affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip, stream=s)
+                for i, (o, Up) in enumerate(zip(self.offs, U_ptrs)):
+                    potential(i, nin + 8 * int(o), Up, skip, s)
                 if switch:
                     plan.launch(skip=flags.data_ptr() + 5 * 4, stream=s)
                     plan64.launch(skip=flags.data_ptr() + 6 * 4, stream=s)

@@ -474,6 +474,13 @@ int negf_affine_potential_masked(const double* K, const double* U0, const double
                                  const int* d_skip, void* stream);
 int negf_affine_potential(const double* d_K, const double* d_U0, const double* d_Q, double* d_U, int n,
                           void* stream);
+/* The same operator when K depends on the lattice distance only
+ * (K[i][j] = tab[|idx[i] - idx[j]|], the sites on an integer lattice idx, as
+ * the rings of a zigzag tube are): d_U[i] = d_U0[i] + sum_j tab[|idx[i] -
+ * idx[j]|] d_Q[j], entries at distances >= ntab read as 0 (device pointers;
+ * no n x n matrix is read). */
+int negf_affine_potential_toeplitz(const double* d_tab, int ntab, const int* d_idx, const double* d_U0,
+                                   const double* d_Q, double* d_U, int n, const int* d_skip, void* stream);
 
 /* Write_Data (NEGF_Common.cpp:1407-1418, 3043-3112, 4221-4254):
  * <prefix>_Qout.dat, <prefix>_norm.dat (axial position [nm], value; one

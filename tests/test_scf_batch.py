@@ -268,3 +268,22 @@ def test_batch_scf_precision_switch_matches_fp64(oracle):
     a, b = r_sw.steps[0], r_64.steps[0]
     assert 0 < a.lowprec_iterations < a.iterations
     assert np.max(np.abs(a.Q - b.Q)) < 1e-5
+
+
+def test_affine_potential_toeplitz_equals_dense():
+    """negf_affine_potential_toeplitz (the kernel read from its lattice-distance
+    table) equals the dense n x n operator of the same gate-all-around tube."""
+    import torch
+    from electrostatic_b200.negf import affine_potential_masked, affine_potential_toeplitz
+    tubes, electros, _ = _batch(cells=(10, 170, 6))
+    for t, e in zip(tubes, electros):
+        N = t.num_field_sites
+        Kd, U0 = e.device_operator(0.2)
+        tab, idx = e.device_toeplitz()
+        q = torch.randn(N, dtype=torch.float64, device="cuda", generator=torch.Generator(device="cuda").manual_seed(N))
+        Ua = torch.empty(N, dtype=torch.float64, device="cuda")
+        Ub = torch.empty(N, dtype=torch.float64, device="cuda")
+        affine_potential_masked(Kd, U0, q, Ua, N, None)
+        affine_potential_toeplitz(tab, idx, U0, q, Ub, N, None)
+        torch.cuda.synchronize()
+        assert float((Ua - Ub).abs().max()) <= 1e-12 * float(Ua.abs().max())
