@@ -275,7 +275,7 @@ def test_affine_potential_toeplitz_equals_dense():
     table) equals the dense n x n operator of the same gate-all-around tube."""
     import torch
     from electrostatic_b200.negf import affine_potential_masked, affine_potential_toeplitz
-    tubes, electros, _ = _batch(cells=(10, 170, 6))
+    tubes, electros, _ = _batch(cells=(10, 300, 6))  # 1200 sites: two staged chunks
     for t, e in zip(tubes, electros):
         N = t.num_field_sites
         Kd, U0 = e.device_operator(0.2)
