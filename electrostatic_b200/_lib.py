@@ -38,7 +38,8 @@ EXPORTED = [
     "negf_charge_plan_create", "negf_charge_plan_launch", "negf_charge_plan_info", "negf_charge_plan_destroy",
     "negf_broyden_step_device_switch", "negf_rs_compute_charge", "negf_nn_gemm", "negf_nn_gelu_fwd",
     "negf_nn_gelu_bwd", "negf_nn_colsum", "negf_nn_cast_bf16", "negf_nn_adam", "negf_nn_rowdot", "negf_nn_outer",
-    "negf_nn_mse", "negf_affine_potential_toeplitz",
+    "negf_nn_mse", "negf_affine_potential_toeplitz", "negf_potential_batch_create", "negf_potential_batch_launch",
+    "negf_potential_batch_destroy",
 ]
 
 
@@ -180,6 +181,10 @@ def load():
         "negf_nn_mse": [C.c_longlong, vp, vp, vp, vp, vp],
         "negf_affine_potential_masked": [vp, vp, vp, vp, C.c_int, vp, vp],
         "negf_affine_potential_toeplitz": [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp],
+        "negf_potential_batch_create": [C.POINTER(vp), ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                        ip, C.POINTER(vp)],
+        "negf_potential_batch_launch": [vp, vp, vp],
+        "negf_potential_batch_destroy": [vp],
         "negf_charge_plan_create": [C.POINTER(vp), C.c_int, vp, C.c_int, C.POINTER(vp)],
         "negf_charge_plan_launch": [vp, vp, vp],
         "negf_charge_plan_info": [vp, ip, ip, dp, C.POINTER(C.c_longlong)],

@@ -1914,6 +1914,50 @@ int negf_affine_potential_toeplitz(const double* tab, int ntab, const int* idx, 
     return NEGF_OK;
 }
 
+struct negf_potential_batch {
+    negf::ToeplitzOp* d_ops = nullptr;
+    int2* d_blocks = nullptr;
+    int num_blocks = 0;
+    ~negf_potential_batch() {
+        if (d_ops) cudaFree(d_ops);
+        if (d_blocks) cudaFree(d_blocks);
+    }
+};
+
+int negf_potential_batch_create(int ntubes, const double* const* d_tab, const int* ntab, const int* const* d_idx,
+                                const double* const* d_U0, const double* const* d_Q, double* const* d_U, const int* n,
+                                negf_potential_batch** out) {
+    if (!out || ntubes <= 0 || !d_tab || !ntab || !d_idx || !d_U0 || !d_Q || !d_U || !n)
+        return fail(NEGF_ERR_ARG, "bad potential-batch arguments");
+    std::vector<negf::ToeplitzOp> ops(ntubes);
+    std::vector<int2> blocks;
+    for (int t = 0; t < ntubes; ++t) {
+        if (!d_tab[t] || ntab[t] <= 0 || !d_idx[t] || !d_U0[t] || !d_Q[t] || !d_U[t] || n[t] <= 0)
+            return fail(NEGF_ERR_ARG, "bad potential-batch entry " + std::to_string(t));
+        ops[t] = {d_tab[t], d_idx[t], d_U0[t], d_Q[t], d_U[t], ntab[t], n[t]};
+        for (int r = 0; r < n[t]; r += 8) blocks.push_back(make_int2(t, r));
+    }
+    std::unique_ptr<negf_potential_batch> b(new negf_potential_batch());
+    NEGF_CUDA(cudaMalloc(&b->d_ops, sizeof(negf::ToeplitzOp) * ops.size()));
+    NEGF_CUDA(cudaMalloc(&b->d_blocks, sizeof(int2) * blocks.size()));
+    NEGF_CUDA(cudaMemcpy(b->d_ops, ops.data(), sizeof(negf::ToeplitzOp) * ops.size(), cudaMemcpyHostToDevice));
+    NEGF_CUDA(cudaMemcpy(b->d_blocks, blocks.data(), sizeof(int2) * blocks.size(), cudaMemcpyHostToDevice));
+    b->num_blocks = (int)blocks.size();
+    *out = b.release();
+    return NEGF_OK;
+}
+
+int negf_potential_batch_launch(negf_potential_batch* b, const int* d_skip, void* stream) {
+    if (!b) return fail(NEGF_ERR_ARG, "null potential batch");
+    NEGF_CUDA(negf::affine_toeplitz_batch(b->d_ops, b->d_blocks, b->num_blocks, (cudaStream_t)stream, d_skip));
+    return NEGF_OK;
+}
+
+int negf_potential_batch_destroy(negf_potential_batch* b) {
+    delete b;
+    return NEGF_OK;
+}
+
 // ------------------------------------------------------------------ surrogate-model kernels
 int negf_nn_gemm(int a_trans, int b_trans, int M, int N, int K, int batch, const void* A, int lda, long long sA,
                  const void* B, int ldb, long long sB, float* C, int ldc, long long sC, void* C_bf16, int accumulate,

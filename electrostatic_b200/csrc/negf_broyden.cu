@@ -280,7 +280,50 @@ __global__ void __launch_bounds__(256) toeplitz_kernel(const double* __restrict_
     if (row < n && lane == 0) U[row] = U0[row] + acc;
 }
 
+// Batched form: every row of every tube in one launch.  Block b covers rows
+// [first, first + 8) of tube tube_of[b] (blocks never straddle tubes), so the
+// tubes' potentials are formed concurrently instead of one launch each.
+__global__ void __launch_bounds__(256) toeplitz_batch_kernel(const ToeplitzOp* __restrict__ ops,
+                                                             const int2* __restrict__ blocks, const int* skip) {
+    if (skip && *skip) return;
+    __shared__ double sq[kToeChunk];
+    __shared__ int si[kToeChunk];
+    const int2 bt = blocks[blockIdx.x];  // (tube, first row)
+    const ToeplitzOp op = ops[bt.x];
+    const int n = op.n;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int row = bt.y + wib;
+    const int ir = row < n ? op.idx[row] : 0;
+    double acc = 0.0;
+    for (int c0 = 0; c0 < n; c0 += kToeChunk) {
+        const int cn = min(kToeChunk, n - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cn; t += blockDim.x) {
+            sq[t] = op.Q[c0 + t];
+            si[t] = op.idx[c0 + t];
+        }
+        __syncthreads();
+        if (row < n) {
+            for (int t = lane; t < cn; t += 32) {
+                int d = ir - si[t];
+                d = d < 0 ? -d : d;
+                acc = fma(d < op.ntab ? __ldg(op.tab + d) : 0.0, sq[t], acc);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (row < n && lane == 0) op.U[row] = op.U0[row] + acc;
+}
+
 }  // namespace
+
+cudaError_t affine_toeplitz_batch(const ToeplitzOp* d_ops, const int2* d_blocks, int num_blocks, cudaStream_t s,
+                                  const int* skip) {
+    if (num_blocks <= 0) return cudaSuccess;
+    toeplitz_batch_kernel<<<num_blocks, 256, 0, s>>>(d_ops, d_blocks, skip);
+    return cudaGetLastError();
+}
 
 cudaError_t affine_toeplitz(const double* tab, int ntab, const int* idx, const double* U0, const double* Q, double* U,
                             int n, cudaStream_t s, const int* skip) {

@@ -223,5 +223,15 @@ cudaError_t affine_potential(const double* K, const double* U0, const double* Q,
                              const int* skip = nullptr);
 cudaError_t affine_toeplitz(const double* tab, int ntab, const int* idx, const double* U0, const double* Q, double* U,
                             int n, cudaStream_t s, const int* skip = nullptr);
+struct ToeplitzOp {  // one tube of a batched lattice-distance potential update
+    const double* tab;
+    const int* idx;
+    const double* U0;
+    const double* Q;
+    double* U;
+    int ntab, n;
+};
+cudaError_t affine_toeplitz_batch(const ToeplitzOp* d_ops, const int2* d_blocks, int num_blocks, cudaStream_t s,
+                                  const int* skip = nullptr);
 
 }  // namespace negf

@@ -606,6 +606,41 @@ def affine_potential_toeplitz(tab_dev, idx_dev, U0_dev, Q_dev, U_dev, n, skip, s
           "negf_affine_potential_toeplitz")
 
 
+class PotentialBatch:
+    """negf_potential_batch: the lattice-distance potential update of a batch of
+    tubes in one launch (tables, lattice indices and U0 as device tensors; Q and
+    U as device tensors or addresses, fixed at creation)."""
+
+    def __init__(self, tabs, idxs, U0s, Qs, Us, ns):
+        T = len(ns)
+
+        def arr(vals):
+            return (C.c_void_p * T)(*[_ptr(v) for v in vals])
+
+        ntab = (C.c_int * T)(*[int(t.numel()) for t in tabs])
+        nn = (C.c_int * T)(*[int(n) for n in ns])
+        h = C.c_void_p()
+        check(_lib.load().negf_potential_batch_create(T, arr(tabs), ntab, arr(idxs), arr(U0s), arr(Qs), arr(Us), nn,
+                                                      C.byref(h)), "negf_potential_batch_create")
+        self._h = h
+        self._keep = (list(tabs), list(idxs), list(U0s), list(Qs), list(Us))
+
+    def launch(self, skip=None, stream=None):
+        check(_lib.load().negf_potential_batch_launch(self._h, _ptr(skip), _stream(stream)),
+              "negf_potential_batch_launch")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().negf_potential_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def affine_potential_masked(K_dev, U0_dev, Q_dev, U_dev, n, skip, stream=None):
     check(_lib.load().negf_affine_potential_masked(_ptr(K_dev), _ptr(U0_dev), _ptr(Q_dev), _ptr(U_dev), int(n),
                                                    _ptr(skip), _stream(stream)), "negf_affine_potential_masked")

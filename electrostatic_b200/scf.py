@@ -130,7 +130,7 @@ class BatchSCF:
                  initial_charge=0.0, use_graph=True, iters_per_graph=8, autotune=True, switch_norm=None,
                  segments=False):
         import torch
-        from .negf import Broyden, ChargePlan, affine_potential_masked, affine_potential_toeplitz
+        from .negf import Broyden, ChargePlan, PotentialBatch, affine_potential_masked
 
         dev = torch.device("cuda")
         self.tubes, self.electros = list(tubes), list(electros)
@@ -147,33 +147,37 @@ class BatchSCF:
                 br.set_segments(self.offs, stream=stream)
             nin = br.input_device_ptr()
             self.n_in = device_view(nin, S)
+            self.U_ptrs = U_ptrs = [t.potential_device_ptr() for t in tubes]
             self.ops = ops = []
             for e in electros:
                 Kd, U0 = e.device_operator(0.0)
                 ops.append((Kd, U0.clone()))
             # lattice-distance kernels (every zigzag tube of the gate-all-around stand-in) are
-            # applied from their table instead of the n x n matrix
+            # applied from their tables, all tubes in one launch, instead of the n x n matrices
             toes = [e.device_toeplitz() if hasattr(e, "device_toeplitz") else None for e in electros]
+            self.potbatch = None
+            if all(t is not None for t in toes):
+                self.potbatch = PotentialBatch([t[0] for t in toes], [t[1] for t in toes], [U0 for _, U0 in ops],
+                                               [nin + 8 * int(o) for o in self.offs[:-1]], list(self.U_ptrs),
+                                               self.Ns)
 
-            def potential(i, q_ptr, u_ptr, skip_ptr, s):
-                Kd, U0 = ops[i]
-                if toes[i] is not None:
-                    affine_potential_toeplitz(toes[i][0], toes[i][1], U0, q_ptr, u_ptr, self.Ns[i], skip_ptr, stream=s)
-                else:
-                    affine_potential_masked(Kd, U0, q_ptr, u_ptr, self.Ns[i], skip_ptr, stream=s)
-            self.U_ptrs = U_ptrs = [t.potential_device_ptr() for t in tubes]
+            def potentials(skip_ptr, s):
+                if self.potbatch is not None:
+                    self.potbatch.launch(skip=skip_ptr, stream=s)
+                    return
+                for (Kd, U0), o, N, Up in zip(ops, self.offs, self.Ns, self.U_ptrs):
+                    affine_potential_masked(Kd, U0, nin + 8 * int(o), Up, N, skip_ptr, stream=s)
+
             self.flags = flags = torch.zeros(8, dtype=torch.int32, device=dev)
             skip = flags.data_ptr() + 3 * 4
             self.switch = switch = switch_norm is not None and switch_norm > 0
             # the initial potential (paths do not depend on it; contact potentials are read on the device)
-            for i, (o, Up) in enumerate(zip(self.offs, U_ptrs)):
-                potential(i, nin + 8 * int(o), Up, None, stream)
+            potentials(None, stream)
             self.plan = plan = ChargePlan(tubes, Q, autotune=autotune)
             self.plan64 = plan64 = ChargePlan(tubes, Q, autotune=autotune, fp64=True) if switch else None
 
             def body(s):
-                for i, (o, Up) in enumerate(zip(self.offs, U_ptrs)):
-                    potential(i, nin + 8 * int(o), Up, skip, s)
+                potentials(skip, s)
                 if switch:
                     plan.launch(skip=flags.data_ptr() + 5 * 4, stream=s)
                     plan64.launch(skip=flags.data_ptr() + 6 * 4, stream=s)
@@ -242,6 +246,8 @@ class BatchSCF:
     def close(self):
         self.stream.synchronize()
         self.graph = None
+        if self.potbatch is not None:
+            self.potbatch.close()
         self.plan.close()
         if self.plan64 is not None:
             self.plan64.close()

@@ -481,6 +481,17 @@ int negf_affine_potential(const double* d_K, const double* d_U0, const double* d
  * no n x n matrix is read). */
 int negf_affine_potential_toeplitz(const double* d_tab, int ntab, const int* d_idx, const double* d_U0,
                                    const double* d_Q, double* d_U, int n, const int* d_skip, void* stream);
+/* The lattice-distance update of a batch of tubes in one launch: tube t
+ * writes d_U[t][i] = d_U0[t][i] + sum_j d_tab[t][|d_idx[t][i] - d_idx[t][j]|]
+ * d_Q[t][j] for its n[t] sites (host arrays of device pointers, read once at
+ * create; the launch reads the buffers they point to, so it can be captured
+ * and replayed as the buffers change).  No counterpart in the reference. */
+typedef struct negf_potential_batch negf_potential_batch;
+int negf_potential_batch_create(int ntubes, const double* const* d_tab, const int* ntab, const int* const* d_idx,
+                                const double* const* d_U0, const double* const* d_Q, double* const* d_U, const int* n,
+                                negf_potential_batch** out);
+int negf_potential_batch_launch(negf_potential_batch* b, const int* d_skip, void* stream);
+int negf_potential_batch_destroy(negf_potential_batch* b);
 
 /* Write_Data (NEGF_Common.cpp:1407-1418, 3043-3112, 4221-4254):
  * <prefix>_Qout.dat, <prefix>_norm.dat (axial position [nm], value; one

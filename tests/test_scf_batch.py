@@ -287,3 +287,27 @@ def test_affine_potential_toeplitz_equals_dense():
         affine_potential_toeplitz(tab, idx, U0, q, Ub, N, None)
         torch.cuda.synchronize()
         assert float((Ua - Ub).abs().max()) <= 1e-12 * float(Ua.abs().max())
+
+
+def test_potential_batch_equals_dense():
+    """negf_potential_batch (every tube's lattice-distance update in one launch)
+    equals the dense operators tube by tube."""
+    import torch
+    from electrostatic_b200.negf import PotentialBatch, affine_potential_masked
+    tubes, electros, _ = _batch(cells=(10, 300, 6))
+    Ns = [t.num_field_sites for t in tubes]
+    offs = np.concatenate([[0], np.cumsum(Ns)]).astype(int)
+    q = torch.randn(int(offs[-1]), dtype=torch.float64, device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
+    Ub = torch.zeros(int(offs[-1]), dtype=torch.float64, device="cuda")
+    ops = [e.device_operator(0.1) for e in electros]
+    toes = [e.device_toeplitz() for e in electros]
+    pb = PotentialBatch([t[0] for t in toes], [t[1] for t in toes], [U0 for _, U0 in ops],
+                        [q.data_ptr() + 8 * int(o) for o in offs[:-1]], [Ub.data_ptr() + 8 * int(o) for o in offs[:-1]],
+                        Ns)
+    pb.launch()
+    for (Kd, U0), a, b in zip(ops, offs[:-1], offs[1:]):
+        Ua = torch.empty(b - a, dtype=torch.float64, device="cuda")
+        affine_potential_masked(Kd, U0, q[a:b], Ua, b - a, None)
+        torch.cuda.synchronize()
+        assert float((Ua - Ub[a:b]).abs().max()) <= 1e-12 * float(Ua.abs().max())
+    pb.close()
