@@ -181,8 +181,8 @@ def load():
         "negf_nn_mse": [C.c_longlong, vp, vp, vp, vp, vp],
         "negf_affine_potential_masked": [vp, vp, vp, vp, C.c_int, vp, vp],
         "negf_affine_potential_toeplitz": [vp, C.c_int, vp, vp, vp, vp, C.c_int, vp, vp],
-        "negf_potential_batch_create": [C.POINTER(vp), ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
-                                        ip, C.POINTER(vp)],
+        "negf_potential_batch_create": [C.c_int, C.POINTER(vp), ip, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                        C.POINTER(vp), ip, C.POINTER(vp)],
         "negf_potential_batch_launch": [vp, vp, vp],
         "negf_potential_batch_destroy": [vp],
         "negf_charge_plan_create": [C.POINTER(vp), C.c_int, vp, C.c_int, C.POINTER(vp)],
