@@ -58,6 +58,12 @@ def test_argument_errors(negf_lib):
     assert b"num_noneq_paths" in negf_lib.negf_last_error()
     lo, hi = C.c_int(), C.c_int()
     assert negf_lib.negf_shard_range(10, 3, 2, C.byref(lo), C.byref(hi)) == -1
+    # argument checks that run before any device work (through the declared ctypes signatures)
+    null1 = (C.c_void_p * 1)(None)
+    zero1 = (C.c_int * 1)(0)
+    assert negf_lib.negf_potential_batch_create(0, null1, zero1, null1, null1, null1, null1, zero1, C.byref(h)) == -1
+    assert negf_lib.negf_affine_potential_toeplitz(None, 0, None, None, None, None, 0, None, None) == -1
+    assert negf_lib.negf_broyden_set_segments(None, 2, None, None) == -1
 
 
 def test_shard_ranges_partition(negf_lib):
