@@ -39,7 +39,7 @@ EXPORTED = [
     "negf_broyden_step_device_switch", "negf_rs_compute_charge", "negf_nn_gemm", "negf_nn_gelu_fwd",
     "negf_nn_gelu_bwd", "negf_nn_colsum", "negf_nn_cast_bf16", "negf_nn_adam", "negf_nn_rowdot", "negf_nn_outer",
     "negf_nn_mse", "negf_affine_potential_toeplitz", "negf_potential_batch_create", "negf_potential_batch_launch",
-    "negf_potential_batch_destroy",
+    "negf_potential_batch_destroy", "negf_charge_plan_pieces",
 ]
 
 
@@ -189,6 +189,7 @@ def load():
         "negf_charge_plan_launch": [vp, vp, vp],
         "negf_charge_plan_info": [vp, ip, ip, dp, C.POINTER(C.c_longlong)],
         "negf_charge_plan_destroy": [vp],
+        "negf_charge_plan_pieces": [vp, ip],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -207,8 +207,9 @@ struct negf_broyden {
 struct negf_charge_plan {
     std::vector<negf_tube*> tubes;
     std::vector<int> versions;
-    DevBuf d_tubes, d_chains, d_warps, d_units, d_rts, d_partial, d_scratch, d_order;
+    DevBuf d_tubes, d_chains, d_warps, d_units, d_rts, d_partial, d_scratch, d_order, d_pieces;
     int num_warps = 0, num_units = 0, max_N = 0;
+    int pieces = 1;  // pass-1 pieces of the two-pass schedule (parallel in length)
     int n64 = 0, n32 = 0;  // fused schedule: FP64 / FP32 warps in d_order
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
@@ -675,6 +676,15 @@ int device_sm_count() {
 // sweeps run as one piece and the warps fill at least one per SM
 // sub-partition (4 per SM), else two-pass (its segment tiles spread few
 // chains over the whole GPU).
+// Parallel in length when the chains alone cannot fill the GPU: about 8
+// one-warp blocks per SM, pieces of >= 32 segments, at most 128 pieces (the
+// prefix over the pieces is sequential per chain).
+int auto_pieces(int nw, int max_N) {
+    const int target = 8 * device_sm_count();
+    const int maxp = std::min(128, std::max(1, ((max_N + negf::kSeg - 1) / negf::kSeg) / 32));
+    return nw >= target / 2 ? 1 : std::min(maxp, (target + nw - 1) / std::max(nw, 1));
+}
+
 int choose_schedule(int setting, int nw, int pieces) {
     if (pieces > 1) return negf::kScheduleTwoPass;
     if (setting == NEGF_SCHEDULE_FUSED) return negf::kScheduleFused;
@@ -815,16 +825,9 @@ int upload_and_launch(Workspace& W, const std::vector<TubePass>& passes, const s
             if (!e) NEGF_CUDA(cudaEventCreate(&e));
         NEGF_CUDA(cudaEventRecord(W.ev[0], stream));
     }
-    // parallel in length when the chains alone cannot fill the GPU: about 8
-    // one-warp blocks per SM, pieces of >= 32 segments, at most 128 pieces
-    // (the prefix over the pieces is sequential per chain)
     int pieces = G.pass1_pieces;
     if (pieces == 0 && G.schedule == NEGF_SCHEDULE_FUSED) pieces = 1;  // an explicit fused request wins
-    if (pieces == 0) {
-        const int target = 8 * device_sm_count();
-        const int maxp = std::min(128, std::max(1, ((ct.max_N + negf::kSeg - 1) / negf::kSeg) / 32));
-        pieces = nw >= target / 2 ? 1 : std::min(maxp, (target + nw - 1) / std::max(nw, 1));
-    }
+    if (pieces == 0) pieces = auto_pieces(nw, ct.max_N);
     pieces = std::max(1, pieces);
     const int schedule = choose_schedule(G.schedule, nw, pieces);
     if (schedule == negf::kScheduleFused) pieces = 1;
@@ -1479,8 +1482,9 @@ cudaError_t plan_launch(const negf_charge_plan& p, const int* skip, cudaStream_t
     const negf::FusedOrder fo{p.d_order.as<int>(), p.n64, p.n32, p.side, p.fork, p.join};
     cudaError_t e = negf::launch_rgf(p.d_tubes.as<negf::TubeDev>(), p.d_chains.as<negf::ChainRec>(),
                                      p.d_warps.as<negf::WarpRec>(), p.num_warps, p.d_units.as<negf::SegUnit>(),
-                                     p.num_units, p.d_partial.as<double>(), p.d_scratch.p, p.wpb, s, nullptr, skip, 1,
-                                     nullptr, p.schedule, &fo);
+                                     p.num_units, p.d_partial.as<double>(), p.d_scratch.p, p.wpb, s, nullptr, skip,
+                                     p.schedule == negf::kScheduleFused ? 1 : p.pieces, p.d_pieces.as<double>(),
+                                     p.schedule, &fo);
     if (e != cudaSuccess) return e;
     return negf::launch_reduce(p.d_rts.as<negf::ReduceTube>(), (int)p.tubes.size(), p.max_N,
                                p.d_partial.as<double>(), p.d_Q, s, skip);
@@ -1510,40 +1514,68 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
     p->wpb = settings().warps_per_block;
     rc = plan_tables(*p, negf::kSegsPerUnit, true);
     if (rc) return rc;
-    p->schedule = choose_schedule(settings().schedule, p->num_warps, 1);
+    {
+        // pass-1 pieces as negf_compute_charge chooses them (the setting, else the automatic rule)
+        int pc = settings().pass1_pieces;
+        if (pc == 0 && settings().schedule == NEGF_SCHEDULE_FUSED) pc = 1;
+        if (pc == 0) pc = auto_pieces(p->num_warps, p->max_N);
+        p->pieces = std::max(1, pc);
+    }
+    p->schedule = choose_schedule(settings().schedule, p->num_warps, p->pieces);
+    if (p->schedule == negf::kScheduleFused) p->pieces = 1;
+    // piece candidates of the autotuner: only when the chains cannot fill the GPU
+    std::vector<int> piece_cands = {1};
+    if ((flags & NEGF_PLAN_AUTOTUNE) && p->num_warps < 4 * device_sm_count()) {
+        const int maxp = std::min(128, std::max(1, ((p->max_N + negf::kSeg - 1) / negf::kSeg) / 32));
+        for (int q : {2, 4, 8, auto_pieces(p->num_warps, p->max_N)})
+            if (q > 1 && q <= maxp && std::find(piece_cands.begin(), piece_cands.end(), q) == piece_cands.end())
+                piece_cands.push_back(q);
+    }
+    {
+        int maxpc = p->pieces;
+        for (int q : piece_cands) maxpc = std::max(maxpc, q);
+        if (maxpc > 1)
+            NEGF_CUDA(p->d_pieces.reserve(sizeof(double) * (size_t)std::max(1, p->num_warps) * maxpc * 24 *
+                                          negf::kWarp));
+    }
     if (flags & NEGF_PLAN_AUTOTUNE) {
         // time the fused schedule (wpb 0 below) and every two-pass shape
-        // (segments per pass-2 unit x pass-2 warps per block) on this batch
+        // (segments per pass-2 unit x pass-2 warps per block x pass-1 pieces) on this batch
         cudaEvent_t e0, e1;
         NEGF_CUDA(cudaEventCreate(&e0));
         NEGF_CUDA(cudaEventCreate(&e1));
         double best = 1e300;
-        int best_spu = negf::kSegsPerUnit, best_wpb = p->wpb;
+        int best_spu = negf::kSegsPerUnit, best_wpb = p->wpb, best_pc = 1;
         for (int spu : {16, 32, 64}) {
             rc = plan_tables(*p, spu, false);
             if (rc) break;
             for (int wpb : {0, 1, 2, 4}) {
                 if (wpb == 0 && spu != 16) continue;  // the fused schedule has no segment units
-                p->wpb = wpb == 0 ? 4 : wpb;
-                p->schedule = wpb == 0 ? negf::kScheduleFused : negf::kScheduleTwoPass;
-                cudaError_t e = plan_launch(*p, nullptr, 0);
-                for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
-                    if (r == 1) e = cudaEventRecord(e0, 0);
-                    if (e == cudaSuccess) e = plan_launch(*p, nullptr, 0);
-                }
-                if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
-                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-                float ms = 0.f;
-                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-                if (e != cudaSuccess) {
-                    cudaEventDestroy(e0);
-                    cudaEventDestroy(e1);
-                    return fail(NEGF_ERR_CUDA, cudaGetErrorString(e));
-                }
-                if (ms / 2 < best) {
-                    best = ms / 2;
-                    best_spu = spu;
-                    best_wpb = wpb;
+                for (int pc : piece_cands) {
+                    if (wpb == 0 && pc != 1) continue;  // the fused schedule runs whole chains
+                    p->wpb = wpb == 0 ? 4 : wpb;
+                    p->schedule = wpb == 0 ? negf::kScheduleFused : negf::kScheduleTwoPass;
+                    p->pieces = pc;
+                    cudaError_t e = plan_launch(*p, nullptr, 0);
+                    for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+                        if (r == 1) e = cudaEventRecord(e0, 0);
+                        if (e == cudaSuccess) e = plan_launch(*p, nullptr, 0);
+                    }
+                    if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+                    if (e != cudaSuccess) {
+                        cudaEventDestroy(e0);
+                        cudaEventDestroy(e1);
+                        return fail(NEGF_ERR_CUDA, cudaGetErrorString(e));
+                    }
+                    if (ms / 2 < best) {
+                        best = ms / 2;
+                        best_spu = spu;
+                        best_wpb = wpb;
+                        best_pc = pc;
+                    }
                 }
             }
         }
@@ -1552,6 +1584,7 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
         if (rc) return rc;
         p->schedule = best_wpb == 0 ? negf::kScheduleFused : negf::kScheduleTwoPass;
         p->wpb = best_wpb == 0 ? 4 : best_wpb;
+        p->pieces = best_pc;
         p->tuned_ms = best;
         rc = plan_tables(*p, best_spu, false);
         if (rc) return rc;
@@ -1567,6 +1600,12 @@ int negf_charge_plan_launch(negf_charge_plan* p, const int* d_skip, void* stream
             return fail(NEGF_ERR_STATE, "charge plan is stale: the energy paths of tube " + std::to_string(i) +
                                             " changed after the plan was made");
     NEGF_CUDA(plan_launch(*p, d_skip, (cudaStream_t)stream));
+    return NEGF_OK;
+}
+
+int negf_charge_plan_pieces(const negf_charge_plan* p, int* pieces) {
+    if (!p || !pieces) return fail(NEGF_ERR_ARG, "null argument");
+    *pieces = p->schedule == negf::kScheduleFused ? 1 : p->pieces;
     return NEGF_OK;
 }
 

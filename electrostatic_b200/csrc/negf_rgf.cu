@@ -1291,7 +1291,9 @@ __device__ __forceinline__ void normalise(M2& m, int& e) {
 __global__ void __launch_bounds__(32) rgf_piece_transfer_kernel(const TubeDev* __restrict__ tubes,
                                                                 const ChainRec* __restrict__ chains,
                                                                 const WarpRec* __restrict__ warps, int num_warps,
-                                                                int pieces, double* __restrict__ out) {
+                                                                int pieces, double* __restrict__ out,
+                                                                const int* __restrict__ skip) {
+    if (skip && *skip) return;
     constexpr int K = kSeg;
     const int lane = threadIdx.x & 31;
     const int w = blockIdx.x / pieces, p = blockIdx.x % pieces;
@@ -1398,7 +1400,9 @@ __global__ void __launch_bounds__(32) rgf_piece_prefix_kernel(const TubeDev* __r
                                                               const ChainRec* __restrict__ chains,
                                                               const WarpRec* __restrict__ warps, int num_warps,
                                                               int pieces, const double* __restrict__ tm,
-                                                              double* __restrict__ states) {
+                                                              double* __restrict__ states,
+                                                              const int* __restrict__ skip) {
+    if (skip && *skip) return;
     const int lane = threadIdx.x & 31;
     const int w = blockIdx.x;
     if (w >= num_warps) return;
@@ -1797,11 +1801,11 @@ cudaError_t launch_rgf(const TubeDev* d_tubes, const ChainRec* d_chains, const W
         double* tm = d_piece_work;
         states = d_piece_work + (size_t)num_warps * pieces * 18 * kWarp;
         rgf_piece_transfer_kernel<<<num_warps * pieces, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps,
-                                                                            pieces, tm);
+                                                                            pieces, tm, skip);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         rgf_piece_prefix_kernel<<<num_warps, kWarp, 0, stream>>>(d_tubes, d_chains, d_warps, num_warps, pieces, tm,
-                                                                 states);
+                                                                 states, skip);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     } else {

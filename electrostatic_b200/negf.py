@@ -585,7 +585,10 @@ class ChargePlan:
         w, s, ms, up = C.c_int(), C.c_int(), C.c_double(), C.c_longlong()
         check(_lib.load().negf_charge_plan_info(self._h, C.byref(w), C.byref(s), C.byref(ms), C.byref(up)),
               "negf_charge_plan_info")
-        return dict(pass2_warps_per_block=w.value, segs_per_unit=s.value, tuned_ms=ms.value, updates=up.value)
+        pc = C.c_int()
+        check(_lib.load().negf_charge_plan_pieces(self._h, C.byref(pc)), "negf_charge_plan_pieces")
+        return dict(pass2_warps_per_block=w.value, segs_per_unit=s.value, tuned_ms=ms.value, updates=up.value,
+                    pieces=pc.value)
 
     def close(self):
         if getattr(self, "_h", None):

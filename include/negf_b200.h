@@ -359,9 +359,12 @@ int negf_write_integrand(negf_tube* t, const char* path, int count, const double
  * Nanostructure.cpp:500-504).  d_Q: device output of sum N doubles (tube
  * order).  With NEGF_PLAN_AUTOTUNE the fused (warp per chain) schedule and
  * every two-pass (segment tile) schedule -- segments per unit 16/32/64 x
- * pass-2 warps per block 1/2/4 -- are timed on the batch and the fastest is
- * kept (results agree to rounding; bitwise within the two-pass shapes).
- * Without it the schedule follows NEGF_TUNE_SCHEDULE's automatic rule.
+ * pass-2 warps per block 1/2/4, and, when the chains fill fewer than 4 warps
+ * per SM, pass-1 pieces 1/2/4/8/automatic (parallel in length) -- are timed
+ * on the batch and the fastest is kept (results agree to rounding; bitwise
+ * within the two-pass shapes of one piece count).  Without it the schedule
+ * and the pieces follow NEGF_TUNE_SCHEDULE's and NEGF_TUNE_PASS1_PIECES's
+ * rules, as in negf_compute_charge.
  * negf_charge_plan_info's *pass2_warps_per_block is 0 when the fused
  * schedule was chosen.  A plan is stale (NEGF_ERR_STATE at
  * launch) once a tube's energy paths change (contact mu, adaptive limits);
@@ -373,6 +376,8 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
 int negf_charge_plan_launch(negf_charge_plan* plan, const int* d_skip, void* stream);
 int negf_charge_plan_info(const negf_charge_plan* plan, int* pass2_warps_per_block, int* segs_per_unit,
                           double* tuned_ms, long long* updates);
+/* Pass-1 pieces of the plan's schedule (1 for the fused schedule). */
+int negf_charge_plan_pieces(const negf_charge_plan* plan, int* pieces);
 int negf_charge_plan_destroy(negf_charge_plan* plan);
 
 /* Broyden modified-second mixing (Transport.H:203-208):

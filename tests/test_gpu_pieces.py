@@ -55,3 +55,63 @@ def test_long_tube_automatic_pieces():
     assert st["pieces"] > 1
     Q1, _ = _with_pieces(g, 1)
     assert _rel(Qa, Q1) <= 1e-10, _rel(Qa, Q1)
+
+
+def _long_tubes():
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import site_potential
+    tubes = []
+    for k, (uc, mu) in enumerate([(3000, -0.2), (2000, -0.1)]):
+        t = CNT(type_id=(17, 0), num_unitcells=uc, num_modes=2, contact_mu=(0.0, mu), contact_T=(300.0, 300.0),
+                eq_integration_pts=(8, 8, 16), noneq_integration_pts=(24,), E_zPlus_imag=1e-3)
+        U = site_potential(t.site_positions(), 11 + k, amp=0.2, ramp=0.2)
+        t.set_potential(U, (U[0], U[-1]))
+        tubes.append(t)
+    return tubes
+
+
+def _plan_charge(tubes, P, autotune=False):
+    import torch
+    from electrostatic_b200 import _lib
+    from electrostatic_b200.negf import ChargePlan
+    L = _lib.load()
+    assert L.negf_set_tuning(4, P) == 0
+    try:
+        Q = torch.zeros(sum(t.num_field_sites for t in tubes), dtype=torch.float64, device="cuda")
+        plan = ChargePlan(tubes, Q, autotune=autotune)
+        plan.launch()
+        torch.cuda.synchronize()
+        info = plan.info()
+        skip = torch.ones(1, dtype=torch.int32, device="cuda")
+        Qs = Q.clone()
+        plan.launch(skip=skip)  # a set skip flag leaves the charge untouched
+        torch.cuda.synchronize()
+        assert torch.equal(Q, Qs)
+        plan.close()
+        return Q.cpu().numpy(), info
+    finally:
+        L.negf_set_tuning(4, 0)
+
+
+def test_plan_pieces_equal_single_sweep():
+    """Charge plans of long tubes with few energies: the automatic rule and a
+    forced piece count split the sweeps, with the charge of the single sweep."""
+    tubes = _long_tubes()
+    Q1, i1 = _plan_charge(tubes, 1)
+    assert i1["pieces"] == 1
+    Qa, ia = _plan_charge(tubes, 0)
+    assert ia["pieces"] > 1 and ia["pass2_warps_per_block"] > 0
+    assert _rel(Qa, Q1) <= 1e-10, _rel(Qa, Q1)
+    Q6, i6 = _plan_charge(tubes, 6)
+    assert i6["pieces"] == 6
+    assert _rel(Q6, Q1) <= 1e-10, _rel(Q6, Q1)
+
+
+def test_plan_autotune_considers_pieces():
+    tubes = _long_tubes()
+    Q1, _ = _plan_charge(tubes, 1)
+    Qt, it = _plan_charge(tubes, 0, autotune=True)
+    assert it["pieces"] >= 1 and it["tuned_ms"] > 0
+    if it["pass2_warps_per_block"] == 0:
+        assert it["pieces"] == 1
+    assert _rel(Qt, Q1) <= 1e-10, _rel(Qt, Q1)
