@@ -244,7 +244,7 @@ struct Workspace {
     cudaStream_t side = nullptr;                 // the FP32 warps of the fused schedule
     cudaEvent_t fork = nullptr, join = nullptr;  // around them
     // real-space pass (negf_rs_compute_charge)
-    DevBuf rsE, rsFlags, rsU0, rsUa, rsCorners, rsGL, rsRows, rsStatus;
+    DevBuf rsE, rsFlags, rsU0, rsUa, rsCorners, rsGL, rsGLn, rsRows, rsStatus;
     // cached chain table
     std::vector<long long> key_serials;
     std::vector<int> key_versions;
@@ -264,7 +264,8 @@ struct Workspace {
         if (join) cudaEventDestroy(join);
         if (side) cudaStreamDestroy(side);
         DevBuf* bufs[] = {&tubes, &chains, &warps, &rts,  &units, &partial,   &scratch, &qbuf,   &pieces,
-                          &order, &rsE,    &rsFlags, &rsU0, &rsUa, &rsCorners, &rsGL,    &rsRows, &rsStatus};
+                          &order, &rsE,    &rsFlags, &rsU0, &rsUa, &rsCorners, &rsGL,    &rsGLn,  &rsRows,
+                          &rsStatus};
         for (DevBuf* b : bufs) {
             if (b->p) cudaFree(b->p);
             b->p = nullptr;
@@ -2067,25 +2068,31 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     if (2 * m > negf::rs_max_atoms_per_block())
         return fail(NEGF_ERR_ARG, "real-space blocks hold at most " + std::to_string(negf::rs_max_atoms_per_block()) +
                                       " atoms (m <= 16)");
-    if (t->noneq) return fail(NEGF_ERR_STATE, "the real-space pass covers the equilibrium charge (contour and poles)");
     cudaStream_t s = (cudaStream_t)stream;
     const int N = t->N, K = N / 2;
     // energies: RhoEq contour and poles (coefficients as in the mode-space
-    // pass).  In mixed mode the points at least mixed_fp64_band above the
-    // real axis run in FP32; the FP64 chains go first in the launch.  Rho0
-    // (U = 0, FP64) does not depend on the potential: like the mode-space
-    // Rho0 of negf_tube_create (Compute_Rho0 once at initialisation,
+    // pass) and, for a biased tube, the real-axis points of RhoNonEq
+    // (Compute_RhoNonEq, NEGF_Common.cpp:3115-3578: b0 A^L + b1 A^R per ring,
+    // FP64).  In mixed mode the contour and pole points at least
+    // mixed_fp64_band above the real axis run in FP32; the FP64 chains go
+    // first in the launch, the real-axis points last.  Rho0 (U = 0, FP64)
+    // does not depend on the potential: like the mode-space Rho0 of
+    // negf_tube_create (Compute_Rho0 once at initialisation,
     // NEGF_Common.cpp:1300) it is computed by the first real-space call for
     // the tube and kept.
     struct RsE {
         double Er, Ei, cr, ci;
         int flags;
     };
-    std::vector<RsE> e64, e32, e0;
+    std::vector<RsE> e64, e32, eneq, e0;
     const bool mixed = t->d.precision == NEGF_PREC_MIXED;
     const int neq = pass_items(*t, false);
     for (int idx = 0; idx < neq; ++idx) {
         const Item it = pass_item(*t, false, idx);
+        if (it.kind == negf::kRealAxis) {
+            eneq.push_back({it.E.real(), it.E.imag(), it.b0, it.b1, 0});
+            continue;
+        }
         const bool fp32 = mixed && std::fabs(it.E.imag()) >= t->d.mixed_fp64_band;
         (fp32 ? e32 : e64).push_back({it.E.real(), it.E.imag(), it.c.real(), it.c.imag(), fp32 ? 1 : 0});
     }
@@ -2099,7 +2106,8 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     }
     std::vector<RsE> all(e64);
     all.insert(all.end(), e32.begin(), e32.end());
-    const int P = (int)all.size(), P0 = (int)e0.size();
+    all.insert(all.end(), eneq.begin(), eneq.end());
+    const int P = (int)all.size(), P0 = (int)e0.size(), Pn = (int)eneq.size();
     const size_t mm = (size_t)m * m;
     const size_t pe = (size_t)std::max(std::max(P, P0), 1);
     // grow-only buffers of this (device, stream) kept across calls
@@ -2107,17 +2115,21 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
     Workspace* Wp = nullptr;
     if (int rc = get_workspace(s, &Wp)) return rc;
     DevBuf &bE = Wp->rsE, &bFlags = Wp->rsFlags, &bU0 = Wp->rsU0, &bUa = Wp->rsUa, &bCorners = Wp->rsCorners,
-           &bGL = Wp->rsGL, &bRows = Wp->rsRows, &bStatus = Wp->rsStatus;
+           &bGL = Wp->rsGL, &bGLn = Wp->rsGLn, &bRows = Wp->rsRows, &bStatus = Wp->rsStatus;
     NEGF_CUDA(bE.reserve(sizeof(double) * 4 * pe));
     NEGF_CUDA(bFlags.reserve(sizeof(int) * pe));
     NEGF_CUDA(bUa.reserve(sizeof(double) * (size_t)N * m));
     NEGF_CUDA(bU0.reserve(sizeof(double) * (size_t)N * m));
     NEGF_CUDA(bCorners.reserve(16 * 2 * mm * pe));
-    NEGF_CUDA(bGL.reserve(16 * mm * K * pe));
+    NEGF_CUDA(bGL.reserve(16 * mm * K * (size_t)std::max(std::max(P - Pn, P0), 1)));
+    if (Pn > 0) NEGF_CUDA(bGLn.reserve(16 * mm * (2 * (size_t)K + 1) * Pn));
     NEGF_CUDA(bRows.reserve(sizeof(double) * (size_t)N * pe));
     NEGF_CUDA(bStatus.reserve(sizeof(int)));
     NEGF_CUDA(cudaMemsetAsync(bStatus.p, 0, sizeof(int), s));
-    const int iters = t->d.decimation_max_iter + 2;
+    negf::RsLeads leads;
+    leads.use_decimation = t->d.use_decimation;
+    leads.dec_layers = t->d.decimation_layers;
+    leads.dec_iters = t->d.decimation_max_iter + 2;
     double* dE = bE.as<double>();
     auto upload = [&](const std::vector<RsE>& v, std::vector<double>& host, std::vector<int>& hflags) -> int {
         const int n = (int)v.size();
@@ -2142,9 +2154,9 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
         t->d_rs_rho0 = d_rho;
         NEGF_CUDA(cudaMemsetAsync(bU0.p, 0, sizeof(double) * (size_t)N * m, s));
         if (int rc = upload(e0, host0, hflags0)) return rc;
-        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P0, dE + 2 * P0, dE + 3 * P0, P0,
-                                         bFlags.as<int>(), bU0.as<double>(), bU0.as<double>(), 0.0, 0.0, iters,
-                                         bCorners.p, bGL.p, bRows.as<double>(), t->d_rs_rho0, nullptr,
+        NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P0, dE + 2 * P0, dE + 3 * P0, P0, 0,
+                                         bFlags.as<int>(), bU0.as<double>(), bU0.as<double>(), 0.0, 0.0, leads,
+                                         bCorners.p, bGL.p, nullptr, bRows.as<double>(), t->d_rs_rho0, nullptr,
                                          bStatus.as<int>(), s));
         NEGF_CUDA(cudaStreamSynchronize(s));  // the host energy tables are rewritten below
     }
@@ -2154,8 +2166,8 @@ int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, vo
         Ua = bUa.as<double>();
     }
     if (int rc = upload(all, host1, hflags1)) return rc;
-    NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, P, bFlags.as<int>(), Ua,
-                                     bU0.as<double>(), t->Uc[0], t->Uc[1], iters, bCorners.p, bGL.p,
+    NEGF_CUDA(negf::launch_realspace(m, K, t->d.gamma, dE, dE + P, dE + 2 * P, dE + 3 * P, P, Pn, bFlags.as<int>(),
+                                     Ua, bU0.as<double>(), t->Uc[0], t->Uc[1], leads, bCorners.p, bGL.p, bGLn.p,
                                      bRows.as<double>(), d_Q, t->d_rs_rho0, bStatus.as<int>(), s));
     int status = 0;
     NEGF_CUDA(cudaMemcpyAsync(&status, bStatus.p, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -83,17 +83,27 @@ cudaError_t launch_transport(const TubeDev* d_tubes, const ChainRec* d_chains, c
                              double* d_red, double* d_ldos, int N, cudaStream_t stream);
 // Real-space ring-block RGF (negf_realspace.cu): leads, chain and reduction
 // for num_e >= 0 energies with coefficients c, Q[r] = sum_e Im(c sum_atoms
-// G_jj) - d_sub[r] (d_sub may be null).
+// G_jj) - d_sub[r] (d_sub may be null).  The last num_neq energies are
+// real-axis points whose coefficients (b0, b1) = (c_re, c_im) weight the
+// source and drain spectral functions: they add b0 A^L + b1 A^R per ring
+// (FP64).
 // d_flags[e]: 1 = chain in FP32 (tensor-core products), 2 = U = 0 pass
 // (d_Uzero on the atoms and 0 at the contacts; with negated c it subtracts
 // Rho0); otherwise the atom potentials d_Uatoms ([2K][m]) and Uc0, Uc1.
-// d_corners: num_e * 2 * m^2 complex, d_gL: num_e * K * m^2 complex,
-// d_rows: num_e * 2K doubles; *d_status set to 1 on a zero pivot.
+// d_corners: num_e * 2 * m^2 complex, d_gL: (num_e - num_neq) * K * m^2
+// complex, d_gLn: num_neq * (2K + 1) * m^2 complex, d_rows: num_e * 2K
+// doubles; *d_status set to 1 on a zero pivot.
+// Leads of the real-space pass: the mode chains' surface values by the
+// analytic formula, or by the reference's decimation (dec_layers layers,
+// dec_iters iterations) when use_decimation is set.
+struct RsLeads {
+    int use_decimation = 0, dec_layers = 10, dec_iters = 32;
+};
 cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
-                             const double* d_cre, const double* d_cim, int num_e, const int* d_flags,
-                             const double* d_Uatoms, const double* d_Uzero, double Uc0, double Uc1, int lead_iters,
-                             void* d_corners, void* d_gL, double* d_rows, double* d_Q, const double* d_sub,
-                             int* d_status, cudaStream_t stream);
+                             const double* d_cre, const double* d_cim, int num_e, int num_neq, const int* d_flags,
+                             const double* d_Uatoms, const double* d_Uzero, double Uc0, double Uc1,
+                             const RsLeads& leads, void* d_corners, void* d_gL, void* d_gLn, double* d_rows,
+                             double* d_Q, const double* d_sub, int* d_status, cudaStream_t stream);
 cudaError_t rs_expand(const double* d_U, int N, int m, double* d_Ua, cudaStream_t stream);
 // Self-test of the real-space tile primitives for m in {4, 13, 16}: which 2 / 3
 // inverts count m x m complex matrices in FP64 / FP32, which 4 / 5 forms

@@ -25,23 +25,22 @@
 // One block update costs one m x m inversion and three m x m products
 // instead of three 2m x 2m inversions (about 10x fewer operations).
 //
-// Leads: Lopez Sancho-Sancho-Rubio decimation of the two-ring cell in the
-// same corner form.  With s the ring that faces the device and t the other,
-// the coupling alpha between cells lives in the [t][s'] corner A and every
-// update stays in ring corners:
-//   eps[t][t] -= A g[s][s] A^T (also the surface cell), eps[s][s] -= A^T
-//   g[t][t] A, A <- A g[s][t] A,
-// with g the cell inverse through the same Schur complement (two m x m
-// inversions and a few products per iteration).  The iteration stops early
-// once both updates fall below 1e-18 of the energy scale (later ones are
-// smaller still: the decimation converges quadratically).
-//
+// Leads: a lead is uniform (the contact potential on every atom), so the
+// ring Fourier modes decouple it into the mode chains of the mode-space pass;
+// the ring corner of its surface Green's function is the circulant of the
+// per-mode surface values (rs_lead_kernel).
+
 // Kernels (one warp per energy; m x m complex tiles in shared memory,
 // row-major; m x m products on the FP64 tensor cores, mma.sync m8n8k4, with
 // the results staged in registers so that outputs may alias inputs):
-//   rs_lead_kernel   both lead corners s_L = g[b][b], s_R = g[a][a];
+//   rs_lead_kernel   both lead corners s_L = g[b][b], s_R = g[a][a] (ring
+//                    Fourier modes, per-mode surface values);
 //   rs_chain_kernel  forward sweep (X_k to global scratch), backward sweep
 //                    with the ring sums of c G_jj written per energy;
+//   rs_chain_neq_kernel  the same sweeps at a real-axis energy of a biased
+//                    tube, carrying the source and drain columns of G in
+//                    ring corners: ring sums of the contact spectral
+//                    functions (the non-equilibrium term, FP64);
 //   rs_reduce_kernel sum over energies per ring in a fixed order (Kahan).
 // The energies of the U = 0 pass (Rho0) run in the same launches with
 // negated coefficients, so one reduction gives the induced charge.
@@ -65,6 +64,8 @@ namespace negf {
 namespace {
 
 constexpr int kMaxM = 16;  // atoms per ring: [S | I] has one lane per column
+
+#include "negf_sgf.cuh"  // cd, sgf_analytic, sgf_decimation (lead mode chains)
 
 template <typename R>
 struct __align__(2 * sizeof(R)) cplx {
@@ -102,7 +103,6 @@ template <typename R>
 __device__ __forceinline__ cplx<R> cfms(cplx<R> a, cplx<R> b, cplx<R> acc) {
     return {fma(-a.x, b.x, fma(a.y, b.y, acc.x)), fma(-a.x, b.y, fma(-a.y, b.x, acc.y))};
 }
-__device__ __forceinline__ double cabs1(cplxd a) { return fabs(a.x) + fabs(a.y); }
 // Reciprocal: hardware approximation y0 = rcp.approx.ftz(x) with relative
 // error e = 1 - x y0 (|e| <= 2^-20 or better), corrected by the truncated
 // series 1/x = y0 (1 + e + e^2 + ...) to a relative error of order e^3 (FP64)
@@ -433,11 +433,6 @@ __device__ __forceinline__ bool invert(Mat<m, R> out, Mat<m, R> S, cplx<R>* buf,
     return true;
 }
 
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
 __device__ __forceinline__ cplxd warp_sum(cplxd v) {
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
@@ -465,107 +460,155 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // atoms and the contacts (the Rho0 pass).
 constexpr int kRsFP32 = 1, kRsZeroU = 2;
 
-// Lead kernel: warp w -> energy w / 2, lead w % 2 (0 left: s = ring b, the
-// intra-cell bond from s to t is C^T; 1 right: s = ring a, bond C), the lead
-// cell at the contact potential.  corners[e][side] = g_surface[s][s] (m x m,
-// row-major).
+// Lead kernel: block e -> energy e, lanes 0-15 the left lead, 16-31 the
+// right one.  A lead is uniform (the contact potential u on every atom), so
+// the Fourier vectors of a ring, v_k[j] = exp(2 pi i k j / m) / sqrt(m),
+// decouple it: C v_k = (1 + exp(2 pi i k / m)) v_k, and with a gauge phase
+// per ring mode k is the chain of alternating hoppings
+// beta_k = 2 gamma cos(pi k / m) (the double bond) and gamma (the single
+// bond), the surface ring's first bond being beta_k on both sides (left:
+// surface ring b bonded to ring a of its cell; right: surface ring a bonded
+// to ring b).  These are the mode chains of the mode-space pass
+// (CNT.cpp:288-336), so the ring corner of the lead's surface Green's
+// function is the circulant
+//   s[j][l] = (1/m) sum_k cos(2 pi k (j - l) / m) s_k,
+// s_k the mode chain's surface value by the mode-space formula
+// (sgf_analytic, CNT.cpp:354-393, or the reference's decimation when the
+// tube uses it).  Exact in O(m^2) per energy and lead, with no matrix
+// iteration (an iterated decimation on the 2m-atom cell loses accuracy on
+// the real axis, where its Schur complements divide by E - u).
+// corners[e][side] = g_surface[s][s] (m x m, row-major).
 template <int m>
-__global__ void __launch_bounds__(32, 8) rs_lead_kernel(double gamma, const double* __restrict__ Ere,
-                                                        const double* __restrict__ Eim, int num_e,
-                                                        const int* __restrict__ flags, double Uc0, double Uc1,
-                                                        int iters,
-                                                        cplxd* __restrict__ corners, int* __restrict__ status) {
-    extern __shared__ cplxd sh[];
+__global__ void __launch_bounds__(32) rs_lead_kernel(double gamma, const double* __restrict__ Ere,
+                                                     const double* __restrict__ Eim, int num_e,
+                                                     const int* __restrict__ flags, double Uc0, double Uc1,
+                                                     int use_decimation, int dec_layers, int dec_iters,
+                                                     cplxd* __restrict__ corners) {
+    __shared__ cd sk[2][kMaxM], cdiff[2][kMaxM];
     const int lane = threadIdx.x;
-    const int w = blockIdx.x;
-    if (w >= 2 * num_e) return;
-    const int e = w / 2, side = w % 2;
-    const int dir = side == 0 ? -1 : 1;  // C_st[i][l] != 0 for l in {i, i + dir}
-    constexpr int mm2 = m * m;
-    const Mat<m, double> Ess{sh}, Ett{sh + mm2}, Est{sh + 2 * mm2}, Al{sh + 3 * mm2}, Qi{sh + 4 * mm2},
-        Gss{sh + 5 * mm2}, V{sh + 6 * mm2}, U1{sh + 7 * mm2}, P{sh + 8 * mm2}, T{sh + 9 * mm2};
-    cplxd* buf = sh + 10 * mm2;  // pivot column
+    const int e = blockIdx.x;
+    if (e >= num_e) return;
+    const int side = lane >> 4, k = lane & 15;
     const double u = (flags[e] & kRsZeroU) ? 0.0 : (side == 0 ? Uc0 : Uc1);
-    const cplxd eu = cmk(Ere[e] - u, Eim[e]);
-    const double g2 = gamma * gamma;
-    const double tol = 1e-18 * (cabs1(eu) + fabs(gamma));
-    RS_FOR_ENTRIES(m, lane, {
-        const cplxd d = r == c ? eu : cmk(0.0, 0.0);
-        Ess.at(r, c) = d;
-        Ett.at(r, c) = d;
-        Est.at(r, c) = d;
-        Al.at(r, c) = cmk(r == c ? -gamma : 0.0, 0.0);
-    })
-    __syncwarp();
-    bool ok = true;
-    for (int it = 0; it < iters; ++it) {
-        // cell inverse: Qi = Ett^-1, g[s][s] = (Ess - gamma^2 C Qi C^T)^-1,
-        // V = C Qi, U1 = g[s][s] V (g[s][t] = gamma U1),
-        // g[t][t] = Qi + gamma^2 V^T U1 (kept in Qi)
-        ok = invert<m>(Qi, Ett, buf, lane) && ok;
-        RS_FOR_ENTRIES(m, lane, {
-            const int r1 = wrap<m>(r + dir), c1 = wrap<m>(c + dir);
-            const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
-            Gss.at(r, c) = csub(Ess.at(r, c), cscale(q, g2));
-            V.at(r, c) = cadd(Qi.at(r, c), Qi.at(r1, c));
-        })
-        ok = invert<m>(Gss, Gss, buf, lane) && ok;
-        mm<m, false, false, false>(U1, Gss, V, Gss, 1.0, lane);
-        mm<m, true, false, true>(Qi, V, U1, Qi, g2, lane);
-        // eps[t][t] -= A g[s][s] A^T (bulk and surface), eps[s][s] -= A^T g[t][t] A
-        mm<m, false, false, false>(P, Al, Gss, P, 1.0, lane);
-        mm<m, false, true, false>(T, P, Al, T, 1.0, lane);
-        double d1 = 0.0;
-        RS_FOR_ENTRIES(m, lane, {
-            const cplxd t = T.at(r, c);
-            Ett.at(r, c) = csub(Ett.at(r, c), t);
-            Est.at(r, c) = csub(Est.at(r, c), t);
-            d1 = fmax(d1, cabs1(t));
-        })
-        __syncwarp();
-        mm<m, true, false, false>(P, Al, Qi, P, 1.0, lane);
-        mm<m, false, false, false>(T, P, Al, T, 1.0, lane);
-        RS_FOR_ENTRIES(m, lane, {
-            const cplxd t = T.at(r, c);
-            Ess.at(r, c) = csub(Ess.at(r, c), t);
-            d1 = fmax(d1, cabs1(t));
-        })
-        __syncwarp();
-        // A <- A g[s][t] A = gamma A U1 A
-        mm<m, false, false, false>(P, Al, U1, P, 1.0, lane);
-        mm<m, false, false, false>(Al, P, Al, Al, gamma, lane);
-        if (warp_max(d1) <= tol) break;
+    const cd EmU = {Ere[e] - u, Eim[e]};
+    if (k < m) {
+        const double beta = 2.0 * gamma * cospi((double)k / m);
+        sk[side][k] = use_decimation ? sgf_decimation(EmU, beta, gamma, dec_layers, dec_iters)
+                                     : sgf_analytic(EmU, beta, gamma);
     }
-    // surface: g_s[s][s] = ((E - u) I - gamma^2 C Est^-1 C^T)^-1
-    ok = invert<m>(Qi, Est, buf, lane) && ok;
-    RS_FOR_ENTRIES(m, lane, {
-        const int r1 = wrap<m>(r + dir), c1 = wrap<m>(c + dir);
-        const cplxd q = cadd(cadd(Qi.at(r, c), Qi.at(r, c1)), cadd(Qi.at(r1, c), Qi.at(r1, c1)));
-        Gss.at(r, c) = csub(r == c ? eu : cmk(0.0, 0.0), cscale(q, g2));
-    })
-    ok = invert<m>(Gss, Gss, buf, lane) && ok;
-    cplxd* out = corners + ((size_t)e * 2 + side) * mm2;
-    for (int i = lane; i < mm2; i += 32) out[i] = Gss.a[i];
-    if (!ok && lane == 0) atomicExch(status, 1);
+    __syncwarp();
+    if (k < m) {  // circulant value of ring-index difference d = k
+        cd acc = {0.0, 0.0};
+        for (int q = 0; q < m; ++q) acc = cadd(acc, cscale(cospi(2.0 * (double)((q * k) % m) / m), sk[side][q]));
+        cdiff[side][k] = cscale(1.0 / m, acc);
+    }
+    __syncwarp();
+    cplxd* out = corners + ((size_t)e * 2 + side) * m * m;
+    for (int i = k; i < m * m; i += 16) {
+        const int j = i / m, l = i % m;
+        const cd v = cdiff[side][j >= l ? j - l : j - l + m];
+        out[i] = cmk(v.x, v.y);
+    }
+}
+
+// Gamma = i (Sigma - Sigma^dagger) = -2 gamma^2 Im s of a contact (s: the
+// lead's surface corner, complex symmetric), factored as L L^T by Cholesky
+// with diagonal pivoting (Gamma is real symmetric positive semidefinite);
+// columns past the numerical rank (pivots below 1e-13 of the largest
+// diagonal entry) stay zero.  One lane, once per energy and contact; L times
+// `scale` into a complex tile (imaginary parts zero).
+template <int m>
+__device__ __noinline__ void gamma_factor(const cplxd* __restrict__ s, double g2, double scale, Mat<m, double> L,
+                                          int lane) {
+    if (lane == 0) {
+        double a[m][m];
+        int perm[m];
+        double dmax = 0.0;
+        for (int i = 0; i < m; ++i) {
+            perm[i] = i;
+            for (int j = 0; j < m; ++j) a[i][j] = -g2 * (s[i * m + j].y + s[j * m + i].y);
+            dmax = fmax(dmax, a[i][i]);
+        }
+        int rank = 0;
+        for (int p = 0; p < m; ++p) {
+            int q = p;
+            for (int i = p + 1; i < m; ++i)
+                if (a[i][i] > a[q][q]) q = i;
+            if (!(a[q][q] > 1e-13 * dmax)) break;
+            if (q != p) {
+                for (int j = 0; j < m; ++j) {
+                    const double t = a[p][j];
+                    a[p][j] = a[q][j];
+                    a[q][j] = t;
+                }
+                for (int i = 0; i < m; ++i) {
+                    const double t = a[i][p];
+                    a[i][p] = a[i][q];
+                    a[i][q] = t;
+                }
+                const int t = perm[p];
+                perm[p] = perm[q];
+                perm[q] = t;
+            }
+            const double l = sqrt(a[p][p]), il = 1.0 / l;
+            a[p][p] = l;
+            for (int i = p + 1; i < m; ++i) a[i][p] *= il;
+            for (int j = p + 1; j < m; ++j)
+                for (int i = j; i < m; ++i) {
+                    a[i][j] -= a[i][p] * a[j][p];
+                    a[j][i] = a[i][j];
+                }
+            rank = p + 1;
+        }
+        for (int i = 0; i < m * m; ++i) L.a[i] = cmk(0.0, 0.0);
+        for (int p = 0; p < rank; ++p)
+            for (int i = p; i < m; ++i) L.at(perm[i], p) = cmk(a[i][p] * scale, 0.0);
+    }
+    __syncwarp();
 }
 
 // One energy's chain in precision R (warp e): atom potentials Ua, lead
 // corners (FP64, m x m, row-major), scratch myX for X_k (K m^2 complex R),
 // row of 2K ring sums Im(c sum_j G_jj) written in FP64.  The potentials of
 // the next block are loaded while the current block is computed.
-template <int m, typename R>
+//
+// NEQ (a real-axis energy, FP64): the row holds instead the ring sums of the
+// contact spectral functions, b0 A^L + b1 A^R with (b0, b1) = cc and
+// A^c_ring = sum_{n in ring} [G_{n,c} Gamma_c G_{n,c}^dagger]_nn
+// = || G_{ring,c} L_c ||_F^2 (Gamma_c = L_c L_c^T).  The contact columns of
+// G are carried through the sweeps in ring corners:
+//   source (ring a of block 0): Q_k = g_L[k]_{b_k, a_0} L_L with
+//     Q_{-1} = L_L / gamma, Q_k = gamma^2 Y^T (X_k Q_{k-1}) (forward, kept in
+//     myQ); G_{k,0}[a] L_L = gamma G_kk[a][a] Q_{k-1} and
+//     G_{k,0}[b] L_L = (I + gamma^2 g_L[b][b] G') Q_k (backward);
+//   drain (ring b of block K-1): T_k = G_{k,c}[a] L_R with
+//     T_K = (I + gamma^2 G'_K g_L[b][b]) L_R / gamma (G'_K of the right lead),
+//     T_k = gamma^2 X_k (Y T_{k+1}) and G_{k,c}[b] L_R = gamma g_L[b][b] T_{k+1}.
+// Four more m x m products per block in the backward sweep and one in the
+// forward sweep; no G_jj sums (the real-axis energies carry no contour term).
+template <int m, typename R, bool NEQ = false>
 __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, const double* __restrict__ Ua,
                                          const cplxd* __restrict__ sL, const cplxd* __restrict__ sR,
-                                         cplx<R>* __restrict__ myX, double* __restrict__ row, cplx<R>* sh, int lane) {
+                                         cplx<R>* __restrict__ myX, cplx<R>* __restrict__ myQ,
+                                         double* __restrict__ row, cplx<R>* sh, int lane) {
+    static_assert(!NEQ || sizeof(R) == 8, "the non-equilibrium chains run in FP64");
     using C = cplx<R>;
     constexpr int mm2 = m * m;
+    constexpr int tiles = NEQ ? 9 : 5;
     const R g2 = gamma * gamma, g4 = g2 * g2;
     const R zero(0), one(1);
     const Mat<m, R> X{sh}, Gbb{sh + mm2}, Gn{sh + 2 * mm2}, Z{sh + 3 * mm2}, W{sh + 4 * mm2};
-    C* dv = sh + 5 * mm2;  // D^-1 of the current ring b
-    C* da = dv + kMaxM;    // E - U of the current ring a
-    C* buf = da + kMaxM;   // pivot column
+    // NEQ: source columns (current / previous block), drain column, product tile
+    const Mat<m, R> Qa{sh + 5 * mm2}, Qb{sh + 6 * mm2}, T{sh + 7 * mm2}, P{sh + 8 * mm2};
+    C* dv = sh + tiles * mm2;  // D^-1 of the current ring b
+    C* da = dv + kMaxM;        // E - U of the current ring a
+    C* buf = da + kMaxM;       // pivot column
     bool ok = true;
+    if constexpr (NEQ) {
+        gamma_factor<m>(sL, g2, one / gamma, Qa, lane);  // Q_{-1}
+        gamma_factor<m>(sR, g2, one, T, lane);           // L_R
+        for (int i = lane; i < mm2; i += 32) myQ[i] = Qa.a[i];
+    }
     // lane j < m: potentials of atom j on rings a and b of the next block
     R ua_n = zero, ub_n = zero;
     auto fetch_u = [&](int k) {
@@ -610,6 +653,17 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
         ok = invert<m>(X, X, buf, lane) && ok;
         C* dst = myX + (size_t)k * mm2;
         for (int i = lane; i < mm2; i += 32) dst[i] = X.a[i];
+        if constexpr (NEQ) {
+            // Q_k = gamma^2 Y^T (X_k Q_{k-1}), (Y^T M)[r][c] = D^-1_r (M[r][c] + M[r-1][c])
+            mm<m, false, false, false>(P, X, Qa, P, one, lane);
+            RS_FOR_ENTRIES(m, lane, {
+                const int r0 = wrap<m>(r - 1);
+                Qa.at(r, c) = cscale(cmul(dv[r], cadd(P.at(r, c), P.at(r0, c))), g2);
+            })
+            __syncwarp();
+            C* qd = myQ + (size_t)(k + 1) * mm2;
+            for (int i = lane; i < mm2; i += 32) qd[i] = Qa.a[i];
+        }
         form_gbb(X);
     }
     // G_K[a][a] of the right lead's first ring: (I - gamma^2 s_R g_L[b][b])^-1 s_R
@@ -619,21 +673,54 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
     if (lane < m) Gn.at(lane, lane) = cadd(Gn.at(lane, lane), cmk(one, zero));
     ok = invert<m>(Gn, Gn, buf, lane) && ok;
     mm<m, false, false, false>(Gn, Gn, X, Gn, one, lane);
+    if constexpr (NEQ) {
+        // T_K = (L_R + gamma^2 G'_K (g_L[b][b] L_R)) / gamma
+        mm<m, false, false, false>(P, Gbb, T, P, one, lane);
+        mm<m, false, false, true>(T, Gn, P, T, g2, lane);
+        RS_FOR_ENTRIES(m, lane, { T.at(r, c) = cscale(T.at(r, c), one / gamma); })
+        __syncwarp();
+    }
     fetch_u(K - 1);
     // Backward.  X_{k-1} is copied into the tile that held the product W of
     // step k (free once tr G[b][b] is formed) while the last two products of
     // step k run; the two tiles swap roles every step.
     Mat<m, R> Xc = X, Wc = W;
+    // NEQ: Qc = Q_k, Qp = Q_{k-1}; Q_{k-2} is copied into Qc once Q_k is used
+    Mat<m, R> Qc = Qa, Qp = Qb;
     {
         const C* src = myX + (size_t)(K - 1) * mm2;
         for (int i = lane; i < mm2; i += 32) Xc.a[i] = src[i];
+        if constexpr (NEQ) {
+            for (int i = lane; i < mm2; i += 32) {
+                Qc.a[i] = myQ[(size_t)K * mm2 + i];
+                Qp.a[i] = myQ[(size_t)(K - 1) * mm2 + i];
+            }
+        }
     }
     for (int k = K - 1; k >= 0; --k) {
-        cp_async_wait_all();  // X_k (issued during step k + 1) has landed
+        cp_async_wait_all();  // X_k (and Q_{k-1}), issued during step k + 1, have landed
         if (lane < m) dv[lane] = crcp(cmk(E.x - ub_n, E.y));
         if (k > 0) fetch_u(k - 1);
         __syncwarp();
         form_gbb(Xc);
+        double tRa = 0.0, tRb = 0.0, tLa = 0.0, tLb = 0.0;
+        if constexpr (NEQ) {
+            // drain column, ring b: gamma g_L[b][b] T_{k+1}; then Y T_{k+1} into P
+            mm<m, false, false, false>(P, Gbb, T, P, gamma, lane);
+            RS_FOR_ENTRIES(m, lane, {
+                const C v = P.at(r, c);
+                tRb = fma(v.x, v.x, fma(v.y, v.y, tRb));
+                const int r1 = wrap<m>(r + 1);
+                P.at(r, c) = cadd(cmul(dv[r], T.at(r, c)), cmul(dv[r1], T.at(r1, c)));
+            })
+            __syncwarp();
+            // ring a: T_k = gamma^2 X_k (Y T_{k+1})
+            mm<m, false, false, false>(T, Xc, P, T, g2, lane);
+            RS_FOR_ENTRIES(m, lane, {
+                const C v = T.at(r, c);
+                tRa = fma(v.x, v.x, fma(v.y, v.y, tRa));
+            })
+        }
         // Z = Y G' Y^T = C (D^-1 G' D^-1) C^T, Y = C D^-1: H = D^-1 G' D^-1 in the
         // free tile Wc, then four neighbours of H per entry
         RS_FOR_ENTRIES(m, lane, { Wc.at(r, c) = cmul(cmul(dv[r], Gn.at(r, c)), dv[c]); })
@@ -643,18 +730,31 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
             Z.at(r, c) = cadd(cadd(Wc.at(r, c), Wc.at(r, c1)), cadd(Wc.at(r1, c), Wc.at(r1, c1)));
         })
         __syncwarp();
-        // tr G[b][b] = tr g_L[b][b] + gamma^2 sum_rc (g_L[b][b] G')[r][c] g_L[b][b][c][r]
+        // W = g_L[b][b] G'; tr G[b][b] = tr g_L[b][b] + gamma^2 sum_rc W[r][c] g_L[b][b][c][r]
         mm<m, false, false, false>(Wc, Gbb, Gn, Wc, one, lane);
         cplxd tb = cmk(0.0, 0.0);
-        RS_FOR_ENTRIES(m, lane, {
-            const C w = cmul(cscale(Wc.at(r, c), g2), Gbb.at(c, r));
-            tb = cadd(tb, cmk((double)w.x, (double)w.y));
-            if (r == c) tb = cadd(tb, cmk((double)Gbb.at(r, r).x, (double)Gbb.at(r, r).y));
-        })
-        __syncwarp();  // every lane is done with Wc
+        if constexpr (NEQ) {
+            // source column, ring b: (I + gamma^2 W) Q_k
+            mm<m, false, false, true>(P, Wc, Qc, Qc, g2, lane);
+            RS_FOR_ENTRIES(m, lane, {
+                const C v = P.at(r, c);
+                tLb = fma(v.x, v.x, fma(v.y, v.y, tLb));
+            })
+        } else {
+            RS_FOR_ENTRIES(m, lane, {
+                const C w = cmul(cscale(Wc.at(r, c), g2), Gbb.at(c, r));
+                tb = cadd(tb, cmk((double)w.x, (double)w.y));
+                if (r == c) tb = cadd(tb, cmk((double)Gbb.at(r, r).x, (double)Gbb.at(r, r).y));
+            })
+        }
+        __syncwarp();  // every lane is done with Wc (and Qc)
         if (k > 0) {
             const C* src = myX + (size_t)(k - 1) * mm2;
             for (int i = lane; i < mm2; i += 32) cp_async(Wc.a + i, src + i);
+            if constexpr (NEQ) {
+                const C* qs = myQ + (size_t)(k - 1) * mm2;  // Q_{k-2}
+                for (int i = lane; i < mm2; i += 32) cp_async(Qc.a + i, qs + i);
+            }
             cp_async_commit();
         }
         // G[a][a] = X + gamma^4 (X Z) X
@@ -665,13 +765,30 @@ __device__ __forceinline__ bool rs_chain(int K, R gamma, cplx<R> E, cplxd cc, co
             Xc = Wc;
             Wc = tt;
         }
-        cplxd ta = cmk(0.0, 0.0);
-        if (lane < m) ta = cmk((double)Gn.at(lane, lane).x, (double)Gn.at(lane, lane).y);
-        ta = warp_sum(ta);
-        tb = warp_sum(tb);
-        if (lane == 0) {
-            row[2 * k] = fma(cc.x, ta.y, cc.y * ta.x);      // Im(c tr G[a][a])
-            row[2 * k + 1] = fma(cc.x, tb.y, cc.y * tb.x);  // Im(c tr G[b][b])
+        if constexpr (NEQ) {
+            // source column, ring a: gamma G_kk[a][a] Q_{k-1}
+            mm<m, false, false, false>(P, Gn, Qp, P, gamma, lane);
+            RS_FOR_ENTRIES(m, lane, {
+                const C v = P.at(r, c);
+                tLa = fma(v.x, v.x, fma(v.y, v.y, tLa));
+            })
+            const Mat<m, R> tt = Qc;
+            Qc = Qp;
+            Qp = tt;
+            const cplxd sa = warp_sum(cmk(tLa, tRa)), sb = warp_sum(cmk(tLb, tRb));
+            if (lane == 0) {
+                row[2 * k] = fma(cc.x, sa.x, cc.y * sa.y);
+                row[2 * k + 1] = fma(cc.x, sb.x, cc.y * sb.y);
+            }
+        } else {
+            cplxd ta = cmk(0.0, 0.0);
+            if (lane < m) ta = cmk((double)Gn.at(lane, lane).x, (double)Gn.at(lane, lane).y);
+            ta = warp_sum(ta);
+            tb = warp_sum(tb);
+            if (lane == 0) {
+                row[2 * k] = fma(cc.x, ta.y, cc.y * ta.x);      // Im(c tr G[a][a])
+                row[2 * k + 1] = fma(cc.x, tb.y, cc.y * tb.x);  // Im(c tr G[b][b])
+            }
         }
     }
     return ok;
@@ -705,10 +822,39 @@ __global__ void __launch_bounds__(32, 16) rs_chain_kernel(int K, double gamma, c
     const cplxd cc = cmk(cre[e], cim[e]);
     bool ok;
     if (!(fl & kRsFP32))
-        ok = rs_chain<m, double>(K, gamma, cmk(Ere[e], Eim[e]), cc, Ua, sL, sR, myX, row, sh, lane);
+        ok = rs_chain<m, double>(K, gamma, cmk(Ere[e], Eim[e]), cc, Ua, sL, sR, myX, nullptr, row, sh, lane);
     else
         ok = rs_chain<m, float>(K, (float)gamma, cmk((float)Ere[e], (float)Eim[e]), cc, Ua, sL, sR,
-                                reinterpret_cast<cplxf*>(myX), row, reinterpret_cast<cplxf*>(sh), lane);
+                                reinterpret_cast<cplxf*>(myX), nullptr, row, reinterpret_cast<cplxf*>(sh), lane);
+    if (!ok && lane == 0) atomicExch(status, 1);
+}
+
+// Non-equilibrium chain kernel: warp i -> real-axis energy e = e_off + i in
+// FP64 with the atom potentials and coefficients (b0, b1) = (cre, cim)[e].
+// gXn: [num][2K + 1][m*m] FP64-complex (X_k, then Q_{-1} ... Q_{K-1});
+// rows: [e][2K] as for the other energies.
+template <int m>
+__global__ void __launch_bounds__(32, 8) rs_chain_neq_kernel(int K, double gamma, const double* __restrict__ Ere,
+                                                             const double* __restrict__ Eim,
+                                                             const double* __restrict__ cre,
+                                                             const double* __restrict__ cim, int e_off, int num,
+                                                             const double* __restrict__ Uatoms,
+                                                             const cplxd* __restrict__ corners,
+                                                             cplxd* __restrict__ gXn, double* __restrict__ rows,
+                                                             int* __restrict__ status) {
+    extern __shared__ cplxd sh[];
+    const int lane = threadIdx.x;
+    const int i = blockIdx.x;
+    if (i >= num) return;
+    constexpr int mm2 = m * m;
+    const int e = e_off + i;
+    const cplxd* sL = corners + (size_t)e * 2 * mm2;
+    const cplxd* sR = sL + mm2;
+    cplxd* myX = gXn + (size_t)i * (2 * K + 1) * mm2;
+    cplxd* myQ = myX + (size_t)K * mm2;
+    double* row = rows + (size_t)e * 2 * K;
+    const bool ok = rs_chain<m, double, true>(K, gamma, cmk(Ere[e], Eim[e]), cmk(cre[e], cim[e]), Uatoms, sL, sR,
+                                              myX, myQ, row, sh, lane);
     if (!ok && lane == 0) atomicExch(status, 1);
 }
 
@@ -781,8 +927,8 @@ __global__ void rs_expand_kernel(const double* __restrict__ U, int N, int m, dou
     if (i < N * m) Ua[i] = U[i / m];
 }
 
-size_t rs_lead_smem_bytes(int m) { return sizeof(cplxd) * (10 * m * m + kMaxM); }
 size_t rs_chain_smem_bytes(int m) { return sizeof(cplxd) * (5 * m * m + 3 * kMaxM); }
+size_t rs_chain_neq_smem_bytes(int m) { return sizeof(cplxd) * (9 * m * m + 3 * kMaxM); }
 
 }  // namespace
 
@@ -817,23 +963,36 @@ cudaError_t rs_selftest(int which, int m, int count, const double* d_in, double*
 namespace {
 template <int m>
 cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_Eim, const double* d_cre,
-                      const double* d_cim, int num_e, const int* d_flags, const double* d_Uatoms,
-                      const double* d_Uzero,
-                      double Uc0, double Uc1, int lead_iters, void* d_corners, void* d_gL, double* d_rows, double* d_Q,
-                      const double* d_sub, int* d_status, cudaStream_t stream) {
-    cudaError_t e = cudaFuncSetAttribute(rs_lead_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)rs_lead_smem_bytes(m));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(rs_chain_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                      const double* d_cim, int num_e, int num_neq, const int* d_flags, const double* d_Uatoms,
+                      const double* d_Uzero, double Uc0, double Uc1, const RsLeads& leads, void* d_corners,
+                      void* d_gL,
+                      void* d_gLn, double* d_rows, double* d_Q, const double* d_sub, int* d_status,
+                      cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(rs_chain_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)rs_chain_smem_bytes(m));
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(rs_chain_neq_kernel<m>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)rs_chain_neq_smem_bytes(m));
+    if (e != cudaSuccess) return e;
+    const int num_eq = num_e - num_neq;
     if (num_e > 0) {
-        rs_lead_kernel<m><<<2 * num_e, 32, rs_lead_smem_bytes(m), stream>>>(
-            gamma, d_Ere, d_Eim, num_e, d_flags, Uc0, Uc1, lead_iters, static_cast<cplxd*>(d_corners), d_status);
+        rs_lead_kernel<m><<<num_e, 32, 0, stream>>>(gamma, d_Ere, d_Eim, num_e, d_flags, Uc0, Uc1,
+                                                    leads.use_decimation, leads.dec_layers, leads.dec_iters,
+                                                    static_cast<cplxd*>(d_corners));
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
-        rs_chain_kernel<m><<<num_e, 32, rs_chain_smem_bytes(m), stream>>>(
-            K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_flags, d_Uatoms, d_Uzero,
+    }
+    if (num_neq > 0) {
+        // the longer chains first
+        rs_chain_neq_kernel<m><<<num_neq, 32, rs_chain_neq_smem_bytes(m), stream>>>(
+            K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_eq, num_neq, d_Uatoms, static_cast<const cplxd*>(d_corners),
+            static_cast<cplxd*>(d_gLn), d_rows, d_status);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (num_eq > 0) {
+        rs_chain_kernel<m><<<num_eq, 32, rs_chain_smem_bytes(m), stream>>>(
+            K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_eq, d_flags, d_Uatoms, d_Uzero,
             static_cast<const cplxd*>(d_corners), static_cast<cplxd*>(d_gL), d_rows, d_status);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -845,16 +1004,16 @@ cudaError_t launch_rs(int K, double gamma, const double* d_Ere, const double* d_
 }  // namespace
 
 cudaError_t launch_realspace(int m, int K, double gamma, const double* d_Ere, const double* d_Eim,
-                             const double* d_cre, const double* d_cim, int num_e, const int* d_flags,
-                             const double* d_Uatoms,
-                             const double* d_Uzero, double Uc0, double Uc1, int lead_iters, void* d_corners,
-                             void* d_gL, double* d_rows, double* d_Q, const double* d_sub, int* d_status,
-                             cudaStream_t stream) {
-    if (num_e < 0 || K < 1) return cudaErrorInvalidValue;
+                             const double* d_cre, const double* d_cim, int num_e, int num_neq, const int* d_flags,
+                             const double* d_Uatoms, const double* d_Uzero, double Uc0, double Uc1,
+                             const RsLeads& leads,
+                             void* d_corners, void* d_gL, void* d_gLn, double* d_rows, double* d_Q,
+                             const double* d_sub, int* d_status, cudaStream_t stream) {
+    if (num_e < 0 || num_neq < 0 || num_neq > num_e || K < 1) return cudaErrorInvalidValue;
 #define RS_CASE(M)                                                                                                 \
     case M:                                                                                                        \
-        return launch_rs<M>(K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, d_flags, d_Uatoms, d_Uzero, Uc0, Uc1,      \
-                            lead_iters, d_corners, d_gL, d_rows, d_Q, d_sub, d_status, stream);
+        return launch_rs<M>(K, gamma, d_Ere, d_Eim, d_cre, d_cim, num_e, num_neq, d_flags, d_Uatoms, d_Uzero, Uc0,  \
+                            Uc1, leads, d_corners, d_gL, d_gLn, d_rows, d_Q, d_sub, d_status, stream);
     switch (m) {
         RS_CASE(1) RS_CASE(2) RS_CASE(3) RS_CASE(4) RS_CASE(5) RS_CASE(6) RS_CASE(7) RS_CASE(8)
         RS_CASE(9) RS_CASE(10) RS_CASE(11) RS_CASE(12) RS_CASE(13) RS_CASE(14) RS_CASE(15) RS_CASE(16)

@@ -245,20 +245,26 @@ int negf_set_timing(int enable);
  * no counterpart there).  Zigzag (m,0) tubes, m <= 16: blocks of two rings
  * (2m atoms) with the double bond inside a block and the single bond
  * between blocks, 2m x 2m complex FP64 blocks handled through Schur
- * complements on their m x m ring corners, leads by the Lopez
- * Sancho-Sancho-Rubio decimation (at most decimation_max_iter + 2
- * iterations, stopped once the updates fall below rounding).
- * Equilibrium charge per ring into d_Q (device, N doubles): the tube's
- * contour and pole points with the mode-space coefficients, minus Rho0 at
- * U = 0.  d_Uatoms (device, [N][m]) gives per-atom potentials; null uses the
+ * complements on their m x m ring corners; the leads' ring corners from
+ * the ring Fourier modes (a uniform lead decouples into the mode-space
+ * chains: per-mode surface values by the analytic formula, or by the
+ * decimation when the tube sets use_decimation, summed into a circulant).
+ * Induced charge per ring into d_Q (device, N doubles): the tube's contour
+ * and pole points with the mode-space coefficients, minus Rho0 at U = 0,
+ * and for a biased tube the non-equilibrium real-axis term
+ * (Compute_RhoNonEq, NEGF_Common.cpp:3115-3578): per real-axis point the
+ * ring sums of the source and drain spectral functions
+ * G_{n,c} Gamma_c G_{n,c}^dagger (Gamma_c = i (Sigma_c - Sigma_c^dagger) on
+ * the contact ring's atoms) weighted by the mode-space coefficients, in
+ * FP64.  d_Uatoms (device, [N][m]) gives per-atom potentials; null uses the
  * tube's ring potential on every atom, in which case the result equals the
  * mode-space charge with all m//2 + 1 distinct modes.  Tubes in mixed
  * precision run the contour and pole chains at least mixed_fp64_band above
  * the real axis in FP32 (m x m products on the tensor cores in TF32 with a
  * high/remainder split, the complex product in three real products); the
- * leads, the Rho0 pass and the energy sum stay FP64.  The Rho0 pass (U = 0)
- * does not depend on the potential: the first call for a tube computes it
- * and later calls reuse it.  Synchronous. */
+ * leads, the real-axis points, the Rho0 pass and the energy sum stay FP64.
+ * The Rho0 pass (U = 0) does not depend on the potential: the first call for
+ * a tube computes it and later calls reuse it.  Synchronous. */
 int negf_rs_compute_charge(negf_tube* t, const double* d_Uatoms, double* d_Q, void* stream);
 
 /* Surrogate-model kernels (no counterpart in the reference): the training

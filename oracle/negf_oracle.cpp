@@ -881,6 +881,112 @@ void rs_diag(int m, int K, double gamma, cplx E, const double* Uatoms, double Uc
     }
 }
 
+// Non-equilibrium ring sums at one real-axis energy: for every ring the sum
+// over its atoms of the contact spectral functions A^c_nn = [G_{n,c} Gamma_c
+// G_{n,c}^dagger]_nn (Compute_RhoNonEq, NEGF_Common.cpp:3372-3466, on the
+// atom basis: Gamma_c = i (Sigma_c - Sigma_c^dagger), Sigma_L = gamma^2 sL on
+// ring a of block 0, Sigma_R = gamma^2 sR on ring b of block K-1).  Dense
+// 2m x 2m blocks: left-connected g_L for the source column (G_{k,0} =
+// gamma G_kk[:, a] g_L[k-1]_{b,0}), right-connected g_R for the drain column
+// (G_{k,K-1} = gamma G_kk[:, b] g_R[k+1]_{a,K-1}), G_kk from both sides.
+// outL / outR: [2K] ring sums.
+void rs_noneq(int m, int K, double gamma, cplx E, const double* Uatoms, double Uc0, double Uc1, int iters,
+              std::vector<double>& outL, std::vector<double>& outR) {
+    const int n = 2 * m, mm = m * m;
+    const double g2 = gamma * gamma;
+    const CMat sL = rs_lead_corner(m, gamma, E, Uc0, true, iters);
+    const CMat sR = rs_lead_corner(m, gamma, E, Uc1, false, iters);
+    std::vector<CMat> gL(K), gR(K);
+    for (int k = 0; k < K; ++k) {
+        CMat M = rs_block(m, gamma, E, Uatoms + (size_t)k * n);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j)
+                M[i * n + j] -= g2 * (k == 0 ? sL[i * m + j] : gL[k - 1][(m + i) * n + (m + j)]);
+        cinvert(M, n);
+        gL[k] = M;
+    }
+    for (int k = K - 1; k >= 0; --k) {
+        CMat M = rs_block(m, gamma, E, Uatoms + (size_t)k * n);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j)
+                M[(m + i) * n + (m + j)] -= g2 * (k == K - 1 ? sR[i * m + j] : gR[k + 1][i * n + j]);
+        cinvert(M, n);
+        gR[k] = M;
+    }
+    // Gamma of each contact (m x m)
+    CMat GamL(mm), GamR(mm);
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+            const cplx a = g2 * sL[i * m + j], at = std::conj(g2 * sL[j * m + i]);
+            const cplx b = g2 * sR[i * m + j], bt = std::conj(g2 * sR[j * m + i]);
+            GamL[i * m + j] = cplx(0.0, 1.0) * (a - at);
+            GamR[i * m + j] = cplx(0.0, 1.0) * (b - bt);
+        }
+    // PL[k] = g_L[k]_{b_k, a_0} (m x m), PR[k] = g_R[k]_{a_k, b_{K-1}}
+    std::vector<CMat> PL(K, CMat(mm)), PR(K, CMat(mm));
+    for (int k = 0; k < K; ++k)
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) {
+                cplx v = 0.0;
+                if (k == 0) {
+                    v = gL[0][(m + i) * n + j];
+                } else {
+                    for (int l = 0; l < m; ++l) v += gL[k][(m + i) * n + l] * PL[k - 1][l * m + j];
+                    v *= gamma;
+                }
+                PL[k][i * m + j] = v;
+            }
+    for (int k = K - 1; k >= 0; --k)
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) {
+                cplx v = 0.0;
+                if (k == K - 1) {
+                    v = gR[k][i * n + (m + j)];
+                } else {
+                    for (int l = 0; l < m; ++l) v += gR[k][i * n + (m + l)] * PR[k + 1][l * m + j];
+                    v *= gamma;
+                }
+                PR[k][i * m + j] = v;
+            }
+    outL.assign(2 * (size_t)K, 0.0);
+    outR.assign(2 * (size_t)K, 0.0);
+    std::vector<cplx> col(n * m);
+    for (int k = 0; k < K; ++k) {
+        CMat M = rs_block(m, gamma, E, Uatoms + (size_t)k * n);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) {
+                M[i * n + j] -= g2 * (k == 0 ? sL[i * m + j] : gL[k - 1][(m + i) * n + (m + j)]);
+                M[(m + i) * n + (m + j)] -= g2 * (k == K - 1 ? sR[i * m + j] : gR[k + 1][i * n + j]);
+            }
+        cinvert(M, n);  // G_kk
+        for (int side = 0; side < 2; ++side) {
+            // col = G_{k,c} restricted to the contact ring's atoms (2m x m)
+            const int off = side == 0 ? 0 : m;  // G_kk column block touching the neighbour towards the contact
+            const bool at_contact = side == 0 ? k == 0 : k == K - 1;
+            for (int r = 0; r < n; ++r)
+                for (int j = 0; j < m; ++j) {
+                    cplx v = 0.0;
+                    if (at_contact) {
+                        v = M[r * n + off + j];
+                    } else {
+                        const CMat& Pn = side == 0 ? PL[k - 1] : PR[k + 1];
+                        for (int l = 0; l < m; ++l) v += M[r * n + off + l] * Pn[l * m + j];
+                        v *= gamma;
+                    }
+                    col[r * m + j] = v;
+                }
+            const CMat& Gam = side == 0 ? GamL : GamR;
+            std::vector<double>& out = side == 0 ? outL : outR;
+            for (int r = 0; r < n; ++r) {
+                cplx a = 0.0;
+                for (int i = 0; i < m; ++i)
+                    for (int j = 0; j < m; ++j) a += col[r * m + i] * Gam[i * m + j] * std::conj(col[r * m + j]);
+                out[2 * k + r / m] += a.real();
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- Broyden
 // T/Broyden_Second_Parallel.cpp:9-211 (CPU branch) and
 // T/Broyden_Parallel_General.cpp:68-355 (set-up and reset).
@@ -1337,15 +1443,16 @@ int orc_tube_noneq_layout(void* h, int* pts, double* cuts, double* E_at_max) {
     return np;
 }
 
-// Real-space equilibrium charge per ring of a zigzag tube over the tube's
-// contour + poles (and Rho0 at U = 0): Q_ring = sum_atoms Im(RhoEq - Rho0)
-// with the same coefficients as the mode-space pass.  Uatoms: [N][m] per-atom
-// potentials (null: ring-uniform from the tube's U).  Returns -1 when biased.
+// Real-space charge per ring of a zigzag tube over the tube's contour + poles
+// (and Rho0 at U = 0) and, when biased, its non-equilibrium paths:
+// Q_ring = sum_atoms [Im(RhoEq - Rho0) + Re RhoNonEq] with the same
+// coefficients as the mode-space pass.  Uatoms: [N][m] per-atom potentials
+// (null: ring-uniform from the tube's U).  Returns -1 for a chiral tube.
 int orc_tube_rs_charge(void* h, const double* Uatoms, int iters, int nthreads, double* Q) {
     Tube* t = static_cast<Tube*>(h);
     energy_limits(*t);
     build_eq_noneq_paths(*t);
-    if (t->noneq || t->n != 0) return -1;
+    if (t->n != 0) return -1;
     const int m = t->m, N = t->N, K = N / 2, n = 2 * m;
     std::vector<double> Ua((size_t)N * m), U0((size_t)N * m, 0.0);
     for (int r = 0; r < N; ++r)
@@ -1389,10 +1496,32 @@ int orc_tube_rs_charge(void* h, const double* Uatoms, int iters, int nthreads, d
         for (int i = 0; i < T; ++i)
             for (int r = 0; r < N; ++r) acc[r] += part[i][r];
     };
-    std::vector<double> eq, r0;
+    std::vector<double> eq, r0, ne(N, 0.0);
     run(pts, Ua, t->Uc[0], t->Uc[1], eq);
     run(pts0, U0, 0.0, 0.0, r0);
-    for (int r = 0; r < N; ++r) Q[r] = eq[r] - r0[r];
+    if (t->noneq) {
+        // Re RhoNonEq: sum_c Re(-spin/2pi w J f_c) A^c per ring
+        auto pn = collect(t->noneq_paths, 3, *t);
+        const int T = std::max(1, std::min<int>(nthreads, (int)pn.size()));
+        std::vector<std::vector<double>> part(T, std::vector<double>(N, 0.0));
+        auto worker = [&](int tid) {
+            std::vector<double> aL, aR;
+            for (size_t i = pn.size() * tid / T; i < pn.size() * (tid + 1) / T; ++i) {
+                const EPoint& ep = pn[i];
+                rs_noneq(m, K, t->gamma, ep.E, Ua.data(), t->Uc[0], t->Uc[1], iters, aL, aR);
+                const cplx base = cmul((-1. * kSpinDegen / (2 * kPi)) * ep.w, ep.J);
+                const double b0 = cmul(base, fermi(ep.E - t->mu[0], t->kT[0])).real();
+                const double b1 = cmul(base, fermi(ep.E - t->mu[1], t->kT[1])).real();
+                for (int r = 0; r < N; ++r) part[tid][r] += b0 * aL[r] + b1 * aR[r];
+            }
+        };
+        std::vector<std::thread> th;
+        for (int i = 0; i < T; ++i) th.emplace_back(worker, i);
+        for (auto& x : th) x.join();
+        for (int i = 0; i < T; ++i)
+            for (int r = 0; r < N; ++r) ne[r] += part[i][r];
+    }
+    for (int r = 0; r < N; ++r) Q[r] = eq[r] + ne[r] - r0[r];
     return 0;
 }
 

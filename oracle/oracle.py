@@ -264,7 +264,8 @@ OracleTube.noneq_integrand = _noneq_integrand
 OracleTube.correct_limits = _correct_limits
 OracleTube.noneq_layout = _noneq_layout
 def _rs_charge(self, Uatoms=None, iters=32, nthreads=1):
-    """Real-space ring-block equilibrium charge per ring (zigzag tubes)."""
+    """Real-space ring-block charge per ring (zigzag tubes): contour, poles and,
+    when biased, the non-equilibrium real-axis term."""
     Q = np.zeros(self.N)
     ua = None
     if Uatoms is not None:
@@ -272,7 +273,7 @@ def _rs_charge(self, Uatoms=None, iters=32, nthreads=1):
         ua = self._ua.ctypes.data_as(C.c_void_p)
     rc = lib().orc_tube_rs_charge(self._h, ua, int(iters), int(nthreads), Q)
     if rc != 0:
-        raise ValueError("real-space charge needs a zigzag tube at equilibrium")
+        raise ValueError("real-space charge needs a zigzag tube")
     return Q
 
 

@@ -89,9 +89,52 @@ def test_realspace_rejections():
     t = CNT(type_id=(17, 0), num_unitcells=2, num_modes=2, contact_mu=(-0.8, -0.8))
     with pytest.raises(NEGFError, match="at most 32 atoms"):
         t.realspace_charge()
-    b = CNT(type_id=(13, 0), num_unitcells=2, num_modes=2, contact_mu=(0.0, -0.3))
-    with pytest.raises(NEGFError, match="equilibrium"):
-        b.realspace_charge()
+
+
+def _bias_kw(m, cells, **extra):
+    kw = dict(type_id=(m, 0), num_unitcells=cells, num_modes=1, contact_mu=(0.0, -0.3), contact_T=(300.0, 320.0),
+              eq_integration_pts=(16, 16, 24), noneq_integration_pts=(48,), E_pole_max=3.0, E_zPlus_imag=1e-4)
+    kw.update(extra)
+    return kw
+
+
+@pytest.mark.parametrize("m,cells", [(13, 4), (7, 3), (16, 2), (4, 3), (10, 2), (1, 3)])
+def test_realspace_noneq_against_block_oracle(oracle, m, cells):
+    """Biased tubes: the real-axis points add the source and drain spectral
+    functions (carried through the sweeps as ring-corner columns) against the
+    dense-block oracle (left- and right-connected recursions)."""
+    g, o = _pair(oracle, seed=35, **_bias_kw(m, cells))
+    assert g.noneq()
+    Qg = g.realspace_charge()
+    Qo = o.rs_charge(nthreads=8)
+    assert _rel(Qg, Qo) <= TOL, _rel(Qg, Qo)
+
+
+def test_realspace_noneq_per_atom_potential_and_mixed(oracle):
+    import torch
+    kw = _bias_kw(13, 4, contact_mu=(-0.1, -0.5))
+    g, o = _pair(oracle, seed=36, **kw)
+    rng = np.random.default_rng(6)
+    Ua = (np.repeat(np.asarray(g_U(g)), 13) + 0.05 * rng.standard_normal(g.num_field_sites * 13)).reshape(-1, 13)
+    Qo = o.rs_charge(Uatoms=Ua, nthreads=8)
+    Qg = g.realspace_charge(U_atoms=torch.tensor(Ua, device="cuda"))
+    assert _rel(Qg, Qo) <= TOL, _rel(Qg, Qo)
+    gm, _ = _pair(oracle, seed=36, **kw, precision="mixed")
+    Qm = gm.realspace_charge(U_atoms=torch.tensor(Ua, device="cuda"))
+    assert _rel(Qm, Qo) <= MIXED_TOL, _rel(Qm, Qo)
+
+
+def test_realspace_noneq_equals_all_modes_mode_space():
+    """A biased 300-block (13,0) tube with a ring-uniform potential: the
+    real-space charge equals the mode-space charge over all 7 modes."""
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import site_potential
+    g = CNT(**_bias_kw(13, 150, num_modes=7, eq_integration_pts=(32, 32, 48), noneq_integration_pts=(96,)))
+    U = site_potential(g.site_positions(), 20261203 + 5)
+    g.set_potential(U, (U[0], U[-1]))
+    Qr = g.realspace_charge()
+    Qm = g.Solve_NEGF()
+    assert _rel(Qr, Qm) <= TOL, _rel(Qr, Qm)
 
 
 def _tiles(negf_lib, which, m, data, count, out_per):

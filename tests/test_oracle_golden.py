@@ -214,3 +214,21 @@ def test_current_against_dense_inverse(oracle):
     assert abs(I[0] - Iref) / abs(Iref) < 1e-8
     assert abs(I[1] + Iref) / abs(Iref) < 1e-8
     assert probes.shape == (3, len(E)) and np.all(np.isfinite(probes))
+
+
+@pytest.mark.parametrize("m,cells,mu", [(7, 3, (0.0, -0.3)), (13, 2, (-0.2, -0.5)), (4, 2, (0.1, -0.2))])
+def test_oracle_realspace_noneq_equals_mode_space(oracle, m, cells, mu):
+    """The oracle's dense-block real-space charge of a biased tube (contour,
+    poles and the source/drain spectral functions at the real-axis points)
+    equals its mode-space charge over all m // 2 + 1 distinct modes for a
+    ring-uniform potential."""
+    kw = dict(type_id=(m, 0), num_unitcells=cells, num_modes=m // 2 + 1, contact_mu=mu, contact_T=(300.0, 320.0),
+              eq_integration_pts=(16, 16, 24), noneq_integration_pts=(40,), E_pole_max=3.0, E_zPlus_imag=1e-3)
+    o = oracle.OracleTube(noneq_percent_intercuts=None, **kw)
+    assert o.noneq()
+    rng = np.random.default_rng(1)
+    U = 0.1 * rng.standard_normal(o.N)
+    o.set_potential(U, (U[0], U[-1]))
+    Qm = o.charge(nthreads=4)
+    Qr = o.rs_charge(nthreads=4)
+    assert np.abs(Qm - Qr).max() <= 1e-12 * np.abs(Qm).max()
