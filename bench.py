@@ -435,8 +435,8 @@ def config3_measure(torch, passes=2, small=False):
     Qr = Q.cpu().numpy()
     return {"workload": "(13,0) CNT, %d blocks of 2 rings (26 atoms), %d contour+pole energies per pass (the "
                         "%d-energy Rho0 pass at U = 0 runs once per tube, in the warm-up call, as the mode-space "
-                        "Rho0 does at tube creation), Sancho-Rubio leads (at most 32 iterations), FP64, seeded "
-                        "config-2 ring potential" % (K, E, E0),
+                        "Rho0 does at tube creation), lead corners from the ring Fourier modes (analytic per-mode "
+                        "surface values), FP64, seeded config-2 ring potential" % (K, E, E0),
             "seconds_per_pass": sec, "block_updates_per_s": E * K / sec,
             "achieved_tflops": flops / sec / 1e12, "flops_per_pass": flops,
             "flop_convention": "ring corners m=13: inverse 8m^3 + three complex products 8m^3 per block update "

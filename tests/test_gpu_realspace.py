@@ -180,3 +180,19 @@ def test_tile_inversion_and_products(negf_lib, m):
         Cg = _tiles(negf_lib, which, m, np.stack([_cplx_pack(P[:, 0]), _cplx_pack(P[:, 1])], axis=1), n, 2 * m * m)
         err = np.abs(Cg - ref).max() / np.abs(ref).max()
         assert err <= tol, (which, err)
+
+
+@pytest.mark.parametrize("bias", [False, True])
+def test_realspace_decimation_leads_equal_mode_space(bias):
+    """A tube with the reference's decimation leads: the real-space lead
+    corners take the same per-mode decimated surface values, so the charge
+    equals the mode-space charge over all modes."""
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import site_potential
+    kw = _bias_kw(13, 20, num_modes=7, use_decimation=1) if bias else _eq_kw(13, 20, num_modes=7, use_decimation=1)
+    g = CNT(**kw)
+    U = site_potential(g.site_positions(), 20261203 + 7, amp=0.2)
+    g.set_potential(U, (U[0], U[-1]))
+    Qr = g.realspace_charge()
+    Qm = g.Solve_NEGF()
+    assert _rel(Qr, Qm) <= TOL, _rel(Qr, Qm)
