@@ -396,10 +396,9 @@ def config3_measure(torch, passes=2, small=False):
     tube with all 7 modes (equal for this ring-uniform potential).  small:
     the profiling case, 200 blocks and 256 contour energies."""
     from electrostatic_b200.negf import CNT, last_stats, set_timing
-    from electrostatic_b200.workloads import SEED_BASE, site_potential
-    kw = dict(type_id=(13, 0), num_unitcells=100 if small else 300, num_modes=7, contact_mu=(-0.8, -0.8),
-              contact_T=(300.0, 300.0), eq_integration_pts=(64, 64, 128) if small else (512, 512, 1024),
-              E_pole_max=3.0, E_zPlus_imag=1e-6)
+    from electrostatic_b200.workloads import SEED_BASE, config3_kwargs, site_potential
+    kw = config3_kwargs(small=small)
+    kw.pop("precision")
     t = CNT(**kw)
     U = site_potential(t.site_positions(), SEED_BASE + 3)
     t.set_potential(U, (U[0], U[-1]))
@@ -435,8 +434,9 @@ def config3_measure(torch, passes=2, small=False):
     Qr = Q.cpu().numpy()
     return {"workload": "(13,0) CNT, %d blocks of 2 rings (26 atoms), %d contour+pole energies per pass (the "
                         "%d-energy Rho0 pass at U = 0 runs once per tube, in the warm-up call, as the mode-space "
-                        "Rho0 does at tube creation), lead corners from the ring Fourier modes (analytic per-mode "
-                        "surface values), FP64, seeded config-2 ring potential" % (K, E, E0),
+                        "Rho0 does at tube creation), the leads' exact surface Green's function (ring Fourier modes, "
+                        "analytic per mode; what Sancho-Rubio decimation of the lead cell converges to), FP64, "
+                        "seeded config-2 ring potential" % (K, E, E0),
             "seconds_per_pass": sec, "block_updates_per_s": E * K / sec,
             "achieved_tflops": flops / sec / 1e12, "flops_per_pass": flops,
             "flop_convention": "ring corners m=13: inverse 8m^3 + three complex products 8m^3 per block update "

@@ -80,7 +80,9 @@ def config3_kwargs(precision="fp64", small=False):
     """Real-space benchmark tube (config id 3): (13,0), 300 unit cells = 600
     ring blocks of 26 atoms, 2048 equilibrium-contour points (512 + 512
     line, 1024 arc) plus the Matsubara poles up to 3 eV, mu = -0.8 eV at
-    300 K.  small: 200 blocks and 256 contour points (the profiling case)."""
+    300 K; the leads' exact surface Green's function (what Sancho-Rubio
+    decimation of the 26-atom lead cell converges to).  small: 200 blocks and
+    256 contour points (the profiling case)."""
     return dict(type_id=(13, 0), num_unitcells=100 if small else 300, num_modes=7, contact_mu=(-0.8, -0.8),
                 contact_T=(300.0, 300.0), eq_integration_pts=(64, 64, 128) if small else (512, 512, 1024),
                 E_pole_max=3.0, E_zPlus_imag=1e-6, precision=precision)
