@@ -287,11 +287,12 @@ class CNT:
         return compute_charge([self], out=out, stream=stream)
 
     def realspace_charge(self, out=None, U_atoms=None, stream=None):
-        """Equilibrium charge per ring from the real-space ring-block RGF
-        (zigzag tubes).  U_atoms: optional device tensor [N][m] of per-atom
-        potentials.  Mixed-precision tubes run the chains far from the real
-        axis in FP32 on the tensor cores.  Returns numpy unless `out` (device
-        float64) is given."""
+        """Induced charge per ring from the real-space ring-block RGF (zigzag
+        tubes): contour and poles, plus the non-equilibrium real-axis term
+        when the tube is biased.  U_atoms: optional device tensor [N][m] of
+        per-atom potentials.  Mixed-precision tubes run the contour chains far
+        from the real axis in FP32 on the tensor cores.  Returns numpy unless
+        `out` (device float64) is given."""
         import torch
         Q = out if out is not None else torch.zeros(self.num_field_sites, dtype=torch.float64, device="cuda")
         check(_lib.load().negf_rs_compute_charge(self._h, _ptr(U_atoms), _ptr(Q), _stream(stream)),
