@@ -232,3 +232,88 @@ def test_oracle_realspace_noneq_equals_mode_space(oracle, m, cells, mu):
     Qm = o.charge(nthreads=4)
     Qr = o.rs_charge(nthreads=4)
     assert np.abs(Qm - Qr).max() <= 1e-12 * np.abs(Qm).max()
+
+
+def _dense_rs_sums(m, K, g, E, Ua, Uc0, Uc1, iters=40):
+    """Numpy dense twin of the real-space energy point: lead corners by
+    Sancho-Rubio decimation of the 2m-atom cell, the whole device inverted at
+    once; returns (tr G per ring, A^L per ring, A^R per ring)."""
+    n = 2 * m
+
+    def block(E, u):
+        A = np.diag(E - u).astype(complex)
+        for j in range(m):
+            for b in (m + j, m + (j + 1) % m):
+                A[j, b] -= g
+                A[b, j] -= g
+        return A
+
+    def lead(u, left):
+        eps = block(E, np.full(n, u))
+        eps_s = eps.copy()
+        tau = np.zeros((n, n))
+        for j in range(m):
+            tau[m + j, j] = -g
+        al, be = (tau.T, tau) if left else (tau, tau.T)
+        for _ in range(iters):
+            G = np.linalg.inv(eps)
+            agb, bga = al @ G @ be, be @ G @ al
+            eps_s, eps = eps_s - agb, eps - agb - bga
+            al, be = al @ G @ al, be @ G @ be
+        gs = np.linalg.inv(eps_s)
+        o = m if left else 0
+        return gs[o:o + m, o:o + m]
+
+    sL, sR = lead(Uc0, True), lead(Uc1, False)
+    N = n * K
+    M = np.zeros((N, N), complex)
+    for k in range(K):
+        M[k * n:(k + 1) * n, k * n:(k + 1) * n] = block(E, np.concatenate([Ua[2 * k], Ua[2 * k + 1]]))
+        if k + 1 < K:
+            for j in range(m):
+                M[k * n + m + j, (k + 1) * n + j] = M[(k + 1) * n + j, k * n + m + j] = -g
+    SL, SR = g * g * sL, g * g * sR
+    M[:m, :m] -= SL
+    M[N - m:, N - m:] -= SR
+    G = np.linalg.inv(M)
+    GL, GR = 1j * (SL - SL.conj().T), 1j * (SR - SR.conj().T)
+    AL = np.einsum("ni,ij,nj->n", G[:, :m], GL, G[:, :m].conj()).real
+    AR = np.einsum("ni,ij,nj->n", G[:, N - m:], GR, G[:, N - m:].conj()).real
+    ring = lambda v: v.reshape(2 * K, m).sum(1)
+    return ring(np.diag(G)), ring(AL), ring(AR)
+
+
+def test_oracle_realspace_noneq_per_atom_against_dense(oracle):
+    """Per-atom potentials (no mode decoupling): the oracle's biased
+    real-space charge difference between two potentials equals a dense numpy
+    evaluation over the same energy points (contour: Im(c tr G); real axis:
+    b0 A^L + b1 A^R); the U = 0 Rho0 term cancels in the difference."""
+    m, cells, g = 4, 2, 2.5
+    kw = dict(type_id=(m, 0), num_unitcells=cells, num_modes=1, contact_mu=(0.0, -0.3), contact_T=(300.0, 320.0),
+              eq_integration_pts=(12, 12, 16), noneq_integration_pts=(24,), E_pole_max=3.0, E_zPlus_imag=1e-2)
+    o = oracle.OracleTube(noneq_percent_intercuts=None, **kw)
+    N, K = o.N, o.N // 2
+    rng = np.random.default_rng(11)
+    kT = 8.617333262e-5 * np.array(kw["contact_T"])
+    mu = np.array(kw["contact_mu"])
+    fermi = lambda E, mu_, kT_: 1.0 / (1.0 + np.exp((E - mu_) / kT_))
+    Ee, we, Je = o.paths(1)
+    En, wn, Jn = o.paths(3)
+    assert len(o.paths(2)[0]) == 0  # biased: no poles
+    qs, dense = [], []
+    for _ in range(2):
+        U = 0.1 * rng.standard_normal(N)
+        Ua = U[:, None] + 0.05 * rng.standard_normal((N, m))
+        o.set_potential(U, (U[0], U[-1]))
+        qs.append(o.rs_charge(Uatoms=Ua, nthreads=4))
+        q = np.zeros(N)
+        for E, w, J in zip(Ee, we, Je):
+            c = (-2.0 / np.pi) * w * J * fermi(E, mu.min(), kT.min())
+            q += (c * _dense_rs_sums(m, K, g, E, Ua, U[0], U[-1])[0]).imag
+        for E, w, J in zip(En, wn, Jn):
+            base = (-2.0 / (2 * np.pi)) * w * J
+            _, aL, aR = _dense_rs_sums(m, K, g, E, Ua, U[0], U[-1])
+            q += (base * fermi(E, mu[0], kT[0])).real * aL + (base * fermi(E, mu[1], kT[1])).real * aR
+        dense.append(q)
+    d_or, d_np = qs[0] - qs[1], dense[0] - dense[1]
+    assert np.abs(d_or - d_np).max() <= 1e-9 * np.abs(d_np).max(), np.abs(d_or - d_np).max() / np.abs(d_np).max()
