@@ -445,7 +445,7 @@ def config3_measure(torch, passes=2, small=False):
                                  "effective_tflops": E * K * 56 * (2 * m) ** 3 / sec / 1e12,
                                  "note": "the dense 2m x 2m block algorithm's count (56 n^3 per block update, n = 26: "
                                          "forward inverse + 2 GEMM, backward the same, G_nn inverse), which the "
-                                         "ring-corner algebra replaces with about 1/11 of the operations"},
+                                         "ring-corner algebra replaces with 1/14 of the operations (32 m^3 per update)"},
             "path": "negf_rs_compute_charge (FP64 CUDA cores, one warp per energy, Schur complements on ring corners)",
             "max_rel_vs_mode_space_all_modes": float(np.max(np.abs(Qr - Qm)) / np.max(np.abs(Qm))),
             "mixed": {"seconds_per_pass": sec_mixed, "block_updates_per_s": E * K / sec_mixed,
