@@ -211,12 +211,10 @@ struct negf_charge_plan {
     int num_warps = 0, num_units = 0, max_N = 0;
     int pieces = 1;  // pass-1 pieces of the two-pass schedule (parallel in length)
     int n64 = 0, n32 = 0;  // fused schedule: FP64 / FP32 warps in d_order
-    cudaStream_t side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;  // around the FP32 warps on the launch stream's side stream
     ~negf_charge_plan() {
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
-        if (side) cudaStreamDestroy(side);
     }
     int wpb = 4, spu = negf::kSegsPerUnit;
     int schedule = 0;  // negf::kScheduleTwoPass or kScheduleFused
@@ -297,9 +295,9 @@ struct WsKey {
     }
 };
 
-// Workspace of the current device and `stream` (callers hold g_mu); waits on
-// the stream for the previous call that used it.
-int get_workspace(cudaStream_t stream, Workspace** out) {
+// Workspace of the current device and `stream`, made on first use (callers
+// hold g_mu).
+int find_workspace(cudaStream_t stream, Workspace** out) {
     static std::map<WsKey, std::unique_ptr<Workspace>> all;
     int dev = 0;
     NEGF_CUDA(cudaGetDevice(&dev));
@@ -313,8 +311,29 @@ int get_workspace(cudaStream_t stream, Workspace** out) {
         NEGF_CUDA(cudaEventCreateWithFlags(&w->join, cudaEventDisableTiming));
         NEGF_CUDA(cudaStreamCreateWithFlags(&w->side, cudaStreamNonBlocking));
     }
-    if (w->used) NEGF_CUDA(cudaStreamWaitEvent(stream, w->done, 0));
     *out = w.get();
+    return NEGF_OK;
+}
+
+// The same, waiting on the stream for the previous call that used it.
+int get_workspace(cudaStream_t stream, Workspace** out) {
+    if (int rc = find_workspace(stream, out)) return rc;
+    if ((*out)->used) NEGF_CUDA(cudaStreamWaitEvent(stream, (*out)->done, 0));
+    return NEGF_OK;
+}
+
+// Side stream for the FP32 warps of a charge plan launched on `stream`: the
+// one of that stream's workspace (callers hold g_mu).  One side stream per
+// (device, launch stream), shared with negf_compute_charge on that stream,
+// instead of one per plan: the block scheduler's interleaving of the two
+// concurrent fused kernels came out differently for different side streams
+// (config-4 batch with FP32 real axis: 1.59 or 1.80 ms per pass from one
+// plan to the next); with the launch stream's side stream it was 1.59 ms
+// in every run measured.
+int plan_side_stream(cudaStream_t stream, cudaStream_t* side) {
+    Workspace* w = nullptr;
+    if (int rc = find_workspace(stream, &w)) return rc;
+    *side = w->side;
     return NEGF_OK;
 }
 
@@ -1479,8 +1498,8 @@ int plan_tables(negf_charge_plan& p, int spu, bool upload_all) {
     return NEGF_OK;
 }
 
-cudaError_t plan_launch(const negf_charge_plan& p, const int* skip, cudaStream_t s) {
-    const negf::FusedOrder fo{p.d_order.as<int>(), p.n64, p.n32, p.side, p.fork, p.join};
+cudaError_t plan_launch(const negf_charge_plan& p, const int* skip, cudaStream_t s, cudaStream_t side) {
+    const negf::FusedOrder fo{p.d_order.as<int>(), p.n64, p.n32, side, p.fork, p.join};
     cudaError_t e = negf::launch_rgf(p.d_tubes.as<negf::TubeDev>(), p.d_chains.as<negf::ChainRec>(),
                                      p.d_warps.as<negf::WarpRec>(), p.num_warps, p.d_units.as<negf::SegUnit>(),
                                      p.num_units, p.d_partial.as<double>(), p.d_scratch.p, p.wpb, s, nullptr, skip,
@@ -1511,7 +1530,8 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
     p->force_fp64 = (flags & NEGF_PLAN_FP64) != 0;
     NEGF_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
     NEGF_CUDA(cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming));
-    NEGF_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+    cudaStream_t side0 = nullptr;  // the autotuner's launches run on the legacy default stream
+    if (int rc3 = plan_side_stream(0, &side0)) return rc3;
     p->wpb = settings().warps_per_block;
     rc = plan_tables(*p, negf::kSegsPerUnit, true);
     if (rc) return rc;
@@ -1557,10 +1577,10 @@ int negf_charge_plan_create(negf_tube* const* tubes, int num_tubes, double* d_Q,
                     p->wpb = wpb == 0 ? 4 : wpb;
                     p->schedule = wpb == 0 ? negf::kScheduleFused : negf::kScheduleTwoPass;
                     p->pieces = pc;
-                    cudaError_t e = plan_launch(*p, nullptr, 0);
+                    cudaError_t e = plan_launch(*p, nullptr, 0, side0);
                     for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
                         if (r == 1) e = cudaEventRecord(e0, 0);
-                        if (e == cudaSuccess) e = plan_launch(*p, nullptr, 0);
+                        if (e == cudaSuccess) e = plan_launch(*p, nullptr, 0, side0);
                     }
                     if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
                     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
@@ -1600,7 +1620,12 @@ int negf_charge_plan_launch(negf_charge_plan* p, const int* d_skip, void* stream
         if (p->tubes[i]->version != p->versions[i] || p->tubes[i]->limits_dirty)
             return fail(NEGF_ERR_STATE, "charge plan is stale: the energy paths of tube " + std::to_string(i) +
                                             " changed after the plan was made");
-    NEGF_CUDA(plan_launch(*p, d_skip, (cudaStream_t)stream));
+    cudaStream_t side = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (int rc = plan_side_stream((cudaStream_t)stream, &side)) return rc;
+    }
+    NEGF_CUDA(plan_launch(*p, d_skip, (cudaStream_t)stream, side));
     return NEGF_OK;
 }
 

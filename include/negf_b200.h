@@ -359,7 +359,11 @@ int negf_write_integrand(negf_tube* t, const char* path, int count, const double
 
 /* Charge plans: the launch tables of a batch uploaded once, so that
  * negf_charge_plan_launch is kernel launches only (no allocation, no host
- * copy, no synchronisation) and can be captured in a CUDA graph.  The
+ * copy, no synchronisation) and can be captured in a CUDA graph.  A plan
+ * with both FP64 and FP32 chains runs the FP32 ones beside the FP64 ones
+ * on a side stream of the launch stream, made by the first launch (or
+ * negf_compute_charge call) on that stream: make that first launch before
+ * capturing the stream.  The
  * contact potentials are read on the device as U[0] and U[N-1] of each
  * tube's potential buffer (U_contact = U at the end sites,
  * Nanostructure.cpp:500-504).  d_Q: device output of sum N doubles (tube
