@@ -39,7 +39,7 @@ EXPORTED = [
     "negf_broyden_step_device_switch", "negf_rs_compute_charge", "negf_nn_gemm", "negf_nn_gelu_fwd",
     "negf_nn_gelu_bwd", "negf_nn_colsum", "negf_nn_cast_bf16", "negf_nn_adam", "negf_nn_rowdot", "negf_nn_outer",
     "negf_nn_mse", "negf_affine_potential_toeplitz", "negf_potential_batch_create", "negf_potential_batch_launch",
-    "negf_potential_batch_destroy", "negf_charge_plan_pieces",
+    "negf_potential_batch_destroy", "negf_charge_plan_pieces", "negf_release_scratch",
 ]
 
 
@@ -136,6 +136,7 @@ def load():
         "negf_compute_charge": [C.POINTER(vp), C.c_int, vp, C.c_int, vp],
         "negf_compute_charge_noalloc": [C.POINTER(vp), C.c_int, vp, vp],
         "negf_last_stats": [C.POINTER(Stats)],
+        "negf_release_scratch": [vp],
         "negf_set_timing": [C.c_int],
         "negf_set_tuning": [C.c_int, C.c_int],
         "negf_broyden_create": [C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(vp)],

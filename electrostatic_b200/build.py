@@ -48,14 +48,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if verbose:
         cmd += ["-Xptxas", "-v"]
     cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    cmd += ["-o", LIB + ".tmp"]
+    # a temporary name per process: ranks that start together may all build,
+    # and each one's rename below is atomic
+    tmp = f"{LIB}.{os.getpid()}.tmp"
+    cmd += ["-o", tmp]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if verbose or res.returncode != 0:
         sys.stdout.write(res.stdout)
         sys.stderr.write(res.stderr)
     if res.returncode != 0:
+        if os.path.exists(tmp):
+            os.remove(tmp)
         raise RuntimeError("nvcc failed building libnegf_b200.so")
-    os.replace(LIB + ".tmp", LIB)
+    os.replace(tmp, LIB)
     return LIB
 
 

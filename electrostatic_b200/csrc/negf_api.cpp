@@ -295,13 +295,17 @@ struct WsKey {
     }
 };
 
+std::map<WsKey, std::unique_ptr<Workspace>>& workspaces() {
+    static std::map<WsKey, std::unique_ptr<Workspace>> all;
+    return all;
+}
+
 // Workspace of the current device and `stream`, made on first use (callers
 // hold g_mu).
 int find_workspace(cudaStream_t stream, Workspace** out) {
-    static std::map<WsKey, std::unique_ptr<Workspace>> all;
     int dev = 0;
     NEGF_CUDA(cudaGetDevice(&dev));
-    std::unique_ptr<Workspace>& w = all[WsKey{dev, stream}];
+    std::unique_ptr<Workspace>& w = workspaces()[WsKey{dev, stream}];
     if (!w) {
         w.reset(new Workspace());
         w->device = dev;
@@ -1685,9 +1689,10 @@ int negf_set_timing(int enable) {
     return NEGF_OK;
 }
 
-int negf_last_stats(negf_stats* s) {
-    if (!s) return fail(NEGF_ERR_ARG, "null argument");
-    std::lock_guard<std::mutex> lk(g_mu);
+namespace {
+// Kernel times of the last timed charge call, read from its workspace's
+// events into the statistics (callers hold g_mu).
+int collect_stats_times() {
     Settings& G = settings();
     if (Workspace* W = G.stats_ws) {
         NEGF_CUDA(cudaEventSynchronize(W->ev[2]));
@@ -1701,9 +1706,36 @@ int negf_last_stats(negf_stats* s) {
         G.stats.reduce_kernel_ms = b;
         G.stats_ws = nullptr;
     }
-    *s = G.stats;
     return NEGF_OK;
 }
+}  // namespace
+
+int negf_release_scratch(void* stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int dev = 0;
+    NEGF_CUDA(cudaGetDevice(&dev));
+    auto& all = workspaces();
+    auto it = all.find(WsKey{dev, (cudaStream_t)stream});
+    if (it == all.end()) return NEGF_OK;
+    Workspace* w = it->second.get();
+    // the last call's kernels (and the FP32 warps it ran on the side stream,
+    // joined before `done`) must be finished before their buffers go
+    if (w->used) NEGF_CUDA(cudaEventSynchronize(w->done));
+    // the kernel times of a timed last call are read before its events go
+    if (settings().stats_ws == w)
+        if (int rc = collect_stats_times()) return rc;
+    all.erase(it);
+    return NEGF_OK;
+}
+
+int negf_last_stats(negf_stats* s) {
+    if (!s) return fail(NEGF_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (int rc = collect_stats_times()) return rc;
+    *s = settings().stats;
+    return NEGF_OK;
+}
+
 
 // ------------------------------------------------------------------ Broyden
 int negf_broyden_create(int S, int max_step, double fraction, int norm_type, negf_broyden** out) {

@@ -370,6 +370,13 @@ def compute_charge(tubes: Sequence[CNT], out=None, stream=None):
     return out
 
 
+def release_scratch(stream=None):
+    """negf_release_scratch: hand back the device scratch that the charge
+    calls keep for the current device and `stream` (reallocated by the next
+    call on that stream)."""
+    check(_lib.load().negf_release_scratch(_stream(stream)), "negf_release_scratch")
+
+
 def last_stats() -> dict:
     s = _lib.Stats()
     check(_lib.load().negf_last_stats(C.byref(s)), "negf_last_stats")

@@ -16,8 +16,9 @@
  *   - one handle is not thread-safe; distinct handles are independent.
  *     Charge calls keep their device scratch per (device, stream): calls
  *     on different streams or devices never share scratch, and calls on one
- *     stream reuse it in stream order.  Each stream's scratch is held until
- *     the process exits (it grows to the largest problem seen on it).
+ *     stream reuse it in stream order.  Each stream's scratch grows to the
+ *     largest problem seen on it and is held until negf_release_scratch()
+ *     or process exit.
  *   - every tube of a call must live on the current device (NEGF_ERR_ARG).
  *   - reductions are deterministic: the same inputs give bitwise-identical
  *     charge on the same GPU and launch configuration.
@@ -175,6 +176,17 @@ int negf_compute_charge(negf_tube* const* tubes, int num_tubes, double* Q, int q
  * before any stream capture.  All calls share the array: calls that overlap
  * on the GPU race and must be serialised by the caller. */
 int negf_compute_charge_noalloc(negf_tube* const* tubes, int num_tubes, double* d_Q, void* stream);
+
+/* Frees the device scratch (launch tables, partial rows, checkpoints) that
+ * negf_compute_charge and negf_rs_compute_charge keep for the current device
+ * and `stream`, after waiting for the last call made on it; the next call on
+ * that stream allocates it again.  No counterpart in the reference, whose
+ * charge routines allocate and free their device vectors on every call; here
+ * the scratch is kept between calls (a self-consistent loop reuses it every
+ * iteration) and this call hands it back, e.g. before destroying `stream` or
+ * after the last solve of a sweep.  A stream with no scratch is a no-op.
+ * Charge plans and the allocation-free entry point are not affected. */
+int negf_release_scratch(void* stream);
 
 /* Per-call timing and work counters of the last negf_compute_charge
  * (kernel milliseconds measured with CUDA events on `stream`). */

@@ -52,3 +52,42 @@ def test_two_streams_distinct_tubes_match_oracle(negf_lib, oracle):
     errA = _rel(QA.cpu().numpy(), cases[0][1])
     errB = _rel(QB.cpu().numpy(), cases[1][1])
     assert errA <= FP64_TOL and errB <= FP64_TOL, (errA, errB)
+
+
+def test_release_scratch_frees_and_next_call_reallocates(negf_lib, oracle):
+    """negf_release_scratch hands a stream's scratch back to the device (the
+    free memory grows by at least the checkpoint bytes of the last call) and
+    the next call on that stream allocates it again and gives the same charge,
+    bitwise, with the kernel times of a timed call still readable."""
+    import torch
+    from electrostatic_b200.negf import CNT, compute_charge, last_stats, release_scratch, set_timing
+    from electrostatic_b200.workloads import site_potential
+
+    g = CNT(**CASE_A)
+    U = site_potential(g.site_positions(), 91)
+    g.set_potential(U, (U[0], U[-1]))
+    o = oracle.OracleTube(**CASE_A)
+    o.set_potential(U, (U[0], U[-1]))
+    Qo = o.charge(nthreads=8)
+    s = torch.cuda.Stream()
+    Q1 = torch.zeros(g.num_field_sites, dtype=torch.float64, device="cuda")
+    Q2 = torch.zeros_like(Q1)
+    set_timing(True)
+    try:
+        compute_charge([g], out=Q1, stream=s)
+        scratch = last_stats()["checkpoint_bytes"]
+        compute_charge([g], out=Q1, stream=s)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        release_scratch(s)  # the timed call's events go with the workspace
+        free_after = torch.cuda.mem_get_info()[0]
+        st = last_stats()
+    finally:
+        set_timing(False)
+    assert st["rgf_kernel_ms"] > 0.0
+    assert free_after - free_before >= scratch // 2, (free_before, free_after, scratch)
+    release_scratch(s)  # nothing left on that stream: a no-op
+    compute_charge([g], out=Q2, stream=s)
+    torch.cuda.synchronize()
+    assert torch.equal(Q1, Q2)
+    assert _rel(Q2.cpu().numpy(), Qo) <= FP64_TOL
