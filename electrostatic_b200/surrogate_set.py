@@ -62,14 +62,11 @@ Richardson step for a spectrum in [1, 1 + lambda_max] (measured on the
 """
 from __future__ import annotations
 
-import ctypes as C
 import math
 import time
 
 import numpy as np
 
-from . import _lib
-from ._lib import check
 from .surrogate import MODES, WIN, FourierOperator
 
 FEAT_SET = 40

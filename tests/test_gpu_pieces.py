@@ -1,7 +1,6 @@
 """Parallel-in-length pass 1: the sweeps of every chain split into pieces
 (transfer matrices, prefix over the pieces, piece sweeps) give the charge of
 the single sweep."""
-import numpy as np
 import pytest
 
 from test_gpu_parity import CASES, _pair, _rel
