@@ -91,6 +91,35 @@ def test_config3_realspace_matches_block_oracle(negf_lib, config3, precision, to
     assert err <= tol, err
 
 
+def test_config3_biased_realspace_matches_mode_space_and_oracle(negf_lib, oracle):
+    """The config-3 tube at a 0.3 V drain bias (contacts at -0.8 / -1.1 eV,
+    3072 real-axis points at 1e-4 eV broadening, the biased workload bench.py
+    times): the real-space pass, whose source and drain columns of G travel
+    through 600 ring blocks, equals the mode-space pass over all 7 modes and
+    the oracle's mode-space charge (equal for this ring-uniform potential).
+    At this broadening the block products on the real axis are differences of
+    large terms: a mirrored (assumed symmetric) product tile moved this charge
+    by 40x its size, which the small biased cases did not show."""
+    from electrostatic_b200.negf import CNT
+    from electrostatic_b200.workloads import SEED_BASE, config3_kwargs, site_potential
+    kw = config3_kwargs()
+    kw.pop("precision")
+    kb = dict(kw, contact_mu=(-0.8, -1.1), noneq_integration_pts=(3072,), E_zPlus_imag=1e-4)
+    g = CNT(**kb)
+    assert g.num_field_sites == 1200
+    U = site_potential(g.site_positions(), SEED_BASE + 3)
+    g.set_potential(U, (U[0], U[-1]))
+    assert g.noneq()
+    Qr = g.realspace_charge()
+    Qm = g.Solve_NEGF()
+    o = oracle.OracleTube(**_oracle_kwargs(kb))
+    o.set_potential(U, (U[0], U[-1]))
+    Qo = o.charge(nthreads=THREADS)
+    err_m, err_o = _rel(Qr, Qm), _rel(Qr, Qo)
+    print(f"config 3 biased: real space vs mode space {err_m:.3e}, vs oracle {err_o:.3e}")
+    assert err_m <= FP64_TOL and err_o <= FP64_TOL, (err_m, err_o)
+
+
 @pytest.fixture(scope="module")
 def config4(oracle):
     from electrostatic_b200.workloads import SEED_BASE, site_potential, uneven_batch
