@@ -46,6 +46,7 @@ def test_compute_fails_loudly_without_device(negf_lib):
     assert b"CUDA" in negf_lib.negf_last_error() or b"device" in negf_lib.negf_last_error()
     b = C.c_void_p()
     assert negf_lib.negf_broyden_create(10, 20, 0.1, 0, C.byref(b)) == -2
+    assert negf_lib.negf_release_scratch(None) == -2
 
 
 def test_argument_errors(negf_lib):
