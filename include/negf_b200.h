@@ -185,6 +185,7 @@ int negf_compute_charge_noalloc(negf_tube* const* tubes, int num_tubes, double* 
  * the scratch is kept between calls (a self-consistent loop reuses it every
  * iteration) and this call hands it back, e.g. before destroying `stream` or
  * after the last solve of a sweep.  A stream with no scratch is a no-op.
+ * It waits on the host, so it is not for a stream that is being captured.
  * Charge plans and the allocation-free entry point are not affected. */
 int negf_release_scratch(void* stream);
 
