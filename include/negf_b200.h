@@ -181,10 +181,13 @@ int negf_compute_charge_noalloc(negf_tube* const* tubes, int num_tubes, double* 
  * negf_compute_charge and negf_rs_compute_charge keep for the current device
  * and `stream`, after waiting for the last call made on it; the next call on
  * that stream allocates it again.  No counterpart in the reference, whose
- * charge routines allocate and free their device vectors on every call; here
- * the scratch is kept between calls (a self-consistent loop reuses it every
- * iteration) and this call hands it back, e.g. before destroying `stream` or
- * after the last solve of a sweep.  A stream with no scratch is a no-op.
+ * device tables are members of each nanostructure object (Allocate_Arrays,
+ * NEGF_Common.cpp:1421-1653, called from Initialize_NEGF; freed with the
+ * object); here
+ * the scratch belongs to the (device, stream) pair, not to a tube, is kept
+ * between calls (a self-consistent loop reuses it every iteration), and this
+ * call hands it back, e.g. before destroying `stream` or after the last
+ * solve of a sweep.  A stream with no scratch is a no-op.
  * It waits on the host, so it is not for a stream that is being captured.
  * Charge plans and the allocation-free entry point are not affected. */
 int negf_release_scratch(void* stream);
